@@ -1,0 +1,422 @@
+#!/usr/bin/env python3
+"""Benchmark: CNAB2 steps/s of the full MHD shell step at lmax=255, nr=129
+(nlat=384, nlon=768; fields u_tor, u_pol, B_tor, B_pol, T), graph-captured on
+one B200 per rank.
+
+One "step" is step_once! (scripts/bench_timestepping.jl:6-18): temperature,
+velocity and magnetic nonlinear terms (4 scalar + 4 vector syntheses, 1 scalar
++ 2 vector analyses, the grid products) and the five CNAB2 banded solves.
+
+Arms:
+  default            this package through its C ABI (libgdb200.so)
+  --impl reference   the FP64 CPU restatement of the reference step (oracle/),
+                     timed on the host cores on a bounded sample (nr = 9 of the
+                     129 shells, scaled by 129/9; every kernel of the step is
+                     linear in the shell count).
+
+Multi-GPU (torchrun): the step does not shard without a transpose, so every
+rank runs an independent replica of the same workload ("replicas only", weak
+scaling); value = N x steps / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "geodynamo.jl_b200"))
+
+METRIC = "CNAB2 steps/s lmax255 nr129: mixed-prec vs FP64 GPU at 1e-9 energy err"
+WORKLOAD = "shell_l255_nr129"
+CPU_SAMPLE_NR = 9
+
+
+def load_package():
+    import importlib.util
+    if "gdb200" in sys.modules:
+        return sys.modules["gdb200"]
+    pkg_dir = os.path.join(ROOT, "geodynamo.jl_b200")
+    spec = importlib.util.spec_from_file_location("gdb200", os.path.join(pkg_dir, "__init__.py"),
+                                                  submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["gdb200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_params():
+    import workloads
+    c = dict(workloads.CONFIGS[WORKLOAD])
+    c.update(workloads.SHELL_PHYSICS)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work per kernel launch (bytes or flops), for the roofline
+# ---------------------------------------------------------------------------
+def kernel_work(name, p, nlm, precision):
+    L, nlat, nlon, nr = p["lmax"], p["nlat"], p["nlon"], p["nr"]
+    G = nlat * nlon * nr                      # grid points per field
+    F = nr * (L + 1) * nlat                   # Fourier coefficients per component
+    S = 2 * nr * nlm                          # spectral doubles per field
+    rb = 8 if precision == "fp64" else 4      # grid real bytes
+    cb = 2 * rb                               # Fourier complex bytes
+    legendre = {
+        # (flops per launch, launches per step are counted live)
+        "legendre_synth_scalar": 2.0 * nlm * nlat * nr * 4,
+        "legendre_synth_vector": 8.0 * nlm * nlat * nr,
+        "legendre_analysis_scalar": 2.0 * nlm * nlat * nr,
+        "legendre_analysis_vector": 8.0 * nlm * nlat * nr,
+    }
+    for k, v in legendre.items():
+        if name.startswith(k):
+            return ("flops", v)
+    if name.startswith("fft_synth"):
+        return None  # component count varies per launch (4 or 2); handled by caller
+    table = {
+        "nl_temperature": 6 * G * rb,
+        "nl_velocity": 10 * G * rb,
+        "nl_induction": 6 * G * rb,
+        "cnab2_solve": 5 * 5 * S * 8,
+        "spectral_gradients": 4 * S * 8,
+        "spectral_curl": 4 * S * 8,
+        "temperature_bc": 4 * nlm * 8,
+    }
+    for k, v in table.items():
+        if name.startswith(k):
+            return ("bytes", v)
+    return None
+
+
+def fft_bytes(p, ncomp, precision):
+    L, nlat, nlon, nr = p["lmax"], p["nlat"], p["nlon"], p["nr"]
+    rb = 8 if precision == "fp64" else 4
+    return ncomp * (nr * (L + 1) * nlat * 2 * rb + nr * nlat * nlon * rb)
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(steps, warmup, threads=None):
+    """Oracle steps/s at lmax=255 (sample of nr = 9 shells, scaled to 129)."""
+    from oracle.oracle import Oracle
+    import workloads
+    p = workload_params()
+    nr = CPU_SAMPLE_NR
+    o = Oracle(lmax=p["lmax"], nlat=p["nlat"], nlon=p["nlon"], nr=nr, dt=p["dt"], threads=threads)
+    for k, (a, b) in workloads.seeded_state(p["lmax"], p["lmax"], nr, seed=0).items():
+        o.set_field(k, a, b)
+    for _ in range(warmup):
+        o.step(1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(1)
+    dt = (time.perf_counter() - t0) / steps
+    full = dt * p["nr"] / nr
+    return 1.0 / full, dt, os.cpu_count() if threads is None else threads
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, 3))
+    warm = 1
+    rate, dt_sample, cores = cpu_reference_rate(steps, warm)
+    sample = (f"oracle (C++ FP64 restatement of step_once!) at lmax=255 nlat=384 nlon=768 on nr={CPU_SAMPLE_NR} "
+              f"of 129 shells, {steps} timed steps after {warm} warm-up, {dt_sample:.3f} s per sample step, "
+              f"scaled by 129/{CPU_SAMPLE_NR}")
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 / rate, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, default_rng(0))",
+            "config": {"workload": WORKLOAD, "lmax": 255, "nlat": 384, "nlon": 768, "nr": 129},
+            "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--accuracy-steps", type=int, default=100,
+                    help="steps of the FP64 vs mixed energy comparison (0 = skip)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    gdb = load_package()
+    import workloads
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    p = workload_params()
+    st = workloads.seeded_state(p["lmax"], p["lmax"], p["nr"], seed=0)
+
+    def make(precision):
+        g = gdb.SHTnsKitConfig(p["lmax"], p["nlat"], p["nlon"], p["nr"], dt=p["dt"], rratio=p["rratio"],
+                               ekman=p["ekman"], rayleigh=p["rayleigh"], prandtl=p["prandtl"],
+                               magnetic_prandtl=p["magnetic_prandtl"], implicit_theta=p["implicit_theta"],
+                               precision="fp64", device=local)
+        if precision == "mixed":
+            g.set_precision("mixed")
+        for k, (a, b) in st.items():
+            g.set_field(k, a, b)
+        return g
+
+    precision = args.precision
+    if precision == "auto":
+        try:
+            probe = gdb.SHTnsKitConfig(7, 12, 24, 9, device=local)
+            probe.set_precision("mixed")
+            probe.close()
+            precision = "mixed"
+        except gdb.GeoDynamoError:
+            precision = "fp64"
+
+    def timed_steps(g, K, W):
+        ext = torch.cuda.ExternalStream(g.stream_ptr())
+        g.step(W)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        g.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        g.step_async(K)
+        e1.record(ext)
+        e1.synchronize()
+        g.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # ---- main timed region ----
+    g = make(precision)
+    clocks = ClockSampler(local)
+    g.step(args.warmup)
+    clocks.start()
+    ms_total = timed_steps(g, args.steps, 0)
+    clk = clocks.stop()
+    value = world * args.steps / (ms_total / 1e3)
+    ms_per_step = ms_total / args.steps
+
+    # ---- per-kernel breakdown (events around each launch, eager replay) ----
+    g.profile_enable(True)
+    nprof = 2
+    g.step(nprof)
+    prof = g.profile_read()
+    g.profile_enable(False)
+    kernels = []
+    for name, (ms, cnt) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
+        per = ms / cnt
+        w = kernel_work(name, p, g.nlm, precision)
+        ent = {"name": name, "share": None, "launches_per_step": cnt / nprof, "ms_per_launch": per}
+        if name.startswith("fft_"):
+            # 4-component synth launches and 2-component ones share a name; use the per-step mix
+            ncomp = (4 + 2 * 4) if "synth" in name else (1 + 2 + 2)
+            ent["gbs"] = fft_bytes(p, ncomp, precision) / (ms / nprof / 1e3) / 1e9
+        elif w is not None:
+            kind, amount = w
+            if kind == "flops":
+                ent["tflops"] = amount / (per / 1e3) / 1e12
+            else:
+                ent["gbs"] = amount / (per / 1e3) / 1e9
+        kernels.append(ent)
+    tot = sum(v[0] for v in prof.values())
+    for ent in kernels:
+        ent["share"] = prof[ent["name"]][0] / tot if tot else None
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    top = kernels[0] if kernels else None
+    roofline = None
+    if top is not None:
+        if "gbs" in top:
+            roofline = {"kernel": top["name"], "bound": "hbm", "achieved": top["gbs"], "peak": hbm_peak,
+                        "unit": "GB/s", "frac": top["gbs"] / hbm_peak, "traffic": None,
+                        "peak_source": peak_src}
+        elif "tflops" in top:
+            if top["name"].endswith("fp64"):
+                pk, src = 40.0, "nominal FP64 tensor (no measured FP64 peak on this pool)"
+            else:
+                pk, src = peaks.get("bf16_tflops", 1590.0) / 2.0, "half the measured bf16 peak (tf32 rate)"
+            roofline = {"kernel": top["name"], "bound": "tensor", "achieved": top["tflops"], "peak": pk,
+                        "unit": "TFLOP/s", "frac": top["tflops"] / pk, "traffic": None, "peak_source": src}
+
+    # ---- FP64 reference step on the GPU (denominator of the metric) ----
+    fp64_value = None
+    if precision == "mixed":
+        g64 = make("fp64")
+        g64.step(args.warmup)
+        ms64 = timed_steps(g64, args.steps, 0)
+        fp64_value = world * args.steps / (ms64 / 1e3)
+        g64.close()
+    else:
+        fp64_value = value
+
+    # ---- energy agreement, mixed vs FP64 ----
+    accuracy = None
+    if precision == "mixed" and args.accuracy_steps > 0:
+        ga = make("mixed")
+        gb = make("fp64")
+        ga.step(args.accuracy_steps)
+        gb.step(args.accuracy_steps)
+        ea, eb = ga.energy(), gb.energy()
+        accuracy = {"steps": args.accuracy_steps,
+                    "ekin_rel_err": abs(ea[0] - eb[0]) / abs(eb[0]),
+                    "emag_rel_err": abs(ea[1] - eb[1]) / abs(eb[1]),
+                    "ekin_fp64": eb[0], "emag_fp64": eb[1]}
+        ga.close(); gb.close()
+
+    # ---- end to end through the C ABI with host buffers ----
+    names = list(workloads.FIELD_ORDER)
+    pinned = {}
+    for k in names:
+        a, b = st[k]
+        ta = torch.from_numpy(a).pin_memory()
+        tb = torch.from_numpy(b).pin_memory()
+        pinned[k] = (ta, tb)
+    out_pinned = {k: (torch.empty(st[k][0].shape, dtype=torch.float64).pin_memory(),
+                      torch.empty(st[k][1].shape, dtype=torch.float64).pin_memory()) for k in names}
+    import ctypes
+    lib = g.lib
+    D = ctypes.POINTER(ctypes.c_double)
+    ptr = lambda t: ctypes.cast(t.data_ptr(), D)  # noqa: E731
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in names:
+        g._check(lib.gd_upload_spectral(g.h, gdb.FIELDS[k], ptr(pinned[k][0]), ptr(pinned[k][1])))
+    g.step_async(args.steps)
+    ek, em = g.energy()
+    for k in names:
+        g._check(lib.gd_download_spectral(g.h, gdb.FIELDS[k], ptr(out_pinned[k][0]), ptr(out_pinned[k][1])))
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    state_bytes = sum(a.nbytes + b.nbytes for a, b in st.values())
+    e2e = {"value": world * args.steps / e2e_s, "unit": "steps/s",
+           "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": (state_bytes + 16) / args.steps,
+           "job": f"upload 5 fields from pinned host memory, {args.steps} graph steps, energies and 5 fields back"}
+
+    # ---- CPU baseline (rank 0, N = 1) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, dts, cores = cpu_reference_rate(1, 1)
+        cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port",
+               "sample": f"oracle at lmax=255 nlat=384 nlon=768 nr={CPU_SAMPLE_NR} (of 129 shells), 1 timed step "
+                         f"after 1 warm-up ({dts:.3f} s), scaled by 129/{CPU_SAMPLE_NR}"}
+
+    gpu_launches = sum(int(round(cnt / nprof)) for _, cnt in prof.values()) * args.steps
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32/tf32x3 (FP64 solves)",
+                "data": "synthetic (seeded default_rng(0) state, amplitude 1e-3 (l+1)^-2)",
+                "config": {"workload": WORKLOAD, "lmax": 255, "nlat": 384, "nlon": 768, "nr": 129,
+                           "dt": p["dt"], "precision": precision, "parallelism": f"replicas x{world}",
+                           "l2": "working set 5+ GB of grids per step, larger than L2; no flush"},
+                "fp64_gpu_value": fp64_value, "ratio_vs_fp64_gpu": value / fp64_value if fp64_value else None,
+                "accuracy": accuracy, "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,510 @@
+"""Host-side mirror of GeoDynamo.jl's transform / nonlinear / timestep API over
+libgdb200.so (the sm_100a kernels of this package, reached through the C ABI in
+``include/gdb200.h``).
+
+The functions keep the reference's names, argument meaning and in-place
+behaviour (Julia's ``!`` suffix dropped):
+
+=====================================  ==============================================
+reference (src/...)                    here
+=====================================  ==============================================
+create_shtnskit_config (shtnskit_transforms.jl:102)   :func:`create_shtnskit_config`
+shtnskit_spectral_to_physical! (shtnskit_field_functions.jl:11)  :func:`shtnskit_spectral_to_physical`
+shtnskit_physical_to_spectral! (:131)  :func:`shtnskit_physical_to_spectral`
+shtnskit_vector_synthesis! (:252)      :func:`shtnskit_vector_synthesis`
+shtnskit_vector_analysis! (:291)       :func:`shtnskit_vector_analysis`
+batch_spectral_to_physical! (:674)     :func:`batch_spectral_to_physical`
+compute_temperature_nonlinear! (thermal.jl:149)  :func:`compute_temperature_nonlinear`
+compute_velocity_nonlinear! (velocity.jl:312)    :func:`compute_velocity_nonlinear`
+compute_magnetic_nonlinear! (magnetic.jl:131)    :func:`compute_magnetic_nonlinear`
+apply_master_implicit_step! (simulation.jl:1151) :func:`apply_master_implicit_step`
+step_once! (scripts/bench_timestepping.jl:6)     :func:`step_once`
+compute_kinetic_energy / compute_magnetic_energy :func:`compute_kinetic_energy`, ...
+=====================================  ==============================================
+
+Errors raise :class:`GeoDynamoError` (the reference raises Julia exceptions).
+There is no CPU fallback: if ``libgdb200.so`` is missing or no CUDA device is
+present, every call that needs the device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libgdb200.so")
+_CSRC = os.path.join(_HERE, "csrc")
+
+GD_OK = 0
+STATUS_NAMES = {0: "GD_OK", 1: "GD_ERR_ARG", 2: "GD_ERR_CONFIG", 3: "GD_ERR_CUDA", 4: "GD_ERR_NONFINITE",
+                5: "GD_ERR_SINGULAR", 6: "GD_ERR_UNSUPPORTED", 7: "GD_ERR_STATE"}
+FIELDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4}
+GRIDS = {
+    "u_th": 0, "u_ph": 1, "w_th": 2, "w_ph": 3, "b_th": 4, "b_ph": 5, "j_th": 6, "j_ph": 7,
+    "t": 8, "gth": 9, "gph": 10, "gr": 11, "tadv": 12, "vadv_th": 13, "vadv_ph": 14,
+    "ind_th": 15, "ind_ph": 16,
+}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+# Every symbol include/gdb200.h declares.
+EXPORTS = (
+    "gd_create", "gd_destroy", "gd_last_error", "gd_info", "gd_grid", "gd_set_precision", "gd_synchronize",
+    "gd_upload_spectral", "gd_download_spectral", "gd_download_nonlinear", "gd_download_grid",
+    "gd_set_temperature_bc", "gd_spectral_to_physical", "gd_physical_to_spectral", "gd_vector_synthesis",
+    "gd_vector_analysis", "gd_temperature_nonlinear", "gd_velocity_nonlinear", "gd_magnetic_nonlinear",
+    "gd_implicit_step", "gd_step", "gd_step_async", "gd_set_dt", "gd_energy", "gd_check_finite",
+    "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
+)
+
+
+class GeoDynamoError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class GDConfig(ctypes.Structure):
+    """``gd_config`` of include/gdb200.h (GeoDynamoParameters subset)."""
+    _fields_ = [
+        ("lmax", ctypes.c_int), ("mmax", ctypes.c_int), ("nlat", ctypes.c_int),
+        ("nlon", ctypes.c_int), ("nr", ctypes.c_int), ("kl", ctypes.c_int),
+        ("rratio", ctypes.c_double), ("ekman", ctypes.c_double), ("rayleigh", ctypes.c_double),
+        ("prandtl", ctypes.c_double), ("magnetic_prandtl", ctypes.c_double),
+        ("dt", ctypes.c_double), ("implicit_theta", ctypes.c_double),
+        ("ab_mode", ctypes.c_int), ("bc_mode", ctypes.c_int), ("fd_mode", ctypes.c_int),
+        ("precision", ctypes.c_int), ("magnetic", ctypes.c_int),
+    ]
+
+
+def build(verbose: bool = False) -> str:
+    """Compile libgdb200.so for sm_100a in-tree (nvcc cross-compiles without a GPU)."""
+    out = subprocess.run(["make", "-C", _CSRC, "-j8"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("libgdb200 build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])
+    if verbose:
+        print(out.stdout[-2000:])
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def load_library():
+    """Load libgdb200.so and declare its signatures; raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise GeoDynamoError(6, f"{_LIB_PATH} is missing; run geodynamo build() first")
+    lib = ctypes.CDLL(_LIB_PATH)
+    P = ctypes.c_void_p
+    D = ctypes.POINTER(ctypes.c_double)
+    I = ctypes.c_int
+    sigs = {
+        "gd_create": ([ctypes.POINTER(GDConfig), I, ctypes.POINTER(P)], I),
+        "gd_destroy": ([P], I),
+        "gd_last_error": ([P], ctypes.c_char_p),
+        "gd_info": ([P, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_size_t)], I),
+        "gd_grid": ([P, D, D, D], I),
+        "gd_set_precision": ([P, I], I),
+        "gd_synchronize": ([P], I),
+        "gd_upload_spectral": ([P, I, D, D], I),
+        "gd_download_spectral": ([P, I, D, D], I),
+        "gd_download_nonlinear": ([P, I, D, D], I),
+        "gd_download_grid": ([P, I, D], I),
+        "gd_set_temperature_bc": ([P, D, D], I),
+        "gd_spectral_to_physical": ([P, I, D, D, D], I),
+        "gd_physical_to_spectral": ([P, I, D, D, D], I),
+        "gd_vector_synthesis": ([P, D, D, D, D, D, D], I),
+        "gd_vector_analysis": ([P, D, D, D, D, D, D], I),
+        "gd_temperature_nonlinear": ([P], I),
+        "gd_velocity_nonlinear": ([P], I),
+        "gd_magnetic_nonlinear": ([P], I),
+        "gd_implicit_step": ([P], I),
+        "gd_step": ([P, I], I),
+        "gd_step_async": ([P, I], I),
+        "gd_set_dt": ([P, ctypes.c_double], I),
+        "gd_energy": ([P, D, D], I),
+        "gd_check_finite": ([P], I),
+        "gd_step_count": ([P], ctypes.c_long),
+        "gd_get_stream": ([P, ctypes.POINTER(P)], I),
+        "gd_profile_enable": ([P, I], I),
+        "gd_profile_read": ([P, I, ctypes.c_char_p, D, ctypes.POINTER(I), ctypes.POINTER(I)], I),
+    }
+    for name, (args, res) in sigs.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _dptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise GeoDynamoError(1, "arrays must be C-contiguous float64")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def lm_pairs(lmax: int, mmax: int):
+    """(l, m) per l-major index (``shtnskit_transforms.jl:177-188``)."""
+    return [(l, m) for l in range(lmax + 1) for m in range(min(l, mmax) + 1)]
+
+
+def index_to_lm_shtnskit(idx: int, lmax: int, mmax: int):
+    """1-based index -> (l, m) (``shtnskit_field_functions.jl:450-462``), in O(1)."""
+    q = idx - 1
+    if q < 0:
+        return (0, 0)
+    full = (mmax + 1) * (mmax + 2) // 2
+    if q < full:
+        l = int((np.sqrt(8 * q + 1) - 1) // 2)
+        while (l + 1) * (l + 2) // 2 <= q:
+            l += 1
+        while l * (l + 1) // 2 > q:
+            l -= 1
+        return (l, q - l * (l + 1) // 2)
+    rest = q - full
+    l = mmax + 1 + rest // (mmax + 1)
+    if l > lmax:
+        return (0, 0)
+    return (l, rest % (mmax + 1))
+
+
+class SHTnsKitConfig:
+    """Grid and handle of one transform / model configuration.
+
+    Mirrors ``SHTnsKitConfig`` (``shtnskit_transforms.jl:61-93``): lmax, mmax,
+    nlat, nlon, nlm, l_values, m_values, theta_grid, phi_grid, gauss_weights.
+    The device handle also owns the model state used by the step functions.
+    """
+
+    def __init__(self, lmax, nlat, nlon, nr, mmax=None, kl=4, rratio=0.35, ekman=3e-4, rayleigh=80.0,
+                 prandtl=1.0, magnetic_prandtl=4.0, dt=1e-5, implicit_theta=0.5, ab_mode=0, bc_mode=0,
+                 fd_mode=0, precision="fp64", magnetic=1, device=0):
+        self.lib = load_library()
+        mmax = lmax if mmax is None else mmax
+        self.cfg = GDConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl, magnetic_prandtl,
+                            dt, implicit_theta, ab_mode, bc_mode, fd_mode, PRECISIONS[precision], magnetic)
+        h = ctypes.c_void_p()
+        st = self.lib.gd_create(ctypes.byref(self.cfg), int(device), ctypes.byref(h))
+        if st != GD_OK:
+            raise GeoDynamoError(st, "gd_create failed (see stderr)")
+        self.h = h
+        self.lmax, self.mmax, self.nlat, self.nlon, self.nr = lmax, mmax, nlat, nlon, nr
+        n = ctypes.c_int()
+        b = ctypes.c_size_t()
+        self._check(self.lib.gd_info(self.h, ctypes.byref(n), ctypes.byref(b)))
+        self.nlm = n.value
+        pairs = lm_pairs(lmax, mmax)
+        self.l_values = np.array([p[0] for p in pairs])
+        self.m_values = np.array([p[1] for p in pairs])
+        th = np.zeros(nlat); w = np.zeros(nlat); r = np.zeros(nr)
+        self._check(self.lib.gd_grid(self.h, _dptr(th), _dptr(w), _dptr(r)))
+        self.theta_grid, self.gauss_weights, self.r = th, w, r
+        self.phi_grid = 2 * np.pi * np.arange(nlon) / nlon
+        self.precision = precision
+
+    # -- plumbing -------------------------------------------------------------
+    def _check(self, st):
+        if st != GD_OK:
+            msg = self.lib.gd_last_error(self.h).decode() if getattr(self, "h", None) else ""
+            raise GeoDynamoError(st, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_bytes(self):
+        n = ctypes.c_int(); b = ctypes.c_size_t()
+        self._check(self.lib.gd_info(self.h, ctypes.byref(n), ctypes.byref(b)))
+        return b.value
+
+    def set_precision(self, precision):
+        self._check(self.lib.gd_set_precision(self.h, PRECISIONS[precision]))
+        self.precision = precision
+
+    def spec_shape(self):
+        return (self.nr, self.nlm)
+
+    def grid_shape(self):
+        return (self.nr, self.nlon, self.nlat)
+
+    # -- raw transforms on numpy arrays in the reference layout ------------------
+    def synth_scalar(self, re, im):
+        re = _f64(re); im = _f64(im)
+        nf = re.size // (self.nr * self.nlm)
+        out = np.zeros((nf,) + self.grid_shape()) if re.ndim == 3 else np.zeros(self.grid_shape())
+        self._check(self.lib.gd_spectral_to_physical(self.h, nf, _dptr(re), _dptr(im), _dptr(out)))
+        return out
+
+    def analysis_scalar(self, grid):
+        grid = _f64(grid)
+        nf = grid.size // (self.nr * self.nlat * self.nlon)
+        shape = ((nf,) + self.spec_shape()) if grid.ndim == 4 else self.spec_shape()
+        re = np.zeros(shape); im = np.zeros(shape)
+        self._check(self.lib.gd_physical_to_spectral(self.h, nf, _dptr(grid), _dptr(re), _dptr(im)))
+        return re, im
+
+    def synth_vector(self, tre, tim, pre, pim):
+        vt = np.zeros(self.grid_shape()); vp = np.zeros(self.grid_shape())
+        self._check(self.lib.gd_vector_synthesis(self.h, _dptr(_f64(tre)), _dptr(_f64(tim)), _dptr(_f64(pre)),
+                                                 _dptr(_f64(pim)), _dptr(vt), _dptr(vp)))
+        return vt, vp
+
+    def analysis_vector(self, vt, vp):
+        out = [np.zeros(self.spec_shape()) for _ in range(4)]
+        self._check(self.lib.gd_vector_analysis(self.h, _dptr(_f64(vt)), _dptr(_f64(vp)), *[_dptr(o) for o in out]))
+        return out
+
+    # -- model state ------------------------------------------------------------
+    def set_field(self, name, re, im):
+        self._check(self.lib.gd_upload_spectral(self.h, FIELDS[name], _dptr(_f64(re)), _dptr(_f64(im))))
+
+    def get_field(self, name):
+        re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
+        self._check(self.lib.gd_download_spectral(self.h, FIELDS[name], _dptr(re), _dptr(im)))
+        return re, im
+
+    def get_nl(self, name):
+        re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
+        self._check(self.lib.gd_download_nonlinear(self.h, FIELDS[name], _dptr(re), _dptr(im)))
+        return re, im
+
+    def get_grid(self, name):
+        g = np.zeros(self.grid_shape())
+        self._check(self.lib.gd_download_grid(self.h, GRIDS[name], _dptr(g)))
+        return g
+
+    def set_temperature_bc(self, bvals=None, sources=None):
+        self._check(self.lib.gd_set_temperature_bc(
+            self.h, _dptr(_f64(bvals)) if bvals is not None else None,
+            _dptr(_f64(sources)) if sources is not None else None))
+
+    def temperature_nl(self):
+        self._check(self.lib.gd_temperature_nonlinear(self.h))
+
+    def velocity_nl(self):
+        self._check(self.lib.gd_velocity_nonlinear(self.h))
+
+    def magnetic_nl(self):
+        self._check(self.lib.gd_magnetic_nonlinear(self.h))
+
+    def implicit_step(self):
+        self._check(self.lib.gd_implicit_step(self.h))
+
+    def step(self, n=1):
+        self._check(self.lib.gd_step(self.h, int(n)))
+
+    def step_async(self, n=1):
+        self._check(self.lib.gd_step_async(self.h, int(n)))
+
+    def synchronize(self):
+        self._check(self.lib.gd_synchronize(self.h))
+
+    def set_dt(self, dt):
+        self._check(self.lib.gd_set_dt(self.h, float(dt)))
+
+    def energy(self):
+        ek = ctypes.c_double(); em = ctypes.c_double()
+        self._check(self.lib.gd_energy(self.h, ctypes.byref(ek), ctypes.byref(em)))
+        return ek.value, em.value
+
+    def check_finite(self):
+        self._check(self.lib.gd_check_finite(self.h))
+
+    def step_count(self):
+        return self.lib.gd_step_count(self.h)
+
+    def stream_ptr(self) -> int:
+        """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        p = ctypes.c_void_p()
+        self._check(self.lib.gd_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def profile_enable(self, on=True):
+        self._check(self.lib.gd_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self):
+        """{kernel name: (total ms, launches)} accumulated since the last read."""
+        mx = 64
+        names = ctypes.create_string_buffer(32 * mx)
+        ms = np.zeros(mx)
+        cnt = (ctypes.c_int * mx)()
+        n = ctypes.c_int()
+        self._check(self.lib.gd_profile_read(self.h, mx, names, _dptr(ms), cnt, ctypes.byref(n)))
+        out = {}
+        for k in range(min(n.value, mx)):
+            nm = names.raw[32 * k: 32 * k + 32].split(b"\0", 1)[0].decode()
+            out[nm] = (float(ms[k]), int(cnt[k]))
+        return out
+
+
+# ---------------------------------------------------------------------------
+# Reference-shaped field containers (src/fields.jl:6-32) and functions.
+# ---------------------------------------------------------------------------
+class SHTnsSpectralField:
+    """``SHTnsSpectralField``: Re/Im planes, shape (nr, nlm), l-major index fastest."""
+
+    def __init__(self, config: SHTnsKitConfig):
+        self.config = config
+        self.nlm = config.nlm
+        self.data_real = np.zeros(config.spec_shape())
+        self.data_imag = np.zeros(config.spec_shape())
+
+
+class SHTnsPhysicalField:
+    """``SHTnsPhysicalField``: shape (nr, nlon, nlat), theta fastest."""
+
+    def __init__(self, config: SHTnsKitConfig):
+        self.config = config
+        self.nlat, self.nlon = config.nlat, config.nlon
+        self.data = np.zeros(config.grid_shape())
+
+
+class SHTnsVectorField:
+    def __init__(self, config: SHTnsKitConfig):
+        self.r_component = SHTnsPhysicalField(config)
+        self.theta_component = SHTnsPhysicalField(config)
+        self.phi_component = SHTnsPhysicalField(config)
+
+
+def create_shtnskit_config(*, lmax, mmax=None, nlat=None, nlon=None, nr=64, **kw) -> SHTnsKitConfig:
+    """Defaults follow ``create_shtnskit_config`` (nlat = lmax + 2, nlon = max(2 lmax + 1, 4)),
+    rounded up to an even nlat and a 2/3/5-smooth nlon."""
+    mmax = lmax if mmax is None else mmax
+    if nlat is None:
+        nlat = lmax + 2
+        nlat += nlat & 1
+    if nlon is None:
+        nlon = max(2 * lmax + 1, 4)
+        while True:
+            m = nlon
+            for p in (2, 3, 5):
+                while m % p == 0:
+                    m //= p
+            if m == 1:
+                break
+            nlon += 1
+    return SHTnsKitConfig(lmax, nlat, nlon, nr, mmax=mmax, **kw)
+
+
+def create_shtns_spectral_field(config):
+    return SHTnsSpectralField(config)
+
+
+def create_shtns_physical_field(config):
+    return SHTnsPhysicalField(config)
+
+
+def create_shtns_vector_field(config):
+    return SHTnsVectorField(config)
+
+
+def shtnskit_spectral_to_physical(spec: SHTnsSpectralField, phys: SHTnsPhysicalField):
+    phys.data[...] = spec.config.synth_scalar(spec.data_real, spec.data_imag)
+    return phys
+
+
+def shtnskit_physical_to_spectral(phys: SHTnsPhysicalField, spec: SHTnsSpectralField):
+    re, im = spec.config.analysis_scalar(phys.data)
+    spec.data_real[...] = re
+    spec.data_imag[...] = im
+    return spec
+
+
+def batch_spectral_to_physical(specs, physs):
+    """One batched launch for all fields (``shtnskit_field_functions.jl:651-677``)."""
+    if len(specs) != len(physs):
+        raise GeoDynamoError(1, "specs and physs differ in length")
+    if not specs:
+        return
+    cfg = specs[0].config
+    re = np.stack([s.data_real for s in specs])
+    im = np.stack([s.data_imag for s in specs])
+    out = cfg.synth_scalar(re, im)
+    for p, g in zip(physs, out):
+        p.data[...] = g
+
+
+def shtnskit_vector_synthesis(tor: SHTnsSpectralField, pol: SHTnsSpectralField, vec: SHTnsVectorField):
+    vt, vp = tor.config.synth_vector(tor.data_real, tor.data_imag, pol.data_real, pol.data_imag)
+    vec.theta_component.data[...] = vt
+    vec.phi_component.data[...] = vp
+    return vec
+
+
+def shtnskit_vector_analysis(vec: SHTnsVectorField, tor: SHTnsSpectralField, pol: SHTnsSpectralField):
+    tre, tim, pre, pim = tor.config.analysis_vector(vec.theta_component.data, vec.phi_component.data)
+    tor.data_real[...] = tre
+    tor.data_imag[...] = tim
+    pol.data_real[...] = pre
+    pol.data_imag[...] = pim
+    return tor, pol
+
+
+class SimulationState:
+    """Device-resident model state of one shell run (``SimulationState``,
+    ``simulation.jl``), created from a config handle.  Field arrays live on
+    the device; :meth:`field` / :meth:`set_field` copy them in the reference layout."""
+
+    def __init__(self, config: SHTnsKitConfig):
+        self.config = config
+
+    def set_field(self, name, re, im):
+        self.config.set_field(name, re, im)
+
+    def field(self, name):
+        return self.config.get_field(name)
+
+    def nonlinear(self, name):
+        return self.config.get_nl(name)
+
+
+def compute_temperature_nonlinear(state: SimulationState):
+    state.config.temperature_nl()
+
+
+def compute_velocity_nonlinear(state: SimulationState):
+    state.config.velocity_nl()
+
+
+def compute_magnetic_nonlinear(state: SimulationState):
+    state.config.magnetic_nl()
+
+
+def apply_master_implicit_step(state: SimulationState, dt=None):
+    if dt is not None and dt != state.config.cfg.dt:
+        state.config.set_dt(dt)
+        state.config.cfg.dt = dt
+    state.config.implicit_step()
+
+
+def step_once(state: SimulationState):
+    """``step_once!`` (scripts/bench_timestepping.jl:6-18) as one graph replay."""
+    state.config.step(1)
+
+
+def compute_kinetic_energy(state: SimulationState):
+    return state.config.energy()[0]
+
+
+def compute_magnetic_energy(state: SimulationState):
+    return state.config.energy()[1]

@@ -1,0 +1,730 @@
+// gd_api.cu -- the C ABI (include/gdb200.h): handle lifetime, device-resident
+// model state, the step sequence of step_once! and its CUDA-graph replay.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gd_handle.cuh"
+#include "gd_internal.cuh"
+#include "gd_mixed.cuh"
+
+using namespace gd;
+
+
+namespace {
+
+int fail(gd_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(h, GD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+int dalloc(gd_handle* h, T** p, size_t n) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, n * sizeof(T) > 0 ? n * sizeof(T) : 16);
+  if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  h->allocs.push_back(q);
+  h->bytes += n * sizeof(T);
+  *p = static_cast<T*>(q);
+  return GD_OK;
+}
+
+#define AL(ptr, n)                             \
+  do {                                         \
+    int s_ = dalloc(h, &(ptr), (size_t)(n));   \
+    if (s_) return s_;                         \
+  } while (0)
+
+int check_launch(gd_handle* h, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return GD_OK;
+}
+
+int build_implicit(gd_handle* h) {
+  const Dims& d = h->d;
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  launch_build_lu(h->stream, d.nr, d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->c.dt,
+                  h->c.implicit_theta, h->d_lin, h->d_lu, h->d_flag);
+  int s = check_launch(h, "build_lu");
+  if (s) return s;
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flag) return fail(h, GD_ERR_SINGULAR, "zero pivot in a banded LU factorisation");
+  return GD_OK;
+}
+
+int setup(gd_handle* h) {
+  const gd_config& c = h->c;
+  Dims& d = h->d;
+  d.L = c.lmax; d.M = c.mmax; d.nlat = c.nlat; d.nlon = c.nlon; d.nr = c.nr; d.kl = c.kl;
+  d.nth = c.nlat / 2;
+  for (int l = 0; l <= d.L; ++l)
+    for (int m = 0; m <= (l < d.M ? l : d.M); ++m) { h->lv.push_back(l); h->mv.push_back(m); }
+  d.nlm = (int)h->lv.size();
+  h->moff.assign(d.M + 2, 0);
+  for (int m = 0; m <= d.M; ++m) h->moff[m + 1] = h->moff[m] + (d.L - m + 1);
+  h->perm.resize(d.nlm);
+  h->lof.resize(d.nlm);
+  h->mof.resize(d.nlm);
+  for (int q = 0; q < d.nlm; ++q) {
+    const int j = h->moff[h->mv[q]] + (h->lv[q] - h->mv[q]);
+    h->perm[q] = j;
+    h->lof[j] = h->lv[q];
+    h->mof[j] = h->mv[q];
+  }
+  h->plan = make_fft_plan(d.nlon);
+  if (h->plan.nstage < 0) return fail(h, GD_ERR_CONFIG, "nlon must factor into 2, 3 and 5");
+
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  const size_t NL = d.nlm, NT = d.nth, NR = d.nr, nbw = 2 * d.kl + 1;
+  AL(h->d_moff, d.M + 2); AL(h->d_lof, NL); AL(h->d_mof, NL); AL(h->d_perm, NL); AL(h->d_flag, 4);
+  AL(h->d_x, d.nlat); AL(h->d_w, d.nlat); AL(h->d_th, d.nlat); AL(h->d_sth, d.nlat);
+  AL(h->d_cth, d.nlat); AL(h->d_sthc, d.nlat);
+  AL(h->d_r, NR); AL(h->d_rinv, NR); AL(h->d_rinv2, NR); AL(h->d_nu, 3);
+  AL(h->d_P, NL * NT); AL(h->d_dP, NL * NT); AL(h->d_Q, NL * NT);
+  AL(h->d_d1, nbw * NR); AL(h->d_d2, nbw * NR);
+  AL(h->d_lin, 3 * NR * nbw * (d.L + 1)); AL(h->d_lu, 3 * NR * nbw * (d.L + 1));
+  AL(h->d_tw, 2 * (size_t)d.nlon); AL(h->d_twf, 2 * (size_t)d.nlon);
+  AL(h->d_state, 5 * h->spec_elems()); AL(h->d_nl, 5 * h->spec_elems()); AL(h->d_prev, 5 * h->spec_elems());
+  AL(h->d_work, 8 * h->spec_elems());
+  AL(h->d_bvals, 2 * NL); AL(h->d_sources, NR);
+  AL(h->d_grid, NGRID * h->grid_elems());
+  AL(h->d_F, (size_t)4 * NR * (d.M + 1) * d.nlat);
+  AL(h->d_epart, 2 * 296); AL(h->d_eout, 2);
+
+  cudaStream_t s = h->stream;
+  CK(cudaMemcpyAsync(h->d_moff, h->moff.data(), sizeof(int) * (d.M + 2), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_lof, h->lof.data(), sizeof(int) * NL, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_mof, h->mof.data(), sizeof(int) * NL, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_perm, h->perm.data(), sizeof(int) * NL, cudaMemcpyHostToDevice, s));
+  // Radial nodes r_n = ri + (1 + cos(pi (N - n) / (N - 1))) / 2 (src/fields.jl:108-131),
+  // with the powers r^-1, r^-2 of its columns 3 and 2.
+  std::vector<double> r(NR), ri(NR), ri2(NR);
+  const double rin = c.rratio / (1.0 - c.rratio);
+  const double kPi = 3.14159265358979323846;
+  for (int n = 1; n <= d.nr; ++n) r[n - 1] = 0.5 * (1.0 + std::cos(kPi * (double)(d.nr - n) / (double)(d.nr - 1))) + rin;
+  for (int n = 0; n < d.nr; ++n) { ri[n] = std::pow(r[n], -1.0); ri2[n] = std::pow(r[n], -2.0); }
+  CK(cudaMemcpyAsync(h->d_r, r.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_rinv, ri.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_rinv2, ri2.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
+  // Diffusivities: velocity Pm, magnetic 1, temperature Pm/Pr (src/simulation.jl:228-231).
+  const double nu[3] = {c.magnetic_prandtl, 1.0, c.magnetic_prandtl / c.prandtl};
+  CK(cudaMemcpyAsync(h->d_nu, nu, sizeof(nu), cudaMemcpyHostToDevice, s));
+  std::vector<double> tw;
+  make_twiddles(d.nlon, tw);
+  std::vector<float> twf(tw.size());
+  for (size_t i = 0; i < tw.size(); ++i) twf[i] = (float)tw[i];
+  CK(cudaMemcpyAsync(h->d_tw, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_twf, twf.data(), sizeof(float) * twf.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));  // host vectors above go out of scope
+
+  launch_gauss(s, d.nlat, h->d_x, h->d_w, h->d_th, h->d_sth);
+  launch_tables(s, d, h->d_moff, h->d_x, h->d_sth, h->d_P, h->d_dP, h->d_Q);
+  launch_fd_weights(s, d.nr, d.kl, c.fd_mode, h->d_r, h->d_d1, h->d_d2);
+  int st = check_launch(h, "set-up kernels");
+  if (st) return st;
+  // Coriolis factors sin/cos of the colatitude grid (src/velocity.jl:278-282).
+  {
+    std::vector<double> th(d.nlat), cth(d.nlat), sth(d.nlat);
+    CK(cudaMemcpyAsync(th.data(), h->d_th, sizeof(double) * d.nlat, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < d.nlat; ++i) { sth[i] = std::sin(th[i]); cth[i] = std::cos(th[i]); }
+    CK(cudaMemcpyAsync(h->d_sthc, sth.data(), sizeof(double) * d.nlat, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->d_cth, cth.data(), sizeof(double) * d.nlat, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  CK(cudaMemsetAsync(h->d_state, 0, sizeof(double) * 5 * h->spec_elems(), s));
+  CK(cudaMemsetAsync(h->d_nl, 0, sizeof(double) * 5 * h->spec_elems(), s));
+  CK(cudaMemsetAsync(h->d_prev, 0, sizeof(double) * 5 * h->spec_elems(), s));
+  CK(cudaMemsetAsync(h->d_work, 0, sizeof(double) * 8 * h->spec_elems(), s));
+  CK(cudaMemsetAsync(h->d_bvals, 0, sizeof(double) * 2 * NL, s));
+  CK(cudaMemsetAsync(h->d_sources, 0, sizeof(double) * NR, s));
+  CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * NGRID * h->grid_elems(), s));
+  return build_implicit(h);
+}
+
+// ---- transform building blocks on device buffers (native layouts) ----
+int synth_scalar(gd_handle* h, const double* const* coef, int nf, double* grid_out) {
+  SynthArgs a{};
+  a.table0 = h->d_P;
+  for (int i = 0; i < nf; ++i) a.coef[i] = coef[i];
+  a.nf = nf;
+  a.out = h->d_F;
+  { ProfScope p(h, "legendre_synth_scalar_fp64"); launch_synth_fp64(h->stream, h->d, h->d_moff, a, false); }
+  { ProfScope p(h, "fft_synth_fp64"); launch_fft_synth<double>(h->stream, h->d, h->plan, h->d_tw, h->d_F, grid_out, nf, h->grid_elems()); }
+  return check_launch(h, "scalar synthesis");
+}
+
+int synth_vector(gd_handle* h, const double* tor, const double* pol, double* grid_out /* 2 comps */) {
+  SynthArgs a{};
+  a.table0 = h->d_dP;
+  a.table1 = h->d_Q;
+  a.coef[0] = pol;
+  a.coef[1] = tor;
+  a.nf = 1;
+  a.out = h->d_F;
+  { ProfScope p(h, "legendre_synth_vector_fp64"); launch_synth_fp64(h->stream, h->d, h->d_moff, a, true); }
+  { ProfScope p(h, "fft_synth_fp64"); launch_fft_synth<double>(h->stream, h->d, h->plan, h->d_tw, h->d_F, grid_out, 2, h->grid_elems()); }
+  return check_launch(h, "vector synthesis");
+}
+
+int analysis_scalar(gd_handle* h, const double* grid_in, int nf, double* const* out) {
+  { ProfScope p(h, "fft_analysis_fp64"); launch_fft_analysis<double>(h->stream, h->d, h->plan, h->d_tw, grid_in, h->grid_elems(), h->d_w, h->d_F, nf); }
+  AnalysisArgs a{};
+  a.table0 = h->d_P;
+  a.in = h->d_F;
+  for (int i = 0; i < nf; ++i) a.out[i] = out[i];
+  a.nf = nf;
+  a.epi = EPI_SCALAR;
+  { ProfScope p(h, "legendre_analysis_scalar_fp64"); launch_analysis_fp64(h->stream, h->d, h->d_moff, a); }
+  return check_launch(h, "scalar analysis");
+}
+
+int analysis_vector(gd_handle* h, const double* grid_in /* 2 comps */, double* out_tor, double* out_pol, int epi) {
+  { ProfScope p(h, "fft_analysis_fp64"); launch_fft_analysis<double>(h->stream, h->d, h->plan, h->d_tw, grid_in, h->grid_elems(), h->d_w, h->d_F, 2); }
+  AnalysisArgs a{};
+  a.table0 = h->d_dP;
+  a.table1 = h->d_Q;
+  a.in = h->d_F;
+  a.out[0] = out_tor;
+  a.out[1] = out_pol;
+  a.nf = 1;
+  a.epi = epi;
+  { ProfScope p(h, "legendre_analysis_vector_fp64"); launch_analysis_fp64(h->stream, h->d, h->d_moff, a); }
+  return check_launch(h, "vector analysis");
+}
+
+// ---- the physics sequence (FP64) ----
+int temperature_nl_fp64(gd_handle* h) {
+  const Dims& d = h->d;
+  { ProfScope p(h, "spectral_gradients");
+    launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), h->work(0), h->work(1),
+                     h->work(2)); }
+  const double* coef[4] = {h->field(F_TEMP), h->work(0), h->work(1), h->work(2)};
+  int s = synth_scalar(h, coef, 4, h->grid(GD_GRID_T));
+  if (s) return s;
+  ProfScope pa(h, "nl_temperature_fp64");
+  launch_temperature_advection<double>(h->stream, d, h->grid(GD_GRID_U_TH), h->grid(GD_GRID_U_PH),
+                                       h->grid(GD_GRID_GTH), h->grid(GD_GRID_GPH), h->grid(GD_GRID_GR),
+                                       h->d_sources, h->grid(GD_GRID_TADV));
+  double* out[1] = {h->nlf(F_TEMP)};
+  s = analysis_scalar(h, h->grid(GD_GRID_TADV), 1, out);
+  if (s) return s;
+  { ProfScope p(h, "temperature_bc"); launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP)); }
+  return check_launch(h, "temperature nonlinear");
+}
+
+int velocity_nl_fp64(gd_handle* h) {
+  const Dims& d = h->d;
+  int s = synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), h->grid(GD_GRID_U_TH));
+  if (s) return s;
+  { ProfScope p(h, "spectral_curl");
+    launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR), h->field(F_UPOL),
+                h->work(3), h->work(4)); }
+  s = synth_vector(h, h->work(3), h->work(4), h->grid(GD_GRID_W_TH));
+  if (s) return s;
+  const double rf = h->c.magnetic_prandtl / h->c.ekman;
+  { ProfScope p(h, "nl_velocity_fp64");
+  launch_velocity_nl<double>(h->stream, d, h->d_cth, h->d_sthc, rf, rf, h->c.magnetic, h->grid(GD_GRID_U_TH),
+                             h->grid(GD_GRID_U_PH), h->grid(GD_GRID_W_TH), h->grid(GD_GRID_W_PH),
+                             h->grid(GD_GRID_J_TH), h->grid(GD_GRID_J_PH), h->grid(GD_GRID_B_TH),
+                             h->grid(GD_GRID_B_PH), h->grid(GD_GRID_VADV_TH), h->grid(GD_GRID_VADV_PH)); }
+  return analysis_vector(h, h->grid(GD_GRID_VADV_TH), h->nlf(F_UTOR), h->nlf(F_UPOL), EPI_VECTOR);
+}
+
+int magnetic_nl_fp64(gd_handle* h) {
+  const Dims& d = h->d;
+  int s = synth_vector(h, h->field(F_BTOR), h->field(F_BPOL), h->grid(GD_GRID_B_TH));
+  if (s) return s;
+  { ProfScope p(h, "spectral_curl");
+    launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR), h->field(F_BPOL),
+                h->work(5), h->work(6)); }
+  s = synth_vector(h, h->work(5), h->work(6), h->grid(GD_GRID_J_TH));
+  if (s) return s;
+  { ProfScope p(h, "nl_induction_fp64");
+    launch_induction<double>(h->stream, d, h->grid(GD_GRID_U_TH), h->grid(GD_GRID_U_PH), h->grid(GD_GRID_B_TH),
+                             h->grid(GD_GRID_B_PH), h->grid(GD_GRID_IND_TH), h->grid(GD_GRID_IND_PH)); }
+  return analysis_vector(h, h->grid(GD_GRID_IND_TH), h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
+}
+
+int implicit_launch(gd_handle* h, int boot) {
+  Cnab2Args a{};
+  const int order[5] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL};
+  const int kinds[5] = {2, 0, 0, 1, 1};
+  a.nfield = h->c.magnetic ? 5 : 3;
+  for (int i = 0; i < a.nfield; ++i) {
+    a.u[i] = h->field(order[i]);
+    a.nl[i] = h->nlf(order[i]);
+    a.prev[i] = h->prevf(order[i]);
+    a.kind[i] = kinds[i];
+  }
+  a.boot = boot;
+  a.clamp_rows = h->c.bc_mode == 1;
+  a.inv_dt = 1.0 / h->c.dt;
+  a.lin_weight = 1.0 - h->c.implicit_theta;
+  { ProfScope p(h, "cnab2_solve"); launch_cnab2(h->stream, h->d, h->d_lof, h->d_lin, h->d_lu, a); }
+  return check_launch(h, "cnab2");
+}
+
+int temperature_nl(gd_handle* h) {
+  return h->precision == GD_PREC_MIXED ? mixed_temperature_nl(h) : temperature_nl_fp64(h);
+}
+int velocity_nl(gd_handle* h) {
+  return h->precision == GD_PREC_MIXED ? mixed_velocity_nl(h) : velocity_nl_fp64(h);
+}
+int magnetic_nl(gd_handle* h) {
+  return h->precision == GD_PREC_MIXED ? mixed_magnetic_nl(h) : magnetic_nl_fp64(h);
+}
+
+int step_sequence(gd_handle* h, int boot) {
+  int s = temperature_nl(h);
+  if (s) return s;
+  s = velocity_nl(h);
+  if (s) return s;
+  if (h->c.magnetic) {
+    s = magnetic_nl(h);
+    if (s) return s;
+  }
+  return implicit_launch(h, boot);
+}
+
+void drop_graphs(gd_handle* h) {
+  for (int i = 0; i < 2; ++i)
+    if (h->gexec[i]) { cudaGraphExecDestroy(h->gexec[i]); h->gexec[i] = nullptr; }
+}
+
+int ensure_graph(gd_handle* h, int boot) {
+  if (h->gexec[boot]) return GD_OK;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int s = step_sequence(h, boot);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (s) { if (g) cudaGraphDestroy(g); return s; }
+  if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&h->gexec[boot], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return GD_OK;
+}
+
+int stage_alloc(gd_handle* h) {
+  if (h->d_stage_spec) return GD_OK;
+  AL(h->d_stage_spec, 4 * h->spec_elems());
+  AL(h->d_stage_spec2, 4 * h->spec_elems());
+  AL(h->d_stage_grid, 4 * h->grid_elems());
+  AL(h->d_stage_grid2, 4 * h->grid_elems());
+  return GD_OK;
+}
+
+bool valid_config(const gd_config* c, std::string& why) {
+  if (c->lmax < 1 || c->mmax < 0 || c->mmax > c->lmax) { why = "need 1 <= lmax, 0 <= mmax <= lmax"; return false; }
+  if (c->nlat < 2 || (c->nlat & 1)) { why = "nlat must be even"; return false; }
+  if (c->nlat <= c->lmax) { why = "nlat must exceed lmax (Gauss quadrature exactness)"; return false; }
+  if (2 * c->mmax >= c->nlon) { why = "nlon must exceed 2 mmax"; return false; }
+  if (c->nr < 3) { why = "nr must be at least 3"; return false; }
+  if (c->kl != GD_MAX_KL) { why = "kl must be 4 (i_KL)"; return false; }
+  if (!(c->dt > 0.0)) { why = "dt must be positive"; return false; }
+  if (c->ekman == 0.0) { why = "Ekman number must be nonzero (src/velocity.jl:450-452)"; return false; }
+  if (c->rratio <= 0.0 || c->rratio >= 1.0) { why = "rratio must lie in (0, 1)"; return false; }
+  if (c->precision != GD_PREC_FP64 && c->precision != GD_PREC_MIXED) { why = "unknown precision"; return false; }
+  return true;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+int gd_create(const gd_config* cfg, int device, gd_handle** out) {
+  if (!cfg || !out) return GD_ERR_ARG;
+  *out = nullptr;
+  std::string why;
+  if (!valid_config(cfg, why)) {
+    fprintf(stderr, "gd_create: %s\n", why.c_str());
+    return GD_ERR_CONFIG;
+  }
+  gd_handle* h = new gd_handle();
+  h->c = *cfg;
+  h->device = device;
+  int s = setup(h);
+  if (s == GD_OK && cfg->precision == GD_PREC_MIXED) s = gd_set_precision(h, GD_PREC_MIXED);
+  if (s != GD_OK) {
+    fprintf(stderr, "gd_create: %s\n", h->err.c_str());
+    gd_destroy(h);
+    return s;
+  }
+  *out = h;
+  return GD_OK;
+}
+
+int gd_destroy(gd_handle* h) {
+  if (!h) return GD_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graphs(h);
+  if (h->mixed) mixed_destroy(h);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return GD_OK;
+}
+
+const char* gd_last_error(const gd_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int gd_info(const gd_handle* h, int* nlm, size_t* device_bytes) {
+  if (!h) return GD_ERR_ARG;
+  if (nlm) *nlm = h->d.nlm;
+  if (device_bytes) *device_bytes = h->bytes + (h->mixed ? mixed_bytes(h) : 0);
+  return GD_OK;
+}
+
+int gd_grid(gd_handle* h, double* theta, double* weights, double* r) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  if (theta) CK(cudaMemcpyAsync(theta, h->d_th, sizeof(double) * h->d.nlat, cudaMemcpyDeviceToHost, h->stream));
+  if (weights) CK(cudaMemcpyAsync(weights, h->d_w, sizeof(double) * h->d.nlat, cudaMemcpyDeviceToHost, h->stream));
+  if (r) CK(cudaMemcpyAsync(r, h->d_r, sizeof(double) * h->d.nr, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+
+int gd_set_precision(gd_handle* h, int mode) {
+  if (!h) return GD_ERR_ARG;
+  if (mode != GD_PREC_FP64 && mode != GD_PREC_MIXED) return fail(h, GD_ERR_ARG, "unknown precision mode");
+  CK(cudaSetDevice(h->device));
+  if (mode == GD_PREC_MIXED && !h->mixed) {
+    int s = mixed_create(h);
+    if (s) return s;
+  }
+  if (mode != h->precision) drop_graphs(h);
+  h->precision = mode;
+  return GD_OK;
+}
+
+int gd_synchronize(gd_handle* h) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+
+int gd_upload_spectral(gd_handle* h, int field, const double* re, const double* im) {
+  if (!h || !re || !im || field < 0 || field > 4) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm;
+  CK(cudaMemcpyAsync(h->d_stage_spec, re, plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_stage_spec + plane, im, plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_lmajor_to_native(h->stream, h->d, h->d_perm, h->d_stage_spec, h->field(field), 2);
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "upload");
+}
+
+static int download_spec(gd_handle* h, const double* src, double* re, double* im) {
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm;
+  launch_native_to_lmajor(h->stream, h->d, h->d_perm, src, h->d_stage_spec, 2);
+  CK(cudaMemcpyAsync(re, h->d_stage_spec, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(im, h->d_stage_spec + plane, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "download");
+}
+
+int gd_download_spectral(gd_handle* h, int field, double* re, double* im) {
+  if (!h || !re || !im || field < 0 || field > 4) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  return download_spec(h, h->field(field), re, im);
+}
+
+int gd_download_nonlinear(gd_handle* h, int field, double* re, double* im) {
+  if (!h || !re || !im || field < 0 || field > 4) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  return download_spec(h, h->nlf(field), re, im);
+}
+
+int gd_download_grid(gd_handle* h, int grid, double* out) {
+  if (!h || !out || grid < 0 || grid >= NGRID) return h ? fail(h, GD_ERR_ARG, "bad grid id or pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const double* src = h->grid(grid);
+  if (h->precision == GD_PREC_MIXED) {
+    mixed_grid_to_double(h, grid, h->d_stage_grid2);
+    src = h->d_stage_grid2;
+  }
+  launch_grid_to_reference(h->stream, h->d, src, h->d_stage_grid, 1);
+  CK(cudaMemcpyAsync(out, h->d_stage_grid, h->grid_elems() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "download grid");
+}
+
+int gd_set_temperature_bc(gd_handle* h, const double* bvals, const double* sources) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  if (bvals) {
+    CK(cudaMemcpyAsync(h->d_stage_spec, bvals, 2 * (size_t)h->d.nlm * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    // two rows of nlm, permuted like one two-row plane
+    Dims d1 = h->d;
+    d1.nr = 1;
+    launch_lmajor_to_native(h->stream, d1, h->d_perm, h->d_stage_spec, h->d_bvals, 2);
+  }
+  if (sources) CK(cudaMemcpyAsync(h->d_sources, sources, h->d.nr * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "set temperature bc");
+}
+
+int gd_spectral_to_physical(gd_handle* h, int nfield, const double* re, const double* im, double* grid) {
+  if (!h || !re || !im || !grid || nfield < 1) return h ? fail(h, GD_ERR_ARG, "bad arguments") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm, G = h->grid_elems();
+  for (int f0 = 0; f0 < nfield; f0 += 4) {
+    const int nf = nfield - f0 < 4 ? nfield - f0 : 4;
+    const double* coef[4];
+    for (int i = 0; i < nf; ++i) {
+      CK(cudaMemcpyAsync(h->d_stage_spec + 2 * plane * i, re + plane * (f0 + i), plane * sizeof(double),
+                         cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(h->d_stage_spec + 2 * plane * i + plane, im + plane * (f0 + i), plane * sizeof(double),
+                         cudaMemcpyHostToDevice, h->stream));
+    }
+    launch_lmajor_to_native(h->stream, h->d, h->d_perm, h->d_stage_spec, h->d_stage_spec2, 2 * nf);
+    for (int i = 0; i < nf; ++i) coef[i] = h->d_stage_spec2 + 2 * plane * i;
+    if (h->precision == GD_PREC_MIXED) s = mixed_api_synth_scalar(h, coef, nf, h->d_stage_grid2);
+    else s = synth_scalar(h, coef, nf, h->d_stage_grid2);
+    if (s) return s;
+    launch_grid_to_reference(h->stream, h->d, h->d_stage_grid2, h->d_stage_grid, nf);
+    CK(cudaMemcpyAsync(grid + G * f0, h->d_stage_grid, G * nf * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return check_launch(h, "spectral_to_physical");
+}
+
+int gd_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double* re, double* im) {
+  if (!h || !re || !im || !grid || nfield < 1) return h ? fail(h, GD_ERR_ARG, "bad arguments") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm, G = h->grid_elems();
+  for (int f0 = 0; f0 < nfield; f0 += 4) {
+    const int nf = nfield - f0 < 4 ? nfield - f0 : 4;
+    CK(cudaMemcpyAsync(h->d_stage_grid, grid + G * f0, G * nf * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    launch_grid_to_native(h->stream, h->d, h->d_stage_grid, h->d_stage_grid2, nf);
+    double* out[4];
+    for (int i = 0; i < nf; ++i) out[i] = h->d_stage_spec2 + 2 * plane * i;
+    if (h->precision == GD_PREC_MIXED) s = mixed_api_analysis_scalar(h, h->d_stage_grid2, nf, out);
+    else s = analysis_scalar(h, h->d_stage_grid2, nf, out);
+    if (s) return s;
+    launch_native_to_lmajor(h->stream, h->d, h->d_perm, h->d_stage_spec2, h->d_stage_spec, 2 * nf);
+    for (int i = 0; i < nf; ++i) {
+      CK(cudaMemcpyAsync(re + plane * (f0 + i), h->d_stage_spec + 2 * plane * i, plane * sizeof(double),
+                         cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(im + plane * (f0 + i), h->d_stage_spec + 2 * plane * i + plane, plane * sizeof(double),
+                         cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return check_launch(h, "physical_to_spectral");
+}
+
+int gd_vector_synthesis(gd_handle* h, const double* tor_re, const double* tor_im, const double* pol_re,
+                        const double* pol_im, double* v_theta, double* v_phi) {
+  if (!h || !tor_re || !tor_im || !pol_re || !pol_im || !v_theta || !v_phi)
+    return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm, G = h->grid_elems();
+  const double* src[4] = {tor_re, tor_im, pol_re, pol_im};
+  for (int i = 0; i < 4; ++i)
+    CK(cudaMemcpyAsync(h->d_stage_spec + plane * i, src[i], plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_lmajor_to_native(h->stream, h->d, h->d_perm, h->d_stage_spec, h->d_stage_spec2, 4);
+  const double* tor = h->d_stage_spec2;
+  const double* pol = h->d_stage_spec2 + 2 * plane;
+  if (h->precision == GD_PREC_MIXED) s = mixed_api_synth_vector(h, tor, pol, h->d_stage_grid2);
+  else s = synth_vector(h, tor, pol, h->d_stage_grid2);
+  if (s) return s;
+  launch_grid_to_reference(h->stream, h->d, h->d_stage_grid2, h->d_stage_grid, 2);
+  CK(cudaMemcpyAsync(v_theta, h->d_stage_grid, G * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(v_phi, h->d_stage_grid + G, G * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "vector synthesis");
+}
+
+int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re, double* tor_im,
+                       double* pol_re, double* pol_im) {
+  if (!h || !tor_re || !tor_im || !pol_re || !pol_im || !v_theta || !v_phi)
+    return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm, G = h->grid_elems();
+  CK(cudaMemcpyAsync(h->d_stage_grid, v_theta, G * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_stage_grid + G, v_phi, G * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_grid_to_native(h->stream, h->d, h->d_stage_grid, h->d_stage_grid2, 2);
+  double* tor = h->d_stage_spec2;
+  double* pol = h->d_stage_spec2 + 2 * plane;
+  if (h->precision == GD_PREC_MIXED) s = mixed_api_analysis_vector(h, h->d_stage_grid2, tor, pol);
+  else s = analysis_vector(h, h->d_stage_grid2, tor, pol, EPI_VECTOR);
+  if (s) return s;
+  launch_native_to_lmajor(h->stream, h->d, h->d_perm, h->d_stage_spec2, h->d_stage_spec, 4);
+  double* dst[4] = {tor_re, tor_im, pol_re, pol_im};
+  for (int i = 0; i < 4; ++i)
+    CK(cudaMemcpyAsync(dst[i], h->d_stage_spec + plane * i, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "vector analysis");
+}
+
+int gd_temperature_nonlinear(gd_handle* h) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = temperature_nl(h);
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+int gd_velocity_nonlinear(gd_handle* h) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = velocity_nl(h);
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+int gd_magnetic_nonlinear(gd_handle* h) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = magnetic_nl(h);
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+int gd_implicit_step(gd_handle* h) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  const int boot = (h->c.ab_mode == 1 || h->step_count == 0) ? 1 : 0;
+  int s = implicit_launch(h, boot);
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  h->step_count++;
+  return GD_OK;
+}
+
+int gd_step_async(gd_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return h ? fail(h, GD_ERR_ARG, "nsteps must be >= 0") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  for (int i = 0; i < nsteps; ++i) {
+    const int boot = (h->c.ab_mode == 1 || h->step_count == 0) ? 1 : 0;
+    if (h->profiling) {
+      int s = step_sequence(h, boot);
+      if (s) return s;
+    } else {
+      int s = ensure_graph(h, boot);
+      if (s) return s;
+      CK(cudaGraphLaunch(h->gexec[boot], h->stream));
+    }
+    h->step_count++;
+  }
+  return GD_OK;
+}
+
+int gd_step(gd_handle* h, int nsteps) {
+  int s = gd_step_async(h, nsteps);
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+
+int gd_set_dt(gd_handle* h, double dt) {
+  if (!h || !(dt > 0.0)) return h ? fail(h, GD_ERR_ARG, "dt must be positive") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  h->c.dt = dt;
+  drop_graphs(h);
+  return build_implicit(h);
+}
+
+int gd_energy(gd_handle* h, double* ekin, double* emag) {
+  if (!h || !ekin || !emag) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  launch_energy(h->stream, h->d, h->d_lof, h->field(F_UTOR), h->field(F_UPOL), h->c.magnetic ? h->field(F_BTOR) : nullptr,
+                h->field(F_BPOL), h->d_epart, h->d_eout);
+  double e[2];
+  CK(cudaMemcpyAsync(e, h->d_eout, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *ekin = e[0];
+  *emag = e[1];
+  return check_launch(h, "energy");
+}
+
+int gd_check_finite(gd_handle* h) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  launch_check_finite(h->stream, 5 * h->spec_elems(), h->d_state, h->d_flag);
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flag) return fail(h, GD_ERR_NONFINITE, "non-finite value in the spectral state");
+  return check_launch(h, "check_finite");
+}
+
+long gd_step_count(const gd_handle* h) { return h ? h->step_count : -1; }
+
+int gd_get_stream(gd_handle* h, void** stream) {
+  if (!h || !stream) return GD_ERR_ARG;
+  *stream = (void*)h->stream;
+  return GD_OK;
+}
+
+int gd_profile_enable(gd_handle* h, int enable) {
+  if (!h) return GD_ERR_ARG;
+  h->profiling = enable != 0;
+  return GD_OK;
+}
+
+int gd_profile_read(gd_handle* h, int max, char* names, double* ms, int* launches, int* count) {
+  if (!h || !count || max < 0) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  for (auto& p : h->prof_pending) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, p.a, p.b);
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+    size_t k = 0;
+    while (k < h->prof_names.size() && h->prof_names[k] != p.name) ++k;
+    if (k == h->prof_names.size()) { h->prof_names.push_back(p.name); h->prof_ms.push_back(0.0); h->prof_count.push_back(0); }
+    h->prof_ms[k] += t;
+    h->prof_count[k] += 1;
+  }
+  h->prof_pending.clear();
+  const int n = (int)h->prof_names.size();
+  *count = n;
+  for (int k = 0; k < n && k < max; ++k) {
+    if (names) { std::strncpy(names + 32 * k, h->prof_names[k].c_str(), 31); names[32 * k + 31] = 0; }
+    if (ms) ms[k] = h->prof_ms[k];
+    if (launches) launches[k] = h->prof_count[k];
+  }
+  h->prof_names.clear(); h->prof_ms.clear(); h->prof_count.clear();
+  return GD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// gd_handle.cuh -- the handle behind the opaque gd_handle* of the C ABI.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "gd_internal.cuh"
+
+namespace gd {
+struct MixedState;
+}
+
+struct gd_handle {
+  gd_config c{};
+  gd::Dims d{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long step_count = 0;
+  int precision = GD_PREC_FP64;
+  size_t bytes = 0;
+  std::vector<void*> allocs;
+
+  std::vector<int> lv, mv, moff, perm, lof, mof;
+  gd::FftPlan plan{};
+
+  int *d_moff = nullptr, *d_lof = nullptr, *d_mof = nullptr, *d_perm = nullptr, *d_flag = nullptr;
+  double *d_x = nullptr, *d_w = nullptr, *d_th = nullptr, *d_sth = nullptr, *d_cth = nullptr, *d_sthc = nullptr;
+  double *d_r = nullptr, *d_rinv = nullptr, *d_rinv2 = nullptr, *d_nu = nullptr;
+  double *d_P = nullptr, *d_dP = nullptr, *d_Q = nullptr;
+  double *d_d1 = nullptr, *d_d2 = nullptr, *d_lin = nullptr, *d_lu = nullptr;
+  double* d_tw = nullptr;
+  float* d_twf = nullptr;
+  double* d_state = nullptr;  // 5 fields
+  double* d_nl = nullptr;     // 5 fields
+  double* d_prev = nullptr;   // 5 fields
+  double* d_work = nullptr;   // 8 derived spectral fields
+  double *d_bvals = nullptr, *d_sources = nullptr;
+  double* d_grid = nullptr;   // NGRID grids (FP64)
+  double2* d_F = nullptr;     // Fourier buffer, 4 components
+  double *d_epart = nullptr, *d_eout = nullptr;
+  // host-ABI staging (lazy)
+  double *d_stage_spec = nullptr, *d_stage_spec2 = nullptr, *d_stage_grid = nullptr, *d_stage_grid2 = nullptr;
+  // mixed precision state (lazy)
+  gd::MixedState* mixed = nullptr;
+  // graphs (index: boot flag)
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  // per-kernel event timing (gd_profile_enable)
+  bool profiling = false;
+  struct ProfRec { const char* name; cudaEvent_t a, b; };
+  std::vector<ProfRec> prof_pending;
+  std::vector<std::string> prof_names;
+  std::vector<double> prof_ms;
+  std::vector<int> prof_count;
+
+  size_t spec_elems() const { return (size_t)2 * d.nr * d.nlm; }
+  size_t grid_elems() const { return (size_t)d.nlat * d.nlon * d.nr; }
+  double* field(int f) { return d_state + spec_elems() * f; }
+  double* nlf(int f) { return d_nl + spec_elems() * f; }
+  double* prevf(int f) { return d_prev + spec_elems() * f; }
+  double* work(int k) { return d_work + spec_elems() * k; }
+  double* grid(int g) { return d_grid + grid_elems() * g; }
+};
+
+namespace gd {
+// Brackets the launches of its lifetime with CUDA events when profiling is on.
+struct ProfScope {
+  gd_handle* h;
+  const char* name;
+  cudaEvent_t a = nullptr;
+  ProfScope(gd_handle* h_, const char* n) : h(h_), name(n) {
+    if (h->profiling) {
+      cudaEventCreate(&a);
+      cudaEventRecord(a, h->stream);
+    }
+  }
+  ~ProfScope() {
+    if (h->profiling && a) {
+      cudaEvent_t b;
+      cudaEventCreate(&b);
+      cudaEventRecord(b, h->stream);
+      h->prof_pending.push_back({name, a, b});
+    }
+  }
+};
+
+inline int set_error(gd_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+}  // namespace gd

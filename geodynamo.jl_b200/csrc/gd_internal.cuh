@@ -1,0 +1,132 @@
+// gd_internal.cuh -- shared definitions of libgdb200.so (not part of the ABI).
+//
+// Device layouts (native; the host ABI converts to and from the reference's):
+//   mode index j      m-major: j = moff[m] + (l - m), l = m..lmax.
+//   spectral field    two planes (Re, Im), each [r][j] doubles.
+//   tables P, dP, Q   [j][ith], ith = north-half colatitude index (0..nlat/2-1);
+//                     Q = m Pbar_lm / sin(theta).
+//   Fourier buffer    [comp][r][m][s][ith] complex.  Synthesis: s = 0 north row,
+//                     s = 1 south row (ith mirrored).  Analysis: s = 0 holds
+//                     w (G_north + G_south), s = 1 holds w (G_north - G_south),
+//                     with G the (2 pi / nlon)-scaled phi transform.
+//   grid              [comp][r][itheta][jphi] (phi fastest).
+//   LU / linear bands [kind][col][band][l] (l fastest; kind 0 velocity,
+//                     1 magnetic, 2 temperature).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/gdb200.h"
+
+#define GD_MAX_KL 4
+#define GD_NBW (2 * GD_MAX_KL + 1)
+
+namespace gd {
+
+enum { F_UTOR = 0, F_UPOL = 1, F_BTOR = 2, F_BPOL = 3, F_TEMP = 4, NFIELD = 5 };
+enum { NGRID = 17 };
+
+struct Dims {
+  int L, M, nlat, nlon, nr, nth, nlm, kl;
+};
+
+// Analysis epilogue variants.
+enum { EPI_SCALAR = 0, EPI_VECTOR = 1, EPI_CURL_INDUCTION = 2 };
+
+// ---- set-up kernels (gd_setup.cu) ----
+void launch_gauss(cudaStream_t s, int nlat, double* x, double* w, double* th, double* sth);
+void launch_tables(cudaStream_t s, const Dims& d, const int* moff, const double* x, const double* sth,
+                   double* P, double* dP, double* Q);
+void launch_fd_weights(cudaStream_t s, int nr, int kl, int fd_mode, const double* r, double* d1, double* d2);
+void launch_build_lu(cudaStream_t s, int nr, int kl, int L, const double* d1, const double* d2,
+                     const double* rinv, const double* rinv2, const double* nu, double dt, double theta,
+                     double* lin, double* lu, int* status);
+
+// ---- Legendre (gd_legendre.cu) ----
+struct SynthArgs {
+  const double* table0;  // scalar: P ; vector: dP
+  const double* table1;  // vector: Q
+  const double* coef[4]; // scalar: nf fields ; vector: [0] = S (poloidal), [1] = T (toroidal)
+  double2* out;          // Fourier buffer, comps consecutive
+  int nf;                // scalar: number of fields (comps) ; vector: 1 (outputs 2 comps)
+};
+void launch_synth_fp64(cudaStream_t s, const Dims& d, const int* moff, const SynthArgs& a, bool vec);
+
+struct AnalysisArgs {
+  const double* table0;  // scalar: P ; vector: dP
+  const double* table1;  // vector: Q
+  const double2* in;     // folded Fourier buffer (comps consecutive)
+  double* out[4];        // scalar: nf outputs ; vector: [0] tor, [1] pol
+  int nf;
+  int epi;
+  const double* sth;
+};
+void launch_analysis_fp64(cudaStream_t s, const Dims& d, const int* moff, const AnalysisArgs& a);
+
+// ---- phi transforms (gd_fft.cu) ----
+struct FftPlan {
+  int n;
+  int nstage;
+  int radix[16];
+  int tb;  // theta pairs per CTA
+};
+FftPlan make_fft_plan(int nlon);
+template <typename R>
+void launch_fft_synth(cudaStream_t s, const Dims& d, const FftPlan& p, const void* twiddle, const void* F,
+                      R* grid, int ncomp, size_t grid_comp_stride);
+template <typename R>
+void launch_fft_analysis(cudaStream_t s, const Dims& d, const FftPlan& p, const void* twiddle, const R* grid,
+                         size_t grid_comp_stride, const double* w, void* G, int ncomp);
+void make_twiddles(int n, std::vector<double>& tw);
+
+// ---- nonlinear terms (gd_nonlinear.cu) ----
+template <typename R>
+void launch_temperature_advection(cudaStream_t s, const Dims& d, const R* uth, const R* uph, const R* gth,
+                                  const R* gph, const R* gr, const double* sources, R* out);
+template <typename R>
+void launch_velocity_nl(cudaStream_t s, const Dims& d, const double* cth, const double* sth_cor, double rf,
+                        double lf, int magnetic, const R* uth, const R* uph, const R* wth, const R* wph,
+                        const R* jth, const R* jph, const R* bth, const R* bph, R* ath, R* aph);
+template <typename R>
+void launch_induction(cudaStream_t s, const Dims& d, const R* uth, const R* uph, const R* bth, const R* bph,
+                      R* oth, R* oph);
+
+// ---- spectral operators (gd_spectral.cu) ----
+void launch_gradients(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
+                      const double* d1, const double* T, double* gth, double* gph, double* gr);
+void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* rinv, const double* rinv2,
+                 const double* d1, const double* d2, const double* tor, const double* pol, double* otor,
+                 double* opol);
+void launch_temperature_bc(cudaStream_t s, const Dims& d, const double* bvals_native, double* T);
+void launch_lmajor_to_native(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,
+                             double* dst, int nplanes);
+void launch_native_to_lmajor(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,
+                             double* dst, int nplanes);
+void launch_grid_to_native(cudaStream_t s, const Dims& d, const double* ref, double* nat, int ncomp);
+void launch_grid_to_reference(cudaStream_t s, const Dims& d, const double* nat, double* ref, int ncomp);
+template <typename R>
+void launch_grid_cast(cudaStream_t s, size_t n, const R* src, double* dst);
+
+// ---- CNAB2 (gd_cnab2.cu) ----
+struct Cnab2Args {
+  double* u[5];
+  const double* nl[5];
+  double* prev[5];
+  int kind[5];
+  int nfield;
+  int boot;
+  int clamp_rows;
+  double inv_dt, lin_weight;
+};
+void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,
+                  const Cnab2Args& a);
+void launch_energy(cudaStream_t s, const Dims& d, const int* lof, const double* utor, const double* upol,
+                   const double* btor, const double* bpol, double* partial, double* out);
+void launch_check_finite(cudaStream_t s, size_t n, const double* a, int* flag);
+
+inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace gd

@@ -1,0 +1,182 @@
+// gd_spectral.cu -- spectral-space operators on the native layout (two planes
+// Re/Im of [r][j], j m-major), plus layout conversions used by the host ABI.
+#include "gd_internal.cuh"
+
+namespace gd {
+
+// compute_all_gradients_spectral! (src/scalar_field_common.jl:125-345):
+// theta derivative by the reference's recurrence coefficients (:158,171), phi
+// derivative i m, radial derivative by the banded D1, then x 1/r on the
+// angular components (:317-321).  In m-major order (l +- 1, m) sits at j +- 1.
+__global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __restrict__ mof,
+                            const double* __restrict__ rinv, const double* __restrict__ d1,
+                            const double* __restrict__ T, double* __restrict__ gth, double* __restrict__ gph,
+                            double* __restrict__ gr) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (j >= d.nlm) return;
+  const int l = lof[j], m = mof[j];
+  const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
+  const double* Tre = T;
+  const double* Tim = T + plane;
+  const size_t at = (size_t)k * NM + j;
+  double dr = 0.0, di = 0.0;
+  if (l + 1 <= d.L) {
+    const double Ap = sqrt((double)(l + 1) * (l + 1) - (double)m * m) * sqrt((double)(l + 1 + m) * (double)(l + 1 - m)) /
+                      (2.0 * l + 1.0);
+    dr += Ap * Tre[at + 1];
+    di += Ap * Tim[at + 1];
+  }
+  if (l >= 1 && l - 1 >= m) {
+    const double Am = -sqrt((double)l * l - (double)m * m) * sqrt((double)(l + m) * (double)(l - m)) / (2.0 * l - 1.0);
+    dr += Am * Tre[at - 1];
+    di += Am * Tim[at - 1];
+  }
+  const double ri = rinv[k];
+  gth[at] = dr * ri;
+  gth[plane + at] = di * ri;
+  gph[at] = (-(double)m * Tim[at]) * ri;
+  gph[plane + at] = ((double)m * Tre[at]) * ri;
+  const int nbw = 2 * d.kl + 1;
+  double sr = 0.0, si = 0.0;
+  const int j0 = k - d.kl > 0 ? k - d.kl : 0;
+  const int j1 = k + d.kl < d.nr - 1 ? k + d.kl : d.nr - 1;
+  for (int jj = j0; jj <= j1; ++jj) {
+    const double cf = d1[(d.kl + k - jj) + (size_t)nbw * jj];
+    sr += cf * Tre[(size_t)jj * NM + j];
+    si += cf * Tim[(size_t)jj * NM + j];
+  }
+  gr[at] = sr;
+  gr[plane + at] = si;
+}
+
+void launch_gradients(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
+                      const double* d1, const double* T, double* gth, double* gph, double* gr) {
+  dim3 grid(ceil_div(d.nlm, 128), d.nr);
+  k_gradients<<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr);
+}
+
+// compute_vorticity_spectral_full! (src/velocity.jl:340-441) and
+// compute_current_density_spectral! (src/magnetic.jl:253-349):
+//   curl_tor = l(l+1)/r^2 P - D2 P - (2/r) D1 P,   curl_pol = -l(l+1)/r^2 T.
+__global__ void k_curl(Dims d, const int* __restrict__ lof, const double* __restrict__ rinv,
+                       const double* __restrict__ rinv2, const double* __restrict__ d1,
+                       const double* __restrict__ d2, const double* __restrict__ tor,
+                       const double* __restrict__ pol, double* __restrict__ otor, double* __restrict__ opol) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (j >= d.nlm) return;
+  const double lf = (double)lof[j] * (lof[j] + 1.0);
+  const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
+  const int nbw = 2 * d.kl + 1;
+  const int j0 = k - d.kl > 0 ? k - d.kl : 0;
+  const int j1 = k + d.kl < d.nr - 1 ? k + d.kl : d.nr - 1;
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const double* P = pol + c * plane;
+    double a1 = 0.0, a2 = 0.0;
+    for (int jj = j0; jj <= j1; ++jj) {
+      const size_t q = (d.kl + k - jj) + (size_t)nbw * jj;
+      const double v = P[(size_t)jj * NM + j];
+      a1 += d1[q] * v;
+      a2 += d2[q] * v;
+    }
+    const size_t at = (size_t)k * NM + j;
+    otor[c * plane + at] = lf * rinv2[k] * P[at] - a2 - 2.0 * rinv[k] * a1;
+    opol[c * plane + at] = -lf * rinv2[k] * tor[c * plane + at];
+  }
+}
+
+void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* rinv, const double* rinv2,
+                 const double* d1, const double* d2, const double* tor, const double* pol, double* otor,
+                 double* opol) {
+  dim3 grid(ceil_div(d.nlm, 128), d.nr);
+  k_curl<<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol);
+}
+
+// apply_temperature_boundary_conditions_spectral! (src/thermal.jl:262-303):
+// Dirichlet rows r = ri and r = ro of the temperature state.
+__global__ void k_temperature_bc(Dims d, const double* __restrict__ bv, double* __restrict__ T) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.nlm) return;
+  const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
+  T[j] = bv[j];
+  T[plane + j] = 0.0;
+  T[(size_t)(d.nr - 1) * NM + j] = bv[NM + j];
+  T[plane + (size_t)(d.nr - 1) * NM + j] = 0.0;
+}
+
+void launch_temperature_bc(cudaStream_t s, const Dims& d, const double* bvals_native, double* T) {
+  k_temperature_bc<<<ceil_div(d.nlm, 256), 256, 0, s>>>(d, bvals_native, T);
+}
+
+__global__ void k_perm(int nlm, size_t rows, const int* __restrict__ perm, const double* __restrict__ src,
+                       double* __restrict__ dst, int to_native) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t row = blockIdx.y + (size_t)gridDim.y * blockIdx.z;
+  if (q >= nlm || row >= rows) return;
+  const size_t base = row * nlm;
+  if (to_native) dst[base + perm[q]] = src[base + q];
+  else dst[base + q] = src[base + perm[q]];
+}
+
+static void launch_perm(cudaStream_t s, const Dims& d, const int* perm, const double* src, double* dst, int nplanes,
+                        int to_native) {
+  const size_t rows = (size_t)nplanes * d.nr;
+  const unsigned gy = (unsigned)(rows < 65535 ? rows : 65535);
+  const unsigned gz = (unsigned)((rows + gy - 1) / gy);
+  dim3 grid(ceil_div(d.nlm, 256), gy, gz);
+  k_perm<<<grid, 256, 0, s>>>(d.nlm, rows, perm, src, dst, to_native);
+}
+
+void launch_lmajor_to_native(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,
+                             double* dst, int nplanes) {
+  launch_perm(s, d, native_of_lmajor, src, dst, nplanes, 1);
+}
+void launch_native_to_lmajor(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,
+                             double* dst, int nplanes) {
+  launch_perm(s, d, native_of_lmajor, src, dst, nplanes, 0);
+}
+
+// Per-shell transpose between the reference grid layout [r][phi][theta] and
+// the native [r][theta][phi].
+__global__ void k_transpose(int rows_in, int cols_in, const double* __restrict__ src, double* __restrict__ dst) {
+  __shared__ double tile[32][33];
+  const size_t shell = blockIdx.z;
+  const double* s = src + shell * (size_t)rows_in * cols_in;
+  double* o = dst + shell * (size_t)rows_in * cols_in;
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = r0 + k, c = c0 + threadIdx.x;
+    if (r < rows_in && c < cols_in) tile[k][threadIdx.x] = s[(size_t)r * cols_in + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int c = c0 + k, r = r0 + threadIdx.x;
+    if (r < rows_in && c < cols_in) o[(size_t)c * rows_in + r] = tile[threadIdx.x][k];
+  }
+}
+
+void launch_grid_to_native(cudaStream_t s, const Dims& d, const double* ref, double* nat, int ncomp) {
+  // ref: rows = phi (nlon), cols = theta (nlat)
+  dim3 grid(ceil_div(d.nlat, 32), ceil_div(d.nlon, 32), (unsigned)(d.nr * ncomp));
+  k_transpose<<<grid, dim3(32, 8), 0, s>>>(d.nlon, d.nlat, ref, nat);
+}
+void launch_grid_to_reference(cudaStream_t s, const Dims& d, const double* nat, double* ref, int ncomp) {
+  dim3 grid(ceil_div(d.nlon, 32), ceil_div(d.nlat, 32), (unsigned)(d.nr * ncomp));
+  k_transpose<<<grid, dim3(32, 8), 0, s>>>(d.nlat, d.nlon, nat, ref);
+}
+
+template <typename R>
+__global__ void k_cast(size_t n, const R* __restrict__ src, double* __restrict__ dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+template <typename R>
+void launch_grid_cast(cudaStream_t s, size_t n, const R* src, double* dst) {
+  k_cast<R><<<148 * 8, 256, 0, s>>>(n, src, dst);
+}
+template void launch_grid_cast<float>(cudaStream_t, size_t, const float*, double*);
+template void launch_grid_cast<double>(cudaStream_t, size_t, const double*, double*);
+
+}  // namespace gd

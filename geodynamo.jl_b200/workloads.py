@@ -1,0 +1,74 @@
+"""Seeded synthetic workloads (no dataset is involved anywhere on this path).
+
+Shell physics shared by every configuration: ri/ro = 0.35, E = 3e-4, Ra = 80,
+Pr = 1, Pm = 4, theta = 0.5, i_KL = 4; fields u_tor, u_pol, B_tor, B_pol, T.
+
+Initial state: ``numpy.random.default_rng(seed)`` draws standard normals in the
+order field (u_tor, u_pol, b_tor, b_pol, temp) -> r -> l-major (l, m) -> (Re, Im);
+coefficient = g * amp * (l + 1)^-power * sin(pi (r - ri) / (ro - ri)); Im = 0 at
+m = 0; l = 0 of the toroidal/poloidal fields is zero (as randomize_vector_field!,
+src/InitialConditions.jl:81).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+FIELD_ORDER = ("u_tor", "u_pol", "b_tor", "b_pol", "temp")
+
+SHELL_PHYSICS = dict(rratio=0.35, ekman=3e-4, rayleigh=80.0, prandtl=1.0, magnetic_prandtl=4.0,
+                     implicit_theta=0.5, kl=4)
+
+# Named workloads (sizes of the reference's documented configurations).
+CONFIGS = {
+    "shell_l31_nr32": dict(lmax=31, nlat=48, nlon=96, nr=32, dt=1e-5, steps=100),
+    "transform_l127_nr97x9": dict(lmax=127, nlat=192, nlon=384, nr=97, nfield=9),
+    "shell_l255_nr129": dict(lmax=255, nlat=384, nlon=768, nr=129, dt=2e-6, steps=1000),
+    "adjoint_l63_nr65": dict(lmax=63, nlat=96, nlon=192, nr=65, dt=1e-5, steps=200),
+}
+
+
+def lm_arrays(lmax: int, mmax: int):
+    L = np.array([l for l in range(lmax + 1) for m in range(min(l, mmax) + 1)])
+    M = np.array([m for l in range(lmax + 1) for m in range(min(l, mmax) + 1)])
+    return L, M
+
+
+def radial_nodes(nr: int, rratio: float = 0.35):
+    """r_n = ri + (1 + cos(pi (N - n) / (N - 1))) / 2, n = 1..N (src/fields.jl:108-131)."""
+    ri = rratio / (1.0 - rratio)
+    n = np.arange(1, nr + 1)
+    return 0.5 * (1.0 + np.cos(np.pi * (nr - n) / (nr - 1))) + ri
+
+
+def seeded_state(lmax: int, mmax: int, nr: int, seed: int = 0, amp: float = 1e-3, power: float = 2.0,
+                 rratio: float = 0.35):
+    """Dict field -> (re, im), each (nr, nlm) in the reference layout."""
+    rng = np.random.default_rng(seed)
+    L, M = lm_arrays(lmax, mmax)
+    r = radial_nodes(nr, rratio)
+    ri, ro = r[0], r[-1]
+    prof = np.sin(np.pi * (r - ri) / (ro - ri))
+    out = {}
+    for name in FIELD_ORDER:
+        g = rng.standard_normal((nr, L.size, 2))
+        c = g * amp * ((L + 1.0) ** -power)[None, :, None] * prof[:, None, None]
+        re = np.ascontiguousarray(c[..., 0])
+        im = np.ascontiguousarray(c[..., 1])
+        im[:, M == 0] = 0.0
+        if name != "temp":
+            re[:, L == 0] = 0.0
+            im[:, L == 0] = 0.0
+        out[name] = (re, im)
+    return out
+
+
+def transform_batch(lmax: int, mmax: int, nr: int, nfield: int, seed: int = 0, power: float = 1.5):
+    """Complex Gaussian coefficients x (l+1)^-power for nfield fields: (nfield, nr, nlm) x2."""
+    rng = np.random.default_rng(seed)
+    L, M = lm_arrays(lmax, mmax)
+    g = rng.standard_normal((nfield, nr, L.size, 2))
+    c = g * ((L + 1.0) ** -power)[None, None, :, None]
+    re = np.ascontiguousarray(c[..., 0])
+    im = np.ascontiguousarray(c[..., 1])
+    im[:, :, M == 0] = 0.0
+    return re, im

@@ -1,0 +1,170 @@
+/*
+ * gdb200.h -- C ABI of libgdb200.so, the B200 (sm_100a) implementation of
+ * GeoDynamo.jl's per-step hot path: spherical-harmonic transforms, grid-space
+ * nonlinear terms and the CNAB2 banded radial solves.
+ *
+ * Conventions shared by every entry point:
+ *   - Every function returns an int status (GD_OK = 0).  Nothing aborts or
+ *     traps; gd_last_error() returns a message for the last failure on a handle.
+ *   - Host arrays are borrowed for the duration of the call only.
+ *   - Host spectral arrays use the reference layout: two planes (Re, Im), each
+ *     nr x nlm doubles, the (l, m) index fastest in l-major order
+ *     "for l in 0:lmax, m in 0:min(l,mmax)"  (src/fields.jl:6-15,
+ *     src/shtnskit_transforms.jl:177-188).
+ *   - Host physical arrays use the reference layout nr x nlon x nlat doubles,
+ *     theta fastest (src/fields.jl:18-24).
+ *   - Device ("_dev") entry points take device pointers in the native layout
+ *     documented at each declaration and run asynchronously on the handle's
+ *     stream.
+ *   - One host thread per handle; one CUDA stream per handle.
+ */
+#ifndef GDB200_H
+#define GDB200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+enum {
+  GD_OK = 0,
+  GD_ERR_ARG = 1,         /* null pointer, bad id or bad size               */
+  GD_ERR_CONFIG = 2,      /* unsupported grid / parameter combination       */
+  GD_ERR_CUDA = 3,        /* a CUDA runtime call failed                     */
+  GD_ERR_NONFINITE = 4,   /* a NaN/Inf was detected in the state            */
+  GD_ERR_SINGULAR = 5,    /* zero pivot in a banded LU factorisation        */
+  GD_ERR_UNSUPPORTED = 6, /* feature not available on this device           */
+  GD_ERR_STATE = 7        /* call order violated                            */
+};
+
+/* Field ids (state, nonlinear terms). */
+enum { GD_U_TOR = 0, GD_U_POL = 1, GD_B_TOR = 2, GD_B_POL = 3, GD_TEMP = 4 };
+
+/* Physical grids kept by the model (velocity.jl, magnetic.jl, thermal.jl). */
+enum {
+  GD_GRID_U_TH = 0, GD_GRID_U_PH = 1, GD_GRID_W_TH = 2, GD_GRID_W_PH = 3,
+  GD_GRID_B_TH = 4, GD_GRID_B_PH = 5, GD_GRID_J_TH = 6, GD_GRID_J_PH = 7,
+  GD_GRID_T = 8, GD_GRID_GTH = 9, GD_GRID_GPH = 10, GD_GRID_GR = 11,
+  GD_GRID_TADV = 12, GD_GRID_VADV_TH = 13, GD_GRID_VADV_PH = 14,
+  GD_GRID_IND_TH = 15, GD_GRID_IND_PH = 16
+};
+
+/* Precision modes. */
+enum { GD_PREC_FP64 = 0, GD_PREC_MIXED = 1 };
+
+/*
+ * Model configuration.  Mirrors GeoDynamoParameters (src/parameters.jl:14-76):
+ * i_L/i_M/i_Th/i_Ph/i_N/i_KL, d_rratio, d_E, d_Ra, d_Pr, d_Pm, d_timestep,
+ * d_implicit, i_B.  The three mode switches resolve reference quirks:
+ *   ab_mode   0: CNAB2, AB1 on the first step only; 1: AB1 on every step
+ *             (step_once! never advances the step counter, simulation.jl:1153).
+ *   bc_mode   0: reference behaviour (temperature Dirichlet rows only,
+ *             thermal.jl:262-303); 1: also zero the r=ri and r=ro rows of all
+ *             five fields after each solve.
+ *   fd_mode   0: radial difference weights from V^T w = rhs (the intent of
+ *             create_derivative_matrix, linear_algebra.jl:90-132);
+ *             1: the literal V c = rhs solve (ill-conditioned, kept for study).
+ */
+typedef struct gd_config {
+  int lmax, mmax, nlat, nlon, nr;
+  int kl;
+  double rratio;
+  double ekman, rayleigh, prandtl, magnetic_prandtl;
+  double dt, implicit_theta;
+  int ab_mode;
+  int bc_mode;
+  int fd_mode;
+  int precision;
+  int magnetic;
+} gd_config;
+
+typedef struct gd_handle gd_handle;
+
+/* ---- lifetime ---------------------------------------------------------------
+ * Replaces initialize_simulation's transform and matrix set-up:
+ * create_shtnskit_config (src/shtnskit_transforms.jl:102-200),
+ * create_radial_domain (src/fields.jl:108-131) and
+ * create_shtns_timestepping_matrices x3 (src/timestep.jl:498-543,
+ * src/simulation.jl:228-231).  Tables, difference weights and LU factors are
+ * computed on the device in FP64. */
+int gd_create(const gd_config* cfg, int device, gd_handle** out);
+int gd_destroy(gd_handle* h);
+const char* gd_last_error(const gd_handle* h);
+/* nlm, bytes of device memory held by the handle. */
+int gd_info(const gd_handle* h, int* nlm, size_t* device_bytes);
+/* Gauss colatitudes (north to south), weights and radial nodes (host out). */
+int gd_grid(gd_handle* h, double* theta, double* weights, double* r);
+/* Switch precision of transforms and nonlinear terms (GD_PREC_*). */
+int gd_set_precision(gd_handle* h, int mode);
+int gd_synchronize(gd_handle* h);
+
+/* ---- state ------------------------------------------------------------------
+ * Host <-> device copies of the five spectral fields in the reference layout. */
+int gd_upload_spectral(gd_handle* h, int field, const double* re, const double* im);
+int gd_download_spectral(gd_handle* h, int field, double* re, double* im);
+int gd_download_nonlinear(gd_handle* h, int field, double* re, double* im);
+int gd_download_grid(gd_handle* h, int grid, double* out);
+/* Temperature Dirichlet values [2][nlm] (inner, outer; boundary_values in
+ * thermal.jl:285,297) and internal sources [nr] (add_internal_sources_local!,
+ * scalar_field_common.jl:416-443).  Either pointer may be NULL. */
+int gd_set_temperature_bc(gd_handle* h, const double* bvals, const double* sources);
+
+/* ---- transforms on host arrays (reference layout) ---------------------------
+ * shtnskit_spectral_to_physical! / batch_spectral_to_physical!
+ * (src/shtnskit_field_functions.jl:11-21, 674-677): nfield scalar fields,
+ * re/im are nfield consecutive nr x nlm planes, grid nfield consecutive grids. */
+int gd_spectral_to_physical(gd_handle* h, int nfield, const double* re, const double* im, double* grid);
+/* shtnskit_physical_to_spectral! (src/shtnskit_field_functions.jl:131-141). */
+int gd_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double* re, double* im);
+/* shtnskit_vector_synthesis!(tor, pol, vec) (src/shtnskit_field_functions.jl:252-282):
+ * poloidal coefficients act as the spheroidal potential; only theta/phi written. */
+int gd_vector_synthesis(gd_handle* h, const double* tor_re, const double* tor_im, const double* pol_re,
+                        const double* pol_im, double* v_theta, double* v_phi);
+/* shtnskit_vector_analysis!(vec, tor, pol) (src/shtnskit_field_functions.jl:291-321). */
+int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re,
+                       double* tor_im, double* pol_re, double* pol_im);
+
+/* ---- model step ---------------------------------------------------------------
+ * compute_temperature_nonlinear! (src/thermal.jl:149-190),
+ * compute_velocity_nonlinear! (src/velocity.jl:312-332),
+ * compute_magnetic_nonlinear! (src/magnetic.jl:131-159) on the device state. */
+int gd_temperature_nonlinear(gd_handle* h);
+int gd_velocity_nonlinear(gd_handle* h);
+int gd_magnetic_nonlinear(gd_handle* h);
+/* apply_master_implicit_step! (src/simulation.jl:1151-1330) with
+ * build_rhs_cnab2! + solve_implicit_step! (src/timestep.jl:610-730). */
+int gd_implicit_step(gd_handle* h);
+/* step_once! (scripts/bench_timestepping.jl:6-18) repeated nsteps times;
+ * after the first step the sequence is replayed from a captured CUDA graph. */
+int gd_step(gd_handle* h, int nsteps);
+/* Like gd_step, but records nothing to host and returns immediately
+ * (asynchronous on the handle's stream). */
+int gd_step_async(gd_handle* h, int nsteps);
+/* Rebuild the implicit matrices for a new time step (src/simulation.jl:335-337). */
+int gd_set_dt(gd_handle* h, double dt);
+/* compute_kinetic_energy / compute_magnetic_energy (src/velocity.jl:782-825,
+ * src/magnetic.jl:504-543), both as 0.5 sum (T^2+P^2)/max(l(l+1),1). */
+int gd_energy(gd_handle* h, double* ekin, double* emag);
+/* Scan the five fields for NaN/Inf; returns GD_ERR_NONFINITE if found. */
+int gd_check_finite(gd_handle* h);
+long gd_step_count(const gd_handle* h);
+
+/* ---- tracing ------------------------------------------------------------------
+ * The handle's CUDA stream (a cudaStream_t passed as void*), so a caller can
+ * time work on it with its own events. */
+int gd_get_stream(gd_handle* h, void** stream);
+/* Per-kernel timing: while enabled, gd_step runs the step sequence without graph
+ * replay and brackets every kernel launch with CUDA events on the handle's
+ * stream; timings accumulate per kernel name. */
+int gd_profile_enable(gd_handle* h, int enable);
+/* Copies up to max entries: names (max x 32 chars, NUL-terminated), total ms and
+ * launch counts; *count receives the number of entries.  Resets the totals. */
+int gd_profile_read(gd_handle* h, int max, char* names, double* ms, int* launches, int* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GDB200_H */

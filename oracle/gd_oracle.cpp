@@ -1,0 +1,991 @@
+// gd_oracle.cpp -- CPU FP64 restatement of GeoDynamo.jl's per-step hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This library is the parity oracle for the CUDA
+// path and the timed CPU baseline.  Only tests/, __graft_entry__.smoke() and
+// bench.py's CPU-baseline / reference legs load it.  The product library
+// (libgdb200.so) never links, loads or calls anything in this directory.
+//
+// Parity status: the reference's transform arithmetic lives in SHTnsKit.jl
+// v1.1.10 (not vendored, no Julia toolchain here), so the SHT conventions below
+// are chosen, documented and pinned by (a) the reference's own scalar
+// round-trip test (test/shtnskit_roundtrip.jl:21-54, relative squared error
+// < 1e-7 at lmax=6, nlat=12, nlon=24, nr=6) and (b) independent scipy/numpy
+// known-answer checks (sph_harm_y, leggauss, dense solves).  Vector
+// transforms, CNAB2 and the nonlinear terms have no reference test; they are
+// restated line by line from the cited Julia sources.
+//
+// Conventions (chosen, documented):
+//   * Gauss-Legendre colatitudes theta_i, ordered north -> south, x_i = cos theta_i.
+//   * phi_j = 2 pi j / nlon.
+//   * Orthonormal Y_lm = Pbar_lm(cos theta) e^{i m phi} with Condon-Shortley phase.
+//   * Real synthesis: f = Re F_0 + 2 Re sum_{m>=1} F_m e^{i m phi},
+//     F_m(theta) = sum_l a_lm Pbar_lm.
+//   * Analysis: a_lm = sum_i w_i Pbar_lm(x_i) (2 pi / nlon) sum_j f e^{-i m phi_j};
+//     Im a_l0 := 0 (shtnskit_field_functions.jl:433-435).
+//   * Vector (spheroidal S = poloidal coefficients, toroidal T):
+//       v_theta = dS/dtheta + (1/sin) dT/dphi,  v_phi = (1/sin) dS/dphi - dT/dtheta,
+//     analysis is the l(l+1)-normalised projection; l = 0 gives 0.
+//
+// Reference-quirk resolutions (literal unless stated):
+//   Q1/Q2  vector synthesis writes only theta/phi; r-components are 0; vector
+//          analysis reads only theta/phi (shtnskit_field_functions.jl:252-321).
+//   Q3     Coriolis latitude index = min(phi index, nlat) (velocity.jl:492-496).
+//   Q4     theta-gradient coefficients literal (scalar_field_common.jl:158,171),
+//          (l+-1, m) located by the l-major ordering (shtnskit_transforms.jl:177-188).
+//   Q5     d/dphi: Re <- -m Im, Im <- m Re, then x 1/r (scalar_field_common.jl:218-219,317-321).
+//   Q6     ab_mode 0: AB1 bootstrap on the first step only; ab_mode 1: AB1 every
+//          step (simulation.jl:1153 with a step counter that never advances).
+//   Q7     bc_mode 0: only temperature Dirichlet rows (thermal.jl:262-303);
+//          bc_mode 1: additionally zero r=ri and r=ro rows of all five fields
+//          after each solve.
+//   Q8     energies 0.5 sum (T^2+P^2)/max(l(l+1),1) (magnetic.jl:519-542).
+//   Q14    create_derivative_matrix (linear_algebra.jl:90-132) solves V c = rhs,
+//          which yields interpolation coefficients, not difference weights
+//          (entries ~1e21, condition ~1e104 at nr=129).  fd_mode 0 (default)
+//          solves the transposed system V^T w = rhs (the stated intent:
+//          "finite difference coefficients"); fd_mode 1 keeps the literal solve.
+//
+// Build: oracle/Makefile (g++ -O3 -fopenmp -ffp-contract=off).
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef std::complex<double> cplx;
+
+extern "C" {
+// Field order is shared with include/gdb200.h (gd_config).
+typedef struct oc_config {
+  int lmax, mmax, nlat, nlon, nr;
+  int kl;
+  double rratio;
+  double ekman, rayleigh, prandtl, magnetic_prandtl;
+  double dt, implicit_theta;
+  int ab_mode;
+  int bc_mode;
+  int fd_mode;
+  int precision;   // ignored by the oracle (always FP64)
+  int magnetic;    // i_B
+} oc_config;
+}
+
+namespace {
+
+const double kPi = 3.14159265358979323846;
+
+// ----------------------------------------------------------------------------
+// Mixed-radix complex FFT (decimation in time, recursive).  Used for the phi
+// direction of every transform (the reference delegates this to FFTW through
+// SHTnsKit).
+// ----------------------------------------------------------------------------
+struct FFT {
+  int n = 0;
+  std::vector<int> factors;
+  std::vector<cplx> tw;  // tw[k] = exp(-2 pi i k / n)
+
+  void init(int n_) {
+    n = n_;
+    factors.clear();
+    int m = n;
+    for (int p : {4, 2, 3, 5}) {
+      while (m % p == 0) { factors.push_back(p); m /= p; }
+    }
+    for (int p = 7; m > 1; p += 2) {
+      while (m % p == 0) { factors.push_back(p); m /= p; }
+    }
+    tw.resize(n);
+    for (int k = 0; k < n; ++k) tw[k] = std::polar(1.0, -2.0 * kPi * k / n);
+  }
+
+  // out[k] = sum_j in[j*istride] exp(sign * 2 pi i j k / len), len = product of f[..]
+  void rec(const cplx* in, int istride, cplx* out, int len, const int* f, int sign) const {
+    if (len == 1) { out[0] = in[0]; return; }
+    const int p = f[0], q = len / p;
+    for (int s = 0; s < p; ++s) rec(in + s * istride, istride * p, out + s * q, q, f + 1, sign);
+    const int step = n / len;  // W_len^e = tw[e*step]
+    cplx tmp[64];
+    std::vector<cplx> big;
+    cplx* t = tmp;
+    if (p > 64) { big.resize(p); t = big.data(); }
+    for (int k = 0; k < q; ++k) {
+      for (int s = 0; s < p; ++s) t[s] = out[s * q + k];
+      for (int u = 0; u < p; ++u) {
+        const int kk = k + q * u;
+        cplx acc = t[0];
+        for (int s = 1; s < p; ++s) {
+          long e = (long)s * kk % len;
+          cplx w = tw[e * step];
+          if (sign > 0) w = std::conj(w);
+          acc += t[s] * w;
+        }
+        out[u * q + k] = acc;
+      }
+    }
+  }
+  void forward(const cplx* in, cplx* out) const { rec(in, 1, out, n, factors.data(), -1); }
+  void backward(const cplx* in, cplx* out) const { rec(in, 1, out, n, factors.data(), +1); }
+};
+
+inline long lm_index_lmajor(int l, int m, int mmax) {
+  // l-major ordering "for l in 0:lmax, m in 0:min(l,mmax)" (shtnskit_transforms.jl:177-188)
+  long base;
+  if (l <= mmax) base = (long)l * (l + 1) / 2;
+  else base = (long)mmax * (mmax + 1) / 2 + (long)(mmax + 1) * (l - mmax);
+  return base + m;
+}
+
+// Dense solve with partial pivoting (stand-in for Julia's V \ rhs, LAPACK getrf/getrs).
+void dense_solve(int n, std::vector<double> A /* row-major n x n */, std::vector<double>& b) {
+  std::vector<int> piv(n);
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = std::fabs(A[k * n + k]);
+    for (int i = k + 1; i < n; ++i) {
+      double v = std::fabs(A[i * n + k]);
+      if (v > best) { best = v; p = i; }
+    }
+    piv[k] = p;
+    if (p != k) {
+      for (int j = 0; j < n; ++j) std::swap(A[k * n + j], A[p * n + j]);
+      std::swap(b[k], b[p]);
+    }
+    const double d = A[k * n + k];
+    for (int i = k + 1; i < n; ++i) {
+      const double f = A[i * n + k] / d;
+      A[i * n + k] = f;
+      for (int j = k + 1; j < n; ++j) A[i * n + j] = A[i * n + j] - f * A[k * n + j];
+      b[i] = b[i] - f * b[k];
+    }
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int j = i + 1; j < n; ++j) s = s - A[i * n + j] * b[j];
+    b[i] = s / A[i * n + i];
+  }
+}
+
+enum { F_UTOR = 0, F_UPOL = 1, F_BTOR = 2, F_BPOL = 3, F_TEMP = 4, NFIELD = 5 };
+
+struct Oracle {
+  oc_config c{};
+  int nlm = 0, nth = 0, nbw = 0;  // nbw = 2*kl+1
+  std::vector<int> lv, mv;        // l, m per l-major index
+  std::vector<long> moff;         // m-block offsets for [m][l-m] tables
+  std::vector<double> x, w, th, sth;
+  std::vector<double> r, rinv, rinv2;
+  std::vector<double> P, dP;      // [moff[m] + (l-m)] * nth + ith  (north half)
+  std::vector<double> d1, d2, lap;  // band (2kl+1) x nr, Julia column-major
+  std::vector<double> lin[3], lu[3];  // per diffusivity kind: [l][band]
+  double nu[3] = {0, 0, 0};
+  FFT fft;
+  // state, reference layout: [r][lm] (lm fastest)
+  std::vector<double> fre[NFIELD], fim[NFIELD];
+  std::vector<double> nre[NFIELD], nim[NFIELD], pre[NFIELD], pim[NFIELD];
+  // persistent physical grids, reference layout [r][phi][theta]
+  std::vector<double> u_th, u_ph, w_th, w_ph, b_th, b_ph, j_th, j_ph;
+  std::vector<double> t_grid, gth_grid, gph_grid, gr_grid, tadv, vadv_th, vadv_ph, ind_th, ind_ph;
+  std::vector<double> bvals;      // [2][nlm] temperature Dirichlet values
+  std::vector<double> sources;    // [nr] internal heat sources
+  long step_count = 0;
+  int nthreads = 1;
+
+  size_t grid_size() const { return (size_t)c.nlat * c.nlon * c.nr; }
+  size_t spec_size() const { return (size_t)nlm * c.nr; }
+
+  int setup(const oc_config* cfg) {
+    c = *cfg;
+    if (c.lmax < 1 || c.mmax < 0 || c.mmax > c.lmax || c.nlat < 2 || (c.nlat & 1) || c.nr < 3)
+      return 1;
+    if (2 * c.mmax >= c.nlon) return 1;
+    if (c.nlat <= c.lmax) return 1;
+    nth = c.nlat / 2;
+    nbw = 2 * c.kl + 1;
+    for (int l = 0; l <= c.lmax; ++l)
+      for (int m = 0; m <= std::min(l, c.mmax); ++m) { lv.push_back(l); mv.push_back(m); }
+    nlm = (int)lv.size();
+    moff.resize(c.mmax + 2);
+    moff[0] = 0;
+    for (int m = 0; m <= c.mmax; ++m) moff[m + 1] = moff[m] + (c.lmax - m + 1);
+    gauss();
+    tables();
+    radial();
+    fft.init(c.nlon);
+    for (int f = 0; f < NFIELD; ++f) {
+      fre[f].assign(spec_size(), 0.0); fim[f].assign(spec_size(), 0.0);
+      nre[f].assign(spec_size(), 0.0); nim[f].assign(spec_size(), 0.0);
+      pre[f].assign(spec_size(), 0.0); pim[f].assign(spec_size(), 0.0);
+    }
+    for (auto* g : {&u_th, &u_ph, &w_th, &w_ph, &b_th, &b_ph, &j_th, &j_ph, &t_grid, &gth_grid,
+                    &gph_grid, &gr_grid, &tadv, &vadv_th, &vadv_ph, &ind_th, &ind_ph})
+      g->assign(grid_size(), 0.0);
+    bvals.assign(2 * (size_t)nlm, 0.0);
+    sources.assign(c.nr, 0.0);
+    build_implicit();
+    return 0;
+  }
+
+  // Gauss-Legendre nodes: Newton iteration on P_n(cos theta) in the theta variable
+  // (the reference obtains them from SHTnsKit.create_gauss_config, shtnskit_transforms.jl:109-112).
+  void gauss() {
+    const int n = c.nlat;
+    x.assign(n, 0); w.assign(n, 0); th.assign(n, 0); sth.assign(n, 0);
+    for (int i = 0; i < (n + 1) / 2; ++i) {
+      double t = kPi * (i + 0.75) / (n + 0.5);
+      double dpdx = 0;
+      for (int it = 0; it < 100; ++it) {
+        const double xx = std::cos(t);
+        double p0 = 1.0, p1 = xx;
+        for (int k = 2; k <= n; ++k) {
+          const double p2 = ((2.0 * k - 1.0) * xx * p1 - (k - 1.0) * p0) / k;
+          p0 = p1; p1 = p2;
+        }
+        // dP_n/dx = n (x P_n - P_{n-1}) / (x^2 - 1)
+        dpdx = n * (xx * p1 - p0) / (xx * xx - 1.0);
+        const double dpdt = -std::sin(t) * dpdx;
+        const double dt = p1 / dpdt;
+        t -= dt;
+        if (std::fabs(dt) < 1e-16 * std::max(1.0, t)) break;
+      }
+      {
+        const double xx = std::cos(t);
+        double p0 = 1.0, p1 = xx;
+        for (int k = 2; k <= n; ++k) {
+          const double p2 = ((2.0 * k - 1.0) * xx * p1 - (k - 1.0) * p0) / k;
+          p0 = p1; p1 = p2;
+        }
+        const double s = std::sin(t);
+        // w = 2 / ((1-x^2) P_n'(x)^2) with (1-x^2) P_n' = n (P_{n-1} - x P_n)
+        const double q = n * (p0 - xx * p1);
+        const double wi = 2.0 * s * s / (q * q);
+        th[i] = t; x[i] = xx; sth[i] = s; w[i] = wi;
+        th[n - 1 - i] = kPi - t; x[n - 1 - i] = -xx; sth[n - 1 - i] = s; w[n - 1 - i] = wi;
+      }
+    }
+  }
+
+  // Orthonormal associated Legendre functions with Condon-Shortley phase and
+  // their theta-derivatives at the north-half nodes.
+  void tables() {
+    const int L = c.lmax;
+    P.assign((size_t)moff[c.mmax + 1] * nth, 0.0);
+    dP.assign((size_t)moff[c.mmax + 1] * nth, 0.0);
+    const int mtop = std::min(c.mmax + 1, L);  // m=1 column needed for m=0 derivatives
+    std::vector<double> col((size_t)(L + 1) * (mtop + 1));
+    for (int i = 0; i < nth; ++i) {
+      const double xx = x[i], s = sth[i];
+      // pmm[m] = Pbar_mm; psm[m] = Pbar_lm / sin for the m>=1 columns (derivative use)
+      double pmm = 1.0 / std::sqrt(4.0 * kPi);
+      for (int m = 0; m <= mtop; ++m) {
+        if (m > 0) pmm = -std::sqrt((2.0 * m + 1.0) / (2.0 * m)) * s * pmm;
+        // column m: l = m..L
+        double* pc = &col[(size_t)m * (L + 1)];
+        pc[m] = pmm;
+        if (m + 1 <= L) pc[m + 1] = std::sqrt(2.0 * m + 3.0) * xx * pmm;
+        for (int l = m + 2; l <= L; ++l) {
+          const double a = std::sqrt((4.0 * l * l - 1.0) / ((double)l * l - (double)m * m));
+          const double b = std::sqrt(((l - 1.0) * (l - 1.0) - (double)m * m) / (4.0 * (l - 1.0) * (l - 1.0) - 1.0));
+          pc[l] = a * (xx * pc[l - 1] - b * pc[l - 2]);
+        }
+      }
+      for (int m = 0; m <= c.mmax; ++m) {
+        const double* pc = &col[(size_t)m * (L + 1)];
+        for (int l = m; l <= L; ++l) {
+          const size_t idx = (size_t)(moff[m] + (l - m)) * nth + i;
+          P[idx] = pc[l];
+          double d;
+          if (m == 0) {
+            d = (l == 0) ? 0.0 : std::sqrt((double)l * (l + 1.0)) * col[(size_t)1 * (L + 1) + l];
+          } else {
+            // dPbar_lm/dtheta = [ l x Pbar_lm - sqrt((2l+1)(l^2-m^2)/(2l-1)) Pbar_{l-1,m} ] / sin
+            const double prev = (l - 1 >= m) ? pc[l - 1] : 0.0;
+            const double cf = (l > m) ? std::sqrt((2.0 * l + 1.0) * ((double)l * l - (double)m * m) / (2.0 * l - 1.0)) : 0.0;
+            d = (l * xx * pc[l] - cf * prev) / s;
+          }
+          dP[idx] = d;
+        }
+      }
+    }
+  }
+
+  // Radial grid (fields.jl:108-131) and banded operators (linear_algebra.jl:90-151).
+  void radial() {
+    const int N = c.nr;
+    r.assign(N, 0); rinv.assign(N, 0); rinv2.assign(N, 0);
+    const double ri = c.rratio / (1.0 - c.rratio);
+    for (int n = 1; n <= N; ++n) {
+      r[n - 1] = 0.5 * (1.0 + std::cos(kPi * (double)(N - n) / (double)(N - 1))) + ri;
+    }
+    for (int n = 0; n < N; ++n) { rinv[n] = std::pow(r[n], -1.0); rinv2[n] = std::pow(r[n], -2.0); }
+    d1 = fd_matrix(1);
+    d2 = fd_matrix(2);
+    lap = d2;
+    for (int n = 0; n < N; ++n) {
+      for (int j = std::max(0, n - c.kl); j <= std::min(N - 1, n + c.kl); ++j) {
+        const int br = c.kl + n - j;
+        lap[br + (size_t)nbw * j] = lap[br + (size_t)nbw * j] + 2.0 * rinv[n] * d1[br + (size_t)nbw * j];
+      }
+    }
+  }
+
+  std::vector<double> fd_matrix(int order) const {
+    const int N = c.nr, bw = c.kl;
+    std::vector<double> data((size_t)nbw * N, 0.0);
+    for (int n = 0; n < N; ++n) {
+      const int left = std::max(0, n - bw), right = std::min(N - 1, n + bw);
+      const int S = right - left + 1;
+      std::vector<double> V((size_t)S * S, 1.0);  // V[i][j] = (r_i - r_n)^j
+      for (int j = 1; j < S; ++j)
+        for (int i = 0; i < S; ++i) V[(size_t)i * S + j] = V[(size_t)i * S + j - 1] * (r[left + i] - r[n]);
+      std::vector<double> rhs(S, 0.0);
+      if (order <= S) rhs[order] = (order == 2) ? 2.0 : 1.0;
+      if (c.fd_mode == 0) {
+        std::vector<double> VT((size_t)S * S);
+        for (int i = 0; i < S; ++i)
+          for (int j = 0; j < S; ++j) VT[(size_t)i * S + j] = V[(size_t)j * S + i];
+        dense_solve(S, VT, rhs);
+      } else {
+        dense_solve(S, V, rhs);
+      }
+      for (int i = 0; i < S; ++i) {
+        const int idx = left + i;
+        const int br = bw + n - idx;
+        data[br + (size_t)nbw * idx] = rhs[i];
+      }
+    }
+    return data;
+  }
+
+  // create_shtns_timestepping_matrices + factorize_banded (timestep.jl:498-543,
+  // linear_algebra.jl:23-57), one LU per unique l and diffusivity kind.
+  void build_implicit() {
+    nu[0] = c.magnetic_prandtl;                    // velocity (simulation.jl:229)
+    nu[1] = 1.0;                                   // magnetic (simulation.jl:230)
+    nu[2] = c.magnetic_prandtl / c.prandtl;        // temperature (simulation.jl:231)
+    const int N = c.nr, bw = c.kl;
+    const size_t bsz = (size_t)nbw * N;
+    const double inv_dt = 1.0 / c.dt, mth = -c.implicit_theta;
+    for (int k = 0; k < 3; ++k) {
+      lin[k].assign(bsz * (c.lmax + 1), 0.0);
+      lu[k].assign(bsz * (c.lmax + 1), 0.0);
+      for (int l = 0; l <= c.lmax; ++l) {
+        double* L = &lin[k][bsz * l];
+        double* A = &lu[k][bsz * l];
+        for (size_t q = 0; q < bsz; ++q) L[q] = nu[k] * lap[q];
+        const double lf = (double)l * (l + 1);
+        for (int n = 0; n < N; ++n) L[bw + (size_t)nbw * n] = L[bw + (size_t)nbw * n] - nu[k] * lf * rinv2[n];
+        for (size_t q = 0; q < bsz; ++q) A[q] = L[q] * mth;
+        for (int n = 0; n < N; ++n) A[bw + (size_t)nbw * n] = A[bw + (size_t)nbw * n] + inv_dt;
+        factorize(A);
+      }
+    }
+  }
+
+  void factorize(double* lu_) const {
+    const int N = c.nr, bw = c.kl;
+    auto at = [&](int i, int j) -> double& { return lu_[(bw + i - j) + (size_t)nbw * j]; };
+    for (int k = 0; k < N - 1; ++k) {
+      const double piv = at(k, k);
+      const int imax = std::min(N - 1, k + bw);
+      for (int i = k + 1; i <= imax; ++i) {
+        const double Lf = at(i, k) / piv;
+        at(i, k) = Lf;
+        for (int j = k + 1; j <= imax; ++j) at(i, j) = at(i, j) - Lf * at(k, j);
+      }
+    }
+  }
+
+  void solve(const double* lu_, double* xv) const {
+    const int N = c.nr, bw = c.kl;
+    auto at = [&](int i, int j) -> double { return lu_[(bw + i - j) + (size_t)nbw * j]; };
+    for (int i = 0; i < N; ++i) {
+      double s = 0.0;
+      for (int j = std::max(0, i - bw); j < i; ++j) s += at(i, j) * xv[j];
+      xv[i] = xv[i] - s;
+    }
+    for (int i = N - 1; i >= 0; --i) {
+      double s = 0.0;
+      for (int j = i + 1; j <= std::min(N - 1, i + bw); ++j) s += at(i, j) * xv[j];
+      xv[i] = (xv[i] - s) / at(i, i);
+    }
+  }
+
+  // banded matvec: out[i] = sum_j A[i,j] v[j] (apply_banded_full!, timestep.jl:89-101)
+  void band_apply(const double* A, const double* v, double* out) const {
+    const int N = c.nr, bw = c.kl;
+    for (int i = 0; i < N; ++i) out[i] = 0.0;
+    for (int j = 0; j < N; ++j)
+      for (int i = std::max(0, j - bw); i <= std::min(N - 1, j + bw); ++i)
+        out[i] += A[(bw + i - j) + (size_t)nbw * j] * v[j];
+  }
+
+  // ------------------------------------------------------------------------
+  // Transforms, one shell at a time (SHTnsKit.synthesis / analysis /
+  // SHsphtor_to_spat / spat_to_SHsphtor as called from
+  // shtnskit_field_functions.jl:102-123, 218-239, 252-321).
+  // ------------------------------------------------------------------------
+  // Inverse real DFT of rows: F[theta][m] (m = 0..mmax) -> grid column k of reference layout.
+  void phi_synth(const std::vector<cplx>& F, double* grid_r /* [phi][theta] */) const {
+    const int n = c.nlon, M = c.mmax;
+    std::vector<cplx> Z(n), z(n);
+    for (int i = 0; i < c.nlat; i += 2) {
+      const int i2 = i + 1;
+      std::fill(Z.begin(), Z.end(), cplx(0, 0));
+      const cplx* A = &F[(size_t)i * (M + 1)];
+      const cplx* B = &F[(size_t)i2 * (M + 1)];
+      Z[0] = cplx(A[0].real(), 0) + cplx(0, 1) * cplx(B[0].real(), 0);
+      for (int m = 1; m <= M; ++m) {
+        Z[m] += A[m] + cplx(0, 1) * B[m];
+        Z[n - m] += std::conj(A[m]) + cplx(0, 1) * std::conj(B[m]);
+      }
+      fft.backward(Z.data(), z.data());
+      for (int j = 0; j < n; ++j) {
+        grid_r[(size_t)j * c.nlat + i] = z[j].real();
+        grid_r[(size_t)j * c.nlat + i2] = z[j].imag();
+      }
+    }
+  }
+  // Forward real DFT of rows, scaled by 2 pi / nlon: grid -> G[theta][m]
+  void phi_analysis(const double* grid_r, std::vector<cplx>& G) const {
+    const int n = c.nlon, M = c.mmax;
+    std::vector<cplx> z(n), Z(n);
+    const double sc = 2.0 * kPi / n;
+    for (int i = 0; i < c.nlat; i += 2) {
+      const int i2 = i + 1;
+      for (int j = 0; j < n; ++j)
+        z[j] = cplx(grid_r[(size_t)j * c.nlat + i], grid_r[(size_t)j * c.nlat + i2]);
+      fft.forward(z.data(), Z.data());
+      for (int m = 0; m <= M; ++m) {
+        const cplx zk = Z[m], zn = std::conj(Z[(n - m) % n]);
+        const cplx X = 0.5 * (zk + zn);
+        const cplx Y = cplx(0, -0.5) * (zk - zn);
+        G[(size_t)i * (M + 1) + m] = sc * X;
+        G[(size_t)i2 * (M + 1) + m] = sc * Y;
+      }
+    }
+  }
+
+  void gather_shell(const double* re, const double* im, int k, std::vector<cplx>& a) const {
+    // a in [m][l-m] order for shell k
+    a.resize(moff[c.mmax + 1]);
+    for (int q = 0; q < nlm; ++q) {
+      const int l = lv[q], m = mv[q];
+      a[moff[m] + (l - m)] = cplx(re[(size_t)k * nlm + q], im[(size_t)k * nlm + q]);
+    }
+  }
+  void scatter_shell(const std::vector<cplx>& a, int k, double* re, double* im) const {
+    for (int q = 0; q < nlm; ++q) {
+      const int l = lv[q], m = mv[q];
+      const cplx v = a[moff[m] + (l - m)];
+      re[(size_t)k * nlm + q] = v.real();
+      im[(size_t)k * nlm + q] = (m == 0) ? 0.0 : v.imag();  // shtnskit_field_functions.jl:433-435
+    }
+  }
+
+  void synth_scalar_shell(const double* re, const double* im, int k, double* grid) const {
+    const int M = c.mmax;
+    std::vector<cplx> a, F((size_t)c.nlat * (M + 1));
+    gather_shell(re, im, k, a);
+    for (int m = 0; m <= M; ++m) {
+      const cplx* am = &a[moff[m]];
+      const int nl = c.lmax - m + 1;
+      for (int i = 0; i < nth; ++i) {
+        cplx e(0, 0), o(0, 0);
+        for (int q = 0; q < nl; ++q) {
+          const double p = P[(size_t)(moff[m] + q) * nth + i];
+          if (q & 1) o += p * am[q]; else e += p * am[q];
+        }
+        F[(size_t)i * (M + 1) + m] = e + o;
+        F[(size_t)(c.nlat - 1 - i) * (M + 1) + m] = e - o;
+      }
+    }
+    phi_synth(F, grid + (size_t)k * c.nlat * c.nlon);
+  }
+
+  void analysis_scalar_shell(const double* grid, int k, double* re, double* im) const {
+    const int M = c.mmax;
+    std::vector<cplx> G((size_t)c.nlat * (M + 1)), a(moff[M + 1]);
+    phi_analysis(grid + (size_t)k * c.nlat * c.nlon, G);
+    for (int m = 0; m <= M; ++m) {
+      const int nl = c.lmax - m + 1;
+      for (int q = 0; q < nl; ++q) a[moff[m] + q] = 0;
+      for (int i = 0; i < nth; ++i) {
+        const cplx gn = G[(size_t)i * (M + 1) + m], gs = G[(size_t)(c.nlat - 1 - i) * (M + 1) + m];
+        const cplx ge = w[i] * (gn + gs), go = w[i] * (gn - gs);
+        for (int q = 0; q < nl; ++q) {
+          const double p = P[(size_t)(moff[m] + q) * nth + i];
+          a[moff[m] + q] += p * ((q & 1) ? go : ge);
+        }
+      }
+    }
+    scatter_shell(a, k, re, im);
+  }
+
+  void synth_vector_shell(const double* tre, const double* tim, const double* pre_, const double* pim_,
+                          int k, double* vth, double* vph) const {
+    const int M = c.mmax;
+    std::vector<cplx> S, T, Ft((size_t)c.nlat * (M + 1)), Fp((size_t)c.nlat * (M + 1));
+    gather_shell(pre_, pim_, k, S);  // poloidal -> spheroidal (shtnskit_field_functions.jl:274)
+    gather_shell(tre, tim, k, T);
+    const cplx I(0, 1);
+    for (int m = 0; m <= M; ++m) {
+      const cplx* Sm = &S[moff[m]];
+      const cplx* Tm = &T[moff[m]];
+      const int nl = c.lmax - m + 1;
+      for (int i = 0; i < nth; ++i) {
+        cplx PSe(0, 0), PSo(0, 0), PTe(0, 0), PTo(0, 0), DSe(0, 0), DSo(0, 0), DTe(0, 0), DTo(0, 0);
+        for (int q = 0; q < nl; ++q) {
+          const size_t ix = (size_t)(moff[m] + q) * nth + i;
+          const double p = P[ix], d = dP[ix];
+          if (q & 1) { PSo += p * Sm[q]; PTo += p * Tm[q]; DSo += d * Sm[q]; DTo += d * Tm[q]; }
+          else { PSe += p * Sm[q]; PTe += p * Tm[q]; DSe += d * Sm[q]; DTe += d * Tm[q]; }
+        }
+        const double ims = (double)m / sth[i];
+        // north
+        {
+          const cplx PS = PSe + PSo, PT = PTe + PTo, DS = DSe + DSo, DT = DTe + DTo;
+          Ft[(size_t)i * (M + 1) + m] = DS + I * ims * PT;
+          Fp[(size_t)i * (M + 1) + m] = I * ims * PS - DT;
+        }
+        // south: P parity (-1)^(l-m), dP parity (-1)^(l-m+1)
+        {
+          const cplx PS = PSe - PSo, PT = PTe - PTo, DS = DSo - DSe, DT = DTo - DTe;
+          const int is = c.nlat - 1 - i;
+          Ft[(size_t)is * (M + 1) + m] = DS + I * ims * PT;
+          Fp[(size_t)is * (M + 1) + m] = I * ims * PS - DT;
+        }
+      }
+    }
+    phi_synth(Ft, vth + (size_t)k * c.nlat * c.nlon);
+    phi_synth(Fp, vph + (size_t)k * c.nlat * c.nlon);
+  }
+
+  void analysis_vector_shell(const double* vth, const double* vph, int k, double* tre, double* tim,
+                             double* pre_, double* pim_) const {
+    const int M = c.mmax;
+    std::vector<cplx> Gt((size_t)c.nlat * (M + 1)), Gp((size_t)c.nlat * (M + 1));
+    std::vector<cplx> S(moff[M + 1]), T(moff[M + 1]);
+    phi_analysis(vth + (size_t)k * c.nlat * c.nlon, Gt);
+    phi_analysis(vph + (size_t)k * c.nlat * c.nlon, Gp);
+    const cplx I(0, 1);
+    for (int m = 0; m <= M; ++m) {
+      const int nl = c.lmax - m + 1;
+      for (int q = 0; q < nl; ++q) { S[moff[m] + q] = 0; T[moff[m] + q] = 0; }
+      for (int i = 0; i < nth; ++i) {
+        const int is = c.nlat - 1 - i;
+        const cplx tn = Gt[(size_t)i * (M + 1) + m], ts = Gt[(size_t)is * (M + 1) + m];
+        const cplx pn = Gp[(size_t)i * (M + 1) + m], ps = Gp[(size_t)is * (M + 1) + m];
+        const double ims = (double)m / sth[i];
+        const cplx tp = w[i] * (tn + ts), tm = w[i] * (tn - ts);
+        const cplx pp = w[i] * (pn + ps), pm = w[i] * (pn - ps);
+        for (int q = 0; q < nl; ++q) {
+          const size_t ix = (size_t)(moff[m] + q) * nth + i;
+          const double p = P[ix], d = dP[ix];
+          // P-weighted terms use the P parity, dP-weighted terms the opposite parity
+          const cplx Pt = (q & 1) ? tm : tp, Pp = (q & 1) ? pm : pp;
+          const cplx Dt = (q & 1) ? tp : tm, Dp = (q & 1) ? pp : pm;
+          S[moff[m] + q] += d * Dt - I * ims * p * Pp;
+          T[moff[m] + q] += -I * ims * p * Pt - d * Dp;
+        }
+      }
+      for (int q = 0; q < nl; ++q) {
+        const int l = m + q;
+        const double f = (l == 0) ? 0.0 : 1.0 / ((double)l * (l + 1.0));
+        S[moff[m] + q] *= f;
+        T[moff[m] + q] *= f;
+      }
+    }
+    scatter_shell(S, k, pre_, pim_);  // spat_to_SHsphtor returns (pol=S, tor=T), :313-317
+    scatter_shell(T, k, tre, tim);
+  }
+
+  void synth_scalar(const double* re, const double* im, double* grid) const {
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads)
+    for (int k = 0; k < c.nr; ++k) synth_scalar_shell(re, im, k, grid);
+  }
+  void analysis_scalar(const double* grid, double* re, double* im) const {
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads)
+    for (int k = 0; k < c.nr; ++k) analysis_scalar_shell(grid, k, re, im);
+  }
+  void synth_vector(const double* tre, const double* tim, const double* pre_, const double* pim_,
+                    double* vth, double* vph) const {
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads)
+    for (int k = 0; k < c.nr; ++k) synth_vector_shell(tre, tim, pre_, pim_, k, vth, vph);
+  }
+  void analysis_vector(const double* vth, const double* vph, double* tre, double* tim, double* pre_,
+                       double* pim_) const {
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads)
+    for (int k = 0; k < c.nr; ++k) analysis_vector_shell(vth, vph, k, tre, tim, pre_, pim_);
+  }
+
+  // ------------------------------------------------------------------------
+  // Spectral operators
+  // ------------------------------------------------------------------------
+  // compute_all_gradients_spectral! (scalar_field_common.jl:125-345)
+  void gradients(const double* re, const double* im, double* gt_re, double* gt_im, double* gp_re,
+                 double* gp_im, double* gr_re, double* gr_im) const {
+    const int N = c.nr, bw = c.kl;
+#pragma omp parallel for num_threads(nthreads)
+    for (int k = 0; k < N; ++k) {
+      for (int q = 0; q < nlm; ++q) {
+        const int l = lv[q], m = mv[q];
+        double dr = 0, di = 0;
+        if (l + 1 <= c.lmax && m <= c.mmax) {
+          const long qp = lm_index_lmajor(l + 1, m, c.mmax);
+          const double Ap = std::sqrt((double)(l + 1) * (l + 1) - (double)m * m) *
+                            std::sqrt((double)(l + 1 + m) * (double)(l + 1 - m)) / (2.0 * l + 1.0);
+          dr += Ap * re[(size_t)k * nlm + qp];
+          di += Ap * im[(size_t)k * nlm + qp];
+        }
+        if (l >= 1 && l - 1 >= m) {
+          const long qm = lm_index_lmajor(l - 1, m, c.mmax);
+          const double Am = -std::sqrt((double)l * l - (double)m * m) *
+                            std::sqrt((double)(l + m) * (double)(l - m)) / (2.0 * l - 1.0);
+          dr += Am * re[(size_t)k * nlm + qm];
+          di += Am * im[(size_t)k * nlm + qm];
+        }
+        const double ri_ = rinv[k];
+        gt_re[(size_t)k * nlm + q] = dr * ri_;
+        gt_im[(size_t)k * nlm + q] = di * ri_;
+        gp_re[(size_t)k * nlm + q] = (-(double)m * im[(size_t)k * nlm + q]) * ri_;
+        gp_im[(size_t)k * nlm + q] = ((double)m * re[(size_t)k * nlm + q]) * ri_;
+        double sr = 0, si = 0;
+        for (int j = std::max(0, k - bw); j <= std::min(N - 1, k + bw); ++j) {
+          const double cf = d1[(bw + k - j) + (size_t)nbw * j];
+          sr += cf * re[(size_t)j * nlm + q];
+          si += cf * im[(size_t)j * nlm + q];
+        }
+        gr_re[(size_t)k * nlm + q] = sr;
+        gr_im[(size_t)k * nlm + q] = si;
+      }
+    }
+  }
+
+  // compute_vorticity_spectral_full! (velocity.jl:340-441) and
+  // compute_current_density_spectral! (magnetic.jl:253-349): identical algebra.
+  void curl_spectral(const double* tre, const double* tim, const double* pre_, const double* pim_,
+                     double* otre, double* otim, double* opre, double* opim) const {
+    const int N = c.nr, bw = c.kl;
+#pragma omp parallel for num_threads(nthreads)
+    for (int q = 0; q < nlm; ++q) {
+      const double lf = (double)lv[q] * (lv[q] + 1.0);
+      std::vector<double> pr(N), pi(N), d1r(N), d1i(N), d2r(N), d2i(N);
+      for (int k = 0; k < N; ++k) { pr[k] = pre_[(size_t)k * nlm + q]; pi[k] = pim_[(size_t)k * nlm + q]; }
+      band_apply(d1.data(), pr.data(), d1r.data());
+      band_apply(d1.data(), pi.data(), d1i.data());
+      band_apply(d2.data(), pr.data(), d2r.data());
+      band_apply(d2.data(), pi.data(), d2i.data());
+      (void)bw;
+      for (int k = 0; k < N; ++k) {
+        otre[(size_t)k * nlm + q] = lf * rinv2[k] * pr[k] - d2r[k] - 2.0 * rinv[k] * d1r[k];
+        otim[(size_t)k * nlm + q] = lf * rinv2[k] * pi[k] - d2i[k] - 2.0 * rinv[k] * d1i[k];
+        opre[(size_t)k * nlm + q] = -lf * rinv2[k] * tre[(size_t)k * nlm + q];
+        opim[(size_t)k * nlm + q] = -lf * rinv2[k] * tim[(size_t)k * nlm + q];
+      }
+    }
+  }
+
+  // ------------------------------------------------------------------------
+  // Nonlinear terms
+  // ------------------------------------------------------------------------
+  // compute_temperature_nonlinear! (thermal.jl:149-190)
+  void temperature_nl() {
+    const size_t ss = spec_size();
+    std::vector<double> gtr(ss), gti(ss), gpr(ss), gpi(ss), grr(ss), gri(ss);
+    gradients(fre[F_TEMP].data(), fim[F_TEMP].data(), gtr.data(), gti.data(), gpr.data(), gpi.data(),
+              grr.data(), gri.data());
+    synth_scalar(fre[F_TEMP].data(), fim[F_TEMP].data(), t_grid.data());
+    synth_scalar(gtr.data(), gti.data(), gth_grid.data());
+    synth_scalar(gpr.data(), gpi.data(), gph_grid.data());
+    synth_scalar(grr.data(), gri.data(), gr_grid.data());
+    // -(u . grad T) with u_r = 0 (Q1), u from the previous velocity step (Q13)
+    const size_t plane = (size_t)c.nlat * c.nlon;
+#pragma omp parallel for num_threads(nthreads)
+    for (int k = 0; k < c.nr; ++k) {
+      const double src = sources[k];
+      for (size_t q = 0; q < plane; ++q) {
+        const size_t i = (size_t)k * plane + q;
+        const double ur = 0.0;
+        double v = -(ur * gr_grid[i] + u_th[i] * gth_grid[i] + u_ph[i] * gph_grid[i]);
+        if (src != 0.0) v += src;  // add_internal_sources_local! skips all-zero sources
+        tadv[i] = v;
+      }
+    }
+    analysis_scalar(tadv.data(), nre[F_TEMP].data(), nim[F_TEMP].data());
+    // apply_temperature_boundary_conditions_spectral! (thermal.jl:262-303): on the state.
+    for (int q = 0; q < nlm; ++q) {
+      fre[F_TEMP][q] = bvals[q];
+      fim[F_TEMP][q] = 0.0;
+      fre[F_TEMP][(size_t)(c.nr - 1) * nlm + q] = bvals[(size_t)nlm + q];
+      fim[F_TEMP][(size_t)(c.nr - 1) * nlm + q] = 0.0;
+    }
+  }
+
+  // compute_velocity_nonlinear! (velocity.jl:312-332, 447-548, 638-672)
+  void velocity_nl() {
+    const size_t ss = spec_size();
+    synth_vector(fre[F_UTOR].data(), fim[F_UTOR].data(), fre[F_UPOL].data(), fim[F_UPOL].data(),
+                 u_th.data(), u_ph.data());
+    std::vector<double> otr(ss), oti(ss), opr(ss), opi(ss);
+    curl_spectral(fre[F_UTOR].data(), fim[F_UTOR].data(), fre[F_UPOL].data(), fim[F_UPOL].data(),
+                  otr.data(), oti.data(), opr.data(), opi.data());
+    synth_vector(otr.data(), oti.data(), opr.data(), opi.data(), w_th.data(), w_ph.data());
+    const double rf = c.magnetic_prandtl / c.ekman;  // rossby_factor, velocity.jl:456
+    const double adv_coeff = -rf;
+    const double lf = c.magnetic_prandtl / c.ekman;  // lorentz_factor, velocity.jl:649
+    const size_t plane = (size_t)c.nlat * c.nlon;
+#pragma omp parallel for num_threads(nthreads)
+    for (int k = 0; k < c.nr; ++k) {
+      for (int j = 0; j < c.nlon; ++j) {
+        const int tidx = std::min(j, c.nlat - 1);  // Q3: theta_idx = min(j, nlat)
+        const double st = std::sin(th[tidx]), ct = std::cos(th[tidx]);
+        for (int i = 0; i < c.nlat; ++i) {
+          const size_t q = (size_t)k * plane + (size_t)j * c.nlat + i;
+          const double ur = 0.0, wr = 0.0;
+          const double uth = u_th[q], uph = u_ph[q], wth = w_th[q], wph = w_ph[q];
+          double ath = adv_coeff * (uph * wr - ur * wph);
+          double aph = adv_coeff * (ur * wth - uth * wr);
+          const double zth = -ct * uph, zph = ct * uth + st * ur;
+          ath += -rf * zth;
+          aph += -rf * zph;
+          if (c.magnetic) {
+            const double jr = 0.0, br = 0.0;
+            ath += lf * (j_ph[q] * br - jr * b_ph[q]);
+            aph += lf * (jr * b_th[q] - j_th[q] * br);
+          }
+          vadv_th[q] = ath;
+          vadv_ph[q] = aph;
+        }
+      }
+    }
+    analysis_vector(vadv_th.data(), vadv_ph.data(), nre[F_UTOR].data(), nim[F_UTOR].data(),
+                    nre[F_UPOL].data(), nim[F_UPOL].data());
+  }
+
+  // compute_magnetic_nonlinear! (magnetic.jl:131-159, 375-445)
+  void magnetic_nl() {
+    const size_t ss = spec_size();
+    synth_vector(fre[F_BTOR].data(), fim[F_BTOR].data(), fre[F_BPOL].data(), fim[F_BPOL].data(),
+                 b_th.data(), b_ph.data());
+    std::vector<double> jtr(ss), jti(ss), jpr(ss), jpi(ss);
+    curl_spectral(fre[F_BTOR].data(), fim[F_BTOR].data(), fre[F_BPOL].data(), fim[F_BPOL].data(),
+                  jtr.data(), jti.data(), jpr.data(), jpi.data());
+    synth_vector(jtr.data(), jti.data(), jpr.data(), jpi.data(), j_th.data(), j_ph.data());
+    const size_t n = grid_size();
+#pragma omp parallel for num_threads(nthreads)
+    for (long q = 0; q < (long)n; ++q) {
+      const double ur = 0.0, br = 0.0;
+      ind_th[q] = u_ph[q] * br - ur * b_ph[q];
+      ind_ph[q] = ur * b_th[q] - u_th[q] * br;
+    }
+    std::vector<double> wtr(ss), wti(ss), wpr(ss), wpi(ss);
+    analysis_vector(ind_th.data(), ind_ph.data(), wtr.data(), wti.data(), wpr.data(), wpi.data());
+    // compute_curl_of_induction! (magnetic.jl:407-445)
+    for (int k = 0; k < c.nr; ++k)
+      for (int q = 0; q < nlm; ++q) {
+        const double lfq = (double)lv[q] * (lv[q] + 1.0);
+        const size_t i = (size_t)k * nlm + q;
+        nre[F_BTOR][i] = lfq * wpr[i];
+        nim[F_BTOR][i] = lfq * wpi[i];
+        nre[F_BPOL][i] = -lfq * wtr[i];
+        nim[F_BPOL][i] = -lfq * wti[i];
+      }
+  }
+
+  // apply_master_implicit_step! (simulation.jl:1151-1330) with
+  // build_rhs_cnab2! + solve_implicit_step! (timestep.jl:610-730)
+  void implicit_step() {
+    const bool boot = (c.ab_mode == 1) || (step_count == 0);
+    const int nf = c.magnetic ? NFIELD : 3;
+    const int fields[5] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL};
+    const int N = c.nr;
+    const size_t bsz = (size_t)nbw * N;
+    const double inv_dt = 1.0 / c.dt, lw = 1.0 - c.implicit_theta;
+    for (int fi = 0; fi < nf; ++fi) {
+      const int f = fields[fi];
+      if (boot) { pre[f] = nre[f]; pim[f] = nim[f]; }
+      const int kind = (f == F_TEMP) ? 2 : (f == F_UTOR || f == F_UPOL) ? 0 : 1;
+#pragma omp parallel for num_threads(nthreads)
+      for (int q = 0; q < nlm; ++q) {
+        const int l = lv[q];
+        std::vector<double> ur(N), ui(N), Lr(N), Li(N), xr(N), xi(N);
+        for (int k = 0; k < N; ++k) { ur[k] = fre[f][(size_t)k * nlm + q]; ui[k] = fim[f][(size_t)k * nlm + q]; }
+        band_apply(&lin[kind][bsz * l], ur.data(), Lr.data());
+        band_apply(&lin[kind][bsz * l], ui.data(), Li.data());
+        for (int k = 0; k < N; ++k) {
+          const size_t i = (size_t)k * nlm + q;
+          double vr = inv_dt * ur[k] + 1.5 * nre[f][i] - 0.5 * pre[f][i];
+          double vi = inv_dt * ui[k] + 1.5 * nim[f][i] - 0.5 * pim[f][i];
+          vr += lw * Lr[k];
+          vi += lw * Li[k];
+          xr[k] = vr; xi[k] = vi;
+        }
+        solve(&lu[kind][bsz * l], xr.data());
+        solve(&lu[kind][bsz * l], xi.data());
+        for (int k = 0; k < N; ++k) { fre[f][(size_t)k * nlm + q] = xr[k]; fim[f][(size_t)k * nlm + q] = xi[k]; }
+      }
+    }
+    if (c.bc_mode == 1) {
+      for (int fi = 0; fi < nf; ++fi) {
+        const int f = fields[fi];
+        for (int q = 0; q < nlm; ++q) {
+          fre[f][q] = 0; fim[f][q] = 0;
+          fre[f][(size_t)(N - 1) * nlm + q] = 0; fim[f][(size_t)(N - 1) * nlm + q] = 0;
+        }
+      }
+    }
+    for (int fi = 0; fi < nf; ++fi) { const int f = fields[fi]; pre[f] = nre[f]; pim[f] = nim[f]; }
+    step_count++;
+  }
+
+  void step() {
+    temperature_nl();
+    velocity_nl();
+    if (c.magnetic) magnetic_nl();
+    implicit_step();
+  }
+
+  void energies(double* ekin, double* emag) const {
+    double ek = 0, em = 0;
+    for (int k = 0; k < c.nr; ++k)
+      for (int q = 0; q < nlm; ++q) {
+        const double wgt = 1.0 / std::max((double)lv[q] * (lv[q] + 1.0), 1.0);
+        const size_t i = (size_t)k * nlm + q;
+        ek += wgt * (fre[F_UTOR][i] * fre[F_UTOR][i] + fim[F_UTOR][i] * fim[F_UTOR][i] +
+                     fre[F_UPOL][i] * fre[F_UPOL][i] + fim[F_UPOL][i] * fim[F_UPOL][i]);
+        em += wgt * (fre[F_BTOR][i] * fre[F_BTOR][i] + fim[F_BTOR][i] * fim[F_BTOR][i] +
+                     fre[F_BPOL][i] * fre[F_BPOL][i] + fim[F_BPOL][i] * fim[F_BPOL][i]);
+      }
+    *ekin = 0.5 * ek;
+    *emag = 0.5 * em;
+  }
+
+  std::vector<double>* grid_by_id(int id) {
+    std::vector<double>* g[] = {&u_th, &u_ph, &w_th, &w_ph, &b_th, &b_ph, &j_th, &j_ph, &t_grid,
+                                &gth_grid, &gph_grid, &gr_grid, &tadv, &vadv_th, &vadv_ph, &ind_th, &ind_ph};
+    if (id < 0 || id >= (int)(sizeof(g) / sizeof(g[0]))) return nullptr;
+    return g[id];
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+void* oc_create(const oc_config* cfg) {
+  Oracle* o = new Oracle();
+#ifdef _OPENMP
+  o->nthreads = omp_get_max_threads();
+#endif
+  if (o->setup(cfg) != 0) { delete o; return nullptr; }
+  return o;
+}
+void oc_destroy(void* h) { delete static_cast<Oracle*>(h); }
+void oc_set_threads(void* h, int n) { static_cast<Oracle*>(h)->nthreads = n < 1 ? 1 : n; }
+int oc_nlm(void* h) { return static_cast<Oracle*>(h)->nlm; }
+
+void oc_grid(void* h, double* x, double* w, double* theta, double* r) {
+  Oracle* o = static_cast<Oracle*>(h);
+  for (int i = 0; i < o->c.nlat; ++i) { x[i] = o->x[i]; w[i] = o->w[i]; theta[i] = o->th[i]; }
+  for (int k = 0; k < o->c.nr; ++k) r[k] = o->r[k];
+}
+// Tables in [l-major lm][north theta] order.
+void oc_tables(void* h, double* P, double* dP) {
+  Oracle* o = static_cast<Oracle*>(h);
+  for (int q = 0; q < o->nlm; ++q) {
+    const int l = o->lv[q], m = o->mv[q];
+    for (int i = 0; i < o->nth; ++i) {
+      P[(size_t)q * o->nth + i] = o->P[(size_t)(o->moff[m] + l - m) * o->nth + i];
+      dP[(size_t)q * o->nth + i] = o->dP[(size_t)(o->moff[m] + l - m) * o->nth + i];
+    }
+  }
+}
+// Banded operators in Julia layout ((2kl+1) x nr, column-major).
+void oc_fd_matrix(void* h, int which, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const std::vector<double>& src = which == 1 ? o->d1 : which == 2 ? o->d2 : o->lap;
+  std::memcpy(out, src.data(), src.size() * sizeof(double));
+}
+void oc_lu(void* h, int kind, int l, double* lin_out, double* lu_out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t bsz = (size_t)o->nbw * o->c.nr;
+  std::memcpy(lin_out, &o->lin[kind][bsz * l], bsz * sizeof(double));
+  std::memcpy(lu_out, &o->lu[kind][bsz * l], bsz * sizeof(double));
+}
+void oc_band_solve(void* h, int kind, int l, double* x) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t bsz = (size_t)o->nbw * o->c.nr;
+  o->solve(&o->lu[kind][bsz * l], x);
+}
+
+void oc_synth_scalar(void* h, const double* re, const double* im, double* grid) {
+  static_cast<Oracle*>(h)->synth_scalar(re, im, grid);
+}
+void oc_analysis_scalar(void* h, const double* grid, double* re, double* im) {
+  static_cast<Oracle*>(h)->analysis_scalar(grid, re, im);
+}
+void oc_synth_vector(void* h, const double* tre, const double* tim, const double* pre_, const double* pim_,
+                     double* vth, double* vph) {
+  static_cast<Oracle*>(h)->synth_vector(tre, tim, pre_, pim_, vth, vph);
+}
+void oc_analysis_vector(void* h, const double* vth, const double* vph, double* tre, double* tim,
+                        double* pre_, double* pim_) {
+  static_cast<Oracle*>(h)->analysis_vector(vth, vph, tre, tim, pre_, pim_);
+}
+void oc_gradients(void* h, const double* re, const double* im, double* out /* 6 planes */) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t s = o->spec_size();
+  o->gradients(re, im, out, out + s, out + 2 * s, out + 3 * s, out + 4 * s, out + 5 * s);
+}
+void oc_curl(void* h, const double* tre, const double* tim, const double* pre_, const double* pim_,
+             double* out /* 4 planes: tor re, tor im, pol re, pol im */) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const size_t s = o->spec_size();
+  o->curl_spectral(tre, tim, pre_, pim_, out, out + s, out + 2 * s, out + 3 * s);
+}
+
+void oc_set_field(void* h, int f, const double* re, const double* im) {
+  Oracle* o = static_cast<Oracle*>(h);
+  std::memcpy(o->fre[f].data(), re, o->spec_size() * sizeof(double));
+  std::memcpy(o->fim[f].data(), im, o->spec_size() * sizeof(double));
+}
+void oc_get_field(void* h, int f, double* re, double* im) {
+  Oracle* o = static_cast<Oracle*>(h);
+  std::memcpy(re, o->fre[f].data(), o->spec_size() * sizeof(double));
+  std::memcpy(im, o->fim[f].data(), o->spec_size() * sizeof(double));
+}
+void oc_get_nl(void* h, int f, double* re, double* im) {
+  Oracle* o = static_cast<Oracle*>(h);
+  std::memcpy(re, o->nre[f].data(), o->spec_size() * sizeof(double));
+  std::memcpy(im, o->nim[f].data(), o->spec_size() * sizeof(double));
+}
+int oc_get_grid_field(void* h, int id, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  std::vector<double>* g = o->grid_by_id(id);
+  if (!g) return 1;
+  std::memcpy(out, g->data(), g->size() * sizeof(double));
+  return 0;
+}
+void oc_set_temperature_bc(void* h, const double* bvals /* [2][nlm] */, const double* sources /* [nr] */) {
+  Oracle* o = static_cast<Oracle*>(h);
+  if (bvals) std::memcpy(o->bvals.data(), bvals, 2 * (size_t)o->nlm * sizeof(double));
+  if (sources) std::memcpy(o->sources.data(), sources, (size_t)o->c.nr * sizeof(double));
+}
+void oc_temperature_nl(void* h) { static_cast<Oracle*>(h)->temperature_nl(); }
+void oc_velocity_nl(void* h) { static_cast<Oracle*>(h)->velocity_nl(); }
+void oc_magnetic_nl(void* h) { static_cast<Oracle*>(h)->magnetic_nl(); }
+void oc_implicit_step(void* h) { static_cast<Oracle*>(h)->implicit_step(); }
+void oc_step(void* h, int n) {
+  Oracle* o = static_cast<Oracle*>(h);
+  for (int i = 0; i < n; ++i) o->step();
+}
+void oc_energy(void* h, double* ekin, double* emag) { static_cast<Oracle*>(h)->energies(ekin, emag); }
+long oc_step_count(void* h) { return static_cast<Oracle*>(h)->step_count; }
+
+}  // extern "C"

@@ -1,0 +1,246 @@
+"""ctypes front end of the CPU FP64 oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline and
+reference legs import this module.  It loads ``oracle/_build/libgdoracle.so``
+(built by ``oracle/Makefile``), a C++ restatement of GeoDynamo.jl's per-step
+hot path; see the header of ``gd_oracle.cpp`` for the conventions and the
+reference lines each routine follows.
+
+Arrays use the reference's layouts: spectral planes are ``(nr, nlm)`` with the
+l-major (l, m) index fastest (``src/fields.jl:6-15``); physical grids are
+``(nr, nlon, nlat)`` with theta fastest (``src/fields.jl:18-24``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libgdoracle.so")
+
+FIELD_IDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4}
+GRID_IDS = {
+    "u_th": 0, "u_ph": 1, "w_th": 2, "w_ph": 3, "b_th": 4, "b_ph": 5, "j_th": 6, "j_ph": 7,
+    "t": 8, "gth": 9, "gph": 10, "gr": 11, "tadv": 12, "vadv_th": 13, "vadv_ph": 14,
+    "ind_th": 15, "ind_ph": 16,
+}
+
+
+class OcConfig(ctypes.Structure):
+    _fields_ = [
+        ("lmax", ctypes.c_int), ("mmax", ctypes.c_int), ("nlat", ctypes.c_int),
+        ("nlon", ctypes.c_int), ("nr", ctypes.c_int), ("kl", ctypes.c_int),
+        ("rratio", ctypes.c_double), ("ekman", ctypes.c_double), ("rayleigh", ctypes.c_double),
+        ("prandtl", ctypes.c_double), ("magnetic_prandtl", ctypes.c_double),
+        ("dt", ctypes.c_double), ("implicit_theta", ctypes.c_double),
+        ("ab_mode", ctypes.c_int), ("bc_mode", ctypes.c_int), ("fd_mode", ctypes.c_int),
+        ("precision", ctypes.c_int), ("magnetic", ctypes.c_int),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        lib = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        D = ctypes.POINTER(ctypes.c_double)
+        lib.oc_create.restype = P
+        lib.oc_create.argtypes = [ctypes.POINTER(OcConfig)]
+        lib.oc_destroy.argtypes = [P]
+        lib.oc_set_threads.argtypes = [P, ctypes.c_int]
+        lib.oc_nlm.argtypes = [P]
+        lib.oc_nlm.restype = ctypes.c_int
+        lib.oc_grid.argtypes = [P, D, D, D, D]
+        lib.oc_tables.argtypes = [P, D, D]
+        lib.oc_fd_matrix.argtypes = [P, ctypes.c_int, D]
+        lib.oc_lu.argtypes = [P, ctypes.c_int, ctypes.c_int, D, D]
+        lib.oc_band_solve.argtypes = [P, ctypes.c_int, ctypes.c_int, D]
+        lib.oc_synth_scalar.argtypes = [P, D, D, D]
+        lib.oc_analysis_scalar.argtypes = [P, D, D, D]
+        lib.oc_synth_vector.argtypes = [P, D, D, D, D, D, D]
+        lib.oc_analysis_vector.argtypes = [P, D, D, D, D, D, D]
+        lib.oc_gradients.argtypes = [P, D, D, D]
+        lib.oc_curl.argtypes = [P, D, D, D, D, D]
+        lib.oc_set_field.argtypes = [P, ctypes.c_int, D, D]
+        lib.oc_get_field.argtypes = [P, ctypes.c_int, D, D]
+        lib.oc_get_nl.argtypes = [P, ctypes.c_int, D, D]
+        lib.oc_get_grid_field.argtypes = [P, ctypes.c_int, D]
+        lib.oc_get_grid_field.restype = ctypes.c_int
+        lib.oc_set_temperature_bc.argtypes = [P, D, D]
+        for name in ("oc_temperature_nl", "oc_velocity_nl", "oc_magnetic_nl", "oc_implicit_step"):
+            getattr(lib, name).argtypes = [P]
+        lib.oc_step.argtypes = [P, ctypes.c_int]
+        lib.oc_energy.argtypes = [P, D, D]
+        lib.oc_step_count.argtypes = [P]
+        lib.oc_step_count.restype = ctypes.c_long
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def lm_pairs(lmax: int, mmax: int):
+    """(l, m) per l-major index (``shtnskit_transforms.jl:177-188``)."""
+    return [(l, m) for l in range(lmax + 1) for m in range(min(l, mmax) + 1)]
+
+
+class Oracle:
+    """One oracle instance: grid, tables, radial operators and a model state."""
+
+    def __init__(self, lmax, nlat, nlon, nr, mmax=None, kl=4, rratio=0.35, ekman=3e-4,
+                 rayleigh=80.0, prandtl=1.0, magnetic_prandtl=4.0, dt=1e-5, implicit_theta=0.5,
+                 ab_mode=0, bc_mode=0, fd_mode=0, magnetic=1, threads=None):
+        self.lib = _load()
+        mmax = lmax if mmax is None else mmax
+        self.cfg = OcConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl,
+                            magnetic_prandtl, dt, implicit_theta, ab_mode, bc_mode, fd_mode, 0,
+                            magnetic)
+        self.h = self.lib.oc_create(ctypes.byref(self.cfg))
+        if not self.h:
+            raise ValueError("oracle rejected the configuration")
+        if threads is not None:
+            self.lib.oc_set_threads(self.h, int(threads))
+        self.lmax, self.mmax, self.nlat, self.nlon, self.nr = lmax, mmax, nlat, nlon, nr
+        self.nlm = self.lib.oc_nlm(self.h)
+        self.kl = kl
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.oc_destroy(h)
+            self.h = None
+
+    # -- geometry -----------------------------------------------------------------
+    def grid(self):
+        x = np.zeros(self.nlat); w = np.zeros(self.nlat); th = np.zeros(self.nlat)
+        r = np.zeros(self.nr)
+        self.lib.oc_grid(self.h, _ptr(x), _ptr(w), _ptr(th), _ptr(r))
+        return x, w, th, r
+
+    def tables(self):
+        nth = self.nlat // 2
+        P = np.zeros((self.nlm, nth)); dP = np.zeros((self.nlm, nth))
+        self.lib.oc_tables(self.h, _ptr(P), _ptr(dP))
+        return P, dP
+
+    def fd_matrix(self, which):
+        out = np.zeros((self.nr, 2 * self.kl + 1))  # column-major (2kl+1) x nr
+        self.lib.oc_fd_matrix(self.h, which, _ptr(out))
+        return out.T.copy()  # rows = band row, cols = column j
+
+    def implicit_matrices(self, kind, l):
+        lin = np.zeros((self.nr, 2 * self.kl + 1)); lu = np.zeros((self.nr, 2 * self.kl + 1))
+        self.lib.oc_lu(self.h, kind, l, _ptr(lin), _ptr(lu))
+        return lin.T.copy(), lu.T.copy()
+
+    def band_solve(self, kind, l, b):
+        x = _c(b).copy()
+        self.lib.oc_band_solve(self.h, kind, l, _ptr(x))
+        return x
+
+    # -- transforms ---------------------------------------------------------------
+    def spec_shape(self):
+        return (self.nr, self.nlm)
+
+    def grid_shape(self):
+        return (self.nr, self.nlon, self.nlat)
+
+    def synth_scalar(self, re, im):
+        g = np.zeros(self.grid_shape())
+        self.lib.oc_synth_scalar(self.h, _ptr(_c(re)), _ptr(_c(im)), _ptr(g))
+        return g
+
+    def analysis_scalar(self, grid):
+        re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
+        self.lib.oc_analysis_scalar(self.h, _ptr(_c(grid)), _ptr(re), _ptr(im))
+        return re, im
+
+    def synth_vector(self, tre, tim, pre, pim):
+        vt = np.zeros(self.grid_shape()); vp = np.zeros(self.grid_shape())
+        self.lib.oc_synth_vector(self.h, _ptr(_c(tre)), _ptr(_c(tim)), _ptr(_c(pre)), _ptr(_c(pim)),
+                                 _ptr(vt), _ptr(vp))
+        return vt, vp
+
+    def analysis_vector(self, vt, vp):
+        out = [np.zeros(self.spec_shape()) for _ in range(4)]
+        self.lib.oc_analysis_vector(self.h, _ptr(_c(vt)), _ptr(_c(vp)), *[_ptr(o) for o in out])
+        return out  # tor re, tor im, pol re, pol im
+
+    def gradients(self, re, im):
+        out = np.zeros((6,) + self.spec_shape())
+        self.lib.oc_gradients(self.h, _ptr(_c(re)), _ptr(_c(im)), _ptr(out))
+        return out
+
+    def curl(self, tre, tim, pre, pim):
+        out = np.zeros((4,) + self.spec_shape())
+        self.lib.oc_curl(self.h, _ptr(_c(tre)), _ptr(_c(tim)), _ptr(_c(pre)), _ptr(_c(pim)), _ptr(out))
+        return out
+
+    # -- state --------------------------------------------------------------------
+    def set_field(self, name, re, im):
+        self.lib.oc_set_field(self.h, FIELD_IDS[name], _ptr(_c(re)), _ptr(_c(im)))
+
+    def get_field(self, name):
+        re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
+        self.lib.oc_get_field(self.h, FIELD_IDS[name], _ptr(re), _ptr(im))
+        return re, im
+
+    def get_nl(self, name):
+        re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
+        self.lib.oc_get_nl(self.h, FIELD_IDS[name], _ptr(re), _ptr(im))
+        return re, im
+
+    def get_grid(self, name):
+        g = np.zeros(self.grid_shape())
+        if self.lib.oc_get_grid_field(self.h, GRID_IDS[name], _ptr(g)) != 0:
+            raise KeyError(name)
+        return g
+
+    def set_temperature_bc(self, bvals=None, sources=None):
+        self.lib.oc_set_temperature_bc(
+            self.h, _ptr(_c(bvals)) if bvals is not None else None,
+            _ptr(_c(sources)) if sources is not None else None)
+
+    def temperature_nl(self):
+        self.lib.oc_temperature_nl(self.h)
+
+    def velocity_nl(self):
+        self.lib.oc_velocity_nl(self.h)
+
+    def magnetic_nl(self):
+        self.lib.oc_magnetic_nl(self.h)
+
+    def implicit_step(self):
+        self.lib.oc_implicit_step(self.h)
+
+    def step(self, n=1):
+        self.lib.oc_step(self.h, int(n))
+
+    def energy(self):
+        ek = ctypes.c_double(); em = ctypes.c_double()
+        self.lib.oc_energy(self.h, ctypes.byref(ek), ctypes.byref(em))
+        return ek.value, em.value
+
+    def step_count(self):
+        return self.lib.oc_step_count(self.h)

@@ -1,0 +1,207 @@
+"""GPU parity: libgdb200.so (through its C ABI) against the FP64 oracle and the
+golden fixtures.  Tolerances: relative max-norm error (max |a - b| / max |b|)
+of 1e-12 for every transform, nonlinear term and single step of the all-FP64
+path, as the requirement for the FP64 GPU step states; multi-step trajectories
+are held to 1e-11 because the radial operators' conditioning (~1e7 at nr = 129)
+amplifies last-bit differences step over step."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, os.path.join(ROOT, "geodynamo.jl_b200"))
+import workloads  # noqa: E402
+
+TOL = 1e-12
+NAMES = ("u_tor", "u_pol", "b_tor", "b_pol", "temp")
+
+
+def rel(a, b):
+    a = np.asarray(a); b = np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def make_pair(gdb, oracle_mod, lmax, nlat, nlon, nr, mmax=None, **kw):
+    g = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, mmax=mmax, **kw)
+    o = oracle_mod.Oracle(lmax=lmax, nlat=nlat, nlon=nlon, nr=nr, mmax=mmax, **kw)
+    return g, o
+
+
+SHAPES = [
+    (6, 12, 24, 6, None),      # the reference's round-trip test size
+    (31, 48, 96, 32, None),    # shell_l31_nr32
+    (20, 34, 40, 7, 10),       # mmax < lmax, nlon with a factor 5, odd tiles
+    (47, 72, 144, 5, None),    # 9 | nlon
+]
+
+
+@pytest.mark.parametrize("lmax,nlat,nlon,nr,mmax", SHAPES)
+def test_scalar_transforms_match_oracle(gdb, oracle_mod, lmax, nlat, nlon, nr, mmax):
+    g, o = make_pair(gdb, oracle_mod, lmax, nlat, nlon, nr, mmax)
+    re, im = workloads.transform_batch(lmax, g.mmax, nr, 3, seed=lmax)
+    grid = g.synth_scalar(re, im)
+    for f in range(3):
+        assert rel(grid[f], o.synth_scalar(re[f], im[f])) < TOL
+    re2, im2 = g.analysis_scalar(grid)
+    for f in range(3):
+        ore, oim = o.analysis_scalar(grid[f])
+        assert rel(re2[f], ore) < TOL
+        assert rel(im2[f], oim) < TOL
+        assert rel(re2[f], re[f]) < 1e-11   # round trip
+
+
+@pytest.mark.parametrize("lmax,nlat,nlon,nr,mmax", SHAPES)
+def test_vector_transforms_match_oracle(gdb, oracle_mod, lmax, nlat, nlon, nr, mmax):
+    g, o = make_pair(gdb, oracle_mod, lmax, nlat, nlon, nr, mmax)
+    re, im = workloads.transform_batch(lmax, g.mmax, nr, 2, seed=7 + lmax)
+    L, M = workloads.lm_arrays(lmax, g.mmax)
+    re[:, :, L == 0] = 0; im[:, :, L == 0] = 0
+    vt, vp = g.synth_vector(re[0], im[0], re[1], im[1])
+    ovt, ovp = o.synth_vector(re[0], im[0], re[1], im[1])
+    assert rel(vt, ovt) < TOL and rel(vp, ovp) < TOL
+    out = g.analysis_vector(vt, vp)
+    oout = o.analysis_vector(vt, vp)
+    for a, b in zip(out, oout):
+        assert rel(a, b) < TOL
+    assert rel(out[0], re[0]) < 1e-11 and rel(out[2], re[1]) < 1e-11
+
+
+def test_golden_transforms(gdb):
+    d = dict(np.load(os.path.join(GOLD, "sht_l6.npz")))
+    g = gdb.SHTnsKitConfig(6, 12, 24, 6)
+    assert rel(g.theta_grid, np.arccos(d["x"])) < 1e-14
+    assert rel(g.gauss_weights, d["w"]) < 1e-13
+    assert rel(g.synth_scalar(d["re"], d["im"]), d["grid"]) < 1e-13
+    vt, vp = g.synth_vector(d["tre"], d["tim"], d["pre"], d["pim"])
+    assert rel(vt, d["vt"]) < 1e-12 and rel(vp, d["vp"]) < 1e-12
+    # the reference's own criterion (test/shtnskit_roundtrip.jl:54)
+    re2, im2 = g.analysis_scalar(d["grid"])
+    err = np.sum((re2 - d["re"]) ** 2) + np.sum((im2 - d["im"]) ** 2)
+    assert err / (np.sum(d["re"] ** 2) + np.sum(d["im"] ** 2)) < 1e-7
+
+
+def test_reference_api_mirror(gdb):
+    d = dict(np.load(os.path.join(GOLD, "sht_l6.npz")))
+    cfg = gdb.create_shtnskit_config(lmax=6, nlat=12, nlon=24, nr=6)
+    spec = gdb.create_shtns_spectral_field(cfg)
+    spec.data_real[...] = d["re"]; spec.data_imag[...] = d["im"]
+    phys = gdb.create_shtns_physical_field(cfg)
+    gdb.shtnskit_spectral_to_physical(spec, phys)
+    spec2 = gdb.create_shtns_spectral_field(cfg)
+    gdb.shtnskit_physical_to_spectral(phys, spec2)
+    assert rel(spec2.data_real, d["re"]) < 1e-12
+    physs = [gdb.create_shtns_physical_field(cfg) for _ in range(5)]
+    gdb.batch_spectral_to_physical([spec] * 5, physs)
+    for p in physs:
+        assert rel(p.data, phys.data) < 1e-15
+
+
+def load_state(g, o, st):
+    for k, (a, b) in st.items():
+        g.set_field(k, a, b)
+        o.set_field(k, a, b)
+
+
+def test_nonlinear_terms_match_oracle(gdb, oracle_mod):
+    g, o = make_pair(gdb, oracle_mod, 31, 48, 96, 32)
+    st = workloads.seeded_state(31, 31, 32, seed=0)
+    load_state(g, o, st)
+    bv = np.random.default_rng(5).standard_normal((2, g.nlm)) * 1e-3
+    src = np.linspace(0.0, 1e-3, 32)
+    g.set_temperature_bc(bv, src); o.set_temperature_bc(bv, src)
+    # a first full step populates the grids carried between sub-steps
+    g.step(1); o.step(1)
+    g.temperature_nl(); o.temperature_nl()
+    for grid in ("t", "gth", "gph", "gr", "tadv"):
+        assert rel(g.get_grid(grid), o.get_grid(grid)) < TOL, grid
+    assert rel(g.get_nl("temp")[0], o.get_nl("temp")[0]) < TOL
+    assert rel(g.get_field("temp")[0], o.get_field("temp")[0]) < TOL   # Dirichlet rows
+    g.velocity_nl(); o.velocity_nl()
+    for grid in ("u_th", "u_ph", "w_th", "w_ph", "vadv_th", "vadv_ph"):
+        assert rel(g.get_grid(grid), o.get_grid(grid)) < TOL, grid
+    for k in ("u_tor", "u_pol"):
+        a, b = g.get_nl(k), o.get_nl(k)
+        assert rel(a[0], b[0]) < TOL and rel(a[1], b[1]) < TOL, k
+    g.magnetic_nl(); o.magnetic_nl()
+    for grid in ("b_th", "b_ph", "j_th", "j_ph"):
+        assert rel(g.get_grid(grid), o.get_grid(grid)) < TOL, grid
+    for k in ("b_tor", "b_pol"):
+        a, b = g.get_nl(k), o.get_nl(k)
+        assert np.max(np.abs(a[0] - b[0])) <= 1e-30 + TOL * max(np.max(np.abs(b[0])), 1.0)
+
+
+def test_single_step_matches_oracle(gdb, oracle_mod):
+    g, o = make_pair(gdb, oracle_mod, 31, 48, 96, 32)
+    load_state(g, o, workloads.seeded_state(31, 31, 32, seed=0))
+    g.step(1); o.step(1)
+    for k in NAMES:
+        a, b = g.get_field(k), o.get_field(k)
+        assert rel(a[0], b[0]) < TOL and rel(a[1], b[1]) < TOL, k
+
+
+def test_trajectory_shell_l31_nr32(gdb, oracle_mod):
+    # 100 CNAB2 steps at dt = 1e-5 (the oracle configuration)
+    g, o = make_pair(gdb, oracle_mod, 31, 48, 96, 32, dt=1e-5)
+    load_state(g, o, workloads.seeded_state(31, 31, 32, seed=0))
+    for _ in range(4):
+        g.step(25); o.step(25)
+        for k in NAMES:
+            a, b = g.get_field(k), o.get_field(k)
+            assert rel(a[0], b[0]) < 1e-11 and rel(a[1], b[1]) < 1e-11, k
+    ek, em = g.energy(); oek, oem = o.energy()
+    assert abs(ek - oek) / oek < 1e-11 and abs(em - oem) / oem < 1e-11
+
+
+def test_golden_trajectory(gdb):
+    d = dict(np.load(os.path.join(GOLD, "step_l7.npz")))
+    lm, nlat, nlon, nr = [int(v) for v in d["dims"]]
+    g = gdb.SHTnsKitConfig(lm, nlat, nlon, nr, dt=1e-5)
+    for k in NAMES:
+        g.set_field(k, d[f"u0_{k}_re"], d[f"u0_{k}_im"])
+    g.step(1)
+    for k in NAMES:
+        assert rel(g.get_nl(k)[0], d[f"nl_{k}_re"]) < TOL or np.max(np.abs(d[f"nl_{k}_re"])) == 0.0, k
+    g.step(2)
+    for k in NAMES:
+        assert rel(g.get_field(k)[0], d[f"u3_{k}_re"]) < 1e-11, k
+    assert rel(np.array(g.energy()), d["energy3"]) < 1e-11
+
+
+def test_graph_replay_equals_eager_substeps(gdb):
+    st = workloads.seeded_state(15, 15, 12, seed=3)
+    a = gdb.SHTnsKitConfig(15, 24, 48, 12)
+    b = gdb.SHTnsKitConfig(15, 24, 48, 12)
+    for k, (x, y) in st.items():
+        a.set_field(k, x, y); b.set_field(k, x, y)
+    a.step(3)
+    for _ in range(3):
+        b.temperature_nl(); b.velocity_nl(); b.magnetic_nl(); b.implicit_step()
+    for k in NAMES:
+        assert np.array_equal(a.get_field(k)[0], b.get_field(k)[0]), k
+
+
+def test_ab_mode_literal_bootstrap_every_step(gdb, oracle_mod):
+    g, o = make_pair(gdb, oracle_mod, 15, 24, 48, 12, ab_mode=1)
+    load_state(g, o, workloads.seeded_state(15, 15, 12, seed=1))
+    g.step(3); o.step(3)
+    for k in NAMES:
+        assert rel(g.get_field(k)[0], o.get_field(k)[0]) < 1e-11, k
+
+
+def test_errors_are_status_codes(gdb):
+    g = gdb.SHTnsKitConfig(7, 12, 24, 9)
+    with pytest.raises(gdb.GeoDynamoError) as e:
+        g.lib.gd_upload_spectral(g.h, 9, None, None) and g._check(1)
+    bad = np.zeros(g.spec_shape())
+    bad[3, 5] = np.nan
+    g.set_field("u_pol", bad, np.zeros(g.spec_shape()))
+    with pytest.raises(gdb.GeoDynamoError) as e:
+        g.check_finite()
+    assert e.value.status == 4
+    with pytest.raises(gdb.GeoDynamoError):
+        g.set_dt(-1.0)
