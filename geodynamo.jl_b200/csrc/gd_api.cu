@@ -55,7 +55,7 @@ int build_implicit(gd_handle* h) {
   const Dims& d = h->d;
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
   launch_build_lu(h->stream, d.nr, d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->c.dt,
-                  h->c.implicit_theta, h->d_lin, h->d_lu, h->d_flag);
+                  h->c.implicit_theta, h->c.bc_mode == 2, h->d_lin, h->d_lu, h->d_flag);
   int s = check_launch(h, "build_lu");
   if (s) return s;
   int flag = 0;
@@ -216,10 +216,10 @@ int temperature_nl_fp64(gd_handle* h) {
   const double* coef[4] = {h->field(F_TEMP), h->work(0), h->work(1), h->work(2)};
   int s = synth_scalar(h, coef, 4, h->grid(GD_GRID_T));
   if (s) return s;
-  ProfScope pa(h, "nl_temperature_fp64");
-  launch_temperature_advection<double>(h->stream, d, h->grid(GD_GRID_U_TH), h->grid(GD_GRID_U_PH),
-                                       h->grid(GD_GRID_GTH), h->grid(GD_GRID_GPH), h->grid(GD_GRID_GR),
-                                       h->d_sources, h->grid(GD_GRID_TADV));
+  { ProfScope pa(h, "nl_temperature_fp64");
+    launch_temperature_advection<double>(h->stream, d, h->grid(GD_GRID_U_TH), h->grid(GD_GRID_U_PH),
+                                         h->grid(GD_GRID_GTH), h->grid(GD_GRID_GPH), h->grid(GD_GRID_GR),
+                                         h->d_sources, h->grid(GD_GRID_TADV)); }
   double* out[1] = {h->nlf(F_TEMP)};
   s = analysis_scalar(h, h->grid(GD_GRID_TADV), 1, out);
   if (s) return s;
@@ -273,6 +273,9 @@ int implicit_launch(gd_handle* h, int boot) {
   }
   a.boot = boot;
   a.clamp_rows = h->c.bc_mode == 1;
+  a.bc_rows = h->c.bc_mode == 2;
+  a.bvals = h->d_bvals;
+  a.temp_slot = 0;
   a.inv_dt = 1.0 / h->c.dt;
   a.lin_weight = 1.0 - h->c.implicit_theta;
   { ProfScope p(h, "cnab2_solve"); launch_cnab2(h->stream, h->d, h->d_lof, h->d_lin, h->d_lu, a); }
@@ -339,6 +342,9 @@ bool valid_config(const gd_config* c, std::string& why) {
   if (!(c->dt > 0.0)) { why = "dt must be positive"; return false; }
   if (c->ekman == 0.0) { why = "Ekman number must be nonzero (src/velocity.jl:450-452)"; return false; }
   if (c->rratio <= 0.0 || c->rratio >= 1.0) { why = "rratio must lie in (0, 1)"; return false; }
+  if (c->bc_mode < 0 || c->bc_mode > 2) { why = "bc_mode must be 0, 1 or 2"; return false; }
+  if (c->ab_mode < 0 || c->ab_mode > 1) { why = "ab_mode must be 0 or 1"; return false; }
+  if (c->fd_mode < 0 || c->fd_mode > 1) { why = "fd_mode must be 0 or 1"; return false; }
   if (c->precision != GD_PREC_FP64 && c->precision != GD_PREC_MIXED) { why = "unknown precision"; return false; }
   return true;
 }
@@ -418,6 +424,7 @@ int gd_synchronize(gd_handle* h) {
   if (!h) return GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
+  if (h->precision == GD_PREC_MIXED) return mixed_check_error(h);
   return GD_OK;
 }
 
@@ -598,7 +605,7 @@ int gd_temperature_nonlinear(gd_handle* h) {
   int s = temperature_nl(h);
   if (s) return s;
   CK(cudaStreamSynchronize(h->stream));
-  return GD_OK;
+  return h->precision == GD_PREC_MIXED ? mixed_check_error(h) : GD_OK;
 }
 int gd_velocity_nonlinear(gd_handle* h) {
   if (!h) return GD_ERR_ARG;
@@ -606,7 +613,7 @@ int gd_velocity_nonlinear(gd_handle* h) {
   int s = velocity_nl(h);
   if (s) return s;
   CK(cudaStreamSynchronize(h->stream));
-  return GD_OK;
+  return h->precision == GD_PREC_MIXED ? mixed_check_error(h) : GD_OK;
 }
 int gd_magnetic_nonlinear(gd_handle* h) {
   if (!h) return GD_ERR_ARG;
@@ -614,7 +621,7 @@ int gd_magnetic_nonlinear(gd_handle* h) {
   int s = magnetic_nl(h);
   if (s) return s;
   CK(cudaStreamSynchronize(h->stream));
-  return GD_OK;
+  return h->precision == GD_PREC_MIXED ? mixed_check_error(h) : GD_OK;
 }
 int gd_implicit_step(gd_handle* h) {
   if (!h) return GD_ERR_ARG;
@@ -649,6 +656,7 @@ int gd_step(gd_handle* h, int nsteps) {
   int s = gd_step_async(h, nsteps);
   if (s) return s;
   CK(cudaStreamSynchronize(h->stream));
+  if (h->precision == GD_PREC_MIXED) return mixed_check_error(h);
   return GD_OK;
 }
 

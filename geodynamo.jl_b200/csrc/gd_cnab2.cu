@@ -66,6 +66,10 @@ __global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ l
     double vi = a.inv_dt * wi[KL] + 1.5 * n_i - 0.5 * p_i;
     vr += a.lin_weight * Lr;
     vi += a.lin_weight * Li;
+    if (a.bc_rows && (i == 0 || i == N - 1)) {
+      vr = (fs == a.temp_slot) ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
+      vi = 0.0;
+    }
     // history roll: prev := nl
     pre[at] = n_r;
     pim[at] = n_i;

@@ -4,8 +4,8 @@
 // Each CTA transforms `tb` north/south row pairs of one (component, shell):
 // the two real rows are packed into one complex sequence (north = real part,
 // south = imaginary part) and transformed with a shared-memory Stockham
-// mixed-radix FFT (radices 4, 2, 3, 5).  Every stage reads its butterflies
-// into registers, synchronises, and writes them back in place.
+// mixed-radix FFT that ping-pongs between two buffers (radix 16 passes for
+// the power-of-two part, then 8/4/2, 3 and 5; nlon = 768 takes 16 x 16 x 3).
 //
 // Synthesis consumes the Legendre output F[comp][r][m][s][ith] and writes
 // grid rows [comp][r][theta][phi].  Analysis writes the Gauss-weighted folds
@@ -30,34 +30,43 @@ template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
 
 static const int kThreads = 256;
-// Complex elements each thread keeps in registers during a stage.
-template <typename R> struct Emax;
-template <> struct Emax<double> { static const int v = 24; };
-template <> struct Emax<float> { static const int v = 48; };
 
-template <int R, typename C>
-__device__ __forceinline__ void dft(C* v) {
-  typedef decltype(v[0].x) S;
-  if (R == 2) {
+// Forward DFT of R points in registers, natural order in and out.
+template <typename C> __device__ __forceinline__ C mul_mi(C a) { C r; r.x = a.y; r.y = -a.x; return r; }  // -i a
+
+template <int R, typename C> struct Dft;
+
+template <typename C> struct Dft<2, C> {
+  static __device__ __forceinline__ void run(C* v) {
     const C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
-  } else if (R == 4) {
+  }
+};
+template <typename C> struct Dft<4, C> {
+  static __device__ __forceinline__ void run(C* v) {
     const C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]), t2 = cadd(v[1], v[3]);
-    const C d = csub(v[1], v[3]);
-    C t3; t3.x = d.y; t3.y = -d.x;  // -i * d
+    const C t3 = mul_mi(csub(v[1], v[3]));
     v[0] = cadd(t0, t2);
     v[2] = csub(t0, t2);
     v[1] = cadd(t1, t3);
     v[3] = csub(t1, t3);
-  } else if (R == 3) {
+  }
+};
+template <typename C> struct Dft<3, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    typedef decltype(v[0].x) S;
     const S h = (S)0.86602540378443864676;
     const C a0 = v[0], s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
     C m; m.x = a0.x - (S)0.5 * s.x; m.y = a0.y - (S)0.5 * s.y;
     v[0] = cadd(a0, s);
     v[1].x = m.x + h * d.y; v[1].y = m.y - h * d.x;
     v[2].x = m.x - h * d.y; v[2].y = m.y + h * d.x;
-  } else if (R == 5) {
+  }
+};
+template <typename C> struct Dft<5, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    typedef decltype(v[0].x) S;
     const S c1 = (S)0.30901699437494742410, c2 = (S)-0.80901699437494742410;
     const S s1 = (S)0.95105651629515357212, s2 = (S)0.58778525229247312917;
     const C a0 = v[0];
@@ -67,107 +76,160 @@ __device__ __forceinline__ void dft(C* v) {
     C r1, r2, i1, i2;
     r1.x = a0.x + c1 * p1.x + c2 * p2.x; r1.y = a0.y + c1 * p1.y + c2 * p2.y;
     r2.x = a0.x + c2 * p1.x + c1 * p2.x; r2.y = a0.y + c2 * p1.y + c1 * p2.y;
-    // forward: -i (s1 m1 + s2 m2), -i (s2 m1 - s1 m2)
     i1.x = s1 * m1.y + s2 * m2.y; i1.y = -(s1 * m1.x + s2 * m2.x);
     i2.x = s2 * m1.y - s1 * m2.y; i2.y = -(s2 * m1.x - s1 * m2.x);
     v[1] = cadd(r1, i1); v[4] = csub(r1, i1);
     v[2] = cadd(r2, i2); v[3] = csub(r2, i2);
   }
-}
+};
+// Radix 8 and 16 by one decimation-in-frequency split into two half-size DFTs:
+//   u_n = x_n + x_{n+R/2},  v_n = (x_n - x_{n+R/2}) W_R^n,
+//   X_{2k} = DFT(u)_k,  X_{2k+1} = DFT(v)_k.
+template <typename C> struct Dft<8, C> {
+  static __device__ __forceinline__ void run(C* x) {
+    typedef decltype(x[0].x) S;
+    const S c = (S)0.70710678118654752440;
+    C u[4], w[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { u[n] = cadd(x[n], x[n + 4]); w[n] = csub(x[n], x[n + 4]); }
+    // W8^1 = c (1 - i), W8^2 = -i, W8^3 = -c (1 + i)
+    { C t = w[1]; w[1].x = c * (t.x + t.y); w[1].y = c * (t.y - t.x); }
+    w[2] = mul_mi(w[2]);
+    { C t = w[3]; w[3].x = c * (t.y - t.x); w[3].y = -c * (t.x + t.y); }
+    Dft<4, C>::run(u);
+    Dft<4, C>::run(w);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { x[2 * k] = u[k]; x[2 * k + 1] = w[k]; }
+  }
+};
+template <typename C> struct Dft<16, C> {
+  static __device__ __forceinline__ void run(C* x) {
+    typedef decltype(x[0].x) S;
+    // W16^n = cos(pi n / 8) - i sin(pi n / 8), n = 0..7
+    const S cs[8] = {(S)1.0, (S)0.92387953251128675613, (S)0.70710678118654752440, (S)0.38268343236508977173,
+                     (S)0.0, (S)-0.38268343236508977173, (S)-0.70710678118654752440, (S)-0.92387953251128675613};
+    const S sn[8] = {(S)0.0, (S)0.38268343236508977173, (S)0.70710678118654752440, (S)0.92387953251128675613,
+                     (S)1.0, (S)0.92387953251128675613, (S)0.70710678118654752440, (S)0.38268343236508977173};
+    C u[8], w[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      u[n] = cadd(x[n], x[n + 8]);
+      const C d = csub(x[n], x[n + 8]);
+      w[n].x = d.x * cs[n] + d.y * sn[n];
+      w[n].y = d.y * cs[n] - d.x * sn[n];
+    }
+    Dft<8, C>::run(u);
+    Dft<8, C>::run(w);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { x[2 * k] = u[k]; x[2 * k + 1] = w[k]; }
+  }
+};
 
-// One Stockham stage over all rows of `buf` ([tb][n]).
-template <int R, typename RT>
-__device__ void fft_stage(typename C2<RT>::T* buf, int tb, int n, int Ns, const typename C2<RT>::T* tw) {
-  typedef typename C2<RT>::T C;
-  constexpr int MAXB = (Emax<RT>::v + R - 1) / R;
+// Shared-memory rows are padded by one element every 16 so the stride-16
+// stores of the first radix-16 pass do not all fall into one bank.
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+__host__ __device__ __forceinline__ int prow(int n) { return n + (n >> 4); }
+
+// One Stockham pass from src to dst ([tb][n] each): radix R, Ns = product of
+// the radices of the earlier passes.
+template <int R, typename C>
+__device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restrict__ dst, int tb, int n, int Ns,
+                                         const C* __restrict__ tw) {
   const int nbf = n / R;
   const int total = tb * nbf;
   const int twstep = n / (Ns * R);
-  C v[MAXB][R];
+  for (int b = threadIdx.x; b < total; b += kThreads) {
+    const int row = b / nbf, j = b - row * nbf;
+    const int k = j % Ns;
+    const C* s = src + (size_t)row * prow(n);
+    C v[R];
 #pragma unroll
-  for (int i = 0; i < MAXB; ++i) {
-    const int b = threadIdx.x + i * kThreads;
-    if (b < total) {
-      const int row = b / nbf, j = b - row * nbf;
-      const int k = j % Ns;
-      const C* src = buf + (size_t)row * n + j;
+    for (int r = 0; r < R; ++r) v[r] = s[pidx(j + r * nbf)];
+    if (k > 0) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        C x = src[r * nbf];
-        if (r > 0 && k > 0) x = cmul(x, tw[(r * k * twstep) % n]);
-        v[i][r] = x;
-      }
-      dft<R>(v[i]);
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(&tw[r * k * twstep]));
     }
-  }
-  __syncthreads();
+    Dft<R, C>::run(v);
+    C* o = dst + (size_t)row * prow(n);
+    const int o0 = (j / Ns) * Ns * R + k;
 #pragma unroll
-  for (int i = 0; i < MAXB; ++i) {
-    const int b = threadIdx.x + i * kThreads;
-    if (b < total) {
-      const int row = b / nbf, j = b - row * nbf;
-      const int k = j % Ns;
-      const int idxD = (j / Ns) * Ns * R + k;
-      C* dst = buf + (size_t)row * n + idxD;
-#pragma unroll
-      for (int r = 0; r < R; ++r) dst[r * Ns] = v[i][r];
-    }
+    for (int r = 0; r < R; ++r) o[pidx(o0 + r * Ns)] = v[r];
   }
-  __syncthreads();
 }
 
+// Runs all passes; returns the buffer holding the result.
 template <typename RT>
-__device__ void fft_forward(typename C2<RT>::T* buf, int tb, const FftPlan& p, const typename C2<RT>::T* tw) {
+__device__ typename C2<RT>::T* fft_forward(typename C2<RT>::T* a, typename C2<RT>::T* b, int tb, const FftPlan& p,
+                                           const typename C2<RT>::T* tw) {
+  typedef typename C2<RT>::T C;
   int Ns = 1;
+  C* src = a;
+  C* dst = b;
   for (int s = 0; s < p.nstage; ++s) {
     const int R = p.radix[s];
-    if (R == 4) fft_stage<4, RT>(buf, tb, p.n, Ns, tw);
-    else if (R == 2) fft_stage<2, RT>(buf, tb, p.n, Ns, tw);
-    else if (R == 3) fft_stage<3, RT>(buf, tb, p.n, Ns, tw);
-    else fft_stage<5, RT>(buf, tb, p.n, Ns, tw);
+    switch (R) {
+      case 16: fft_pass<16, C>(src, dst, tb, p.n, Ns, tw); break;
+      case 8: fft_pass<8, C>(src, dst, tb, p.n, Ns, tw); break;
+      case 4: fft_pass<4, C>(src, dst, tb, p.n, Ns, tw); break;
+      case 2: fft_pass<2, C>(src, dst, tb, p.n, Ns, tw); break;
+      case 3: fft_pass<3, C>(src, dst, tb, p.n, Ns, tw); break;
+      default: fft_pass<5, C>(src, dst, tb, p.n, Ns, tw); break;
+    }
+    __syncthreads();
     Ns *= R;
+    C* t = src; src = dst; dst = t;
   }
+  return src;
 }
 
 template <typename RT>
-__global__ void __launch_bounds__(256) k_fft_synth(Dims d, FftPlan p, const typename C2<RT>::T* __restrict__ twg,
+__global__ void __launch_bounds__(256) k_fft_synth(Dims d, FftPlan p, const typename C2<RT>::T* __restrict__ tw,
                                                    const typename C2<RT>::T* __restrict__ F, RT* __restrict__ grid,
                                                    size_t grid_comp_stride) {
   typedef typename C2<RT>::T C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tw = reinterpret_cast<C*>(smem_raw);
-  C* buf = tw + p.n;
   const int n = p.n, tb = p.tb, M = d.M;
+  const int rs = prow(n);
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + (size_t)tb * rs;
   const int i0 = blockIdx.x * tb;
   const int r = blockIdx.y, comp = blockIdx.z;
   const int rows = min(tb, d.nth - i0);
-  for (int k = threadIdx.x; k < n; k += kThreads) tw[k] = twg[k];
-  for (int e = threadIdx.x; e < tb * n; e += kThreads) { buf[e].x = 0; buf[e].y = 0; }
-  __syncthreads();
+  // zero the band of unused frequencies M < k < n - M (and whole unused rows)
+  const int band = n - 2 * M - 1;
+  for (int e = threadIdx.x; e < tb * band; e += kThreads) {
+    const int ii = e / band, k = M + 1 + (e - ii * band);
+    bufA[(size_t)ii * rs + pidx(k)].x = 0; bufA[(size_t)ii * rs + pidx(k)].y = 0;
+  }
   const size_t fbase = ((size_t)(comp * d.nr + r) * (M + 1)) * 2 * d.nth;
-  for (int e = threadIdx.x; e < (M + 1) * rows; e += kThreads) {
-    const int m = e / rows, ii = e - m * rows;
-    const int ith = i0 + ii;
-    const C fn = F[fbase + ((size_t)m * 2 + 0) * d.nth + ith];
-    const C fs = F[fbase + ((size_t)m * 2 + 1) * d.nth + ith];
-    C* row = buf + (size_t)ii * n;
-    // Z_m = F_N + i F_S ; stored conjugated (inverse via conj(FFT(conj)))
+  for (int e = threadIdx.x; e < (M + 1) * tb; e += kThreads) {
+    const int m = e / tb, ii = e - m * tb;
+    C* row = bufA + (size_t)ii * rs;
+    C fn, fs;
+    if (ii < rows) {
+      fn = F[fbase + ((size_t)m * 2 + 0) * d.nth + i0 + ii];
+      fs = F[fbase + ((size_t)m * 2 + 1) * d.nth + i0 + ii];
+    } else {
+      fn.x = fn.y = fs.x = fs.y = 0;
+    }
+    // Z_m = F_N + i F_S, Z_{n-m} = conj(F_N) + i conj(F_S); stored conjugated
+    // (the inverse transform is conj(FFT(conj(Z)))).
     if (m == 0) {
       C z; z.x = fn.x; z.y = -fs.x;
       row[0] = z;
     } else {
       C z; z.x = fn.x - fs.y; z.y = -(fn.y + fs.x);
-      row[m] = z;
-      C zc; zc.x = fn.x + fs.y; zc.y = -(-fn.y + fs.x);
-      row[n - m] = zc;
+      row[pidx(m)] = z;
+      C zc; zc.x = fn.x + fs.y; zc.y = fn.y - fs.x;
+      row[pidx(n - m)] = zc;
     }
   }
   __syncthreads();
-  fft_forward<RT>(buf, tb, p, tw);
+  const C* res = fft_forward<RT>(bufA, bufB, tb, p, tw);
   RT* gbase = grid + grid_comp_stride * comp + (size_t)r * d.nlat * n;
   for (int e = threadIdx.x; e < rows * n; e += kThreads) {
     const int ii = e / n, j = e - ii * n;
-    const C z = buf[(size_t)ii * n + j];
+    const C z = res[(size_t)ii * rs + pidx(j)];
     const int ith = i0 + ii;
     gbase[(size_t)ith * n + j] = z.x;
     gbase[(size_t)(d.nlat - 1 - ith) * n + j] = -z.y;
@@ -175,18 +237,18 @@ __global__ void __launch_bounds__(256) k_fft_synth(Dims d, FftPlan p, const type
 }
 
 template <typename RT>
-__global__ void __launch_bounds__(256) k_fft_analysis(Dims d, FftPlan p, const typename C2<RT>::T* __restrict__ twg,
+__global__ void __launch_bounds__(256) k_fft_analysis(Dims d, FftPlan p, const typename C2<RT>::T* __restrict__ tw,
                                                       const RT* __restrict__ grid, size_t grid_comp_stride,
                                                       const double* __restrict__ w, typename C2<RT>::T* __restrict__ G) {
   typedef typename C2<RT>::T C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* tw = reinterpret_cast<C*>(smem_raw);
-  C* buf = tw + p.n;
   const int n = p.n, tb = p.tb, M = d.M;
+  const int rs = prow(n);
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + (size_t)tb * rs;
   const int i0 = blockIdx.x * tb;
   const int r = blockIdx.y, comp = blockIdx.z;
   const int rows = min(tb, d.nth - i0);
-  for (int k = threadIdx.x; k < n; k += kThreads) tw[k] = twg[k];
   const RT* gbase = grid + grid_comp_stride * comp + (size_t)r * d.nlat * n;
   for (int e = threadIdx.x; e < tb * n; e += kThreads) {
     const int ii = e / n, j = e - ii * n;
@@ -196,23 +258,22 @@ __global__ void __launch_bounds__(256) k_fft_analysis(Dims d, FftPlan p, const t
       z.x = gbase[(size_t)ith * n + j];
       z.y = gbase[(size_t)(d.nlat - 1 - ith) * n + j];
     }
-    buf[e] = z;
+    bufA[(size_t)ii * rs + pidx(j)] = z;
   }
   __syncthreads();
-  fft_forward<RT>(buf, tb, p, tw);
+  const C* res = fft_forward<RT>(bufA, bufB, tb, p, tw);
   const RT sc = (RT)(2.0 * 3.14159265358979323846 / n);
   const size_t gb = ((size_t)(comp * d.nr + r) * (M + 1)) * 2 * d.nth;
   for (int e = threadIdx.x; e < (M + 1) * rows; e += kThreads) {
     const int m = e / rows, ii = e - m * rows;
     const int ith = i0 + ii;
-    const C* row = buf + (size_t)ii * n;
-    const C zk = row[m];
-    C zn = row[(n - m) % n];
+    const C* row = res + (size_t)ii * rs;
+    const C zk = row[pidx(m)];
+    C zn = row[pidx((n - m) % n)];
     zn.y = -zn.y;
     C X, Y;
     X.x = (RT)0.5 * (zk.x + zn.x); X.y = (RT)0.5 * (zk.y + zn.y);
-    // Y = -i/2 (zk - zn)
-    Y.x = (RT)0.5 * (zk.y - zn.y); Y.y = (RT)-0.5 * (zk.x - zn.x);
+    Y.x = (RT)0.5 * (zk.y - zn.y); Y.y = (RT)-0.5 * (zk.x - zn.x);  // -i/2 (zk - zn)
     C gn, gs;
     gn.x = sc * X.x; gn.y = sc * X.y;
     gs.x = sc * Y.x; gs.y = sc * Y.y;
@@ -228,10 +289,17 @@ __global__ void __launch_bounds__(256) k_fft_analysis(Dims d, FftPlan p, const t
 FftPlan make_fft_plan(int nlon) {
   FftPlan p{};
   p.n = nlon;
-  int m = nlon;
-  for (int rr : {4, 2, 3, 5}) {
-    while (m % rr == 0) { p.radix[p.nstage++] = rr; m /= rr; }
-  }
+  int m = nlon, a = 0;
+  while (m % 2 == 0) { m /= 2; ++a; }
+  // powers of two in passes of 16, then one pass of 8, 4 or 2 (8 x 4 instead of 16 x 2)
+  int rest = a;
+  if (rest >= 5 && rest % 4 == 1) { p.radix[p.nstage++] = 8; p.radix[p.nstage++] = 4; rest -= 5; }
+  while (rest >= 4) { p.radix[p.nstage++] = 16; rest -= 4; }
+  if (rest == 3) p.radix[p.nstage++] = 8;
+  if (rest == 2) p.radix[p.nstage++] = 4;
+  if (rest == 1) p.radix[p.nstage++] = 2;
+  while (m % 3 == 0) { p.radix[p.nstage++] = 3; m /= 3; }
+  while (m % 5 == 0) { p.radix[p.nstage++] = 5; m /= 5; }
   if (m != 1) p.nstage = -1;  // unsupported prime factor
   return p;
 }
@@ -247,9 +315,9 @@ void make_twiddles(int n, std::vector<double>& tw) {
 
 template <typename RT>
 static int pick_tb(const Dims& d, int n) {
-  const int by_regs = Emax<RT>::v * kThreads / n;
-  const int by_smem = (int)((96 * 1024) / (n * sizeof(typename C2<RT>::T))) - 1;
-  int tb = by_regs < by_smem ? by_regs : by_smem;
+  // two [tb][n] complex buffers within ~56 KB (four CTAs per SM)
+  int tb = (int)((56 * 1024) / (2 * (size_t)prow(n) * sizeof(typename C2<RT>::T)));
+  if (tb > 16) tb = 16;
   if (tb > d.nth) tb = d.nth;
   if (tb < 1) tb = 1;
   return tb;
@@ -261,7 +329,7 @@ void launch_fft_synth(cudaStream_t s, const Dims& d, const FftPlan& p0, const vo
   typedef typename C2<RT>::T C;
   FftPlan p = p0;
   p.tb = pick_tb<RT>(d, p.n);
-  const size_t sm = (size_t)(p.n + p.tb * p.n) * sizeof(C);
+  const size_t sm = (size_t)2 * p.tb * prow(p.n) * sizeof(C);
   static bool attr_done = false;
   if (!attr_done) {
     cudaFuncSetAttribute(k_fft_synth<RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -277,7 +345,7 @@ void launch_fft_analysis(cudaStream_t s, const Dims& d, const FftPlan& p0, const
   typedef typename C2<RT>::T C;
   FftPlan p = p0;
   p.tb = pick_tb<RT>(d, p.n);
-  const size_t sm = (size_t)(p.n + p.tb * p.n) * sizeof(C);
+  const size_t sm = (size_t)2 * p.tb * prow(p.n) * sizeof(C);
   static bool attr_done = false;
   if (!attr_done) {
     cudaFuncSetAttribute(k_fft_analysis<RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -43,7 +43,7 @@ void launch_tables(cudaStream_t s, const Dims& d, const int* moff, const double*
 void launch_fd_weights(cudaStream_t s, int nr, int kl, int fd_mode, const double* r, double* d1, double* d2);
 void launch_build_lu(cudaStream_t s, int nr, int kl, int L, const double* d1, const double* d2,
                      const double* rinv, const double* rinv2, const double* nu, double dt, double theta,
-                     double* lin, double* lu, int* status);
+                     int bc_rows, double* lin, double* lu, int* status);
 
 // ---- Legendre (gd_legendre.cu) ----
 struct SynthArgs {
@@ -119,6 +119,9 @@ struct Cnab2Args {
   int nfield;
   int boot;
   int clamp_rows;
+  int bc_rows;                // Dirichlet rows in the operator: boundary rhs = bval (temperature) or 0
+  const double* bvals;        // temperature boundary values [2][nlm] (native order)
+  int temp_slot;              // slot index of the temperature field
   double inv_dt, lin_weight;
 };
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,

@@ -1,17 +1,259 @@
-// gd_mixed.cu -- mixed-precision path (placeholder until the tensor-core kernels land).
+// gd_mixed.cu -- the mixed-precision step: FP32 grids, phi transforms and
+// grid products; split-TF32 tensor-core Legendre contractions
+// (gd_legendre_tc.cu); FP64 spectral operators, CNAB2 solves and energies
+// (shared with the FP64 path).
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "gd_handle.cuh"
+#include "gd_internal.cuh"
 #include "gd_mixed.cuh"
+#include "gd_mixed_kernels.cuh"
 
 namespace gd {
-int mixed_create(gd_handle* h) { return set_error(h, GD_ERR_UNSUPPORTED, "mixed precision not built"); }
-void mixed_destroy(gd_handle*) {}
-size_t mixed_bytes(const gd_handle*) { return 0; }
-int mixed_temperature_nl(gd_handle* h) { return set_error(h, GD_ERR_UNSUPPORTED, "mixed precision not built"); }
-int mixed_velocity_nl(gd_handle* h) { return set_error(h, GD_ERR_UNSUPPORTED, "mixed precision not built"); }
-int mixed_magnetic_nl(gd_handle* h) { return set_error(h, GD_ERR_UNSUPPORTED, "mixed precision not built"); }
-void mixed_grid_to_double(gd_handle*, int, double*) {}
-int mixed_api_synth_scalar(gd_handle* h, const double* const*, int, double*) { return set_error(h, GD_ERR_UNSUPPORTED, "mixed"); }
-int mixed_api_synth_vector(gd_handle* h, const double*, const double*, double*) { return set_error(h, GD_ERR_UNSUPPORTED, "mixed"); }
-int mixed_api_analysis_scalar(gd_handle* h, const double*, int, double* const*) { return set_error(h, GD_ERR_UNSUPPORTED, "mixed"); }
-int mixed_api_analysis_vector(gd_handle* h, const double*, double*, double*) { return set_error(h, GD_ERR_UNSUPPORTED, "mixed"); }
+
+struct MixedState {
+  long* d_cofs = nullptr;
+  float* img_synth[3] = {nullptr, nullptr, nullptr};  // P, dP, Q
+  float* img_anal[3] = {nullptr, nullptr, nullptr};
+  float2* d_F = nullptr;       // 4 components
+  float* d_grid = nullptr;     // NGRID FP32 grids
+  float* d_stage = nullptr;    // 4 FP32 grids for the host-array entry points
+  int* d_err = nullptr;
+  size_t bytes = 0;
+  std::vector<void*> allocs;
+  float* grid(const gd_handle* h, int g) const { return d_grid + h->grid_elems() * g; }
+};
+
+namespace {
+
+int mcheck(gd_handle* h, cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return set_error(h, GD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return GD_OK;
+}
+
+template <typename T>
+int malloc_m(gd_handle* h, T** p, size_t n) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, n * sizeof(T) > 0 ? n * sizeof(T) : 16);
+  if (e != cudaSuccess) return set_error(h, GD_ERR_CUDA, std::string("cudaMalloc (mixed): ") + cudaGetErrorString(e));
+  h->mixed->allocs.push_back(q);
+  h->mixed->bytes += n * sizeof(T);
+  *p = static_cast<T*>(q);
+  return GD_OK;
+}
+
+#define MAL(ptr, n)                             \
+  do {                                          \
+    int s_ = malloc_m(h, &(ptr), (size_t)(n));  \
+    if (s_) return s_;                          \
+  } while (0)
+
+int launched(gd_handle* h, const char* what) { return mcheck(h, cudaGetLastError(), what); }
+
+int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float* grid_out) {
+  MixedState* x = h->mixed;
+  TcSynthArgs a{};
+  for (int i = 0; i < nf; ++i) a.coef[i] = coef[i];
+  a.nf = nf;
+  a.out = x->d_F;
+  a.err = x->d_err;
+  { ProfScope p(h, "legendre_synth_scalar_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], nullptr, a, false); }
+  { ProfScope p(h, "fft_synth_fp32"); launch_fft_synth<float>(h->stream, h->d, h->plan, h->d_twf, x->d_F, grid_out, nf, h->grid_elems()); }
+  return launched(h, "mixed scalar synthesis");
+}
+
+int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float* grid_out) {
+  MixedState* x = h->mixed;
+  TcSynthArgs a{};
+  a.coef[0] = pol;
+  a.coef[1] = tor;
+  a.nf = 1;
+  a.out = x->d_F;
+  a.err = x->d_err;
+  { ProfScope p(h, "legendre_synth_vector_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[1], x->img_synth[2], a, true); }
+  { ProfScope p(h, "fft_synth_fp32"); launch_fft_synth<float>(h->stream, h->d, h->plan, h->d_twf, x->d_F, grid_out, 2, h->grid_elems()); }
+  return launched(h, "mixed vector synthesis");
+}
+
+int tc_analysis_scalar(gd_handle* h, const float* grid_in, int nf, double* const* out) {
+  MixedState* x = h->mixed;
+  { ProfScope p(h, "fft_analysis_fp32"); launch_fft_analysis<float>(h->stream, h->d, h->plan, h->d_twf, grid_in, h->grid_elems(), h->d_w, x->d_F, nf); }
+  TcAnalysisArgs a{};
+  a.in = x->d_F;
+  for (int i = 0; i < nf; ++i) a.out[i] = out[i];
+  a.nf = nf;
+  a.epi = EPI_SCALAR;
+  a.err = x->d_err;
+  { ProfScope p(h, "legendre_analysis_scalar_tc"); launch_tc_analysis(h->stream, h->d, h->d_moff, x->img_anal[0], nullptr, a); }
+  return launched(h, "mixed scalar analysis");
+}
+
+int tc_analysis_vector(gd_handle* h, const float* grid_in, double* out_tor, double* out_pol, int epi) {
+  MixedState* x = h->mixed;
+  { ProfScope p(h, "fft_analysis_fp32"); launch_fft_analysis<float>(h->stream, h->d, h->plan, h->d_twf, grid_in, h->grid_elems(), h->d_w, x->d_F, 2); }
+  TcAnalysisArgs a{};
+  a.in = x->d_F;
+  a.out[0] = out_tor;
+  a.out[1] = out_pol;
+  a.nf = 1;
+  a.epi = epi;
+  a.err = x->d_err;
+  { ProfScope p(h, "legendre_analysis_vector_tc"); launch_tc_analysis(h->stream, h->d, h->d_moff, x->img_anal[1], x->img_anal[2], a); }
+  return launched(h, "mixed vector analysis");
+}
+
+}  // namespace
+
+int mixed_create(gd_handle* h) {
+  if (h->mixed) return GD_OK;
+  int major = 0, minor = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, h->device);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, h->device);
+  if (major != 10 || minor != 0)
+    return set_error(h, GD_ERR_UNSUPPORTED, "the mixed path needs an sm_100 (B200) device for tcgen05");
+  h->mixed = new MixedState();
+  MixedState* x = h->mixed;
+  const Dims& d = h->d;
+  std::vector<long> cofs;
+  const long nsyn = tc_synth_chunks(d, cofs);
+  const long nana = tc_analysis_chunks(d);
+  const size_t cb = tc_chunk_bytes() / sizeof(float);
+  MAL(x->d_cofs, cofs.size());
+  for (int t = 0; t < 3; ++t) {
+    MAL(x->img_synth[t], (size_t)nsyn * cb);
+    MAL(x->img_anal[t], (size_t)nana * cb);
+  }
+  MAL(x->d_F, (size_t)4 * d.nr * (d.M + 1) * d.nlat);
+  MAL(x->d_grid, (size_t)NGRID * h->grid_elems());
+  MAL(x->d_stage, (size_t)4 * h->grid_elems());
+  MAL(x->d_err, 4);
+  int s = mcheck(h, cudaMemcpyAsync(x->d_cofs, cofs.data(), sizeof(long) * cofs.size(), cudaMemcpyHostToDevice,
+                                    h->stream), "cofs upload");
+  if (s) return s;
+  const double* tabs[3] = {h->d_P, h->d_dP, h->d_Q};
+  for (int t = 0; t < 3; ++t)
+    launch_build_tc_images(h->stream, d, h->d_moff, x->d_cofs, tabs[t], x->img_synth[t], x->img_anal[t]);
+  s = launched(h, "table images");
+  if (s) return s;
+  s = mcheck(h, cudaMemsetAsync(x->d_grid, 0, sizeof(float) * NGRID * h->grid_elems(), h->stream), "memset");
+  if (s) return s;
+  s = mcheck(h, cudaMemsetAsync(x->d_err, 0, sizeof(int), h->stream), "memset");
+  if (s) return s;
+  return mcheck(h, cudaStreamSynchronize(h->stream), "mixed set-up");
+}
+
+void mixed_destroy(gd_handle* h) {
+  if (!h->mixed) return;
+  for (void* p : h->mixed->allocs) cudaFree(p);
+  delete h->mixed;
+  h->mixed = nullptr;
+}
+
+size_t mixed_bytes(const gd_handle* h) { return h->mixed ? h->mixed->bytes : 0; }
+
+int mixed_check_error(gd_handle* h) {
+  if (!h->mixed) return GD_OK;
+  int flag = 0;
+  int s = mcheck(h, cudaMemcpyAsync(&flag, h->mixed->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "err");
+  if (s) return s;
+  s = mcheck(h, cudaStreamSynchronize(h->stream), "err sync");
+  if (s) return s;
+  if (flag) return set_error(h, GD_ERR_CUDA, "a tensor-core pipeline wait expired (results of that call are invalid)");
+  return GD_OK;
+}
+
+int mixed_temperature_nl(gd_handle* h) {
+  MixedState* x = h->mixed;
+  const Dims& d = h->d;
+  { ProfScope p(h, "spectral_gradients");
+    launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), h->work(0), h->work(1), h->work(2)); }
+  const double* coef[4] = {h->field(F_TEMP), h->work(0), h->work(1), h->work(2)};
+  int s = tc_synth_scalar(h, coef, 4, x->grid(h, GD_GRID_T));
+  if (s) return s;
+  { ProfScope p(h, "nl_temperature_fp32");
+    launch_temperature_advection<float>(h->stream, d, x->grid(h, GD_GRID_U_TH), x->grid(h, GD_GRID_U_PH),
+                                        x->grid(h, GD_GRID_GTH), x->grid(h, GD_GRID_GPH), x->grid(h, GD_GRID_GR),
+                                        h->d_sources, x->grid(h, GD_GRID_TADV)); }
+  double* out[1] = {h->nlf(F_TEMP)};
+  s = tc_analysis_scalar(h, x->grid(h, GD_GRID_TADV), 1, out);
+  if (s) return s;
+  { ProfScope p(h, "temperature_bc"); launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP)); }
+  return launched(h, "mixed temperature nonlinear");
+}
+
+int mixed_velocity_nl(gd_handle* h) {
+  MixedState* x = h->mixed;
+  const Dims& d = h->d;
+  int s = tc_synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), x->grid(h, GD_GRID_U_TH));
+  if (s) return s;
+  { ProfScope p(h, "spectral_curl");
+    launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR), h->field(F_UPOL), h->work(3), h->work(4)); }
+  s = tc_synth_vector(h, h->work(3), h->work(4), x->grid(h, GD_GRID_W_TH));
+  if (s) return s;
+  const double rf = h->c.magnetic_prandtl / h->c.ekman;
+  { ProfScope p(h, "nl_velocity_fp32");
+    launch_velocity_nl<float>(h->stream, d, h->d_cth, h->d_sthc, rf, rf, h->c.magnetic, x->grid(h, GD_GRID_U_TH),
+                              x->grid(h, GD_GRID_U_PH), x->grid(h, GD_GRID_W_TH), x->grid(h, GD_GRID_W_PH),
+                              x->grid(h, GD_GRID_J_TH), x->grid(h, GD_GRID_J_PH), x->grid(h, GD_GRID_B_TH),
+                              x->grid(h, GD_GRID_B_PH), x->grid(h, GD_GRID_VADV_TH), x->grid(h, GD_GRID_VADV_PH)); }
+  return tc_analysis_vector(h, x->grid(h, GD_GRID_VADV_TH), h->nlf(F_UTOR), h->nlf(F_UPOL), EPI_VECTOR);
+}
+
+int mixed_magnetic_nl(gd_handle* h) {
+  MixedState* x = h->mixed;
+  const Dims& d = h->d;
+  int s = tc_synth_vector(h, h->field(F_BTOR), h->field(F_BPOL), x->grid(h, GD_GRID_B_TH));
+  if (s) return s;
+  { ProfScope p(h, "spectral_curl");
+    launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR), h->field(F_BPOL), h->work(5), h->work(6)); }
+  s = tc_synth_vector(h, h->work(5), h->work(6), x->grid(h, GD_GRID_J_TH));
+  if (s) return s;
+  { ProfScope p(h, "nl_induction_fp32");
+    launch_induction<float>(h->stream, d, x->grid(h, GD_GRID_U_TH), x->grid(h, GD_GRID_U_PH), x->grid(h, GD_GRID_B_TH),
+                            x->grid(h, GD_GRID_B_PH), x->grid(h, GD_GRID_IND_TH), x->grid(h, GD_GRID_IND_PH)); }
+  return tc_analysis_vector(h, x->grid(h, GD_GRID_IND_TH), h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
+}
+
+void mixed_grid_to_double(gd_handle* h, int grid, double* out) {
+  launch_grid_cast<float>(h->stream, h->grid_elems(), h->mixed->grid(h, grid), out);
+}
+
+int mixed_api_synth_scalar(gd_handle* h, const double* const* coef, int nf, double* grid_out) {
+  int s = tc_synth_scalar(h, coef, nf, h->mixed->d_stage);
+  if (s) return s;
+  launch_grid_cast<float>(h->stream, (size_t)nf * h->grid_elems(), h->mixed->d_stage, grid_out);
+  s = launched(h, "cast");
+  return s ? s : mixed_check_error(h);
+}
+
+int mixed_api_synth_vector(gd_handle* h, const double* tor, const double* pol, double* grid_out) {
+  int s = tc_synth_vector(h, tor, pol, h->mixed->d_stage);
+  if (s) return s;
+  launch_grid_cast<float>(h->stream, 2 * h->grid_elems(), h->mixed->d_stage, grid_out);
+  s = launched(h, "cast");
+  return s ? s : mixed_check_error(h);
+}
+
+int mixed_api_analysis_scalar(gd_handle* h, const double* grid_in, int nf, double* const* out) {
+  launch_cast_d2f(h->stream, (size_t)nf * h->grid_elems(), grid_in, h->mixed->d_stage);
+  int s = tc_analysis_scalar(h, h->mixed->d_stage, nf, out);
+  return s ? s : mixed_check_error(h);
+}
+
+int mixed_api_analysis_vector(gd_handle* h, const double* grid_in, double* tor, double* pol) {
+  launch_cast_d2f(h->stream, 2 * h->grid_elems(), grid_in, h->mixed->d_stage);
+  int s = tc_analysis_vector(h, h->mixed->d_stage, tor, pol, EPI_VECTOR);
+  return s ? s : mixed_check_error(h);
+}
+
+__global__ void k_cast_d2f(size_t n, const double* __restrict__ src, float* __restrict__ dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+void launch_cast_d2f(cudaStream_t s, size_t n, const double* src, float* dst) {
+  k_cast_d2f<<<148 * 8, 256, 0, s>>>(n, src, dst);
+}
+
 }  // namespace gd

@@ -8,6 +8,8 @@ struct gd_handle;
 
 namespace gd {
 int mixed_create(gd_handle* h);
+// GD_ERR_CUDA if a tensor-core wait expired since creation (synchronises the stream).
+int mixed_check_error(gd_handle* h);
 void mixed_destroy(gd_handle* h);
 size_t mixed_bytes(const gd_handle* h);
 int mixed_temperature_nl(gd_handle* h);

@@ -1,0 +1,36 @@
+// gd_mixed_kernels.cuh -- launch interface of the tensor-core Legendre kernels.
+#pragma once
+
+#include <vector>
+
+#include "gd_internal.cuh"
+
+namespace gd {
+
+struct TcSynthArgs {
+  const double* coef[4];  // scalar: nf fields ; vector: [0] = S (poloidal), [1] = T (toroidal)
+  float2* out;            // FP32 Fourier buffer [comp][r][m][s][ith]
+  int nf;
+  int* err;               // set to 1 if a bounded wait expires
+};
+
+struct TcAnalysisArgs {
+  const float2* in;       // folded FP32 Fourier buffer
+  double* out[4];         // scalar: nf outputs ; vector: [0] toroidal slot, [1] poloidal slot
+  int nf;
+  int epi;
+  int* err;
+};
+
+long tc_synth_chunks(const Dims& d, std::vector<long>& cofs);
+long tc_analysis_chunks(const Dims& d);
+size_t tc_chunk_bytes();
+void launch_build_tc_images(cudaStream_t s, const Dims& d, const int* moff, const long* cofs, const double* T,
+                            float* synth_img, float* anal_img);
+void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long* cofs, const float* img0,
+                     const float* img1, const TcSynthArgs& a, bool vec);
+void launch_tc_analysis(cudaStream_t s, const Dims& d, const int* moff, const float* img0, const float* img1,
+                        const TcAnalysisArgs& a);
+void launch_cast_d2f(cudaStream_t s, size_t n, const double* src, float* dst);
+
+}  // namespace gd

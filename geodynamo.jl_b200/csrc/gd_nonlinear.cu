@@ -10,16 +10,18 @@ namespace gd {
 
 // compute_scalar_advection_local! + add_internal_sources_local!
 // (src/scalar_field_common.jl:390-443): -(u . grad T) + S(r).
+// Grid: blockIdx.y = shell, grid-stride over the shell's theta-phi plane.
 template <typename R>
 __global__ void k_temperature_advection(Dims d, const R* __restrict__ uth, const R* __restrict__ uph,
                                         const R* __restrict__ gth, const R* __restrict__ gph,
                                         const R* __restrict__ gr, const double* __restrict__ src, R* __restrict__ out) {
-  const size_t plane = (size_t)d.nlat * d.nlon;
-  const size_t n = plane * d.nr;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+  const int plane = d.nlat * d.nlon;
+  const size_t base = (size_t)blockIdx.y * plane;
+  const double s = src[blockIdx.y];
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += gridDim.x * blockDim.x) {
+    const size_t i = base + q;
     const R ur = 0;
     R v = -(ur * gr[i] + uth[i] * gth[i] + uph[i] * gph[i]);
-    const double s = src[i / plane];
     if (s != 0.0) v += (R)s;
     out[i] = v;
   }
@@ -35,10 +37,12 @@ __global__ void k_velocity_nl(Dims d, const double* __restrict__ cth, const doub
                               const R* __restrict__ wth, const R* __restrict__ wph, const R* __restrict__ jth,
                               const R* __restrict__ jph, const R* __restrict__ bth, const R* __restrict__ bph,
                               R* __restrict__ ath, R* __restrict__ aph) {
-  const size_t n = (size_t)d.nlat * d.nlon * d.nr;
+  const int plane = d.nlat * d.nlon;
+  const size_t base = (size_t)blockIdx.y * plane;
   const R adv = (R)(-rf), mrf = (R)(-rf), lfr = (R)lf;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int jphi = (int)(i % d.nlon);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += gridDim.x * blockDim.x) {
+    const size_t i = base + q;
+    const int jphi = q % d.nlon;
     const int tidx = jphi < d.nlat - 1 ? jphi : d.nlat - 1;
     const R ct = (R)cth[tidx], st = (R)sth[tidx];
     const R ur = 0, wr = 0;
@@ -62,39 +66,40 @@ __global__ void k_velocity_nl(Dims d, const double* __restrict__ cth, const doub
 template <typename R>
 __global__ void k_induction(Dims d, const R* __restrict__ uth, const R* __restrict__ uph, const R* __restrict__ bth,
                             const R* __restrict__ bph, R* __restrict__ oth, R* __restrict__ oph) {
-  const size_t n = (size_t)d.nlat * d.nlon * d.nr;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+  const int plane = d.nlat * d.nlon;
+  const size_t base = (size_t)blockIdx.y * plane;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += gridDim.x * blockDim.x) {
+    const size_t i = base + q;
     const R ur = 0, br = 0;
     oth[i] = uph[i] * br - ur * bph[i];
     oph[i] = ur * bth[i] - uth[i] * br;
   }
 }
 
-static int grid_blocks(size_t n) {
-  size_t b = (n + 255) / 256;
-  const size_t cap = 148 * 16;
-  return (int)(b < cap ? b : cap);
+// blocks per shell: enough to cover ~4 elements per thread
+static dim3 grid_blocks(const Dims& d) {
+  const int plane = d.nlat * d.nlon;
+  int bx = (plane + 1023) / 1024;
+  if (bx < 1) bx = 1;
+  return dim3(bx, d.nr);
 }
 
 template <typename R>
 void launch_temperature_advection(cudaStream_t s, const Dims& d, const R* uth, const R* uph, const R* gth,
                                   const R* gph, const R* gr, const double* sources, R* out) {
-  const size_t n = (size_t)d.nlat * d.nlon * d.nr;
-  k_temperature_advection<R><<<grid_blocks(n), 256, 0, s>>>(d, uth, uph, gth, gph, gr, sources, out);
+  k_temperature_advection<R><<<grid_blocks(d), 256, 0, s>>>(d, uth, uph, gth, gph, gr, sources, out);
 }
 template <typename R>
 void launch_velocity_nl(cudaStream_t s, const Dims& d, const double* cth, const double* sth_cor, double rf,
                         double lf, int magnetic, const R* uth, const R* uph, const R* wth, const R* wph,
                         const R* jth, const R* jph, const R* bth, const R* bph, R* ath, R* aph) {
-  const size_t n = (size_t)d.nlat * d.nlon * d.nr;
-  k_velocity_nl<R><<<grid_blocks(n), 256, 0, s>>>(d, cth, sth_cor, rf, lf, magnetic, uth, uph, wth, wph, jth, jph,
+  k_velocity_nl<R><<<grid_blocks(d), 256, 0, s>>>(d, cth, sth_cor, rf, lf, magnetic, uth, uph, wth, wph, jth, jph,
                                                    bth, bph, ath, aph);
 }
 template <typename R>
 void launch_induction(cudaStream_t s, const Dims& d, const R* uth, const R* uph, const R* bth, const R* bph,
                       R* oth, R* oph) {
-  const size_t n = (size_t)d.nlat * d.nlon * d.nr;
-  k_induction<R><<<grid_blocks(n), 256, 0, s>>>(d, uth, uph, bth, bph, oth, oph);
+  k_induction<R><<<grid_blocks(d), 256, 0, s>>>(d, uth, uph, bth, bph, oth, oph);
 }
 
 template void launch_temperature_advection<double>(cudaStream_t, const Dims&, const double*, const double*,

@@ -195,8 +195,8 @@ void launch_fd_weights(cudaStream_t s, int nr, int kl, int fd_mode, const double
 // then factorize_banded (src/linear_algebra.jl:23-57, no pivoting).
 // One thread per (kind, l).  Bands in [kind][col][band][l] order.
 __global__ void k_build_lu(int N, int kl, int L, const double* d1, const double* d2, const double* rinv,
-                           const double* rinv2, const double* nu, double inv_dt, double mth, double* lin,
-                           double* lu, int* status) {
+                           const double* rinv2, const double* nu, double inv_dt, double mth, int bc_rows,
+                           double* lin, double* lu, int* status) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   const int kind = blockIdx.y;
   if (l > L) return;
@@ -219,6 +219,7 @@ __global__ void k_build_lu(int N, int kl, int L, const double* d1, const double*
       }
       double sv = __dmul_rn(lv, mth);
       if (i == j) sv = __dadd_rn(sv, inv_dt);
+      if (bc_rows && (i == 0 || i == N - 1)) sv = (i == j) ? 1.0 : 0.0;  // Dirichlet rows (bc_mode 2)
       lin[(((size_t)kind * N + j) * nbw + b) * Lp1 + l] = lv;
       lu[(((size_t)kind * N + j) * nbw + b) * Lp1 + l] = sv;
     }
@@ -240,9 +241,9 @@ __global__ void k_build_lu(int N, int kl, int L, const double* d1, const double*
 
 void launch_build_lu(cudaStream_t s, int nr, int kl, int L, const double* d1, const double* d2,
                      const double* rinv, const double* rinv2, const double* nu, double dt, double theta,
-                     double* lin, double* lu, int* status) {
+                     int bc_rows, double* lin, double* lu, int* status) {
   dim3 grid(ceil_div(L + 1, 32), 3);
-  k_build_lu<<<grid, 32, 0, s>>>(nr, kl, L, d1, d2, rinv, rinv2, nu, 1.0 / dt, -theta, lin, lu, status);
+  k_build_lu<<<grid, 32, 0, s>>>(nr, kl, L, d1, d2, rinv, rinv2, nu, 1.0 / dt, -theta, bc_rows, lin, lu, status);
 }
 
 }  // namespace gd

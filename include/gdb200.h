@@ -62,7 +62,9 @@ enum { GD_PREC_FP64 = 0, GD_PREC_MIXED = 1 };
  *             (step_once! never advances the step counter, simulation.jl:1153).
  *   bc_mode   0: reference behaviour (temperature Dirichlet rows only,
  *             thermal.jl:262-303); 1: also zero the r=ri and r=ro rows of all
- *             five fields after each solve.
+ *             five fields after each solve; 2: Dirichlet rows inside the
+ *             implicit operators of all five fields (well-posed variant; the
+ *             reference's operators have no boundary rows).
  *   fd_mode   0: radial difference weights from V^T w = rhs (the intent of
  *             create_derivative_matrix, linear_algebra.jl:90-132);
  *             1: the literal V c = rhs solve (ill-conditioned, kept for study).

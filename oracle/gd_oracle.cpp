@@ -37,7 +37,11 @@
 //          step (simulation.jl:1153 with a step counter that never advances).
 //   Q7     bc_mode 0: only temperature Dirichlet rows (thermal.jl:262-303);
 //          bc_mode 1: additionally zero r=ri and r=ro rows of all five fields
-//          after each solve.
+//          after each solve; bc_mode 2: Dirichlet rows inside the implicit
+//          operators of all five fields (identity rows at r=ri, r=ro; boundary
+//          values 0, or the temperature boundary values).  The reference's
+//          operators carry no boundary rows; mode 2 is the well-posed variant
+//          (bounded ||A^n||) used for accuracy studies.
 //   Q8     energies 0.5 sum (T^2+P^2)/max(l(l+1),1) (magnetic.jl:519-542).
 //   Q14    create_derivative_matrix (linear_algebra.jl:90-132) solves V c = rhs,
 //          which yields interpolation coefficients, not difference weights
@@ -382,6 +386,11 @@ struct Oracle {
         for (int n = 0; n < N; ++n) L[bw + (size_t)nbw * n] = L[bw + (size_t)nbw * n] - nu[k] * lf * rinv2[n];
         for (size_t q = 0; q < bsz; ++q) A[q] = L[q] * mth;
         for (int n = 0; n < N; ++n) A[bw + (size_t)nbw * n] = A[bw + (size_t)nbw * n] + inv_dt;
+        if (c.bc_mode == 2) {
+          for (int i : {0, N - 1})
+            for (int j = std::max(0, i - bw); j <= std::min(N - 1, i + bw); ++j)
+              A[(bw + i - j) + (size_t)nbw * j] = (i == j) ? 1.0 : 0.0;
+        }
         factorize(A);
       }
     }
@@ -825,6 +834,12 @@ struct Oracle {
           vr += lw * Lr[k];
           vi += lw * Li[k];
           xr[k] = vr; xi[k] = vi;
+        }
+        if (c.bc_mode == 2) {
+          xr[0] = (f == F_TEMP) ? bvals[q] : 0.0;
+          xr[N - 1] = (f == F_TEMP) ? bvals[(size_t)nlm + q] : 0.0;
+          xi[0] = 0.0;
+          xi[N - 1] = 0.0;
         }
         solve(&lu[kind][bsz * l], xr.data());
         solve(&lu[kind][bsz * l], xi.data());
