@@ -278,7 +278,7 @@ int implicit_launch(gd_handle* h, int boot) {
   a.temp_slot = 0;
   a.inv_dt = 1.0 / h->c.dt;
   a.lin_weight = 1.0 - h->c.implicit_theta;
-  { ProfScope p(h, "cnab2_solve"); launch_cnab2(h->stream, h->d, h->d_lof, h->d_lin, h->d_lu, a); }
+  { ProfScope p(h, "cnab2_solve"); launch_cnab2(h->stream, h->d, h->d_lof, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->d_lu, a); }
   return check_launch(h, "cnab2");
 }
 

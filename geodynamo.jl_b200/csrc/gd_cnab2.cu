@@ -13,123 +13,189 @@
 
 namespace gd {
 
-template <int KL>
-__global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ lof, const double* __restrict__ lin,
-                                               const double* __restrict__ lu, Cnab2Args a) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int fs = blockIdx.y;
-  if (j >= d.nlm || fs >= a.nfield) return;
+// One thread solves the (l, m) column of NF fields that share a diffusivity
+// (u_tor + u_pol, B_tor + B_pol, or T), so the per-l LU factors are loaded
+// once for both.  The linear operator L_l = nu lap - nu l(l+1)/r^2 is rebuilt
+// from the shared Laplacian band with the same roundings as the set-up kernel.
+template <int KL, int NF>
+__device__ __forceinline__ void cnab2_columns(const Dims& d, int j, int l, const double* __restrict__ lu,
+                                              const double* __restrict__ sband /* nu lap, smem */,
+                                              const double* __restrict__ srinv2, double nu, const Cnab2Args& a,
+                                              const int* slots) {
   const int N = d.nr;
-  const int l = lof[j];
-  const int kind = a.kind[fs];
   const size_t NM = d.nlm, plane = (size_t)N * NM;
   const size_t Lp1 = (size_t)d.L + 1;
   constexpr int NB = 2 * KL + 1;
-  double* ure = a.u[fs];
-  double* uim = ure + plane;
-  const double* nre = a.nl[fs];
-  const double* nim = nre + plane;
-  double* pre = a.prev[fs];
-  double* pim = pre + plane;
-  const double* LIN = lin + (size_t)kind * N * NB * Lp1 + l;
-  const double* LU = lu + (size_t)kind * N * NB * Lp1 + l;
-
-  // window wr[t] = u[i - KL + t]
-  double wr[NB], wi[NB];
+  const double nulf = __dmul_rn(nu, (double)l * (l + 1));
+  double* ure[NF]; double* uim[NF]; const double* nre[NF]; const double* nim[NF]; double* pre[NF]; double* pim[NF];
 #pragma unroll
-  for (int t = 0; t < NB; ++t) {
-    const int idx = t - KL;
-    wr[t] = (idx >= 0 && idx < N) ? ure[(size_t)idx * NM + j] : 0.0;
-    wi[t] = (idx >= 0 && idx < N) ? uim[(size_t)idx * NM + j] : 0.0;
+  for (int f = 0; f < NF; ++f) {
+    ure[f] = a.u[slots[f]]; uim[f] = ure[f] + plane;
+    nre[f] = a.nl[slots[f]]; nim[f] = nre[f] + plane;
+    pre[f] = a.prev[slots[f]]; pim[f] = pre[f] + plane;
   }
-  double yr[KL], yi[KL];  // y[i - KL + t]
+  const double* LU = lu + l;  // kind offset applied by the caller
+  double wr[NF][NB], wi[NF][NB];
 #pragma unroll
-  for (int t = 0; t < KL; ++t) yr[t] = yi[t] = 0.0;
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+      const int idx = t - KL;
+      wr[f][t] = (idx >= 0 && idx < N) ? ure[f][(size_t)idx * NM + j] : 0.0;
+      wi[f][t] = (idx >= 0 && idx < N) ? uim[f][(size_t)idx * NM + j] : 0.0;
+    }
+  double yr[NF][KL], yi[NF][KL];
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int t = 0; t < KL; ++t) yr[f][t] = yi[f][t] = 0.0;
 
   for (int i = 0; i < N; ++i) {
     const size_t at = (size_t)i * NM + j;
-    // (1 - theta) L u, summed over columns in ascending order
-    double Lr = 0.0, Li = 0.0;
+    double cfl[NB];
 #pragma unroll
     for (int t = 0; t < NB; ++t) {
       const int col = i - KL + t;
+      double cf = 0.0;
       if (col >= 0 && col < N) {
-        const double cf = LIN[((size_t)col * NB + (KL + i - col)) * Lp1];
-        Lr += cf * wr[t];
-        Li += cf * wi[t];
+        cf = sband[col * NB + (KL + i - col)];
+        if (t == KL) cf = __dsub_rn(cf, __dmul_rn(nulf, srinv2[i]));
       }
+      cfl[t] = cf;
     }
-    const double n_r = nre[at], n_i = nim[at];
-    double p_r, p_i;
-    if (a.boot) { p_r = n_r; p_i = n_i; } else { p_r = pre[at]; p_i = pim[at]; }
-    double vr = a.inv_dt * wr[KL] + 1.5 * n_r - 0.5 * p_r;
-    double vi = a.inv_dt * wi[KL] + 1.5 * n_i - 0.5 * p_i;
-    vr += a.lin_weight * Lr;
-    vi += a.lin_weight * Li;
-    if (a.bc_rows && (i == 0 || i == N - 1)) {
-      vr = (fs == a.temp_slot) ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
-      vi = 0.0;
-    }
-    // history roll: prev := nl
-    pre[at] = n_r;
-    pim[at] = n_i;
-    // forward substitution (unit lower factor)
-    double sr = 0.0, si = 0.0;
+    double lfac[KL];
 #pragma unroll
     for (int t = 0; t < KL; ++t) {
       const int col = i - KL + t;
-      if (col >= 0) {
-        const double cf = LU[((size_t)col * NB + (KL + i - col)) * Lp1];
-        sr += cf * yr[t];
-        si += cf * yi[t];
-      }
+      lfac[t] = (col >= 0) ? LU[((size_t)col * NB + (KL + i - col)) * Lp1] : 0.0;
     }
-    const double y_r = vr - sr, y_i = vi - si;
-    ure[at] = y_r;
-    uim[at] = y_i;
 #pragma unroll
-    for (int t = 0; t < KL - 1; ++t) { yr[t] = yr[t + 1]; yi[t] = yi[t + 1]; }
-    yr[KL - 1] = y_r;
-    yi[KL - 1] = y_i;
+    for (int f = 0; f < NF; ++f) {
+      double Lr = 0.0, Li = 0.0;
 #pragma unroll
-    for (int t = 0; t < NB - 1; ++t) { wr[t] = wr[t + 1]; wi[t] = wi[t + 1]; }
-    const int nxt = i + KL + 1;
-    wr[NB - 1] = (nxt < N) ? ure[(size_t)nxt * NM + j] : 0.0;
-    wi[NB - 1] = (nxt < N) ? uim[(size_t)nxt * NM + j] : 0.0;
+      for (int t = 0; t < NB; ++t) {
+        const int col = i - KL + t;
+        if (col >= 0 && col < N) {
+          Lr += cfl[t] * wr[f][t];
+          Li += cfl[t] * wi[f][t];
+        }
+      }
+      const double n_r = nre[f][at], n_i = nim[f][at];
+      double p_r, p_i;
+      if (a.boot) { p_r = n_r; p_i = n_i; } else { p_r = pre[f][at]; p_i = pim[f][at]; }
+      double vr = a.inv_dt * wr[f][KL] + 1.5 * n_r - 0.5 * p_r;
+      double vi = a.inv_dt * wi[f][KL] + 1.5 * n_i - 0.5 * p_i;
+      vr += a.lin_weight * Lr;
+      vi += a.lin_weight * Li;
+      if (a.bc_rows && (i == 0 || i == N - 1)) {
+        vr = (slots[f] == a.temp_slot) ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
+        vi = 0.0;
+      }
+      pre[f][at] = n_r;
+      pim[f][at] = n_i;
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int t = 0; t < KL; ++t) {
+        const int col = i - KL + t;
+        if (col >= 0) {
+          sr += lfac[t] * yr[f][t];
+          si += lfac[t] * yi[f][t];
+        }
+      }
+      const double y_r = vr - sr, y_i = vi - si;
+      ure[f][at] = y_r;
+      uim[f][at] = y_i;
+#pragma unroll
+      for (int t = 0; t < KL - 1; ++t) { yr[f][t] = yr[f][t + 1]; yi[f][t] = yi[f][t + 1]; }
+      yr[f][KL - 1] = y_r;
+      yi[f][KL - 1] = y_i;
+#pragma unroll
+      for (int t = 0; t < NB - 1; ++t) { wr[f][t] = wr[f][t + 1]; wi[f][t] = wi[f][t + 1]; }
+      const int nxt = i + KL + 1;
+      wr[f][NB - 1] = (nxt < N) ? ure[f][(size_t)nxt * NM + j] : 0.0;
+      wi[f][NB - 1] = (nxt < N) ? uim[f][(size_t)nxt * NM + j] : 0.0;
+    }
   }
-  // back substitution; xr[t] = x[i + 1 + t]
-  double xr[KL], xi[KL];
+  double xr[NF][KL], xi[NF][KL];
 #pragma unroll
-  for (int t = 0; t < KL; ++t) xr[t] = xi[t] = 0.0;
+  for (int f = 0; f < NF; ++f)
+#pragma unroll
+    for (int t = 0; t < KL; ++t) xr[f][t] = xi[f][t] = 0.0;
   for (int i = N - 1; i >= 0; --i) {
     const size_t at = (size_t)i * NM + j;
-    double sr = 0.0, si = 0.0;
+    double ufac[KL];
 #pragma unroll
     for (int t = 0; t < KL; ++t) {
       const int col = i + 1 + t;
-      if (col < N) {
-        const double cf = LU[((size_t)col * NB + (KL + i - col)) * Lp1];
-        sr += cf * xr[t];
-        si += cf * xi[t];
-      }
+      ufac[t] = (col < N) ? LU[((size_t)col * NB + (KL + i - col)) * Lp1] : 0.0;
     }
     const double dg = LU[((size_t)i * NB + KL) * Lp1];
-    double x_r = (ure[at] - sr) / dg;
-    double x_i = (uim[at] - si) / dg;
-    if (a.clamp_rows && (i == 0 || i == N - 1)) { x_r = 0.0; x_i = 0.0; }
-    ure[at] = x_r;
-    uim[at] = x_i;
 #pragma unroll
-    for (int t = KL - 1; t > 0; --t) { xr[t] = xr[t - 1]; xi[t] = xi[t - 1]; }
-    xr[0] = x_r;
-    xi[0] = x_i;
+    for (int f = 0; f < NF; ++f) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int t = 0; t < KL; ++t) {
+        const int col = i + 1 + t;
+        if (col < N) {
+          sr += ufac[t] * xr[f][t];
+          si += ufac[t] * xi[f][t];
+        }
+      }
+      double x_r = (ure[f][at] - sr) / dg;
+      double x_i = (uim[f][at] - si) / dg;
+      if (a.clamp_rows && (i == 0 || i == N - 1)) { x_r = 0.0; x_i = 0.0; }
+      ure[f][at] = x_r;
+      uim[f][at] = x_i;
+#pragma unroll
+      for (int t = KL - 1; t > 0; --t) { xr[f][t] = xr[f][t - 1]; xi[f][t] = xi[f][t - 1]; }
+      xr[f][0] = x_r;
+      xi[f][0] = x_i;
+    }
   }
 }
 
-void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,
-                  const Cnab2Args& a) {
-  dim3 grid(ceil_div(d.nlm, 128), a.nfield);
-  k_cnab2<GD_MAX_KL><<<grid, 128, 0, s>>>(d, lof, lin, lu, a);
+// blockIdx.y = diffusivity group g: fields with kind g (velocity pair, magnetic pair, temperature).
+template <int KL>
+__global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ lof, const double* __restrict__ d1,
+                                               const double* __restrict__ d2, const double* __restrict__ rinv,
+                                               const double* __restrict__ rinv2, const double* __restrict__ nu,
+                                               const double* __restrict__ lu, Cnab2Args a) {
+  constexpr int NB = 2 * KL + 1;
+  extern __shared__ double sm[];
+  double* sband = sm;                 // nu * lap, [col][band]
+  double* srinv2 = sm + (size_t)d.nr * NB;
+  const int g = blockIdx.y;
+  int slots[2], nf = 0;
+  for (int s = 0; s < a.nfield && nf < 2; ++s)
+    if (a.kind[s] == g) slots[nf++] = s;
+  if (nf == 0) return;
+  const double nuk = nu[g];
+  const int N = d.nr;
+  for (int e = threadIdx.x; e < N * NB; e += blockDim.x) {
+    const int col = e / NB, b = e % NB, i = col + b - KL;
+    double v = 0.0;
+    if (i >= 0 && i < N) {
+      const size_t q = b + (size_t)NB * col;
+      // same roundings as the set-up kernel: nu * (d2 + (2 r^-1) d1)
+      v = __dmul_rn(nuk, __dadd_rn(d2[q], __dmul_rn(__dmul_rn(2.0, rinv[i]), d1[q])));
+    }
+    sband[e] = v;
+  }
+  for (int i = threadIdx.x; i < N; i += blockDim.x) srinv2[i] = rinv2[i];
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.nlm) return;
+  const int l = lof[j];
+  const double* LUk = lu + (size_t)g * N * NB * ((size_t)d.L + 1);
+  if (nf == 2) cnab2_columns<KL, 2>(d, j, l, LUk, sband, srinv2, nuk, a, slots);
+  else cnab2_columns<KL, 1>(d, j, l, LUk, sband, srinv2, nuk, a, slots);
+}
+
+void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
+                  const double* rinv, const double* rinv2, const double* nu, const double* lu, const Cnab2Args& a) {
+  dim3 grid(ceil_div(d.nlm, 128), 3);
+  const size_t smem = ((size_t)d.nr * GD_NBW + d.nr) * sizeof(double);
+  k_cnab2<GD_MAX_KL><<<grid, 128, smem, s>>>(d, lof, d1, d2, rinv, rinv2, nu, lu, a);
 }
 
 // 0.5 sum over (r, l, m) of (T^2 + P^2) / max(l(l+1), 1) for velocity and

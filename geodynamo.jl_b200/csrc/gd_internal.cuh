@@ -41,6 +41,8 @@ void launch_gauss(cudaStream_t s, int nlat, double* x, double* w, double* th, do
 void launch_tables(cudaStream_t s, const Dims& d, const int* moff, const double* x, const double* sth,
                    double* P, double* dP, double* Q);
 void launch_fd_weights(cudaStream_t s, int nr, int kl, int fd_mode, const double* r, double* d1, double* d2);
+void launch_rec_tables(cudaStream_t s, const Dims& d, const int* moff, const double* x, const double* sth,
+                       double* ra, double* rb, double* rc, double* r1a, double* r1b, double* pmm, double* sinv);
 void launch_build_lu(cudaStream_t s, int nr, int kl, int L, const double* d1, const double* d2,
                      const double* rinv, const double* rinv2, const double* nu, double dt, double theta,
                      int bc_rows, double* lin, double* lu, int* status);
@@ -124,8 +126,8 @@ struct Cnab2Args {
   int temp_slot;              // slot index of the temperature field
   double inv_dt, lin_weight;
 };
-void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,
-                  const Cnab2Args& a);
+void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
+                  const double* rinv, const double* rinv2, const double* nu, const double* lu, const Cnab2Args& a);
 void launch_energy(cudaStream_t s, const Dims& d, const int* lof, const double* utor, const double* upol,
                    const double* btor, const double* bpol, double* partial, double* out);
 void launch_check_finite(cudaStream_t s, size_t n, const double* a, int* flag);

@@ -14,9 +14,11 @@
 namespace gd {
 
 struct MixedState {
+  double *ra = nullptr, *rb = nullptr, *rc = nullptr, *r1a = nullptr, *r1b = nullptr, *pmm = nullptr,
+         *sinv = nullptr;
   long* d_cofs = nullptr;
-  float* img_synth[3] = {nullptr, nullptr, nullptr};  // P, dP, Q
-  float* img_anal[3] = {nullptr, nullptr, nullptr};
+  float* img_synth[2] = {nullptr, nullptr};          // Pbar, dPbar/dtheta (synthesis orientation)
+  float* img_anal[3] = {nullptr, nullptr, nullptr};  // Pbar, dPbar/dtheta, Q (analysis orientation)
   float2* d_F = nullptr;       // 4 components
   float* d_grid = nullptr;     // NGRID FP32 grids
   float* d_stage = nullptr;    // 4 FP32 grids for the host-array entry points
@@ -52,6 +54,7 @@ int malloc_m(gd_handle* h, T** p, size_t n) {
 
 int launched(gd_handle* h, const char* what) { return mcheck(h, cudaGetLastError(), what); }
 
+
 int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float* grid_out) {
   MixedState* x = h->mixed;
   TcSynthArgs a{};
@@ -59,7 +62,7 @@ int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float* grid
   a.nf = nf;
   a.out = x->d_F;
   a.err = x->d_err;
-  { ProfScope p(h, "legendre_synth_scalar_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], nullptr, a, false); }
+  { ProfScope p(h, "legendre_synth_scalar_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], nullptr, x->sinv, a, false); }
   { ProfScope p(h, "fft_synth_fp32"); launch_fft_synth<float>(h->stream, h->d, h->plan, h->d_twf, x->d_F, grid_out, nf, h->grid_elems()); }
   return launched(h, "mixed scalar synthesis");
 }
@@ -72,7 +75,7 @@ int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float* g
   a.nf = 1;
   a.out = x->d_F;
   a.err = x->d_err;
-  { ProfScope p(h, "legendre_synth_vector_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[1], x->img_synth[2], a, true); }
+  { ProfScope p(h, "legendre_synth_vector_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], x->img_synth[1], x->sinv, a, true); }
   { ProfScope p(h, "fft_synth_fp32"); launch_fft_synth<float>(h->stream, h->d, h->plan, h->d_twf, x->d_F, grid_out, 2, h->grid_elems()); }
   return launched(h, "mixed vector synthesis");
 }
@@ -121,10 +124,11 @@ int mixed_create(gd_handle* h) {
   const long nana = tc_analysis_chunks(d);
   const size_t cb = tc_chunk_bytes() / sizeof(float);
   MAL(x->d_cofs, cofs.size());
-  for (int t = 0; t < 3; ++t) {
-    MAL(x->img_synth[t], (size_t)nsyn * cb);
-    MAL(x->img_anal[t], (size_t)nana * cb);
-  }
+  for (int t = 0; t < 2; ++t) MAL(x->img_synth[t], (size_t)nsyn * cb);
+  for (int t = 0; t < 3; ++t) MAL(x->img_anal[t], (size_t)nana * cb);
+  MAL(x->ra, d.nlm); MAL(x->rb, d.nlm); MAL(x->rc, d.nlm);
+  MAL(x->r1a, d.L + 1); MAL(x->r1b, d.L + 1);
+  MAL(x->pmm, (size_t)(d.M + 1) * d.nth); MAL(x->sinv, d.nth);
   MAL(x->d_F, (size_t)4 * d.nr * (d.M + 1) * d.nlat);
   MAL(x->d_grid, (size_t)NGRID * h->grid_elems());
   MAL(x->d_stage, (size_t)4 * h->grid_elems());
@@ -132,9 +136,16 @@ int mixed_create(gd_handle* h) {
   int s = mcheck(h, cudaMemcpyAsync(x->d_cofs, cofs.data(), sizeof(long) * cofs.size(), cudaMemcpyHostToDevice,
                                     h->stream), "cofs upload");
   if (s) return s;
+  s = mcheck(h, cudaMemsetAsync(x->r1a, 0, sizeof(double) * (d.L + 1), h->stream), "memset");
+  if (s) return s;
+  s = mcheck(h, cudaMemsetAsync(x->r1b, 0, sizeof(double) * (d.L + 1), h->stream), "memset");
+  if (s) return s;
+  launch_rec_tables(h->stream, d, h->d_moff, h->d_x, h->d_sth, x->ra, x->rb, x->rc, x->r1a, x->r1b, x->pmm, x->sinv);
   const double* tabs[3] = {h->d_P, h->d_dP, h->d_Q};
   for (int t = 0; t < 3; ++t)
-    launch_build_tc_images(h->stream, d, h->d_moff, x->d_cofs, tabs[t], x->img_synth[t], x->img_anal[t]);
+    launch_build_tc_images(h->stream, d, h->d_moff, x->d_cofs, tabs[t], t < 2 ? x->img_synth[t] : nullptr,
+                           x->img_anal[t]);
+  s = mcheck(h, cudaStreamSynchronize(h->stream), "cofs lifetime");
   s = launched(h, "table images");
   if (s) return s;
   s = mcheck(h, cudaMemsetAsync(x->d_grid, 0, sizeof(float) * NGRID * h->grid_elems(), h->stream), "memset");

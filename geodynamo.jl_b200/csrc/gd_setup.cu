@@ -247,3 +247,60 @@ void launch_build_lu(cudaStream_t s, int nr, int kl, int L, const double* d1, co
 }
 
 }  // namespace gd
+
+namespace gd {
+
+// Coefficients of the three-term recurrence, per m-major mode j = (l, m):
+//   Pbar_lm = a_lm (x Pbar_{l-1,m} - b_lm Pbar_{l-2,m})   (l >= m + 1; b = 0 at l = m + 1)
+// the derivative coefficient c_lm = sqrt((2l+1)(l^2-m^2)/(2l-1)) of
+//   dPbar_lm/dtheta = (l x Pbar_lm - c_lm Pbar_{l-1,m}) / sin(theta),
+// the m = 1 column coefficients for the m = 0 derivative, Pbar_mm at the
+// north nodes and 1/sin(theta).  Used by the tensor-core synthesis, which
+// regenerates the table rows on the fly.
+__global__ void k_rec_tables(int L, int M, int nth, const int* moff, const double* x, const double* sth,
+                             double* ra, double* rb, double* rc, double* r1a, double* r1b, double* pmm,
+                             double* sinv) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = blockIdx.y;
+  if (m <= M && l >= m && l <= L) {
+    const int j = moff[m] + (l - m);
+    double a = 0.0, b = 0.0, c = 0.0;
+    if (l == m + 1) {
+      a = sqrt(2.0 * m + 3.0);
+    } else if (l >= m + 2) {
+      a = sqrt((4.0 * l * l - 1.0) / ((double)l * l - (double)m * m));
+      b = sqrt(((l - 1.0) * (l - 1.0) - (double)m * m) / (4.0 * (l - 1.0) * (l - 1.0) - 1.0));
+    }
+    if (l > m) c = sqrt((2.0 * l + 1.0) * ((double)l * l - (double)m * m) / (2.0 * l - 1.0));
+    ra[j] = a;
+    rb[j] = b;
+    rc[j] = c;
+  }
+  if (m == 0 && l <= L) {
+    double a = 0.0, b = 0.0;
+    if (l == 2) {
+      a = sqrt(5.0);
+    } else if (l >= 3) {
+      a = sqrt((4.0 * l * l - 1.0) / ((double)l * l - 1.0));
+      b = sqrt(((l - 1.0) * (l - 1.0) - 1.0) / (4.0 * (l - 1.0) * (l - 1.0) - 1.0));
+    }
+    r1a[l] = a;
+    r1b[l] = b;
+  }
+  if (m <= M && l < nth) {
+    const double s = sth[l];
+    double p = 1.0 / sqrt(4.0 * kPi);
+    for (int mm = 1; mm <= m; ++mm) p = -sqrt((2.0 * mm + 1.0) / (2.0 * mm)) * s * p;
+    pmm[(size_t)m * nth + l] = p;
+    if (m == 0) sinv[l] = 1.0 / s;
+  }
+}
+
+void launch_rec_tables(cudaStream_t s, const Dims& d, const int* moff, const double* x, const double* sth,
+                       double* ra, double* rb, double* rc, double* r1a, double* r1b, double* pmm, double* sinv) {
+  const int n = (d.L + 1 > d.nth ? d.L + 1 : d.nth);
+  dim3 grid(ceil_div(n, 128), d.M + 1);
+  k_rec_tables<<<grid, 128, 0, s>>>(d.L, d.M, d.nth, moff, x, sth, ra, rb, rc, r1a, r1b, pmm, sinv);
+}
+
+}  // namespace gd
