@@ -27,7 +27,12 @@ __device__ __forceinline__ void cnab2_columns(const Dims& d, int j, int l, const
   const size_t Lp1 = (size_t)d.L + 1;
   constexpr int NB = 2 * KL + 1;
   const double nulf = __dmul_rn(nu, (double)l * (l + 1));
-  double* ure[NF]; double* uim[NF]; const double* nre[NF]; const double* nim[NF]; double* pre[NF]; double* pim[NF];
+  double* __restrict__ ure[NF];
+  double* __restrict__ uim[NF];
+  const double* __restrict__ nre[NF];
+  const double* __restrict__ nim[NF];
+  double* __restrict__ pre[NF];
+  double* __restrict__ pim[NF];
 #pragma unroll
   for (int f = 0; f < NF; ++f) {
     ure[f] = a.u[slots[f]]; uim[f] = ure[f] + plane;
@@ -50,6 +55,7 @@ __device__ __forceinline__ void cnab2_columns(const Dims& d, int j, int l, const
 #pragma unroll
     for (int t = 0; t < KL; ++t) yr[f][t] = yi[f][t] = 0.0;
 
+#pragma unroll 4
   for (int i = 0; i < N; ++i) {
     const size_t at = (size_t)i * NM + j;
     double cfl[NB];
@@ -121,6 +127,7 @@ __device__ __forceinline__ void cnab2_columns(const Dims& d, int j, int l, const
   for (int f = 0; f < NF; ++f)
 #pragma unroll
     for (int t = 0; t < KL; ++t) xr[f][t] = xi[f][t] = 0.0;
+#pragma unroll 4
   for (int i = N - 1; i >= 0; --i) {
     const size_t at = (size_t)i * NM + j;
     double ufac[KL];
@@ -154,7 +161,7 @@ __device__ __forceinline__ void cnab2_columns(const Dims& d, int j, int l, const
   }
 }
 
-// blockIdx.y = diffusivity group g: fields with kind g (velocity pair, magnetic pair, temperature).
+// blockIdx.y = field slot; the block's Laplacian band uses that field's diffusivity.
 template <int KL>
 __global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ lof, const double* __restrict__ d1,
                                                const double* __restrict__ d2, const double* __restrict__ rinv,
@@ -164,11 +171,10 @@ __global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ l
   extern __shared__ double sm[];
   double* sband = sm;                 // nu * lap, [col][band]
   double* srinv2 = sm + (size_t)d.nr * NB;
-  const int g = blockIdx.y;
-  int slots[2], nf = 0;
-  for (int s = 0; s < a.nfield && nf < 2; ++s)
-    if (a.kind[s] == g) slots[nf++] = s;
-  if (nf == 0) return;
+  const int slot = blockIdx.y;
+  if (slot >= a.nfield) return;
+  const int g = a.kind[slot];
+  const int slots[1] = {slot};
   const double nuk = nu[g];
   const int N = d.nr;
   for (int e = threadIdx.x; e < N * NB; e += blockDim.x) {
@@ -187,13 +193,12 @@ __global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ l
   if (j >= d.nlm) return;
   const int l = lof[j];
   const double* LUk = lu + (size_t)g * N * NB * ((size_t)d.L + 1);
-  if (nf == 2) cnab2_columns<KL, 2>(d, j, l, LUk, sband, srinv2, nuk, a, slots);
-  else cnab2_columns<KL, 1>(d, j, l, LUk, sband, srinv2, nuk, a, slots);
+  cnab2_columns<KL, 1>(d, j, l, LUk, sband, srinv2, nuk, a, slots);
 }
 
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
                   const double* rinv, const double* rinv2, const double* nu, const double* lu, const Cnab2Args& a) {
-  dim3 grid(ceil_div(d.nlm, 128), 3);
+  dim3 grid(ceil_div(d.nlm, 128), a.nfield);
   const size_t smem = ((size_t)d.nr * GD_NBW + d.nr) * sizeof(double);
   k_cnab2<GD_MAX_KL><<<grid, 128, smem, s>>>(d, lof, d1, d2, rinv, rinv2, nu, lu, a);
 }
