@@ -57,6 +57,7 @@ EXPORTS = (
     "gd_vector_analysis", "gd_temperature_nonlinear", "gd_velocity_nonlinear", "gd_magnetic_nonlinear",
     "gd_implicit_step", "gd_step", "gd_step_async", "gd_set_dt", "gd_energy", "gd_check_finite",
     "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
+    "gd_spectral_to_physical_noalloc",
 )
 
 
@@ -137,6 +138,7 @@ def load_library():
         "gd_get_stream": ([P, ctypes.POINTER(P)], I),
         "gd_profile_enable": ([P, I], I),
         "gd_profile_read": ([P, I, ctypes.c_char_p, D, ctypes.POINTER(I), ctypes.POINTER(I)], I),
+        "gd_spectral_to_physical_noalloc": ([P, I, ctypes.c_void_p, ctypes.c_void_p], I),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)

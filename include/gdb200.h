@@ -128,6 +128,23 @@ int gd_vector_synthesis(gd_handle* h, const double* tor_re, const double* tor_im
 int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re,
                        double* tor_im, double* pol_re, double* pol_im);
 
+/* No counterpart in the reference.  Scalar synthesis (as
+ * gd_spectral_to_physical, always FP64) for callers that must not allocate
+ * device memory during the call -- for example a Julia session whose GPU memory
+ * is owned by CUDA.jl's pool, or a solver loop that forbids allocation after
+ * set-up.  d_coef and d_grid are the caller's device buffers in the native
+ * layout: d_coef holds nfield fields of two planes (Re, Im) of nr x nlm doubles
+ * with the m-major mode index j = moff[m] + (l - m); d_grid receives nfield
+ * grids of nr x nlat x nlon doubles, phi fastest.  The Fourier intermediate
+ * uses a fixed 64 MiB array in the library's device image instead of
+ * cudaMalloc: min(nfield, 4) x nr x (mmax+1) x nlat x 16 bytes must fit, else
+ * GD_ERR_CONFIG.  The first call on a device looks up that array's device
+ * address; make it before any stream capture.  The array is shared by every
+ * call and keeps the last call's contents (each call overwrites what it
+ * reads), so calls that overlap on the GPU (other streams, other threads)
+ * race.  Runs asynchronously on the handle's stream; gd_synchronize() waits. */
+int gd_spectral_to_physical_noalloc(gd_handle* h, int nfield, const double* d_coef, double* d_grid);
+
 /* ---- model step ---------------------------------------------------------------
  * compute_temperature_nonlinear! (src/thermal.jl:149-190),
  * compute_velocity_nonlinear! (src/velocity.jl:312-332),
