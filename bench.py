@@ -208,7 +208,11 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=100,
                     help="steps of the FP64 vs mixed energy comparison (0 = skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    help="named shell workload (the headline metric is shell_l255_nr129; smaller ones are for profiling)")
     args = ap.parse_args()
+    if args.workload != WORKLOAD:
+        globals()["WORKLOAD"] = args.workload
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -404,7 +408,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32/tf32x3 (FP64 solves)",
                 "data": "synthetic (seeded default_rng(0) state, amplitude 1e-3 (l+1)^-2)",
-                "config": {"workload": WORKLOAD, "lmax": 255, "nlat": 384, "nlon": 768, "nr": 129,
+                "config": {"workload": WORKLOAD, "lmax": p["lmax"], "nlat": p["nlat"], "nlon": p["nlon"], "nr": p["nr"],
                            "dt": p["dt"], "precision": precision, "parallelism": f"replicas x{world}",
                            "l2": "working set 5+ GB of grids per step, larger than L2; no flush"},
                 "fp64_gpu_value": fp64_value, "ratio_vs_fp64_gpu": value / fp64_value if fp64_value else None,

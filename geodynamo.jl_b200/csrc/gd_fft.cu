@@ -127,8 +127,10 @@ template <typename C> struct Dft<16, C> {
 
 // Shared-memory rows are padded by one element every 16 so the stride-16
 // stores of the first radix-16 pass do not all fall into one bank.
+// Rows are further padded to an odd number of elements so the transposed
+// (m, row) accesses of the load and store phases spread over the banks.
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
-__host__ __device__ __forceinline__ int prow(int n) { return n + (n >> 4); }
+__host__ __device__ __forceinline__ int prow(int n) { return (n + (n >> 4)) | 1; }
 
 // One Stockham pass from src to dst ([tb][n] each): radix R, Ns = product of
 // the radices of the earlier passes.
@@ -286,6 +288,216 @@ __global__ void __launch_bounds__(256) k_fft_analysis(Dims d, FftPlan p, const t
   }
 }
 
+// ---------------------------------------------------------------------------
+// Compile-time variants for the transform lengths in use: every index
+// division below is by a constant (the runtime-plan kernels above spend most
+// of their instructions in integer division).
+// ---------------------------------------------------------------------------
+struct CPlan {
+  int n, ns;
+  int r[12];
+};
+constexpr CPlan make_cplan(int n) {
+  CPlan p{n, 0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+  int m = n, a = 0;
+  while (m % 2 == 0) { m /= 2; ++a; }
+  int rest = a;
+  if (rest >= 5 && rest % 4 == 1) { p.r[p.ns++] = 8; p.r[p.ns++] = 4; rest -= 5; }
+  while (rest >= 4) { p.r[p.ns++] = 16; rest -= 4; }
+  if (rest == 3) p.r[p.ns++] = 8;
+  if (rest == 2) p.r[p.ns++] = 4;
+  if (rest == 1) p.r[p.ns++] = 2;
+  while (m % 3 == 0) { p.r[p.ns++] = 3; m /= 3; }
+  while (m % 5 == 0) { p.r[p.ns++] = 5; m /= 5; }
+  return p;
+}
+template <int N> struct PlanOf { static constexpr CPlan p = make_cplan(N); };
+
+template <typename RT, int N> struct CtGeom {
+  typedef typename C2<RT>::T C;
+  static constexpr int RS = (N + (N >> 4)) | 1;  // padded row stride (elements)
+  static constexpr int TB0 = (int)((56 * 1024) / (2 * (size_t)RS * sizeof(C)));
+  static constexpr int TB = TB0 > 16 ? 16 : (TB0 < 1 ? 1 : TB0);
+};
+
+template <int R, int N, int TB, int NS, typename C>
+__device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw) {
+  constexpr int RS = (N + (N >> 4)) | 1;
+  constexpr int NBF = N / R;
+  constexpr int TOTAL = TB * NBF;
+  constexpr int TWSTEP = N / (NS * R);
+  for (int b = threadIdx.x; b < TOTAL; b += kThreads) {
+    const int row = b / NBF, j = b - row * NBF;
+    const int k = j % NS;
+    const C* s = src + row * RS;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = s[pidx(j + r * NBF)];
+    if (NS > 1 && k > 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(&tw[r * k * TWSTEP]));
+    }
+    Dft<R, C>::run(v);
+    C* o = dst + row * RS;
+    const int o0 = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) o[pidx(o0 + r * NS)] = v[r];
+  }
+}
+
+template <int N, int TB, int S, int NS, typename C>
+__device__ __forceinline__ C* ct_passes(C* src, C* dst, const C* tw) {
+  constexpr CPlan P = PlanOf<N>::p;
+  if constexpr (S >= P.ns) {
+    return src;
+  } else {
+    constexpr int R = P.r[S];
+    ct_pass<R, N, TB, NS, C>(src, dst, tw);
+    __syncthreads();
+    return ct_passes<N, TB, S + 1, NS * R, C>(dst, src, tw);
+  }
+}
+
+template <typename RT, int N>
+__global__ void __launch_bounds__(256) k_fft_synth_ct(Dims d, const typename C2<RT>::T* __restrict__ tw,
+                                                      const typename C2<RT>::T* __restrict__ F, RT* __restrict__ grid,
+                                                      size_t grid_comp_stride) {
+  typedef typename C2<RT>::T C;
+  constexpr int RS = CtGeom<RT, N>::RS, TB = CtGeom<RT, N>::TB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + TB * RS;
+  const int M = d.M;
+  const int i0 = blockIdx.x * TB;
+  const int r = blockIdx.y, comp = blockIdx.z;
+  const int rows = min(TB, d.nth - i0);
+  for (int e = threadIdx.x; e < TB * N; e += kThreads) {
+    const int ii = e / N, k = e - ii * N;
+    if (k > M && k < N - M) { bufA[ii * RS + pidx(k)].x = 0; bufA[ii * RS + pidx(k)].y = 0; }
+  }
+  const size_t fbase = ((size_t)(comp * d.nr + r) * (M + 1)) * 2 * d.nth + i0;
+  for (int e = threadIdx.x; e < (M + 1) * TB; e += kThreads) {
+    const int m = e / TB, ii = e - m * TB;
+    C* row = bufA + ii * RS;
+    C fn, fs;
+    if (ii < rows) {
+      fn = F[fbase + ((size_t)m * 2 + 0) * d.nth + ii];
+      fs = F[fbase + ((size_t)m * 2 + 1) * d.nth + ii];
+    } else {
+      fn.x = fn.y = fs.x = fs.y = 0;
+    }
+    if (m == 0) {
+      C z; z.x = fn.x; z.y = -fs.x;
+      row[0] = z;
+    } else {
+      C z; z.x = fn.x - fs.y; z.y = -(fn.y + fs.x);
+      row[pidx(m)] = z;
+      C zc; zc.x = fn.x + fs.y; zc.y = fn.y - fs.x;
+      row[pidx(N - m)] = zc;
+    }
+  }
+  __syncthreads();
+  const C* res = ct_passes<N, TB, 0, 1, C>(bufA, bufB, tw);
+  RT* gbase = grid + grid_comp_stride * comp + (size_t)r * d.nlat * N;
+  for (int e = threadIdx.x; e < rows * N; e += kThreads) {
+    const int ii = e / N, j = e - ii * N;
+    const C z = res[ii * RS + pidx(j)];
+    const int ith = i0 + ii;
+    gbase[(size_t)ith * N + j] = z.x;
+    gbase[(size_t)(d.nlat - 1 - ith) * N + j] = -z.y;
+  }
+}
+
+template <typename RT, int N>
+__global__ void __launch_bounds__(256) k_fft_analysis_ct(Dims d, const typename C2<RT>::T* __restrict__ tw,
+                                                         const RT* __restrict__ grid, size_t grid_comp_stride,
+                                                         const double* __restrict__ w,
+                                                         typename C2<RT>::T* __restrict__ G) {
+  typedef typename C2<RT>::T C;
+  constexpr int RS = CtGeom<RT, N>::RS, TB = CtGeom<RT, N>::TB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + TB * RS;
+  const int M = d.M;
+  const int i0 = blockIdx.x * TB;
+  const int r = blockIdx.y, comp = blockIdx.z;
+  const int rows = min(TB, d.nth - i0);
+  const RT* gbase = grid + grid_comp_stride * comp + (size_t)r * d.nlat * N;
+  for (int e = threadIdx.x; e < TB * N; e += kThreads) {
+    const int ii = e / N, j = e - ii * N;
+    C z; z.x = 0; z.y = 0;
+    if (ii < rows) {
+      const int ith = i0 + ii;
+      z.x = gbase[(size_t)ith * N + j];
+      z.y = gbase[(size_t)(d.nlat - 1 - ith) * N + j];
+    }
+    bufA[ii * RS + pidx(j)] = z;
+  }
+  __syncthreads();
+  const C* res = ct_passes<N, TB, 0, 1, C>(bufA, bufB, tw);
+  const RT sc = (RT)(2.0 * 3.14159265358979323846 / N);
+  const size_t gb = ((size_t)(comp * d.nr + r) * (M + 1)) * 2 * d.nth;
+  for (int e = threadIdx.x; e < (M + 1) * TB; e += kThreads) {
+    const int m = e / TB, ii = e - m * TB;
+    if (ii >= rows) continue;
+    const int ith = i0 + ii;
+    const C* row = res + ii * RS;
+    const C zk = row[pidx(m)];
+    C zn = row[pidx(m == 0 ? 0 : N - m)];
+    zn.y = -zn.y;
+    C X, Y;
+    X.x = (RT)0.5 * (zk.x + zn.x); X.y = (RT)0.5 * (zk.y + zn.y);
+    Y.x = (RT)0.5 * (zk.y - zn.y); Y.y = (RT)-0.5 * (zk.x - zn.x);
+    C gn, gs;
+    gn.x = sc * X.x; gn.y = sc * X.y;
+    gs.x = sc * Y.x; gs.y = sc * Y.y;
+    const RT wi = (RT)w[ith];
+    C gp, gm;
+    gp.x = wi * (gn.x + gs.x); gp.y = wi * (gn.y + gs.y);
+    gm.x = wi * (gn.x - gs.x); gm.y = wi * (gn.y - gs.y);
+    G[gb + ((size_t)m * 2 + 0) * d.nth + ith] = gp;
+    G[gb + ((size_t)m * 2 + 1) * d.nth + ith] = gm;
+  }
+}
+
+template <typename RT, int N>
+static bool launch_ct(cudaStream_t s, const Dims& d, const void* tw, const void* F, RT* grid, size_t stride,
+                      int ncomp, bool synth, const double* w) {
+  typedef typename C2<RT>::T C;
+  constexpr int RS = CtGeom<RT, N>::RS, TB = CtGeom<RT, N>::TB;
+  const size_t sm = (size_t)2 * TB * RS * sizeof(C);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_fft_synth_ct<RT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    cudaFuncSetAttribute(k_fft_analysis_ct<RT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    attr = true;
+  }
+  dim3 g(ceil_div(d.nth, TB), d.nr, ncomp);
+  if (synth)
+    k_fft_synth_ct<RT, N><<<g, kThreads, sm, s>>>(d, (const C*)tw, (const C*)F, grid, stride);
+  else
+    k_fft_analysis_ct<RT, N><<<g, kThreads, sm, s>>>(d, (const C*)tw, grid, stride, w, (C*)const_cast<void*>(F));
+  return true;
+}
+
+// Dispatch to a compile-time length when there is one.
+template <typename RT>
+static bool launch_fixed(cudaStream_t s, const Dims& d, int n, const void* tw, const void* F, RT* grid,
+                         size_t stride, int ncomp, bool synth, const double* w) {
+  switch (n) {
+    case 24: return launch_ct<RT, 24>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    case 40: return launch_ct<RT, 40>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    case 48: return launch_ct<RT, 48>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    case 96: return launch_ct<RT, 96>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    case 144: return launch_ct<RT, 144>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    case 192: return launch_ct<RT, 192>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    case 288: return launch_ct<RT, 288>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    case 384: return launch_ct<RT, 384>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    case 768: return launch_ct<RT, 768>(s, d, tw, F, grid, stride, ncomp, synth, w);
+    default: return false;
+  }
+}
+
 FftPlan make_fft_plan(int nlon) {
   FftPlan p{};
   p.n = nlon;
@@ -327,6 +539,7 @@ template <typename RT>
 void launch_fft_synth(cudaStream_t s, const Dims& d, const FftPlan& p0, const void* twiddle, const void* F,
                       RT* grid, int ncomp, size_t grid_comp_stride) {
   typedef typename C2<RT>::T C;
+  if (launch_fixed<RT>(s, d, p0.n, twiddle, F, grid, grid_comp_stride, ncomp, true, nullptr)) return;
   FftPlan p = p0;
   p.tb = pick_tb<RT>(d, p.n);
   const size_t sm = (size_t)2 * p.tb * prow(p.n) * sizeof(C);
@@ -343,6 +556,7 @@ template <typename RT>
 void launch_fft_analysis(cudaStream_t s, const Dims& d, const FftPlan& p0, const void* twiddle, const RT* grid,
                          size_t grid_comp_stride, const double* w, void* G, int ncomp) {
   typedef typename C2<RT>::T C;
+  if (launch_fixed<RT>(s, d, p0.n, twiddle, G, const_cast<RT*>(grid), grid_comp_stride, ncomp, false, w)) return;
   FftPlan p = p0;
   p.tb = pick_tb<RT>(d, p.n);
   const size_t sm = (size_t)2 * p.tb * prow(p.n) * sizeof(C);

@@ -214,11 +214,13 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
                                                       const long* __restrict__ cofs, const float* __restrict__ imgP,
                                                       const float* __restrict__ imgD, const double* __restrict__ sinv,
                                                       TcSynthArgs a) {
-  constexpr int S = VEC ? 2 : 3;
+  constexpr int S = 2;
+  constexpr int NCS = VEC ? TC_N2 : 2 * TC_N2;   // columns per CTA: vector 128, scalar 256
   constexpr int A_FL = (VEC ? 2 : 1) * CHUNK_FLOATS;
-  constexpr int BT = TC_N2 * TC_K;  // one B image (hi or lo): 4096 floats
+  constexpr int BT = NCS * TC_K;  // one B image (hi or lo)
   constexpr int ST_FL = A_FL + 2 * BT;
-  constexpr uint32_t NCOL = VEC ? 512 : 256;
+  constexpr uint32_t NCOL = 512;
+  constexpr uint32_t IDS = idesc_tf32(TC_M, NCS);
   extern __shared__ unsigned char smem_raw[];
   const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   float* stg = reinterpret_cast<float*>(base);
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
   const int L = d.L, mb = moff[m];
   const size_t NM = d.nlm;
   const int Ntot = a.nf * d.nr * 2;
-  const int n0 = blockIdx.x * TC_N2;
+  const int n0 = blockIdx.x * NCS;
   const int r0 = blockIdx.x * 32;
   if (tile * TC_M >= d.nth || (VEC ? r0 >= d.nr : n0 >= Ntot)) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -254,10 +256,10 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
     if (VEC) async_chunk(A + CHUNK_FLOATS, imgD, synth_chunk(cofs, L, m, tile, p, kc));
     cp_async_commit();
     const int l = m + p + 2 * (TC_K * kc + lane);
-    // all 16 loads of this thread first (memory-level parallelism), then split
-    double v[TC_N2 / 8];
+    // all loads of this thread first (memory-level parallelism), then split
+    double v[NCS / 8];
 #pragma unroll
-    for (int i = 0; i < TC_N2 / 8; ++i) {
+    for (int i = 0; i < NCS / 8; ++i) {
       const int row = warp + 8 * i;
       const double* src = nullptr;
       if (VEC) {
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
       v[i] = (src != nullptr && l <= L) ? __ldg(src + l) : 0.0;
     }
 #pragma unroll
-    for (int i = 0; i < TC_N2 / 8; ++i) put_split_d(B, B + BT, warp + 8 * i, lane, v[i]);
+    for (int i = 0; i < NCS / 8; ++i) put_split_d(B, B + BT, warp + 8 * i, lane, v[i]);
   };
 
   bool ok = true;
@@ -291,8 +293,8 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
       const float* B = A + A_FL;
 #pragma unroll
       for (int t = 0; t < (VEC ? 2 : 1); ++t)
-        issue_chunk(tmem, (t * 2 + p) * TC_N2, A + t * CHUNK_FLOATS, A + t * CHUNK_FLOATS + TILE_A_FLOATS, B, B + BT,
-                    kc == 0, IDESC2);
+        issue_chunk(tmem, (t * 2 + p) * NCS, A + t * CHUNK_FLOATS, A + t * CHUNK_FLOATS + TILE_A_FLOATS, B, B + BT,
+                    kc == 0, IDS);
       mma_commit(smem_addr(&bars[s]));
     }
     if (it + 1 < T) {
@@ -315,10 +317,10 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
     const int ith = tile * TC_M + q * 32 + lane;
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
     if (!VEC) {
-      for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 8) {
+      for (int c0 = (NCS / 2) * half; c0 < (NCS / 2) * (half + 1); c0 += 8) {
         float e[8], o[8];
         tmem_ld8(trow + c0, e);
-        if (nc1 > 0) tmem_ld8(trow + TC_N2 + c0, o);
+        if (nc1 > 0) tmem_ld8(trow + NCS + c0, o);
         tmem_ld_wait();
         if (nc1 == 0) {
 #pragma unroll
@@ -591,7 +593,7 @@ static void smem_attr(K k, size_t bytes) {
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 static size_t synth_smem(bool vec) {
-  const int S = vec ? 2 : 3, A = (vec ? 2 : 1) * CHUNK_FLOATS, B = 2 * TC_N2 * TC_K;
+  const int S = 2, A = (vec ? 2 : 1) * CHUNK_FLOATS, B = 2 * (vec ? TC_N2 : 2 * TC_N2) * TC_K;
   return 1024 + (size_t)S * (A + B) * 4 + 64;
 }
 static size_t analysis_smem(bool vec) {
@@ -614,7 +616,7 @@ void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long*
   set_attrs();
   const int ntile = (d.nth + TC_M - 1) / TC_M;
   if (!vec) {
-    dim3 grid(ceil_div(a.nf * d.nr * 2, TC_N2), ntile, d.M + 1);
+    dim3 grid(ceil_div(a.nf * d.nr * 2, 2 * TC_N2), ntile, d.M + 1);
     k_tc_synth3<false><<<grid, 256, synth_smem(false), s>>>(d, moff, cofs, imgP, imgD, sinv, a);
   } else {
     dim3 grid(ceil_div(d.nr, 32), ntile, d.M + 1);
