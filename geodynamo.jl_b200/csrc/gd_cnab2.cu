@@ -13,150 +13,171 @@
 
 namespace gd {
 
-// One thread solves the (l, m) column of NF fields that share a diffusivity
-// (u_tor + u_pol, B_tor + B_pol, or T), so the per-l LU factors are loaded
-// once for both.  The linear operator L_l = nu lap - nu l(l+1)/r^2 is rebuilt
-// from the shared Laplacian band with the same roundings as the set-up kernel.
-template <int KL, int NF>
-__device__ __forceinline__ void cnab2_columns(const Dims& d, int j, int l, const double* __restrict__ lu,
-                                              const double* __restrict__ sband /* nu lap, smem */,
-                                              const double* __restrict__ srinv2, double nu, const Cnab2Args& a,
-                                              const int* slots) {
+// One thread solves the (l, m) column of one field.  Three sweeps over r, each
+// with loads that do not depend on the running recurrence so the unrolled
+// loops keep many loads in flight:
+//   1. rhs = u/dt + 1.5 N - 0.5 N_prev + (1 - theta) L_l u  (written over u),
+//      history roll N_prev := N;
+//   2. forward substitution with the unit lower factor (y over u);
+//   3. back substitution with the upper factor (x over u).
+// L_l = nu lap - nu l(l+1)/r^2 is rebuilt from the block's shared Laplacian
+// band with the same roundings as the set-up kernel.
+template <int KL>
+__device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const double* __restrict__ LU,
+                                             const double* __restrict__ sband, const double* __restrict__ srinv2,
+                                             double nu, const Cnab2Args& a, int slot) {
   const int N = d.nr;
   const size_t NM = d.nlm, plane = (size_t)N * NM;
   const size_t Lp1 = (size_t)d.L + 1;
   constexpr int NB = 2 * KL + 1;
   const double nulf = __dmul_rn(nu, (double)l * (l + 1));
-  double* __restrict__ ure[NF];
-  double* __restrict__ uim[NF];
-  const double* __restrict__ nre[NF];
-  const double* __restrict__ nim[NF];
-  double* __restrict__ pre[NF];
-  double* __restrict__ pim[NF];
-#pragma unroll
-  for (int f = 0; f < NF; ++f) {
-    ure[f] = a.u[slots[f]]; uim[f] = ure[f] + plane;
-    nre[f] = a.nl[slots[f]]; nim[f] = nre[f] + plane;
-    pre[f] = a.prev[slots[f]]; pim[f] = pre[f] + plane;
-  }
-  const double* LU = lu + l;  // kind offset applied by the caller
-  double wr[NF][NB], wi[NF][NB];
-#pragma unroll
-  for (int f = 0; f < NF; ++f)
-#pragma unroll
-    for (int t = 0; t < NB; ++t) {
-      const int idx = t - KL;
-      wr[f][t] = (idx >= 0 && idx < N) ? ure[f][(size_t)idx * NM + j] : 0.0;
-      wi[f][t] = (idx >= 0 && idx < N) ? uim[f][(size_t)idx * NM + j] : 0.0;
-    }
-  double yr[NF][KL], yi[NF][KL];
-#pragma unroll
-  for (int f = 0; f < NF; ++f)
-#pragma unroll
-    for (int t = 0; t < KL; ++t) yr[f][t] = yi[f][t] = 0.0;
+  double* __restrict__ ure = a.u[slot] + j;
+  double* __restrict__ uim = a.u[slot] + plane + j;
+  const double* __restrict__ nre = a.nl[slot] + j;
+  const double* __restrict__ nim = a.nl[slot] + plane + j;
+  double* __restrict__ pre = a.prev[slot] + j;
+  double* __restrict__ pim = a.prev[slot] + plane + j;
+  const double* __restrict__ F = LU + l;
+  const bool boot = a.boot != 0;
+  const bool rows = a.bc_rows != 0;
+  const bool is_temp = slot == a.temp_slot;
 
-#pragma unroll 4
-  for (int i = 0; i < N; ++i) {
-    const size_t at = (size_t)i * NM + j;
-    double cfl[NB];
+  // sweep 1: right-hand side, rows in batches of RB whose loads are issued first
+  constexpr int RB = 8;
+  double wr[NB], wi[NB];
 #pragma unroll
-    for (int t = 0; t < NB; ++t) {
-      const int col = i - KL + t;
-      double cf = 0.0;
-      if (col >= 0 && col < N) {
-        cf = sband[col * NB + (KL + i - col)];
-        if (t == KL) cf = __dsub_rn(cf, __dmul_rn(nulf, srinv2[i]));
+  for (int t = 0; t < NB; ++t) {
+    const int idx = t - KL;
+    wr[t] = (idx >= 0 && idx < N) ? ure[(size_t)idx * NM] : 0.0;
+    wi[t] = (idx >= 0 && idx < N) ? uim[(size_t)idx * NM] : 0.0;
+  }
+  for (int i0 = 0; i0 < N; i0 += RB) {
+    double unr[RB], uni[RB], nr_[RB], ni_[RB], pr_[RB], pi_[RB];
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const int i = i0 + b, nxt = i + KL + 1;
+      unr[b] = (nxt < N) ? ure[(size_t)nxt * NM] : 0.0;
+      uni[b] = (nxt < N) ? uim[(size_t)nxt * NM] : 0.0;
+      if (i < N) {
+        nr_[b] = nre[(size_t)i * NM];
+        ni_[b] = nim[(size_t)i * NM];
+        pr_[b] = boot ? nr_[b] : pre[(size_t)i * NM];
+        pi_[b] = boot ? ni_[b] : pim[(size_t)i * NM];
+      } else {
+        nr_[b] = ni_[b] = pr_[b] = pi_[b] = 0.0;
       }
-      cfl[t] = cf;
-    }
-    double lfac[KL];
-#pragma unroll
-    for (int t = 0; t < KL; ++t) {
-      const int col = i - KL + t;
-      lfac[t] = (col >= 0) ? LU[((size_t)col * NB + (KL + i - col)) * Lp1] : 0.0;
     }
 #pragma unroll
-    for (int f = 0; f < NF; ++f) {
+    for (int b = 0; b < RB; ++b) {
+      const int i = i0 + b;
+      if (i >= N) break;
+      const size_t at = (size_t)i * NM;
       double Lr = 0.0, Li = 0.0;
 #pragma unroll
       for (int t = 0; t < NB; ++t) {
         const int col = i - KL + t;
         if (col >= 0 && col < N) {
-          Lr += cfl[t] * wr[f][t];
-          Li += cfl[t] * wi[f][t];
+          double cf = sband[col * NB + (KL + i - col)];
+          if (t == KL) cf = __dsub_rn(cf, __dmul_rn(nulf, srinv2[i]));
+          Lr += cf * wr[t];
+          Li += cf * wi[t];
         }
       }
-      const double n_r = nre[f][at], n_i = nim[f][at];
-      double p_r, p_i;
-      if (a.boot) { p_r = n_r; p_i = n_i; } else { p_r = pre[f][at]; p_i = pim[f][at]; }
-      double vr = a.inv_dt * wr[f][KL] + 1.5 * n_r - 0.5 * p_r;
-      double vi = a.inv_dt * wi[f][KL] + 1.5 * n_i - 0.5 * p_i;
+      double vr = a.inv_dt * wr[KL] + 1.5 * nr_[b] - 0.5 * pr_[b];
+      double vi = a.inv_dt * wi[KL] + 1.5 * ni_[b] - 0.5 * pi_[b];
       vr += a.lin_weight * Lr;
       vi += a.lin_weight * Li;
-      if (a.bc_rows && (i == 0 || i == N - 1)) {
-        vr = (slots[f] == a.temp_slot) ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
+      if (rows && (i == 0 || i == N - 1)) {
+        vr = is_temp ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
         vi = 0.0;
       }
-      pre[f][at] = n_r;
-      pim[f][at] = n_i;
-      double sr = 0.0, si = 0.0;
+      pre[at] = nr_[b];
+      pim[at] = ni_[b];
+      ure[at] = vr;
+      uim[at] = vi;
+#pragma unroll
+      for (int t = 0; t < NB - 1; ++t) { wr[t] = wr[t + 1]; wi[t] = wi[t + 1]; }
+      wr[NB - 1] = unr[b];
+      wi[NB - 1] = uni[b];
+    }
+  }
+  // sweep 2: forward substitution (unit lower factor), y[i - KL + t] in yr[t]
+  double yr[KL], yi[KL];
+#pragma unroll
+  for (int t = 0; t < KL; ++t) yr[t] = yi[t] = 0.0;
+  for (int i0 = 0; i0 < N; i0 += RB) {
+    double br[RB], bi[RB], lf[RB][KL];
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const int i = i0 + b;
+      br[b] = (i < N) ? ure[(size_t)i * NM] : 0.0;
+      bi[b] = (i < N) ? uim[(size_t)i * NM] : 0.0;
 #pragma unroll
       for (int t = 0; t < KL; ++t) {
         const int col = i - KL + t;
-        if (col >= 0) {
-          sr += lfac[t] * yr[f][t];
-          si += lfac[t] * yi[f][t];
-        }
+        lf[b][t] = (i < N && col >= 0) ? F[((size_t)col * NB + (KL + i - col)) * Lp1] : 0.0;
       }
-      const double y_r = vr - sr, y_i = vi - si;
-      ure[f][at] = y_r;
-      uim[f][at] = y_i;
-#pragma unroll
-      for (int t = 0; t < KL - 1; ++t) { yr[f][t] = yr[f][t + 1]; yi[f][t] = yi[f][t + 1]; }
-      yr[f][KL - 1] = y_r;
-      yi[f][KL - 1] = y_i;
-#pragma unroll
-      for (int t = 0; t < NB - 1; ++t) { wr[f][t] = wr[f][t + 1]; wi[f][t] = wi[f][t + 1]; }
-      const int nxt = i + KL + 1;
-      wr[f][NB - 1] = (nxt < N) ? ure[f][(size_t)nxt * NM + j] : 0.0;
-      wi[f][NB - 1] = (nxt < N) ? uim[f][(size_t)nxt * NM + j] : 0.0;
     }
-  }
-  double xr[NF][KL], xi[NF][KL];
 #pragma unroll
-  for (int f = 0; f < NF; ++f)
-#pragma unroll
-    for (int t = 0; t < KL; ++t) xr[f][t] = xi[f][t] = 0.0;
-#pragma unroll 4
-  for (int i = N - 1; i >= 0; --i) {
-    const size_t at = (size_t)i * NM + j;
-    double ufac[KL];
-#pragma unroll
-    for (int t = 0; t < KL; ++t) {
-      const int col = i + 1 + t;
-      ufac[t] = (col < N) ? LU[((size_t)col * NB + (KL + i - col)) * Lp1] : 0.0;
-    }
-    const double dg = LU[((size_t)i * NB + KL) * Lp1];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
+    for (int b = 0; b < RB; ++b) {
+      const int i = i0 + b;
+      if (i >= N) break;
       double sr = 0.0, si = 0.0;
 #pragma unroll
       for (int t = 0; t < KL; ++t) {
-        const int col = i + 1 + t;
-        if (col < N) {
-          sr += ufac[t] * xr[f][t];
-          si += ufac[t] * xi[f][t];
+        if (i - KL + t >= 0) {
+          sr += lf[b][t] * yr[t];
+          si += lf[b][t] * yi[t];
         }
       }
-      double x_r = (ure[f][at] - sr) / dg;
-      double x_i = (uim[f][at] - si) / dg;
-      if (a.clamp_rows && (i == 0 || i == N - 1)) { x_r = 0.0; x_i = 0.0; }
-      ure[f][at] = x_r;
-      uim[f][at] = x_i;
+      const double y_r = br[b] - sr, y_i = bi[b] - si;
+      ure[(size_t)i * NM] = y_r;
+      uim[(size_t)i * NM] = y_i;
 #pragma unroll
-      for (int t = KL - 1; t > 0; --t) { xr[f][t] = xr[f][t - 1]; xi[f][t] = xi[f][t - 1]; }
-      xr[f][0] = x_r;
-      xi[f][0] = x_i;
+      for (int t = 0; t < KL - 1; ++t) { yr[t] = yr[t + 1]; yi[t] = yi[t + 1]; }
+      yr[KL - 1] = y_r;
+      yi[KL - 1] = y_i;
+    }
+  }
+  // sweep 3: back substitution, x[i + 1 + t] in xr[t]
+  double xr[KL], xi[KL];
+#pragma unroll
+  for (int t = 0; t < KL; ++t) xr[t] = xi[t] = 0.0;
+  for (int i0 = N - 1; i0 >= 0; i0 -= RB) {
+    double yv[RB], yw[RB], uf[RB][KL], dg[RB];
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const int i = i0 - b;
+      yv[b] = (i >= 0) ? ure[(size_t)i * NM] : 0.0;
+      yw[b] = (i >= 0) ? uim[(size_t)i * NM] : 0.0;
+      dg[b] = (i >= 0) ? F[((size_t)i * NB + KL) * Lp1] : 1.0;
+#pragma unroll
+      for (int t = 0; t < KL; ++t) {
+        const int col = i + 1 + t;
+        uf[b][t] = (i >= 0 && col < N) ? F[((size_t)col * NB + (KL + i - col)) * Lp1] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const int i = i0 - b;
+      if (i < 0) break;
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int t = 0; t < KL; ++t) {
+        if (i + 1 + t < N) {
+          sr += uf[b][t] * xr[t];
+          si += uf[b][t] * xi[t];
+        }
+      }
+      double x_r = (yv[b] - sr) / dg[b];
+      double x_i = (yw[b] - si) / dg[b];
+      if (a.clamp_rows && (i == 0 || i == N - 1)) { x_r = 0.0; x_i = 0.0; }
+      ure[(size_t)i * NM] = x_r;
+      uim[(size_t)i * NM] = x_i;
+#pragma unroll
+      for (int t = KL - 1; t > 0; --t) { xr[t] = xr[t - 1]; xi[t] = xi[t - 1]; }
+      xr[0] = x_r;
+      xi[0] = x_i;
     }
   }
 }
@@ -174,7 +195,6 @@ __global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ l
   const int slot = blockIdx.y;
   if (slot >= a.nfield) return;
   const int g = a.kind[slot];
-  const int slots[1] = {slot};
   const double nuk = nu[g];
   const int N = d.nr;
   for (int e = threadIdx.x; e < N * NB; e += blockDim.x) {
@@ -193,7 +213,7 @@ __global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ l
   if (j >= d.nlm) return;
   const int l = lof[j];
   const double* LUk = lu + (size_t)g * N * NB * ((size_t)d.L + 1);
-  cnab2_columns<KL, 1>(d, j, l, LUk, sband, srinv2, nuk, a, slots);
+  cnab2_column<KL>(d, j, l, LUk, sband, srinv2, nuk, a, slot);
 }
 
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
