@@ -193,6 +193,23 @@ def test_ab_mode_literal_bootstrap_every_step(gdb, oracle_mod):
         assert rel(g.get_field(k)[0], o.get_field(k)[0]) < 1e-11, k
 
 
+@pytest.mark.parametrize("bc_mode", [1, 2])
+def test_boundary_modes_match_oracle(gdb, oracle_mod, bc_mode):
+    # 1: clamp the boundary rows after the solve; 2: Dirichlet rows inside the operator
+    g, o = make_pair(gdb, oracle_mod, 15, 24, 48, 12, bc_mode=bc_mode)
+    load_state(g, o, workloads.seeded_state(15, 15, 12, seed=2))
+    bv = np.stack([np.linspace(0.1, 0.3, g.nlm), np.linspace(-0.2, 0.05, g.nlm)])
+    src = np.linspace(0.0, 1e-3, 12)
+    g.set_temperature_bc(bv, src); o.set_temperature_bc(bv, src)
+    g.step(4); o.step(4)
+    for k in NAMES:
+        a, b = g.get_field(k), o.get_field(k)
+        assert rel(a[0], b[0]) < 1e-11 and rel(a[1], b[1]) < 1e-11, k
+    if bc_mode == 2:
+        re = g.get_field("u_tor")[0]
+        assert np.max(np.abs(re[0])) == 0.0 and np.max(np.abs(re[-1])) == 0.0
+
+
 def test_errors_are_status_codes(gdb):
     g = gdb.SHTnsKitConfig(7, 12, 24, 9)
     with pytest.raises(gdb.GeoDynamoError) as e:
