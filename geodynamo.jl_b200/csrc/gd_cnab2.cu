@@ -169,11 +169,13 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
           si += uf[b][t] * xi[t];
         }
       }
-      double x_r = (yv[b] - sr) / dg[b];
-      double x_i = (yw[b] - si) / dg[b];
-      if (a.clamp_rows && (i == 0 || i == N - 1)) { x_r = 0.0; x_i = 0.0; }
-      ure[(size_t)i * NM] = x_r;
-      uim[(size_t)i * NM] = x_i;
+      const double x_r = (yv[b] - sr) / dg[b];
+      const double x_i = (yw[b] - si) / dg[b];
+      // bc_mode 1 zeroes the boundary rows after the whole solve: the
+      // substitution itself continues with the solved values
+      const bool clamp = a.clamp_rows && (i == 0 || i == N - 1);
+      ure[(size_t)i * NM] = clamp ? 0.0 : x_r;
+      uim[(size_t)i * NM] = clamp ? 0.0 : x_i;
 #pragma unroll
       for (int t = KL - 1; t > 0; --t) { xr[t] = xr[t - 1]; xi[t] = xi[t - 1]; }
       xr[0] = x_r;

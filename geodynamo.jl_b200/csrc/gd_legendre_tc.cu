@@ -226,6 +226,10 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
   float* stg = reinterpret_cast<float*>(base);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + (size_t)S * ST_FL * 4);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + S);
+  // scalar: column -> coefficient row (null past the last column); column
+  // pair -> Fourier output base (-1 past the last column)
+  const double** colp = reinterpret_cast<const double**>(bars + S + 2);
+  long long* colo = reinterpret_cast<long long*>(colp + NCS);
 
   const int m = blockIdx.z, tile = blockIdx.y;
   const int L = d.L, mb = moff[m];
@@ -238,6 +242,25 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
   if (tid == 0)
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
   if (warp == 0) tmem_alloc(tslot, NCOL);
+  if (!VEC) {
+    for (int c = tid; c < NCS; c += blockDim.x) {
+      const int ng = n0 + c;
+      const double* src = nullptr;
+      if (ng < Ntot) {
+        const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, ci = rem & 1;
+        src = a.coef[f] + ((size_t)ci * d.nr + r) * NM + mb - m;
+      }
+      colp[c] = src;
+      if ((c & 1) == 0) {
+        long long ob = -1;
+        if (ng < Ntot) {
+          const int f = ng / (2 * d.nr), r = (ng % (2 * d.nr)) >> 1;
+          ob = (long long)((((size_t)(f * d.nr + r) * (d.M + 1) + m) * 2) * d.nth);
+        }
+        colo[c >> 1] = ob;
+      }
+    }
+  }
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
@@ -266,11 +289,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
         const int fld = row >> 6, r = r0 + ((row & 63) >> 1), c = row & 1;
         if (r < d.nr) src = a.coef[fld] + ((size_t)c * d.nr + r) * NM + mb - m;
       } else {
-        const int ng = n0 + row;
-        if (ng < Ntot) {
-          const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, c = rem & 1;
-          src = a.coef[f] + ((size_t)c * d.nr + r) * NM + mb - m;
-        }
+        src = colp[row];
       }
       v[i] = (src != nullptr && l <= L) ? __ldg(src + l) : 0.0;
     }
@@ -329,10 +348,9 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
         if (ith < d.nth) {
 #pragma unroll
           for (int j = 0; j < 8; j += 2) {
-            const int ng = n0 + c0 + j;
-            if (ng >= Ntot) continue;
-            const int f = ng / (2 * d.nr), r = (ng % (2 * d.nr)) >> 1;
-            const size_t ob = (((size_t)(f * d.nr + r) * (d.M + 1) + m) * 2) * d.nth + ith;
+            const long long obase = colo[(c0 + j) >> 1];
+            if (obase < 0) continue;
+            const size_t ob = (size_t)obase + ith;
             a.out[ob] = make_float2(e[j] + o[j], e[j + 1] + o[j + 1]);
             a.out[ob + d.nth] = make_float2(e[j] - o[j], e[j + 1] - o[j + 1]);
           }
@@ -415,6 +433,10 @@ __global__ void __launch_bounds__(256, 1) k_tc_analysis3(Dims d, const int* __re
   float* stg = reinterpret_cast<float*>(base);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + (size_t)S * ST_FL * 4);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + S);
+  // scalar: column pair -> folded-input base (-1 past the last column);
+  // column -> output row (null past the last column)
+  long long* colin = reinterpret_cast<long long*>(bars + S + 2);
+  double** colout = reinterpret_cast<double**>(colin + NC / 2);
 
   const int m = blockIdx.z;
   const int L = d.L, mb = moff[m];
@@ -427,6 +449,26 @@ __global__ void __launch_bounds__(256, 1) k_tc_analysis3(Dims d, const int* __re
   if (tid == 0)
     for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
   if (warp == 0) tmem_alloc(tslot, NCOL);
+  if (!VEC) {
+    for (int c = tid; c < NC; c += blockDim.x) {
+      const int ng = n0 + c;
+      double* dst = nullptr;
+      if (ng < Ntot) {
+        const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, ci = rem & 1;
+        dst = a.out[f] + ((size_t)ci * d.nr + r) * NM + mb - m;
+      }
+      colout[c] = dst;
+      if ((c & 1) == 0) {
+        const int pg = ng >> 1;
+        long long ib = -1;
+        if (pg < Ntot / 2) {
+          const int f = pg / d.nr, r = pg % d.nr;
+          ib = (long long)((((size_t)(f * d.nr + r) * (d.M + 1) + m) * 2) * d.nth);
+        }
+        colin[c >> 1] = ib;
+      }
+    }
+  }
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
@@ -451,12 +493,9 @@ __global__ void __launch_bounds__(256, 1) k_tc_analysis3(Dims d, const int* __re
 #pragma unroll
       for (int i = 0; i < NC / 16; ++i) {
         const int pr = warp + 8 * i;
-        const int pg = n0 / 2 + pr;
+        const long long ib = colin[pr];
         v[i] = make_float2(0.f, 0.f);
-        if (pg < Ntot / 2 && ith < d.nth) {
-          const int f = pg / d.nr, r = pg % d.nr;
-          v[i] = __ldg(&a.in[(((size_t)(f * d.nr + r) * (d.M + 1) + m) * 2 + p) * d.nth + ith]);
-        }
+        if (ib >= 0 && ith < d.nth) v[i] = __ldg(&a.in[(size_t)ib + (size_t)p * d.nth + ith]);
       }
 #pragma unroll
       for (int i = 0; i < NC / 16; ++i) {
@@ -538,11 +577,11 @@ __global__ void __launch_bounds__(256, 1) k_tc_analysis3(Dims d, const int* __re
           if (i < kp) {
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-              const int ng = n0 + c0 + j;
-              if (ng >= Ntot) continue;
-              const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, c = rem & 1;
-              const double val = (c == 1 && m == 0) ? 0.0 : (double)v[j];
-              a.out[f][((size_t)c * d.nr + r) * NM + mb + (l - m)] = val;
+              double* dst = colout[c0 + j];
+              if (dst == nullptr) continue;
+              // columns alternate (Re, Im); Im of m = 0 is stored as 0
+              const double val = (((c0 + j) & 1) == 1 && m == 0) ? 0.0 : (double)v[j];
+              dst[l] = val;
             }
           }
         }
@@ -592,14 +631,16 @@ template <typename K>
 static void smem_attr(K k, size_t bytes) {
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
+// stages + mbarriers and TMEM slot (16 bytes past the stages) + the scalar
+// kernels' per-column tables (one pointer per column, one offset per pair)
 static size_t synth_smem(bool vec) {
-  const int S = 2, A = (vec ? 2 : 1) * CHUNK_FLOATS, B = 2 * (vec ? TC_N2 : 2 * TC_N2) * TC_K;
-  return 1024 + (size_t)S * (A + B) * 4 + 64;
+  const int S = 2, NCS = vec ? TC_N2 : 2 * TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS, B = 2 * NCS * TC_K;
+  return 1024 + (size_t)S * (A + B) * 4 + 8 * (S + 2) + (size_t)NCS * 8 + (size_t)(NCS / 2) * 8;
 }
 static size_t analysis_smem(bool vec) {
   const int S = vec ? 2 : 3, NC = vec ? TC_N : TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS;
   const int B = (vec ? 2 : 1) * 2 * NC * TC_K;
-  return 1024 + (size_t)S * (A + B) * 4 + 64;
+  return 1024 + (size_t)S * (A + B) * 4 + 8 * (S + 2) + (size_t)NC * 8 + (size_t)(NC / 2) * 8;
 }
 static bool g_attr_done = false;
 static void set_attrs() {

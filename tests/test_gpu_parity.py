@@ -210,6 +210,20 @@ def test_boundary_modes_match_oracle(gdb, oracle_mod, bc_mode):
         assert np.max(np.abs(re[0])) == 0.0 and np.max(np.abs(re[-1])) == 0.0
 
 
+def test_literal_temperature_growth_matches_oracle(gdb, oracle_mod):
+    # bc_mode 0 (the operator as written) amplifies the temperature by a factor
+    # of several hundred per step at nr = 129, dt = 2e-6; the device follows it
+    g, o = make_pair(gdb, oracle_mod, 7, 12, 24, 129, dt=2e-6)
+    load_state(g, o, workloads.seeded_state(7, 7, 129, seed=0))
+    t0 = np.max(np.abs(o.get_field("temp")[0]))
+    g.step(4); o.step(4)
+    a, b = g.get_field("temp"), o.get_field("temp")
+    assert np.max(np.abs(b[0])) > 1e6 * t0
+    assert rel(a[0], b[0]) < 1e-10 and rel(a[1], b[1]) < 1e-10
+    for k in NAMES[:4]:
+        assert rel(g.get_field(k)[0], o.get_field(k)[0]) < 1e-10, k
+
+
 def test_errors_are_status_codes(gdb):
     g = gdb.SHTnsKitConfig(7, 12, 24, 9)
     with pytest.raises(gdb.GeoDynamoError) as e:

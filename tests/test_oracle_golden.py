@@ -134,3 +134,24 @@ def test_energy_formula(orc6, sht):
     ek_ref = 0.5 * np.sum(w[None, :] * (sht["re"] ** 2 + sht["im"] ** 2))
     assert abs(em - em_ref) / em_ref < 1e-14
     assert abs(ek - ek_ref) / ek_ref < 1e-14
+
+
+def test_literal_operator_amplifies_temperature(oracle_mod):
+    # The implicit operator as written has no boundary rows (timestep.jl:519-539)
+    # while the temperature's boundary rows are overwritten before each solve
+    # (thermal.jl:262-303): at nr = 129, dt = 2e-6 the temperature then grows by
+    # a factor of several hundred per step.  With Dirichlet rows in the
+    # operator (bc_mode 2) it decays.
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(GOLD), "..", "geodynamo.jl_b200"))
+    import workloads
+    growth = {}
+    for bc in (0, 2):
+        o = oracle_mod.Oracle(lmax=7, nlat=12, nlon=24, nr=129, dt=2e-6, bc_mode=bc)
+        for k, (a, b) in workloads.seeded_state(7, 7, 129, seed=0).items():
+            o.set_field(k, a, b)
+        t0 = np.abs(o.get_field("temp")[0]).max()
+        o.step(4)
+        growth[bc] = np.abs(o.get_field("temp")[0]).max() / t0
+    assert growth[0] > 1e6
+    assert growth[2] < 1.0
