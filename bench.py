@@ -81,6 +81,10 @@ def kernel_work(name, p, nlm, precision):
     if name.startswith("fft_synth"):
         return None  # component count varies per launch (4 or 2); handled by caller
     table = {
+        # fused phase kernels: blocked Fourier components in, folded transforms out
+        "fused_temperature": 6 * F * cb + G * rb + F * cb,
+        "fused_velocity": 8 * F * cb + 2 * F * cb,
+        "fused_induction": 4 * F * cb + 2 * F * cb,
         "nl_temperature": 6 * G * rb,
         "nl_velocity": 10 * G * rb,
         "nl_induction": 6 * G * rb,

@@ -471,7 +471,8 @@ int gd_download_grid(gd_handle* h, int grid, double* out) {
   if (s) return s;
   const double* src = h->grid(grid);
   if (h->precision == GD_PREC_MIXED) {
-    mixed_grid_to_double(h, grid, h->d_stage_grid2);
+    s = mixed_grid_to_double(h, grid, h->d_stage_grid2);
+    if (s) return s;
     src = h->d_stage_grid2;
   }
   launch_grid_to_reference(h->stream, h->d, src, h->d_stage_grid, 1);

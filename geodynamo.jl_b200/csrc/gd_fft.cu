@@ -12,177 +12,10 @@
 // G_+ = w (G_N + G_S), G_- = w (G_N - G_S) with G = (2 pi / nlon) sum_j f e^{-i m phi_j}.
 #include <cmath>
 
+#include "gd_fft_core.cuh"
 #include "gd_internal.cuh"
 
 namespace gd {
-
-template <typename R> struct C2;
-template <> struct C2<double> { typedef double2 T; };
-template <> struct C2<float> { typedef float2 T; };
-
-template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
-  C r;
-  r.x = a.x * b.x - a.y * b.y;
-  r.y = a.x * b.y + a.y * b.x;
-  return r;
-}
-template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
-template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
-
-static const int kThreads = 256;
-
-// Forward DFT of R points in registers, natural order in and out.
-template <typename C> __device__ __forceinline__ C mul_mi(C a) { C r; r.x = a.y; r.y = -a.x; return r; }  // -i a
-
-template <int R, typename C> struct Dft;
-
-template <typename C> struct Dft<2, C> {
-  static __device__ __forceinline__ void run(C* v) {
-    const C a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
-  }
-};
-template <typename C> struct Dft<4, C> {
-  static __device__ __forceinline__ void run(C* v) {
-    const C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]), t2 = cadd(v[1], v[3]);
-    const C t3 = mul_mi(csub(v[1], v[3]));
-    v[0] = cadd(t0, t2);
-    v[2] = csub(t0, t2);
-    v[1] = cadd(t1, t3);
-    v[3] = csub(t1, t3);
-  }
-};
-template <typename C> struct Dft<3, C> {
-  static __device__ __forceinline__ void run(C* v) {
-    typedef decltype(v[0].x) S;
-    const S h = (S)0.86602540378443864676;
-    const C a0 = v[0], s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-    C m; m.x = a0.x - (S)0.5 * s.x; m.y = a0.y - (S)0.5 * s.y;
-    v[0] = cadd(a0, s);
-    v[1].x = m.x + h * d.y; v[1].y = m.y - h * d.x;
-    v[2].x = m.x - h * d.y; v[2].y = m.y + h * d.x;
-  }
-};
-template <typename C> struct Dft<5, C> {
-  static __device__ __forceinline__ void run(C* v) {
-    typedef decltype(v[0].x) S;
-    const S c1 = (S)0.30901699437494742410, c2 = (S)-0.80901699437494742410;
-    const S s1 = (S)0.95105651629515357212, s2 = (S)0.58778525229247312917;
-    const C a0 = v[0];
-    const C p1 = cadd(v[1], v[4]), m1 = csub(v[1], v[4]);
-    const C p2 = cadd(v[2], v[3]), m2 = csub(v[2], v[3]);
-    v[0].x = a0.x + p1.x + p2.x; v[0].y = a0.y + p1.y + p2.y;
-    C r1, r2, i1, i2;
-    r1.x = a0.x + c1 * p1.x + c2 * p2.x; r1.y = a0.y + c1 * p1.y + c2 * p2.y;
-    r2.x = a0.x + c2 * p1.x + c1 * p2.x; r2.y = a0.y + c2 * p1.y + c1 * p2.y;
-    i1.x = s1 * m1.y + s2 * m2.y; i1.y = -(s1 * m1.x + s2 * m2.x);
-    i2.x = s2 * m1.y - s1 * m2.y; i2.y = -(s2 * m1.x - s1 * m2.x);
-    v[1] = cadd(r1, i1); v[4] = csub(r1, i1);
-    v[2] = cadd(r2, i2); v[3] = csub(r2, i2);
-  }
-};
-// Radix 8 and 16 by one decimation-in-frequency split into two half-size DFTs:
-//   u_n = x_n + x_{n+R/2},  v_n = (x_n - x_{n+R/2}) W_R^n,
-//   X_{2k} = DFT(u)_k,  X_{2k+1} = DFT(v)_k.
-template <typename C> struct Dft<8, C> {
-  static __device__ __forceinline__ void run(C* x) {
-    typedef decltype(x[0].x) S;
-    const S c = (S)0.70710678118654752440;
-    C u[4], w[4];
-#pragma unroll
-    for (int n = 0; n < 4; ++n) { u[n] = cadd(x[n], x[n + 4]); w[n] = csub(x[n], x[n + 4]); }
-    // W8^1 = c (1 - i), W8^2 = -i, W8^3 = -c (1 + i)
-    { C t = w[1]; w[1].x = c * (t.x + t.y); w[1].y = c * (t.y - t.x); }
-    w[2] = mul_mi(w[2]);
-    { C t = w[3]; w[3].x = c * (t.y - t.x); w[3].y = -c * (t.x + t.y); }
-    Dft<4, C>::run(u);
-    Dft<4, C>::run(w);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) { x[2 * k] = u[k]; x[2 * k + 1] = w[k]; }
-  }
-};
-template <typename C> struct Dft<16, C> {
-  static __device__ __forceinline__ void run(C* x) {
-    typedef decltype(x[0].x) S;
-    // W16^n = cos(pi n / 8) - i sin(pi n / 8), n = 0..7
-    const S cs[8] = {(S)1.0, (S)0.92387953251128675613, (S)0.70710678118654752440, (S)0.38268343236508977173,
-                     (S)0.0, (S)-0.38268343236508977173, (S)-0.70710678118654752440, (S)-0.92387953251128675613};
-    const S sn[8] = {(S)0.0, (S)0.38268343236508977173, (S)0.70710678118654752440, (S)0.92387953251128675613,
-                     (S)1.0, (S)0.92387953251128675613, (S)0.70710678118654752440, (S)0.38268343236508977173};
-    C u[8], w[8];
-#pragma unroll
-    for (int n = 0; n < 8; ++n) {
-      u[n] = cadd(x[n], x[n + 8]);
-      const C d = csub(x[n], x[n + 8]);
-      w[n].x = d.x * cs[n] + d.y * sn[n];
-      w[n].y = d.y * cs[n] - d.x * sn[n];
-    }
-    Dft<8, C>::run(u);
-    Dft<8, C>::run(w);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) { x[2 * k] = u[k]; x[2 * k + 1] = w[k]; }
-  }
-};
-
-// Shared-memory rows are padded by one element every 16 so the stride-16
-// stores of the first radix-16 pass do not all fall into one bank.
-// Rows are further padded to an odd number of elements so the transposed
-// (m, row) accesses of the load and store phases spread over the banks.
-__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
-__host__ __device__ __forceinline__ int prow(int n) { return (n + (n >> 4)) | 1; }
-
-// One Stockham pass from src to dst ([tb][n] each): radix R, Ns = product of
-// the radices of the earlier passes.
-template <int R, typename C>
-__device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restrict__ dst, int tb, int n, int Ns,
-                                         const C* __restrict__ tw) {
-  const int nbf = n / R;
-  const int total = tb * nbf;
-  const int twstep = n / (Ns * R);
-  for (int b = threadIdx.x; b < total; b += kThreads) {
-    const int row = b / nbf, j = b - row * nbf;
-    const int k = j % Ns;
-    const C* s = src + (size_t)row * prow(n);
-    C v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = s[pidx(j + r * nbf)];
-    if (k > 0) {
-#pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(&tw[r * k * twstep]));
-    }
-    Dft<R, C>::run(v);
-    C* o = dst + (size_t)row * prow(n);
-    const int o0 = (j / Ns) * Ns * R + k;
-#pragma unroll
-    for (int r = 0; r < R; ++r) o[pidx(o0 + r * Ns)] = v[r];
-  }
-}
-
-// Runs all passes; returns the buffer holding the result.
-template <typename RT>
-__device__ typename C2<RT>::T* fft_forward(typename C2<RT>::T* a, typename C2<RT>::T* b, int tb, const FftPlan& p,
-                                           const typename C2<RT>::T* tw) {
-  typedef typename C2<RT>::T C;
-  int Ns = 1;
-  C* src = a;
-  C* dst = b;
-  for (int s = 0; s < p.nstage; ++s) {
-    const int R = p.radix[s];
-    switch (R) {
-      case 16: fft_pass<16, C>(src, dst, tb, p.n, Ns, tw); break;
-      case 8: fft_pass<8, C>(src, dst, tb, p.n, Ns, tw); break;
-      case 4: fft_pass<4, C>(src, dst, tb, p.n, Ns, tw); break;
-      case 2: fft_pass<2, C>(src, dst, tb, p.n, Ns, tw); break;
-      case 3: fft_pass<3, C>(src, dst, tb, p.n, Ns, tw); break;
-      default: fft_pass<5, C>(src, dst, tb, p.n, Ns, tw); break;
-    }
-    __syncthreads();
-    Ns *= R;
-    C* t = src; src = dst; dst = t;
-  }
-  return src;
-}
 
 template <typename RT>
 __global__ void __launch_bounds__(256) k_fft_synth(Dims d, FftPlan p, const typename C2<RT>::T* __restrict__ tw,
@@ -285,76 +118,6 @@ __global__ void __launch_bounds__(256) k_fft_analysis(Dims d, FftPlan p, const t
     gm.x = wi * (gn.x - gs.x); gm.y = wi * (gn.y - gs.y);
     G[gb + ((size_t)m * 2 + 0) * d.nth + ith] = gp;
     G[gb + ((size_t)m * 2 + 1) * d.nth + ith] = gm;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Compile-time variants for the transform lengths in use: every index
-// division below is by a constant (the runtime-plan kernels above spend most
-// of their instructions in integer division).
-// ---------------------------------------------------------------------------
-struct CPlan {
-  int n, ns;
-  int r[12];
-};
-constexpr CPlan make_cplan(int n) {
-  CPlan p{n, 0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
-  int m = n, a = 0;
-  while (m % 2 == 0) { m /= 2; ++a; }
-  int rest = a;
-  if (rest >= 5 && rest % 4 == 1) { p.r[p.ns++] = 8; p.r[p.ns++] = 4; rest -= 5; }
-  while (rest >= 4) { p.r[p.ns++] = 16; rest -= 4; }
-  if (rest == 3) p.r[p.ns++] = 8;
-  if (rest == 2) p.r[p.ns++] = 4;
-  if (rest == 1) p.r[p.ns++] = 2;
-  while (m % 3 == 0) { p.r[p.ns++] = 3; m /= 3; }
-  while (m % 5 == 0) { p.r[p.ns++] = 5; m /= 5; }
-  return p;
-}
-template <int N> struct PlanOf { static constexpr CPlan p = make_cplan(N); };
-
-template <typename RT, int N> struct CtGeom {
-  typedef typename C2<RT>::T C;
-  static constexpr int RS = (N + (N >> 4)) | 1;  // padded row stride (elements)
-  static constexpr int TB0 = (int)((56 * 1024) / (2 * (size_t)RS * sizeof(C)));
-  static constexpr int TB = TB0 > 16 ? 16 : (TB0 < 1 ? 1 : TB0);
-};
-
-template <int R, int N, int TB, int NS, typename C>
-__device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw) {
-  constexpr int RS = (N + (N >> 4)) | 1;
-  constexpr int NBF = N / R;
-  constexpr int TOTAL = TB * NBF;
-  constexpr int TWSTEP = N / (NS * R);
-  for (int b = threadIdx.x; b < TOTAL; b += kThreads) {
-    const int row = b / NBF, j = b - row * NBF;
-    const int k = j % NS;
-    const C* s = src + row * RS;
-    C v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = s[pidx(j + r * NBF)];
-    if (NS > 1 && k > 0) {
-#pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(&tw[r * k * TWSTEP]));
-    }
-    Dft<R, C>::run(v);
-    C* o = dst + row * RS;
-    const int o0 = (j / NS) * NS * R + k;
-#pragma unroll
-    for (int r = 0; r < R; ++r) o[pidx(o0 + r * NS)] = v[r];
-  }
-}
-
-template <int N, int TB, int S, int NS, typename C>
-__device__ __forceinline__ C* ct_passes(C* src, C* dst, const C* tw) {
-  constexpr CPlan P = PlanOf<N>::p;
-  if constexpr (S >= P.ns) {
-    return src;
-  } else {
-    constexpr int R = P.r[S];
-    ct_pass<R, N, TB, NS, C>(src, dst, tw);
-    __syncthreads();
-    return ct_passes<N, TB, S + 1, NS * R, C>(dst, src, tw);
   }
 }
 
@@ -571,8 +334,6 @@ void launch_fft_analysis(cudaStream_t s, const Dims& d, const FftPlan& p0, const
 
 template void launch_fft_synth<double>(cudaStream_t, const Dims&, const FftPlan&, const void*, const void*, double*,
                                        int, size_t);
-template void launch_fft_synth<float>(cudaStream_t, const Dims&, const FftPlan&, const void*, const void*, float*,
-                                      int, size_t);
 template void launch_fft_analysis<double>(cudaStream_t, const Dims&, const FftPlan&, const void*, const double*,
                                           size_t, const double*, void*, int);
 template void launch_fft_analysis<float>(cudaStream_t, const Dims&, const FftPlan&, const void*, const float*,

@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
         long long ob = -1;
         if (ng < Ntot) {
           const int f = ng / (2 * d.nr), r = (ng % (2 * d.nr)) >> 1;
-          ob = (long long)((((size_t)(f * d.nr + r) * (d.M + 1) + m) * 2) * d.nth);
+          ob = (long long)((size_t)(f * d.nr + r) * a.nblk * (d.M + 1) * FOURIER_BLOCK);
         }
         colo[c >> 1] = ob;
       }
@@ -335,6 +335,8 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
     const int q = warp & 3, half = warp >> 2;
     const int ith = tile * TC_M + q * 32 + lane;
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
+    // offset of (theta block, m, pair) within one (comp, r) run of the blocked layout
+    const size_t ioff = ((size_t)(ith / FOURIER_BLOCK) * (d.M + 1) + m) * FOURIER_BLOCK + ith % FOURIER_BLOCK;
     if (!VEC) {
       for (int c0 = (NCS / 2) * half; c0 < (NCS / 2) * (half + 1); c0 += 8) {
         float e[8], o[8];
@@ -350,9 +352,8 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
           for (int j = 0; j < 8; j += 2) {
             const long long obase = colo[(c0 + j) >> 1];
             if (obase < 0) continue;
-            const size_t ob = (size_t)obase + ith;
-            a.out[ob] = make_float2(e[j] + o[j], e[j + 1] + o[j + 1]);
-            a.out[ob + d.nth] = make_float2(e[j] - o[j], e[j + 1] - o[j + 1]);
+            a.out[(size_t)obase + ioff] =
+                make_float4(e[j] + o[j], e[j + 1] + o[j + 1], e[j] - o[j], e[j + 1] - o[j + 1]);
           }
         }
       }
@@ -380,6 +381,7 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
           for (int j = 0; j < 8; j += 2) {
             const int r = r0 + (jj + j) / 2;
             if (r >= d.nr) continue;
+            float vt[4], vp[4];  // (north Re, north Im, south Re, south Im)
 #pragma unroll
             for (int sN = 0; sN < 2; ++sN) {
               float PS[2], PT[2], DS[2], DT[2];
@@ -394,11 +396,12 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
                 }
               }
               const float QS0 = ms * PS[0], QS1 = ms * PS[1], QT0 = ms * PT[0], QT1 = ms * PT[1];
-              const size_t b0 = (((size_t)(0 * d.nr + r) * (d.M + 1) + m) * 2 + sN) * d.nth + ith;
-              const size_t b1 = (((size_t)(1 * d.nr + r) * (d.M + 1) + m) * 2 + sN) * d.nth + ith;
-              a.out[b0] = make_float2(DS[0] - QT1, DS[1] + QT0);
-              a.out[b1] = make_float2(-QS1 - DT[0], QS0 - DT[1]);
+              vt[2 * sN] = DS[0] - QT1; vt[2 * sN + 1] = DS[1] + QT0;
+              vp[2 * sN] = -QS1 - DT[0]; vp[2 * sN + 1] = QS0 - DT[1];
             }
+            const size_t run = (size_t)a.nblk * (d.M + 1) * FOURIER_BLOCK;
+            a.out[(size_t)(0 * d.nr + r) * run + ioff] = make_float4(vt[0], vt[1], vt[2], vt[3]);
+            a.out[(size_t)(1 * d.nr + r) * run + ioff] = make_float4(vp[0], vp[1], vp[2], vp[3]);
           }
         }
       }

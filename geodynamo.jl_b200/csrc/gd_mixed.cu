@@ -9,9 +9,19 @@
 #include "gd_handle.cuh"
 #include "gd_internal.cuh"
 #include "gd_mixed.cuh"
+#include "gd_fused.cuh"
 #include "gd_mixed_kernels.cuh"
 
 namespace gd {
+
+// Blocked FP32 Fourier buffers of the synthesized components (the fused
+// phase kernels transform them in shared memory; the physical grids are not
+// kept in HBM, except the temperature grid).
+enum {
+  FC_T = 0, FC_GTH = 1, FC_GPH = 2, FC_GR = 3,  // temperature phase (scalar synthesis order)
+  FC_U = 4, FC_W = 6, FC_B = 8, FC_J = 10,      // theta, phi pairs
+  FC_COUNT = 12
+};
 
 struct MixedState {
   double *ra = nullptr, *rb = nullptr, *rc = nullptr, *r1a = nullptr, *r1b = nullptr, *pmm = nullptr,
@@ -19,13 +29,15 @@ struct MixedState {
   long* d_cofs = nullptr;
   float* img_synth[2] = {nullptr, nullptr};          // Pbar, dPbar/dtheta (synthesis orientation)
   float* img_anal[3] = {nullptr, nullptr, nullptr};  // Pbar, dPbar/dtheta, Q (analysis orientation)
-  float2* d_F = nullptr;       // 4 components
-  float* d_grid = nullptr;     // NGRID FP32 grids
-  float* d_stage = nullptr;    // 4 FP32 grids for the host-array entry points
+  float4* d_Fall = nullptr;    // FC_COUNT blocked components
+  size_t fcomp = 0;            // float4 per component
+  float2* d_G = nullptr;       // folded transforms for the analysis, 2 components
+  float* d_tgrid = nullptr;    // the temperature grid (FP32)
+  float* d_stage = nullptr;    // 4 FP32 grids for the host-array entry points and grid downloads
   int* d_err = nullptr;
   size_t bytes = 0;
   std::vector<void*> allocs;
-  float* grid(const gd_handle* h, int g) const { return d_grid + h->grid_elems() * g; }
+  float4* F(int c) const { return d_Fall + fcomp * c; }
 };
 
 namespace {
@@ -55,36 +67,51 @@ int malloc_m(gd_handle* h, T** p, size_t n) {
 int launched(gd_handle* h, const char* what) { return mcheck(h, cudaGetLastError(), what); }
 
 
-int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float* grid_out) {
+int nblocks(const gd_handle* h) { return fourier_blocks(h->d); }
+
+// Legendre synthesis of nf scalar fields into consecutive blocked components from `out`.
+int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float4* out) {
   MixedState* x = h->mixed;
   TcSynthArgs a{};
   for (int i = 0; i < nf; ++i) a.coef[i] = coef[i];
   a.nf = nf;
-  a.out = x->d_F;
+  a.out = out;
+  a.nblk = nblocks(h);
   a.err = x->d_err;
   { ProfScope p(h, "legendre_synth_scalar_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], nullptr, x->sinv, a, false); }
-  { ProfScope p(h, "fft_synth_fp32"); launch_fft_synth<float>(h->stream, h->d, h->plan, h->d_twf, x->d_F, grid_out, nf, h->grid_elems()); }
   return launched(h, "mixed scalar synthesis");
 }
 
-int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float* grid_out) {
+// Vector synthesis (tor, pol) -> (theta, phi) blocked components at out, out + 1.
+int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float4* out) {
   MixedState* x = h->mixed;
   TcSynthArgs a{};
   a.coef[0] = pol;
   a.coef[1] = tor;
   a.nf = 1;
-  a.out = x->d_F;
+  a.out = out;
+  a.nblk = nblocks(h);
   a.err = x->d_err;
   { ProfScope p(h, "legendre_synth_vector_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], x->img_synth[1], x->sinv, a, true); }
-  { ProfScope p(h, "fft_synth_fp32"); launch_fft_synth<float>(h->stream, h->d, h->plan, h->d_twf, x->d_F, grid_out, 2, h->grid_elems()); }
   return launched(h, "mixed vector synthesis");
 }
 
-int tc_analysis_scalar(gd_handle* h, const float* grid_in, int nf, double* const* out) {
+// Physical grids of ncomp blocked components (grid-only fused kernel).
+int fourier_to_grid(gd_handle* h, const float4* const* fin, int ncomp, float* grid_out) {
+  FusedArgs f{};
+  for (int i = 0; i < ncomp; ++i) {
+    f.fin[i] = fin[i];
+    f.gout[i] = grid_out + h->grid_elems() * i;
+  }
+  f.nin = ncomp;
+  { ProfScope p(h, "fft_synth_fp32"); launch_fused(h->stream, h->d, h->plan, h->d_twf, FUSED_GRID, f); }
+  return launched(h, "fourier to grid");
+}
+
+int tc_analysis_scalar_G(gd_handle* h, int nf, double* const* out) {
   MixedState* x = h->mixed;
-  { ProfScope p(h, "fft_analysis_fp32"); launch_fft_analysis<float>(h->stream, h->d, h->plan, h->d_twf, grid_in, h->grid_elems(), h->d_w, x->d_F, nf); }
   TcAnalysisArgs a{};
-  a.in = x->d_F;
+  a.in = x->d_G;
   for (int i = 0; i < nf; ++i) a.out[i] = out[i];
   a.nf = nf;
   a.epi = EPI_SCALAR;
@@ -93,11 +120,10 @@ int tc_analysis_scalar(gd_handle* h, const float* grid_in, int nf, double* const
   return launched(h, "mixed scalar analysis");
 }
 
-int tc_analysis_vector(gd_handle* h, const float* grid_in, double* out_tor, double* out_pol, int epi) {
+int tc_analysis_vector_G(gd_handle* h, double* out_tor, double* out_pol, int epi) {
   MixedState* x = h->mixed;
-  { ProfScope p(h, "fft_analysis_fp32"); launch_fft_analysis<float>(h->stream, h->d, h->plan, h->d_twf, grid_in, h->grid_elems(), h->d_w, x->d_F, 2); }
   TcAnalysisArgs a{};
-  a.in = x->d_F;
+  a.in = x->d_G;
   a.out[0] = out_tor;
   a.out[1] = out_pol;
   a.nf = 1;
@@ -105,6 +131,31 @@ int tc_analysis_vector(gd_handle* h, const float* grid_in, double* out_tor, doub
   a.err = x->d_err;
   { ProfScope p(h, "legendre_analysis_vector_tc"); launch_tc_analysis(h->stream, h->d, h->d_moff, x->img_anal[1], x->img_anal[2], a); }
   return launched(h, "mixed vector analysis");
+}
+
+// Analysis of FP32 grids (host-array entry points): phi transform into d_G, then Legendre.
+int tc_analysis_scalar(gd_handle* h, const float* grid_in, int nf, double* const* out) {
+  MixedState* x = h->mixed;
+  { ProfScope p(h, "fft_analysis_fp32"); launch_fft_analysis<float>(h->stream, h->d, h->plan, h->d_twf, grid_in, h->grid_elems(), h->d_w, x->d_G, nf); }
+  return tc_analysis_scalar_G(h, nf, out);
+}
+
+int tc_analysis_vector(gd_handle* h, const float* grid_in, double* out_tor, double* out_pol, int epi) {
+  MixedState* x = h->mixed;
+  { ProfScope p(h, "fft_analysis_fp32"); launch_fft_analysis<float>(h->stream, h->d, h->plan, h->d_twf, grid_in, h->grid_elems(), h->d_w, x->d_G, 2); }
+  return tc_analysis_vector_G(h, out_tor, out_pol, epi);
+}
+
+FusedArgs phase_args(gd_handle* h) {
+  FusedArgs f{};
+  f.G = h->mixed->d_G;
+  f.w = h->d_w;
+  f.cth = h->d_cth;
+  f.sthc = h->d_sthc;
+  f.sources = h->d_sources;
+  f.rf = (float)(h->c.magnetic_prandtl / h->c.ekman);
+  f.lf = f.rf;
+  return f;
 }
 
 }  // namespace
@@ -129,8 +180,10 @@ int mixed_create(gd_handle* h) {
   MAL(x->ra, d.nlm); MAL(x->rb, d.nlm); MAL(x->rc, d.nlm);
   MAL(x->r1a, d.L + 1); MAL(x->r1b, d.L + 1);
   MAL(x->pmm, (size_t)(d.M + 1) * d.nth); MAL(x->sinv, d.nth);
-  MAL(x->d_F, (size_t)4 * d.nr * (d.M + 1) * d.nlat);
-  MAL(x->d_grid, (size_t)NGRID * h->grid_elems());
+  x->fcomp = fourier_comp_elems(d);
+  MAL(x->d_Fall, (size_t)FC_COUNT * x->fcomp);
+  MAL(x->d_G, (size_t)2 * d.nr * (d.M + 1) * 2 * d.nth);
+  MAL(x->d_tgrid, h->grid_elems());
   MAL(x->d_stage, (size_t)4 * h->grid_elems());
   MAL(x->d_err, 4);
   int s = mcheck(h, cudaMemcpyAsync(x->d_cofs, cofs.data(), sizeof(long) * cofs.size(), cudaMemcpyHostToDevice,
@@ -148,7 +201,11 @@ int mixed_create(gd_handle* h) {
   s = mcheck(h, cudaStreamSynchronize(h->stream), "cofs lifetime");
   s = launched(h, "table images");
   if (s) return s;
-  s = mcheck(h, cudaMemsetAsync(x->d_grid, 0, sizeof(float) * NGRID * h->grid_elems(), h->stream), "memset");
+  // the carried components start as zero grids (the reference's physical
+  // fields are zero-filled at allocation, src/fields.jl:82)
+  s = mcheck(h, cudaMemsetAsync(x->d_Fall, 0, sizeof(float4) * FC_COUNT * x->fcomp, h->stream), "memset");
+  if (s) return s;
+  s = mcheck(h, cudaMemsetAsync(x->d_tgrid, 0, sizeof(float) * h->grid_elems(), h->stream), "memset");
   if (s) return s;
   s = mcheck(h, cudaMemsetAsync(x->d_err, 0, sizeof(int), h->stream), "memset");
   if (s) return s;
@@ -181,14 +238,19 @@ int mixed_temperature_nl(gd_handle* h) {
   { ProfScope p(h, "spectral_gradients");
     launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), h->work(0), h->work(1), h->work(2)); }
   const double* coef[4] = {h->field(F_TEMP), h->work(0), h->work(1), h->work(2)};
-  int s = tc_synth_scalar(h, coef, 4, x->grid(h, GD_GRID_T));
+  int s = tc_synth_scalar(h, coef, 4, x->F(FC_T));
   if (s) return s;
-  { ProfScope p(h, "nl_temperature_fp32");
-    launch_temperature_advection<float>(h->stream, d, x->grid(h, GD_GRID_U_TH), x->grid(h, GD_GRID_U_PH),
-                                        x->grid(h, GD_GRID_GTH), x->grid(h, GD_GRID_GPH), x->grid(h, GD_GRID_GR),
-                                        h->d_sources, x->grid(h, GD_GRID_TADV)); }
+  // the velocity grid is the previous velocity phase's (carried in F(FC_U))
+  FusedArgs f = phase_args(h);
+  const float4* fin[6] = {x->F(FC_U), x->F(FC_U + 1), x->F(FC_GR), x->F(FC_GTH), x->F(FC_GPH), x->F(FC_T)};
+  for (int i = 0; i < 6; ++i) f.fin[i] = fin[i];
+  f.nin = 6;
+  f.gout[0] = x->d_tgrid;
+  { ProfScope p(h, "fused_temperature_fp32"); launch_fused(h->stream, d, h->plan, h->d_twf, FUSED_TEMPERATURE, f); }
+  s = launched(h, "fused temperature phase");
+  if (s) return s;
   double* out[1] = {h->nlf(F_TEMP)};
-  s = tc_analysis_scalar(h, x->grid(h, GD_GRID_TADV), 1, out);
+  s = tc_analysis_scalar_G(h, 1, out);
   if (s) return s;
   { ProfScope p(h, "temperature_bc"); launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP)); }
   return launched(h, "mixed temperature nonlinear");
@@ -197,52 +259,99 @@ int mixed_temperature_nl(gd_handle* h) {
 int mixed_velocity_nl(gd_handle* h) {
   MixedState* x = h->mixed;
   const Dims& d = h->d;
-  int s = tc_synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), x->grid(h, GD_GRID_U_TH));
+  int s = tc_synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), x->F(FC_U));
   if (s) return s;
   { ProfScope p(h, "spectral_curl");
     launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR), h->field(F_UPOL), h->work(3), h->work(4)); }
-  s = tc_synth_vector(h, h->work(3), h->work(4), x->grid(h, GD_GRID_W_TH));
+  s = tc_synth_vector(h, h->work(3), h->work(4), x->F(FC_W));
   if (s) return s;
-  const double rf = h->c.magnetic_prandtl / h->c.ekman;
-  { ProfScope p(h, "nl_velocity_fp32");
-    launch_velocity_nl<float>(h->stream, d, h->d_cth, h->d_sthc, rf, rf, h->c.magnetic, x->grid(h, GD_GRID_U_TH),
-                              x->grid(h, GD_GRID_U_PH), x->grid(h, GD_GRID_W_TH), x->grid(h, GD_GRID_W_PH),
-                              x->grid(h, GD_GRID_J_TH), x->grid(h, GD_GRID_J_PH), x->grid(h, GD_GRID_B_TH),
-                              x->grid(h, GD_GRID_B_PH), x->grid(h, GD_GRID_VADV_TH), x->grid(h, GD_GRID_VADV_PH)); }
-  return tc_analysis_vector(h, x->grid(h, GD_GRID_VADV_TH), h->nlf(F_UTOR), h->nlf(F_UPOL), EPI_VECTOR);
+  // current density and magnetic field of the previous magnetic phase (F(FC_J), F(FC_B))
+  FusedArgs f = phase_args(h);
+  const float4* fin[8] = {x->F(FC_U), x->F(FC_U + 1), x->F(FC_W), x->F(FC_W + 1),
+                          x->F(FC_J), x->F(FC_J + 1), x->F(FC_B), x->F(FC_B + 1)};
+  for (int i = 0; i < 8; ++i) f.fin[i] = fin[i];
+  f.nin = h->c.magnetic ? 8 : 4;
+  { ProfScope p(h, "fused_velocity_fp32"); launch_fused(h->stream, d, h->plan, h->d_twf, FUSED_VELOCITY, f); }
+  s = launched(h, "fused velocity phase");
+  if (s) return s;
+  return tc_analysis_vector_G(h, h->nlf(F_UTOR), h->nlf(F_UPOL), EPI_VECTOR);
 }
 
 int mixed_magnetic_nl(gd_handle* h) {
   MixedState* x = h->mixed;
   const Dims& d = h->d;
-  int s = tc_synth_vector(h, h->field(F_BTOR), h->field(F_BPOL), x->grid(h, GD_GRID_B_TH));
+  int s = tc_synth_vector(h, h->field(F_BTOR), h->field(F_BPOL), x->F(FC_B));
   if (s) return s;
   { ProfScope p(h, "spectral_curl");
     launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR), h->field(F_BPOL), h->work(5), h->work(6)); }
-  s = tc_synth_vector(h, h->work(5), h->work(6), x->grid(h, GD_GRID_J_TH));
+  s = tc_synth_vector(h, h->work(5), h->work(6), x->F(FC_J));
   if (s) return s;
-  { ProfScope p(h, "nl_induction_fp32");
-    launch_induction<float>(h->stream, d, x->grid(h, GD_GRID_U_TH), x->grid(h, GD_GRID_U_PH), x->grid(h, GD_GRID_B_TH),
-                            x->grid(h, GD_GRID_B_PH), x->grid(h, GD_GRID_IND_TH), x->grid(h, GD_GRID_IND_PH)); }
-  return tc_analysis_vector(h, x->grid(h, GD_GRID_IND_TH), h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
+  FusedArgs f = phase_args(h);
+  const float4* fin[4] = {x->F(FC_U), x->F(FC_U + 1), x->F(FC_B), x->F(FC_B + 1)};
+  for (int i = 0; i < 4; ++i) f.fin[i] = fin[i];
+  f.nin = 4;
+  { ProfScope p(h, "fused_induction_fp32"); launch_fused(h->stream, d, h->plan, h->d_twf, FUSED_INDUCTION, f); }
+  s = launched(h, "fused induction phase");
+  if (s) return s;
+  return tc_analysis_vector_G(h, h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
 }
 
-void mixed_grid_to_double(gd_handle* h, int grid, double* out) {
-  launch_grid_cast<float>(h->stream, h->grid_elems(), h->mixed->grid(h, grid), out);
+// Grid download in the mixed path: synthesized components are transformed
+// from their Fourier buffers on request; the products' grids exist only
+// inside the fused kernels.
+int mixed_grid_to_double(gd_handle* h, int grid, double* out) {
+  MixedState* x = h->mixed;
+  const float* src = nullptr;
+  int fc = -1;
+  switch (grid) {
+    case GD_GRID_U_TH: fc = FC_U; break;
+    case GD_GRID_U_PH: fc = FC_U + 1; break;
+    case GD_GRID_W_TH: fc = FC_W; break;
+    case GD_GRID_W_PH: fc = FC_W + 1; break;
+    case GD_GRID_B_TH: fc = FC_B; break;
+    case GD_GRID_B_PH: fc = FC_B + 1; break;
+    case GD_GRID_J_TH: fc = FC_J; break;
+    case GD_GRID_J_PH: fc = FC_J + 1; break;
+    case GD_GRID_GTH: fc = FC_GTH; break;
+    case GD_GRID_GPH: fc = FC_GPH; break;
+    case GD_GRID_GR: fc = FC_GR; break;
+    case GD_GRID_T: src = x->d_tgrid; break;
+    default:
+      return set_error(h, GD_ERR_UNSUPPORTED,
+                       "the mixed-precision step forms the nonlinear products in shared memory only; download "
+                       "product grids with precision fp64");
+  }
+  if (fc >= 0) {
+    const float4* fin[1] = {x->F(fc)};
+    int s = fourier_to_grid(h, fin, 1, x->d_stage);
+    if (s) return s;
+    src = x->d_stage;
+  }
+  launch_grid_cast<float>(h->stream, h->grid_elems(), src, out);
+  return launched(h, "grid cast");
 }
 
 int mixed_api_synth_scalar(gd_handle* h, const double* const* coef, int nf, double* grid_out) {
-  int s = tc_synth_scalar(h, coef, nf, h->mixed->d_stage);
+  MixedState* x = h->mixed;
+  int s = tc_synth_scalar(h, coef, nf, x->F(FC_T));
   if (s) return s;
-  launch_grid_cast<float>(h->stream, (size_t)nf * h->grid_elems(), h->mixed->d_stage, grid_out);
+  const float4* fin[4] = {x->F(FC_T), x->F(FC_T + 1), x->F(FC_T + 2), x->F(FC_T + 3)};
+  s = fourier_to_grid(h, fin, nf, x->d_stage);
+  if (s) return s;
+  launch_grid_cast<float>(h->stream, (size_t)nf * h->grid_elems(), x->d_stage, grid_out);
   s = launched(h, "cast");
   return s ? s : mixed_check_error(h);
 }
 
+// Uses the vorticity buffers, which no later phase reads.
 int mixed_api_synth_vector(gd_handle* h, const double* tor, const double* pol, double* grid_out) {
-  int s = tc_synth_vector(h, tor, pol, h->mixed->d_stage);
+  MixedState* x = h->mixed;
+  int s = tc_synth_vector(h, tor, pol, x->F(FC_W));
   if (s) return s;
-  launch_grid_cast<float>(h->stream, 2 * h->grid_elems(), h->mixed->d_stage, grid_out);
+  const float4* fin[2] = {x->F(FC_W), x->F(FC_W + 1)};
+  s = fourier_to_grid(h, fin, 2, x->d_stage);
+  if (s) return s;
+  launch_grid_cast<float>(h->stream, 2 * h->grid_elems(), x->d_stage, grid_out);
   s = launched(h, "cast");
   return s ? s : mixed_check_error(h);
 }

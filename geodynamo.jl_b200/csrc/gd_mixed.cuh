@@ -1,7 +1,8 @@
-// gd_mixed.cuh -- mixed-precision path: FP32 grids, phi transforms and
-// nonlinear products; Legendre contractions on the tcgen05 tensor cores in
-// split TF32 (hi*hi + hi*lo + lo*hi, FP32 accumulation in tensor memory);
-// spectral state, radial operators and CNAB2 stay FP64.
+// gd_mixed.cuh -- mixed-precision path: FP32 phi transforms and nonlinear
+// products (fused per phase, grids in shared memory); Legendre contractions
+// on the tcgen05 tensor cores in split TF32 (hi*hi + hi*lo + lo*hi, FP32
+// accumulation in tensor memory); spectral state, radial operators and CNAB2
+// stay FP64.
 #pragma once
 
 struct gd_handle;
@@ -15,7 +16,8 @@ size_t mixed_bytes(const gd_handle* h);
 int mixed_temperature_nl(gd_handle* h);
 int mixed_velocity_nl(gd_handle* h);
 int mixed_magnetic_nl(gd_handle* h);
-void mixed_grid_to_double(gd_handle* h, int grid, double* out);
+// GD_ERR_UNSUPPORTED for the product grids, which the mixed step does not store.
+int mixed_grid_to_double(gd_handle* h, int grid, double* out);
 int mixed_api_synth_scalar(gd_handle* h, const double* const* coef, int nf, double* grid_out);
 int mixed_api_synth_vector(gd_handle* h, const double* tor, const double* pol, double* grid_out);
 int mixed_api_analysis_scalar(gd_handle* h, const double* grid_in, int nf, double* const* out);

@@ -7,9 +7,15 @@
 
 namespace gd {
 
+// Colatitude pairs per block of the blocked Fourier layout written by the
+// synthesis and read by the fused phase kernels: float4 (north Re, north Im,
+// south Re, south Im) at [comp][r][theta block][m][pair in block].
+constexpr int FOURIER_BLOCK = 2;
+
 struct TcSynthArgs {
   const double* coef[4];  // scalar: nf fields ; vector: [0] = S (poloidal), [1] = T (toroidal)
-  float2* out;            // FP32 Fourier buffer [comp][r][m][s][ith]
+  float4* out;            // blocked FP32 Fourier buffer, comps consecutive
+  int nblk;               // theta blocks (ceil(nth / FOURIER_BLOCK))
   int nf;
   int* err;               // set to 1 if a bounded wait expires
 };

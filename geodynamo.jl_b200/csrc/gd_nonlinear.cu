@@ -1,5 +1,7 @@
-// gd_nonlinear.cu -- grid-space nonlinear products, streamed over the native
-// grid layout [r][theta][phi].  Each kernel is the fused loop of the cited
+// gd_nonlinear.cu -- grid-space nonlinear products of the FP64 step, streamed
+// over the native grid layout [r][theta][phi] (the mixed-precision step forms
+// the same products inside its fused phase kernels, gd_fused.cu).  Each kernel
+// is the fused loop of the cited
 // reference function; the radial vector components are identically zero on
 // this path because the reference's vector synthesis writes only theta/phi
 // (src/shtnskit_field_functions.jl:264-279), and the expressions keep those
@@ -105,17 +107,10 @@ void launch_induction(cudaStream_t s, const Dims& d, const R* uth, const R* uph,
 template void launch_temperature_advection<double>(cudaStream_t, const Dims&, const double*, const double*,
                                                    const double*, const double*, const double*, const double*,
                                                    double*);
-template void launch_temperature_advection<float>(cudaStream_t, const Dims&, const float*, const float*,
-                                                  const float*, const float*, const float*, const double*, float*);
 template void launch_velocity_nl<double>(cudaStream_t, const Dims&, const double*, const double*, double, double, int,
                                          const double*, const double*, const double*, const double*, const double*,
                                          const double*, const double*, const double*, double*, double*);
-template void launch_velocity_nl<float>(cudaStream_t, const Dims&, const double*, const double*, double, double, int,
-                                        const float*, const float*, const float*, const float*, const float*,
-                                        const float*, const float*, const float*, float*, float*);
 template void launch_induction<double>(cudaStream_t, const Dims&, const double*, const double*, const double*,
                                        const double*, double*, double*);
-template void launch_induction<float>(cudaStream_t, const Dims&, const float*, const float*, const float*,
-                                      const float*, float*, float*);
 
 }  // namespace gd
