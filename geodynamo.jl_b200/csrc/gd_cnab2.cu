@@ -43,7 +43,7 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
   const bool is_temp = slot == a.temp_slot;
 
   // sweep 1: right-hand side, rows in batches of RB whose loads are issued first
-  constexpr int RB = 8;
+  constexpr int RB = 4;
   double wr[NB], wi[NB];
 #pragma unroll
   for (int t = 0; t < NB; ++t) {
@@ -186,7 +186,9 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
 
 // blockIdx.y = field slot; the block's Laplacian band uses that field's diffusivity.
 template <int KL>
-__global__ void __launch_bounds__(128) k_cnab2(Dims d, const int* __restrict__ lof, const double* __restrict__ d1,
+// 160 registers, three 128-thread blocks per SM (more columns in flight than
+// wider row batches would give)
+__global__ void __launch_bounds__(128, 3) k_cnab2(Dims d, const int* __restrict__ lof, const double* __restrict__ d1,
                                                const double* __restrict__ d2, const double* __restrict__ rinv,
                                                const double* __restrict__ rinv2, const double* __restrict__ nu,
                                                const double* __restrict__ lu, Cnab2Args a) {

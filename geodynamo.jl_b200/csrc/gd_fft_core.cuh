@@ -142,7 +142,7 @@ __device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restric
     for (int r = 0; r < R; ++r) v[r] = s[pidx(j + r * nbf)];
     if (k > 0) {
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(&tw[r * k * twstep]));
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * k * twstep]);
     }
     Dft<R, C>::run(v);
     C* o = dst + (size_t)row * prow(n);
@@ -209,6 +209,11 @@ template <typename RT, int N> struct CtGeom {
   static constexpr int TB = TB0 > 16 ? 16 : (TB0 < 1 ? 1 : TB0);
 };
 
+// One compile-time Stockham pass.  Padded indices pidx(j + r * stride) are
+// formed as pidx(j) + r * (stride + stride / 16) when the stride is a multiple
+// of 16 (and as pidx(group base) + offset when a radix group cannot cross a
+// 16-element boundary), so the inner loops carry no index arithmetic.  The
+// twiddle table may live in global or shared memory.
 template <int R, int N, int TB, int NS, typename C, int NT = kThreads>
 __device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw) {
   constexpr int RS = (N + (N >> 4)) | 1;
@@ -220,17 +225,34 @@ __device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict
     const int k = j % NS;
     const C* s = src + row * RS;
     C v[R];
+    if constexpr (NBF % 16 == 0) {
+      const C* sj = s + pidx(j);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = s[pidx(j + r * NBF)];
-    if (NS > 1 && k > 0) {
+      for (int r = 0; r < R; ++r) v[r] = sj[r * (NBF + NBF / 16)];
+    } else {
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], __ldg(&tw[r * k * TWSTEP]));
+      for (int r = 0; r < R; ++r) v[r] = s[pidx(j + r * NBF)];
+    }
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * k * TWSTEP]);
     }
     Dft<R, C>::run(v);
     C* o = dst + row * RS;
-    const int o0 = (j / NS) * NS * R + k;
+    const int base = (j / NS) * NS * R;
+    const int o0 = base + k;
+    if constexpr (NS % 16 == 0) {
+      C* oo = o + pidx(o0);
 #pragma unroll
-    for (int r = 0; r < R; ++r) o[pidx(o0 + r * NS)] = v[r];
+      for (int r = 0; r < R; ++r) oo[r * (NS + NS / 16)] = v[r];
+    } else if constexpr (16 % (NS * R) == 0) {
+      C* oo = o + o0 + (base >> 4);
+#pragma unroll
+      for (int r = 0; r < R; ++r) oo[r * NS] = v[r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) o[pidx(o0 + r * NS)] = v[r];
+    }
   }
 }
 

@@ -69,8 +69,13 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
   C* acc1 = acc0 + FB * rs;
   C* u0 = acc1;            // phase T (one product): u_theta, u_phi rows
   C* u1 = acc1 + FB * rs;
-  float* sct = reinterpret_cast<float*>(acc1 + FB * rs);  // phase V: Coriolis cos / sin by phi index
+  // phase V: Coriolis cos / sin by phi index (after the four buffers);
+  // every phase: the twiddle table after its buffers
+  float* sct = reinterpret_cast<float*>(acc1 + FB * rs);
   float* sst = sct + n;
+  const int nbuf = PH == FUSED_GRID ? 2 : (PH == FUSED_TEMPERATURE ? 5 : 4);
+  C* stw = reinterpret_cast<C*>(smem_raw + (size_t)nbuf * FB * rs * sizeof(C) +
+                                (PH == FUSED_VELOCITY ? 2 * (size_t)n * sizeof(float) : 0));
 
   const int tid = threadIdx.x;
   const int ib = blockIdx.x, r = blockIdx.y;
@@ -80,6 +85,7 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
   const int tot = (M + 1) * FB;
   const size_t boff = ((size_t)r * gridDim.x + ib) * (size_t)tot;
 
+  for (int j = tid; j < n; j += FNT) stw[j] = tw[j];
   if (PH == FUSED_VELOCITY) {
     for (int j = tid; j < n; j += FNT) {
       const int t = j < d.nlat - 1 ? j : d.nlat - 1;
@@ -136,7 +142,7 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
     build(c);
     __syncthreads();
     if (c + 1 < a.nin) prefetch(c + 1);
-    const C* res = run_fft<N>(bufA, bufB, tw, p);
+    const C* res = run_fft<N>(bufA, bufB, stw, p);
     if (PH == FUSED_GRID) {
       write_grid(res, a.gout[c]);
     } else if (PH == FUSED_TEMPERATURE && c == 5) {
@@ -170,37 +176,41 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
         } else if (PH == FUSED_VELOCITY) {
           // theta: adv (u_ph w_r - u_r w_ph) + mrf (-ct u_ph) + lf (j_ph b_r - j_r b_ph)
           // phi:   adv (u_r w_th - u_th w_r) + mrf (ct u_th + st u_r) + lf (j_r b_th - j_th b_r)
-          const float ct = sct[j], st = sst[j];
-          C t0 = acc0[q], t1 = acc1[q];
+          // even inputs (theta components) feed the phi product, odd ones the theta product
+          C* acc = (c & 1) ? acc0 : acc1;
+          C t = acc[q];
           switch (c) {
-            case 0:
-              t1.x += adv * (-(vN * wr)) + mrf * (ct * vN + st * ur);
-              t1.y += adv * (-(vS * wr)) + mrf * (ct * vS + st * ur);
+            case 0: {
+              const float ct = sct[j], st = sst[j];
+              t.x += adv * (-(vN * wr)) + mrf * (ct * vN + st * ur);
+              t.y += adv * (-(vS * wr)) + mrf * (ct * vS + st * ur);
               break;
-            case 1:
-              t0.x += adv * (vN * wr) + mrf * (-ct * vN);
-              t0.y += adv * (vS * wr) + mrf * (-ct * vS);
+            }
+            case 1: {
+              const float ct = sct[j];
+              t.x += adv * (vN * wr) + mrf * (-ct * vN);
+              t.y += adv * (vS * wr) + mrf * (-ct * vS);
               break;
-            case 2: t1.x += adv * (ur * vN); t1.y += adv * (ur * vS); break;
-            case 3: t0.x += adv * (-(ur * vN)); t0.y += adv * (-(ur * vS)); break;
-            case 4: t1.x += lfr * (-(vN * br)); t1.y += lfr * (-(vS * br)); break;
-            case 5: t0.x += lfr * (vN * br); t0.y += lfr * (vS * br); break;
-            case 6: t1.x += lfr * (jr * vN); t1.y += lfr * (jr * vS); break;
-            default: t0.x += lfr * (-(jr * vN)); t0.y += lfr * (-(jr * vS)); break;
+            }
+            case 2: t.x += adv * (ur * vN); t.y += adv * (ur * vS); break;
+            case 3: t.x += adv * (-(ur * vN)); t.y += adv * (-(ur * vS)); break;
+            case 4: t.x += lfr * (-(vN * br)); t.y += lfr * (-(vS * br)); break;
+            case 5: t.x += lfr * (vN * br); t.y += lfr * (vS * br); break;
+            case 6: t.x += lfr * (jr * vN); t.y += lfr * (jr * vS); break;
+            default: t.x += lfr * (-(jr * vN)); t.y += lfr * (-(jr * vS)); break;
           }
-          acc0[q] = t0;
-          acc1[q] = t1;
+          acc[q] = t;
         } else {
           // induction: theta u_ph b_r - u_r b_ph, phi u_r b_th - u_th b_r
-          C t0 = acc0[q], t1 = acc1[q];
+          C* acc = (c & 1) ? acc0 : acc1;
+          C t = acc[q];
           switch (c) {
-            case 0: t1.x += -(vN * br); t1.y += -(vS * br); break;
-            case 1: t0.x += vN * br; t0.y += vS * br; break;
-            case 2: t1.x += ur * vN; t1.y += ur * vS; break;
-            default: t0.x += -(ur * vN); t0.y += -(ur * vS); break;
+            case 0: t.x += -(vN * br); t.y += -(vS * br); break;
+            case 1: t.x += vN * br; t.y += vS * br; break;
+            case 2: t.x += ur * vN; t.y += ur * vS; break;
+            default: t.x += -(ur * vN); t.y += -(ur * vS); break;
           }
-          acc0[q] = t0;
-          acc1[q] = t1;
+          acc[q] = t;
         }
       }
     }
@@ -213,7 +223,7 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
   const int nout = (PH == FUSED_TEMPERATURE) ? 1 : 2;
   for (int o = 0; o < nout; ++o) {
     C* src = o == 0 ? acc0 : acc1;
-    const C* res = run_fft<N>(src, o == 0 ? bufA : bufB, tw, p);
+    const C* res = run_fft<N>(src, o == 0 ? bufA : bufB, stw, p);
     const size_t gb = ((size_t)(o * d.nr + r) * (M + 1)) * 2 * d.nth;
     for (int e = tid; e < tot; e += FNT) {
       const int m = e / FB, ii = e - m * FB;
@@ -238,11 +248,12 @@ namespace {
 
 size_t fused_smem(int phase, int n) {
   const size_t buf = (size_t)FB * prow(n) * sizeof(float2);
+  const size_t twb = (size_t)n * sizeof(float2);
   switch (phase) {
-    case FUSED_GRID: return 2 * buf;
-    case FUSED_TEMPERATURE: return 5 * buf;
-    case FUSED_VELOCITY: return 4 * buf + 2 * (size_t)n * sizeof(float);
-    default: return 4 * buf;
+    case FUSED_GRID: return 2 * buf + twb;
+    case FUSED_TEMPERATURE: return 5 * buf + twb;
+    case FUSED_VELOCITY: return 4 * buf + 2 * (size_t)n * sizeof(float) + twb;
+    default: return 4 * buf + twb;
   }
 }
 
