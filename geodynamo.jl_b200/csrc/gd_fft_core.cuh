@@ -214,7 +214,10 @@ template <typename RT, int N> struct CtGeom {
 // of 16 (and as pidx(group base) + offset when a radix group cannot cross a
 // 16-element boundary), so the inner loops carry no index arithmetic.  The
 // twiddle table may live in global or shared memory.
-template <int R, int N, int TB, int NS, typename C, int NT = kThreads>
+// PT: tw is this pass's own table [r - 1][k] (k < NS, consecutive k in
+// consecutive entries, so a warp's twiddle reads are conflict-free in shared
+// memory); otherwise tw is the full table W_N^i.
+template <int R, int N, int TB, int NS, typename C, int NT = kThreads, bool PT = false>
 __device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw) {
   constexpr int RS = (N + (N >> 4)) | 1;
   constexpr int NBF = N / R;
@@ -235,7 +238,7 @@ __device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict
     }
     if constexpr (NS > 1) {
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * k * TWSTEP]);
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], PT ? tw[(r - 1) * NS + k] : tw[r * k * TWSTEP]);
     }
     Dft<R, C>::run(v);
     C* o = dst + row * RS;
@@ -266,6 +269,52 @@ __device__ __forceinline__ C* ct_passes(C* src, C* dst, const C* tw) {
     ct_pass<R, N, TB, NS, C, NT>(src, dst, tw);
     __syncthreads();
     return ct_passes<N, TB, S + 1, NS * R, C, NT>(dst, src, tw);
+  }
+}
+
+// Per-pass twiddle tables: pass s (NS_s > 1) owns (R_s - 1) NS_s entries
+// W_N^(r k N / (NS_s R_s)) at [r - 1][k], one after the other.
+constexpr int ct_pass_tw_entries(int N) {
+  const CPlan p = make_cplan(N);
+  int ns = 1, tot = 0;
+  for (int s = 0; s < p.ns; ++s) {
+    if (ns > 1) tot += (p.r[s] - 1) * ns;
+    ns *= p.r[s];
+  }
+  return tot;
+}
+
+// Fills the per-pass tables from the full table W_N^i (global memory).
+template <int N, int NT>
+__device__ __forceinline__ void ct_fill_pass_twiddles(const float2* __restrict__ tw_full, float2* __restrict__ out) {
+  constexpr CPlan P = PlanOf<N>::p;
+  int ns = 1, off = 0;
+#pragma unroll
+  for (int s = 0; s < P.ns; ++s) {
+    const int R = P.r[s];
+    if (ns > 1) {
+      const int step = N / (ns * R);
+      for (int e = threadIdx.x; e < (R - 1) * ns; e += NT) {
+        const int r = e / ns + 1, k = e - (r - 1) * ns;
+        out[off + e] = tw_full[r * k * step];
+      }
+      off += (R - 1) * ns;
+    }
+    ns *= R;
+  }
+}
+
+// ct_passes with per-pass twiddle tables (ct_fill_pass_twiddles layout).
+template <int N, int TB, int S, int NS, typename C, int NT, int OFF = 0>
+__device__ __forceinline__ C* ct_passes_pt(C* src, C* dst, const C* tw) {
+  constexpr CPlan P = PlanOf<N>::p;
+  if constexpr (S >= P.ns) {
+    return src;
+  } else {
+    constexpr int R = P.r[S];
+    ct_pass<R, N, TB, NS, C, NT, true>(src, dst, tw + OFF);
+    __syncthreads();
+    return ct_passes_pt<N, TB, S + 1, NS * R, C, NT, (NS > 1 ? OFF + (R - 1) * NS : OFF)>(dst, src, tw);
   }
 }
 

@@ -35,7 +35,7 @@ constexpr int PF = 4;     // prefetched float4 per thread (covers (M+1) FB <= 51
 template <int N>
 __device__ __forceinline__ float2* run_fft(float2* a, float2* b, const float2* tw, const FftPlan& p) {
   if constexpr (N > 0) {
-    return ct_passes<N, FB, 0, 1, float2, FNT>(a, b, tw);
+    return ct_passes_pt<N, FB, 0, 1, float2, FNT>(a, b, tw);
   } else {
     return fft_forward<float, FNT>(a, b, FB, p, tw);
   }
@@ -85,7 +85,12 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
   const int tot = (M + 1) * FB;
   const size_t boff = ((size_t)r * gridDim.x + ib) * (size_t)tot;
 
-  for (int j = tid; j < n; j += FNT) stw[j] = tw[j];
+  if constexpr (N > 0) {
+    static_assert(ct_pass_tw_entries(N) <= N, "per-pass twiddles exceed the table space");
+    ct_fill_pass_twiddles<N, FNT>(tw, stw);
+  } else {
+    for (int j = tid; j < n; j += FNT) stw[j] = tw[j];
+  }
   if (PH == FUSED_VELOCITY) {
     for (int j = tid; j < n; j += FNT) {
       const int t = j < d.nlat - 1 ? j : d.nlat - 1;
