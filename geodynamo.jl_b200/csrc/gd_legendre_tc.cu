@@ -35,6 +35,7 @@ constexpr int TC_N2 = 128;    // synthesis and scalar analysis column tile
 constexpr int TC_K = 32;                       // TF32 elements per 128-byte row
 constexpr int TILE_A_FLOATS = TC_M * TC_K;      // 4096 floats = 16 KB
 constexpr int CHUNK_FLOATS = 2 * TILE_A_FLOATS; // hi image then lo image (32 KB)
+constexpr uint32_t CHUNK_BYTES = CHUNK_FLOATS * 4;
 constexpr uint32_t IDESC = idesc_tf32(TC_M, TC_N);
 constexpr uint32_t IDESC2 = idesc_tf32(TC_M, TC_N2);
 // Pipelined kernels: every stage holds one (chunk, parity) step; stages sit
@@ -76,41 +77,6 @@ __device__ __forceinline__ void issue_chunk(uint32_t tmem, uint32_t dcol, const 
   }
 }
 
-
-// cp.async (16-byte, L2-cached) copies for the table images.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// One 32 KB image chunk (hi + lo) into shared memory, all 256 threads.
-__device__ __forceinline__ void async_chunk(float* dst, const float* img, long chunk) {
-  const char* src = reinterpret_cast<const char*>(img + chunk * CHUNK_FLOATS);
-  char* d = reinterpret_cast<char*>(dst);
-  for (int i = threadIdx.x; i < CHUNK_FLOATS / 4; i += 256) cp_async16(d + 16 * i, src + 16 * i);
-}
-
-// Wait until the MMAs of the previous user of the stage of iteration `it` are done.
-template <int S>
-__device__ __forceinline__ bool stage_free(uint64_t* bars, int it, int* err) {
-  if (it < S) return true;
-  const int prev = it - S;
-  return mbar_wait(&bars[prev % S], (prev / S) & 1, err);
-}
-
-// Wait for the last use of every stage.
-template <int S>
-__device__ __forceinline__ bool drain(uint64_t* bars, int T, int* err) {
-  bool ok = true;
-#pragma unroll
-  for (int s = 0; s < S; ++s) {
-    if (s >= T) continue;
-    const int last = s + S * ((T - 1 - s) / S);
-    ok = mbar_wait(&bars[s], (last / S) & 1, err) && ok;
-  }
-  return ok;
-}
 
 __device__ __forceinline__ void put_split_d(float* hi, float* lo, int row, int k, double x) {
   const float h = tf32_rn((float)x);
@@ -198,19 +164,26 @@ void launch_build_tc_images(cudaStream_t s, const Dims& d, const int* moff, cons
 }
 
 // ---------------------------------------------------------------------------
-// Synthesis.  CTA = (m, 128-row theta tile, 128 columns), 256 threads.
-// One pipeline step per (K chunk, parity): all threads stream the table
-// chunk(s) into the stage with cp.async and split the 128 x 32 FP64
-// coefficient tile into TF32 hi/lo; thread 0 issues the MMAs of the step and
-// commits them to the stage's mbarrier, then the next stage is filled while
-// the tensor core works.  Scalar: 3 stages of 64 KB, accumulators
-// [even | odd] x 128 columns.  Vector: 2 stages of 96 KB holding the Pbar and
-// dPbar/dtheta chunks, accumulators [P even | P odd | dP even | dP odd]; the
-// m/sin(theta) factor of the Q = m Pbar / sin(theta) terms is applied to the
-// Pbar sums in the epilogue.  Vector columns: [S: 32 shells x re/im][T: same].
+// Synthesis.  CTA = (m, 128-row theta tile, column tile), 288 threads:
+// two loader groups of four warps and one MMA warp.  One pipeline step per
+// (K chunk, parity); loader group g fills stage g for the steps it = g, g+2,
+// ...: its first thread starts bulk copies of the table chunk(s) (transaction
+// bytes on the stage's `full` barrier), and all 128 threads load and split the
+// 128-deep (vector) or 256-deep (scalar) x 32 FP64 coefficient tile into TF32
+// hi/lo and arrive on the stage's `full` barrier.  The MMA warp issues the
+// step's MMAs when the stage is full and commits them to the stage's `empty`
+// barrier, which the group waits on before refilling.  The two groups' loads
+// are in flight at the same time, so a step's load latency overlaps the
+// previous step's.  Scalar: accumulators [even | odd] x 256 columns.
+// Vector: stages hold the Pbar and dPbar/dtheta chunks, accumulators [P even
+// | P odd | dP even | dP odd] x 128; the m/sin(theta) factor of the Q = m
+// Pbar / sin(theta) terms is applied to the Pbar sums in the epilogue.
+// Vector columns: [S: 32 shells x re/im][T: same].
 // ---------------------------------------------------------------------------
+constexpr int WS_THREADS = 288;  // 2 loader groups x 4 warps + 1 MMA warp
+
 template <bool VEC>
-__global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restrict__ moff,
+__global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* __restrict__ moff,
                                                       const long* __restrict__ cofs, const float* __restrict__ imgP,
                                                       const float* __restrict__ imgD, const double* __restrict__ sinv,
                                                       TcSynthArgs a) {
@@ -224,11 +197,12 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
   extern __shared__ unsigned char smem_raw[];
   const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   float* stg = reinterpret_cast<float*>(base);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + (size_t)S * ST_FL * 4);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + S);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)S * ST_FL * 4);
+  uint64_t* empty = full + S;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(empty + S);
   // scalar: column -> coefficient row (null past the last column); column
   // pair -> Fourier output base (-1 past the last column)
-  const double** colp = reinterpret_cast<const double**>(bars + S + 2);
+  const double** colp = reinterpret_cast<const double**>(empty + S + 2);
   long long* colo = reinterpret_cast<long long*>(colp + NCS);
 
   const int m = blockIdx.z, tile = blockIdx.y;
@@ -240,7 +214,10 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
   if (tile * TC_M >= d.nth || (VEC ? r0 >= d.nr : n0 >= Ntot)) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0)
-    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 128);
+      mbar_init(&empty[s], 1);
+    }
   if (warp == 0) tmem_alloc(tslot, NCOL);
   if (!VEC) {
     for (int c = tid; c < NCS; c += blockDim.x) {
@@ -269,69 +246,91 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
   const int nc0 = nck_h(L, m, 0), nc1 = nck_h(L, m, 1);
   const int T = nc0 + nc1;
 
-  auto produce = [&](int it) {
-    const int s = it % S;
-    const int kc = it < 2 * nc1 ? (it >> 1) : nc1 + (it - 2 * nc1);
-    const int p = it < 2 * nc1 ? (it & 1) : 0;
-    float* A = stg + s * ST_FL;
-    float* B = A + A_FL;
-    async_chunk(A, imgP, synth_chunk(cofs, L, m, tile, p, kc));
-    if (VEC) async_chunk(A + CHUNK_FLOATS, imgD, synth_chunk(cofs, L, m, tile, p, kc));
-    cp_async_commit();
-    const int l = m + p + 2 * (TC_K * kc + lane);
-    // all loads of this thread first (memory-level parallelism), then split
-    double v[NCS / 8];
-#pragma unroll
-    for (int i = 0; i < NCS / 8; ++i) {
-      const int row = warp + 8 * i;
-      const double* src = nullptr;
-      if (VEC) {
-        const int fld = row >> 6, r = r0 + ((row & 63) >> 1), c = row & 1;
-        if (r < d.nr) src = a.coef[fld] + ((size_t)c * d.nr + r) * NM + mb - m;
-      } else {
-        src = colp[row];
-      }
-      v[i] = (src != nullptr && l <= L) ? __ldg(src + l) : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < NCS / 8; ++i) put_split_d(B, B + BT, warp + 8 * i, lane, v[i]);
+  // step it -> (parity p, K chunk kc): odd-parity chunks interleave with the
+  // even ones while both exist
+  auto step_pk = [&](int it, int& p, int& kc) {
+    kc = it < 2 * nc1 ? (it >> 1) : nc1 + (it - 2 * nc1);
+    p = it < 2 * nc1 ? (it & 1) : 0;
   };
 
   bool ok = true;
-  produce(0);
-  for (int it = 0; it < T; ++it) {
-    const int s = it % S;
-    cp_async_wait_all();
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      fence_after_sync();
-      const int kc = it < 2 * nc1 ? (it >> 1) : nc1 + (it - 2 * nc1);
-      const int p = it < 2 * nc1 ? (it & 1) : 0;
-      const float* A = stg + s * ST_FL;
-      const float* B = A + A_FL;
+  int issued = -1;  // loader thread 0 of a group: last use of its stage with bulk copies issued
+  if (warp < 8) {
+    const int g = warp >> 2, gw = warp & 3, gt = tid & 127;
+    float* A = stg + g * ST_FL;
+    float* B = A + A_FL;
+    constexpr int RPT = NCS / 4;              // coefficient rows per thread
+    constexpr int HALF = RPT > 32 ? 32 : RPT; // loads in flight per batch
+    for (int it = g; it < T; it += 2) {
+      const int u = it >> 1;
+      if (u >= 1 && !mbar_wait(&empty[g], (u - 1) & 1, a.err)) {
+        ok = false;
+        break;
+      }
+      int p, kc;
+      step_pk(it, p, kc);
+      if (gt == 0) {
+        const long ch = synth_chunk(cofs, L, m, tile, p, kc);
+        mbar_expect_tx(&full[g], (VEC ? 2u : 1u) * CHUNK_BYTES);
+        bulk_g2s(A, imgP + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[g]);
+        if (VEC) bulk_g2s(A + CHUNK_FLOATS, imgD + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[g]);
+        issued = u;
+      }
+      const int l = m + p + 2 * (TC_K * kc + lane);
 #pragma unroll
-      for (int t = 0; t < (VEC ? 2 : 1); ++t)
-        issue_chunk(tmem, (t * 2 + p) * NCS, A + t * CHUNK_FLOATS, A + t * CHUNK_FLOATS + TILE_A_FLOATS, B, B + BT,
-                    kc == 0, IDS);
-      mma_commit(smem_addr(&bars[s]));
+      for (int h = 0; h < RPT; h += HALF) {
+        double v[HALF];
+#pragma unroll
+        for (int i = 0; i < HALF; ++i) {
+          const int row = gw + 4 * (h + i);
+          const double* src = nullptr;
+          if (VEC) {
+            const int fld = row >> 6, r = r0 + ((row & 63) >> 1), c = row & 1;
+            if (r < d.nr) src = a.coef[fld] + ((size_t)c * d.nr + r) * NM + mb - m;
+          } else {
+            src = colp[row];
+          }
+          v[i] = (src != nullptr && l <= L) ? __ldg(src + l) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < HALF; ++i) put_split_d(B, B + BT, gw + 4 * (h + i), lane, v[i]);
+      }
+      fence_proxy_async();
+      mbar_arrive(&full[g]);
     }
-    if (it + 1 < T) {
-      const bool w = stage_free<S>(bars, it + 1, a.err);
-      ok = __syncthreads_and(w);
-      if (!ok) break;
-      fence_after_sync();
-      produce(it + 1);
-    }
-  }
-  if (ok) {
-    const bool w = drain<S>(bars, T, a.err);
-    ok = __syncthreads_and(w);
-    fence_after_sync();
   } else {
-    cp_async_wait_all();
+    for (int it = 0; it < T; ++it) {
+      const int s = it & 1;
+      if (!mbar_wait(&full[s], (it >> 1) & 1, a.err)) {
+        ok = false;
+        break;
+      }
+      fence_after_sync();
+      if (lane == 0) {
+        int p, kc;
+        step_pk(it, p, kc);
+        const float* A = stg + s * ST_FL;
+        const float* B = A + A_FL;
+#pragma unroll
+        for (int t = 0; t < (VEC ? 2 : 1); ++t)
+          issue_chunk(tmem, (t * 2 + p) * NCS, A + t * CHUNK_FLOATS, A + t * CHUNK_FLOATS + TILE_A_FLOATS, B,
+                      B + BT, kc == 0, IDS);
+        mma_commit(smem_addr(&empty[s]));
+      }
+      __syncwarp();
+    }
   }
+  // drain: the last MMA batch of each stage
   if (ok) {
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+      if (s < T) ok = mbar_wait(&empty[s], ((T - 1 - s) >> 1) & 1, a.err) && ok;
+  }
+  ok = __syncthreads_and(ok);
+  // after an expired wait, let the last bulk copies land before the CTA exits
+  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err);
+  fence_after_sync();
+  if (ok && warp < 8) {
     const int q = warp & 3, half = warp >> 2;
     const int ith = tile * TC_M + q * 32 + lane;
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
@@ -414,17 +413,18 @@ __global__ void __launch_bounds__(256, 1) k_tc_synth3(Dims d, const int* __restr
 
 // ---------------------------------------------------------------------------
 // Analysis.  CTA = (m, column tile); K = colatitude in chunks of 32; one
-// pipeline step per (theta chunk, parity).  Scalar: 128 columns
-// n = (field, r, re/im), 3 stages of 64 KB, accumulators [even | odd].
-// Vector: 64 columns [G_theta: 16 shells x re/im][G_phi], 2 stages of 96 KB
+// pipeline step per (theta chunk, parity), with the loader groups and MMA
+// warp of the synthesis (group g fills stage g).  Scalar: 128 columns
+// n = (field, r, re/im), stages of 64 KB, accumulators [even | odd].
+// Vector: 64 columns [G_theta: 16 shells x re/im][G_phi], stages of 96 KB
 // holding the dPbar and Q chunks and two B tiles (fold 1 - p for dPbar, fold p
 // for Q), accumulators [dP even | dP odd | Q even | Q odd] x 64.
 // ---------------------------------------------------------------------------
 template <bool VEC>
-__global__ void __launch_bounds__(256, 1) k_tc_analysis3(Dims d, const int* __restrict__ moff,
+__global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const int* __restrict__ moff,
                                                          const float* __restrict__ img0,
                                                          const float* __restrict__ img1, TcAnalysisArgs a) {
-  constexpr int S = VEC ? 2 : 3;
+  constexpr int S = 2;
   constexpr int NC = VEC ? TC_N : TC_N2;         // columns
   constexpr int A_FL = (VEC ? 2 : 1) * CHUNK_FLOATS;
   constexpr int BT = NC * TC_K;                  // one B image (hi or lo)
@@ -434,11 +434,12 @@ __global__ void __launch_bounds__(256, 1) k_tc_analysis3(Dims d, const int* __re
   extern __shared__ unsigned char smem_raw[];
   const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   float* stg = reinterpret_cast<float*>(base);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + (size_t)S * ST_FL * 4);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + S);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)S * ST_FL * 4);
+  uint64_t* empty = full + S;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(empty + S);
   // scalar: column pair -> folded-input base (-1 past the last column);
   // column -> output row (null past the last column)
-  long long* colin = reinterpret_cast<long long*>(bars + S + 2);
+  long long* colin = reinterpret_cast<long long*>(empty + S + 2);
   double** colout = reinterpret_cast<double**>(colin + NC / 2);
 
   const int m = blockIdx.z;
@@ -450,7 +451,10 @@ __global__ void __launch_bounds__(256, 1) k_tc_analysis3(Dims d, const int* __re
   if (VEC ? r0 >= d.nr : n0 >= Ntot) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0)
-    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 128);
+      mbar_init(&empty[s], 1);
+    }
   if (warp == 0) tmem_alloc(tslot, NCOL);
   if (!VEC) {
     for (int c = tid; c < NC; c += blockDim.x) {
@@ -482,90 +486,99 @@ __global__ void __launch_bounds__(256, 1) k_tc_analysis3(Dims d, const int* __re
   const int nthc = (d.nth + TC_K - 1) / TC_K;
   const int T = nthc * np;
 
-  auto produce = [&](int it) {
-    const int s = it % S;
-    const int cc = it / np, p = it % np;
-    float* A = stg + s * ST_FL;
-    float* B = A + A_FL;
-    async_chunk(A, img0, (long)(m * 2 + p) * nthc + cc);
-    if (VEC) async_chunk(A + CHUNK_FLOATS, img1, (long)(m * 2 + p) * nthc + cc);
-    cp_async_commit();
-    const int ith = TC_K * cc + lane;
-    if (!VEC) {
-      float2 v[NC / 16];
-#pragma unroll
-      for (int i = 0; i < NC / 16; ++i) {
-        const int pr = warp + 8 * i;
-        const long long ib = colin[pr];
-        v[i] = make_float2(0.f, 0.f);
-        if (ib >= 0 && ith < d.nth) v[i] = __ldg(&a.in[(size_t)ib + (size_t)p * d.nth + ith]);
-      }
-#pragma unroll
-      for (int i = 0; i < NC / 16; ++i) {
-        const int pr = warp + 8 * i;
-        put_split_f(B, B + BT, 2 * pr, lane, v[i].x);
-        put_split_f(B, B + BT, 2 * pr + 1, lane, v[i].y);
-      }
-    } else {
-      float2 v[NC / 8];
-#pragma unroll
-      for (int i = 0; i < NC / 8; ++i) {
-        const int item = warp + 8 * i;
-        const int slot = item / (NC / 2), pr = item % (NC / 2);
-        const int fold = slot == 0 ? 1 - p : p;
-        const int comp = pr >> 4, r = r0 + (pr & 15);
-        v[i] = make_float2(0.f, 0.f);
-        if (r < d.nr && ith < d.nth)
-          v[i] = __ldg(&a.in[(((size_t)(comp * d.nr + r) * (d.M + 1) + m) * 2 + fold) * d.nth + ith]);
-      }
-#pragma unroll
-      for (int i = 0; i < NC / 8; ++i) {
-        const int item = warp + 8 * i;
-        const int slot = item / (NC / 2), pr = item % (NC / 2);
-        float* Bt = B + slot * 2 * BT;
-        put_split_f(Bt, Bt + BT, 2 * pr, lane, v[i].x);
-        put_split_f(Bt, Bt + BT, 2 * pr + 1, lane, v[i].y);
-      }
-    }
-  };
-
   bool ok = true;
-  produce(0);
-  for (int it = 0; it < T; ++it) {
-    const int s = it % S;
-    cp_async_wait_all();
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      fence_after_sync();
-      const int cc = it / np, p = it % np;
-      const float* A = stg + s * ST_FL;
-      const float* B = A + A_FL;
-      if (!VEC) {
-        issue_chunk(tmem, p * TC_N2, A, A + TILE_A_FLOATS, B, B + BT, cc == 0, IDESC2);
-      } else {
-        issue_chunk(tmem, (0 * 2 + p) * TC_N, A, A + TILE_A_FLOATS, B, B + BT, cc == 0, IDESC);
-        issue_chunk(tmem, (1 * 2 + p) * TC_N, A + CHUNK_FLOATS, A + CHUNK_FLOATS + TILE_A_FLOATS, B + 2 * BT,
-                    B + 3 * BT, cc == 0, IDESC);
+  int issued = -1;  // loader thread 0 of a group: last use of its stage with bulk copies issued
+  if (warp < 8) {
+    const int g = warp >> 2, gw = warp & 3, gt = tid & 127;
+    float* A = stg + g * ST_FL;
+    float* B = A + A_FL;
+    for (int it = g; it < T; it += 2) {
+      const int u = it >> 1;
+      if (u >= 1 && !mbar_wait(&empty[g], (u - 1) & 1, a.err)) {
+        ok = false;
+        break;
       }
-      mma_commit(smem_addr(&bars[s]));
+      const int cc = it / np, p = it % np;
+      if (gt == 0) {
+        const long ch = (long)(m * 2 + p) * nthc + cc;
+        mbar_expect_tx(&full[g], (VEC ? 2u : 1u) * CHUNK_BYTES);
+        bulk_g2s(A, img0 + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[g]);
+        if (VEC) bulk_g2s(A + CHUNK_FLOATS, img1 + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[g]);
+        issued = u;
+      }
+      const int ith = TC_K * cc + lane;
+      // float2 per thread: scalar NC/2 column pairs, vector 2 x NC/2 (slot, pair) items, over 4 warps
+      constexpr int NV = VEC ? NC / 4 : NC / 8;
+      float2 v[NV];
+      if (!VEC) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          const long long ib = colin[gw + 4 * i];
+          v[i] = make_float2(0.f, 0.f);
+          if (ib >= 0 && ith < d.nth) v[i] = __ldg(&a.in[(size_t)ib + (size_t)p * d.nth + ith]);
+        }
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          const int pr = gw + 4 * i;
+          put_split_f(B, B + BT, 2 * pr, lane, v[i].x);
+          put_split_f(B, B + BT, 2 * pr + 1, lane, v[i].y);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          const int item = gw + 4 * i;
+          const int slot = item / (NC / 2), pr = item % (NC / 2);
+          const int fold = slot == 0 ? 1 - p : p;
+          const int comp = pr >> 4, r = r0 + (pr & 15);
+          v[i] = make_float2(0.f, 0.f);
+          if (r < d.nr && ith < d.nth)
+            v[i] = __ldg(&a.in[(((size_t)(comp * d.nr + r) * (d.M + 1) + m) * 2 + fold) * d.nth + ith]);
+        }
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+          const int item = gw + 4 * i;
+          const int slot = item / (NC / 2), pr = item % (NC / 2);
+          float* Bt = B + slot * 2 * BT;
+          put_split_f(Bt, Bt + BT, 2 * pr, lane, v[i].x);
+          put_split_f(Bt, Bt + BT, 2 * pr + 1, lane, v[i].y);
+        }
+      }
+      fence_proxy_async();
+      mbar_arrive(&full[g]);
     }
-    if (it + 1 < T) {
-      const bool w = stage_free<S>(bars, it + 1, a.err);
-      ok = __syncthreads_and(w);
-      if (!ok) break;
-      fence_after_sync();
-      produce(it + 1);
-    }
-  }
-  if (ok) {
-    const bool w = drain<S>(bars, T, a.err);
-    ok = __syncthreads_and(w);
-    fence_after_sync();
   } else {
-    cp_async_wait_all();
+    for (int it = 0; it < T; ++it) {
+      const int s = it & 1;
+      if (!mbar_wait(&full[s], (it >> 1) & 1, a.err)) {
+        ok = false;
+        break;
+      }
+      fence_after_sync();
+      if (lane == 0) {
+        const int cc = it / np, p = it % np;
+        const float* A = stg + s * ST_FL;
+        const float* B = A + A_FL;
+        if (!VEC) {
+          issue_chunk(tmem, p * TC_N2, A, A + TILE_A_FLOATS, B, B + BT, cc == 0, IDESC2);
+        } else {
+          issue_chunk(tmem, (0 * 2 + p) * TC_N, A, A + TILE_A_FLOATS, B, B + BT, cc == 0, IDESC);
+          issue_chunk(tmem, (1 * 2 + p) * TC_N, A + CHUNK_FLOATS, A + CHUNK_FLOATS + TILE_A_FLOATS, B + 2 * BT,
+                      B + 3 * BT, cc == 0, IDESC);
+        }
+        mma_commit(smem_addr(&empty[s]));
+      }
+      __syncwarp();
+    }
   }
   if (ok) {
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+      if (s < T) ok = mbar_wait(&empty[s], ((T - 1 - s) >> 1) & 1, a.err) && ok;
+  }
+  ok = __syncthreads_and(ok);
+  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err);
+  fence_after_sync();
+  if (ok && warp < 8) {
     const int q = warp & 3, half = warp >> 2;
     const int i = q * 32 + lane;
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
@@ -638,12 +651,12 @@ static void smem_attr(K k, size_t bytes) {
 // kernels' per-column tables (one pointer per column, one offset per pair)
 static size_t synth_smem(bool vec) {
   const int S = 2, NCS = vec ? TC_N2 : 2 * TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS, B = 2 * NCS * TC_K;
-  return 1024 + (size_t)S * (A + B) * 4 + 8 * (S + 2) + (size_t)NCS * 8 + (size_t)(NCS / 2) * 8;
+  return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 2) + (size_t)NCS * 8 + (size_t)(NCS / 2) * 8;
 }
 static size_t analysis_smem(bool vec) {
-  const int S = vec ? 2 : 3, NC = vec ? TC_N : TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS;
+  const int S = 2, NC = vec ? TC_N : TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS;
   const int B = (vec ? 2 : 1) * 2 * NC * TC_K;
-  return 1024 + (size_t)S * (A + B) * 4 + 8 * (S + 2) + (size_t)NC * 8 + (size_t)(NC / 2) * 8;
+  return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 2) + (size_t)NC * 8 + (size_t)(NC / 2) * 8;
 }
 static bool g_attr_done = false;
 static void set_attrs() {
@@ -661,10 +674,10 @@ void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long*
   const int ntile = (d.nth + TC_M - 1) / TC_M;
   if (!vec) {
     dim3 grid(ceil_div(a.nf * d.nr * 2, 2 * TC_N2), ntile, d.M + 1);
-    k_tc_synth3<false><<<grid, 256, synth_smem(false), s>>>(d, moff, cofs, imgP, imgD, sinv, a);
+    k_tc_synth3<false><<<grid, WS_THREADS, synth_smem(false), s>>>(d, moff, cofs, imgP, imgD, sinv, a);
   } else {
     dim3 grid(ceil_div(d.nr, 32), ntile, d.M + 1);
-    k_tc_synth3<true><<<grid, 256, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD, sinv, a);
+    k_tc_synth3<true><<<grid, WS_THREADS, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD, sinv, a);
   }
 }
 
@@ -673,10 +686,10 @@ void launch_tc_analysis(cudaStream_t s, const Dims& d, const int* moff, const fl
   set_attrs();
   if (a.epi == EPI_SCALAR) {
     dim3 grid(ceil_div(a.nf * d.nr * 2, TC_N2), 1, d.M + 1);
-    k_tc_analysis3<false><<<grid, 256, analysis_smem(false), s>>>(d, moff, img0, img1, a);
+    k_tc_analysis3<false><<<grid, WS_THREADS, analysis_smem(false), s>>>(d, moff, img0, img1, a);
   } else {
     dim3 grid(ceil_div(d.nr, 16), 1, d.M + 1);
-    k_tc_analysis3<true><<<grid, 256, analysis_smem(true), s>>>(d, moff, img0, img1, a);
+    k_tc_analysis3<true><<<grid, WS_THREADS, analysis_smem(true), s>>>(d, moff, img0, img1, a);
   }
 }
 
