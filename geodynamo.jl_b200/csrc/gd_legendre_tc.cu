@@ -78,12 +78,15 @@ __device__ __forceinline__ void issue_chunk(uint32_t tmem, uint32_t dcol, const 
 }
 
 
-__device__ __forceinline__ void put_split_d(float* hi, float* lo, int row, int k, double x) {
-  const float h = tf32_rn((float)x);
-  const float l = tf32_rn((float)(x - (double)h));
-  const uint32_t o = sw128_offset(row, k) >> 2;
+// Runtime coefficients: x is rounded to FP32 once (relative error 2^-24,
+// the order of the FP32 accumulation), then split in single precision:
+// hi = tf32(f), lo = tf32(f - hi) (f - hi is exact).  o = float offset in the
+// swizzled tile.
+__device__ __forceinline__ void put_split_d_at(float* hi, float* lo, uint32_t o, double x) {
+  const float f = __double2float_rn(x);
+  const float h = tf32_rn(f);
   hi[o] = h;
-  lo[o] = l;
+  lo[o] = tf32_rn(f - h);
 }
 
 }  // namespace
@@ -277,6 +280,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
         issued = u;
       }
       const int l = m + p + 2 * (TC_K * kc + lane);
+      // swizzled offsets of rows gw + 4 i: 8-row atom i / 2, row in atom gw or gw + 4
+      const uint32_t o_even = sw128_offset(gw, lane) >> 2, o_odd = sw128_offset(gw + 4, lane) >> 2;
 #pragma unroll
       for (int h = 0; h < RPT; h += HALF) {
         double v[HALF];
@@ -293,7 +298,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
           v[i] = (src != nullptr && l <= L) ? __ldg(src + l) : 0.0;
         }
 #pragma unroll
-        for (int i = 0; i < HALF; ++i) put_split_d(B, B + BT, gw + 4 * (h + i), lane, v[i]);
+        for (int i = 0; i < HALF; ++i) {
+          const int ii = h + i;
+          put_split_d_at(B, B + BT, (uint32_t)(ii >> 1) * 256u + ((ii & 1) ? o_odd : o_even), v[i]);
+        }
       }
       fence_proxy_async();
       mbar_arrive(&full[g]);
