@@ -272,6 +272,39 @@ __device__ __forceinline__ C* ct_passes(C* src, C* dst, const C* tw) {
   }
 }
 
+// A compile-time pass that hands its outputs (row, natural index, value) to
+// f instead of storing them: the last pass of a transform whose consumer is
+// pointwise in the output index.
+template <int R, int N, int TB, int NS, typename C, int NT, bool PT, class F>
+__device__ __forceinline__ void ct_pass_apply(const C* __restrict__ src, const C* __restrict__ tw, F& f) {
+  constexpr int RS = (N + (N >> 4)) | 1;
+  constexpr int NBF = N / R;
+  constexpr int TOTAL = TB * NBF;
+  constexpr int TWSTEP = N / (NS * R);
+  for (int b = threadIdx.x; b < TOTAL; b += NT) {
+    const int row = b / NBF, j = b - row * NBF;
+    const int k = j % NS;
+    const C* s = src + row * RS;
+    C v[R];
+    if constexpr (NBF % 16 == 0) {
+      const C* sj = s + pidx(j);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = sj[r * (NBF + NBF / 16)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = s[pidx(j + r * NBF)];
+    }
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], PT ? tw[(r - 1) * NS + k] : tw[r * k * TWSTEP]);
+    }
+    Dft<R, C>::run(v);
+    const int o0 = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) f(row, o0 + r * NS, v[r]);
+  }
+}
+
 // Per-pass twiddle tables: pass s (NS_s > 1) owns (R_s - 1) NS_s entries
 // W_N^(r k N / (NS_s R_s)) at [r - 1][k], one after the other.
 constexpr int ct_pass_tw_entries(int N) {
@@ -315,6 +348,20 @@ __device__ __forceinline__ C* ct_passes_pt(C* src, C* dst, const C* tw) {
     ct_pass<R, N, TB, NS, C, NT, true>(src, dst, tw + OFF);
     __syncthreads();
     return ct_passes_pt<N, TB, S + 1, NS * R, C, NT, (NS > 1 ? OFF + (R - 1) * NS : OFF)>(dst, src, tw);
+  }
+}
+
+// ct_passes_pt whose last pass hands its outputs to f (ct_pass_apply).
+template <int N, int TB, int S, int NS, typename C, int NT, int OFF, class F>
+__device__ __forceinline__ void ct_passes_pt_apply(C* src, C* dst, const C* tw, F& f) {
+  constexpr CPlan P = PlanOf<N>::p;
+  constexpr int R = P.r[S];
+  if constexpr (S == P.ns - 1) {
+    ct_pass_apply<R, N, TB, NS, C, NT, true>(src, tw + OFF, f);
+  } else {
+    ct_pass<R, N, TB, NS, C, NT, true>(src, dst, tw + OFF);
+    __syncthreads();
+    ct_passes_pt_apply<N, TB, S + 1, NS * R, C, NT, (NS > 1 ? OFF + (R - 1) * NS : OFF)>(dst, src, tw, f);
   }
 }
 

@@ -114,10 +114,11 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
       pf[k] = e < tot ? __ldg(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
   };
+  const int band = n - 2 * M - 1;  // frequencies M < k < n - M are zero
   auto build = [&](int c) {
-    for (int e = tid; e < FB * n; e += FNT) {
-      const int ii = e / n, k = e - ii * n;
-      if (k > M && k < n - M) bufA[ii * rs + pidx(k)] = make_float2(0.f, 0.f);
+    for (int e = tid; e < FB * band; e += FNT) {
+      const int ii = e / band, k = M + 1 + (e - ii * band);
+      bufA[ii * rs + pidx(k)] = make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int k = 0; k < PF; ++k) {
@@ -127,96 +128,97 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
     const float4* src = a.fin[c] + boff;
     for (int e = tid + PF * FNT; e < tot; e += FNT) pack_z(bufA, rs, n, e, rows, __ldg(src + e));
   };
-  // north/south grid rows of one transformed component
-  auto write_grid = [&](const C* res, float* g) {
-    float* gbase = g + (size_t)r * d.nlat * n;
-    for (int e = tid; e < rows * n; e += FNT) {
-      const int ii = e / n, j = e - ii * n;
-      const C z = res[ii * rs + pidx(j)];
-      const int ith = i0 + ii;
-      gbase[(size_t)ith * n + j] = z.x;
-      gbase[(size_t)(d.nlat - 1 - ith) * n + j] = -z.y;
-    }
-  };
-
   const float ur = 0.f, wr = 0.f, jr = 0.f, br = 0.f;
   const float adv = -a.rf, mrf = -a.rf, lfr = a.lf;
 
+  // consumer of one transformed component: grid rows or the products
+  // inputs: T phase [u_th, u_ph, g_r, g_th, g_ph, T]; V phase [u_th, u_ph,
+  // w_th, w_ph, j_th, j_ph, b_th, b_ph]; M phase [u_th, u_ph, b_th, b_ph]
+  int c = 0;
+  float s_r = (PH == FUSED_TEMPERATURE) ? (float)a.sources[r] : 0.f;
+  auto consume = [&](int ii, int j, C z) {
+    if (PH == FUSED_GRID || (PH == FUSED_TEMPERATURE && c == 5)) {
+      if (ii < rows) {
+        float* gbase = (PH == FUSED_GRID ? a.gout[c] : a.gout[0]) + (size_t)r * d.nlat * n;
+        const int ith = i0 + ii;
+        gbase[(size_t)ith * n + j] = z.x;
+        gbase[(size_t)(d.nlat - 1 - ith) * n + j] = -z.y;
+      }
+      return;
+    }
+    const int q = ii * rs + pidx(j);
+    const float vN = z.x, vS = -z.y;
+    if (PH == FUSED_TEMPERATURE) {
+      // -(u_r g_r + u_th g_th + u_ph g_ph) + S(r)
+      if (c == 0) {
+        u0[q] = make_float2(vN, vS);
+      } else if (c == 1) {
+        u1[q] = make_float2(vN, vS);
+      } else if (c == 2) {
+        acc0[q] = make_float2(ur * vN, ur * vS);
+      } else if (c == 3) {
+        const C u = u0[q], t = acc0[q];
+        acc0[q] = make_float2(t.x + u.x * vN, t.y + u.y * vS);
+      } else {
+        const C u = u1[q], t = acc0[q];
+        float xN = -(t.x + u.x * vN), xS = -(t.y + u.y * vS);
+        if (s_r != 0.f) { xN += s_r; xS += s_r; }
+        acc0[q] = make_float2(xN, xS);
+      }
+    } else if (PH == FUSED_VELOCITY) {
+      // theta: adv (u_ph w_r - u_r w_ph) + mrf (-ct u_ph) + lf (j_ph b_r - j_r b_ph)
+      // phi:   adv (u_r w_th - u_th w_r) + mrf (ct u_th + st u_r) + lf (j_r b_th - j_th b_r)
+      // even inputs (theta components) feed the phi product, odd ones the theta product
+      C* acc = (c & 1) ? acc0 : acc1;
+      C t = acc[q];
+      switch (c) {
+        case 0: {
+          const float ct = sct[j], st = sst[j];
+          t.x += adv * (-(vN * wr)) + mrf * (ct * vN + st * ur);
+          t.y += adv * (-(vS * wr)) + mrf * (ct * vS + st * ur);
+          break;
+        }
+        case 1: {
+          const float ct = sct[j];
+          t.x += adv * (vN * wr) + mrf * (-ct * vN);
+          t.y += adv * (vS * wr) + mrf * (-ct * vS);
+          break;
+        }
+        case 2: t.x += adv * (ur * vN); t.y += adv * (ur * vS); break;
+        case 3: t.x += adv * (-(ur * vN)); t.y += adv * (-(ur * vS)); break;
+        case 4: t.x += lfr * (-(vN * br)); t.y += lfr * (-(vS * br)); break;
+        case 5: t.x += lfr * (vN * br); t.y += lfr * (vS * br); break;
+        case 6: t.x += lfr * (jr * vN); t.y += lfr * (jr * vS); break;
+        default: t.x += lfr * (-(jr * vN)); t.y += lfr * (-(jr * vS)); break;
+      }
+      acc[q] = t;
+    } else {
+      // induction: theta u_ph b_r - u_r b_ph, phi u_r b_th - u_th b_r
+      C* acc = (c & 1) ? acc0 : acc1;
+      C t = acc[q];
+      switch (c) {
+        case 0: t.x += -(vN * br); t.y += -(vS * br); break;
+        case 1: t.x += vN * br; t.y += vS * br; break;
+        case 2: t.x += ur * vN; t.y += ur * vS; break;
+        default: t.x += -(ur * vN); t.y += -(ur * vS); break;
+      }
+      acc[q] = t;
+    }
+  };
+
   prefetch(0);
-  for (int c = 0; c < a.nin; ++c) {
+  for (c = 0; c < a.nin; ++c) {
     build(c);
     __syncthreads();
     if (c + 1 < a.nin) prefetch(c + 1);
-    const C* res = run_fft<N>(bufA, bufB, stw, p);
-    if (PH == FUSED_GRID) {
-      write_grid(res, a.gout[c]);
-    } else if (PH == FUSED_TEMPERATURE && c == 5) {
-      write_grid(res, a.gout[0]);  // the temperature grid itself
+    if constexpr (N > 0) {
+      // the last Stockham pass feeds the consumer directly
+      ct_passes_pt_apply<N, FB, 0, 1, C, FNT, 0>(bufA, bufB, stw, consume);
     } else {
-      // inputs: T phase [u_th, u_ph, g_r, g_th, g_ph, T]; V phase [u_th, u_ph,
-      // w_th, w_ph, j_th, j_ph, b_th, b_ph]; M phase [u_th, u_ph, b_th, b_ph]
-      const float s = (PH == FUSED_TEMPERATURE) ? (float)a.sources[r] : 0.f;
+      const C* res = run_fft<N>(bufA, bufB, stw, p);
       for (int e = tid; e < FB * n; e += FNT) {
         const int ii = e / n, j = e - ii * n;
-        const int q = ii * rs + pidx(j);
-        const C z = res[q];
-        const float vN = z.x, vS = -z.y;
-        if (PH == FUSED_TEMPERATURE) {
-          // -(u_r g_r + u_th g_th + u_ph g_ph) + S(r)
-          if (c == 0) {
-            u0[q] = make_float2(vN, vS);
-          } else if (c == 1) {
-            u1[q] = make_float2(vN, vS);
-          } else if (c == 2) {
-            acc0[q] = make_float2(ur * vN, ur * vS);
-          } else if (c == 3) {
-            const C u = u0[q], t = acc0[q];
-            acc0[q] = make_float2(t.x + u.x * vN, t.y + u.y * vS);
-          } else {
-            const C u = u1[q], t = acc0[q];
-            float xN = -(t.x + u.x * vN), xS = -(t.y + u.y * vS);
-            if (s != 0.f) { xN += s; xS += s; }
-            acc0[q] = make_float2(xN, xS);
-          }
-        } else if (PH == FUSED_VELOCITY) {
-          // theta: adv (u_ph w_r - u_r w_ph) + mrf (-ct u_ph) + lf (j_ph b_r - j_r b_ph)
-          // phi:   adv (u_r w_th - u_th w_r) + mrf (ct u_th + st u_r) + lf (j_r b_th - j_th b_r)
-          // even inputs (theta components) feed the phi product, odd ones the theta product
-          C* acc = (c & 1) ? acc0 : acc1;
-          C t = acc[q];
-          switch (c) {
-            case 0: {
-              const float ct = sct[j], st = sst[j];
-              t.x += adv * (-(vN * wr)) + mrf * (ct * vN + st * ur);
-              t.y += adv * (-(vS * wr)) + mrf * (ct * vS + st * ur);
-              break;
-            }
-            case 1: {
-              const float ct = sct[j];
-              t.x += adv * (vN * wr) + mrf * (-ct * vN);
-              t.y += adv * (vS * wr) + mrf * (-ct * vS);
-              break;
-            }
-            case 2: t.x += adv * (ur * vN); t.y += adv * (ur * vS); break;
-            case 3: t.x += adv * (-(ur * vN)); t.y += adv * (-(ur * vS)); break;
-            case 4: t.x += lfr * (-(vN * br)); t.y += lfr * (-(vS * br)); break;
-            case 5: t.x += lfr * (vN * br); t.y += lfr * (vS * br); break;
-            case 6: t.x += lfr * (jr * vN); t.y += lfr * (jr * vS); break;
-            default: t.x += lfr * (-(jr * vN)); t.y += lfr * (-(jr * vS)); break;
-          }
-          acc[q] = t;
-        } else {
-          // induction: theta u_ph b_r - u_r b_ph, phi u_r b_th - u_th b_r
-          C* acc = (c & 1) ? acc0 : acc1;
-          C t = acc[q];
-          switch (c) {
-            case 0: t.x += -(vN * br); t.y += -(vS * br); break;
-            case 1: t.x += vN * br; t.y += vS * br; break;
-            case 2: t.x += ur * vN; t.y += ur * vS; break;
-            default: t.x += -(ur * vN); t.y += -(ur * vS); break;
-          }
-          acc[q] = t;
-        }
+        consume(ii, j, res[ii * rs + pidx(j)]);
       }
     }
     __syncthreads();
