@@ -4,94 +4,151 @@
 
 namespace gd {
 
+// Radial operators walk r with a register window of 2 KL + 1 levels: each
+// thread owns one mode j and RB_R consecutive levels, so every coefficient is
+// read once per block of levels (plus the window halo) instead of once per
+// band entry.  Band sums run over the same levels in the same order as the
+// banded matrix-vector product they restate.
+constexpr int RB_R = 16;
+
 // compute_all_gradients_spectral! (src/scalar_field_common.jl:125-345):
 // theta derivative by the reference's recurrence coefficients (:158,171), phi
 // derivative i m, radial derivative by the banded D1, then x 1/r on the
 // angular components (:317-321).  In m-major order (l +- 1, m) sits at j +- 1.
+template <int KL>
 __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __restrict__ mof,
                             const double* __restrict__ rinv, const double* __restrict__ d1,
                             const double* __restrict__ T, double* __restrict__ gth, double* __restrict__ gph,
                             double* __restrict__ gr) {
+  constexpr int NB = 2 * KL + 1;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
+  const int k0 = blockIdx.y * RB_R;
   if (j >= d.nlm) return;
   const int l = lof[j], m = mof[j];
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
-  const double* Tre = T;
-  const double* Tim = T + plane;
-  const size_t at = (size_t)k * NM + j;
-  double dr = 0.0, di = 0.0;
-  if (l + 1 <= d.L) {
-    const double Ap = sqrt((double)(l + 1) * (l + 1) - (double)m * m) * sqrt((double)(l + 1 + m) * (double)(l + 1 - m)) /
-                      (2.0 * l + 1.0);
-    dr += Ap * Tre[at + 1];
-    di += Ap * Tim[at + 1];
+  const int N = d.nr;
+  const bool up = l + 1 <= d.L, dn = l >= 1 && l - 1 >= m;
+  const double Ap = up ? sqrt((double)(l + 1) * (l + 1) - (double)m * m) * sqrt((double)(l + 1 + m) * (double)(l + 1 - m)) /
+                             (2.0 * l + 1.0)
+                       : 0.0;
+  const double Am = dn ? -sqrt((double)l * l - (double)m * m) * sqrt((double)(l + m) * (double)(l - m)) / (2.0 * l - 1.0)
+                       : 0.0;
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const double* P = T + c * plane;
+    double w[NB];
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+      const int kk = k0 - KL + t;
+      w[t] = (kk >= 0 && kk < N) ? P[(size_t)kk * NM + j] : 0.0;
+    }
+    for (int b = 0; b < RB_R; ++b) {
+      const int k = k0 + b;
+      if (k >= N) break;
+      const size_t at = (size_t)k * NM + j;
+      double sr = 0.0;
+#pragma unroll
+      for (int t = 0; t < NB; ++t) {
+        const int jj = k - KL + t;
+        if (jj >= 0 && jj < N) sr += d1[(KL + k - jj) + (size_t)NB * jj] * w[t];
+      }
+      gr[c * plane + at] = sr;
+#pragma unroll
+      for (int t = 0; t < NB - 1; ++t) w[t] = w[t + 1];
+      const int nx = k + KL + 1;
+      w[NB - 1] = nx < N ? P[(size_t)nx * NM + j] : 0.0;
+    }
   }
-  if (l >= 1 && l - 1 >= m) {
-    const double Am = -sqrt((double)l * l - (double)m * m) * sqrt((double)(l + m) * (double)(l - m)) / (2.0 * l - 1.0);
-    dr += Am * Tre[at - 1];
-    di += Am * Tim[at - 1];
+  for (int b = 0; b < RB_R; ++b) {
+    const int k = k0 + b;
+    if (k >= N) break;
+    const size_t at = (size_t)k * NM + j;
+    double dr = 0.0, di = 0.0;
+    if (up) {
+      dr += Ap * T[at + 1];
+      di += Ap * T[plane + at + 1];
+    }
+    if (dn) {
+      dr += Am * T[at - 1];
+      di += Am * T[plane + at - 1];
+    }
+    const double ri = rinv[k];
+    gth[at] = dr * ri;
+    gth[plane + at] = di * ri;
+    gph[at] = (-(double)m * T[plane + at]) * ri;
+    gph[plane + at] = ((double)m * T[at]) * ri;
   }
-  const double ri = rinv[k];
-  gth[at] = dr * ri;
-  gth[plane + at] = di * ri;
-  gph[at] = (-(double)m * Tim[at]) * ri;
-  gph[plane + at] = ((double)m * Tre[at]) * ri;
-  const int nbw = 2 * d.kl + 1;
-  double sr = 0.0, si = 0.0;
-  const int j0 = k - d.kl > 0 ? k - d.kl : 0;
-  const int j1 = k + d.kl < d.nr - 1 ? k + d.kl : d.nr - 1;
-  for (int jj = j0; jj <= j1; ++jj) {
-    const double cf = d1[(d.kl + k - jj) + (size_t)nbw * jj];
-    sr += cf * Tre[(size_t)jj * NM + j];
-    si += cf * Tim[(size_t)jj * NM + j];
-  }
-  gr[at] = sr;
-  gr[plane + at] = si;
 }
 
 void launch_gradients(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                       const double* d1, const double* T, double* gth, double* gph, double* gr) {
-  dim3 grid(ceil_div(d.nlm, 128), d.nr);
-  k_gradients<<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr);
+  dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
+  switch (d.kl) {
+    case 1: k_gradients<1><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr); break;
+    case 2: k_gradients<2><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr); break;
+    case 3: k_gradients<3><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr); break;
+    default: k_gradients<4><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr); break;
+  }
 }
 
 // compute_vorticity_spectral_full! (src/velocity.jl:340-441) and
 // compute_current_density_spectral! (src/magnetic.jl:253-349):
 //   curl_tor = l(l+1)/r^2 P - D2 P - (2/r) D1 P,   curl_pol = -l(l+1)/r^2 T.
+template <int KL>
 __global__ void k_curl(Dims d, const int* __restrict__ lof, const double* __restrict__ rinv,
                        const double* __restrict__ rinv2, const double* __restrict__ d1,
                        const double* __restrict__ d2, const double* __restrict__ tor,
                        const double* __restrict__ pol, double* __restrict__ otor, double* __restrict__ opol) {
+  constexpr int NB = 2 * KL + 1;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
+  const int k0 = blockIdx.y * RB_R;
   if (j >= d.nlm) return;
   const double lf = (double)lof[j] * (lof[j] + 1.0);
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
-  const int nbw = 2 * d.kl + 1;
-  const int j0 = k - d.kl > 0 ? k - d.kl : 0;
-  const int j1 = k + d.kl < d.nr - 1 ? k + d.kl : d.nr - 1;
+  const int N = d.nr;
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
     const double* P = pol + c * plane;
-    double a1 = 0.0, a2 = 0.0;
-    for (int jj = j0; jj <= j1; ++jj) {
-      const size_t q = (d.kl + k - jj) + (size_t)nbw * jj;
-      const double v = P[(size_t)jj * NM + j];
-      a1 += d1[q] * v;
-      a2 += d2[q] * v;
+    double w[NB];
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+      const int kk = k0 - KL + t;
+      w[t] = (kk >= 0 && kk < N) ? P[(size_t)kk * NM + j] : 0.0;
     }
-    const size_t at = (size_t)k * NM + j;
-    otor[c * plane + at] = lf * rinv2[k] * P[at] - a2 - 2.0 * rinv[k] * a1;
-    opol[c * plane + at] = -lf * rinv2[k] * tor[c * plane + at];
+    for (int b = 0; b < RB_R; ++b) {
+      const int k = k0 + b;
+      if (k >= N) break;
+      double a1 = 0.0, a2 = 0.0;
+#pragma unroll
+      for (int t = 0; t < NB; ++t) {
+        const int jj = k - KL + t;
+        if (jj >= 0 && jj < N) {
+          const size_t q = (KL + k - jj) + (size_t)NB * jj;
+          a1 += d1[q] * w[t];
+          a2 += d2[q] * w[t];
+        }
+      }
+      const size_t at = (size_t)k * NM + j;
+      otor[c * plane + at] = lf * rinv2[k] * w[KL] - a2 - 2.0 * rinv[k] * a1;
+      opol[c * plane + at] = -lf * rinv2[k] * tor[c * plane + at];
+#pragma unroll
+      for (int t = 0; t < NB - 1; ++t) w[t] = w[t + 1];
+      const int nx = k + KL + 1;
+      w[NB - 1] = nx < N ? P[(size_t)nx * NM + j] : 0.0;
+    }
   }
 }
 
 void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* rinv, const double* rinv2,
                  const double* d1, const double* d2, const double* tor, const double* pol, double* otor,
                  double* opol) {
-  dim3 grid(ceil_div(d.nlm, 128), d.nr);
-  k_curl<<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol);
+  dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
+  switch (d.kl) {
+    case 1: k_curl<1><<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol); break;
+    case 2: k_curl<2><<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol); break;
+    case 3: k_curl<3><<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol); break;
+    default: k_curl<4><<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol); break;
+  }
 }
 
 // apply_temperature_boundary_conditions_spectral! (src/thermal.jl:262-303):
