@@ -62,24 +62,36 @@ def workload_params():
 # algorithmic work per kernel launch (bytes or flops), for the roofline
 # ---------------------------------------------------------------------------
 def kernel_work(name, p, nlm, precision):
+    """Algorithmic work of one launch: {"flops": F or None, "bytes": B or None}.
+
+    Legendre: flops count the contraction once (not the three split-TF32
+    products); bytes are the coefficients, the Fourier components and the
+    table (images) each read or written once."""
     L, nlat, nlon, nr = p["lmax"], p["nlat"], p["nlon"], p["nr"]
+    nth = nlat // 2
     G = nlat * nlon * nr                      # grid points per field
     F = nr * (L + 1) * nlat                   # Fourier coefficients per component
     S = 2 * nr * nlm                          # spectral doubles per field
     rb = 8 if precision == "fp64" else 4      # grid real bytes
     cb = 2 * rb                               # Fourier complex bytes
+    if precision == "fp64":
+        table = nlm * nth * 8                 # one FP64 table [mode][north colatitude]
+        synth_table = anal_table = table
+    else:
+        chunk = 32768                         # split-TF32 hi + lo image chunk of 128 x 32
+        ntile = -(-nth // 128)
+        nck = lambda k: -(-k // 32)  # noqa: E731
+        synth_table = chunk * ntile * sum(nck((L - m + 2) // 2) + nck((L - m + 1) // 2) for m in range(L + 1))
+        anal_table = chunk * (L + 1) * 2 * (-(-nth // 32))
     legendre = {
-        # (flops per launch, launches per step are counted live)
-        "legendre_synth_scalar": 2.0 * nlm * nlat * nr * 4,
-        "legendre_synth_vector": 8.0 * nlm * nlat * nr,
-        "legendre_analysis_scalar": 2.0 * nlm * nlat * nr,
-        "legendre_analysis_vector": 8.0 * nlm * nlat * nr,
+        "legendre_synth_scalar": (2.0 * nlm * nlat * nr * 4, 4 * S * 8 + 4 * F * cb + synth_table),
+        "legendre_synth_vector": (8.0 * nlm * nlat * nr, 2 * S * 8 + 2 * F * cb + 2 * synth_table),
+        "legendre_analysis_scalar": (2.0 * nlm * nlat * nr, F * cb + S * 8 + anal_table),
+        "legendre_analysis_vector": (8.0 * nlm * nlat * nr, 2 * F * cb + 2 * S * 8 + 2 * anal_table),
     }
-    for k, v in legendre.items():
+    for k, (fl, by) in legendre.items():
         if name.startswith(k):
-            return ("flops", v)
-    if name.startswith("fft_synth"):
-        return None  # component count varies per launch (4 or 2); handled by caller
+            return {"flops": fl, "bytes": by}
     table = {
         # fused phase kernels: blocked Fourier components in, folded transforms out
         "fused_temperature": 6 * F * cb + G * rb + F * cb,
@@ -95,7 +107,22 @@ def kernel_work(name, p, nlm, precision):
     }
     for k, v in table.items():
         if name.startswith(k):
-            return ("bytes", v)
+            return {"flops": None, "bytes": v}
+    return None
+
+
+def measured_traffic(name):
+    """DRAM bytes per launch of a kernel from the committed ncu summary of the
+    headline workload (profiles/dram_traffic_shell_l255_nr129.txt), or None."""
+    if WORKLOAD != "shell_l255_nr129":
+        return None
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "dram_traffic_shell_l255_nr129.txt")):
+            f = line.split()
+            if len(f) >= 2 and not line.startswith("#") and f[0] == name:
+                return float(f[1])
+    except OSError:
+        pass
     return None
 
 
@@ -307,11 +334,10 @@ def main():
             ncomp = (4 + 2 * 4) if "synth" in name else (1 + 2 + 2)
             ent["gbs"] = fft_bytes(p, ncomp, precision) / (ms / nprof / 1e3) / 1e9
         elif w is not None:
-            kind, amount = w
-            if kind == "flops":
-                ent["tflops"] = amount / (per / 1e3) / 1e12
-            else:
-                ent["gbs"] = amount / (per / 1e3) / 1e9
+            if w["flops"] is not None:
+                ent["tflops"] = w["flops"] / (per / 1e3) / 1e12
+            if w["bytes"] is not None:
+                ent["gbs"] = w["bytes"] / (per / 1e3) / 1e9
         kernels.append(ent)
     tot = sum(v[0] for v in prof.values())
     for ent in kernels:
@@ -327,17 +353,25 @@ def main():
     top = kernels[0] if kernels else None
     roofline = None
     if top is not None:
+        bounds = []
         if "gbs" in top:
-            roofline = {"kernel": top["name"], "bound": "hbm", "achieved": top["gbs"], "peak": hbm_peak,
-                        "unit": "GB/s", "frac": top["gbs"] / hbm_peak, "traffic": None,
-                        "peak_source": peak_src}
-        elif "tflops" in top:
+            bounds.append({"bound": "hbm", "achieved": top["gbs"], "peak": hbm_peak, "unit": "GB/s",
+                           "frac": top["gbs"] / hbm_peak, "peak_source": peak_src + " HBM copy bandwidth"})
+        if "tflops" in top:
             if top["name"].endswith("fp64"):
                 pk, src = 40.0, "nominal FP64 tensor (no measured FP64 peak on this pool)"
             else:
-                pk, src = peaks.get("bf16_tflops", 1590.0) / 2.0, "half the measured bf16 peak (tf32 rate)"
-            roofline = {"kernel": top["name"], "bound": "tensor", "achieved": top["tflops"], "peak": pk,
-                        "unit": "TFLOP/s", "frac": top["tflops"] / pk, "traffic": None, "peak_source": src}
+                pk, src = peaks.get("bf16_tflops", 1590.0) / 2.0, "half the measured bf16 burst peak (tf32 rate)"
+            bounds.append({"bound": "tensor", "achieved": top["tflops"], "peak": pk, "unit": "TFLOP/s",
+                           "frac": top["tflops"] / pk, "peak_source": src})
+        if bounds:
+            bounds.sort(key=lambda b: -b["frac"])  # the binding roof is the one closest to its limit
+            roofline = dict(bounds[0])
+            roofline["kernel"] = top["name"]
+            roofline["traffic"] = measured_traffic(top["name"])
+            roofline["traffic_unit"] = "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)"
+            if len(bounds) > 1:
+                roofline["other"] = {k: bounds[1][k] for k in ("bound", "achieved", "peak", "unit", "frac")}
 
     # ---- FP64 reference step on the GPU (denominator of the metric) ----
     fp64_value = None
