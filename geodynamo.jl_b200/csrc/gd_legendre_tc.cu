@@ -19,6 +19,8 @@
 // Arithmetic of SHTnsKit.synthesis / analysis / SHsphtor_to_spat /
 // spat_to_SHsphtor as called per shell in src/shtnskit_field_functions.jl
 // (:102-123, :218-239, :252-321); all shells and fields in one launch.
+#include <algorithm>
+
 #include "gd_internal.cuh"
 #include "gd_mixed_kernels.cuh"
 #include "gd_tc.cuh"
@@ -189,7 +191,7 @@ template <bool VEC>
 __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* __restrict__ moff,
                                                       const long* __restrict__ cofs, const float* __restrict__ imgP,
                                                       const float* __restrict__ imgD, const double* __restrict__ sinv,
-                                                      TcSynthArgs a) {
+                                                      TcSynthArgs a, int ntt, int ncol) {
   constexpr int S = 2;
   constexpr int NCS = VEC ? TC_N2 : 2 * TC_N2;   // columns per CTA: vector 128, scalar 256
   constexpr int A_FL = (VEC ? 2 : 1) * CHUNK_FLOATS;
@@ -208,13 +210,9 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
   const double** colp = reinterpret_cast<const double**>(empty + S + 2);
   long long* colo = reinterpret_cast<long long*>(colp + NCS);
 
-  const int m = blockIdx.z, tile = blockIdx.y;
-  const int L = d.L, mb = moff[m];
+  const int L = d.L;
   const size_t NM = d.nlm;
   const int Ntot = a.nf * d.nr * 2;
-  const int n0 = blockIdx.x * NCS;
-  const int r0 = blockIdx.x * 32;
-  if (tile * TC_M >= d.nth || (VEC ? r0 >= d.nr : n0 >= Ntot)) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0)
     for (int s = 0; s < S; ++s) {
@@ -222,6 +220,23 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
       mbar_init(&empty[s], 1);
     }
   if (warp == 0) tmem_alloc(tslot, NCOL);
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = *tslot;
+
+  bool ok = true;
+  int issued = -1;  // loader thread 0 of a group: last use of its stage with bulk copies issued
+  int gs = 0;       // pipeline steps of the earlier tiles (stage and phase of a step follow from gs + it)
+  const int ntiles = (d.M + 1) * ntt * ncol;
+  // persistent CTA: tiles (m, theta tile, column tile), m-major so the
+  // deepest columns (small m) are spread first
+  for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+  const int m = tt / (ntt * ncol), tile = (tt / ncol) % ntt, ct = tt % ncol;
+  const int mb = moff[m];
+  const int n0 = ct * NCS;
+  const int r0 = ct * 32;
+  __syncthreads();  // the previous tile's epilogue is done with TMEM and the column tables
   if (!VEC) {
     for (int c = tid; c < NCS; c += blockDim.x) {
       const int ng = n0 + c;
@@ -240,11 +255,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
         colo[c >> 1] = ob;
       }
     }
+    __syncthreads();
   }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  const uint32_t tmem = *tslot;
 
   const int nc0 = nck_h(L, m, 0), nc1 = nck_h(L, m, 1);
   const int T = nc0 + nc1;
@@ -256,16 +268,14 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
     p = it < 2 * nc1 ? (it & 1) : 0;
   };
 
-  bool ok = true;
-  int issued = -1;  // loader thread 0 of a group: last use of its stage with bulk copies issued
   if (warp < 8) {
     const int g = warp >> 2, gw = warp & 3, gt = tid & 127;
     float* A = stg + g * ST_FL;
     float* B = A + A_FL;
     constexpr int RPT = NCS / 4;              // coefficient rows per thread
     constexpr int HALF = RPT > 32 ? 32 : RPT; // loads in flight per batch
-    for (int it = g; it < T; it += 2) {
-      const int u = it >> 1;
+    for (int it = (g - gs) & 1; it < T; it += 2) {
+      const int u = (gs + it) >> 1;
       if (u >= 1 && !mbar_wait(&empty[g], (u - 1) & 1, a.err)) {
         ok = false;
         break;
@@ -308,8 +318,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
     }
   } else {
     for (int it = 0; it < T; ++it) {
-      const int s = it & 1;
-      if (!mbar_wait(&full[s], (it >> 1) & 1, a.err)) {
+      const int s = (gs + it) & 1;
+      if (!mbar_wait(&full[s], ((gs + it) >> 1) & 1, a.err)) {
         ok = false;
         break;
       }
@@ -328,15 +338,13 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
       __syncwarp();
     }
   }
-  // drain: the last MMA batch of each stage
+  // drain: the last MMA batch of each stage in this tile
   if (ok) {
 #pragma unroll
-    for (int s = 0; s < S; ++s)
-      if (s < T) ok = mbar_wait(&empty[s], ((T - 1 - s) >> 1) & 1, a.err) && ok;
+    for (int q = 1; q <= S; ++q)
+      if (T - q >= 0) ok = mbar_wait(&empty[(gs + T - q) & 1], ((gs + T - q) >> 1) & 1, a.err) && ok;
   }
   ok = __syncthreads_and(ok);
-  // after an expired wait, let the last bulk copies land before the CTA exits
-  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err);
   fence_after_sync();
   if (ok && warp < 8) {
     const int q = warp & 3, half = warp >> 2;
@@ -415,6 +423,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
     }
   }
   fence_before_sync();
+  gs += T;
+  }  // tiles
+  // after an expired wait, let the last bulk copies land before the CTA exits
+  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err);
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, NCOL);
 }
@@ -431,7 +443,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
 template <bool VEC>
 __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const int* __restrict__ moff,
                                                          const float* __restrict__ img0,
-                                                         const float* __restrict__ img1, TcAnalysisArgs a) {
+                                                         const float* __restrict__ img1, TcAnalysisArgs a,
+                                                         int ncol) {
   constexpr int S = 2;
   constexpr int NC = VEC ? TC_N : TC_N2;         // columns
   constexpr int A_FL = (VEC ? 2 : 1) * CHUNK_FLOATS;
@@ -450,13 +463,9 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   long long* colin = reinterpret_cast<long long*>(empty + S + 2);
   double** colout = reinterpret_cast<double**>(colin + NC / 2);
 
-  const int m = blockIdx.z;
-  const int L = d.L, mb = moff[m];
+  const int L = d.L;
   const size_t NM = d.nlm;
   const int Ntot = a.nf * d.nr * 2;
-  const int n0 = blockIdx.x * NC;
-  const int r0 = blockIdx.x * 16;
-  if (VEC ? r0 >= d.nr : n0 >= Ntot) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0)
     for (int s = 0; s < S; ++s) {
@@ -464,6 +473,23 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
       mbar_init(&empty[s], 1);
     }
   if (warp == 0) tmem_alloc(tslot, NCOL);
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = *tslot;
+  const int nthc = (d.nth + TC_K - 1) / TC_K;
+
+  bool ok = true;
+  int issued = -1;  // loader thread 0 of a group: last use of its stage with bulk copies issued
+  int gs = 0;       // pipeline steps of the earlier tiles
+  const int ntiles = (d.M + 1) * ncol;
+  // persistent CTA: tiles (m, column tile), m-major
+  for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+  const int m = tt / ncol, ct = tt % ncol;
+  const int mb = moff[m];
+  const int n0 = ct * NC;
+  const int r0 = ct * 16;
+  __syncthreads();  // the previous tile's epilogue is done with TMEM and the column tables
   if (!VEC) {
     for (int c = tid; c < NC; c += blockDim.x) {
       const int ng = n0 + c;
@@ -483,25 +509,19 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
         colin[c >> 1] = ib;
       }
     }
+    __syncthreads();
   }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  const uint32_t tmem = *tslot;
 
   const int k1 = kpar(L, m, 1);
   const int np = k1 > 0 ? 2 : 1;
-  const int nthc = (d.nth + TC_K - 1) / TC_K;
   const int T = nthc * np;
 
-  bool ok = true;
-  int issued = -1;  // loader thread 0 of a group: last use of its stage with bulk copies issued
   if (warp < 8) {
     const int g = warp >> 2, gw = warp & 3, gt = tid & 127;
     float* A = stg + g * ST_FL;
     float* B = A + A_FL;
-    for (int it = g; it < T; it += 2) {
-      const int u = it >> 1;
+    for (int it = (g - gs) & 1; it < T; it += 2) {
+      const int u = (gs + it) >> 1;
       if (u >= 1 && !mbar_wait(&empty[g], (u - 1) & 1, a.err)) {
         ok = false;
         break;
@@ -556,8 +576,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
     }
   } else {
     for (int it = 0; it < T; ++it) {
-      const int s = it & 1;
-      if (!mbar_wait(&full[s], (it >> 1) & 1, a.err)) {
+      const int s = (gs + it) & 1;
+      if (!mbar_wait(&full[s], ((gs + it) >> 1) & 1, a.err)) {
         ok = false;
         break;
       }
@@ -578,13 +598,13 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
       __syncwarp();
     }
   }
+  // drain: the last MMA batch of each stage in this tile
   if (ok) {
 #pragma unroll
-    for (int s = 0; s < S; ++s)
-      if (s < T) ok = mbar_wait(&empty[s], ((T - 1 - s) >> 1) & 1, a.err) && ok;
+    for (int q = 1; q <= S; ++q)
+      if (T - q >= 0) ok = mbar_wait(&empty[(gs + T - q) & 1], ((gs + T - q) >> 1) & 1, a.err) && ok;
   }
   ok = __syncthreads_and(ok);
-  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err);
   fence_after_sync();
   if (ok && warp < 8) {
     const int q = warp & 3, half = warp >> 2;
@@ -646,6 +666,9 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
     }
   }
   fence_before_sync();
+  gs += T;
+  }  // tiles
+  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err);
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, NCOL);
 }
@@ -676,16 +699,32 @@ static void set_attrs() {
   g_attr_done = true;
 }
 
+// One persistent CTA per SM (at most one tile each when there are fewer tiles).
+static int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
 void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long* cofs, const float* imgP,
                      const float* imgD, const double* sinv, const TcSynthArgs& a, bool vec) {
   set_attrs();
-  const int ntile = (d.nth + TC_M - 1) / TC_M;
+  const int ntt = (d.nth + TC_M - 1) / TC_M;
   if (!vec) {
-    dim3 grid(ceil_div(a.nf * d.nr * 2, 2 * TC_N2), ntile, d.M + 1);
-    k_tc_synth3<false><<<grid, WS_THREADS, synth_smem(false), s>>>(d, moff, cofs, imgP, imgD, sinv, a);
+    const int ncol = ceil_div(a.nf * d.nr * 2, 2 * TC_N2);
+    const int ntiles = (d.M + 1) * ntt * ncol;
+    k_tc_synth3<false><<<std::min(ntiles, sm_count()), WS_THREADS, synth_smem(false), s>>>(d, moff, cofs, imgP,
+                                                                                          imgD, sinv, a, ntt, ncol);
   } else {
-    dim3 grid(ceil_div(d.nr, 32), ntile, d.M + 1);
-    k_tc_synth3<true><<<grid, WS_THREADS, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD, sinv, a);
+    const int ncol = ceil_div(d.nr, 32);
+    const int ntiles = (d.M + 1) * ntt * ncol;
+    k_tc_synth3<true><<<std::min(ntiles, sm_count()), WS_THREADS, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD,
+                                                                                        sinv, a, ntt, ncol);
   }
 }
 
@@ -693,11 +732,15 @@ void launch_tc_analysis(cudaStream_t s, const Dims& d, const int* moff, const fl
                         const TcAnalysisArgs& a) {
   set_attrs();
   if (a.epi == EPI_SCALAR) {
-    dim3 grid(ceil_div(a.nf * d.nr * 2, TC_N2), 1, d.M + 1);
-    k_tc_analysis3<false><<<grid, WS_THREADS, analysis_smem(false), s>>>(d, moff, img0, img1, a);
+    const int ncol = ceil_div(a.nf * d.nr * 2, TC_N2);
+    const int ntiles = (d.M + 1) * ncol;
+    k_tc_analysis3<false><<<std::min(ntiles, sm_count()), WS_THREADS, analysis_smem(false), s>>>(d, moff, img0,
+                                                                                                img1, a, ncol);
   } else {
-    dim3 grid(ceil_div(d.nr, 16), 1, d.M + 1);
-    k_tc_analysis3<true><<<grid, WS_THREADS, analysis_smem(true), s>>>(d, moff, img0, img1, a);
+    const int ncol = ceil_div(d.nr, 16);
+    const int ntiles = (d.M + 1) * ncol;
+    k_tc_analysis3<true><<<std::min(ntiles, sm_count()), WS_THREADS, analysis_smem(true), s>>>(d, moff, img0, img1,
+                                                                                              a, ncol);
   }
 }
 
