@@ -80,17 +80,6 @@ __device__ __forceinline__ void issue_chunk(uint32_t tmem, uint32_t dcol, const 
 }
 
 
-// Runtime coefficients: x is rounded to FP32 once (relative error 2^-24,
-// the order of the FP32 accumulation), then split in single precision:
-// hi = tf32(f), lo = tf32(f - hi) (f - hi is exact).  o = float offset in the
-// swizzled tile.
-__device__ __forceinline__ void put_split_d_at(float* hi, float* lo, uint32_t o, double x) {
-  const float f = __double2float_rn(x);
-  const float h = tf32_rn(f);
-  hi[o] = h;
-  lo[o] = tf32_rn(f - h);
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -169,265 +158,290 @@ void launch_build_tc_images(cudaStream_t s, const Dims& d, const int* moff, cons
 }
 
 // ---------------------------------------------------------------------------
-// Synthesis.  CTA = (m, 128-row theta tile, column tile), 288 threads:
-// two loader groups of four warps and one MMA warp.  One pipeline step per
-// (K chunk, parity); loader group g fills stage g for the steps it = g, g+2,
-// ...: its first thread starts bulk copies of the table chunk(s) (transaction
-// bytes on the stage's `full` barrier), and all 128 threads load and split the
-// 128-deep (vector) or 256-deep (scalar) x 32 FP64 coefficient tile into TF32
-// hi/lo and arrive on the stage's `full` barrier.  The MMA warp issues the
-// step's MMAs when the stage is full and commits them to the stage's `empty`
-// barrier, which the group waits on before refilling.  The two groups' loads
-// are in flight at the same time, so a step's load latency overlaps the
-// previous step's.  Scalar: accumulators [even | odd] x 256 columns.
-// Vector: stages hold the Pbar and dPbar/dtheta chunks, accumulators [P even
-// | P odd | dP even | dP odd] x 128; the m/sin(theta) factor of the Q = m
-// Pbar / sin(theta) terms is applied to the Pbar sums in the epilogue.
-// Vector columns: [S: 32 shells x re/im][T: same].
+// Synthesis, two kernels.
+//
+// 1. k_synth_coef_image: the runtime coefficients of one call as split,
+//    swizzled TF32 B-operand chunks: chunk (column tile ct, m, step it) =
+//    hi then lo image of NCS columns x 32 K (scalar NCS = 256 columns
+//    n = (field, r, re/im); vector NCS = 128: [S: 32 shells x re/im][T]),
+//    K -> l = m + p + 2 (32 kc + k).  One CTA per (kc, m, ct) covers both
+//    parities, so each warp reads l-contiguous runs of every coefficient row.
+// 2. k_tc_synth4: persistent CTAs over tiles (m, 128-row theta tile, column
+//    tile), 192 threads: warp 0 feeds the two pipeline stages with bulk copies
+//    only (table chunk(s) and the coefficient chunk, transaction bytes on the
+//    stage's `full` barrier), warp 1 issues the split-TF32 MMAs (3 products
+//    per 8-deep K slice) and commits them to the stage's `empty` barrier and,
+//    after a tile's last step, to `tfull`; warps 2-5 (one per TMEM lane
+//    quarter) wait on `tfull`, read the accumulators, release them on
+//    `tempty` and write the blocked Fourier layout while the next tile's
+//    stages are already loading.  Scalar: accumulators [even | odd] x 256.
+//    Vector: [P even | P odd | dP even | dP odd] x 128; the m/sin(theta) of
+//    the Q = m Pbar / sin(theta) terms is applied to the Pbar sums.
 // ---------------------------------------------------------------------------
-constexpr int WS_THREADS = 288;  // 2 loader groups x 4 warps + 1 MMA warp
+constexpr int SY_THREADS = 192;
+
+// step it -> (parity p, K chunk kc): odd-parity chunks interleave with the
+// even ones while both exist
+__device__ __forceinline__ void synth_step_pk(int it, int nc1, int& p, int& kc) {
+  kc = it < 2 * nc1 ? (it >> 1) : nc1 + (it - 2 * nc1);
+  p = it < 2 * nc1 ? (it & 1) : 0;
+}
+__device__ __forceinline__ int synth_step_of(int p, int kc, int nc1) { return kc < nc1 ? 2 * kc + p : nc1 + kc; }
 
 template <bool VEC>
-__global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* __restrict__ moff,
-                                                      const long* __restrict__ cofs, const float* __restrict__ imgP,
-                                                      const float* __restrict__ imgD, const double* __restrict__ sinv,
-                                                      TcSynthArgs a, int ntt, int ncol) {
+__global__ void __launch_bounds__(256) k_synth_coef_image(Dims d, const int* __restrict__ moff,
+                                                          const long* __restrict__ cofs, int ntt, TcSynthArgs a) {
+  constexpr int NCS = VEC ? TC_N2 : 2 * TC_N2;
+  constexpr int BT = NCS * TC_K;
+  __shared__ const double* colp[NCS];
+  const int kc = blockIdx.x, m = blockIdx.y, ct = blockIdx.z;
+  const int L = d.L;
+  const int nc0 = nck_h(L, m, 0), nc1 = nck_h(L, m, 1);
+  if (kc >= nc0) return;
+  const size_t NM = d.nlm;
+  const int mb = moff[m];
+  const int Ntot = a.nf * d.nr * 2;
+  for (int c = threadIdx.x; c < NCS; c += blockDim.x) {
+    const double* src = nullptr;
+    if (VEC) {
+      const int fld = c >> 6, r = ct * 32 + ((c & 63) >> 1), ci = c & 1;
+      if (r < d.nr) src = a.coef[fld] + ((size_t)ci * d.nr + r) * NM + mb - m;
+    } else {
+      const int ng = ct * NCS + c;
+      if (ng < Ntot) {
+        const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, ci = rem & 1;
+        src = a.coef[f] + ((size_t)ci * d.nr + r) * NM + mb - m;
+      }
+    }
+    colp[c] = src;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long base = (long)ct * a.ttot + cofs[m] / ntt;
+  float* h0 = a.bimg + (base + synth_step_of(0, kc, nc1)) * (2L * BT);
+  float* h1 = kc < nc1 ? a.bimg + (base + synth_step_of(1, kc, nc1)) * (2L * BT) : nullptr;
+  const int l0 = m + 2 * (TC_K * kc + lane);
+  for (int row = warp; row < NCS; row += 8) {
+    const double* src = colp[row];
+    const double v0 = (src != nullptr && l0 <= L) ? src[l0] : 0.0;
+    const double v1 = (src != nullptr && l0 + 1 <= L) ? src[l0 + 1] : 0.0;
+    const uint32_t o = sw128_offset(row, lane) >> 2;
+    const float f0 = __double2float_rn(v0), g0 = tf32_rn(f0);
+    h0[o] = g0;
+    h0[BT + o] = tf32_rn(f0 - g0);
+    if (h1 != nullptr) {
+      const float f1 = __double2float_rn(v1), g1 = tf32_rn(f1);
+      h1[o] = g1;
+      h1[BT + o] = tf32_rn(f1 - g1);
+    }
+  }
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* __restrict__ moff,
+                                                             const long* __restrict__ cofs,
+                                                             const float* __restrict__ imgP,
+                                                             const float* __restrict__ imgD,
+                                                             const double* __restrict__ sinv, TcSynthArgs a, int ntt,
+                                                             int ncol) {
   constexpr int S = 2;
-  constexpr int NCS = VEC ? TC_N2 : 2 * TC_N2;   // columns per CTA: vector 128, scalar 256
+  constexpr int NCS = VEC ? TC_N2 : 2 * TC_N2;   // columns per tile: vector 128, scalar 256
   constexpr int A_FL = (VEC ? 2 : 1) * CHUNK_FLOATS;
-  constexpr int BT = NCS * TC_K;  // one B image (hi or lo)
+  constexpr int BT = NCS * TC_K;                  // one B image (hi or lo)
   constexpr int ST_FL = A_FL + 2 * BT;
   constexpr uint32_t NCOL = 512;
   constexpr uint32_t IDS = idesc_tf32(TC_M, NCS);
+  constexpr uint32_t STEP_BYTES = (uint32_t)(A_FL + 2 * BT) * 4u;
   extern __shared__ unsigned char smem_raw[];
   const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   float* stg = reinterpret_cast<float*>(base);
   uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)S * ST_FL * 4);
   uint64_t* empty = full + S;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(empty + S);
-  // scalar: column -> coefficient row (null past the last column); column
-  // pair -> Fourier output base (-1 past the last column)
-  const double** colp = reinterpret_cast<const double**>(empty + S + 2);
-  long long* colo = reinterpret_cast<long long*>(colp + NCS);
+  uint64_t* tfull = empty + S;
+  uint64_t* tempty = tfull + 1;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 1);
 
   const int L = d.L;
-  const size_t NM = d.nlm;
   const int Ntot = a.nf * d.nr * 2;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid == 0)
+  if (tid == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&full[s], 128);
+      mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
+    mbar_init(tfull, 1);
+    mbar_init(tempty, 128);
+  }
   if (warp == 0) tmem_alloc(tslot, NCOL);
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = *tslot;
-
-  bool ok = true;
-  int issued = -1;  // loader thread 0 of a group: last use of its stage with bulk copies issued
-  int gs = 0;       // pipeline steps of the earlier tiles (stage and phase of a step follow from gs + it)
   const int ntiles = (d.M + 1) * ntt * ncol;
-  // persistent CTA: tiles (m, theta tile, column tile), m-major so the
-  // deepest columns (small m) are spread first
-  for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
-  const int m = tt / (ntt * ncol), tile = (tt / ncol) % ntt, ct = tt % ncol;
-  const int mb = moff[m];
-  const int n0 = ct * NCS;
-  const int r0 = ct * 32;
-  __syncthreads();  // the previous tile's epilogue is done with TMEM and the column tables
-  if (!VEC) {
-    for (int c = tid; c < NCS; c += blockDim.x) {
-      const int ng = n0 + c;
-      const double* src = nullptr;
-      if (ng < Ntot) {
-        const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, ci = rem & 1;
-        src = a.coef[f] + ((size_t)ci * d.nr + r) * NM + mb - m;
-      }
-      colp[c] = src;
-      if ((c & 1) == 0) {
-        long long ob = -1;
-        if (ng < Ntot) {
-          const int f = ng / (2 * d.nr), r = (ng % (2 * d.nr)) >> 1;
-          ob = (long long)((size_t)(f * d.nr + r) * a.nblk * (d.M + 1) * FOURIER_BLOCK);
+  bool ok = true;
+
+  if (warp == 0) {
+    // producer: bulk copies only
+    int gs = 0, issued = -1;
+    for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
+      const int m = tt / (ntt * ncol), tile = (tt / ncol) % ntt, ct = tt % ncol;
+      const int nc1 = nck_h(L, m, 1), T = nck_h(L, m, 0) + nc1;
+      for (int it = 0; it < T; ++it) {
+        const int G = gs + it, s = G & 1, u = G >> 1;
+        if (u >= 1 && !mbar_wait(&empty[s], (u - 1) & 1, a.err)) {
+          ok = false;
+          break;
         }
-        colo[c >> 1] = ob;
+        if (lane == 0) {
+          int p, kc;
+          synth_step_pk(it, nc1, p, kc);
+          float* A = stg + s * ST_FL;
+          const long ch = synth_chunk(cofs, L, m, tile, p, kc);
+          const long bch = (long)ct * a.ttot + cofs[m] / ntt + it;
+          mbar_arrive_expect_tx(&full[s], STEP_BYTES);
+          bulk_g2s(A, imgP + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[s]);
+          if (VEC) bulk_g2s(A + CHUNK_FLOATS, imgD + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[s]);
+          bulk_g2s(A + A_FL, a.bimg + bch * (2L * BT), (uint32_t)(2 * BT * 4), &full[s]);
+        }
+        issued = G;
+        __syncwarp();
       }
+      gs += T;
     }
-    __syncthreads();
-  }
-
-  const int nc0 = nck_h(L, m, 0), nc1 = nck_h(L, m, 1);
-  const int T = nc0 + nc1;
-
-  // step it -> (parity p, K chunk kc): odd-parity chunks interleave with the
-  // even ones while both exist
-  auto step_pk = [&](int it, int& p, int& kc) {
-    kc = it < 2 * nc1 ? (it >> 1) : nc1 + (it - 2 * nc1);
-    p = it < 2 * nc1 ? (it & 1) : 0;
-  };
-
-  if (warp < 8) {
-    const int g = warp >> 2, gw = warp & 3, gt = tid & 127;
-    float* A = stg + g * ST_FL;
-    float* B = A + A_FL;
-    constexpr int RPT = NCS / 4;              // coefficient rows per thread
-    constexpr int HALF = RPT > 32 ? 32 : RPT; // loads in flight per batch
-    for (int it = (g - gs) & 1; it < T; it += 2) {
-      const int u = (gs + it) >> 1;
-      if (u >= 1 && !mbar_wait(&empty[g], (u - 1) & 1, a.err)) {
+    // after an expired wait, let the last bulk copies land before the CTA exits
+    if (!ok && issued >= 0) mbar_wait(&full[issued & 1], (issued >> 1) & 1, a.err);
+  } else if (warp == 1) {
+    // MMA issuer
+    int gs = 0, q = 0;
+    for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x, ++q) {
+      const int m = tt / (ntt * ncol);
+      const int nc1 = nck_h(L, m, 1), T = nck_h(L, m, 0) + nc1;
+      if (q >= 1 && !mbar_wait(tempty, (q - 1) & 1, a.err)) {
         ok = false;
         break;
       }
-      int p, kc;
-      step_pk(it, p, kc);
-      if (gt == 0) {
-        const long ch = synth_chunk(cofs, L, m, tile, p, kc);
-        mbar_expect_tx(&full[g], (VEC ? 2u : 1u) * CHUNK_BYTES);
-        bulk_g2s(A, imgP + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[g]);
-        if (VEC) bulk_g2s(A + CHUNK_FLOATS, imgD + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[g]);
-        issued = u;
-      }
-      const int l = m + p + 2 * (TC_K * kc + lane);
-      // swizzled offsets of rows gw + 4 i: 8-row atom i / 2, row in atom gw or gw + 4
-      const uint32_t o_even = sw128_offset(gw, lane) >> 2, o_odd = sw128_offset(gw + 4, lane) >> 2;
-#pragma unroll
-      for (int h = 0; h < RPT; h += HALF) {
-        double v[HALF];
-#pragma unroll
-        for (int i = 0; i < HALF; ++i) {
-          const int row = gw + 4 * (h + i);
-          const double* src = nullptr;
-          if (VEC) {
-            const int fld = row >> 6, r = r0 + ((row & 63) >> 1), c = row & 1;
-            if (r < d.nr) src = a.coef[fld] + ((size_t)c * d.nr + r) * NM + mb - m;
-          } else {
-            src = colp[row];
-          }
-          v[i] = (src != nullptr && l <= L) ? __ldg(src + l) : 0.0;
+      for (int it = 0; it < T; ++it) {
+        const int G = gs + it, s = G & 1;
+        if (!mbar_wait(&full[s], (G >> 1) & 1, a.err)) {
+          ok = false;
+          break;
         }
+        fence_after_sync();
+        if (lane == 0) {
+          int p, kc;
+          synth_step_pk(it, nc1, p, kc);
+          const float* A = stg + s * ST_FL;
+          const float* B = A + A_FL;
 #pragma unroll
-        for (int i = 0; i < HALF; ++i) {
-          const int ii = h + i;
-          put_split_d_at(B, B + BT, (uint32_t)(ii >> 1) * 256u + ((ii & 1) ? o_odd : o_even), v[i]);
+          for (int t = 0; t < (VEC ? 2 : 1); ++t)
+            issue_chunk(tmem, (t * 2 + p) * NCS, A + t * CHUNK_FLOATS, A + t * CHUNK_FLOATS + TILE_A_FLOATS, B,
+                        B + BT, kc == 0, IDS);
+          mma_commit(smem_addr(&empty[s]));
+          if (it == T - 1) mma_commit(smem_addr(tfull));
         }
+        __syncwarp();
       }
-      fence_proxy_async();
-      mbar_arrive(&full[g]);
+      gs += T;
     }
   } else {
-    for (int it = 0; it < T; ++it) {
-      const int s = (gs + it) & 1;
-      if (!mbar_wait(&full[s], ((gs + it) >> 1) & 1, a.err)) {
+    // epilogue warps 2-5: TMEM lane quarter warp & 3
+    const int qw = warp & 3;
+    // scalar columns n = (f nr + r) 2 + re/im: the pair n / 2 = f nr + r indexes the (comp, r) run
+    const size_t run = (size_t)a.nblk * (d.M + 1) * FOURIER_BLOCK;
+    const uint32_t trow = tmem + ((uint32_t)(qw * 32) << 16);
+    int q = 0;
+    for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x, ++q) {
+      const int m = tt / (ntt * ncol), tile = (tt / ncol) % ntt, ct = tt % ncol;
+      const int nc1 = nck_h(L, m, 1);
+      if (!mbar_wait(tfull, q & 1, a.err)) {
         ok = false;
         break;
       }
       fence_after_sync();
-      if (lane == 0) {
-        int p, kc;
-        step_pk(it, p, kc);
-        const float* A = stg + s * ST_FL;
-        const float* B = A + A_FL;
+      const int ith = tile * TC_M + qw * 32 + lane;
+      // offset of (theta block, m, pair) within one (comp, r) run of the blocked layout
+      const size_t ioff = ((size_t)(ith / FOURIER_BLOCK) * (d.M + 1) + m) * FOURIER_BLOCK + ith % FOURIER_BLOCK;
+      if (!VEC) {
+        for (int c0 = 0; c0 < NCS; c0 += 8) {
+          float e[8], o[8];
+          tmem_ld8(trow + c0, e);
+          if (nc1 > 0) tmem_ld8(trow + NCS + c0, o);
+          tmem_ld_wait();
+          if (nc1 == 0) {
 #pragma unroll
-        for (int t = 0; t < (VEC ? 2 : 1); ++t)
-          issue_chunk(tmem, (t * 2 + p) * NCS, A + t * CHUNK_FLOATS, A + t * CHUNK_FLOATS + TILE_A_FLOATS, B,
-                      B + BT, kc == 0, IDS);
-        mma_commit(smem_addr(&empty[s]));
+            for (int j = 0; j < 8; ++j) o[j] = 0.f;
+          }
+          if (c0 + 8 == NCS) {
+            fence_before_sync();
+            mbar_arrive(tempty);  // accumulators read: the next tile's MMAs may start
+          }
+          if (ith < d.nth) {
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) {
+              const int ng = ct * NCS + c0 + j;
+              if (ng >= Ntot) continue;
+              a.out[(size_t)(ng >> 1) * run + ioff] =
+                  make_float4(e[j] + o[j], e[j + 1] + o[j + 1], e[j] - o[j], e[j + 1] - o[j + 1]);
+            }
+          }
+        }
+      } else {
+        const int r0 = ct * 32;
+        const float ms = (ith < d.nth) ? (float)((double)m * sinv[ith]) : 0.f;
+        for (int jj = 0; jj < 64; jj += 8) {
+          float pse[8], pso[8], pte[8], pto[8], dse[8], dso[8], dte[8], dto[8];
+          tmem_ld8(trow + 0 * TC_N2 + jj, pse);
+          tmem_ld8(trow + 0 * TC_N2 + 64 + jj, pte);
+          tmem_ld8(trow + 2 * TC_N2 + jj, dse);
+          tmem_ld8(trow + 2 * TC_N2 + 64 + jj, dte);
+          if (nc1 > 0) {
+            tmem_ld8(trow + 1 * TC_N2 + jj, pso);
+            tmem_ld8(trow + 1 * TC_N2 + 64 + jj, pto);
+            tmem_ld8(trow + 3 * TC_N2 + jj, dso);
+            tmem_ld8(trow + 3 * TC_N2 + 64 + jj, dto);
+          }
+          tmem_ld_wait();
+          if (nc1 == 0) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) pso[j] = pto[j] = dso[j] = dto[j] = 0.f;
+          }
+          if (jj + 8 == 64) {
+            fence_before_sync();
+            mbar_arrive(tempty);
+          }
+          if (ith < d.nth) {
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) {
+              const int r = r0 + (jj + j) / 2;
+              if (r >= d.nr) continue;
+              float vt[4], vp[4];  // (north Re, north Im, south Re, south Im)
+#pragma unroll
+              for (int sN = 0; sN < 2; ++sN) {
+                float PS[2], PT[2], DS[2], DT[2];
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                  if (sN == 0) {
+                    PS[c] = pse[j + c] + pso[j + c]; PT[c] = pte[j + c] + pto[j + c];
+                    DS[c] = dse[j + c] + dso[j + c]; DT[c] = dte[j + c] + dto[j + c];
+                  } else {  // dPbar has the opposite north/south symmetry
+                    PS[c] = pse[j + c] - pso[j + c]; PT[c] = pte[j + c] - pto[j + c];
+                    DS[c] = dso[j + c] - dse[j + c]; DT[c] = dto[j + c] - dte[j + c];
+                  }
+                }
+                const float QS0 = ms * PS[0], QS1 = ms * PS[1], QT0 = ms * PT[0], QT1 = ms * PT[1];
+                vt[2 * sN] = DS[0] - QT1; vt[2 * sN + 1] = DS[1] + QT0;
+                vp[2 * sN] = -QS1 - DT[0]; vp[2 * sN + 1] = QS0 - DT[1];
+              }
+              a.out[(size_t)(0 * d.nr + r) * run + ioff] = make_float4(vt[0], vt[1], vt[2], vt[3]);
+              a.out[(size_t)(1 * d.nr + r) * run + ioff] = make_float4(vp[0], vp[1], vp[2], vp[3]);
+            }
+          }
+        }
       }
-      __syncwarp();
     }
-  }
-  // drain: the last MMA batch of each stage in this tile
-  if (ok) {
-#pragma unroll
-    for (int q = 1; q <= S; ++q)
-      if (T - q >= 0) ok = mbar_wait(&empty[(gs + T - q) & 1], ((gs + T - q) >> 1) & 1, a.err) && ok;
   }
   ok = __syncthreads_and(ok);
   fence_after_sync();
-  if (ok && warp < 8) {
-    const int q = warp & 3, half = warp >> 2;
-    const int ith = tile * TC_M + q * 32 + lane;
-    const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
-    // offset of (theta block, m, pair) within one (comp, r) run of the blocked layout
-    const size_t ioff = ((size_t)(ith / FOURIER_BLOCK) * (d.M + 1) + m) * FOURIER_BLOCK + ith % FOURIER_BLOCK;
-    if (!VEC) {
-      for (int c0 = (NCS / 2) * half; c0 < (NCS / 2) * (half + 1); c0 += 8) {
-        float e[8], o[8];
-        tmem_ld8(trow + c0, e);
-        if (nc1 > 0) tmem_ld8(trow + NCS + c0, o);
-        tmem_ld_wait();
-        if (nc1 == 0) {
-#pragma unroll
-          for (int j = 0; j < 8; ++j) o[j] = 0.f;
-        }
-        if (ith < d.nth) {
-#pragma unroll
-          for (int j = 0; j < 8; j += 2) {
-            const long long obase = colo[(c0 + j) >> 1];
-            if (obase < 0) continue;
-            a.out[(size_t)obase + ioff] =
-                make_float4(e[j] + o[j], e[j + 1] + o[j + 1], e[j] - o[j], e[j + 1] - o[j + 1]);
-          }
-        }
-      }
-    } else {
-      const float ms = (ith < d.nth) ? (float)((double)m * sinv[ith]) : 0.f;
-      for (int jj = 32 * half; jj < 32 * half + 32; jj += 8) {
-        float pse[8], pso[8], pte[8], pto[8], dse[8], dso[8], dte[8], dto[8];
-        tmem_ld8(trow + 0 * TC_N2 + jj, pse);
-        tmem_ld8(trow + 0 * TC_N2 + 64 + jj, pte);
-        tmem_ld8(trow + 2 * TC_N2 + jj, dse);
-        tmem_ld8(trow + 2 * TC_N2 + 64 + jj, dte);
-        if (nc1 > 0) {
-          tmem_ld8(trow + 1 * TC_N2 + jj, pso);
-          tmem_ld8(trow + 1 * TC_N2 + 64 + jj, pto);
-          tmem_ld8(trow + 3 * TC_N2 + jj, dso);
-          tmem_ld8(trow + 3 * TC_N2 + 64 + jj, dto);
-        }
-        tmem_ld_wait();
-        if (nc1 == 0) {
-#pragma unroll
-          for (int j = 0; j < 8; ++j) pso[j] = pto[j] = dso[j] = dto[j] = 0.f;
-        }
-        if (ith < d.nth) {
-#pragma unroll
-          for (int j = 0; j < 8; j += 2) {
-            const int r = r0 + (jj + j) / 2;
-            if (r >= d.nr) continue;
-            float vt[4], vp[4];  // (north Re, north Im, south Re, south Im)
-#pragma unroll
-            for (int sN = 0; sN < 2; ++sN) {
-              float PS[2], PT[2], DS[2], DT[2];
-#pragma unroll
-              for (int c = 0; c < 2; ++c) {
-                if (sN == 0) {
-                  PS[c] = pse[j + c] + pso[j + c]; PT[c] = pte[j + c] + pto[j + c];
-                  DS[c] = dse[j + c] + dso[j + c]; DT[c] = dte[j + c] + dto[j + c];
-                } else {  // dPbar has the opposite north/south symmetry
-                  PS[c] = pse[j + c] - pso[j + c]; PT[c] = pte[j + c] - pto[j + c];
-                  DS[c] = dso[j + c] - dse[j + c]; DT[c] = dto[j + c] - dte[j + c];
-                }
-              }
-              const float QS0 = ms * PS[0], QS1 = ms * PS[1], QT0 = ms * PT[0], QT1 = ms * PT[1];
-              vt[2 * sN] = DS[0] - QT1; vt[2 * sN + 1] = DS[1] + QT0;
-              vp[2 * sN] = -QS1 - DT[0]; vp[2 * sN + 1] = QS0 - DT[1];
-            }
-            const size_t run = (size_t)a.nblk * (d.M + 1) * FOURIER_BLOCK;
-            a.out[(size_t)(0 * d.nr + r) * run + ioff] = make_float4(vt[0], vt[1], vt[2], vt[3]);
-            a.out[(size_t)(1 * d.nr + r) * run + ioff] = make_float4(vp[0], vp[1], vp[2], vp[3]);
-          }
-        }
-      }
-    }
-  }
-  fence_before_sync();
-  gs += T;
-  }  // tiles
-  // after an expired wait, let the last bulk copies land before the CTA exits
-  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err);
-  __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, NCOL);
 }
 
@@ -440,6 +454,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_synth3(Dims d, const int* 
 // holding the dPbar and Q chunks and two B tiles (fold 1 - p for dPbar, fold p
 // for Q), accumulators [dP even | dP odd | Q even | Q odd] x 64.
 // ---------------------------------------------------------------------------
+constexpr int WS_THREADS = 288;  // 2 loader groups x 4 warps + 1 MMA warp
+
 template <bool VEC>
 __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const int* __restrict__ moff,
                                                          const float* __restrict__ img0,
@@ -680,9 +696,10 @@ static void smem_attr(K k, size_t bytes) {
 }
 // stages + mbarriers and TMEM slot (16 bytes past the stages) + the scalar
 // kernels' per-column tables (one pointer per column, one offset per pair)
+// stages + full/empty per stage, tfull, tempty and the TMEM address slot
 static size_t synth_smem(bool vec) {
   const int S = 2, NCS = vec ? TC_N2 : 2 * TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS, B = 2 * NCS * TC_K;
-  return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 2) + (size_t)NCS * 8 + (size_t)(NCS / 2) * 8;
+  return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 3);
 }
 static size_t analysis_smem(bool vec) {
   const int S = 2, NC = vec ? TC_N : TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS;
@@ -692,8 +709,8 @@ static size_t analysis_smem(bool vec) {
 static bool g_attr_done = false;
 static void set_attrs() {
   if (g_attr_done) return;
-  smem_attr(k_tc_synth3<false>, synth_smem(false));
-  smem_attr(k_tc_synth3<true>, synth_smem(true));
+  smem_attr(k_tc_synth4<false>, synth_smem(false));
+  smem_attr(k_tc_synth4<true>, synth_smem(true));
   smem_attr(k_tc_analysis3<false>, analysis_smem(false));
   smem_attr(k_tc_analysis3<true>, analysis_smem(true));
   g_attr_done = true;
@@ -715,17 +732,26 @@ void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long*
                      const float* imgD, const double* sinv, const TcSynthArgs& a, bool vec) {
   set_attrs();
   const int ntt = (d.nth + TC_M - 1) / TC_M;
+  const int kcmax = nck_h(d.L, 0, 0);
   if (!vec) {
     const int ncol = ceil_div(a.nf * d.nr * 2, 2 * TC_N2);
     const int ntiles = (d.M + 1) * ntt * ncol;
-    k_tc_synth3<false><<<std::min(ntiles, sm_count()), WS_THREADS, synth_smem(false), s>>>(d, moff, cofs, imgP,
+    k_synth_coef_image<false><<<dim3(kcmax, d.M + 1, ncol), 256, 0, s>>>(d, moff, cofs, ntt, a);
+    k_tc_synth4<false><<<std::min(ntiles, sm_count()), SY_THREADS, synth_smem(false), s>>>(d, moff, cofs, imgP,
                                                                                           imgD, sinv, a, ntt, ncol);
   } else {
     const int ncol = ceil_div(d.nr, 32);
     const int ntiles = (d.M + 1) * ntt * ncol;
-    k_tc_synth3<true><<<std::min(ntiles, sm_count()), WS_THREADS, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD,
+    k_synth_coef_image<true><<<dim3(kcmax, d.M + 1, ncol), 256, 0, s>>>(d, moff, cofs, ntt, a);
+    k_tc_synth4<true><<<std::min(ntiles, sm_count()), SY_THREADS, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD,
                                                                                         sinv, a, ntt, ncol);
   }
+}
+
+size_t tc_synth_bimage_floats(const Dims& d, long ttot) {
+  const long ncol_s = ceil_div(4L * d.nr * 2, 2 * TC_N2), ncol_v = ceil_div(d.nr, 32);
+  const long s = ncol_s * ttot * 2L * (2 * TC_N2) * TC_K, v = ncol_v * ttot * 2L * TC_N2 * TC_K;
+  return (size_t)(s > v ? s : v);
 }
 
 void launch_tc_analysis(cudaStream_t s, const Dims& d, const int* moff, const float* img0, const float* img1,

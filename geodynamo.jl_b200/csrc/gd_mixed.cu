@@ -32,6 +32,8 @@ struct MixedState {
   float4* d_Fall = nullptr;    // FC_COUNT blocked components
   size_t fcomp = 0;            // float4 per component
   float2* d_G = nullptr;       // folded transforms for the analysis, 2 components
+  float* d_bimg = nullptr;     // split coefficient images of one synthesis call
+  long ttot = 0;               // synthesis pipeline steps over all m (one column tile)
   float* d_tgrid = nullptr;    // the temperature grid (FP32)
   float* d_stage = nullptr;    // 4 FP32 grids for the host-array entry points and grid downloads
   int* d_err = nullptr;
@@ -78,6 +80,8 @@ int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float4* out
   a.out = out;
   a.nblk = nblocks(h);
   a.err = x->d_err;
+  a.bimg = x->d_bimg;
+  a.ttot = x->ttot;
   { ProfScope p(h, "legendre_synth_scalar_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], nullptr, x->sinv, a, false); }
   return launched(h, "mixed scalar synthesis");
 }
@@ -92,6 +96,8 @@ int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float4* 
   a.out = out;
   a.nblk = nblocks(h);
   a.err = x->d_err;
+  a.bimg = x->d_bimg;
+  a.ttot = x->ttot;
   { ProfScope p(h, "legendre_synth_vector_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], x->img_synth[1], x->sinv, a, true); }
   return launched(h, "mixed vector synthesis");
 }
@@ -176,6 +182,8 @@ int mixed_create(gd_handle* h) {
   const size_t cb = tc_chunk_bytes() / sizeof(float);
   MAL(x->d_cofs, cofs.size());
   for (int t = 0; t < 2; ++t) MAL(x->img_synth[t], (size_t)nsyn * cb);
+  x->ttot = nsyn / ((d.nth + 127) / 128);
+  MAL(x->d_bimg, tc_synth_bimage_floats(d, x->ttot));
   for (int t = 0; t < 3; ++t) MAL(x->img_anal[t], (size_t)nana * cb);
   MAL(x->ra, d.nlm); MAL(x->rb, d.nlm); MAL(x->rc, d.nlm);
   MAL(x->r1a, d.L + 1); MAL(x->r1b, d.L + 1);

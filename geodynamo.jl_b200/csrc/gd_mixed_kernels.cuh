@@ -18,7 +18,12 @@ struct TcSynthArgs {
   int nblk;               // theta blocks (ceil(nth / FOURIER_BLOCK))
   int nf;
   int* err;               // set to 1 if a bounded wait expires
+  float* bimg;            // scratch for the split coefficient images (tc_synth_bimage_floats)
+  long ttot;              // pipeline steps summed over m (one column tile)
 };
+
+// Floats of coefficient-image scratch the synthesis needs (the scalar case, 4 fields, bounds both).
+size_t tc_synth_bimage_floats(const Dims& d, long ttot);
 
 // Recurrence data for on-the-fly table rows (see k_rec_tables).
 struct TcRec {
