@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(256) k_synth_coef_image(Dims d, const int* __r
   constexpr int NCS = VEC ? TC_N2 : 2 * TC_N2;
   constexpr int BT = NCS * TC_K;
   __shared__ const double* colp[NCS];
+  __shared__ unsigned char mine[NCS];  // column belongs to a field of prep_mask
   const int kc = blockIdx.x, m = blockIdx.y, ct = blockIdx.z;
   const int L = d.L;
   const int nc0 = nck_h(L, m, 0), nc1 = nck_h(L, m, 1);
@@ -203,17 +204,21 @@ __global__ void __launch_bounds__(256) k_synth_coef_image(Dims d, const int* __r
   const int Ntot = a.nf * d.nr * 2;
   for (int c = threadIdx.x; c < NCS; c += blockDim.x) {
     const double* src = nullptr;
+    bool own = true;
     if (VEC) {
       const int fld = c >> 6, r = ct * 32 + ((c & 63) >> 1), ci = c & 1;
+      own = (a.prep_mask >> fld) & 1;
       if (r < d.nr) src = a.coef[fld] + ((size_t)ci * d.nr + r) * NM + mb - m;
     } else {
       const int ng = ct * NCS + c;
       if (ng < Ntot) {
         const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, ci = rem & 1;
+        own = (a.prep_mask >> f) & 1;
         src = a.coef[f] + ((size_t)ci * d.nr + r) * NM + mb - m;
       }
     }
-    colp[c] = src;
+    colp[c] = own ? src : nullptr;
+    mine[c] = own ? 1 : 0;
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -222,6 +227,7 @@ __global__ void __launch_bounds__(256) k_synth_coef_image(Dims d, const int* __r
   float* h1 = kc < nc1 ? a.bimg + (base + synth_step_of(1, kc, nc1)) * (2L * BT) : nullptr;
   const int l0 = m + 2 * (TC_K * kc + lane);
   for (int row = warp; row < NCS; row += 8) {
+    if (!mine[row]) continue;  // written by the field's producer kernel
     const double* src = colp[row];
     const double v0 = (src != nullptr && l0 <= L) ? src[l0] : 0.0;
     const double v1 = (src != nullptr && l0 + 1 <= L) ? src[l0 + 1] : 0.0;
@@ -736,13 +742,13 @@ void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long*
   if (!vec) {
     const int ncol = ceil_div(a.nf * d.nr * 2, 2 * TC_N2);
     const int ntiles = (d.M + 1) * ntt * ncol;
-    k_synth_coef_image<false><<<dim3(kcmax, d.M + 1, ncol), 256, 0, s>>>(d, moff, cofs, ntt, a);
+    if (a.prep_mask) k_synth_coef_image<false><<<dim3(kcmax, d.M + 1, ncol), 256, 0, s>>>(d, moff, cofs, ntt, a);
     k_tc_synth4<false><<<std::min(ntiles, sm_count()), SY_THREADS, synth_smem(false), s>>>(d, moff, cofs, imgP,
                                                                                           imgD, sinv, a, ntt, ncol);
   } else {
     const int ncol = ceil_div(d.nr, 32);
     const int ntiles = (d.M + 1) * ntt * ncol;
-    k_synth_coef_image<true><<<dim3(kcmax, d.M + 1, ncol), 256, 0, s>>>(d, moff, cofs, ntt, a);
+    if (a.prep_mask) k_synth_coef_image<true><<<dim3(kcmax, d.M + 1, ncol), 256, 0, s>>>(d, moff, cofs, ntt, a);
     k_tc_synth4<true><<<std::min(ntiles, sm_count()), SY_THREADS, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD,
                                                                                         sinv, a, ntt, ncol);
   }

@@ -32,7 +32,13 @@ struct MixedState {
   float4* d_Fall = nullptr;    // FC_COUNT blocked components
   size_t fcomp = 0;            // float4 per component
   float2* d_G = nullptr;       // folded transforms for the analysis, 2 components
-  float* d_bimg = nullptr;     // split coefficient images of one synthesis call
+  // split coefficient images of the synthesis (zeroed once; every writer
+  // keeps its layout's padding at zero): scalar (T by the pre-pass, its
+  // gradient by k_gradients), vector state fields (pre-pass), vector curls (k_curl)
+  float* d_bimg_s = nullptr;
+  float* d_bimg_vp = nullptr;
+  float* d_bimg_vc = nullptr;
+  long* d_bofs = nullptr;      // first step of order m within a column tile
   long ttot = 0;               // synthesis pipeline steps over all m (one column tile)
   float* d_tgrid = nullptr;    // the temperature grid (FP32)
   float* d_stage = nullptr;    // 4 FP32 grids for the host-array entry points and grid downloads
@@ -71,8 +77,18 @@ int launched(gd_handle* h, const char* what) { return mcheck(h, cudaGetLastError
 
 int nblocks(const gd_handle* h) { return fourier_blocks(h->d); }
 
-// Legendre synthesis of nf scalar fields into consecutive blocked components from `out`.
-int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float4* out) {
+SynthImageOut image_out(gd_handle* h, float* img) {
+  SynthImageOut o{};
+  o.img = img;
+  o.bofs = h->mixed->d_bofs;
+  o.ttot = h->mixed->ttot;
+  return o;
+}
+
+// Legendre synthesis of nf scalar fields into consecutive blocked components
+// from `out`; the fields of prep_mask are split by the pre-pass, the others
+// are already in the scalar image.
+int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float4* out, int prep_mask) {
   MixedState* x = h->mixed;
   TcSynthArgs a{};
   for (int i = 0; i < nf; ++i) a.coef[i] = coef[i];
@@ -80,13 +96,15 @@ int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float4* out
   a.out = out;
   a.nblk = nblocks(h);
   a.err = x->d_err;
-  a.bimg = x->d_bimg;
+  a.bimg = x->d_bimg_s;
   a.ttot = x->ttot;
+  a.prep_mask = prep_mask;
   { ProfScope p(h, "legendre_synth_scalar_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], nullptr, x->sinv, a, false); }
   return launched(h, "mixed scalar synthesis");
 }
 
-// Vector synthesis (tor, pol) -> (theta, phi) blocked components at out, out + 1.
+// Vector synthesis (tor, pol) -> (theta, phi) blocked components at out,
+// out + 1.  tor/pol null: the coefficients are already in the curl image.
 int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float4* out) {
   MixedState* x = h->mixed;
   TcSynthArgs a{};
@@ -96,8 +114,10 @@ int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float4* 
   a.out = out;
   a.nblk = nblocks(h);
   a.err = x->d_err;
-  a.bimg = x->d_bimg;
+  const bool pre = tor != nullptr;
+  a.bimg = pre ? x->d_bimg_vp : x->d_bimg_vc;
   a.ttot = x->ttot;
+  a.prep_mask = pre ? 3 : 0;
   { ProfScope p(h, "legendre_synth_vector_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], x->img_synth[1], x->sinv, a, true); }
   return launched(h, "mixed vector synthesis");
 }
@@ -182,8 +202,15 @@ int mixed_create(gd_handle* h) {
   const size_t cb = tc_chunk_bytes() / sizeof(float);
   MAL(x->d_cofs, cofs.size());
   for (int t = 0; t < 2; ++t) MAL(x->img_synth[t], (size_t)nsyn * cb);
-  x->ttot = nsyn / ((d.nth + 127) / 128);
-  MAL(x->d_bimg, tc_synth_bimage_floats(d, x->ttot));
+  const int ntt = (d.nth + 127) / 128;
+  x->ttot = nsyn / ntt;
+  const size_t nimg = tc_synth_bimage_floats(d, x->ttot);
+  MAL(x->d_bimg_s, nimg);
+  MAL(x->d_bimg_vp, nimg);
+  MAL(x->d_bimg_vc, nimg);
+  MAL(x->d_bofs, d.M + 2);
+  std::vector<long> bofs(d.M + 2);
+  for (int m = 0; m <= d.M + 1; ++m) bofs[m] = cofs[m] / ntt;
   for (int t = 0; t < 3; ++t) MAL(x->img_anal[t], (size_t)nana * cb);
   MAL(x->ra, d.nlm); MAL(x->rb, d.nlm); MAL(x->rc, d.nlm);
   MAL(x->r1a, d.L + 1); MAL(x->r1b, d.L + 1);
@@ -197,6 +224,13 @@ int mixed_create(gd_handle* h) {
   int s = mcheck(h, cudaMemcpyAsync(x->d_cofs, cofs.data(), sizeof(long) * cofs.size(), cudaMemcpyHostToDevice,
                                     h->stream), "cofs upload");
   if (s) return s;
+  s = mcheck(h, cudaMemcpyAsync(x->d_bofs, bofs.data(), sizeof(long) * bofs.size(), cudaMemcpyHostToDevice,
+                                h->stream), "bofs upload");
+  if (s) return s;
+  for (float* img : {x->d_bimg_s, x->d_bimg_vp, x->d_bimg_vc}) {
+    s = mcheck(h, cudaMemsetAsync(img, 0, sizeof(float) * nimg, h->stream), "memset");
+    if (s) return s;
+  }
   s = mcheck(h, cudaMemsetAsync(x->r1a, 0, sizeof(double) * (d.L + 1), h->stream), "memset");
   if (s) return s;
   s = mcheck(h, cudaMemsetAsync(x->r1b, 0, sizeof(double) * (d.L + 1), h->stream), "memset");
@@ -243,10 +277,11 @@ int mixed_check_error(gd_handle* h) {
 int mixed_temperature_nl(gd_handle* h) {
   MixedState* x = h->mixed;
   const Dims& d = h->d;
+  // the gradient goes straight into the scalar synthesis image (field slots 1-3)
   { ProfScope p(h, "spectral_gradients");
-    launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), h->work(0), h->work(1), h->work(2)); }
-  const double* coef[4] = {h->field(F_TEMP), h->work(0), h->work(1), h->work(2)};
-  int s = tc_synth_scalar(h, coef, 4, x->F(FC_T));
+    launch_gradients_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), image_out(h, x->d_bimg_s)); }
+  const double* coef[4] = {h->field(F_TEMP), nullptr, nullptr, nullptr};
+  int s = tc_synth_scalar(h, coef, 4, x->F(FC_T), 1);
   if (s) return s;
   // the velocity grid is the previous velocity phase's (carried in F(FC_U))
   FusedArgs f = phase_args(h);
@@ -270,8 +305,9 @@ int mixed_velocity_nl(gd_handle* h) {
   int s = tc_synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), x->F(FC_U));
   if (s) return s;
   { ProfScope p(h, "spectral_curl");
-    launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR), h->field(F_UPOL), h->work(3), h->work(4)); }
-  s = tc_synth_vector(h, h->work(3), h->work(4), x->F(FC_W));
+    launch_curl_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR),
+                    h->field(F_UPOL), image_out(h, x->d_bimg_vc)); }
+  s = tc_synth_vector(h, nullptr, nullptr, x->F(FC_W));
   if (s) return s;
   // current density and magnetic field of the previous magnetic phase (F(FC_J), F(FC_B))
   FusedArgs f = phase_args(h);
@@ -291,8 +327,9 @@ int mixed_magnetic_nl(gd_handle* h) {
   int s = tc_synth_vector(h, h->field(F_BTOR), h->field(F_BPOL), x->F(FC_B));
   if (s) return s;
   { ProfScope p(h, "spectral_curl");
-    launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR), h->field(F_BPOL), h->work(5), h->work(6)); }
-  s = tc_synth_vector(h, h->work(5), h->work(6), x->F(FC_J));
+    launch_curl_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR),
+                    h->field(F_BPOL), image_out(h, x->d_bimg_vc)); }
+  s = tc_synth_vector(h, nullptr, nullptr, x->F(FC_J));
   if (s) return s;
   FusedArgs f = phase_args(h);
   const float4* fin[4] = {x->F(FC_U), x->F(FC_U + 1), x->F(FC_B), x->F(FC_B + 1)};
@@ -341,7 +378,7 @@ int mixed_grid_to_double(gd_handle* h, int grid, double* out) {
 
 int mixed_api_synth_scalar(gd_handle* h, const double* const* coef, int nf, double* grid_out) {
   MixedState* x = h->mixed;
-  int s = tc_synth_scalar(h, coef, nf, x->F(FC_T));
+  int s = tc_synth_scalar(h, coef, nf, x->F(FC_T), (1 << nf) - 1);
   if (s) return s;
   const float4* fin[4] = {x->F(FC_T), x->F(FC_T + 1), x->F(FC_T + 2), x->F(FC_T + 3)};
   s = fourier_to_grid(h, fin, nf, x->d_stage);

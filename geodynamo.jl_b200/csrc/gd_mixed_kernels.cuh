@@ -4,8 +4,38 @@
 #include <vector>
 
 #include "gd_internal.cuh"
+#include "gd_tc.cuh"
 
 namespace gd {
+
+// 32-deep K chunks of parity p (l - m even / odd) for order m.
+__host__ __device__ __forceinline__ int tc_nck(int L, int m, int p) {
+  const int k = p == 0 ? (L - m + 2) / 2 : (L - m + 1) / 2;
+  return (k + 31) / 32;
+}
+// Synthesis pipeline step of (parity p, K chunk kc): odd-parity chunks
+// interleave with the even ones while both exist.
+__host__ __device__ __forceinline__ int tc_step_of(int p, int kc, int nc1) { return kc < nc1 ? 2 * kc + p : nc1 + kc; }
+
+// Destination of runtime coefficients written straight into a synthesis
+// B image (split TF32 hi / lo, 128-byte swizzled): chunk (column tile ct, m,
+// step) at ct * ttot + bofs[m] + step, NCS columns x 32 K each.
+struct SynthImageOut {
+  float* img;         // null: write FP64 outputs instead
+  const long* bofs;   // first step of order m within a column tile
+  long ttot;          // steps per column tile
+};
+
+__device__ __forceinline__ void synth_image_put(const SynthImageOut& o, int ncs, int ct, int col, int L, int m, int l,
+                                                double v) {
+  const int q = l - m, p = q & 1, idx = q >> 1, kc = idx >> 5, k = idx & 31;
+  const long chunk = (long)ct * o.ttot + o.bofs[m] + tc_step_of(p, kc, tc_nck(L, m, 1));
+  float* hi = o.img + chunk * (2L * ncs * 32);
+  const uint32_t off = tc::sw128_offset((uint32_t)col, (uint32_t)k) >> 2;
+  const float f = __double2float_rn(v), h = tc::tf32_rn(f);
+  hi[off] = h;
+  hi[(size_t)ncs * 32 + off] = tc::tf32_rn(f - h);
+}
 
 // Colatitude pairs per block of the blocked Fourier layout written by the
 // synthesis and read by the fused phase kernels: float4 (north Re, north Im,
@@ -18,8 +48,9 @@ struct TcSynthArgs {
   int nblk;               // theta blocks (ceil(nth / FOURIER_BLOCK))
   int nf;
   int* err;               // set to 1 if a bounded wait expires
-  float* bimg;            // scratch for the split coefficient images (tc_synth_bimage_floats)
+  float* bimg;            // split coefficient images (tc_synth_bimage_floats floats)
   long ttot;              // pipeline steps summed over m (one column tile)
+  int prep_mask;          // fields the pre-pass writes into bimg (the others are written by their producer)
 };
 
 // Floats of coefficient-image scratch the synthesis needs (the scalar case, 4 fields, bounds both).
@@ -52,5 +83,11 @@ void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long*
 void launch_tc_analysis(cudaStream_t s, const Dims& d, const int* moff, const float* img0, const float* img1,
                         const TcAnalysisArgs& a);
 void launch_cast_d2f(cudaStream_t s, size_t n, const double* src, float* dst);
+// Radial operators of gd_spectral.cu writing a synthesis B image instead of FP64 arrays.
+void launch_gradients_img(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
+                          const double* d1, const double* T, const SynthImageOut& img);
+void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
+                     const double* rinv2, const double* d1, const double* d2, const double* tor, const double* pol,
+                     const SynthImageOut& img);
 
 }  // namespace gd

@@ -1,6 +1,7 @@
 // gd_spectral.cu -- spectral-space operators on the native layout (two planes
 // Re/Im of [r][j], j m-major), plus layout conversions used by the host ABI.
 #include "gd_internal.cuh"
+#include "gd_mixed_kernels.cuh"
 
 namespace gd {
 
@@ -15,11 +16,14 @@ constexpr int RB_R = 16;
 // theta derivative by the reference's recurrence coefficients (:158,171), phi
 // derivative i m, radial derivative by the banded D1, then x 1/r on the
 // angular components (:317-321).  In m-major order (l +- 1, m) sits at j +- 1.
-template <int KL>
+// IMG: the mixed path's scalar synthesis reads g_theta, g_phi, g_r as split
+// TF32 image columns (field slots 1, 2, 3 of n = (field nr + r) 2 + re/im);
+// they are written there instead of to the FP64 arrays.
+template <int KL, bool IMG>
 __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __restrict__ mof,
                             const double* __restrict__ rinv, const double* __restrict__ d1,
                             const double* __restrict__ T, double* __restrict__ gth, double* __restrict__ gph,
-                            double* __restrict__ gr) {
+                            double* __restrict__ gr, SynthImageOut img) {
   constexpr int NB = 2 * KL + 1;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int k0 = blockIdx.y * RB_R;
@@ -52,7 +56,12 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
         const int jj = k - KL + t;
         if (jj >= 0 && jj < N) sr += d1[(KL + k - jj) + (size_t)NB * jj] * w[t];
       }
-      gr[c * plane + at] = sr;
+      if (IMG) {
+        const int n = (3 * N + k) * 2 + c;
+        synth_image_put(img, 256, n >> 8, n & 255, d.L, m, l, sr);
+      } else {
+        gr[c * plane + at] = sr;
+      }
 #pragma unroll
       for (int t = 0; t < NB - 1; ++t) w[t] = w[t + 1];
       const int nx = k + KL + 1;
@@ -73,32 +82,47 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
       di += Am * T[plane + at - 1];
     }
     const double ri = rinv[k];
-    gth[at] = dr * ri;
-    gth[plane + at] = di * ri;
-    gph[at] = (-(double)m * T[plane + at]) * ri;
-    gph[plane + at] = ((double)m * T[at]) * ri;
+    const double v[4] = {dr * ri, di * ri, (-(double)m * T[plane + at]) * ri, ((double)m * T[at]) * ri};
+    if (IMG) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int n = ((1 + (q >> 1)) * N + k) * 2 + (q & 1);
+        synth_image_put(img, 256, n >> 8, n & 255, d.L, m, l, v[q]);
+      }
+    } else {
+      gth[at] = v[0];
+      gth[plane + at] = v[1];
+      gph[at] = v[2];
+      gph[plane + at] = v[3];
+    }
   }
 }
 
 void launch_gradients(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                       const double* d1, const double* T, double* gth, double* gph, double* gr) {
   dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
-  switch (d.kl) {
-    case 1: k_gradients<1><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr); break;
-    case 2: k_gradients<2><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr); break;
-    case 3: k_gradients<3><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr); break;
-    default: k_gradients<4><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr); break;
-  }
+  // the band half-width is validated to GD_MAX_KL at creation
+  k_gradients<GD_MAX_KL, false><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr, SynthImageOut{});
+}
+
+void launch_gradients_img(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
+                          const double* d1, const double* T, const SynthImageOut& img) {
+  dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
+  k_gradients<GD_MAX_KL, true><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, nullptr, nullptr, nullptr, img);
 }
 
 // compute_vorticity_spectral_full! (src/velocity.jl:340-441) and
 // compute_current_density_spectral! (src/magnetic.jl:253-349):
 //   curl_tor = l(l+1)/r^2 P - D2 P - (2/r) D1 P,   curl_pol = -l(l+1)/r^2 T.
-template <int KL>
-__global__ void k_curl(Dims d, const int* __restrict__ lof, const double* __restrict__ rinv,
-                       const double* __restrict__ rinv2, const double* __restrict__ d1,
-                       const double* __restrict__ d2, const double* __restrict__ tor,
-                       const double* __restrict__ pol, double* __restrict__ otor, double* __restrict__ opol) {
+// IMG: the mixed path's vector synthesis of the curl reads it as split TF32
+// image columns [S = curl_pol: 32 shells x re/im][T = curl_tor], column tile
+// r / 32; it is written there instead of to the FP64 arrays.
+template <int KL, bool IMG>
+__global__ void k_curl(Dims d, const int* __restrict__ lof, const int* __restrict__ mof,
+                       const double* __restrict__ rinv, const double* __restrict__ rinv2,
+                       const double* __restrict__ d1, const double* __restrict__ d2, const double* __restrict__ tor,
+                       const double* __restrict__ pol, double* __restrict__ otor, double* __restrict__ opol,
+                       SynthImageOut img) {
   constexpr int NB = 2 * KL + 1;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int k0 = blockIdx.y * RB_R;
@@ -129,8 +153,16 @@ __global__ void k_curl(Dims d, const int* __restrict__ lof, const double* __rest
         }
       }
       const size_t at = (size_t)k * NM + j;
-      otor[c * plane + at] = lf * rinv2[k] * w[KL] - a2 - 2.0 * rinv[k] * a1;
-      opol[c * plane + at] = -lf * rinv2[k] * tor[c * plane + at];
+      const double vt = lf * rinv2[k] * w[KL] - a2 - 2.0 * rinv[k] * a1;
+      const double vp = -lf * rinv2[k] * tor[c * plane + at];
+      if (IMG) {
+        const int l = lof[j], m = mof[j], col = (k & 31) * 2 + c;
+        synth_image_put(img, 128, k >> 5, col, d.L, m, l, vp);
+        synth_image_put(img, 128, k >> 5, 64 + col, d.L, m, l, vt);
+      } else {
+        otor[c * plane + at] = vt;
+        opol[c * plane + at] = vp;
+      }
 #pragma unroll
       for (int t = 0; t < NB - 1; ++t) w[t] = w[t + 1];
       const int nx = k + KL + 1;
@@ -143,12 +175,15 @@ void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* ri
                  const double* d1, const double* d2, const double* tor, const double* pol, double* otor,
                  double* opol) {
   dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
-  switch (d.kl) {
-    case 1: k_curl<1><<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol); break;
-    case 2: k_curl<2><<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol); break;
-    case 3: k_curl<3><<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol); break;
-    default: k_curl<4><<<grid, 128, 0, s>>>(d, lof, rinv, rinv2, d1, d2, tor, pol, otor, opol); break;
-  }
+  k_curl<GD_MAX_KL, false><<<grid, 128, 0, s>>>(d, lof, nullptr, rinv, rinv2, d1, d2, tor, pol, otor, opol,
+                                                SynthImageOut{});
+}
+
+void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
+                     const double* rinv2, const double* d1, const double* d2, const double* tor, const double* pol,
+                     const SynthImageOut& img) {
+  dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
+  k_curl<GD_MAX_KL, true><<<grid, 128, 0, s>>>(d, lof, mof, rinv, rinv2, d1, d2, tor, pol, nullptr, nullptr, img);
 }
 
 // apply_temperature_boundary_conditions_spectral! (src/thermal.jl:262-303):
