@@ -37,9 +37,9 @@ constexpr int TC_N2 = 128;    // synthesis and scalar analysis column tile
 constexpr int TC_K = 32;                       // TF32 elements per 128-byte row
 constexpr int TILE_A_FLOATS = TC_M * TC_K;      // 4096 floats = 16 KB
 constexpr int CHUNK_FLOATS = 2 * TILE_A_FLOATS; // hi image then lo image (32 KB)
-constexpr uint32_t CHUNK_BYTES = CHUNK_FLOATS * 4;
 constexpr uint32_t IDESC = idesc_tf32(TC_M, TC_N);
 constexpr uint32_t IDESC2 = idesc_tf32(TC_M, TC_N2);
+constexpr uint32_t CHUNK_BYTES = CHUNK_FLOATS * 4;
 // Pipelined kernels: every stage holds one (chunk, parity) step; stages sit
 // back to back after a 1024-byte aligned base, then one mbarrier per stage
 // and the TMEM address slot (192 KB + alignment slack per CTA).
@@ -163,7 +163,8 @@ void launch_build_tc_images(cudaStream_t s, const Dims& d, const int* moff, cons
 // 1. k_synth_coef_image: the runtime coefficients of one call as split,
 //    swizzled TF32 B-operand chunks: chunk (column tile ct, m, step it) =
 //    hi then lo image of NCS columns x 32 K (scalar NCS = 256 columns
-//    n = (field, r, re/im); vector NCS = 128: [S: 32 shells x re/im][T]),
+//    n = (field, r, re/im); vector NCS = 128: 32 shells x [S re, S im, T re,
+//    T im]; the valid columns of a tile are a prefix),
 //    K -> l = m + p + 2 (32 kc + k).  One CTA per (kc, m, ct) covers both
 //    parities, so each warp reads l-contiguous runs of every coefficient row.
 // 2. k_tc_synth4: persistent CTAs over tiles (m, 128-row theta tile, column
@@ -176,7 +177,9 @@ void launch_build_tc_images(cudaStream_t s, const Dims& d, const int* moff, cons
 //    `tempty` and write the blocked Fourier layout while the next tile's
 //    stages are already loading.  Scalar: accumulators [even | odd] x 256.
 //    Vector: [P even | P odd | dP even | dP odd] x 128; the m/sin(theta) of
-//    the Q = m Pbar / sin(theta) terms is applied to the Pbar sums.
+//    the Q = m Pbar / sin(theta) terms is applied to the Pbar sums.  Rows past
+//    the last colatitude and columns past the last shell are neither copied
+//    nor (columns) multiplied: the MMA width follows the tile's valid columns.
 // ---------------------------------------------------------------------------
 constexpr int SY_THREADS = 192;
 
@@ -206,7 +209,7 @@ __global__ void __launch_bounds__(256) k_synth_coef_image(Dims d, const int* __r
     const double* src = nullptr;
     bool own = true;
     if (VEC) {
-      const int fld = c >> 6, r = ct * 32 + ((c & 63) >> 1), ci = c & 1;
+      const int fld = (c >> 1) & 1, r = ct * 32 + (c >> 2), ci = c & 1;
       own = (a.prep_mask >> fld) & 1;
       if (r < d.nr) src = a.coef[fld] + ((size_t)ci * d.nr + r) * NM + mb - m;
     } else {
@@ -256,8 +259,6 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
   constexpr int BT = NCS * TC_K;                  // one B image (hi or lo)
   constexpr int ST_FL = A_FL + 2 * BT;
   constexpr uint32_t NCOL = 512;
-  constexpr uint32_t IDS = idesc_tf32(TC_M, NCS);
-  constexpr uint32_t STEP_BYTES = (uint32_t)(A_FL + 2 * BT) * 4u;
   extern __shared__ unsigned char smem_raw[];
   const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   float* stg = reinterpret_cast<float*>(base);
@@ -304,10 +305,22 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
           float* A = stg + s * ST_FL;
           const long ch = synth_chunk(cofs, L, m, tile, p, kc);
           const long bch = (long)ct * a.ttot + cofs[m] / ntt + it;
-          mbar_arrive_expect_tx(&full[s], STEP_BYTES);
-          bulk_g2s(A, imgP + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[s]);
-          if (VEC) bulk_g2s(A + CHUNK_FLOATS, imgD + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[s]);
-          bulk_g2s(A + A_FL, a.bimg + bch * (2L * BT), (uint32_t)(2 * BT * 4), &full[s]);
+          // table rows past the last colatitude and coefficient columns past
+          // the last valid one only reach accumulator rows / columns the
+          // epilogue never reads: copy whole 8-row swizzle atoms of the rest
+          const uint32_t pa = (uint32_t)min(TC_M, (d.nth - tile * TC_M + 7) & ~7) * 128u;
+          const int nvalid = VEC ? 4 * min(32, d.nr - ct * 32) : min(NCS, Ntot - ct * NCS);
+          const uint32_t pb = (uint32_t)((nvalid + 7) & ~7) * 128u;
+          mbar_arrive_expect_tx(&full[s], (VEC ? 4u : 2u) * pa + 2u * pb);
+#pragma unroll
+          for (int t = 0; t < (VEC ? 2 : 1); ++t) {
+            const float* src = (t == 0 ? imgP : imgD) + ch * CHUNK_FLOATS;
+            bulk_g2s(A + t * CHUNK_FLOATS, src, pa, &full[s]);
+            bulk_g2s(A + t * CHUNK_FLOATS + TILE_A_FLOATS, src + TILE_A_FLOATS, pa, &full[s]);
+          }
+          const float* bsrc = a.bimg + bch * (2L * BT);
+          bulk_g2s(A + A_FL, bsrc, pb, &full[s]);
+          bulk_g2s(A + A_FL + BT, bsrc + BT, pb, &full[s]);
         }
         issued = G;
         __syncwarp();
@@ -320,8 +333,10 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
     // MMA issuer
     int gs = 0, q = 0;
     for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x, ++q) {
-      const int m = tt / (ntt * ncol);
+      const int m = tt / (ntt * ncol), ct = tt % ncol;
       const int nc1 = nck_h(L, m, 1), T = nck_h(L, m, 0) + nc1;
+      const int nvalid = VEC ? 4 * min(32, d.nr - ct * 32) : min(NCS, Ntot - ct * NCS);
+      const uint32_t ids = idesc_tf32(TC_M, (nvalid + 15) & ~15);
       if (q >= 1 && !mbar_wait(tempty, (q - 1) & 1, a.err)) {
         ok = false;
         break;
@@ -341,7 +356,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
 #pragma unroll
           for (int t = 0; t < (VEC ? 2 : 1); ++t)
             issue_chunk(tmem, (t * 2 + p) * NCS, A + t * CHUNK_FLOATS, A + t * CHUNK_FLOATS + TILE_A_FLOATS, B,
-                        B + BT, kc == 0, IDS);
+                        B + BT, kc == 0, ids);
           mma_commit(smem_addr(&empty[s]));
           if (it == T - 1) mma_commit(smem_addr(tfull));
         }
@@ -367,8 +382,10 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
       const int ith = tile * TC_M + qw * 32 + lane;
       // offset of (theta block, m, pair) within one (comp, r) run of the blocked layout
       const size_t ioff = ((size_t)(ith / FOURIER_BLOCK) * (d.M + 1) + m) * FOURIER_BLOCK + ith % FOURIER_BLOCK;
+      const int nvalid = VEC ? 4 * min(32, d.nr - ct * 32) : min(NCS, Ntot - ct * NCS);
+      const int cend = (nvalid + 7) & ~7;  // accumulator columns holding valid results
       if (!VEC) {
-        for (int c0 = 0; c0 < NCS; c0 += 8) {
+        for (int c0 = 0; c0 < cend; c0 += 8) {
           float e[8], o[8];
           tmem_ld8(trow + c0, e);
           if (nc1 > 0) tmem_ld8(trow + NCS + c0, o);
@@ -377,7 +394,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
 #pragma unroll
             for (int j = 0; j < 8; ++j) o[j] = 0.f;
           }
-          if (c0 + 8 == NCS) {
+          if (c0 + 8 >= cend) {
             fence_before_sync();
             mbar_arrive(tempty);  // accumulators read: the next tile's MMAs may start
           }
@@ -392,34 +409,32 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
           }
         }
       } else {
+        // columns (shell, component, re/im): 8 columns = 2 shells x [S re, S im, T re, T im]
         const int r0 = ct * 32;
         const float ms = (ith < d.nth) ? (float)((double)m * sinv[ith]) : 0.f;
-        for (int jj = 0; jj < 64; jj += 8) {
-          float pse[8], pso[8], pte[8], pto[8], dse[8], dso[8], dte[8], dto[8];
-          tmem_ld8(trow + 0 * TC_N2 + jj, pse);
-          tmem_ld8(trow + 0 * TC_N2 + 64 + jj, pte);
-          tmem_ld8(trow + 2 * TC_N2 + jj, dse);
-          tmem_ld8(trow + 2 * TC_N2 + 64 + jj, dte);
+        for (int c0 = 0; c0 < cend; c0 += 8) {
+          float pe[8], po[8], de[8], dq[8];
+          tmem_ld8(trow + 0 * TC_N2 + c0, pe);
+          tmem_ld8(trow + 2 * TC_N2 + c0, de);
           if (nc1 > 0) {
-            tmem_ld8(trow + 1 * TC_N2 + jj, pso);
-            tmem_ld8(trow + 1 * TC_N2 + 64 + jj, pto);
-            tmem_ld8(trow + 3 * TC_N2 + jj, dso);
-            tmem_ld8(trow + 3 * TC_N2 + 64 + jj, dto);
+            tmem_ld8(trow + 1 * TC_N2 + c0, po);
+            tmem_ld8(trow + 3 * TC_N2 + c0, dq);
           }
           tmem_ld_wait();
           if (nc1 == 0) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) pso[j] = pto[j] = dso[j] = dto[j] = 0.f;
+            for (int j = 0; j < 8; ++j) po[j] = dq[j] = 0.f;
           }
-          if (jj + 8 == 64) {
+          if (c0 + 8 >= cend) {
             fence_before_sync();
             mbar_arrive(tempty);
           }
           if (ith < d.nth) {
 #pragma unroll
-            for (int j = 0; j < 8; j += 2) {
-              const int r = r0 + (jj + j) / 2;
+            for (int s2 = 0; s2 < 2; ++s2) {
+              const int r = r0 + c0 / 4 + s2;
               if (r >= d.nr) continue;
+              const int b = 4 * s2;
               float vt[4], vp[4];  // (north Re, north Im, south Re, south Im)
 #pragma unroll
               for (int sN = 0; sN < 2; ++sN) {
@@ -427,11 +442,11 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
                   if (sN == 0) {
-                    PS[c] = pse[j + c] + pso[j + c]; PT[c] = pte[j + c] + pto[j + c];
-                    DS[c] = dse[j + c] + dso[j + c]; DT[c] = dte[j + c] + dto[j + c];
+                    PS[c] = pe[b + c] + po[b + c]; PT[c] = pe[b + 2 + c] + po[b + 2 + c];
+                    DS[c] = de[b + c] + dq[b + c]; DT[c] = de[b + 2 + c] + dq[b + 2 + c];
                   } else {  // dPbar has the opposite north/south symmetry
-                    PS[c] = pse[j + c] - pso[j + c]; PT[c] = pte[j + c] - pto[j + c];
-                    DS[c] = dso[j + c] - dse[j + c]; DT[c] = dto[j + c] - dte[j + c];
+                    PS[c] = pe[b + c] - po[b + c]; PT[c] = pe[b + 2 + c] - po[b + 2 + c];
+                    DS[c] = dq[b + c] - de[b + c]; DT[c] = dq[b + 2 + c] - de[b + 2 + c];
                   }
                 }
                 const float QS0 = ms * PS[0], QS1 = ms * PS[1], QT0 = ms * PT[0], QT1 = ms * PT[1];

@@ -115,8 +115,8 @@ void launch_gradients_img(cudaStream_t s, const Dims& d, const int* lof, const i
 // compute_current_density_spectral! (src/magnetic.jl:253-349):
 //   curl_tor = l(l+1)/r^2 P - D2 P - (2/r) D1 P,   curl_pol = -l(l+1)/r^2 T.
 // IMG: the mixed path's vector synthesis of the curl reads it as split TF32
-// image columns [S = curl_pol: 32 shells x re/im][T = curl_tor], column tile
-// r / 32; it is written there instead of to the FP64 arrays.
+// image columns 32 shells x [S re, S im, T re, T im] (S = curl_pol, T =
+// curl_tor), column tile r / 32; written there instead of to the FP64 arrays.
 template <int KL, bool IMG>
 __global__ void k_curl(Dims d, const int* __restrict__ lof, const int* __restrict__ mof,
                        const double* __restrict__ rinv, const double* __restrict__ rinv2,
@@ -156,9 +156,9 @@ __global__ void k_curl(Dims d, const int* __restrict__ lof, const int* __restric
       const double vt = lf * rinv2[k] * w[KL] - a2 - 2.0 * rinv[k] * a1;
       const double vp = -lf * rinv2[k] * tor[c * plane + at];
       if (IMG) {
-        const int l = lof[j], m = mof[j], col = (k & 31) * 2 + c;
+        const int l = lof[j], m = mof[j], col = (k & 31) * 4 + c;
         synth_image_put(img, 128, k >> 5, col, d.L, m, l, vp);
-        synth_image_put(img, 128, k >> 5, 64 + col, d.L, m, l, vt);
+        synth_image_put(img, 128, k >> 5, col + 2, d.L, m, l, vt);
       } else {
         otor[c * plane + at] = vt;
         opol[c * plane + at] = vp;
