@@ -124,6 +124,12 @@ template <typename C> struct Dft<16, C> {
 // (m, row) accesses of the load and store phases spread over the banks.
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
 __host__ __device__ __forceinline__ int prow(int n) { return (n + (n >> 4)) | 1; }
+// Unpadded alternative: element i of a row stored at i ^ ((i >> 4) & 15), a
+// permutation inside each aligned group of 16.  Stride-16 runs (radix-16
+// outputs) and unit-stride runs both spread over distinct bank pairs for
+// 8-byte elements, so rows need no padding (used by the fused kernels, whose
+// occupancy is bounded by shared memory).
+__device__ __forceinline__ int xidx(int i) { return i ^ ((i >> 4) & 15); }
 
 // One Stockham pass from src to dst ([tb][n] each): radix R, Ns = product of
 // the radices of the earlier passes.
@@ -217,9 +223,9 @@ template <typename RT, int N> struct CtGeom {
 // PT: tw is this pass's own table [r - 1][k] (k < NS, consecutive k in
 // consecutive entries, so a warp's twiddle reads are conflict-free in shared
 // memory); otherwise tw is the full table W_N^i.
-template <int R, int N, int TB, int NS, typename C, int NT = kThreads, bool PT = false>
+template <int R, int N, int TB, int NS, typename C, int NT = kThreads, bool PT = false, bool XS = false>
 __device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict__ dst, const C* __restrict__ tw) {
-  constexpr int RS = (N + (N >> 4)) | 1;
+  constexpr int RS = XS ? N : (N + (N >> 4)) | 1;
   constexpr int NBF = N / R;
   constexpr int TOTAL = TB * NBF;
   constexpr int TWSTEP = N / (NS * R);
@@ -228,7 +234,10 @@ __device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict
     const int k = j % NS;
     const C* s = src + row * RS;
     C v[R];
-    if constexpr (NBF % 16 == 0) {
+    if constexpr (XS) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = s[xidx(j + r * NBF)];
+    } else if constexpr (NBF % 16 == 0) {
       const C* sj = s + pidx(j);
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = sj[r * (NBF + NBF / 16)];
@@ -244,7 +253,10 @@ __device__ __forceinline__ void ct_pass(const C* __restrict__ src, C* __restrict
     C* o = dst + row * RS;
     const int base = (j / NS) * NS * R;
     const int o0 = base + k;
-    if constexpr (NS % 16 == 0) {
+    if constexpr (XS) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) o[xidx(o0 + r * NS)] = v[r];
+    } else if constexpr (NS % 16 == 0) {
       C* oo = o + pidx(o0);
 #pragma unroll
       for (int r = 0; r < R; ++r) oo[r * (NS + NS / 16)] = v[r];
@@ -275,9 +287,9 @@ __device__ __forceinline__ C* ct_passes(C* src, C* dst, const C* tw) {
 // A compile-time pass that hands its outputs (row, natural index, value) to
 // f instead of storing them: the last pass of a transform whose consumer is
 // pointwise in the output index.
-template <int R, int N, int TB, int NS, typename C, int NT, bool PT, class F>
+template <int R, int N, int TB, int NS, typename C, int NT, bool PT, bool XS, class F>
 __device__ __forceinline__ void ct_pass_apply(const C* __restrict__ src, const C* __restrict__ tw, F& f) {
-  constexpr int RS = (N + (N >> 4)) | 1;
+  constexpr int RS = XS ? N : (N + (N >> 4)) | 1;
   constexpr int NBF = N / R;
   constexpr int TOTAL = TB * NBF;
   constexpr int TWSTEP = N / (NS * R);
@@ -286,7 +298,10 @@ __device__ __forceinline__ void ct_pass_apply(const C* __restrict__ src, const C
     const int k = j % NS;
     const C* s = src + row * RS;
     C v[R];
-    if constexpr (NBF % 16 == 0) {
+    if constexpr (XS) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = s[xidx(j + r * NBF)];
+    } else if constexpr (NBF % 16 == 0) {
       const C* sj = s + pidx(j);
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = sj[r * (NBF + NBF / 16)];
@@ -337,31 +352,32 @@ __device__ __forceinline__ void ct_fill_pass_twiddles(const float2* __restrict__
   }
 }
 
-// ct_passes with per-pass twiddle tables (ct_fill_pass_twiddles layout).
-template <int N, int TB, int S, int NS, typename C, int NT, int OFF = 0>
+// ct_passes with per-pass twiddle tables (ct_fill_pass_twiddles layout);
+// XS: rows in the unpadded xidx layout.
+template <int N, int TB, int S, int NS, typename C, int NT, int OFF = 0, bool XS = false>
 __device__ __forceinline__ C* ct_passes_pt(C* src, C* dst, const C* tw) {
   constexpr CPlan P = PlanOf<N>::p;
   if constexpr (S >= P.ns) {
     return src;
   } else {
     constexpr int R = P.r[S];
-    ct_pass<R, N, TB, NS, C, NT, true>(src, dst, tw + OFF);
+    ct_pass<R, N, TB, NS, C, NT, true, XS>(src, dst, tw + OFF);
     __syncthreads();
-    return ct_passes_pt<N, TB, S + 1, NS * R, C, NT, (NS > 1 ? OFF + (R - 1) * NS : OFF)>(dst, src, tw);
+    return ct_passes_pt<N, TB, S + 1, NS * R, C, NT, (NS > 1 ? OFF + (R - 1) * NS : OFF), XS>(dst, src, tw);
   }
 }
 
 // ct_passes_pt whose last pass hands its outputs to f (ct_pass_apply).
-template <int N, int TB, int S, int NS, typename C, int NT, int OFF, class F>
+template <int N, int TB, int S, int NS, typename C, int NT, int OFF, bool XS, class F>
 __device__ __forceinline__ void ct_passes_pt_apply(C* src, C* dst, const C* tw, F& f) {
   constexpr CPlan P = PlanOf<N>::p;
   constexpr int R = P.r[S];
   if constexpr (S == P.ns - 1) {
-    ct_pass_apply<R, N, TB, NS, C, NT, true>(src, tw + OFF, f);
+    ct_pass_apply<R, N, TB, NS, C, NT, true, XS>(src, tw + OFF, f);
   } else {
-    ct_pass<R, N, TB, NS, C, NT, true>(src, dst, tw + OFF);
+    ct_pass<R, N, TB, NS, C, NT, true, XS>(src, dst, tw + OFF);
     __syncthreads();
-    ct_passes_pt_apply<N, TB, S + 1, NS * R, C, NT, (NS > 1 ? OFF + (R - 1) * NS : OFF)>(dst, src, tw, f);
+    ct_passes_pt_apply<N, TB, S + 1, NS * R, C, NT, (NS > 1 ? OFF + (R - 1) * NS : OFF), XS>(dst, src, tw, f);
   }
 }
 

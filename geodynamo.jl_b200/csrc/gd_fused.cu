@@ -32,10 +32,23 @@ constexpr int FB = FOURIER_BLOCK;
 constexpr int FNT = 128;  // threads per CTA
 constexpr int PF = 4;     // prefetched float4 per thread (covers (M+1) FB <= 512)
 
+// compile-time lengths keep rows in the unpadded xidx layout, the runtime
+// plan in the padded pidx layout
+template <int N>
+__device__ __forceinline__ int ridx(int i) {
+  if constexpr (N > 0) return xidx(i);
+  else return pidx(i);
+}
+template <int N>
+__host__ __device__ __forceinline__ int row_stride(int n) {
+  if constexpr (N > 0) return N;
+  else return prow(n);
+}
+
 template <int N>
 __device__ __forceinline__ float2* run_fft(float2* a, float2* b, const float2* tw, const FftPlan& p) {
   if constexpr (N > 0) {
-    return ct_passes_pt<N, FB, 0, 1, float2, FNT>(a, b, tw);
+    return ct_passes_pt<N, FB, 0, 1, float2, FNT, 0, true>(a, b, tw);
   } else {
     return fft_forward<float, FNT>(a, b, FB, p, tw);
   }
@@ -43,6 +56,7 @@ __device__ __forceinline__ float2* run_fft(float2* a, float2* b, const float2* t
 
 // Z_m = F_N + i F_S and Z_{n-m} = conj(F_N) + i conj(F_S), stored conjugated
 // (the inverse transform is conj(FFT(conj(Z)))): element e = m * FB + pair.
+template <int N>
 __device__ __forceinline__ void pack_z(float2* bufA, int rs, int n, int e, int rows, float4 v) {
   const int m = e / FB, ii = e - m * FB;
   if (ii >= rows) v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -50,18 +64,18 @@ __device__ __forceinline__ void pack_z(float2* bufA, int rs, int n, int e, int r
   if (m == 0) {
     row[0] = make_float2(v.x, -v.z);
   } else {
-    row[pidx(m)] = make_float2(v.x - v.w, -(v.y + v.z));
-    row[pidx(n - m)] = make_float2(v.x + v.w, v.y - v.z);
+    row[ridx<N>(m)] = make_float2(v.x - v.w, -(v.y + v.z));
+    row[ridx<N>(n - m)] = make_float2(v.x + v.w, v.y - v.z);
   }
 }
 
 }  // namespace
 
 template <int N, int PH>
-__global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* __restrict__ tw, FusedArgs a) {
+__global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float2* __restrict__ tw, FusedArgs a) {
   typedef float2 C;
   const int n = N > 0 ? N : p.n;
-  const int rs = prow(n);
+  const int rs = row_stride<N>(n);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + FB * rs;
@@ -69,13 +83,9 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
   C* acc1 = acc0 + FB * rs;
   C* u0 = acc1;            // phase T (one product): u_theta, u_phi rows
   C* u1 = acc1 + FB * rs;
-  // phase V: Coriolis cos / sin by phi index (after the four buffers);
-  // every phase: the twiddle table after its buffers
-  float* sct = reinterpret_cast<float*>(acc1 + FB * rs);
-  float* sst = sct + n;
+  // the twiddle table after the phase's buffers
   const int nbuf = PH == FUSED_GRID ? 2 : (PH == FUSED_TEMPERATURE ? 5 : 4);
-  C* stw = reinterpret_cast<C*>(smem_raw + (size_t)nbuf * FB * rs * sizeof(C) +
-                                (PH == FUSED_VELOCITY ? 2 * (size_t)n * sizeof(float) : 0));
+  C* stw = reinterpret_cast<C*>(smem_raw + (size_t)nbuf * FB * rs * sizeof(C));
 
   const int tid = threadIdx.x;
   const int ib = blockIdx.x, r = blockIdx.y;
@@ -90,13 +100,6 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
     ct_fill_pass_twiddles<N, FNT>(tw, stw);
   } else {
     for (int j = tid; j < n; j += FNT) stw[j] = tw[j];
-  }
-  if (PH == FUSED_VELOCITY) {
-    for (int j = tid; j < n; j += FNT) {
-      const int t = j < d.nlat - 1 ? j : d.nlat - 1;
-      sct[j] = (float)a.cth[t];
-      sst[j] = (float)a.sthc[t];
-    }
   }
   if (PH != FUSED_GRID) {
     for (int e = tid; e < FB * rs; e += FNT) {
@@ -118,15 +121,15 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
   auto build = [&](int c) {
     for (int e = tid; e < FB * band; e += FNT) {
       const int ii = e / band, k = M + 1 + (e - ii * band);
-      bufA[ii * rs + pidx(k)] = make_float2(0.f, 0.f);
+      bufA[ii * rs + ridx<N>(k)] = make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int k = 0; k < PF; ++k) {
       const int e = tid + k * FNT;
-      if (e < tot) pack_z(bufA, rs, n, e, rows, pf[k]);
+      if (e < tot) pack_z<N>(bufA, rs, n, e, rows, pf[k]);
     }
     const float4* src = a.fin[c] + boff;
-    for (int e = tid + PF * FNT; e < tot; e += FNT) pack_z(bufA, rs, n, e, rows, __ldg(src + e));
+    for (int e = tid + PF * FNT; e < tot; e += FNT) pack_z<N>(bufA, rs, n, e, rows, __ldg(src + e));
   };
   const float ur = 0.f, wr = 0.f, jr = 0.f, br = 0.f;
   const float adv = -a.rf, mrf = -a.rf, lfr = a.lf;
@@ -146,7 +149,7 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
       }
       return;
     }
-    const int q = ii * rs + pidx(j);
+    const int q = ii * rs + ridx<N>(j);
     const float vN = z.x, vS = -z.y;
     if (PH == FUSED_TEMPERATURE) {
       // -(u_r g_r + u_th g_th + u_ph g_ph) + S(r)
@@ -173,13 +176,15 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
       C t = acc[q];
       switch (c) {
         case 0: {
-          const float ct = sct[j], st = sst[j];
+          // Coriolis factors of latitude index min(phi index, nlat - 1) (L1-cached)
+          const int tj = j < d.nlat - 1 ? j : d.nlat - 1;
+          const float ct = (float)__ldg(a.cth + tj), st = (float)__ldg(a.sthc + tj);
           t.x += adv * (-(vN * wr)) + mrf * (ct * vN + st * ur);
           t.y += adv * (-(vS * wr)) + mrf * (ct * vS + st * ur);
           break;
         }
         case 1: {
-          const float ct = sct[j];
+          const float ct = (float)__ldg(a.cth + (j < d.nlat - 1 ? j : d.nlat - 1));
           t.x += adv * (vN * wr) + mrf * (-ct * vN);
           t.y += adv * (vS * wr) + mrf * (-ct * vS);
           break;
@@ -213,12 +218,12 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
     if (c + 1 < a.nin) prefetch(c + 1);
     if constexpr (N > 0) {
       // the last Stockham pass feeds the consumer directly
-      ct_passes_pt_apply<N, FB, 0, 1, C, FNT, 0>(bufA, bufB, stw, consume);
+      ct_passes_pt_apply<N, FB, 0, 1, C, FNT, 0, true>(bufA, bufB, stw, consume);
     } else {
       const C* res = run_fft<N>(bufA, bufB, stw, p);
       for (int e = tid; e < FB * n; e += FNT) {
         const int ii = e / n, j = e - ii * n;
-        consume(ii, j, res[ii * rs + pidx(j)]);
+        consume(ii, j, res[ii * rs + ridx<N>(j)]);
       }
     }
     __syncthreads();
@@ -237,8 +242,8 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
       if (ii >= rows) continue;
       const int ith = i0 + ii;
       const C* row = res + ii * rs;
-      const C zk = row[pidx(m)];
-      C zn = row[pidx(m == 0 ? 0 : n - m)];
+      const C zk = row[ridx<N>(m)];
+      C zn = row[ridx<N>(m == 0 ? 0 : n - m)];
       zn.y = -zn.y;
       const float Xx = 0.5f * (zk.x + zn.x), Xy = 0.5f * (zk.y + zn.y);
       const float Yx = 0.5f * (zk.y - zn.y), Yy = -0.5f * (zk.x - zn.x);
@@ -253,13 +258,12 @@ __global__ void __launch_bounds__(FNT) k_fused(Dims d, FftPlan p, const float2* 
 
 namespace {
 
-size_t fused_smem(int phase, int n) {
-  const size_t buf = (size_t)FB * prow(n) * sizeof(float2);
+size_t fused_smem(int phase, int n, bool unpadded) {
+  const size_t buf = (size_t)FB * (unpadded ? n : prow(n)) * sizeof(float2);
   const size_t twb = (size_t)n * sizeof(float2);
   switch (phase) {
     case FUSED_GRID: return 2 * buf + twb;
     case FUSED_TEMPERATURE: return 5 * buf + twb;
-    case FUSED_VELOCITY: return 4 * buf + 2 * (size_t)n * sizeof(float) + twb;
     default: return 4 * buf + twb;
   }
 }
@@ -267,7 +271,7 @@ size_t fused_smem(int phase, int n) {
 template <int N, int PH>
 void launch_one(cudaStream_t s, const Dims& d, const FftPlan& p, const float2* tw, const FusedArgs& a) {
   const int n = N > 0 ? N : p.n;
-  const size_t sm = fused_smem(PH, n);
+  const size_t sm = fused_smem(PH, n, N > 0);
   static size_t attr = 0;
   if (attr < sm) {
     cudaFuncSetAttribute(k_fused<N, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -293,7 +297,7 @@ int fourier_blocks(const Dims& d) { return ceil_div(d.nth, FB); }
 
 size_t fourier_comp_elems(const Dims& d) { return (size_t)d.nr * fourier_blocks(d) * (d.M + 1) * FB; }
 
-size_t fused_smem_bytes(int phase, int nlon) { return fused_smem(phase, nlon); }
+size_t fused_smem_bytes(int phase, int nlon) { return fused_smem(phase, nlon, false); }
 
 void launch_fused(cudaStream_t s, const Dims& d, const FftPlan& p, const void* twf, int phase, const FusedArgs& a) {
   const float2* tw = static_cast<const float2*>(twf);

@@ -26,12 +26,22 @@ struct SynthImageOut {
   long ttot;          // steps per column tile
 };
 
-__device__ __forceinline__ void synth_image_put(const SynthImageOut& o, int ncs, int ct, int col, int L, int m, int l,
-                                                double v) {
-  const int q = l - m, p = q & 1, idx = q >> 1, kc = idx >> 5, k = idx & 31;
-  const long chunk = (long)ct * o.ttot + o.bofs[m] + tc_step_of(p, kc, tc_nck(L, m, 1));
-  float* hi = o.img + chunk * (2L * ncs * 32);
-  const uint32_t off = tc::sw128_offset((uint32_t)col, (uint32_t)k) >> 2;
+// Where mode (l, m) lands in every chunk of a synthesis image: the step
+// within the column tile and the K index; fixed for a thread that owns one
+// mode and walks r.
+struct SynthImagePos {
+  long step;  // bofs[m] + step of (parity, K chunk)
+  int k;      // K index in the chunk
+};
+__device__ __forceinline__ SynthImagePos synth_image_pos(const SynthImageOut& o, int L, int m, int l) {
+  const int q = l - m, p = q & 1, idx = q >> 1;
+  return SynthImagePos{o.bofs[m] + tc_step_of(p, idx >> 5, tc_nck(L, m, 1)), idx & 31};
+}
+// Split v = hi + lo into column col of column tile ct.
+__device__ __forceinline__ void synth_image_put(const SynthImageOut& o, int ncs, const SynthImagePos& at, int ct,
+                                                int col, double v) {
+  float* hi = o.img + ((long)ct * o.ttot + at.step) * (2L * ncs * 32);
+  const uint32_t off = tc::sw128_offset((uint32_t)col, (uint32_t)at.k) >> 2;
   const float f = __double2float_rn(v), h = tc::tf32_rn(f);
   hi[off] = h;
   hi[(size_t)ncs * 32 + off] = tc::tf32_rn(f - h);

@@ -37,6 +37,7 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
                        : 0.0;
   const double Am = dn ? -sqrt((double)l * l - (double)m * m) * sqrt((double)(l + m) * (double)(l - m)) / (2.0 * l - 1.0)
                        : 0.0;
+  const SynthImagePos ip = IMG ? synth_image_pos(img, d.L, m, l) : SynthImagePos{};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
     const double* P = T + c * plane;
@@ -58,7 +59,7 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
       }
       if (IMG) {
         const int n = (3 * N + k) * 2 + c;
-        synth_image_put(img, 256, n >> 8, n & 255, d.L, m, l, sr);
+        synth_image_put(img, 256, ip, n >> 8, n & 255, sr);
       } else {
         gr[c * plane + at] = sr;
       }
@@ -87,7 +88,7 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int n = ((1 + (q >> 1)) * N + k) * 2 + (q & 1);
-        synth_image_put(img, 256, n >> 8, n & 255, d.L, m, l, v[q]);
+        synth_image_put(img, 256, ip, n >> 8, n & 255, v[q]);
       }
     } else {
       gth[at] = v[0];
@@ -130,6 +131,7 @@ __global__ void k_curl(Dims d, const int* __restrict__ lof, const int* __restric
   const double lf = (double)lof[j] * (lof[j] + 1.0);
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   const int N = d.nr;
+  const SynthImagePos ip = IMG ? synth_image_pos(img, d.L, mof[j], lof[j]) : SynthImagePos{};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
     const double* P = pol + c * plane;
@@ -156,9 +158,9 @@ __global__ void k_curl(Dims d, const int* __restrict__ lof, const int* __restric
       const double vt = lf * rinv2[k] * w[KL] - a2 - 2.0 * rinv[k] * a1;
       const double vp = -lf * rinv2[k] * tor[c * plane + at];
       if (IMG) {
-        const int l = lof[j], m = mof[j], col = (k & 31) * 4 + c;
-        synth_image_put(img, 128, k >> 5, col, d.L, m, l, vp);
-        synth_image_put(img, 128, k >> 5, col + 2, d.L, m, l, vt);
+        const int col = (k & 31) * 4 + c;
+        synth_image_put(img, 128, ip, k >> 5, col, vp);
+        synth_image_put(img, 128, ip, k >> 5, col + 2, vt);
       } else {
         otor[c * plane + at] = vt;
         opol[c * plane + at] = vp;
