@@ -81,10 +81,9 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
   C* bufB = bufA + FB * rs;
   C* acc0 = bufB + FB * rs;
   C* acc1 = acc0 + FB * rs;
-  C* u0 = acc1;            // phase T (one product): u_theta, u_phi rows
-  C* u1 = acc1 + FB * rs;
+  C* u0 = acc1;            // phase T (one product): the velocity component in use
   // the twiddle table after the phase's buffers
-  const int nbuf = PH == FUSED_GRID ? 2 : (PH == FUSED_TEMPERATURE ? 5 : 4);
+  const int nbuf = PH == FUSED_GRID ? 2 : 4;
   C* stw = reinterpret_cast<C*>(smem_raw + (size_t)nbuf * FB * rs * sizeof(C));
 
   const int tid = threadIdx.x;
@@ -135,7 +134,7 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
   const float adv = -a.rf, mrf = -a.rf, lfr = a.lf;
 
   // consumer of one transformed component: grid rows or the products
-  // inputs: T phase [u_th, u_ph, g_r, g_th, g_ph, T]; V phase [u_th, u_ph,
+  // inputs: T phase [g_r, u_th, g_th, u_ph, g_ph, T]; V phase [u_th, u_ph,
   // w_th, w_ph, j_th, j_ph, b_th, b_ph]; M phase [u_th, u_ph, b_th, b_ph]
   int c = 0;
   float s_r = (PH == FUSED_TEMPERATURE) ? (float)a.sources[r] : 0.f;
@@ -152,18 +151,17 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
     const int q = ii * rs + ridx<N>(j);
     const float vN = z.x, vS = -z.y;
     if (PH == FUSED_TEMPERATURE) {
-      // -(u_r g_r + u_th g_th + u_ph g_ph) + S(r)
+      // -(u_r g_r + u_th g_th + u_ph g_ph) + S(r); each velocity component
+      // is held only until its gradient partner arrives
       if (c == 0) {
-        u0[q] = make_float2(vN, vS);
-      } else if (c == 1) {
-        u1[q] = make_float2(vN, vS);
-      } else if (c == 2) {
         acc0[q] = make_float2(ur * vN, ur * vS);
-      } else if (c == 3) {
+      } else if (c == 1 || c == 3) {
+        u0[q] = make_float2(vN, vS);
+      } else if (c == 2) {
         const C u = u0[q], t = acc0[q];
         acc0[q] = make_float2(t.x + u.x * vN, t.y + u.y * vS);
       } else {
-        const C u = u1[q], t = acc0[q];
+        const C u = u0[q], t = acc0[q];
         float xN = -(t.x + u.x * vN), xS = -(t.y + u.y * vS);
         if (s_r != 0.f) { xN += s_r; xS += s_r; }
         acc0[q] = make_float2(xN, xS);
@@ -263,7 +261,6 @@ size_t fused_smem(int phase, int n, bool unpadded) {
   const size_t twb = (size_t)n * sizeof(float2);
   switch (phase) {
     case FUSED_GRID: return 2 * buf + twb;
-    case FUSED_TEMPERATURE: return 5 * buf + twb;
     default: return 4 * buf + twb;
   }
 }

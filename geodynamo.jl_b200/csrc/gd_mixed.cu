@@ -285,7 +285,7 @@ int mixed_temperature_nl(gd_handle* h) {
   if (s) return s;
   // the velocity grid is the previous velocity phase's (carried in F(FC_U))
   FusedArgs f = phase_args(h);
-  const float4* fin[6] = {x->F(FC_U), x->F(FC_U + 1), x->F(FC_GR), x->F(FC_GTH), x->F(FC_GPH), x->F(FC_T)};
+  const float4* fin[6] = {x->F(FC_GR), x->F(FC_U), x->F(FC_GTH), x->F(FC_U + 1), x->F(FC_GPH), x->F(FC_T)};
   for (int i = 0; i < 6; ++i) f.fin[i] = fin[i];
   f.nin = 6;
   f.gout[0] = x->d_tgrid;
