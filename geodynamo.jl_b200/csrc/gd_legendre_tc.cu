@@ -1,5 +1,5 @@
 // gd_legendre_tc.cu -- mixed-precision Legendre synthesis and analysis on the
-// 5th-generation tensor cores (tcgen05.mma kind::tf32, M = 128, N = 64),
+// 5th-generation tensor cores (tcgen05.mma kind::tf32, M = 128, N <= 256),
 // FP32 accumulation in tensor memory.
 //
 // Each FP32/FP64 operand x is split into TF32 hi = rn(x) and lo = rn(x - hi);
@@ -32,14 +32,10 @@ using namespace tc;
 namespace {
 
 constexpr int TC_M = 128;
-constexpr int TC_N = 64;      // analysis (vector) column tile
 constexpr int TC_N2 = 128;    // synthesis and scalar analysis column tile
 constexpr int TC_K = 32;                       // TF32 elements per 128-byte row
 constexpr int TILE_A_FLOATS = TC_M * TC_K;      // 4096 floats = 16 KB
 constexpr int CHUNK_FLOATS = 2 * TILE_A_FLOATS; // hi image then lo image (32 KB)
-constexpr uint32_t IDESC = idesc_tf32(TC_M, TC_N);
-constexpr uint32_t IDESC2 = idesc_tf32(TC_M, TC_N2);
-constexpr uint32_t CHUNK_BYTES = CHUNK_FLOATS * 4;
 // Pipelined kernels: every stage holds one (chunk, parity) step; stages sit
 // back to back after a 1024-byte aligned base, then one mbarrier per stage
 // and the TMEM address slot (192 KB + alignment slack per CTA).
@@ -66,7 +62,7 @@ __device__ __forceinline__ void put_split_f(float* hi, float* lo, int row, int k
 
 // 3 TF32 products of one 32-deep chunk into tmem column offset dcol.
 __device__ __forceinline__ void issue_chunk(uint32_t tmem, uint32_t dcol, const float* Ahi, const float* Alo,
-                                            const float* Bhi, const float* Blo, bool first, uint32_t idesc = IDESC) {
+                                            const float* Bhi, const float* Blo, bool first, uint32_t idesc) {
   const uint32_t ah = smem_addr(Ahi), al = smem_addr(Alo), bh = smem_addr(Bhi), bl = smem_addr(Blo);
 #pragma unroll
   for (int ks = 0; ks < TC_K / 8; ++ks) {
@@ -288,10 +284,29 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
   bool ok = true;
 
   if (warp == 0) {
-    // producer: bulk copies only
+    // producer: bulk copies only.  Step (tile tt, it): table chunk(s) and the
+    // coefficient chunk; table rows past the last colatitude and coefficient
+    // columns past the last valid one only reach accumulator rows / columns
+    // the epilogue never reads, so whole 8-row swizzle atoms of the rest are
+    // copied.
+    auto step_src = [&](int tt, int it, const float*& s0, const float*& s1, const float*& sb, uint32_t& pa,
+                        uint32_t& pb) {
+      const int m = tt / (ntt * ncol), tile = (tt / ncol) % ntt, ct = tt % ncol;
+      const int nc1 = nck_h(L, m, 1);
+      int p, kc;
+      synth_step_pk(it, nc1, p, kc);
+      const long ch = synth_chunk(cofs, L, m, tile, p, kc);
+      const long bch = (long)ct * a.ttot + cofs[m] / ntt + it;
+      pa = (uint32_t)min(TC_M, (d.nth - tile * TC_M + 7) & ~7) * 128u;
+      const int nvalid = VEC ? 4 * min(32, d.nr - ct * 32) : min(NCS, Ntot - ct * NCS);
+      pb = (uint32_t)((nvalid + 7) & ~7) * 128u;
+      s0 = imgP + ch * CHUNK_FLOATS;
+      s1 = imgD + ch * CHUNK_FLOATS;
+      sb = a.bimg + bch * (2L * BT);
+    };
     int gs = 0, issued = -1;
     for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
-      const int m = tt / (ntt * ncol), tile = (tt / ncol) % ntt, ct = tt % ncol;
+      const int m = tt / (ntt * ncol);
       const int nc1 = nck_h(L, m, 1), T = nck_h(L, m, 0) + nc1;
       for (int it = 0; it < T; ++it) {
         const int G = gs + it, s = G & 1, u = G >> 1;
@@ -300,27 +315,19 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
           break;
         }
         if (lane == 0) {
-          int p, kc;
-          synth_step_pk(it, nc1, p, kc);
           float* A = stg + s * ST_FL;
-          const long ch = synth_chunk(cofs, L, m, tile, p, kc);
-          const long bch = (long)ct * a.ttot + cofs[m] / ntt + it;
-          // table rows past the last colatitude and coefficient columns past
-          // the last valid one only reach accumulator rows / columns the
-          // epilogue never reads: copy whole 8-row swizzle atoms of the rest
-          const uint32_t pa = (uint32_t)min(TC_M, (d.nth - tile * TC_M + 7) & ~7) * 128u;
-          const int nvalid = VEC ? 4 * min(32, d.nr - ct * 32) : min(NCS, Ntot - ct * NCS);
-          const uint32_t pb = (uint32_t)((nvalid + 7) & ~7) * 128u;
+          const float *s0, *s1, *sb;
+          uint32_t pa, pb;
+          step_src(tt, it, s0, s1, sb, pa, pb);
           mbar_arrive_expect_tx(&full[s], (VEC ? 4u : 2u) * pa + 2u * pb);
-#pragma unroll
-          for (int t = 0; t < (VEC ? 2 : 1); ++t) {
-            const float* src = (t == 0 ? imgP : imgD) + ch * CHUNK_FLOATS;
-            bulk_g2s(A + t * CHUNK_FLOATS, src, pa, &full[s]);
-            bulk_g2s(A + t * CHUNK_FLOATS + TILE_A_FLOATS, src + TILE_A_FLOATS, pa, &full[s]);
+          bulk_g2s(A, s0, pa, &full[s]);
+          bulk_g2s(A + TILE_A_FLOATS, s0 + TILE_A_FLOATS, pa, &full[s]);
+          if (VEC) {
+            bulk_g2s(A + CHUNK_FLOATS, s1, pa, &full[s]);
+            bulk_g2s(A + CHUNK_FLOATS + TILE_A_FLOATS, s1 + TILE_A_FLOATS, pa, &full[s]);
           }
-          const float* bsrc = a.bimg + bch * (2L * BT);
-          bulk_g2s(A + A_FL, bsrc, pb, &full[s]);
-          bulk_g2s(A + A_FL + BT, bsrc + BT, pb, &full[s]);
+          bulk_g2s(A + A_FL, sb, pb, &full[s]);
+          bulk_g2s(A + A_FL + BT, sb + BT, pb, &full[s]);
         }
         issued = G;
         __syncwarp();
@@ -467,28 +474,35 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
 }
 
 // ---------------------------------------------------------------------------
-// Analysis.  CTA = (m, column tile); K = colatitude in chunks of 32; one
-// pipeline step per (theta chunk, parity), with the loader groups and MMA
-// warp of the synthesis (group g fills stage g).  Scalar: 128 columns
-// n = (field, r, re/im), stages of 64 KB, accumulators [even | odd].
-// Vector: 64 columns [G_theta: 16 shells x re/im][G_phi], stages of 96 KB
-// holding the dPbar and Q chunks and two B tiles (fold 1 - p for dPbar, fold p
-// for Q), accumulators [dP even | dP odd | Q even | Q odd] x 64.
+// Analysis.  CTA = (m, column tile); K = colatitude in chunks of 32; two
+// loader groups of 4 warps (group g fills stage g: bulk copies of the table
+// chunks, FP32 inputs split to TF32 hi/lo while written) and one MMA warp.
+// Scalar: 128 columns n = (field, r, re/im), one step per (theta chunk,
+// parity), stages of 64 KB, accumulators [even | odd] x 128.
+// Vector: 128 columns, 32 shells x [G_theta re, im, G_phi re, im]; one step
+// per (theta chunk, fold f): the B tile holds fold f once and meets both the
+// dPbar chunk of parity 1 - f and the Q chunk of parity f, so every input
+// element is loaded once per tile; stages of 96 KB, accumulators
+// [dP even | dP odd | Q even | Q odd] x 128.  Columns past the last shell or
+// field are not loaded and the MMA width follows the tile's valid columns.
 // ---------------------------------------------------------------------------
 constexpr int WS_THREADS = 288;  // 2 loader groups x 4 warps + 1 MMA warp
+
+// MMA width of a tile with `nval` valid columns (M = 128 takes N % 16 == 0)
+__device__ __forceinline__ int tile_width(int nval) { return (nval + 15) & ~15; }
 
 template <bool VEC>
 __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const int* __restrict__ moff,
                                                          const float* __restrict__ img0,
                                                          const float* __restrict__ img1, TcAnalysisArgs a,
-                                                         int ncol) {
+                                                         int ncol, int csz) {
   constexpr int S = 2;
-  constexpr int NC = VEC ? TC_N : TC_N2;         // columns
+  constexpr int NC = TC_N2;                      // columns
   constexpr int A_FL = (VEC ? 2 : 1) * CHUNK_FLOATS;
   constexpr int BT = NC * TC_K;                  // one B image (hi or lo)
-  constexpr int B_FL = (VEC ? 2 : 1) * 2 * BT;
+  constexpr int B_FL = 2 * BT;
   constexpr int ST_FL = A_FL + B_FL;
-  constexpr uint32_t NCOL = 256;
+  constexpr uint32_t NCOL = VEC ? 512 : 256;
   extern __shared__ unsigned char smem_raw[];
   const uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   float* stg = reinterpret_cast<float*>(base);
@@ -524,14 +538,18 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
   const int m = tt / ncol, ct = tt % ncol;
   const int mb = moff[m];
-  const int n0 = ct * NC;
-  const int r0 = ct * 16;
+  // balanced column tiles: vector csz shells, scalar csz column pairs
+  const int n0 = ct * 2 * csz;
+  const int nval = VEC ? 4 * min(csz, d.nr - ct * csz) : min(2 * csz, Ntot - n0);
+  const int r0 = ct * csz;
+  const int nw = tile_width(nval);
+  const uint32_t idesc = idesc_tf32(TC_M, nw);
   __syncthreads();  // the previous tile's epilogue is done with TMEM and the column tables
   if (!VEC) {
     for (int c = tid; c < NC; c += blockDim.x) {
       const int ng = n0 + c;
       double* dst = nullptr;
-      if (ng < Ntot) {
+      if (c < nval) {
         const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, ci = rem & 1;
         dst = a.out[f] + ((size_t)ci * d.nr + r) * NM + mb - m;
       }
@@ -539,7 +557,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
       if ((c & 1) == 0) {
         const int pg = ng >> 1;
         long long ib = -1;
-        if (pg < Ntot / 2) {
+        if (c < nval) {
           const int f = pg / d.nr, r = pg % d.nr;
           ib = (long long)((((size_t)(f * d.nr + r) * (d.M + 1) + m) * 2) * d.nth);
         }
@@ -551,65 +569,77 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
 
   const int k1 = kpar(L, m, 1);
   const int np = k1 > 0 ? 2 : 1;
-  const int T = nthc * np;
+  // scalar: steps (chunk, parity); vector: steps (chunk, fold), both folds
+  // always (with k1 = 0 the odd-parity chunks hold zeros)
+  const int ns = VEC ? 2 : np;
+  const int T = nthc * ns;
 
   if (warp < 8) {
     const int g = warp >> 2, gw = warp & 3, gt = tid & 127;
     float* A = stg + g * ST_FL;
     float* B = A + A_FL;
-    for (int it = (g - gs) & 1; it < T; it += 2) {
+    // one float2 (re, im column pair) per item; NC / 2 pairs over 4 warps.
+    // The inputs of a group's next step are loaded into registers while the
+    // MMA still reads the stage.
+    constexpr int NV = NC / 8;
+    float2 v[NV];
+    auto load_step = [&](int it) {
+      const int cc = it / ns, p = it % ns;  // vector: p is the fold
+      const int ith = TC_K * cc + lane;
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        const int pr = gw + 4 * i;
+        v[i] = make_float2(0.f, 0.f);
+        if (2 * pr >= nw || ith >= d.nth) continue;
+        if (!VEC) {
+          const long long ib = colin[pr];
+          if (ib >= 0) v[i] = __ldg(&a.in[(size_t)ib + (size_t)p * d.nth + ith]);
+        } else {
+          const int r = r0 + (pr >> 1), comp = pr & 1;
+          if (r < r0 + csz && r < d.nr)
+            v[i] = __ldg(&a.in[(((size_t)(comp * d.nr + r) * (d.M + 1) + m) * 2 + p) * d.nth + ith]);
+        }
+      }
+    };
+    int it = (g - gs) & 1;
+    if (it < T) load_step(it);
+    for (; it < T; it += 2) {
       const int u = (gs + it) >> 1;
       if (u >= 1 && !mbar_wait(&empty[g], (u - 1) & 1, a.err)) {
         ok = false;
         break;
       }
-      const int cc = it / np, p = it % np;
+      const int cc = it / ns, p = it % ns;
       if (gt == 0) {
-        const long ch = (long)(m * 2 + p) * nthc + cc;
-        mbar_expect_tx(&full[g], (VEC ? 2u : 1u) * CHUNK_BYTES);
-        bulk_g2s(A, img0 + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[g]);
-        if (VEC) bulk_g2s(A + CHUNK_FLOATS, img1 + ch * CHUNK_FLOATS, CHUNK_BYTES, &full[g]);
+        // table rows past the parity's last degree only reach accumulator
+        // rows the epilogue never reads: copy whole 8-row swizzle atoms of
+        // the valid ones (hi and lo images separately)
+        const int pa0 = VEC ? 1 - p : p, pa1 = p;  // parity of the first / second table chunk
+        const uint32_t ra0 = (uint32_t)((kpar(L, m, pa0) + 7) & ~7) * 128u;
+        const uint32_t ra1 = VEC ? (uint32_t)((kpar(L, m, pa1) + 7) & ~7) * 128u : 0u;
+        mbar_expect_tx(&full[g], 2u * (ra0 + ra1));
+        const float* s0 = img0 + ((long)(m * 2 + pa0) * nthc + cc) * CHUNK_FLOATS;
+        if (ra0 > 0) {
+          bulk_g2s(A, s0, ra0, &full[g]);
+          bulk_g2s(A + TILE_A_FLOATS, s0 + TILE_A_FLOATS, ra0, &full[g]);
+        }
+        if (VEC && ra1 > 0) {
+          const float* s1 = img1 + ((long)(m * 2 + pa1) * nthc + cc) * CHUNK_FLOATS;
+          bulk_g2s(A + CHUNK_FLOATS, s1, ra1, &full[g]);
+          bulk_g2s(A + CHUNK_FLOATS + TILE_A_FLOATS, s1 + TILE_A_FLOATS, ra1, &full[g]);
+        }
         issued = u;
       }
-      const int ith = TC_K * cc + lane;
-      // float2 per thread: scalar NC/2 column pairs, vector 2 x NC/2 (slot, pair) items, over 4 warps
-      constexpr int NV = VEC ? NC / 4 : NC / 8;
-      float2 v[NV];
-      if (!VEC) {
 #pragma unroll
-        for (int i = 0; i < NV; ++i) {
-          const long long ib = colin[gw + 4 * i];
-          v[i] = make_float2(0.f, 0.f);
-          if (ib >= 0 && ith < d.nth) v[i] = __ldg(&a.in[(size_t)ib + (size_t)p * d.nth + ith]);
-        }
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-          const int pr = gw + 4 * i;
-          put_split_f(B, B + BT, 2 * pr, lane, v[i].x);
-          put_split_f(B, B + BT, 2 * pr + 1, lane, v[i].y);
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-          const int item = gw + 4 * i;
-          const int slot = item / (NC / 2), pr = item % (NC / 2);
-          const int fold = slot == 0 ? 1 - p : p;
-          const int comp = pr >> 4, r = r0 + (pr & 15);
-          v[i] = make_float2(0.f, 0.f);
-          if (r < d.nr && ith < d.nth)
-            v[i] = __ldg(&a.in[(((size_t)(comp * d.nr + r) * (d.M + 1) + m) * 2 + fold) * d.nth + ith]);
-        }
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-          const int item = gw + 4 * i;
-          const int slot = item / (NC / 2), pr = item % (NC / 2);
-          float* Bt = B + slot * 2 * BT;
-          put_split_f(Bt, Bt + BT, 2 * pr, lane, v[i].x);
-          put_split_f(Bt, Bt + BT, 2 * pr + 1, lane, v[i].y);
-        }
+      for (int i = 0; i < NV; ++i) {
+        const int pr = gw + 4 * i;
+        if (2 * pr >= nw) continue;
+        put_split_f(B, B + BT, 2 * pr, lane, v[i].x);
+        put_split_f(B, B + BT, 2 * pr + 1, lane, v[i].y);
       }
       fence_proxy_async();
       mbar_arrive(&full[g]);
+      if (it + 2 < T) load_step(it + 2);
     }
   } else {
     for (int it = 0; it < T; ++it) {
@@ -620,15 +650,15 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
       }
       fence_after_sync();
       if (lane == 0) {
-        const int cc = it / np, p = it % np;
+        const int cc = it / ns, p = it % ns;
         const float* A = stg + s * ST_FL;
         const float* B = A + A_FL;
         if (!VEC) {
-          issue_chunk(tmem, p * TC_N2, A, A + TILE_A_FLOATS, B, B + BT, cc == 0, IDESC2);
-        } else {
-          issue_chunk(tmem, (0 * 2 + p) * TC_N, A, A + TILE_A_FLOATS, B, B + BT, cc == 0, IDESC);
-          issue_chunk(tmem, (1 * 2 + p) * TC_N, A + CHUNK_FLOATS, A + CHUNK_FLOATS + TILE_A_FLOATS, B + 2 * BT,
-                      B + 3 * BT, cc == 0, IDESC);
+          issue_chunk(tmem, p * NC, A, A + TILE_A_FLOATS, B, B + BT, cc == 0, idesc);
+        } else {  // fold p: dPbar rows of parity 1 - p, Q rows of parity p
+          issue_chunk(tmem, (0 * 2 + 1 - p) * NC, A, A + TILE_A_FLOATS, B, B + BT, cc == 0, idesc);
+          issue_chunk(tmem, (1 * 2 + p) * NC, A + CHUNK_FLOATS, A + CHUNK_FLOATS + TILE_A_FLOATS, B, B + BT,
+                      cc == 0, idesc);
         }
         mma_commit(smem_addr(&empty[s]));
       }
@@ -651,9 +681,9 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
       const int kp = kpar(L, m, p);
       const int l = m + p + 2 * i;
       if (!VEC) {
-        for (int c0 = 64 * half; c0 < 64 * half + 64; c0 += 8) {
+        for (int c0 = (NC / 2) * half; c0 < (NC / 2) * half + NC / 2 && c0 < nw; c0 += 8) {
           float v[8];
-          tmem_ld8(trow + p * TC_N2 + c0, v);
+          tmem_ld8(trow + p * NC + c0, v);
           tmem_ld_wait();
           if (i < kp) {
 #pragma unroll
@@ -669,22 +699,22 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
       } else {
         const double fl = (l == 0) ? 0.0 : 1.0 / ((double)l * (l + 1.0));
         const double lf = (double)l * (l + 1.0);
-        for (int jj = 16 * half; jj < 16 * half + 16; jj += 8) {
-          float dth[8], dph[8], qth[8], qph[8];
-          tmem_ld8(trow + (0 * 2 + p) * TC_N + jj, dth);
-          tmem_ld8(trow + (0 * 2 + p) * TC_N + 32 + jj, dph);
-          tmem_ld8(trow + (1 * 2 + p) * TC_N + jj, qth);
-          tmem_ld8(trow + (1 * 2 + p) * TC_N + 32 + jj, qph);
+        // 8 columns = 2 shells x [G_theta re, im, G_phi re, im]
+        for (int c0 = (NC / 2) * half; c0 < (NC / 2) * half + NC / 2 && c0 < nw; c0 += 8) {
+          float dp[8], q[8];
+          tmem_ld8(trow + (0 * 2 + p) * NC + c0, dp);
+          tmem_ld8(trow + (1 * 2 + p) * NC + c0, q);
           tmem_ld_wait();
           if (i >= kp) continue;
 #pragma unroll
-          for (int j = 0; j < 8; j += 2) {
-            const int r = r0 + (jj + j) / 2;
-            if (r >= d.nr) continue;
-            const double Sre = ((double)dth[j] + (double)qph[j + 1]) * fl;
-            const double Sim = ((double)dth[j + 1] - (double)qph[j]) * fl;
-            const double Tre = ((double)qth[j + 1] - (double)dph[j]) * fl;
-            const double Tim = (-(double)qth[j] - (double)dph[j + 1]) * fl;
+          for (int s2 = 0; s2 < 2; ++s2) {
+            const int r = r0 + c0 / 4 + s2;
+            if (4 * (r - r0) >= nval) continue;
+            const int b = 4 * s2;
+            const double Sre = ((double)dp[b] + (double)q[b + 3]) * fl;
+            const double Sim = ((double)dp[b + 1] - (double)q[b + 2]) * fl;
+            const double Tre = ((double)q[b + 1] - (double)dp[b + 2]) * fl;
+            const double Tim = (-(double)q[b] - (double)dp[b + 3]) * fl;
             double o0re, o0im, o1re, o1im;
             if (a.epi == EPI_CURL_INDUCTION) {
               o0re = lf * Sre; o0im = lf * ((m == 0) ? 0.0 : Sim);
@@ -723,8 +753,8 @@ static size_t synth_smem(bool vec) {
   return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 3);
 }
 static size_t analysis_smem(bool vec) {
-  const int S = 2, NC = vec ? TC_N : TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS;
-  const int B = (vec ? 2 : 1) * 2 * NC * TC_K;
+  const int S = 2, NC = TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS;
+  const int B = 2 * NC * TC_K;
   return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 2) + (size_t)NC * 8 + (size_t)(NC / 2) * 8;
 }
 static bool g_attr_done = false;
@@ -779,15 +809,15 @@ void launch_tc_analysis(cudaStream_t s, const Dims& d, const int* moff, const fl
                         const TcAnalysisArgs& a) {
   set_attrs();
   if (a.epi == EPI_SCALAR) {
-    const int ncol = ceil_div(a.nf * d.nr * 2, TC_N2);
+    const int npair = a.nf * d.nr, ncol = ceil_div(2 * npair, TC_N2), csz = ceil_div(npair, ncol);
     const int ntiles = (d.M + 1) * ncol;
     k_tc_analysis3<false><<<std::min(ntiles, sm_count()), WS_THREADS, analysis_smem(false), s>>>(d, moff, img0,
-                                                                                                img1, a, ncol);
+                                                                                                img1, a, ncol, csz);
   } else {
-    const int ncol = ceil_div(d.nr, 16);
+    const int ncol = ceil_div(d.nr, 32), csz = ceil_div(d.nr, ncol);
     const int ntiles = (d.M + 1) * ncol;
     k_tc_analysis3<true><<<std::min(ntiles, sm_count()), WS_THREADS, analysis_smem(true), s>>>(d, moff, img0, img1,
-                                                                                              a, ncol);
+                                                                                              a, ncol, csz);
   }
 }
 
