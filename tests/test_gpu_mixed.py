@@ -32,6 +32,7 @@ SHAPES = [
     (31, 48, 96, 32, None),
     (20, 34, 40, 7, 10),
     (140, 212, 288, 5, None),   # several 128-row theta tiles, K chunks of both parities
+    (255, 384, 768, 3, None),   # the headline grid (lmax 255, nlon 768)
 ]
 
 
@@ -82,6 +83,23 @@ def test_mixed_step_tracks_oracle(gdb, oracle_mod):
         assert rel(a[0], b[0]) < 1e-5 and rel(a[1], b[1]) < 1e-5, k
     ek, em = g.energy(); oek, oem = o.energy()
     assert abs(ek - oek) / oek < 1e-6 and abs(em - oem) / oem < 1e-6
+
+
+def test_mixed_step_l255_tracks_oracle(gdb, oracle_mod):
+    # every fused phase kernel on the headline grid (nlon = 768 = 3 x 256)
+    g = gdb.SHTnsKitConfig(255, 384, 768, 4, dt=2e-6, precision="mixed")
+    o = oracle_mod.Oracle(lmax=255, nlat=384, nlon=768, nr=4, dt=2e-6)
+    for k, (a, b) in workloads.seeded_state(255, 255, 4, seed=0).items():
+        g.set_field(k, a, b)
+        o.set_field(k, a, b)
+    g.step(1); o.step(1)
+    for k in ("temp", "u_tor", "u_pol"):
+        a, b = g.get_nl(k), o.get_nl(k)
+        assert rel(a[0], b[0]) < TOL_T and rel(a[1], b[1]) < TOL_T, k
+    g.step(1); o.step(1)
+    for k in NAMES:
+        a, b = g.get_field(k), o.get_field(k)
+        assert rel(a[0], b[0]) < 1e-5 and rel(a[1], b[1]) < 1e-5, k
 
 
 def test_precision_switch_keeps_state(gdb):
