@@ -229,6 +229,44 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def run_ensemble(args, gdb, workloads, torch):
+    """Batched uneven ensemble: args.ensemble seeded shells (lmax 31-95, nr 33-65,
+    E and Ra drawn per member), one graph launch per step for all of them;
+    aggregate instance-steps/s, device-timed with CUDA events on the ensemble's
+    stream, FP64 and mixed precision."""
+    cfgs = workloads.ensemble_draw(args.ensemble)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        ens = gdb.Ensemble(cfgs, precision=prec)
+        for i, (c, m) in enumerate(zip(cfgs, ens.members)):
+            for k, (a, b) in workloads.seeded_state(c["lmax"], c["lmax"], c["nr"], seed=i).items():
+                m.set_field(k, a, b)
+        ens.step(args.warmup)
+        ext = torch.cuda.ExternalStream(ens.stream_ptr())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(ext)
+        ens.step_async(args.steps)
+        e1.record(ext)
+        ens.step(0)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ek = sum(m.energy()[0] for m in ens.members)
+        res[prec] = {"instance_steps_per_s": args.steps * len(cfgs) / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                     "sum_ekin": ek}
+        ens.close()
+    line = {"metric": f"ensemble instance-steps/s ({len(cfgs)} uneven shells)", "value": res["mixed"]["instance_steps_per_s"],
+            "unit": "instance-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f32/tf32x3 (FP64 solves)", "data": "synthetic (ensemble_draw(seed=3), seeded_state(seed=i))",
+            "config": {"workload": "ensemble", "members": len(cfgs), "lmax": sorted({c["lmax"] for c in cfgs}),
+                       "nr": sorted({c["nr"] for c in cfgs}), "dt": 1e-5, "launch": "one CUDA graph per step"},
+            "fp64": res["fp64"], "mixed": res["mixed"],
+            "ratio_vs_fp64_gpu": res["mixed"]["instance_steps_per_s"] / res["fp64"]["instance_steps_per_s"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -241,6 +279,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD,
                     help="named shell workload (the headline metric is shell_l255_nr129; smaller ones are for profiling)")
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="instead of the headline: the batched uneven ensemble of this many shells")
     args = ap.parse_args()
     if args.workload != WORKLOAD:
         globals()["WORKLOAD"] = args.workload
@@ -257,6 +297,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if args.ensemble > 0:
+        return run_ensemble(args, gdb, workloads, torch)
     dist = None
     if world > 1:
         import datetime

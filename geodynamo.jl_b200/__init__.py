@@ -58,6 +58,8 @@ EXPORTS = (
     "gd_implicit_step", "gd_step", "gd_step_async", "gd_set_dt", "gd_energy", "gd_check_finite",
     "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
     "gd_spectral_to_physical_noalloc",
+    "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
+    "gd_ensemble_step", "gd_ensemble_step_async", "gd_ensemble_failed_member", "gd_ensemble_get_stream",
 )
 
 
@@ -139,6 +141,14 @@ def load_library():
         "gd_profile_enable": ([P, I], I),
         "gd_profile_read": ([P, I, ctypes.c_char_p, D, ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "gd_spectral_to_physical_noalloc": ([P, I, ctypes.c_void_p, ctypes.c_void_p], I),
+        "gd_ensemble_create": ([ctypes.POINTER(GDConfig), I, I, ctypes.POINTER(P)], I),
+        "gd_ensemble_destroy": ([P], I),
+        "gd_ensemble_size": ([P], I),
+        "gd_ensemble_member": ([P, I], P),
+        "gd_ensemble_step": ([P, I], I),
+        "gd_ensemble_step_async": ([P, I], I),
+        "gd_ensemble_failed_member": ([P], I),
+        "gd_ensemble_get_stream": ([P, ctypes.POINTER(P)], I),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(lib, name)
@@ -202,6 +212,22 @@ class SHTnsKitConfig:
         st = self.lib.gd_create(ctypes.byref(self.cfg), int(device), ctypes.byref(h))
         if st != GD_OK:
             raise GeoDynamoError(st, "gd_create failed (see stderr)")
+        self._owned = True
+        self._attach(h, precision)
+
+    @classmethod
+    def _member(cls, lib, h, cfg: GDConfig):
+        """A view of an ensemble member's handle (owned by the ensemble)."""
+        self = cls.__new__(cls)
+        self.lib = lib
+        self.cfg = cfg
+        self._owned = False
+        self._attach(h, {v: k for k, v in PRECISIONS.items()}[cfg.precision])
+        return self
+
+    def _attach(self, h, precision):
+        cfg = self.cfg
+        lmax, mmax, nlat, nlon, nr = cfg.lmax, cfg.mmax, cfg.nlat, cfg.nlon, cfg.nr
         self.h = h
         self.lmax, self.mmax, self.nlat, self.nlon, self.nr = lmax, mmax, nlat, nlon, nr
         n = ctypes.c_int()
@@ -225,7 +251,8 @@ class SHTnsKitConfig:
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.gd_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.lib.gd_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -357,6 +384,71 @@ class SHTnsKitConfig:
             nm = names.raw[32 * k: 32 * k + 32].split(b"\0", 1)[0].decode()
             out[nm] = (float(ms[k]), int(cnt[k]))
         return out
+
+
+class Ensemble:
+    """Independent shells stepped together (gd_ensemble_*): one CUDA graph
+    launch per step runs every member's step as its own branch.  ``members``
+    are SHTnsKitConfig views of the member handles (upload, download, energy,
+    nonlinear terms as for a single model); the ensemble owns the handles."""
+
+    def __init__(self, configs, precision="fp64", device=0):
+        self.lib = load_library()
+        n = len(configs)
+        arr = (GDConfig * n)()
+        for i, c in enumerate(configs):
+            c = dict(c)
+            lmax = c.pop("lmax")
+            mmax = c.pop("mmax", None)
+            mmax = lmax if mmax is None else mmax
+            arr[i] = GDConfig(lmax, mmax, c.pop("nlat"), c.pop("nlon"), c.pop("nr"), c.pop("kl", 4),
+                              c.pop("rratio", 0.35), c.pop("ekman", 3e-4), c.pop("rayleigh", 80.0),
+                              c.pop("prandtl", 1.0), c.pop("magnetic_prandtl", 4.0), c.pop("dt", 1e-5),
+                              c.pop("implicit_theta", 0.5), c.pop("ab_mode", 0), c.pop("bc_mode", 0),
+                              c.pop("fd_mode", 0), PRECISIONS[c.pop("precision", precision)],
+                              c.pop("magnetic", 1))
+        e = ctypes.c_void_p()
+        st = self.lib.gd_ensemble_create(arr, n, int(device), ctypes.byref(e))
+        if st != GD_OK:
+            raise GeoDynamoError(st, "gd_ensemble_create failed (see stderr)")
+        self.e = e
+        self.members = [SHTnsKitConfig._member(self.lib, ctypes.c_void_p(self.lib.gd_ensemble_member(e, i)), arr[i])
+                        for i in range(n)]
+
+    def __len__(self):
+        return len(self.members)
+
+    def step(self, n=1):
+        st = self.lib.gd_ensemble_step(self.e, int(n))
+        if st != GD_OK:
+            i = self.lib.gd_ensemble_failed_member(self.e)
+            msg = self.lib.gd_last_error(self.members[i].h).decode() if i >= 0 else ""
+            raise GeoDynamoError(st, f"member {i}: {msg}")
+
+    def step_async(self, n=1):
+        st = self.lib.gd_ensemble_step_async(self.e, int(n))
+        if st != GD_OK:
+            raise GeoDynamoError(st, "gd_ensemble_step_async failed")
+
+    def stream_ptr(self):
+        s = ctypes.c_void_p()
+        st = self.lib.gd_ensemble_get_stream(self.e, ctypes.byref(s))
+        if st != GD_OK:
+            raise GeoDynamoError(st, "gd_ensemble_get_stream failed")
+        return s.value
+
+    def close(self):
+        if getattr(self, "e", None):
+            for m in self.members:
+                m.h = None
+            self.lib.gd_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

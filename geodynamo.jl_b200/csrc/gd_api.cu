@@ -305,6 +305,7 @@ int step_sequence(gd_handle* h, int boot) {
 }
 
 void drop_graphs(gd_handle* h) {
+  h->graph_gen++;
   for (int i = 0; i < 2; ++i)
     if (h->gexec[i]) { cudaGraphExecDestroy(h->gexec[i]); h->gexec[i] = nullptr; }
 }
@@ -733,6 +734,168 @@ int gd_profile_read(gd_handle* h, int max, char* names, double* ms, int* launche
     if (launches) launches[k] = h->prof_count[k];
   }
   h->prof_names.clear(); h->prof_ms.clear(); h->prof_count.clear();
+  return GD_OK;
+}
+
+// ---- batched ensemble ----------------------------------------------------------
+struct gd_ensemble {
+  std::vector<gd_handle*> members;
+  int device = 0;
+  cudaStream_t master = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  std::vector<int> gens;  // members' graph generations the ensemble graphs were captured at
+  int failed = -1;
+};
+
+int gd_ensemble_destroy(gd_ensemble* e) {
+  if (!e) return GD_ERR_ARG;
+  cudaSetDevice(e->device);
+  if (e->master) cudaStreamSynchronize(e->master);
+  for (int i = 0; i < 2; ++i)
+    if (e->gexec[i]) cudaGraphExecDestroy(e->gexec[i]);
+  for (gd_handle* h : e->members) gd_destroy(h);
+  for (cudaEvent_t ev : e->joins) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->master) cudaStreamDestroy(e->master);
+  delete e;
+  return GD_OK;
+}
+
+int gd_ensemble_create(const gd_config* cfgs, int n, int device, gd_ensemble** out) {
+  if (!cfgs || !out || n <= 0) return GD_ERR_ARG;
+  *out = nullptr;
+  gd_ensemble* e = new gd_ensemble();
+  e->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&e->master, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) {
+    gd_ensemble_destroy(e);
+    return GD_ERR_CUDA;
+  }
+  for (int i = 0; i < n; ++i) {
+    gd_handle* h = nullptr;
+    const int s = gd_create(&cfgs[i], device, &h);
+    if (s != GD_OK) {
+      fprintf(stderr, "gd_ensemble_create: member %d: status %d\n", i, s);
+      gd_ensemble_destroy(e);
+      return s;
+    }
+    e->members.push_back(h);
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      gd_ensemble_destroy(e);
+      return GD_ERR_CUDA;
+    }
+    e->joins.push_back(ev);
+  }
+  *out = e;
+  return GD_OK;
+}
+
+int gd_ensemble_size(const gd_ensemble* e) { return e ? (int)e->members.size() : -1; }
+
+gd_handle* gd_ensemble_member(gd_ensemble* e, int i) {
+  return (e && i >= 0 && i < (int)e->members.size()) ? e->members[i] : nullptr;
+}
+
+int gd_ensemble_failed_member(const gd_ensemble* e) { return e ? e->failed : -1; }
+
+int gd_ensemble_get_stream(gd_ensemble* e, void** stream) {
+  if (!e || !stream) return GD_ERR_ARG;
+  *stream = (void*)e->master;
+  return GD_OK;
+}
+
+// One graph: fork from the master stream to every member's stream, each
+// member's step sequence, join back.
+static int ensemble_graph(gd_ensemble* e, int boot) {
+  bool stale = e->gens.size() != e->members.size();
+  for (size_t i = 0; i < e->members.size() && !stale; ++i) stale = e->gens[i] != e->members[i]->graph_gen;
+  if (stale) {  // a member's parameters, precision or dt changed since the capture
+    for (int b = 0; b < 2; ++b)
+      if (e->gexec[b]) { cudaGraphExecDestroy(e->gexec[b]); e->gexec[b] = nullptr; }
+    e->gens.clear();
+    for (gd_handle* h : e->members) e->gens.push_back(h->graph_gen);
+  }
+  if (e->gexec[boot]) return GD_OK;
+  if (cudaStreamBeginCapture(e->master, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return GD_ERR_CUDA;
+  int st = GD_OK;
+  cudaError_t ce = cudaEventRecord(e->fork, e->master);
+  for (size_t i = 0; i < e->members.size() && st == GD_OK && ce == cudaSuccess; ++i) {
+    gd_handle* h = e->members[i];
+    ce = cudaStreamWaitEvent(h->stream, e->fork, 0);
+    if (ce != cudaSuccess) break;
+    st = step_sequence(h, boot);
+    if (st != GD_OK) { e->failed = (int)i; break; }
+    ce = cudaEventRecord(e->joins[i], h->stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->master, e->joins[i], 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(e->master, &g);
+  if (st != GD_OK || ce != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return st != GD_OK ? st : GD_ERR_CUDA;
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&e->gexec[boot], g, 0);
+  cudaGraphDestroy(g);
+  return ie == cudaSuccess ? GD_OK : GD_ERR_CUDA;
+}
+
+int gd_ensemble_step_async(gd_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return GD_ERR_ARG;
+  if (cudaSetDevice(e->device) != cudaSuccess) return GD_ERR_CUDA;
+  e->failed = -1;
+  for (int k = 0; k < nsteps; ++k) {
+    int boot = -1;
+    bool together = true;
+    for (gd_handle* h : e->members) {
+      const int b = (h->c.ab_mode == 1 || h->step_count == 0) ? 1 : 0;
+      if (boot < 0) boot = b;
+      if (b != boot || h->profiling) together = false;
+    }
+    if (together) {
+      // the members' streams may still run work queued outside the ensemble
+      for (gd_handle* h : e->members) {
+        cudaEvent_t ev = e->joins[0];
+        if (cudaEventRecord(ev, h->stream) != cudaSuccess || cudaStreamWaitEvent(e->master, ev, 0) != cudaSuccess)
+          return GD_ERR_CUDA;
+      }
+      const int s = ensemble_graph(e, boot);
+      if (s != GD_OK) return s;
+      if (cudaGraphLaunch(e->gexec[boot], e->master) != cudaSuccess) return GD_ERR_CUDA;
+      for (gd_handle* h : e->members) h->step_count++;
+    } else {
+      // each member's stream first waits for the ensemble's earlier graph launches
+      if (cudaEventRecord(e->fork, e->master) != cudaSuccess) return GD_ERR_CUDA;
+      for (gd_handle* h : e->members)
+        if (cudaStreamWaitEvent(h->stream, e->fork, 0) != cudaSuccess) return GD_ERR_CUDA;
+      for (size_t i = 0; i < e->members.size(); ++i) {
+        const int s = gd_step_async(e->members[i], 1);
+        if (s != GD_OK) { e->failed = (int)i; return s; }
+        // later graph launches on the master stream wait for this member
+        if (cudaEventRecord(e->joins[i], e->members[i]->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(e->master, e->joins[i], 0) != cudaSuccess)
+          return GD_ERR_CUDA;
+      }
+    }
+  }
+  return GD_OK;
+}
+
+int gd_ensemble_step(gd_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return GD_ERR_ARG;
+  int st = gd_ensemble_step_async(e, nsteps);
+  if (st != GD_OK) return st;
+  if (cudaStreamSynchronize(e->master) != cudaSuccess) return GD_ERR_CUDA;
+  for (size_t i = 0; i < e->members.size(); ++i) {
+    gd_handle* h = e->members[i];
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) { e->failed = (int)i; return GD_ERR_CUDA; }
+    if (h->precision == GD_PREC_MIXED) {
+      const int s = mixed_check_error(h);
+      if (s != GD_OK) { e->failed = (int)i; return s; }
+    }
+  }
   return GD_OK;
 }
 

@@ -45,6 +45,7 @@ struct gd_handle {
   gd::MixedState* mixed = nullptr;
   // graphs (index: boot flag)
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int graph_gen = 0;  // bumped whenever captured step graphs become stale
   // per-kernel event timing (gd_profile_enable)
   bool profiling = false;
   struct ProfRec { const char* name; cudaEvent_t a, b; };

@@ -37,6 +37,32 @@ def lm_arrays(lmax: int, mmax: int):
     return L, M
 
 
+# Batched uneven ensemble: lmax from {31, 47, 63, 95} with the 3/2-rule grid
+# nlat = 3 (lmax + 1) / 2, nlon = 2 nlat; nr from {33, 49, 65}; Ekman
+# log-uniform in [1e-4, 1e-3]; Rayleigh uniform in [50, 150]; all from
+# default_rng(3) in the order (lmax, nr, E, Ra) per instance; 200 steps at
+# dt = 1e-5 (the oracle configuration's step, none being specified);
+# instance i starts from seeded_state(seed=i).
+ENSEMBLE_LMAX = (31, 47, 63, 95)
+ENSEMBLE_NR = (33, 49, 65)
+
+
+def ensemble_draw(n: int = 64, seed: int = 3):
+    """List of n member configurations (dicts of SHTnsKitConfig keywords)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        lmax = int(ENSEMBLE_LMAX[rng.integers(len(ENSEMBLE_LMAX))])
+        nr = int(ENSEMBLE_NR[rng.integers(len(ENSEMBLE_NR))])
+        ekman = float(10.0 ** rng.uniform(-4.0, -3.0))
+        rayleigh = float(rng.uniform(50.0, 150.0))
+        nlat = 3 * (lmax + 1) // 2
+        c = dict(SHELL_PHYSICS)
+        c.update(lmax=lmax, nlat=nlat, nlon=2 * nlat, nr=nr, ekman=ekman, rayleigh=rayleigh, dt=1e-5)
+        out.append(c)
+    return out
+
+
 def radial_nodes(nr: int, rratio: float = 0.35):
     """r_n = ri + (1 + cos(pi (N - n) / (N - 1))) / 2, n = 1..N (src/fields.jl:108-131)."""
     ri = rratio / (1.0 - rratio)

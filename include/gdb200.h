@@ -170,6 +170,34 @@ int gd_energy(gd_handle* h, double* ekin, double* emag);
 int gd_check_finite(gd_handle* h);
 long gd_step_count(const gd_handle* h);
 
+/* ---- batched ensemble ----------------------------------------------------------
+ * Independent shells of different sizes and parameters stepped together (the
+ * batched uneven ensemble of 64 shell runs; the reference runs one model per
+ * process and has no counterpart).  The members are ordinary handles created
+ * from cfgs[0..n-1] on one device; each keeps its own stream and state and
+ * takes every gd_* call between ensemble steps.  gd_ensemble_step runs all
+ * members' steps as independent branches of one CUDA graph, one graph launch
+ * per step for the whole ensemble; when the members' AB-bootstrap flags differ
+ * or a member has per-kernel timing enabled, each member is stepped through
+ * its own graph on its own stream instead. */
+typedef struct gd_ensemble gd_ensemble;
+int gd_ensemble_create(const gd_config* cfgs, int n, int device, gd_ensemble** out);
+int gd_ensemble_destroy(gd_ensemble* e);
+int gd_ensemble_size(const gd_ensemble* e);
+/* Member i, owned by the ensemble (not to be passed to gd_destroy); null if out of range. */
+gd_handle* gd_ensemble_member(gd_ensemble* e, int i);
+/* nsteps steps of every member, then synchronises.  On failure returns the
+ * status of the first failing member; gd_ensemble_failed_member names it. */
+int gd_ensemble_step(gd_ensemble* e, int nsteps);
+/* Like gd_ensemble_step without the final synchronisation (errors raised by the
+ * kernels are reported by the next gd_ensemble_step); a member's own gd_* calls
+ * must wait until the ensemble stream has been synchronised. */
+int gd_ensemble_step_async(gd_ensemble* e, int nsteps);
+int gd_ensemble_failed_member(const gd_ensemble* e);
+/* The ensemble's own stream (cudaStream_t as void*): every graph-launched step is
+ * joined to it, so events recorded on it bracket whole ensemble steps. */
+int gd_ensemble_get_stream(gd_ensemble* e, void** stream);
+
 /* ---- tracing ------------------------------------------------------------------
  * The handle's CUDA stream (a cudaStream_t passed as void*), so a caller can
  * time work on it with its own events. */
