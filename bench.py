@@ -267,6 +267,103 @@ def run_ensemble(args, gdb, workloads, torch):
     return 0
 
 
+def run_adjoint(args, gdb, workloads, torch):
+    """Adjoint configuration (lmax 63, nr 65, 200 steps, literal boundaries,
+    checkpoints every 20 steps): gradient of the r = ro radial-field misfit with
+    respect to the initial B_pol, device time of the forward run and of the
+    reverse pass, and its agreement with FP64 central finite differences of the
+    GPU step on 32 directions and with the forward-mode derivative of the
+    oracle's step on 2 of them."""
+    c = workloads.CONFIGS["adjoint_l63_nr65"]
+    state = workloads.adjoint_state(c["lmax"], c["lmax"], c["nr"], seed=0)
+
+    def make(bpol=None):
+        m = gdb.SHTnsKitConfig(c["lmax"], c["nlat"], c["nlon"], c["nr"], dt=c["dt"], bc_mode=c["bc_mode"])
+        for k, (a, b) in state.items():
+            m.set_field(k, a, b)
+        if bpol is not None:
+            m.set_field("b_pol", *bpol)
+        return m
+
+    m = make()
+    tre, tim = workloads.adjoint_target(c["lmax"], c["lmax"], seed=1)
+    re = np.zeros(m.spec_shape()); im = np.zeros(m.spec_shape())
+    re[-1] = tre; im[-1] = tim
+    target = m.synth_scalar(re, im)[-1]
+    m.close()
+    # timing: forward (200 steps) and the reverse pass on a warm handle
+    m = make()
+    gdb.magnetic_misfit(m, target, c["steps"], c["checkpoint"])
+    for k, (a, b) in state.items():
+        m.set_field(k, a, b)
+    t0 = time.perf_counter()
+    J, gre, gim, ckpt = gdb.magnetic_misfit(m, target, c["steps"], c["checkpoint"])
+    t_total = time.perf_counter() - t0
+    lam = (np.random.default_rng(0).standard_normal(m.spec_shape()),) * 2
+    ext = torch.cuda.ExternalStream(m.stream_ptr())
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    m.synchronize(); e0.record(ext)
+    m.step_async(c["steps"])
+    e1.record(ext); m.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    t1 = time.perf_counter()
+    m.magnetic_pullback("b_pol", c["steps"], *lam)
+    pull_ms = (time.perf_counter() - t1) * 1e3
+    m.close()
+
+    def dot(a, b):
+        return float(np.sum(a[0] * b[0]) + np.sum(a[1] * b[1]))
+
+    def misfit(bpol):
+        mm = make(bpol)
+        mm.step(c["steps"])
+        r = gdb.radial_field_outer(mm, *mm.get_field("b_pol")) - target
+        mm.close()
+        return 0.5 * float(np.sum(r * r))
+
+    b0 = state["b_pol"]
+    dirs = workloads.adjoint_directions(c["lmax"], c["lmax"], c["nr"], count=32, seed=2)
+    fd_err = []
+    for v in dirs:
+        eps = 1e-3 * np.sqrt(dot(b0, b0) / dot(v, v))
+        fd = (misfit((b0[0] + eps * v[0], b0[1] + eps * v[1])) - misfit((b0[0] - eps * v[0], b0[1] - eps * v[1]))) / (2 * eps)
+        ad = dot((gre, gim), v)
+        fd_err.append(abs(fd - ad) / abs(ad))
+    from oracle.oracle import Oracle
+    probe = make()
+
+    def oracle_radial(bpol):
+        o = Oracle(lmax=c["lmax"], nlat=c["nlat"], nlon=c["nlon"], nr=c["nr"], dt=c["dt"], bc_mode=c["bc_mode"])
+        for k, (a, b) in state.items():
+            o.set_field(k, a, b)
+        o.set_field("b_pol", *bpol)
+        o.step(c["steps"])
+        pre, pim = o.get_field("b_pol")
+        f = probe.l_values * (probe.l_values + 1.0) / probe.r[-1] ** 2
+        r2 = np.zeros(probe.spec_shape()); i2 = np.zeros(probe.spec_shape())
+        r2[-1] = f * pre[-1]; i2[-1] = f * pim[-1]
+        return o.synth_scalar(r2, i2)[-1]
+
+    resid = oracle_radial(b0) - target
+    fm_err = []
+    for v in dirs[:2]:
+        fwd = float(np.sum(resid * oracle_radial(v)))
+        ad = dot((gre, gim), v)
+        fm_err.append(abs(fwd - ad) / abs(ad))
+    probe.close()
+    line = {"metric": "adjoint gradient vs FP64 finite differences (max relative error, 32 directions)",
+            "value": max(fd_err), "unit": "relative error", "higher_is_better": False, "n_gpus": 1,
+            "dtype": "f64", "data": "synthetic (adjoint_state(0): seeded_state(0) with zero temperature; adjoint_target(seed=1); directions default_rng(2))",
+            "config": {"workload": "adjoint_l63_nr65", "lmax": c["lmax"], "nlat": c["nlat"], "nlon": c["nlon"],
+                       "nr": c["nr"], "steps": c["steps"], "dt": c["dt"], "bc_mode": c["bc_mode"],
+                       "checkpoint_every": c["checkpoint"]},
+            "J": J, "fd_rel_err_max": max(fd_err), "fd_rel_err_median": float(np.median(fd_err)),
+            "oracle_forward_mode_rel_err_max": max(fm_err), "forward_ms_device": fwd_ms,
+            "pullback_ms_wall": pull_ms, "misfit_and_gradient_s_wall": t_total, "checkpoints": len(ckpt)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -279,6 +376,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD,
                     help="named shell workload (the headline metric is shell_l255_nr129; smaller ones are for profiling)")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="instead of the headline: the adjoint configuration's gradient checks and timings")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead of the headline: the batched uneven ensemble of this many shells")
     args = ap.parse_args()
@@ -299,6 +398,8 @@ def main():
     torch.cuda.set_device(local)
     if args.ensemble > 0:
         return run_ensemble(args, gdb, workloads, torch)
+    if args.adjoint:
+        return run_adjoint(args, gdb, workloads, torch)
     dist = None
     if world > 1:
         import datetime

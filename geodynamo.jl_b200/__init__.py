@@ -58,6 +58,7 @@ EXPORTS = (
     "gd_implicit_step", "gd_step", "gd_step_async", "gd_set_dt", "gd_energy", "gd_check_finite",
     "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
     "gd_spectral_to_physical_noalloc",
+    "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
     "gd_ensemble_step", "gd_ensemble_step_async", "gd_ensemble_failed_member", "gd_ensemble_get_stream",
 )
@@ -141,6 +142,8 @@ def load_library():
         "gd_profile_enable": ([P, I], I),
         "gd_profile_read": ([P, I, ctypes.c_char_p, D, ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "gd_spectral_to_physical_noalloc": ([P, I, ctypes.c_void_p, ctypes.c_void_p], I),
+        "gd_spectral_to_physical_adjoint": ([P, I, D, D, D], I),
+        "gd_magnetic_pullback": ([P, I, I, D, D, D, D], I),
         "gd_ensemble_create": ([ctypes.POINTER(GDConfig), I, I, ctypes.POINTER(P)], I),
         "gd_ensemble_destroy": ([P], I),
         "gd_ensemble_size": ([P], I),
@@ -292,6 +295,23 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_physical_to_spectral(self.h, nf, _dptr(grid), _dptr(re), _dptr(im)))
         return re, im
 
+    def synth_scalar_adjoint(self, grid):
+        """Transpose of synth_scalar: grid cotangent -> (re, im) cotangents."""
+        grid = _f64(grid)
+        nf = grid.size // (self.nr * self.nlat * self.nlon)
+        shape = ((nf,) + self.spec_shape()) if grid.ndim == 4 else self.spec_shape()
+        re = np.zeros(shape); im = np.zeros(shape)
+        self._check(self.lib.gd_spectral_to_physical_adjoint(self.h, nf, _dptr(grid), _dptr(re), _dptr(im)))
+        return re, im
+
+    def magnetic_pullback(self, name, nsteps, lam_re, lam_im):
+        """Pullback of nsteps steps w.r.t. the magnetic component ``name``
+        ("b_tor" or "b_pol") at their start (gd_magnetic_pullback)."""
+        re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
+        self._check(self.lib.gd_magnetic_pullback(self.h, FIELDS[name], int(nsteps), _dptr(_f64(lam_re)),
+                                                  _dptr(_f64(lam_im)), _dptr(re), _dptr(im)))
+        return re, im
+
     def synth_vector(self, tre, tim, pre, pim):
         vt = np.zeros(self.grid_shape()); vp = np.zeros(self.grid_shape())
         self._check(self.lib.gd_vector_synthesis(self.h, _dptr(_f64(tre)), _dptr(_f64(tim)), _dptr(_f64(pre)),
@@ -384,6 +404,53 @@ class SHTnsKitConfig:
             nm = names.raw[32 * k: 32 * k + 32].split(b"\0", 1)[0].decode()
             out[nm] = (float(ms[k]), int(cnt[k]))
         return out
+
+
+def radial_field_outer(model, pol_re, pol_im):
+    """B_r on the grid at r = ro from poloidal coefficients (nr, nlm):
+    l(l+1) / ro^2 P_lm(ro) synthesised (the build's radial-field formula; the
+    reference never forms B_r).  Returns (nlon, nlat)."""
+    ro = model.r[-1]
+    f = model.l_values * (model.l_values + 1.0) / ro ** 2
+    re = np.zeros(model.spec_shape()); im = np.zeros(model.spec_shape())
+    re[-1] = f * pol_re[-1]; im[-1] = f * pol_im[-1]
+    return model.synth_scalar(re, im)[-1]
+
+
+def magnetic_misfit(model, target, nsteps, checkpoint_every=20):
+    """Objective of the adjoint configuration and its gradient.
+
+    Runs ``nsteps`` steps from the model's current state and returns
+    (J, grad_re, grad_im, checkpoints) with
+      J = 1/2 sum_grid (B_r(ro) - target)^2   (target: (nlon, nlat) grid),
+    the gradient of J with respect to the initial poloidal magnetic
+    coefficients (nr x nlm Re and Im planes, l-major), and the state
+    (dict name -> (re, im)) every ``checkpoint_every`` steps.  Reverse pass:
+    the residual goes through the transposed synthesis and the l(l+1)/ro^2
+    factor to the cotangent of B_pol(ro), then through gd_magnetic_pullback.
+    The pullback needs none of the checkpoints: the magnetic propagator of the
+    reference's step does not depend on the state (gd_magnetic_pullback); they
+    are kept for restarts and for objectives whose pullback would."""
+    checkpoints = []
+    done = 0
+    while done < nsteps:
+        if checkpoint_every and done % checkpoint_every == 0:
+            checkpoints.append((done, {k: model.get_field(k) for k in FIELDS}))
+        k = min(checkpoint_every or nsteps, nsteps - done)
+        model.step(k)
+        done += k
+    pre, pim = model.get_field("b_pol")
+    resid = radial_field_outer(model, pre, pim) - target
+    J = 0.5 * float(np.sum(resid * resid))
+    gbar = np.zeros(model.grid_shape())
+    gbar[-1] = resid
+    cre, cim = model.synth_scalar_adjoint(gbar)
+    ro = model.r[-1]
+    f = model.l_values * (model.l_values + 1.0) / ro ** 2
+    lre = np.zeros(model.spec_shape()); lim = np.zeros(model.spec_shape())
+    lre[-1] = f * cre[-1]; lim[-1] = f * cim[-1]
+    gre, gim = model.magnetic_pullback("b_pol", nsteps, lre, lim)
+    return J, gre, gim, checkpoints
 
 
 class Ensemble:

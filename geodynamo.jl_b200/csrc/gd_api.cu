@@ -553,6 +553,58 @@ int gd_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double
   return check_launch(h, "physical_to_spectral");
 }
 
+int gd_spectral_to_physical_adjoint(gd_handle* h, int nfield, const double* grid, double* re, double* im) {
+  if (!h || !re || !im || !grid || nfield < 1) return h ? fail(h, GD_ERR_ARG, "bad arguments") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm, G = h->grid_elems();
+  const double f0 = (double)h->d.nlon / (2.0 * 3.14159265358979323846), f1 = 2.0 * f0;
+  for (int f0i = 0; f0i < nfield; f0i += 4) {
+    const int nf = nfield - f0i < 4 ? nfield - f0i : 4;
+    CK(cudaMemcpyAsync(h->d_stage_grid, grid + G * f0i, G * nf * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    launch_divide_by_weights(h->stream, G * nf, h->d.nlat, h->d_w, h->d_stage_grid);
+    launch_grid_to_native(h->stream, h->d, h->d_stage_grid, h->d_stage_grid2, nf);
+    double* out[4];
+    for (int i = 0; i < nf; ++i) out[i] = h->d_stage_spec2 + 2 * plane * i;
+    if (h->precision == GD_PREC_MIXED) s = mixed_api_analysis_scalar(h, h->d_stage_grid2, nf, out);
+    else s = analysis_scalar(h, h->d_stage_grid2, nf, out);
+    if (s) return s;
+    launch_scale_by_order(h->stream, 2 * (size_t)h->d.nr * nf, h->d.nlm, h->d_mof, f0, f1, h->d_stage_spec2);
+    launch_native_to_lmajor(h->stream, h->d, h->d_perm, h->d_stage_spec2, h->d_stage_spec, 2 * nf);
+    for (int i = 0; i < nf; ++i) {
+      CK(cudaMemcpyAsync(re + plane * (f0i + i), h->d_stage_spec + 2 * plane * i, plane * sizeof(double),
+                         cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaMemcpyAsync(im + plane * (f0i + i), h->d_stage_spec + 2 * plane * i + plane, plane * sizeof(double),
+                         cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return check_launch(h, "spectral_to_physical_adjoint");
+}
+
+int gd_magnetic_pullback(gd_handle* h, int field, int nsteps, const double* lam_re, const double* lam_im,
+                         double* out_re, double* out_im) {
+  if (!h || !lam_re || !lam_im || !out_re || !out_im || nsteps < 0 || (field != GD_B_TOR && field != GD_B_POL))
+    return h ? fail(h, GD_ERR_ARG, "bad arguments (field must be GD_B_TOR or GD_B_POL)") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm;
+  CK(cudaMemcpyAsync(h->d_stage_spec, lam_re, plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_stage_spec + plane, lam_im, plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_lmajor_to_native(h->stream, h->d, h->d_perm, h->d_stage_spec, h->d_stage_spec2, 2);
+  // without the magnetic field the step leaves it untouched: the pullback is the identity
+  if (h->c.magnetic && nsteps > 0)
+    launch_cnab2_pullback(h->stream, h->d, h->d_lof, h->d_lin, h->d_lu, 1, h->c.dt, h->c.implicit_theta,
+                          h->c.bc_mode == 1, h->c.bc_mode == 2, nsteps, h->d_stage_spec2);
+  launch_native_to_lmajor(h->stream, h->d, h->d_perm, h->d_stage_spec2, h->d_stage_spec, 2);
+  CK(cudaMemcpyAsync(out_re, h->d_stage_spec, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(out_im, h->d_stage_spec + plane, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "magnetic_pullback");
+}
+
 int gd_vector_synthesis(gd_handle* h, const double* tor_re, const double* tor_im, const double* pol_re,
                         const double* pol_im, double* v_theta, double* v_phi) {
   if (!h || !tor_re || !tor_im || !pol_re || !pol_im || !v_theta || !v_phi)

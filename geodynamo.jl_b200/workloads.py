@@ -27,7 +27,10 @@ CONFIGS = {
     # workload at a quarter of its memory (profiling captures)
     "shell_l255_nr33": dict(lmax=255, nlat=384, nlon=768, nr=33, dt=2e-6, steps=100),
     "shell_l127_nr65": dict(lmax=127, nlat=192, nlon=384, nr=65, dt=5e-6, steps=100),
-    "adjoint_l63_nr65": dict(lmax=63, nlat=96, nlon=192, nr=65, dt=1e-5, steps=200),
+    # adjoint configuration: the reference's literal boundaries (bc_mode 0; any
+    # Dirichlet row on B would pin B_pol(ro) and the misfit to constants),
+    # started from adjoint_state (temperature zero)
+    "adjoint_l63_nr65": dict(lmax=63, nlat=96, nlon=192, nr=65, dt=1e-5, steps=200, bc_mode=0, checkpoint=20),
 }
 
 
@@ -60,6 +63,50 @@ def ensemble_draw(n: int = 64, seed: int = 3):
         c = dict(SHELL_PHYSICS)
         c.update(lmax=lmax, nlat=nlat, nlon=2 * nlat, nr=nr, ekman=ekman, rayleigh=rayleigh, dt=1e-5)
         out.append(c)
+    return out
+
+
+def adjoint_target(lmax: int, mmax: int, seed: int = 1, lcut: int = 12):
+    """Target radial-field coefficients of the adjoint configuration: complex
+    Gaussian x (l+1)^-2 for l <= lcut, zero above, Im = 0 at m = 0; (re, im),
+    each (nlm,) l-major."""
+    rng = np.random.default_rng(seed)
+    L, M = lm_arrays(lmax, mmax)
+    g = rng.standard_normal((L.size, 2))
+    c = g * ((L + 1.0) ** -2.0)[:, None] * (L <= lcut)[:, None]
+    re = np.ascontiguousarray(c[:, 0])
+    im = np.ascontiguousarray(c[:, 1])
+    im[M == 0] = 0.0
+    return re, im
+
+
+def adjoint_state(lmax: int, mmax: int, nr: int, seed: int = 0):
+    """Initial state of the adjoint configuration: seeded_state with the
+    temperature set to zero.  Under the literal operator a nonzero temperature
+    overflows within ~150 steps at lmax 63, nr 65; from zero (no sources, zero
+    boundary values) it stays exactly zero.  The misfit does not depend on the
+    temperature: it never feeds back into the velocity (the vector analysis
+    drops the radial buoyancy force, src/shtnskit_field_functions.jl:309-313)
+    nor into the magnetic field."""
+    st = seeded_state(lmax, mmax, nr, seed=seed)
+    re, im = st["temp"]
+    st["temp"] = (np.zeros_like(re), np.zeros_like(im))
+    return st
+
+
+def adjoint_directions(lmax: int, mmax: int, nr: int, count: int = 32, seed: int = 2):
+    """Random directions for the finite-difference checks of the gradient with
+    respect to B_pol: standard normals (nr, nlm) x2 with the state's
+    conventions (Im = 0 at m = 0, l = 0 zero), drawn from default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    L, M = lm_arrays(lmax, mmax)
+    out = []
+    for _ in range(count):
+        g = rng.standard_normal((nr, L.size, 2))
+        re = np.ascontiguousarray(g[..., 0]); im = np.ascontiguousarray(g[..., 1])
+        im[:, M == 0] = 0.0
+        re[:, L == 0] = 0.0; im[:, L == 0] = 0.0
+        out.append((re, im))
     return out
 
 

@@ -170,6 +170,33 @@ int gd_energy(gd_handle* h, double* ekin, double* emag);
 int gd_check_finite(gd_handle* h);
 long gd_step_count(const gd_handle* h);
 
+/* ---- reverse mode ---------------------------------------------------------------
+ * Pieces of the gradient of an objective of the state with respect to the
+ * initial state (the adjoint configuration: misfit of the radial magnetic
+ * field at r = ro against a target, with respect to the initial poloidal
+ * magnetic coefficients).  The reference has no adjoint.
+ *
+ * Transpose of gd_spectral_to_physical: for a cotangent of the grids (nfield x
+ * nr x nlon x nlat, reference layout) the cotangents of the Re and Im
+ * coefficients (nfield x nr x nlm each, l-major).  Computed as the Gauss
+ * analysis of grid / w_theta scaled by nlon / 2 pi (m = 0) and nlon / pi (m > 0);
+ * the m = 0 imaginary parts, which the synthesis ignores, get zero. */
+int gd_spectral_to_physical_adjoint(gd_handle* h, int nfield, const double* grid, double* re, double* im);
+/* Pullback of nsteps model steps (gd_step) with respect to the magnetic
+ * field component `field` (GD_B_TOR or GD_B_POL) at their start: given the
+ * cotangent lambda of that component after the steps (nr x nlm Re and Im
+ * planes, l-major), returns M^T ... M^T lambda.  In the reference's step the
+ * magnetic field evolves by its implicit operator alone -- its nonlinear term
+ * u x B and its Lorentz coupling j x B are products with the zero radial
+ * components of the synthesized vectors (src/shtnskit_field_functions.jl:
+ * 264-279, src/magnetic.jl:375-404, src/velocity.jl:638-672), zero in value
+ * and in first derivative -- so M = S^-1 R per step (with the boundary rows
+ * of bc_mode 1 and 2), the same for every step and every state, and this is
+ * the exact gradient of anything that depends on the field after the steps.
+ * FP64 in both precision modes (the implicit solve is FP64 in both). */
+int gd_magnetic_pullback(gd_handle* h, int field, int nsteps, const double* lam_re, const double* lam_im,
+                         double* out_re, double* out_im);
+
 /* ---- batched ensemble ----------------------------------------------------------
  * Independent shells of different sizes and parameters stepped together (the
  * batched uneven ensemble of 64 shell runs; the reference runs one model per
