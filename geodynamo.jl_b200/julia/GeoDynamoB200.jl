@@ -112,6 +112,35 @@ function step!(h::Handle, state; nsteps::Integer = 1)
     return state
 end
 
+# Reverse mode.  magnetic_pullback(h, :b_pol, nsteps, λre, λim) -> (gre, gim):
+# the vector-Jacobian product of nsteps steps with respect to a magnetic
+# component at their start (gd_magnetic_pullback; planes (nlm, nr), as the
+# field data).  A ChainRulesCore rule for the step, for objectives of the
+# magnetic field, is then
+#     function ChainRulesCore.rrule(::typeof(magnetic_steps), h, bpol_re, bpol_im, nsteps)
+#         out = magnetic_steps(h, bpol_re, bpol_im, nsteps)
+#         pullback(Δ) = (NoTangent(), NoTangent(),
+#                        magnetic_pullback(h, :b_pol, nsteps, Δ[1], Δ[2])..., NoTangent())
+#         return out, pullback
+#     end
+# (written here as a comment: ChainRulesCore is not a dependency of this shim).
+function magnetic_pullback(h::Handle, f::Symbol, nsteps::Integer, lre::AbstractArray{Float64},
+                           lim::AbstractArray{Float64})
+    gre = similar(lre); gim = similar(lim)
+    GC.@preserve lre lim gre gim check(h, ccall((:gd_magnetic_pullback, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+        h.ptr, FIELD[f], nsteps, lre, lim, gre, gim))
+    return gre, gim
+end
+
+# Transpose of spectral_to_physical! (gd_spectral_to_physical_adjoint).
+function spectral_to_physical_adjoint!(h::Handle, phys_bar, spec_bar)
+    g = parent(phys_bar.data); re = parent(spec_bar.data_real); im = parent(spec_bar.data_imag)
+    GC.@preserve re im g check(h, ccall((:gd_spectral_to_physical_adjoint, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, 1, g, re, im))
+    return spec_bar
+end
+
 function energies(h::Handle)
     ek = Ref{Cdouble}(0); em = Ref{Cdouble}(0)
     check(h, ccall((:gd_energy, LIB), Cint, (Ptr{Cvoid}, Ref{Cdouble}, Ref{Cdouble}), h.ptr, ek, em))
