@@ -332,8 +332,9 @@ constexpr int ct_pass_tw_entries(int N) {
   return tot;
 }
 
-// Fills the per-pass tables from the full table W_N^i (global memory).
-template <int N, int NT>
+// Fills the per-pass tables from the full table W_N^i (global memory); TS > 1:
+// the table is W_(TS N)^i, read at TS-fold indices.
+template <int N, int NT, int TS = 1>
 __device__ __forceinline__ void ct_fill_pass_twiddles(const float2* __restrict__ tw_full, float2* __restrict__ out) {
   constexpr CPlan P = PlanOf<N>::p;
   int ns = 1, off = 0;
@@ -344,7 +345,7 @@ __device__ __forceinline__ void ct_fill_pass_twiddles(const float2* __restrict__
       const int step = N / (ns * R);
       for (int e = threadIdx.x; e < (R - 1) * ns; e += NT) {
         const int r = e / ns + 1, k = e - (r - 1) * ns;
-        out[off + e] = tw_full[r * k * step];
+        out[off + e] = tw_full[TS * r * k * step];
       }
       off += (R - 1) * ns;
     }

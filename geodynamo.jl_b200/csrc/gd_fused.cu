@@ -69,11 +69,32 @@ __device__ __forceinline__ void pack_z(float2* bufA, int rs, int n, int e, int r
   }
 }
 
+// Lengths n = 3 P with P a power of two (P >= 8).  When every order m <= M
+// < P, the conjugated input y is zero on P <= k <= 2P, so with phi = 3 c + a
+// the inverse transform is three P-point transforms of
+//   W_a[k] = W^(k a) (y_k + y_(k + 2P) W^(2 P a)),   W = exp(-2 pi i / n),
+// built straight from the frequency pair (k, P - k) -- no zero band and no
+// radix-3 pass -- and the forward transform's outputs X_m, X_(n - m) (m <= M)
+// follow from the P-point transforms Y_a of the sub-rows x_(3 c + a):
+//   X_m = sum_a W^(m a) Y_a[m],  X_(n - m) = sum_a W^(-m a) Y_a[(P - m) mod P].
+// Sub-row (pair ii, a) holds P elements at (3 ii + a) P in the xidx layout.
+// The last P-point pass has fewer butterflies than threads, so the split is
+// used where the products are light (the induction phase): with the heavier
+// velocity and temperature products the radix-3 pass, which spreads them over
+// every thread, is faster.
+template <int N> struct Split3 {
+  static constexpr int P = N / 3;
+  static constexpr bool ok = N > 0 && N % 3 == 0 && P >= 8 && (P & (P - 1)) == 0;
+};
+
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+
 }  // namespace
 
-template <int N, int PH>
+template <int N, int PH, bool S3>
 __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float2* __restrict__ tw, FusedArgs a) {
   typedef float2 C;
+  constexpr int P = S3 ? N / 3 : 1;
   const int n = N > 0 ? N : p.n;
   const int rs = row_stride<N>(n);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -94,7 +115,13 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
   const int tot = (M + 1) * FB;
   const size_t boff = ((size_t)r * gridDim.x + ib) * (size_t)tot;
 
-  if constexpr (N > 0) {
+  // S3: the P-point passes' tables, then W^k for k < 2P
+  C* const stw3 = stw + (S3 ? ct_pass_tw_entries(P) : 0);
+  if constexpr (S3) {
+    static_assert(ct_pass_tw_entries(P) + 2 * P <= N, "twiddles exceed the table space");
+    ct_fill_pass_twiddles<P, FNT, 3>(tw, stw);
+    for (int k = tid; k < 2 * P; k += FNT) stw3[k] = tw[k];
+  } else if constexpr (N > 0) {
     static_assert(ct_pass_tw_entries(N) <= N, "per-pass twiddles exceed the table space");
     ct_fill_pass_twiddles<N, FNT>(tw, stw);
   } else {
@@ -108,27 +135,77 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
   }
 
   float4 pf[PF];
+  // S3 items: (pair ii, j) for j = 0..P/2, each the frequencies j and P - j
+  constexpr int H = P / 2 + 1;
+  auto s3_load = [&](const float4* src, int it, float4& v1, float4& v2) {
+    const int ii = it / H, j = it - ii * H;
+    v1 = v2 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (it >= FB * H || ii >= rows) return;
+    if (j <= M) v1 = __ldg(src + j * FB + ii);
+    if (P - j <= M) v2 = __ldg(src + (P - j) * FB + ii);
+  };
   auto prefetch = [&](int c) {
     const float4* src = a.fin[c] + boff;
+    if constexpr (S3) {
 #pragma unroll
-    for (int k = 0; k < PF; ++k) {
-      const int e = tid + k * FNT;
-      pf[k] = e < tot ? __ldg(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int k = 0; k < PF / 2; ++k) s3_load(src, tid + k * FNT, pf[2 * k], pf[2 * k + 1]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < PF; ++k) {
+        const int e = tid + k * FNT;
+        pf[k] = e < tot ? __ldg(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  };
+  // S3: W_a[k] for the sub-rows of pair ii from y_k and y_(k + 2P)
+  auto s3_put = [&](int ii, int k, C y, C y2) {
+    const C cp = stw3[P];  // W^P; W^(2P) = conj(W^P), W^(4P) = W^P
+    C* row = bufA + ii * N;
+    const int xk = xidx(k);
+    row[xk] = cadd(y, y2);
+    row[P + xk] = cmul(cadd(y, cmul(y2, conjf2(cp))), stw3[k]);
+    row[2 * P + xk] = cmul(cadd(y, cmul(y2, cp)), stw3[2 * k]);
+  };
+  auto s3_item = [&](int it, float4 v1, float4 v2) {
+    const int ii = it / H, j = it - ii * H;
+    // conjugated spectrum: y_0 = (N re, -S re); y_m = (N re - S im, -(N im + S re)),
+    // y_(n-m) = (N re + S im, N im - S re) for m >= 1 (pack_z)
+    const C yj = j == 0 ? make_float2(v1.x, -v1.z) : make_float2(v1.x - v1.w, -(v1.y + v1.z));
+    const C yj2 = make_float2(v2.x + v2.w, v2.y - v2.z);  // y_(j + 2P) from m = P - j
+    s3_put(ii, j, yj, yj2);
+    if (j > 0 && j < P - j) {
+      const C yk = make_float2(v2.x - v2.w, -(v2.y + v2.z));  // y_(P - j)
+      const C yk2 = make_float2(v1.x + v1.w, v1.y - v1.z);   // y_(n - j) = y_(P - j + 2P)
+      s3_put(ii, P - j, yk, yk2);
     }
   };
   const int band = n - 2 * M - 1;  // frequencies M < k < n - M are zero
   auto build = [&](int c) {
-    for (int e = tid; e < FB * band; e += FNT) {
-      const int ii = e / band, k = M + 1 + (e - ii * band);
-      bufA[ii * rs + ridx<N>(k)] = make_float2(0.f, 0.f);
-    }
+    if constexpr (S3) {
 #pragma unroll
-    for (int k = 0; k < PF; ++k) {
-      const int e = tid + k * FNT;
-      if (e < tot) pack_z<N>(bufA, rs, n, e, rows, pf[k]);
+      for (int k = 0; k < PF / 2; ++k) {
+        const int it = tid + k * FNT;
+        if (it < FB * H) s3_item(it, pf[2 * k], pf[2 * k + 1]);
+      }
+      const float4* src = a.fin[c] + boff;
+      for (int it = tid + (PF / 2) * FNT; it < FB * H; it += FNT) {
+        float4 v1, v2;
+        s3_load(src, it, v1, v2);
+        s3_item(it, v1, v2);
+      }
+    } else {
+      for (int e = tid; e < FB * band; e += FNT) {
+        const int ii = e / band, k = M + 1 + (e - ii * band);
+        bufA[ii * rs + ridx<N>(k)] = make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int k = 0; k < PF; ++k) {
+        const int e = tid + k * FNT;
+        if (e < tot) pack_z<N>(bufA, rs, n, e, rows, pf[k]);
+      }
+      const float4* src = a.fin[c] + boff;
+      for (int e = tid + PF * FNT; e < tot; e += FNT) pack_z<N>(bufA, rs, n, e, rows, __ldg(src + e));
     }
-    const float4* src = a.fin[c] + boff;
-    for (int e = tid + PF * FNT; e < tot; e += FNT) pack_z<N>(bufA, rs, n, e, rows, __ldg(src + e));
   };
   const float ur = 0.f, wr = 0.f, jr = 0.f, br = 0.f;
   const float adv = -a.rf, mrf = -a.rf, lfr = a.lf;
@@ -138,7 +215,8 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
   // w_th, w_ph, j_th, j_ph, b_th, b_ph]; M phase [u_th, u_ph, b_th, b_ph]
   int c = 0;
   float s_r = (PH == FUSED_TEMPERATURE) ? (float)a.sources[r] : 0.f;
-  auto consume = [&](int ii, int j, C z) {
+  // j: longitude index; q: storage index of (ii, j) in the phase's buffers
+  auto consume = [&](int ii, int j, int q, C z) {
     if (PH == FUSED_GRID || (PH == FUSED_TEMPERATURE && c == 5)) {
       if (ii < rows) {
         float* gbase = (PH == FUSED_GRID ? a.gout[c] : a.gout[0]) + (size_t)r * d.nlat * n;
@@ -148,7 +226,6 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
       }
       return;
     }
-    const int q = ii * rs + ridx<N>(j);
     const float vN = z.x, vS = -z.y;
     if (PH == FUSED_TEMPERATURE) {
       // -(u_r g_r + u_th g_th + u_ph g_ph) + S(r); each velocity component
@@ -209,19 +286,27 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
     }
   };
 
+  auto consume_n = [&](int ii, int j, C z) { consume(ii, j, ii * rs + ridx<N>(j), z); };
+  auto consume_s3 = [&](int sr, int cc, C z) {
+    const int ii = sr / 3, a3 = sr - 3 * ii;
+    consume(ii, 3 * cc + a3, sr * P + xidx(cc), z);
+  };
+
   prefetch(0);
   for (c = 0; c < a.nin; ++c) {
     build(c);
     __syncthreads();
     if (c + 1 < a.nin) prefetch(c + 1);
-    if constexpr (N > 0) {
+    if constexpr (S3) {
+      ct_passes_pt_apply<P, 3 * FB, 0, 1, C, FNT, 0, true>(bufA, bufB, stw, consume_s3);
+    } else if constexpr (N > 0) {
       // the last Stockham pass feeds the consumer directly
-      ct_passes_pt_apply<N, FB, 0, 1, C, FNT, 0, true>(bufA, bufB, stw, consume);
+      ct_passes_pt_apply<N, FB, 0, 1, C, FNT, 0, true>(bufA, bufB, stw, consume_n);
     } else {
       const C* res = run_fft<N>(bufA, bufB, stw, p);
       for (int e = tid; e < FB * n; e += FNT) {
         const int ii = e / n, j = e - ii * n;
-        consume(ii, j, res[ii * rs + ridx<N>(j)]);
+        consume_n(ii, j, res[ii * rs + ridx<N>(j)]);
       }
     }
     __syncthreads();
@@ -233,15 +318,26 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
   const int nout = (PH == FUSED_TEMPERATURE) ? 1 : 2;
   for (int o = 0; o < nout; ++o) {
     C* src = o == 0 ? acc0 : acc1;
-    const C* res = run_fft<N>(src, o == 0 ? bufA : bufB, stw, p);
+    const C* res;
+    if constexpr (S3) res = ct_passes_pt<P, 3 * FB, 0, 1, C, FNT, 0, true>(src, o == 0 ? bufA : bufB, stw);
+    else res = run_fft<N>(src, o == 0 ? bufA : bufB, stw, p);
     const size_t gb = ((size_t)(o * d.nr + r) * (M + 1)) * 2 * d.nth;
     for (int e = tid; e < tot; e += FNT) {
       const int m = e / FB, ii = e - m * FB;
       if (ii >= rows) continue;
       const int ith = i0 + ii;
-      const C* row = res + ii * rs;
-      const C zk = row[ridx<N>(m)];
-      C zn = row[ridx<N>(m == 0 ? 0 : n - m)];
+      C zk, zn;
+      if constexpr (S3) {
+        const C* y = res + ii * N;  // Y_a at y + a P
+        const int xm = xidx(m), xp = xidx(m == 0 ? 0 : P - m);
+        const C w1 = stw3[m], w2 = stw3[2 * m];
+        zk = cadd(y[xm], cadd(cmul(w1, y[P + xm]), cmul(w2, y[2 * P + xm])));
+        zn = cadd(y[xp], cadd(cmul(conjf2(w1), y[P + xp]), cmul(conjf2(w2), y[2 * P + xp])));
+      } else {
+        const C* row = res + ii * rs;
+        zk = row[ridx<N>(m)];
+        zn = row[ridx<N>(m == 0 ? 0 : n - m)];
+      }
       zn.y = -zn.y;
       const float Xx = 0.5f * (zk.x + zn.x), Xy = 0.5f * (zk.y + zn.y);
       const float Yx = 0.5f * (zk.y - zn.y), Yy = -0.5f * (zk.x - zn.x);
@@ -265,17 +361,30 @@ size_t fused_smem(int phase, int n, bool unpadded) {
   }
 }
 
-template <int N, int PH>
-void launch_one(cudaStream_t s, const Dims& d, const FftPlan& p, const float2* tw, const FusedArgs& a) {
+template <int N, int PH, bool S3>
+void launch_one_k(cudaStream_t s, const Dims& d, const FftPlan& p, const float2* tw, const FusedArgs& a) {
   const int n = N > 0 ? N : p.n;
   const size_t sm = fused_smem(PH, n, N > 0);
   static size_t attr = 0;
   if (attr < sm) {
-    cudaFuncSetAttribute(k_fused<N, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(k_fused<N, PH, S3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     attr = sm;
   }
   dim3 g(ceil_div(d.nth, FB), d.nr);
-  k_fused<N, PH><<<g, FNT, sm, s>>>(d, p, tw, a);
+  k_fused<N, PH, S3><<<g, FNT, sm, s>>>(d, p, tw, a);
+}
+
+// the three-way split for the induction phase whenever the orders fit below
+// n / 3 (the usual dealiased grid nlon = 3 (M + 1))
+template <int N, int PH>
+void launch_one(cudaStream_t s, const Dims& d, const FftPlan& p, const float2* tw, const FusedArgs& a) {
+  if constexpr (Split3<N>::ok && PH == FUSED_INDUCTION) {
+    if (d.M + 1 <= N / 3) {
+      launch_one_k<N, PH, true>(s, d, p, tw, a);
+      return;
+    }
+  }
+  launch_one_k<N, PH, false>(s, d, p, tw, a);
 }
 
 template <int N>
