@@ -79,7 +79,7 @@ __device__ __forceinline__ void pack_z(float2* bufA, int rs, int n, int e, int r
 //   X_m = sum_a W^(m a) Y_a[m],  X_(n - m) = sum_a W^(-m a) Y_a[(P - m) mod P].
 // Sub-row (pair ii, a) holds P elements at (3 ii + a) P in the xidx layout.
 // The last P-point pass has fewer butterflies than threads, so the split is
-// used where the products are light (the induction phase): with the heavier
+// used where the products are light (the induction phase, the grid output): with the heavier
 // velocity and temperature products the radix-3 pass, which spreads them over
 // every thread, is faster.
 template <int N> struct Split3 {
@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
     static_assert(ct_pass_tw_entries(P) + 2 * P <= N, "twiddles exceed the table space");
     ct_fill_pass_twiddles<P, FNT, 3>(tw, stw);
     for (int k = tid; k < 2 * P; k += FNT) stw3[k] = tw[k];
+    __syncthreads();  // the input packing (build) reads W^k before the first pass barrier
   } else if constexpr (N > 0) {
     static_assert(ct_pass_tw_entries(N) <= N, "per-pass twiddles exceed the table space");
     ct_fill_pass_twiddles<N, FNT>(tw, stw);
@@ -374,11 +375,11 @@ void launch_one_k(cudaStream_t s, const Dims& d, const FftPlan& p, const float2*
   k_fused<N, PH, S3><<<g, FNT, sm, s>>>(d, p, tw, a);
 }
 
-// the three-way split for the induction phase whenever the orders fit below
-// n / 3 (the usual dealiased grid nlon = 3 (M + 1))
+// the three-way split for the induction phase and the grid output whenever
+// the orders fit below n / 3 (the usual dealiased grid nlon = 3 (M + 1))
 template <int N, int PH>
 void launch_one(cudaStream_t s, const Dims& d, const FftPlan& p, const float2* tw, const FusedArgs& a) {
-  if constexpr (Split3<N>::ok && PH == FUSED_INDUCTION) {
+  if constexpr (Split3<N>::ok && (PH == FUSED_INDUCTION || PH == FUSED_GRID)) {
     if (d.M + 1 <= N / 3) {
       launch_one_k<N, PH, true>(s, d, p, tw, a);
       return;
