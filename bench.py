@@ -267,6 +267,61 @@ def run_ensemble(args, gdb, workloads, torch):
     return 0
 
 
+def run_transforms(args, gdb, workloads, torch):
+    """Transform-only configuration: forward + inverse scalar transforms at
+    lmax 127 over 97 shells x 9 fields (seeded, (l+1)^-1.5), FP64 and mixed:
+    max / RMS relative errors of synthesis, analysis and round trip against
+    the FP64 oracle, device time of the transform kernels (per-kernel events)
+    and wall time of the host-buffer calls."""
+    from oracle.oracle import Oracle
+    c = workloads.CONFIGS["transform_l127_nr97x9"]
+    L, nlat, nlon, nr, nf = c["lmax"], c["nlat"], c["nlon"], c["nr"], c["nfield"]
+    re, im = workloads.transform_batch(L, L, nr, nf, seed=0)
+    o = Oracle(lmax=L, nlat=nlat, nlon=nlon, nr=nr)
+    grids = np.stack([o.synth_scalar(re[f], im[f]) for f in range(nf)])
+    ana = [o.analysis_scalar(grids[f]) for f in range(nf)]
+    nlm = re.shape[-1]
+    gflop = 2.0 * 2 * nlm * (nlat // 2) * 2 * nr * nf / 1e9  # even/odd-folded Legendre, both directions
+
+    def errs(a, b):
+        return (float(np.max(np.abs(a - b)) / np.max(np.abs(b))),
+                float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2))))
+
+    res = {}
+    for prec in ("fp64", "mixed"):
+        g = gdb.SHTnsKitConfig(L, nlat, nlon, nr, precision=prec)
+        for _ in range(args.warmup):
+            g.analysis_scalar(g.synth_scalar(re, im))
+        g.profile_enable(True)
+        g.profile_read()
+        t0 = time.perf_counter()
+        out = g.synth_scalar(re, im)
+        back = g.analysis_scalar(grids)
+        wall = time.perf_counter() - t0
+        prof = g.profile_read()
+        g.profile_enable(False)
+        rt = g.analysis_scalar(out)
+        dev_ms = sum(v[0] for v in prof.values())
+        e_s = [errs(out[f], grids[f]) for f in range(nf)]
+        e_a = [errs(np.concatenate([back[0][f], back[1][f]]), np.concatenate(ana[f])) for f in range(nf)]
+        e_r = [errs(np.concatenate([rt[0][f], rt[1][f]]), np.concatenate([re[f], im[f]])) for f in range(nf)]
+        res[prec] = {"synthesis_max": max(e[0] for e in e_s), "synthesis_rms": max(e[1] for e in e_s),
+                     "analysis_max": max(e[0] for e in e_a), "analysis_rms": max(e[1] for e in e_a),
+                     "roundtrip_max": max(e[0] for e in e_r), "roundtrip_rms": max(e[1] for e in e_r),
+                     "device_ms": dev_ms, "wall_ms_host_buffers": wall * 1e3,
+                     "legendre_gflops_algorithmic": gflop / (dev_ms * 1e-3),
+                     "kernels": {k: v[0] for k, v in prof.items()}}
+        g.close()
+    line = {"metric": "transform batch forward+inverse (lmax 127, 97 shells x 9 fields)",
+            "value": res["mixed"]["device_ms"], "unit": "ms (device, forward+inverse)", "higher_is_better": False,
+            "n_gpus": 1, "data": "synthetic (transform_batch(seed=0), (l+1)^-1.5)",
+            "config": {"workload": "transform_l127_nr97x9", "lmax": L, "nlat": nlat, "nlon": nlon, "nr": nr,
+                       "fields": nf, "legendre_gflop_algorithmic": gflop},
+            "fp64": res["fp64"], "mixed": res["mixed"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_adjoint(args, gdb, workloads, torch):
     """Adjoint configuration (lmax 63, nr 65, 200 steps, literal boundaries,
     checkpoints every 20 steps): gradient of the r = ro radial-field misfit with
@@ -376,6 +431,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD,
                     help="named shell workload (the headline metric is shell_l255_nr129; smaller ones are for profiling)")
+    ap.add_argument("--transforms", action="store_true",
+                    help="instead of the headline: the transform-only batch's errors and timings")
     ap.add_argument("--adjoint", action="store_true",
                     help="instead of the headline: the adjoint configuration's gradient checks and timings")
     ap.add_argument("--ensemble", type=int, default=0,
@@ -400,6 +457,8 @@ def main():
         return run_ensemble(args, gdb, workloads, torch)
     if args.adjoint:
         return run_adjoint(args, gdb, workloads, torch)
+    if args.transforms:
+        return run_transforms(args, gdb, workloads, torch)
     dist = None
     if world > 1:
         import datetime

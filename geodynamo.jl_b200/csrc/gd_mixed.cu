@@ -159,8 +159,10 @@ int tc_analysis_vector_G(gd_handle* h, double* out_tor, double* out_pol, int epi
   return launched(h, "mixed vector analysis");
 }
 
-// Analysis of FP32 grids (host-array entry points): phi transform into d_G, then Legendre.
+// Analysis of FP32 grids (host-array entry points): phi transform into d_G, then Legendre
+// (nf <= 2: the components d_G holds).
 int tc_analysis_scalar(gd_handle* h, const float* grid_in, int nf, double* const* out) {
+  if (nf > 2) return set_error(h, GD_ERR_ARG, "scalar analysis of more than two fields per pass");
   MixedState* x = h->mixed;
   { ProfScope p(h, "fft_analysis_fp32"); launch_fft_analysis<float>(h->stream, h->d, h->plan, h->d_twf, grid_in, h->grid_elems(), h->d_w, x->d_G, nf); }
   return tc_analysis_scalar_G(h, nf, out);
@@ -402,9 +404,15 @@ int mixed_api_synth_vector(gd_handle* h, const double* tor, const double* pol, d
 }
 
 int mixed_api_analysis_scalar(gd_handle* h, const double* grid_in, int nf, double* const* out) {
-  launch_cast_d2f(h->stream, (size_t)nf * h->grid_elems(), grid_in, h->mixed->d_stage);
-  int s = tc_analysis_scalar(h, h->mixed->d_stage, nf, out);
-  return s ? s : mixed_check_error(h);
+  // the folded-transform buffer d_G holds two components: at most two fields per pass
+  for (int f0 = 0; f0 < nf; f0 += 2) {
+    const int nc = nf - f0 < 2 ? nf - f0 : 2;
+    launch_cast_d2f(h->stream, (size_t)nc * h->grid_elems(), grid_in + (size_t)f0 * h->grid_elems(),
+                    h->mixed->d_stage);
+    int s = tc_analysis_scalar(h, h->mixed->d_stage, nc, out + f0);
+    if (s) return s;
+  }
+  return mixed_check_error(h);
 }
 
 int mixed_api_analysis_vector(gd_handle* h, const double* grid_in, double* tor, double* pol) {
