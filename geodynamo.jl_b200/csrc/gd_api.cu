@@ -306,19 +306,30 @@ int step_sequence(gd_handle* h, int boot) {
 
 void drop_graphs(gd_handle* h) {
   h->graph_gen++;
-  for (int i = 0; i < 2; ++i)
-    if (h->gexec[i]) { cudaGraphExecDestroy(h->gexec[i]); h->gexec[i] = nullptr; }
+  for (int p = 0; p < 2; ++p)
+    for (int i = 0; i < 2; ++i)
+      if (h->gexec[p][i]) { cudaGraphExecDestroy(h->gexec[p][i]); h->gexec[p][i] = nullptr; }
 }
 
+// After a step's implicit solve: its nonlinear terms become the history of
+// the next step (the reference's roll N_prev := N, src/simulation.jl:1312-1329).
+void end_step(gd_handle* h) {
+  h->last_nl_par = h->nl_par;
+  h->nl_par ^= 1;
+  h->step_count++;
+}
+
+// The step graph for the current nonlinear bank and bootstrap flag.
 int ensure_graph(gd_handle* h, int boot) {
-  if (h->gexec[boot]) return GD_OK;
+  cudaGraphExec_t& ge = h->gexec[h->nl_par][boot];
+  if (ge) return GD_OK;
   cudaGraph_t g = nullptr;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   int s = step_sequence(h, boot);
   cudaError_t e = cudaStreamEndCapture(h->stream, &g);
   if (s) { if (g) cudaGraphDestroy(g); return s; }
   if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&h->gexec[boot], g, 0);
+  e = cudaGraphInstantiate(&ge, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   return GD_OK;
@@ -462,7 +473,7 @@ int gd_download_spectral(gd_handle* h, int field, double* re, double* im) {
 int gd_download_nonlinear(gd_handle* h, int field, double* re, double* im) {
   if (!h || !re || !im || field < 0 || field > 4) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
-  return download_spec(h, h->nlf(field), re, im);
+  return download_spec(h, h->nl_bank(h->last_nl_par) + h->spec_elems() * field, re, im);
 }
 
 int gd_download_grid(gd_handle* h, int grid, double* out) {
@@ -658,6 +669,7 @@ int gd_temperature_nonlinear(gd_handle* h) {
   CK(cudaSetDevice(h->device));
   int s = temperature_nl(h);
   if (s) return s;
+  h->last_nl_par = h->nl_par;
   CK(cudaStreamSynchronize(h->stream));
   return h->precision == GD_PREC_MIXED ? mixed_check_error(h) : GD_OK;
 }
@@ -666,6 +678,7 @@ int gd_velocity_nonlinear(gd_handle* h) {
   CK(cudaSetDevice(h->device));
   int s = velocity_nl(h);
   if (s) return s;
+  h->last_nl_par = h->nl_par;
   CK(cudaStreamSynchronize(h->stream));
   return h->precision == GD_PREC_MIXED ? mixed_check_error(h) : GD_OK;
 }
@@ -674,6 +687,7 @@ int gd_magnetic_nonlinear(gd_handle* h) {
   CK(cudaSetDevice(h->device));
   int s = magnetic_nl(h);
   if (s) return s;
+  h->last_nl_par = h->nl_par;
   CK(cudaStreamSynchronize(h->stream));
   return h->precision == GD_PREC_MIXED ? mixed_check_error(h) : GD_OK;
 }
@@ -684,7 +698,7 @@ int gd_implicit_step(gd_handle* h) {
   int s = implicit_launch(h, boot);
   if (s) return s;
   CK(cudaStreamSynchronize(h->stream));
-  h->step_count++;
+  end_step(h);
   return GD_OK;
 }
 
@@ -699,9 +713,9 @@ int gd_step_async(gd_handle* h, int nsteps) {
     } else {
       int s = ensure_graph(h, boot);
       if (s) return s;
-      CK(cudaGraphLaunch(h->gexec[boot], h->stream));
+      CK(cudaGraphLaunch(h->gexec[h->nl_par][boot], h->stream));
     }
-    h->step_count++;
+    end_step(h);
   }
   return GD_OK;
 }
@@ -796,7 +810,7 @@ struct gd_ensemble {
   cudaStream_t master = nullptr;
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> joins;
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [nl_par][boot]
   std::vector<int> gens;  // members' graph generations the ensemble graphs were captured at
   int failed = -1;
 };
@@ -805,8 +819,9 @@ int gd_ensemble_destroy(gd_ensemble* e) {
   if (!e) return GD_ERR_ARG;
   cudaSetDevice(e->device);
   if (e->master) cudaStreamSynchronize(e->master);
-  for (int i = 0; i < 2; ++i)
-    if (e->gexec[i]) cudaGraphExecDestroy(e->gexec[i]);
+  for (int p = 0; p < 2; ++p)
+    for (int i = 0; i < 2; ++i)
+      if (e->gexec[p][i]) cudaGraphExecDestroy(e->gexec[p][i]);
   for (gd_handle* h : e->members) gd_destroy(h);
   for (cudaEvent_t ev : e->joins) cudaEventDestroy(ev);
   if (e->fork) cudaEventDestroy(e->fork);
@@ -861,16 +876,17 @@ int gd_ensemble_get_stream(gd_ensemble* e, void** stream) {
 
 // One graph: fork from the master stream to every member's stream, each
 // member's step sequence, join back.
-static int ensemble_graph(gd_ensemble* e, int boot) {
+static int ensemble_graph(gd_ensemble* e, int par, int boot) {
   bool stale = e->gens.size() != e->members.size();
   for (size_t i = 0; i < e->members.size() && !stale; ++i) stale = e->gens[i] != e->members[i]->graph_gen;
   if (stale) {  // a member's parameters, precision or dt changed since the capture
-    for (int b = 0; b < 2; ++b)
-      if (e->gexec[b]) { cudaGraphExecDestroy(e->gexec[b]); e->gexec[b] = nullptr; }
+    for (int p = 0; p < 2; ++p)
+      for (int b = 0; b < 2; ++b)
+        if (e->gexec[p][b]) { cudaGraphExecDestroy(e->gexec[p][b]); e->gexec[p][b] = nullptr; }
     e->gens.clear();
     for (gd_handle* h : e->members) e->gens.push_back(h->graph_gen);
   }
-  if (e->gexec[boot]) return GD_OK;
+  if (e->gexec[par][boot]) return GD_OK;
   if (cudaStreamBeginCapture(e->master, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return GD_ERR_CUDA;
   int st = GD_OK;
   cudaError_t ce = cudaEventRecord(e->fork, e->master);
@@ -889,7 +905,7 @@ static int ensemble_graph(gd_ensemble* e, int boot) {
     if (g) cudaGraphDestroy(g);
     return st != GD_OK ? st : GD_ERR_CUDA;
   }
-  const cudaError_t ie = cudaGraphInstantiate(&e->gexec[boot], g, 0);
+  const cudaError_t ie = cudaGraphInstantiate(&e->gexec[par][boot], g, 0);
   cudaGraphDestroy(g);
   return ie == cudaSuccess ? GD_OK : GD_ERR_CUDA;
 }
@@ -899,12 +915,12 @@ int gd_ensemble_step_async(gd_ensemble* e, int nsteps) {
   if (cudaSetDevice(e->device) != cudaSuccess) return GD_ERR_CUDA;
   e->failed = -1;
   for (int k = 0; k < nsteps; ++k) {
-    int boot = -1;
+    int boot = -1, par = -1;
     bool together = true;
     for (gd_handle* h : e->members) {
       const int b = (h->c.ab_mode == 1 || h->step_count == 0) ? 1 : 0;
-      if (boot < 0) boot = b;
-      if (b != boot || h->profiling) together = false;
+      if (boot < 0) { boot = b; par = h->nl_par; }
+      if (b != boot || h->nl_par != par || h->profiling) together = false;
     }
     if (together) {
       // the members' streams may still run work queued outside the ensemble
@@ -913,10 +929,10 @@ int gd_ensemble_step_async(gd_ensemble* e, int nsteps) {
         if (cudaEventRecord(ev, h->stream) != cudaSuccess || cudaStreamWaitEvent(e->master, ev, 0) != cudaSuccess)
           return GD_ERR_CUDA;
       }
-      const int s = ensemble_graph(e, boot);
+      const int s = ensemble_graph(e, par, boot);
       if (s != GD_OK) return s;
-      if (cudaGraphLaunch(e->gexec[boot], e->master) != cudaSuccess) return GD_ERR_CUDA;
-      for (gd_handle* h : e->members) h->step_count++;
+      if (cudaGraphLaunch(e->gexec[par][boot], e->master) != cudaSuccess) return GD_ERR_CUDA;
+      for (gd_handle* h : e->members) end_step(h);
     } else {
       // each member's stream first waits for the ensemble's earlier graph launches
       if (cudaEventRecord(e->fork, e->master) != cudaSuccess) return GD_ERR_CUDA;

@@ -7,8 +7,9 @@
 // src/linear_algebra.jl:59-88): forward substitution with the unit lower
 // factor, back substitution with the upper factor.  One thread owns one (l, m)
 // column of one field and walks r with register windows; Re and Im share the
-// factors.  The AB bootstrap (src/simulation.jl:1153-1170) and the history roll
-// (:1312-1329) are folded into the same pass.
+// factors.  The AB bootstrap (src/simulation.jl:1153-1170) is folded into the
+// same pass; the history roll (:1312-1329) is the handle's switch of the two
+// banks of nonlinear terms after the step (N_prev is read from the other bank).
 #include "gd_internal.cuh"
 
 namespace gd {
@@ -16,8 +17,7 @@ namespace gd {
 // One thread solves the (l, m) column of one field.  Three sweeps over r, each
 // with loads that do not depend on the running recurrence so the unrolled
 // loops keep many loads in flight:
-//   1. rhs = u/dt + 1.5 N - 0.5 N_prev + (1 - theta) L_l u  (written over u),
-//      history roll N_prev := N;
+//   1. rhs = u/dt + 1.5 N - 0.5 N_prev + (1 - theta) L_l u  (written over u);
 //   2. forward substitution with the unit lower factor (y over u);
 //   3. back substitution with the upper factor (x over u).
 // L_l = nu lap - nu l(l+1)/r^2 is rebuilt from the block's shared Laplacian
@@ -35,8 +35,8 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
   double* __restrict__ uim = a.u[slot] + plane + j;
   const double* __restrict__ nre = a.nl[slot] + j;
   const double* __restrict__ nim = a.nl[slot] + plane + j;
-  double* __restrict__ pre = a.prev[slot] + j;
-  double* __restrict__ pim = a.prev[slot] + plane + j;
+  const double* __restrict__ pre = a.prev[slot] + j;
+  const double* __restrict__ pim = a.prev[slot] + plane + j;
   const double* __restrict__ F = LU + l;
   const bool boot = a.boot != 0;
   const bool rows = a.bc_rows != 0;
@@ -91,8 +91,6 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
         vr = is_temp ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
         vi = 0.0;
       }
-      pre[at] = nr_[b];
-      pim[at] = ni_[b];
       ure[at] = vr;
       uim[at] = vi;
 #pragma unroll

@@ -32,8 +32,13 @@ struct gd_handle {
   double* d_tw = nullptr;
   float* d_twf = nullptr;
   double* d_state = nullptr;  // 5 fields
-  double* d_nl = nullptr;     // 5 fields
-  double* d_prev = nullptr;   // 5 fields
+  // Two banks of the five nonlinear terms: a step writes bank nl_par and the
+  // Adams-Bashforth history is the other bank (the previous step's terms), so
+  // the history roll N_prev := N is a flip of nl_par instead of a copy.
+  double* d_nl = nullptr;     // bank 0
+  double* d_prev = nullptr;   // bank 1
+  int nl_par = 0;             // bank the next nonlinear terms go to
+  int last_nl_par = 0;        // bank holding the most recently computed terms
   double* d_work = nullptr;   // 8 derived spectral fields
   double *d_bvals = nullptr, *d_sources = nullptr;
   double* d_grid = nullptr;   // NGRID grids (FP64)
@@ -44,7 +49,7 @@ struct gd_handle {
   // mixed precision state (lazy)
   gd::MixedState* mixed = nullptr;
   // graphs (index: boot flag)
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [nl_par][boot]
   int graph_gen = 0;  // bumped whenever captured step graphs become stale
   // per-kernel event timing (gd_profile_enable)
   bool profiling = false;
@@ -57,8 +62,9 @@ struct gd_handle {
   size_t spec_elems() const { return (size_t)2 * d.nr * d.nlm; }
   size_t grid_elems() const { return (size_t)d.nlat * d.nlon * d.nr; }
   double* field(int f) { return d_state + spec_elems() * f; }
-  double* nlf(int f) { return d_nl + spec_elems() * f; }
-  double* prevf(int f) { return d_prev + spec_elems() * f; }
+  double* nl_bank(int b) { return b ? d_prev : d_nl; }
+  double* nlf(int f) { return nl_bank(nl_par) + spec_elems() * f; }
+  double* prevf(int f) { return nl_bank(nl_par ^ 1) + spec_elems() * f; }
   double* work(int k) { return d_work + spec_elems() * k; }
   double* grid(int g) { return d_grid + grid_elems() * g; }
 };

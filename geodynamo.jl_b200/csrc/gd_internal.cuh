@@ -116,7 +116,7 @@ void launch_grid_cast(cudaStream_t s, size_t n, const R* src, double* dst);
 struct Cnab2Args {
   double* u[5];
   const double* nl[5];
-  double* prev[5];
+  const double* prev[5];  // the previous step's nonlinear terms (read only)
   int kind[5];
   int nfield;
   int boot;
