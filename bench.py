@@ -100,7 +100,8 @@ def kernel_work(name, p, nlm, precision):
         "nl_temperature": 6 * G * rb,
         "nl_velocity": 10 * G * rb,
         "nl_induction": 6 * G * rb,
-        "cnab2_solve": 5 * 5 * S * 8,
+        # per field: read u, N, N_prev, write u (the history roll is a bank switch)
+        "cnab2_solve": 5 * 4 * S * 8,
         "spectral_gradients": 4 * S * 8,
         "spectral_curl": 4 * S * 8,
         "temperature_bc": 4 * nlm * 8,
