@@ -94,7 +94,7 @@ def kernel_work(name, p, nlm, precision):
             return {"flops": fl, "bytes": by}
     table = {
         # fused phase kernels: blocked Fourier components in, folded transforms out
-        "fused_temperature": 6 * F * cb + G * rb + F * cb,
+        "fused_temperature": 5 * F * cb + F * cb,
         "fused_velocity": 8 * F * cb + 2 * F * cb,
         "fused_induction": 4 * F * cb + 2 * F * cb,
         "nl_temperature": 6 * G * rb,

@@ -212,15 +212,15 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
   const float adv = -a.rf, mrf = -a.rf, lfr = a.lf;
 
   // consumer of one transformed component: grid rows or the products
-  // inputs: T phase [g_r, u_th, g_th, u_ph, g_ph, T]; V phase [u_th, u_ph,
+  // inputs: T phase [g_r, u_th, g_th, u_ph, g_ph]; V phase [u_th, u_ph,
   // w_th, w_ph, j_th, j_ph, b_th, b_ph]; M phase [u_th, u_ph, b_th, b_ph]
   int c = 0;
   float s_r = (PH == FUSED_TEMPERATURE) ? (float)a.sources[r] : 0.f;
   // j: longitude index; q: storage index of (ii, j) in the phase's buffers
   auto consume = [&](int ii, int j, int q, C z) {
-    if (PH == FUSED_GRID || (PH == FUSED_TEMPERATURE && c == 5)) {
+    if (PH == FUSED_GRID) {
       if (ii < rows) {
-        float* gbase = (PH == FUSED_GRID ? a.gout[c] : a.gout[0]) + (size_t)r * d.nlat * n;
+        float* gbase = a.gout[c] + (size_t)r * d.nlat * n;
         const int ith = i0 + ii;
         gbase[(size_t)ith * n + j] = z.x;
         gbase[(size_t)(d.nlat - 1 - ith) * n + j] = -z.y;

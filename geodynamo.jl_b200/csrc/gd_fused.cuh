@@ -11,7 +11,7 @@ enum { FUSED_GRID = 0, FUSED_TEMPERATURE = 1, FUSED_VELOCITY = 2, FUSED_INDUCTIO
 struct FusedArgs {
   const float4* fin[8];  // blocked Fourier coefficients, one pointer per input component
   int nin;
-  float* gout[8];        // grid phase: one grid per input; temperature phase: [0] = T grid
+  float* gout[8];        // grid phase: one grid per input
   float2* G;             // folded transforms of the products [comp][r][m][s][ith]
   const double* w;       // Gauss weights (north half)
   const double* cth;     // Coriolis cos/sin tables, indexed by min(phi index, nlat - 1)

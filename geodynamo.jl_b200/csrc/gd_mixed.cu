@@ -16,7 +16,7 @@ namespace gd {
 
 // Blocked FP32 Fourier buffers of the synthesized components (the fused
 // phase kernels transform them in shared memory; the physical grids are not
-// kept in HBM, except the temperature grid).
+// kept in HBM and are formed on request).
 enum {
   FC_T = 0, FC_GTH = 1, FC_GPH = 2, FC_GR = 3,  // temperature phase (scalar synthesis order)
   FC_U = 4, FC_W = 6, FC_B = 8, FC_J = 10,      // theta, phi pairs
@@ -40,7 +40,6 @@ struct MixedState {
   float* d_bimg_vc = nullptr;
   long* d_bofs = nullptr;      // first step of order m within a column tile
   long ttot = 0;               // synthesis pipeline steps over all m (one column tile)
-  float* d_tgrid = nullptr;    // the temperature grid (FP32)
   float* d_stage = nullptr;    // 4 FP32 grids for the host-array entry points and grid downloads
   int* d_err = nullptr;
   size_t bytes = 0;
@@ -220,7 +219,6 @@ int mixed_create(gd_handle* h) {
   x->fcomp = fourier_comp_elems(d);
   MAL(x->d_Fall, (size_t)FC_COUNT * x->fcomp);
   MAL(x->d_G, (size_t)2 * d.nr * (d.M + 1) * 2 * d.nth);
-  MAL(x->d_tgrid, h->grid_elems());
   MAL(x->d_stage, (size_t)4 * h->grid_elems());
   MAL(x->d_err, 4);
   int s = mcheck(h, cudaMemcpyAsync(x->d_cofs, cofs.data(), sizeof(long) * cofs.size(), cudaMemcpyHostToDevice,
@@ -248,8 +246,6 @@ int mixed_create(gd_handle* h) {
   // the carried components start as zero grids (the reference's physical
   // fields are zero-filled at allocation, src/fields.jl:82)
   s = mcheck(h, cudaMemsetAsync(x->d_Fall, 0, sizeof(float4) * FC_COUNT * x->fcomp, h->stream), "memset");
-  if (s) return s;
-  s = mcheck(h, cudaMemsetAsync(x->d_tgrid, 0, sizeof(float) * h->grid_elems(), h->stream), "memset");
   if (s) return s;
   s = mcheck(h, cudaMemsetAsync(x->d_err, 0, sizeof(int), h->stream), "memset");
   if (s) return s;
@@ -285,12 +281,14 @@ int mixed_temperature_nl(gd_handle* h) {
   const double* coef[4] = {h->field(F_TEMP), nullptr, nullptr, nullptr};
   int s = tc_synth_scalar(h, coef, 4, x->F(FC_T), 1);
   if (s) return s;
-  // the velocity grid is the previous velocity phase's (carried in F(FC_U))
+  // the velocity grid is the previous velocity phase's (carried in F(FC_U));
+  // the temperature grid itself is not a factor of the products: like every
+  // synthesized grid of the mixed step it is formed on request from its
+  // Fourier buffer F(FC_T) (mixed_grid_to_double)
   FusedArgs f = phase_args(h);
-  const float4* fin[6] = {x->F(FC_GR), x->F(FC_U), x->F(FC_GTH), x->F(FC_U + 1), x->F(FC_GPH), x->F(FC_T)};
-  for (int i = 0; i < 6; ++i) f.fin[i] = fin[i];
-  f.nin = 6;
-  f.gout[0] = x->d_tgrid;
+  const float4* fin[5] = {x->F(FC_GR), x->F(FC_U), x->F(FC_GTH), x->F(FC_U + 1), x->F(FC_GPH)};
+  for (int i = 0; i < 5; ++i) f.fin[i] = fin[i];
+  f.nin = 5;
   { ProfScope p(h, "fused_temperature_fp32"); launch_fused(h->stream, d, h->plan, h->d_twf, FUSED_TEMPERATURE, f); }
   s = launched(h, "fused temperature phase");
   if (s) return s;
@@ -362,7 +360,7 @@ int mixed_grid_to_double(gd_handle* h, int grid, double* out) {
     case GD_GRID_GTH: fc = FC_GTH; break;
     case GD_GRID_GPH: fc = FC_GPH; break;
     case GD_GRID_GR: fc = FC_GR; break;
-    case GD_GRID_T: src = x->d_tgrid; break;
+    case GD_GRID_T: fc = FC_T; break;
     default:
       return set_error(h, GD_ERR_UNSUPPORTED,
                        "the mixed-precision step forms the nonlinear products in shared memory only; download "

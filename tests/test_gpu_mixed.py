@@ -102,6 +102,21 @@ def test_mixed_step_l255_tracks_oracle(gdb, oracle_mod):
         assert rel(a[0], b[0]) < 1e-5 and rel(a[1], b[1]) < 1e-5, k
 
 
+def test_mixed_synthesized_grids_match_oracle(gdb, oracle_mod):
+    # grids of the mixed step are formed on request from its Fourier buffers
+    # (the temperature grid included): after a step they are the grids the
+    # step's phases synthesized, as the oracle keeps them
+    g = gdb.SHTnsKitConfig(31, 48, 96, 32, precision="mixed")
+    o = oracle_mod.Oracle(lmax=31, nlat=48, nlon=96, nr=32)
+    for k, (a, b) in workloads.seeded_state(31, 31, 32, seed=0).items():
+        g.set_field(k, a, b)
+        o.set_field(k, a, b)
+    for _ in range(2):
+        g.step(1); o.step(1)
+        for grid in ("t", "gth", "gph", "gr", "u_th", "u_ph", "w_th", "w_ph", "b_th", "b_ph", "j_th", "j_ph"):
+            assert rel(g.get_grid(grid), o.get_grid(grid)) < TOL_T, grid
+
+
 def test_precision_switch_keeps_state(gdb):
     st = workloads.seeded_state(15, 15, 12, seed=4)
     a = gdb.SHTnsKitConfig(15, 24, 48, 12)
