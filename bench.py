@@ -112,6 +112,28 @@ def kernel_work(name, p, nlm, precision):
     return None
 
 
+def fp64_gemm_tflops(n=4096, reps=5):
+    """cuBLAS FP64 GEMM rate (torch.matmul, n^3, best of reps, CUDA events):
+    the measured peak the FP64 step's tensor-core contractions are rated against."""
+    import torch
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
 def measured_traffic(name):
     """DRAM bytes per launch of a kernel from the committed ncu summary of the
     headline workload (profiles/dram_traffic_shell_l255_nr129.txt), or None."""
@@ -522,29 +544,35 @@ def main():
     ms_per_step = ms_total / args.steps
 
     # ---- per-kernel breakdown (events around each launch, eager replay) ----
-    g.profile_enable(True)
     nprof = 2
-    g.step(nprof)
-    prof = g.profile_read()
-    g.profile_enable(False)
-    kernels = []
-    for name, (ms, cnt) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
-        per = ms / cnt
-        w = kernel_work(name, p, g.nlm, precision)
-        ent = {"name": name, "share": None, "launches_per_step": cnt / nprof, "ms_per_launch": per}
-        if name.startswith("fft_"):
-            # 4-component synth launches and 2-component ones share a name; use the per-step mix
-            ncomp = (4 + 2 * 4) if "synth" in name else (1 + 2 + 2)
-            ent["gbs"] = fft_bytes(p, ncomp, precision) / (ms / nprof / 1e3) / 1e9
-        elif w is not None:
-            if w["flops"] is not None:
-                ent["tflops"] = w["flops"] / (per / 1e3) / 1e12
-            if w["bytes"] is not None:
-                ent["gbs"] = w["bytes"] / (per / 1e3) / 1e9
-        kernels.append(ent)
-    tot = sum(v[0] for v in prof.values())
-    for ent in kernels:
-        ent["share"] = prof[ent["name"]][0] / tot if tot else None
+
+    def breakdown(h, prec):
+        h.profile_enable(True)
+        h.step(nprof)
+        pr = h.profile_read()
+        h.profile_enable(False)
+        out = []
+        for name, (ms, cnt) in sorted(pr.items(), key=lambda kv: -kv[1][0]):
+            per = ms / cnt
+            w = kernel_work(name, p, h.nlm, prec)
+            ent = {"name": name, "share": None, "launches_per_step": cnt / nprof, "ms_per_launch": per}
+            if name.startswith("fft_"):
+                # 4-component synth launches and 2-component ones share a name; use the per-step mix
+                ncomp = (4 + 2 * 4) if "synth" in name else (1 + 2 + 2)
+                ent["gbs"] = fft_bytes(p, ncomp, prec) / (ms / nprof / 1e3) / 1e9
+            elif w is not None:
+                if w["flops"] is not None:
+                    ent["tflops"] = w["flops"] / (per / 1e3) / 1e12
+                if w["bytes"] is not None:
+                    ent["gbs"] = w["bytes"] / (per / 1e3) / 1e9
+            out.append(ent)
+        tot = sum(v[0] for v in pr.values())
+        for ent in out:
+            ent["share"] = pr[ent["name"]][0] / tot if tot else None
+        return pr, out
+
+    prof, kernels = breakdown(g, precision)
+    dgemm = fp64_gemm_tflops()
 
     peaks = {}
     try:
@@ -562,7 +590,7 @@ def main():
                            "frac": top["gbs"] / hbm_peak, "peak_source": peak_src + " HBM copy bandwidth"})
         if "tflops" in top:
             if top["name"].endswith("fp64"):
-                pk, src = 40.0, "nominal FP64 tensor (no measured FP64 peak on this pool)"
+                pk, src = dgemm, "cuBLAS FP64 GEMM 4096^3 measured in this run (torch.matmul)"
             else:
                 pk, src = peaks.get("bf16_tflops", 1590.0) / 2.0, "half the measured bf16 burst peak (tf32 rate)"
             bounds.append({"bound": "tensor", "achieved": top["tflops"], "peak": pk, "unit": "TFLOP/s",
@@ -578,14 +606,26 @@ def main():
 
     # ---- FP64 reference step on the GPU (denominator of the metric) ----
     fp64_value = None
+    k64 = kernels
     if precision == "mixed":
         g64 = make("fp64")
         g64.step(args.warmup)
         ms64 = timed_steps(g64, args.steps, 0)
         fp64_value = world * args.steps / (ms64 / 1e3)
+        _, k64 = breakdown(g64, "fp64")
         g64.close()
     else:
         fp64_value = value
+    # how tuned the denominator is: the FP64 step's Legendre contractions
+    # (DMMA) against the measured cuBLAS FP64 GEMM rate
+    leg = [k for k in k64 if k["name"].startswith("legendre_") and "tflops" in k]
+    leg_ms = sum(k["ms_per_launch"] * k["launches_per_step"] for k in leg)
+    leg_tf = sum(k["tflops"] * k["ms_per_launch"] * k["launches_per_step"] for k in leg)
+    fp64_den = {"ms_per_step": 1e3 / (fp64_value / world) if fp64_value else None,
+                "legendre_ms_per_step": leg_ms,
+                "legendre_tflops": leg_tf / leg_ms if leg_ms else None,
+                "fp64_gemm_tflops": dgemm,
+                "legendre_frac_of_gemm": leg_tf / leg_ms / dgemm if leg_ms else None}
 
     # ---- energy agreement, mixed vs FP64 ----
     # bc_mode 0 is the reference's operator as written (no boundary rows; its
@@ -657,6 +697,7 @@ def main():
                            "dt": p["dt"], "precision": precision, "parallelism": f"replicas x{world}",
                            "l2": "working set 5+ GB of grids per step, larger than L2; no flush"},
                 "fp64_gpu_value": fp64_value, "ratio_vs_fp64_gpu": value / fp64_value if fp64_value else None,
+                "fp64_denominator": fp64_den,
                 "accuracy": accuracy, "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk}
         print(json.dumps(line), flush=True)

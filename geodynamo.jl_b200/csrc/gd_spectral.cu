@@ -5,12 +5,79 @@
 
 namespace gd {
 
-// Radial operators walk r with a register window of 2 KL + 1 levels: each
-// thread owns one mode j and RB_R consecutive levels, so every coefficient is
-// read once per block of levels (plus the window halo) instead of once per
-// band entry.  Band sums run over the same levels in the same order as the
-// banded matrix-vector product they restate.
-constexpr int RB_R = 16;
+// Radial operators: each thread owns one mode j and a run of consecutive
+// levels, so every coefficient is read once per run (plus the 2 KL halo).
+// The gradient kernel walks its run with a register window of 2 KL + 1
+// levels.  The curl kernel stages a block's runs (128 modes) plus the halo of
+// both planes in shared memory by asynchronous 8-byte copies, all in flight
+// together, with the band columns and 1/r values those levels use, and reads
+// every level's window and coefficients from there.  Band sums run over the
+// same levels in the same order as the banded matrix-vector product they
+// restate.
+constexpr int RB_R = 16;          // most levels per block
+constexpr int RAD_THREADS = 128;  // modes per block
+
+__device__ __forceinline__ void stage8(double* s, const double* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(s)), "l"(g)
+               : "memory");
+}
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Levels per block: the nr levels split evenly over ceil(nr / RB_R) blocks.
+static inline int radial_rows(int nr) { return ceil_div(nr, ceil_div(nr, RB_R)); }
+
+// Shared-memory image of one block: win[plane][level][thread] holds levels
+// k0 - KL .. k0 + RB_R + KL - 1 (zero outside 0 .. nr-1); band[b][NB (i +
+// KL) + e] holds entry e of band column k0 + i of the block's matrix b; rv[q][i]
+// holds 1/r^(q+1) at level k0 + i.
+template <int KL, int NBAND>
+struct RadialStage {
+  static constexpr int NB = 2 * KL + 1, ROWS = RB_R + 2 * KL;
+  double win[2][ROWS][RAD_THREADS];
+  double band[NBAND][ROWS * NB];
+  double rv[2][RB_R];
+};
+
+template <int KL>
+__device__ __forceinline__ void stage_column(double (*win)[RB_R + 2 * KL][RAD_THREADS], const double* P, size_t plane,
+                                             size_t NM, int N, int k0, int rows, int j) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int t = 0; t < RB_R + 2 * KL; ++t) {
+      const int kk = k0 - KL + t;
+      if (kk >= 0 && kk < N && t < rows + 2 * KL)
+        stage8(&win[c][t][tid], P + c * plane + (size_t)kk * NM + j);
+      else
+        win[c][t][tid] = 0.0;
+    }
+}
+
+// Band columns k0 - KL .. k0 + rows + KL - 1 (those inside 0 .. N-1) of a
+// band matrix stored column by column, NB entries each; plain block-strided
+// copies, ordered before use by the block barrier.
+template <int KL>
+__device__ __forceinline__ void stage_band(double* sb, const double* band, int N, int k0, int rows) {
+  constexpr int NB = 2 * KL + 1;
+  const int c0 = max(0, k0 - KL), c1 = min(N, k0 + rows + KL);
+  const int off = (c0 - (k0 - KL)) * NB;
+  for (int e = threadIdx.x; e < (c1 - c0) * NB; e += RAD_THREADS) sb[off + e] = band[(size_t)c0 * NB + e];
+}
+
+template <int KL, int NBAND>
+static size_t radial_smem() {
+  return sizeof(RadialStage<KL, NBAND>);
+}
+
+// Dynamic shared memory above the 48 KB default, allowed once per kernel.
+template <typename K>
+static void allow_smem(K kernel, size_t bytes, bool& done) {
+  if (!done) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    done = true;
+  }
+}
 
 // compute_all_gradients_spectral! (src/scalar_field_common.jl:125-345):
 // theta derivative by the reference's recurrence coefficients (:158,171), phi
@@ -119,44 +186,64 @@ void launch_gradients_img(cudaStream_t s, const Dims& d, const int* lof, const i
 // image columns 32 shells x [S re, S im, T re, T im] (S = curl_pol, T =
 // curl_tor), column tile r / 32; written there instead of to the FP64 arrays.
 template <int KL, bool IMG>
-__global__ void k_curl(Dims d, const int* __restrict__ lof, const int* __restrict__ mof,
-                       const double* __restrict__ rinv, const double* __restrict__ rinv2,
-                       const double* __restrict__ d1, const double* __restrict__ d2, const double* __restrict__ tor,
-                       const double* __restrict__ pol, double* __restrict__ otor, double* __restrict__ opol,
-                       SynthImageOut img) {
+__global__ void __launch_bounds__(RAD_THREADS, 4) k_curl(Dims d, const int* __restrict__ lof,
+                                                         const int* __restrict__ mof, const double* __restrict__ rinv,
+                                                         const double* __restrict__ rinv2,
+                                                         const double* __restrict__ d1, const double* __restrict__ d2,
+                                                         const double* __restrict__ tor,
+                                                         const double* __restrict__ pol, double* __restrict__ otor,
+                                                         double* __restrict__ opol, int rows, SynthImageOut img) {
   constexpr int NB = 2 * KL + 1;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k0 = blockIdx.y * RB_R;
-  if (j >= d.nlm) return;
-  const double lf = (double)lof[j] * (lof[j] + 1.0);
+  extern __shared__ __align__(16) unsigned char rad_smem[];
+  auto& st = *reinterpret_cast<RadialStage<KL, 2>*>(rad_smem);
+  const int tid = threadIdx.x;
+  const int j = blockIdx.x * RAD_THREADS + tid;
+  const int k0 = blockIdx.y * rows;
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   const int N = d.nr;
+  const bool live = j < d.nlm;
+  if (live) stage_column<KL>(st.win, pol, plane, NM, N, k0, rows, j);
+  stage_band<KL>(st.band[0], d1, N, k0, rows);
+  stage_band<KL>(st.band[1], d2, N, k0, rows);
+  if (tid < rows && k0 + tid < N) {
+    st.rv[0][tid] = rinv[k0 + tid];
+    st.rv[1][tid] = rinv2[k0 + tid];
+  }
+  // the toroidal values of the block's levels: plain loads, in flight with
+  // the staging copies
+  double tv[2][RB_R];
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+#pragma unroll
+    for (int b = 0; b < RB_R; ++b) {
+      const int k = k0 + b;
+      tv[c][b] = (live && b < rows && k < N) ? tor[c * plane + (size_t)k * NM + j] : 0.0;
+    }
+  stage_wait();
+  __syncthreads();
+  if (!live) return;
+  const double lf = (double)lof[j] * (lof[j] + 1.0);
   const SynthImagePos ip = IMG ? synth_image_pos(img, d.L, mof[j], lof[j]) : SynthImagePos{};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
-    const double* P = pol + c * plane;
-    double w[NB];
 #pragma unroll
-    for (int t = 0; t < NB; ++t) {
-      const int kk = k0 - KL + t;
-      w[t] = (kk >= 0 && kk < N) ? P[(size_t)kk * NM + j] : 0.0;
-    }
     for (int b = 0; b < RB_R; ++b) {
       const int k = k0 + b;
-      if (k >= N) break;
+      if (b >= rows || k >= N) break;
       double a1 = 0.0, a2 = 0.0;
 #pragma unroll
       for (int t = 0; t < NB; ++t) {
         const int jj = k - KL + t;
         if (jj >= 0 && jj < N) {
-          const size_t q = (KL + k - jj) + (size_t)NB * jj;
-          a1 += d1[q] * w[t];
-          a2 += d2[q] * w[t];
+          const int q = (2 * KL - t) + NB * (b + t);
+          const double w = st.win[c][b + t][tid];
+          a1 += st.band[0][q] * w;
+          a2 += st.band[1][q] * w;
         }
       }
       const size_t at = (size_t)k * NM + j;
-      const double vt = lf * rinv2[k] * w[KL] - a2 - 2.0 * rinv[k] * a1;
-      const double vp = -lf * rinv2[k] * tor[c * plane + at];
+      const double vt = lf * st.rv[1][b] * st.win[c][b + KL][tid] - a2 - 2.0 * st.rv[0][b] * a1;
+      const double vp = -lf * st.rv[1][b] * tv[c][b];
       if (IMG) {
         const int col = (k & 31) * 4 + c;
         synth_image_put(img, 128, ip, k >> 5, col, vp);
@@ -165,10 +252,6 @@ __global__ void k_curl(Dims d, const int* __restrict__ lof, const int* __restric
         otor[c * plane + at] = vt;
         opol[c * plane + at] = vp;
       }
-#pragma unroll
-      for (int t = 0; t < NB - 1; ++t) w[t] = w[t + 1];
-      const int nx = k + KL + 1;
-      w[NB - 1] = nx < N ? P[(size_t)nx * NM + j] : 0.0;
     }
   }
 }
@@ -176,16 +259,25 @@ __global__ void k_curl(Dims d, const int* __restrict__ lof, const int* __restric
 void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* rinv, const double* rinv2,
                  const double* d1, const double* d2, const double* tor, const double* pol, double* otor,
                  double* opol) {
-  dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
-  k_curl<GD_MAX_KL, false><<<grid, 128, 0, s>>>(d, lof, nullptr, rinv, rinv2, d1, d2, tor, pol, otor, opol,
-                                                SynthImageOut{});
+  const int rows = radial_rows(d.nr);
+  dim3 grid(ceil_div(d.nlm, RAD_THREADS), ceil_div(d.nr, rows));
+  const size_t smem = radial_smem<GD_MAX_KL, 2>();
+  static bool done = false;
+  allow_smem(k_curl<GD_MAX_KL, false>, smem, done);
+  k_curl<GD_MAX_KL, false><<<grid, RAD_THREADS, smem, s>>>(d, lof, nullptr, rinv, rinv2, d1, d2, tor, pol, otor,
+                                                           opol, rows, SynthImageOut{});
 }
 
 void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                      const double* rinv2, const double* d1, const double* d2, const double* tor, const double* pol,
                      const SynthImageOut& img) {
-  dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
-  k_curl<GD_MAX_KL, true><<<grid, 128, 0, s>>>(d, lof, mof, rinv, rinv2, d1, d2, tor, pol, nullptr, nullptr, img);
+  const int rows = radial_rows(d.nr);
+  dim3 grid(ceil_div(d.nlm, RAD_THREADS), ceil_div(d.nr, rows));
+  const size_t smem = radial_smem<GD_MAX_KL, 2>();
+  static bool done = false;
+  allow_smem(k_curl<GD_MAX_KL, true>, smem, done);
+  k_curl<GD_MAX_KL, true><<<grid, RAD_THREADS, smem, s>>>(d, lof, mof, rinv, rinv2, d1, d2, tor, pol, nullptr,
+                                                          nullptr, rows, img);
 }
 
 // apply_temperature_boundary_conditions_spectral! (src/thermal.jl:262-303):

@@ -210,6 +210,21 @@ def test_boundary_modes_match_oracle(gdb, oracle_mod, bc_mode):
         assert np.max(np.abs(re[0])) == 0.0 and np.max(np.abs(re[-1])) == 0.0
 
 
+@pytest.mark.parametrize("bc_mode", [0, 1, 2])
+@pytest.mark.parametrize("lmax,nlat,nlon,nr", [(12, 20, 40, 12), (19, 30, 60, 20), (11, 18, 36, 3)])
+def test_implicit_solve_edges_match_oracle(gdb, oracle_mod, lmax, nlat, nlon, nr, bc_mode):
+    # the implicit solve's edges: an odd mode count (91), a partial second
+    # block of 82 modes (210), fewer levels than the band (nr = 3), under
+    # every boundary mode; three steps cover the AB1 start and two AB2 steps
+    # that read the other bank of nonlinear terms
+    g, o = make_pair(gdb, oracle_mod, lmax, nlat, nlon, nr, bc_mode=bc_mode)
+    load_state(g, o, workloads.seeded_state(lmax, lmax, nr, seed=3))
+    g.step(3); o.step(3)
+    for k in NAMES:
+        a, b = g.get_field(k), o.get_field(k)
+        assert rel(a[0], b[0]) < 1e-11 and rel(a[1], b[1]) < 1e-11, k
+
+
 def test_literal_temperature_growth_matches_oracle(gdb, oracle_mod):
     # bc_mode 0 (the operator as written) amplifies the temperature by a factor
     # of several hundred per step at nr = 129, dt = 2e-6; the device follows it
