@@ -669,3 +669,25 @@ def compute_kinetic_energy(state: SimulationState):
 
 def compute_magnetic_energy(state: SimulationState):
     return state.config.energy()[1]
+
+
+# -- restart files (restart.py): write_restart! / read_restart!
+#    (src/outputs_writer.jl:1221-1371) -------------------------------------------
+def write_restart(model: SHTnsKitConfig, filename, **kw):
+    """The model's spectral state (and physical temperature) in the reference's
+    restart layout; keywords as ``restart.write_restart``."""
+    from . import restart
+    return restart.write_restart(model, filename, **kw)
+
+
+def read_restart(filename):
+    """``(restart_data, metadata)`` of a restart file, as read_restart! returns them."""
+    from . import restart
+    return restart.read_restart(filename)
+
+
+def load_restart(model: SHTnsKitConfig, filename):
+    """Sets a fresh model's five spectral fields from a restart file; the run
+    continues as a new run (AB1 start), like the reference's restarted run."""
+    from . import restart
+    return restart.load_restart(model, filename)
