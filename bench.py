@@ -102,13 +102,17 @@ def kernel_work(name, p, nlm, precision):
         "nl_induction": 6 * G * rb,
         # per field: read u, N, N_prev, write u (the history roll is a bank switch)
         "cnab2_solve": 5 * 4 * S * 8,
+        # the same arrays plus the exponential cache (3 kinds x (L+1) x [E | phi1])
+        "eab2_update": 5 * 4 * S * 8 + 3 * (L + 1) * 2 * nr * nr * 8,
         "spectral_gradients": 4 * S * 8,
         "spectral_curl": 4 * S * 8,
         "temperature_bc": 4 * nlm * 8,
     }
     for k, v in table.items():
         if name.startswith(k):
-            return {"flops": None, "bytes": v}
+            # EAB2: per field and (l, m, plane) column one n x 2n matrix-vector product
+            flops = 5 * S * 2.0 * 2 * nr if k == "eab2_update" else None
+            return {"flops": flops, "bytes": v}
     return None
 
 
@@ -460,6 +464,8 @@ def main():
                     help="instead of the headline: the adjoint configuration's gradient checks and timings")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead of the headline: the batched uneven ensemble of this many shells")
+    ap.add_argument("--scheme", default="cnab2", choices=["cnab2", "eab2"],
+                    help="time-stepping scheme of the step (ts_scheme); the headline metric is CNAB2")
     args = ap.parse_args()
     if args.workload != WORKLOAD:
         globals()["WORKLOAD"] = args.workload
@@ -497,6 +503,8 @@ def main():
                                bc_mode=bc_mode, precision="fp64", device=local)
         if precision == "mixed":
             g.set_precision("mixed")
+        if args.scheme != "cnab2" and bc_mode != 2:
+            g.set_scheme(args.scheme)
         for k, (a, b) in st.items():
             g.set_field(k, a, b)
         return g
@@ -589,7 +597,7 @@ def main():
             bounds.append({"bound": "hbm", "achieved": top["gbs"], "peak": hbm_peak, "unit": "GB/s",
                            "frac": top["gbs"] / hbm_peak, "peak_source": peak_src + " HBM copy bandwidth"})
         if "tflops" in top:
-            if top["name"].endswith("fp64"):
+            if top["name"].endswith("fp64") or top["name"].startswith("eab2"):
                 pk, src = dgemm, "cuBLAS FP64 GEMM 4096^3 measured in this run (torch.matmul)"
             else:
                 pk, src = peaks.get("bf16_tflops", 1590.0) / 2.0, "half the measured bf16 burst peak (tf32 rate)"

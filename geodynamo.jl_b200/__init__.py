@@ -48,6 +48,8 @@ GRIDS = {
     "ind_th": 15, "ind_ph": 16,
 }
 PRECISIONS = {"fp64": 0, "mixed": 1}
+SCHEMES = {"cnab2": 0, "eab2": 1}          # ts_scheme (src/simulation.jl:1176-1300)
+KINDS = {"velocity": 0, "magnetic": 1, "temperature": 2}
 
 # Every symbol include/gdb200.h declares.
 EXPORTS = (
@@ -55,7 +57,8 @@ EXPORTS = (
     "gd_upload_spectral", "gd_download_spectral", "gd_download_nonlinear", "gd_download_grid",
     "gd_set_temperature_bc", "gd_spectral_to_physical", "gd_physical_to_spectral", "gd_vector_synthesis",
     "gd_vector_analysis", "gd_temperature_nonlinear", "gd_velocity_nonlinear", "gd_magnetic_nonlinear",
-    "gd_implicit_step", "gd_step", "gd_step_async", "gd_set_dt", "gd_energy", "gd_check_finite",
+    "gd_implicit_step", "gd_step", "gd_step_async", "gd_set_dt", "gd_set_scheme", "gd_download_etd",
+    "gd_energy", "gd_check_finite",
     "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
     "gd_spectral_to_physical_noalloc",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
@@ -135,6 +138,8 @@ def load_library():
         "gd_step": ([P, I], I),
         "gd_step_async": ([P, I], I),
         "gd_set_dt": ([P, ctypes.c_double], I),
+        "gd_set_scheme": ([P, I], I),
+        "gd_download_etd": ([P, I, I, D, D], I),
         "gd_energy": ([P, D, D], I),
         "gd_check_finite": ([P], I),
         "gd_step_count": ([P], ctypes.c_long),
@@ -245,6 +250,7 @@ class SHTnsKitConfig:
         self.theta_grid, self.gauss_weights, self.r = th, w, r
         self.phi_grid = 2 * np.pi * np.arange(nlon) / nlon
         self.precision = precision
+        self.scheme = "cnab2"
 
     # -- plumbing -------------------------------------------------------------
     def _check(self, st):
@@ -367,6 +373,19 @@ class SHTnsKitConfig:
 
     def synchronize(self):
         self._check(self.lib.gd_synchronize(self.h))
+
+    def set_scheme(self, scheme):
+        """ts_scheme = :cnab2 or :eab2 (src/simulation.jl:1183-1300); "eab2"
+        builds the exponential cache of create_etd_cache on the device."""
+        self._check(self.lib.gd_set_scheme(self.h, SCHEMES[scheme]))
+        self.scheme = scheme
+
+    def etd_matrices(self, kind, l):
+        """(E, phi1) of the EAB2 cache for a field kind ("velocity", "magnetic",
+        "temperature") and degree l, as nr x nr arrays."""
+        E = np.zeros((self.nr, self.nr)); P = np.zeros((self.nr, self.nr))
+        self._check(self.lib.gd_download_etd(self.h, KINDS[kind], int(l), _dptr(E), _dptr(P)))
+        return E, P
 
     def set_dt(self, dt):
         self._check(self.lib.gd_set_dt(self.h, float(dt)))

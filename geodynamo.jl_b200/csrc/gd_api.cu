@@ -278,8 +278,36 @@ int implicit_launch(gd_handle* h, int boot) {
   a.temp_slot = 0;
   a.inv_dt = 1.0 / h->c.dt;
   a.lin_weight = 1.0 - h->c.implicit_theta;
+  a.dt = h->c.dt;
+  if (h->scheme == GD_SCHEME_EAB2) {
+    // eab2_update! takes no AB1 start: N_prev is the other bank (zeros before
+    // the first step, as prev_nonlinear is)
+    { ProfScope p(h, "eab2_update"); launch_eab2(h->stream, h->d, h->d_moff, h->d_etd, a); }
+    return check_launch(h, "eab2");
+  }
   { ProfScope p(h, "cnab2_solve"); launch_cnab2(h->stream, h->d, h->d_lof, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->d_lu, a); }
   return check_launch(h, "cnab2");
+}
+
+// The EAB2 exponential cache for the handle's dt (create_etd_cache,
+// src/timestep.jl:37-70), from the L_l bands of build_implicit.
+int build_etd(gd_handle* h) {
+  const Dims& d = h->d;
+  if (!h->d_etd) AL(h->d_etd, etd_table_doubles(d));
+  double* scratch = nullptr;
+  CK(cudaMalloc(&scratch, etd_scratch_doubles(d) * sizeof(double)));
+  cudaError_t e = cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream);
+  if (e == cudaSuccess) {
+    launch_etd_build(h->stream, d, h->d_lin, h->c.dt, scratch, h->d_etd, h->d_flag);
+    e = cudaGetLastError();
+  }
+  int flag = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(scratch);
+  if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("exponential cache: ") + cudaGetErrorString(e));
+  if (flag) return fail(h, GD_ERR_NONFINITE, "exponential cache: non-finite operator");
+  return GD_OK;
 }
 
 int temperature_nl(gd_handle* h) {
@@ -598,6 +626,7 @@ int gd_magnetic_pullback(gd_handle* h, int field, int nsteps, const double* lam_
                          double* out_re, double* out_im) {
   if (!h || !lam_re || !lam_im || !out_re || !out_im || nsteps < 0 || (field != GD_B_TOR && field != GD_B_POL))
     return h ? fail(h, GD_ERR_ARG, "bad arguments (field must be GD_B_TOR or GD_B_POL)") : GD_ERR_ARG;
+  if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the pullback is of the CNAB2 propagator");
   CK(cudaSetDevice(h->device));
   int s = stage_alloc(h);
   if (s) return s;
@@ -734,7 +763,44 @@ int gd_set_dt(gd_handle* h, double dt) {
   CK(cudaStreamSynchronize(h->stream));
   h->c.dt = dt;
   drop_graphs(h);
-  return build_implicit(h);
+  int s = build_implicit(h);
+  if (s == GD_OK && h->scheme == GD_SCHEME_EAB2) s = build_etd(h);
+  return s;
+}
+
+int gd_set_scheme(gd_handle* h, int scheme) {
+  if (!h || (scheme != GD_SCHEME_CNAB2 && scheme != GD_SCHEME_EAB2))
+    return h ? fail(h, GD_ERR_ARG, "scheme must be GD_SCHEME_CNAB2 or GD_SCHEME_EAB2") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  if (scheme == GD_SCHEME_EAB2) {
+    if (h->c.bc_mode == 2)
+      return fail(h, GD_ERR_UNSUPPORTED, "EAB2 has no boundary rows (bc_mode 2 is a CNAB2 operator option)");
+    if (h->d.nr > 256) return fail(h, GD_ERR_UNSUPPORTED, "EAB2 supports nr <= 256");
+    int s = build_etd(h);
+    if (s) return s;
+  }
+  if (scheme != h->scheme) drop_graphs(h);
+  h->scheme = scheme;
+  return GD_OK;
+}
+
+int gd_download_etd(gd_handle* h, int kind, int l, double* E, double* phi1) {
+  if (!h || !E || !phi1 || kind < 0 || kind > 2 || l < 0 || l > h->d.L)
+    return h ? fail(h, GD_ERR_ARG, "bad kind, degree or pointer") : GD_ERR_ARG;
+  if (h->scheme != GD_SCHEME_EAB2 || !h->d_etd) return fail(h, GD_ERR_ARG, "the scheme is not GD_SCHEME_EAB2");
+  CK(cudaSetDevice(h->device));
+  const size_t n = h->d.nr, n2 = n * n;
+  std::vector<double> t(2 * n2);
+  CK(cudaMemcpyAsync(t.data(), h->d_etd + (size_t)(kind * (h->d.L + 1) + l) * 2 * n2, 2 * n2 * sizeof(double),
+                     cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (size_t i = 0; i < n; ++i)
+    for (size_t k = 0; k < n; ++k) {
+      E[i * n + k] = t[k * n + i];
+      phi1[i * n + k] = t[n2 + k * n + i];
+    }
+  return GD_OK;
 }
 
 int gd_energy(gd_handle* h, double* ekin, double* emag) {

@@ -1,0 +1,365 @@
+// gd_eab2.cu -- the exponential Adams-Bashforth 2 scheme (ts_scheme = :eab2):
+// eab2_update! (src/timestep.jl:429-487) with the dense per-l cache of
+// create_etd_cache (:37-70).  Per radial system (field, l, m):
+//   u^{n+1} = E_l u^n + dt phi1_l (3/2 N^n - 1/2 N^{n-1}),
+//   E_l = exp(dt A_l),  phi1_l = phi1(dt A_l) = (dt A_l)^{-1} (E_l - I),
+// A_l = nu (d2 + (2/r) d1) - nu l(l+1)/r^2, the operator the CNAB2 matrices are
+// built from (the handle's L_l band, same roundings).  The reference applies
+// the same E and phi1 to the velocity and magnetic fields by Krylov
+// approximations (eab2_update_krylov_cached!, :358-427, m = 20, tol 1e-8);
+// here every field uses the dense matrices.
+#include "gd_internal.cuh"
+
+namespace gd {
+
+// ---------------------------------------------------------------------------
+// Exponential cache.  E and phi1 of X = dt A_l by scaling and squaring with a
+// truncated Taylor series: Y = X / 2^s with ||Y||_1 <= 1/2,
+//   E(Y) = sum_{k <= K} Y^k / k!,   P(Y) = sum_{k <= K} Y^k / (k + 1)!,
+// K = 18 (the first omitted term is below 2^-19 / 19! ~ 1.6e-23 of ||Y||^0),
+// then s doublings E(2Y) = E(Y)^2 and P(2Y) = P(Y) (E(Y) + I) / 2 (functions
+// of one matrix commute: phi1(2Y) = (2Y)^-1 (e^Y - I)(e^Y + I)).  This forms
+// phi1 without the inverse of A_l, which create_etd_cache uses and which is
+// nearly singular for l = 0 (A_0 maps a constant to ~0).  One CTA per
+// (kind, l); its n x n matrices live in a global scratch slice and every
+// product is a CTA-wide tiled GEMM.  Output: table [kind][l][k][i] with
+// k < n: E[i][k], k >= n: phi1[i][k - n] (the transposed stacked [E | phi1],
+// so one k-row of the update's operand is contiguous).
+// ---------------------------------------------------------------------------
+constexpr int EX_THREADS = 256;
+constexpr int EX_T = 64;   // GEMM output tile (EX_T x EX_T), 4 x 4 per thread
+constexpr int EX_K = 16;   // GEMM K chunk
+constexpr int EX_TAYLOR = 18;
+
+// C = alpha A B, n x n row-major in global memory (C distinct from A and B).
+__device__ void ex_gemm(int n, const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
+                        double alpha, double* sA, double* sB) {
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  for (int i0 = 0; i0 < n; i0 += EX_T)
+    for (int j0 = 0; j0 < n; j0 += EX_T) {
+      double acc[4][4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = 0.0;
+      for (int k0 = 0; k0 < n; k0 += EX_K) {
+        for (int e = tid; e < EX_T * EX_K; e += EX_THREADS) {
+          const int r = e / EX_K, c = e % EX_K;
+          sA[e] = (i0 + r < n && k0 + c < n) ? A[(size_t)(i0 + r) * n + k0 + c] : 0.0;
+          const int r2 = e / EX_T, c2 = e % EX_T;
+          sB[e] = (k0 + r2 < n && j0 + c2 < n) ? B[(size_t)(k0 + r2) * n + j0 + c2] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < EX_K; ++k) {
+          double a[4], b[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            a[q] = sA[(ty * 4 + q) * EX_K + k];
+            b[q] = sB[k * EX_T + tx * 4 + q];
+          }
+#pragma unroll
+          for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int gi = i0 + ty * 4 + p, gj = j0 + tx * 4 + q;
+          if (gi < n && gj < n) C[(size_t)gi * n + gj] = alpha * acc[p][q];
+        }
+    }
+  __syncthreads();
+}
+
+// lin: the handle's L_l bands, [kind][col][band][l] with entry (row i, col c)
+// at band KL + i - c (k_build_lu).  scratch: 5 n^2 doubles per CTA.
+__global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, const double* __restrict__ lin,
+                                                          double dt, double* __restrict__ scratch,
+                                                          double* __restrict__ tab, int* err) {
+  __shared__ double sA[EX_T * EX_K], sB[EX_K * EX_T];
+  __shared__ double red[EX_THREADS / 32];
+  __shared__ int s_sh;
+  const int g = blockIdx.y, l = blockIdx.x;
+  const int nb = 2 * kl + 1;
+  const size_t n2 = (size_t)n * n;
+  double* X = scratch + (size_t)(g * (L + 1) + l) * 5 * n2;
+  double* Pw = X + n2;
+  double* T = Pw + n2;
+  double* E = T + n2;
+  double* P = E + n2;
+  const double* Lb = lin + (size_t)g * n * nb * (L + 1) + l;
+  const int tid = threadIdx.x;
+  // X = dt A_l (dense)
+  for (size_t e = tid; e < n2; e += EX_THREADS) {
+    const int i = (int)(e / n), c = (int)(e % n);
+    const int b = kl + i - c;
+    X[e] = (b >= 0 && b < nb) ? dt * Lb[((size_t)c * nb + b) * (L + 1)] : 0.0;
+  }
+  __syncthreads();
+  // s from the 1-norm (largest column sum)
+  double cmax = 0.0;
+  for (int c = tid; c < n; c += EX_THREADS) {
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i) sum += fabs(X[(size_t)i * n + c]);
+    cmax = fmax(cmax, sum);
+  }
+  for (int o = 16; o > 0; o >>= 1) cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+  if ((tid & 31) == 0) red[tid >> 5] = cmax;
+  __syncthreads();
+  if (tid == 0) {
+    double v = 0.0;
+    for (int w = 0; w < EX_THREADS / 32; ++w) v = fmax(v, red[w]);
+    int s = 0;
+    if (!(v < 1e300)) {  // not finite: flag and leave the table unusable
+      atomicExch(err, 1);
+      s = -1;
+    } else {
+      while (v > 0.5 && s < 1000) {
+        v *= 0.5;
+        ++s;
+      }
+    }
+    s_sh = s;
+  }
+  __syncthreads();
+  const int s = s_sh;
+  if (s < 0) return;
+  const double sc = ldexp(1.0, -s);
+  // Y = X / 2^s (exact); E = I + Y, P = I + Y / 2, Pw = Y
+  for (size_t e = tid; e < n2; e += EX_THREADS) {
+    const int i = (int)(e / n), c = (int)(e % n);
+    const double y = X[e] * sc, id = i == c ? 1.0 : 0.0;
+    X[e] = y;
+    Pw[e] = y;
+    E[e] = id + y;
+    P[e] = id + 0.5 * y;
+  }
+  __syncthreads();
+  for (int k = 2; k <= EX_TAYLOR; ++k) {
+    ex_gemm(n, Pw, X, T, 1.0 / k, sA, sB);  // T = Y^k / k!
+    const double rk1 = 1.0 / (k + 1);
+    for (size_t e = tid; e < n2; e += EX_THREADS) {
+      const double t = T[e];
+      Pw[e] = t;
+      E[e] += t;
+      P[e] += t * rk1;
+    }
+    __syncthreads();
+  }
+  // doublings
+  for (int it = 0; it < s; ++it) {
+    for (size_t e = tid; e < n2; e += EX_THREADS) {
+      const int i = (int)(e / n), c = (int)(e % n);
+      X[e] = E[e] + (i == c ? 1.0 : 0.0);  // E + I
+    }
+    __syncthreads();
+    ex_gemm(n, P, X, T, 0.5, sA, sB);   // P(2Y) = P (E + I) / 2
+    ex_gemm(n, E, E, Pw, 1.0, sA, sB);  // E(2Y) = E^2
+    for (size_t e = tid; e < n2; e += EX_THREADS) {
+      P[e] = T[e];
+      E[e] = Pw[e];
+    }
+    __syncthreads();
+  }
+  double* out = tab + (size_t)(g * (L + 1) + l) * 2 * n2;
+  for (size_t e = tid; e < n2; e += EX_THREADS) {
+    const int i = (int)(e / n), c = (int)(e % n);
+    out[(size_t)c * n + i] = E[e];
+    out[n2 + (size_t)c * n + i] = P[e];
+  }
+}
+
+size_t etd_table_doubles(const Dims& d) { return (size_t)3 * (d.L + 1) * 2 * d.nr * d.nr; }
+size_t etd_scratch_doubles(const Dims& d) { return (size_t)3 * (d.L + 1) * 5 * d.nr * d.nr; }
+
+void launch_etd_build(cudaStream_t st, const Dims& d, const double* lin, double dt, double* scratch, double* tab,
+                      int* err) {
+  k_etd_build<<<dim3(d.L + 1, 3), EX_THREADS, 0, st>>>(d.nr, d.kl, d.L, lin, dt, scratch, tab, err);
+}
+
+// ---------------------------------------------------------------------------
+// Update.  CTA = (column chunk, l, field slot): the columns of order l are
+// (m, plane) for m = 0 .. min(l, M), 64 per CTA; every thread owns an 8-row x
+// 4-column tile of the output and the K loop runs over the stacked operand
+// [u ; dt w] (2n rows, w = 3/2 N - 1/2 N_prev) against the cached [E | phi1]
+// in chunks of 16 rows, double-buffered: asynchronous 8-byte copies of the
+// next chunk's matrix rows and gathered input columns (u, or N and N_prev,
+// combined into dt w once they land) are in flight while the current chunk is
+// multiplied.  The columns are read in full before the tile is written back
+// over u.  16 x ceil(nr / 8) threads: nr <= 256.
+// ---------------------------------------------------------------------------
+constexpr int EU_COLS = 64;
+constexpr int EU_RT = 8;   // rows per thread
+constexpr int EU_CT = 4;   // columns per thread
+constexpr int EU_KC = 16;  // K rows per chunk
+
+__device__ __forceinline__ void eu_copy8(double* s, const double* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(s)), "l"(g)
+               : "memory");
+}
+
+// MAXT = the thread bound the build is compiled for: 288 (nr <= 144, two CTAs
+// per SM) or 512 (nr <= 256, one).
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 576 / MAXT) k_eab2(Dims d, const int* __restrict__ moff,
+                                                          const double* __restrict__ tab, Cnab2Args a) {
+  extern __shared__ __align__(16) double eu_smem[];
+  const int n = d.nr;
+  const int npad = ((n + EU_RT - 1) / EU_RT) * EU_RT;
+  double* sM = eu_smem;                       // [2][EU_KC][npad]: rows k of the stacked [E | phi1]^T
+  double* sA = sM + 2 * EU_KC * npad;         // [2][EU_KC][EU_COLS]: u rows, or N rows then dt w
+  double* sB = sA + 2 * EU_KC * EU_COLS;      // [2][EU_KC][EU_COLS]: N_prev rows
+  __shared__ int colj[EU_COLS];               // column -> mode index j (-1 past the last column)
+  __shared__ unsigned char colp[EU_COLS];
+  const int slot = blockIdx.z;
+  if (slot >= a.nfield) return;
+  const int l = d.L - (int)blockIdx.y;
+  const int mcount = min(l, d.M) + 1;
+  const int c0 = blockIdx.x * EU_COLS;
+  if (c0 >= 2 * mcount) return;
+  const int g = a.kind[slot];
+  const size_t NM = d.nlm, plane = (size_t)n * NM;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tx = tid % (EU_COLS / EU_CT), ty = tid / (EU_COLS / EU_CT);
+  for (int c = tid; c < EU_COLS; c += nt) {
+    const int cc = c0 + c;
+    if (cc < 2 * mcount) {
+      const int m = cc >> 1;
+      colj[c] = moff[m] + l - m;
+      colp[c] = (unsigned char)(cc & 1);
+    } else {
+      colj[c] = -1;
+      colp[c] = 0;
+    }
+  }
+  __syncthreads();
+  const double* M = tab + (size_t)(g * (d.L + 1) + l) * 2 * (size_t)n * n;
+  const double* __restrict__ u = a.u[slot];
+  const double* __restrict__ nl = a.nl[slot];
+  const double* __restrict__ pv = a.prev[slot];
+  const int nch = (2 * n + EU_KC - 1) / EU_KC;
+  auto issue = [&](int ch, int buf) {
+    const int k0 = ch * EU_KC;
+    double* m_ = sM + buf * EU_KC * npad;
+    double* a_ = sA + buf * EU_KC * EU_COLS;
+    double* b_ = sB + buf * EU_KC * EU_COLS;
+    for (int e = tid; e < EU_KC * npad; e += nt) {
+      const int r = e / npad, i = e % npad, k = k0 + r;
+      if (k < 2 * n && i < n)
+        eu_copy8(m_ + e, M + (size_t)k * n + i);
+      else
+        m_[e] = 0.0;
+    }
+    for (int e = tid; e < EU_KC * EU_COLS; e += nt) {
+      const int r = e / EU_COLS, c = e % EU_COLS, k = k0 + r;
+      const int j = colj[c];
+      if (j >= 0 && k < 2 * n) {
+        const size_t at = (size_t)colp[c] * plane + (size_t)(k < n ? k : k - n) * NM + j;
+        if (k < n) {
+          eu_copy8(a_ + e, u + at);
+        } else {
+          eu_copy8(a_ + e, nl + at);
+          eu_copy8(b_ + e, pv + at);
+        }
+      } else {
+        a_[e] = 0.0;
+        b_[e] = 0.0;
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  double acc[EU_RT][EU_CT];
+#pragma unroll
+  for (int p = 0; p < EU_RT; ++p)
+#pragma unroll
+    for (int q = 0; q < EU_CT; ++q) acc[p][q] = 0.0;
+  issue(0, 0);
+  for (int ch = 0; ch < nch; ++ch) {
+    const int buf = ch & 1;
+    if (ch + 1 < nch) {
+      issue(ch + 1, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    const int k0 = ch * EU_KC;
+    double* a_ = sA + buf * EU_KC * EU_COLS;
+    if (k0 + EU_KC > n) {
+      // rows of the N part: dt w = dt (3/2 N - 1/2 N_prev)
+      const double* b_ = sB + buf * EU_KC * EU_COLS;
+      for (int e = tid; e < EU_KC * EU_COLS; e += nt) {
+        const int k = k0 + e / EU_COLS;
+        if (k >= n && k < 2 * n) a_[e] = a.dt * (1.5 * a_[e] - 0.5 * b_[e]);
+      }
+      __syncthreads();
+    }
+    const double* m_ = sM + buf * EU_KC * npad;
+#pragma unroll 4
+    for (int r = 0; r < EU_KC; ++r) {
+      double mv[EU_RT], xv[EU_CT];
+      const double2* mr = reinterpret_cast<const double2*>(m_ + r * npad + ty * EU_RT);
+      const double2* xr = reinterpret_cast<const double2*>(a_ + r * EU_COLS + tx * EU_CT);
+#pragma unroll
+      for (int p = 0; p < EU_RT / 2; ++p) {
+        const double2 t = mr[p];
+        mv[2 * p] = t.x;
+        mv[2 * p + 1] = t.y;
+      }
+#pragma unroll
+      for (int q = 0; q < EU_CT / 2; ++q) {
+        const double2 t = xr[q];
+        xv[2 * q] = t.x;
+        xv[2 * q + 1] = t.y;
+      }
+#pragma unroll
+      for (int p = 0; p < EU_RT; ++p)
+#pragma unroll
+        for (int q = 0; q < EU_CT; ++q) acc[p][q] = fma(mv[p], xv[q], acc[p][q]);
+    }
+    __syncthreads();
+  }
+  double* __restrict__ uo = a.u[slot];
+#pragma unroll
+  for (int q = 0; q < EU_CT; ++q) {
+    const int c = tx * EU_CT + q;
+    const int j = colj[c];
+    if (j < 0) continue;
+    const size_t base = (size_t)colp[c] * plane + j;
+#pragma unroll
+    for (int p = 0; p < EU_RT; ++p) {
+      const int i = ty * EU_RT + p;
+      if (i >= n) continue;
+      // bc_mode 1 zeroes the boundary rows after the update
+      const bool clamp = a.clamp_rows && (i == 0 || i == n - 1);
+      uo[base + (size_t)i * NM] = clamp ? 0.0 : acc[p][q];
+    }
+  }
+}
+
+int eab2_threads(const Dims& d) { return (EU_COLS / EU_CT) * ((d.nr + EU_RT - 1) / EU_RT); }
+
+void launch_eab2(cudaStream_t st, const Dims& d, const int* moff, const double* tab, const Cnab2Args& a) {
+  const int npad = ((d.nr + EU_RT - 1) / EU_RT) * EU_RT;
+  const size_t smem = (size_t)2 * EU_KC * (npad + 2 * EU_COLS) * sizeof(double);
+  static size_t attr = 0;
+  if (attr < smem) {
+    cudaFuncSetAttribute(k_eab2<288>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_eab2<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = smem;
+  }
+  const int ncc = ceil_div(2 * (d.M + 1), EU_COLS);
+  const dim3 grid(ncc, d.L + 1, a.nfield);
+  const int nt = eab2_threads(d);
+  if (nt <= 288)
+    k_eab2<288><<<grid, nt, smem, st>>>(d, moff, tab, a);
+  else
+    k_eab2<512><<<grid, nt, smem, st>>>(d, moff, tab, a);
+}
+
+}  // namespace gd

@@ -46,6 +46,9 @@ struct gd_handle {
   double *d_epart = nullptr, *d_eout = nullptr;
   // host-ABI staging (lazy)
   double *d_stage_spec = nullptr, *d_stage_spec2 = nullptr, *d_stage_grid = nullptr, *d_stage_grid2 = nullptr;
+  // time-stepping scheme and the EAB2 exponential cache (lazy)
+  int scheme = 0;             // GD_SCHEME_*
+  double* d_etd = nullptr;    // [kind][l][2 nr][nr]: transposed [E | phi1]
   // mixed precision state (lazy)
   gd::MixedState* mixed = nullptr;
   // graphs (index: boot flag)

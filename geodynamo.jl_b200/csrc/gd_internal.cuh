@@ -125,7 +125,14 @@ struct Cnab2Args {
   const double* bvals;        // temperature boundary values [2][nlm] (native order)
   int temp_slot;              // slot index of the temperature field
   double inv_dt, lin_weight;
+  double dt;                  // EAB2: the time step applied to the phi1 term
 };
+// ---- exponential Adams-Bashforth 2 (gd_eab2.cu) ----
+size_t etd_table_doubles(const Dims& d);
+size_t etd_scratch_doubles(const Dims& d);
+void launch_etd_build(cudaStream_t s, const Dims& d, const double* lin, double dt, double* scratch, double* tab,
+                      int* err);
+void launch_eab2(cudaStream_t s, const Dims& d, const int* moff, const double* tab, const Cnab2Args& a);
 // ---- reverse mode (gd_adjoint.cu) ----
 void launch_cnab2_pullback(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,
                            int kind, double dt, double theta, int clamp_rows, int bc_rows, int nsteps, double* lam);

@@ -112,6 +112,11 @@ function step!(h::Handle, state; nsteps::Integer = 1)
     return state
 end
 
+# ts_scheme (src/simulation.jl:1176-1300): :cnab2 or :eab2 for the steps of h.
+const SCHEME = Dict(:cnab2 => 0, :eab2 => 1)
+set_scheme!(h::Handle, scheme::Symbol) =
+    check(h, ccall((:gd_set_scheme, LIB), Cint, (Ptr{Cvoid}, Cint), h.ptr, SCHEME[scheme]))
+
 # Reverse mode.  magnetic_pullback(h, :b_pol, nsteps, λre, λim) -> (gre, gim):
 # the vector-Jacobian product of nsteps steps with respect to a magnetic
 # component at their start (gd_magnetic_pullback; planes (nlm, nr), as the

@@ -49,8 +49,9 @@ COMPONENTS = {
 
 def write_restart(model, filename, time=0.0, step=None, last_output_time=0.0, output_count=0, restart_count=0,
                   grid_file_written=True, rank=0, nprocs=1, physical_temperature=True, metadata=None):
-    """Writes the model's spectral state (and its physical temperature) to
-    ``filename`` in the restart layout of write_restart! (outputs_writer.jl:1221).
+    """Writes the model's spectral state (and its physical temperature, the
+    model's own synthesis of the spectral temperature) to ``filename`` in the
+    restart layout of write_restart! (outputs_writer.jl:1221).
 
     ``step`` defaults to the model's step count; the tracker counters are
     stored as given.  Returns the filename."""

@@ -54,6 +54,11 @@ enum {
 /* Precision modes. */
 enum { GD_PREC_FP64 = 0, GD_PREC_MIXED = 1 };
 
+/* Time-stepping schemes of gd_step (the reference's ts_scheme,
+ * src/simulation.jl:1176-1300): CNAB2 (build_rhs_cnab2! + solve_implicit_step!)
+ * or EAB2 (eab2_update! with the exponential cache of create_etd_cache). */
+enum { GD_SCHEME_CNAB2 = 0, GD_SCHEME_EAB2 = 1 };
+
 /*
  * Model configuration.  Mirrors GeoDynamoParameters (src/parameters.jl:14-76):
  * i_L/i_M/i_Th/i_Ph/i_N/i_KL, d_rratio, d_E, d_Ra, d_Pr, d_Pm, d_timestep,
@@ -161,8 +166,22 @@ int gd_step(gd_handle* h, int nsteps);
 /* Like gd_step, but records nothing to host and returns immediately
  * (asynchronous on the handle's stream). */
 int gd_step_async(gd_handle* h, int nsteps);
-/* Rebuild the implicit matrices for a new time step (src/simulation.jl:335-337). */
+/* Rebuild the implicit matrices (and, under EAB2, the exponential cache) for a
+ * new time step (src/simulation.jl:335-337). */
 int gd_set_dt(gd_handle* h, double dt);
+/* Select the time-stepping scheme of gd_step: ts_scheme = :cnab2 or :eab2
+ * (src/simulation.jl:1183-1300).  GD_SCHEME_EAB2 builds, per field kind and
+ * degree l, E = exp(dt A_l) and phi1(dt A_l) (create_etd_cache,
+ * src/timestep.jl:37-70, A_l the operator of the CNAB2 matrices) on the device
+ * and replaces the banded solve by u <- E u + dt phi1 (3/2 N - 1/2 N_prev)
+ * (eab2_update!, :429-487; no AB1 start: the history starts as zeros, as
+ * prev_nonlinear does).  GD_ERR_UNSUPPORTED with bc_mode 2 (the reference's
+ * exponential scheme has no boundary rows) or nr > 256. */
+int gd_set_scheme(gd_handle* h, int scheme);
+/* The exponential cache of field kind `kind` (0 velocity, 1 magnetic,
+ * 2 temperature) at degree l: E and phi1 as nr x nr row-major matrices.
+ * GD_ERR_ARG unless the scheme is GD_SCHEME_EAB2. */
+int gd_download_etd(gd_handle* h, int kind, int l, double* E, double* phi1);
 /* compute_kinetic_energy / compute_magnetic_energy (src/velocity.jl:782-825,
  * src/magnetic.jl:504-543), both as 0.5 sum (T^2+P^2)/max(l(l+1),1). */
 int gd_energy(gd_handle* h, double* ekin, double* emag);

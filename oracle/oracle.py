@@ -244,3 +244,63 @@ class Oracle:
 
     def step_count(self):
         return self.lib.oc_step_count(self.h)
+
+    # -- ts_scheme = :eab2 (test restatement) -----------------------------------
+    def etd_cache(self, kind):
+        """create_etd_cache (src/timestep.jl:37-70) for a field kind (0 velocity,
+        1 magnetic, 2 temperature) at the configuration's dt: per degree l the
+        dense operator A_l (the L_l band of the implicit matrices,
+        src/timestep.jl:498-543), E_l = exp(dt A_l) and phi1_l = phi1(dt A_l).
+        exp is scipy.linalg.expm (scaling and squaring with Pade approximants,
+        Al-Mohy and Higham 2009; Julia's matrix exp follows Higham 2005).  phi1
+        is the top-right block of exp([[dt A, I], [0, 0]]), the same function
+        the reference forms as A^-1 (E - I) / dt; that solve loses accuracy
+        where A_l is nearly singular, as A_0 is (it maps a constant to ~0).
+        Returns (A, E, phi1), lists indexed by l."""
+        from scipy.linalg import expm
+        n, kl, dt = self.nr, self.kl, self.cfg.dt
+        A, E, P = [], [], []
+        for l in range(self.lmax + 1):
+            lin, _ = self.implicit_matrices(kind, l)   # band rows kl + i - c, columns c
+            a = np.zeros((n, n))
+            for c in range(n):
+                for b in range(2 * kl + 1):
+                    i = c + b - kl
+                    if 0 <= i < n:
+                        a[i, c] = lin[b, c]
+            big = np.zeros((2 * n, 2 * n))
+            big[:n, :n] = dt * a
+            big[:n, n:] = np.eye(n)
+            ex = expm(big)
+            A.append(a)
+            E.append(ex[:n, :n].copy())
+            P.append(ex[:n, n:].copy())
+        return A, E, P
+
+    def eab2_step(self, caches, history):
+        """One step of step_once! under ts_scheme = :eab2: the three nonlinear
+        phases, then for every field u <- E_l u + dt phi1_l (3/2 N - 1/2 N_prev)
+        per (l, m) column (eab2_update!, src/timestep.jl:429-487) and the roll
+        N_prev := N (src/simulation.jl:1311-1329).  caches[kind] = etd_cache(kind);
+        history maps a field name to its (re, im) N_prev (missing: zeros, as
+        prev_nonlinear starts) and is updated in place."""
+        dt = self.cfg.dt
+        self.temperature_nl()
+        self.velocity_nl()
+        self.magnetic_nl()
+        lv = np.array([p[0] for p in lm_pairs(self.lmax, self.mmax)])
+        for name, kind in (("u_tor", 0), ("u_pol", 0), ("b_tor", 1), ("b_pol", 1), ("temp", 2)):
+            _, E, P = caches[kind]
+            re, im = self.get_field(name)
+            nre, nim = self.get_nl(name)
+            pre, pim = history.get(name, (np.zeros_like(re), np.zeros_like(im)))
+            out = []
+            for u, nn, pp in ((re, nre, pre), (im, nim, pim)):
+                w = 1.5 * nn - 0.5 * pp
+                v = np.empty_like(u)
+                for l in range(self.lmax + 1):
+                    cols = lv == l
+                    v[:, cols] = E[l] @ u[:, cols] + dt * (P[l] @ w[:, cols])
+                out.append(v)
+            self.set_field(name, *out)
+            history[name] = (nre, nim)
