@@ -104,14 +104,20 @@ def kernel_work(name, p, nlm, precision):
         "cnab2_solve": 5 * 4 * S * 8,
         # the same arrays plus the exponential cache (3 kinds x (L+1) x [E | phi1])
         "eab2_update": 5 * 4 * S * 8 + 3 * (L + 1) * 2 * nr * nr * 8,
+        # linear = E u, k1 = phi1 N, stage = E_h u + phi1_h N over u: 7 arrays per field, 4 matrices
+        "erk2_prepare": 5 * 7 * S * 8 + 3 * (L + 1) * 4 * nr * nr * 8,
+        # u = linear + dt (k1 + phi2 (N_stage - N)): 5 arrays per field, 1 matrix
+        "erk2_finalize": 5 * 5 * S * 8 + 3 * (L + 1) * nr * nr * 8,
         "spectral_gradients": 4 * S * 8,
         "spectral_curl": 4 * S * 8,
         "temperature_bc": 4 * nlm * 8,
     }
     for k, v in table.items():
         if name.startswith(k):
-            # EAB2: per field and (l, m, plane) column one n x 2n matrix-vector product
-            flops = 5 * S * 2.0 * 2 * nr if k == "eab2_update" else None
+            # per field and (l, m, plane) column: EAB2 one n x 2n matrix-vector
+            # product, the ERK2 prepare four n x n ones, the finalize one
+            mv = {"eab2_update": 2, "erk2_prepare": 4, "erk2_finalize": 1}.get(k)
+            flops = 5 * S * 2.0 * mv * nr if mv else None
             return {"flops": flops, "bytes": v}
     return None
 
@@ -464,7 +470,7 @@ def main():
                     help="instead of the headline: the adjoint configuration's gradient checks and timings")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead of the headline: the batched uneven ensemble of this many shells")
-    ap.add_argument("--scheme", default="cnab2", choices=["cnab2", "eab2"],
+    ap.add_argument("--scheme", default="cnab2", choices=["cnab2", "eab2", "erk2"],
                     help="time-stepping scheme of the step (ts_scheme); the headline metric is CNAB2")
     args = ap.parse_args()
     if args.workload != WORKLOAD:
@@ -597,7 +603,7 @@ def main():
             bounds.append({"bound": "hbm", "achieved": top["gbs"], "peak": hbm_peak, "unit": "GB/s",
                            "frac": top["gbs"] / hbm_peak, "peak_source": peak_src + " HBM copy bandwidth"})
         if "tflops" in top:
-            if top["name"].endswith("fp64") or top["name"].startswith("eab2"):
+            if top["name"].endswith("fp64") or top["name"].startswith(("eab2", "erk2")):
                 pk, src = dgemm, "cuBLAS FP64 GEMM 4096^3 measured in this run (torch.matmul)"
             else:
                 pk, src = peaks.get("bf16_tflops", 1590.0) / 2.0, "half the measured bf16 burst peak (tf32 rate)"

@@ -48,7 +48,8 @@ GRIDS = {
     "ind_th": 15, "ind_ph": 16,
 }
 PRECISIONS = {"fp64": 0, "mixed": 1}
-SCHEMES = {"cnab2": 0, "eab2": 1}          # ts_scheme (src/simulation.jl:1176-1300)
+SCHEMES = {"cnab2": 0, "eab2": 1, "erk2": 2}   # ts_scheme (src/simulation.jl:1054-1300)
+ETD_MATRICES = ("E", "phi1", "phi2", "E_half", "phi1_half")   # ERK2Cache fields (src/timestep.jl:830-853)
 KINDS = {"velocity": 0, "magnetic": 1, "temperature": 2}
 
 # Every symbol include/gdb200.h declares.
@@ -139,7 +140,7 @@ def load_library():
         "gd_step_async": ([P, I], I),
         "gd_set_dt": ([P, ctypes.c_double], I),
         "gd_set_scheme": ([P, I], I),
-        "gd_download_etd": ([P, I, I, D, D], I),
+        "gd_download_etd": ([P, I, I, I, D], I),
         "gd_energy": ([P, D, D], I),
         "gd_check_finite": ([P], I),
         "gd_step_count": ([P], ctypes.c_long),
@@ -375,17 +376,22 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_synchronize(self.h))
 
     def set_scheme(self, scheme):
-        """ts_scheme = :cnab2 or :eab2 (src/simulation.jl:1183-1300); "eab2"
-        builds the exponential cache of create_etd_cache on the device."""
+        """ts_scheme = :cnab2, :eab2 or :erk2 (src/simulation.jl:1054-1300); the
+        exponential schemes build the cache of create_etd_cache /
+        create_erk2_cache on the device."""
         self._check(self.lib.gd_set_scheme(self.h, SCHEMES[scheme]))
         self.scheme = scheme
 
     def etd_matrices(self, kind, l):
-        """(E, phi1) of the EAB2 cache for a field kind ("velocity", "magnetic",
-        "temperature") and degree l, as nr x nr arrays."""
-        E = np.zeros((self.nr, self.nr)); P = np.zeros((self.nr, self.nr))
-        self._check(self.lib.gd_download_etd(self.h, KINDS[kind], int(l), _dptr(E), _dptr(P)))
-        return E, P
+        """The exponential cache for a field kind ("velocity", "magnetic",
+        "temperature") and degree l: {"E", "phi1", "phi2", "E_half",
+        "phi1_half"} as nr x nr arrays."""
+        out = {}
+        for w, name in enumerate(ETD_MATRICES):
+            m = np.zeros((self.nr, self.nr))
+            self._check(self.lib.gd_download_etd(self.h, KINDS[kind], int(l), w, _dptr(m)))
+            out[name] = m
+        return out
 
     def set_dt(self, dt):
         self._check(self.lib.gd_set_dt(self.h, float(dt)))

@@ -260,6 +260,93 @@ int magnetic_nl_fp64(gd_handle* h) {
   return analysis_vector(h, h->grid(GD_GRID_IND_TH), h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
 }
 
+ExpApply exp_apply_args(gd_handle* h, const Cnab2Args& a) {
+  ExpApply e{};
+  e.nfield = a.nfield;
+  for (int i = 0; i < a.nfield; ++i) e.kind[i] = a.kind[i];
+  e.top_block = e.bot_block = -1;
+  e.bot_scale = 1.0;
+  e.dt = h->c.dt;
+  return e;
+}
+
+int temperature_nl(gd_handle* h);
+int velocity_nl(gd_handle* h);
+int magnetic_nl(gd_handle* h);
+
+// compute_all_nonlinear_terms! (src/simulation.jl:800-813): velocity, magnetic,
+// temperature, in that order (the carried grids make the order matter).
+int all_nonlinear(gd_handle* h) {
+  int s = velocity_nl(h);
+  if (s) return s;
+  if (h->c.magnetic) {
+    s = magnetic_nl(h);
+    if (s) return s;
+  }
+  return temperature_nl(h);
+}
+
+// erk2_integrate_full_step! (src/simulation.jl:1054-1149) after the step's
+// nonlinear terms N^n (bank nl_par): erk2_prepare_field! (linear = E u,
+// k1 = phi1 N^n, stage = E_h u + dt/2 phi1_h N^n written over u), the
+// nonlinear terms of the stage into the other bank, erk2_finalize_field!
+// (u = linear + dt (k1 + phi2 (N_stage - N^n))), and the closing evaluation of
+// the nonlinear terms at the new state (into bank nl_par), whose only lasting
+// effect is on the physical grids the next step carries.
+int erk2_launch(gd_handle* h, const Cnab2Args& a) {
+  const size_t se = h->spec_elems();
+  ExpApply e = exp_apply_args(h, a);
+  const int order[5] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL};
+  double* lin[5];
+  double* k1[5];
+  for (int i = 0; i < a.nfield; ++i) {
+    lin[i] = h->d_erk2 + (size_t)order[i] * se;
+    k1[i] = h->d_erk2 + (size_t)(5 + order[i]) * se;
+  }
+  {
+    ProfScope p(h, "erk2_prepare");
+    ExpApply x = e;  // linear = E u
+    for (int i = 0; i < a.nfield; ++i) { x.top[i] = a.u[i]; x.out[i] = lin[i]; }
+    x.top_block = 0;
+    launch_exp_apply(h->stream, h->d, h->d_moff, h->d_etd, x);
+    x = e;           // k1 = phi1 N^n
+    for (int i = 0; i < a.nfield; ++i) { x.bot_a[i] = a.nl[i]; x.out[i] = k1[i]; }
+    x.bot_block = 1;
+    launch_exp_apply(h->stream, h->d, h->d_moff, h->d_etd, x);
+    x = e;           // stage = E_h u + dt/2 phi1_h N^n, over u
+    for (int i = 0; i < a.nfield; ++i) { x.top[i] = a.u[i]; x.bot_a[i] = a.nl[i]; x.out[i] = a.u[i]; }
+    x.top_block = 3;
+    x.bot_block = 4;
+    x.bot_scale = 0.5 * h->c.dt;
+    launch_exp_apply(h->stream, h->d, h->d_moff, h->d_etd, x);
+  }
+  int s = check_launch(h, "erk2 prepare");
+  if (s) return s;
+  h->nl_par ^= 1;  // the stage's terms go to the other bank
+  s = all_nonlinear(h);
+  h->nl_par ^= 1;
+  if (s) return s;
+  {
+    ProfScope p(h, "erk2_finalize");
+    ExpApply x = e;  // u = linear + dt (k1 + phi2 (N_stage - N^n))
+    for (int i = 0; i < a.nfield; ++i) {
+      x.bot_a[i] = h->nl_bank(h->nl_par ^ 1) + (size_t)order[i] * se;
+      x.bot_b[i] = a.nl[i];
+      x.out[i] = a.u[i];
+      x.lin[i] = lin[i];
+      x.k1[i] = k1[i];
+    }
+    x.bot_block = 2;
+    x.bot_mode = 2;
+    x.epilogue = 1;
+    x.clamp_rows = a.clamp_rows;
+    launch_exp_apply(h->stream, h->d, h->d_moff, h->d_etd, x);
+  }
+  s = check_launch(h, "erk2 finalize");
+  if (s) return s;
+  return all_nonlinear(h);
+}
+
 int implicit_launch(gd_handle* h, int boot) {
   Cnab2Args a{};
   const int order[5] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL};
@@ -282,9 +369,22 @@ int implicit_launch(gd_handle* h, int boot) {
   if (h->scheme == GD_SCHEME_EAB2) {
     // eab2_update! takes no AB1 start: N_prev is the other bank (zeros before
     // the first step, as prev_nonlinear is)
-    { ProfScope p(h, "eab2_update"); launch_eab2(h->stream, h->d, h->d_moff, h->d_etd, a); }
+    ExpApply e = exp_apply_args(h, a);
+    for (int i = 0; i < a.nfield; ++i) {
+      e.top[i] = a.u[i];
+      e.bot_a[i] = a.nl[i];
+      e.bot_b[i] = a.prev[i];
+      e.out[i] = a.u[i];
+    }
+    e.top_block = 0;
+    e.bot_block = 1;
+    e.bot_mode = 1;
+    e.bot_scale = h->c.dt;
+    e.clamp_rows = a.clamp_rows;
+    { ProfScope p(h, "eab2_update"); launch_exp_apply(h->stream, h->d, h->d_moff, h->d_etd, e); }
     return check_launch(h, "eab2");
   }
+  if (h->scheme == GD_SCHEME_ERK2) return erk2_launch(h, a);
   { ProfScope p(h, "cnab2_solve"); launch_cnab2(h->stream, h->d, h->d_lof, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->d_lu, a); }
   return check_launch(h, "cnab2");
 }
@@ -764,19 +864,21 @@ int gd_set_dt(gd_handle* h, double dt) {
   h->c.dt = dt;
   drop_graphs(h);
   int s = build_implicit(h);
-  if (s == GD_OK && h->scheme == GD_SCHEME_EAB2) s = build_etd(h);
+  if (s == GD_OK && h->scheme != GD_SCHEME_CNAB2) s = build_etd(h);
   return s;
 }
 
 int gd_set_scheme(gd_handle* h, int scheme) {
-  if (!h || (scheme != GD_SCHEME_CNAB2 && scheme != GD_SCHEME_EAB2))
-    return h ? fail(h, GD_ERR_ARG, "scheme must be GD_SCHEME_CNAB2 or GD_SCHEME_EAB2") : GD_ERR_ARG;
+  if (!h || (scheme != GD_SCHEME_CNAB2 && scheme != GD_SCHEME_EAB2 && scheme != GD_SCHEME_ERK2))
+    return h ? fail(h, GD_ERR_ARG, "scheme must be GD_SCHEME_CNAB2, GD_SCHEME_EAB2 or GD_SCHEME_ERK2") : GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
-  if (scheme == GD_SCHEME_EAB2) {
+  if (scheme != GD_SCHEME_CNAB2) {
     if (h->c.bc_mode == 2)
-      return fail(h, GD_ERR_UNSUPPORTED, "EAB2 has no boundary rows (bc_mode 2 is a CNAB2 operator option)");
-    if (h->d.nr > 256) return fail(h, GD_ERR_UNSUPPORTED, "EAB2 supports nr <= 256");
+      return fail(h, GD_ERR_UNSUPPORTED,
+                  "the exponential schemes have no boundary rows (bc_mode 2 is a CNAB2 operator option)");
+    if (h->d.nr > 256) return fail(h, GD_ERR_UNSUPPORTED, "the exponential schemes support nr <= 256");
+    if (scheme == GD_SCHEME_ERK2 && !h->d_erk2) AL(h->d_erk2, 10 * h->spec_elems());
     int s = build_etd(h);
     if (s) return s;
   }
@@ -785,21 +887,18 @@ int gd_set_scheme(gd_handle* h, int scheme) {
   return GD_OK;
 }
 
-int gd_download_etd(gd_handle* h, int kind, int l, double* E, double* phi1) {
-  if (!h || !E || !phi1 || kind < 0 || kind > 2 || l < 0 || l > h->d.L)
-    return h ? fail(h, GD_ERR_ARG, "bad kind, degree or pointer") : GD_ERR_ARG;
-  if (h->scheme != GD_SCHEME_EAB2 || !h->d_etd) return fail(h, GD_ERR_ARG, "the scheme is not GD_SCHEME_EAB2");
+int gd_download_etd(gd_handle* h, int kind, int l, int which, double* out) {
+  if (!h || !out || kind < 0 || kind > 2 || l < 0 || l > h->d.L || which < 0 || which > 4)
+    return h ? fail(h, GD_ERR_ARG, "bad kind, degree, matrix or pointer") : GD_ERR_ARG;
+  if (h->scheme == GD_SCHEME_CNAB2 || !h->d_etd) return fail(h, GD_ERR_ARG, "no exponential scheme is selected");
   CK(cudaSetDevice(h->device));
   const size_t n = h->d.nr, n2 = n * n;
-  std::vector<double> t(2 * n2);
-  CK(cudaMemcpyAsync(t.data(), h->d_etd + (size_t)(kind * (h->d.L + 1) + l) * 2 * n2, 2 * n2 * sizeof(double),
+  std::vector<double> t(n2);
+  CK(cudaMemcpyAsync(t.data(), h->d_etd + ((size_t)(kind * (h->d.L + 1) + l) * 5 + which) * n2, n2 * sizeof(double),
                      cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   for (size_t i = 0; i < n; ++i)
-    for (size_t k = 0; k < n; ++k) {
-      E[i * n + k] = t[k * n + i];
-      phi1[i * n + k] = t[n2 + k * n + i];
-    }
+    for (size_t k = 0; k < n; ++k) out[i * n + k] = t[k * n + i];
   return GD_OK;
 }
 

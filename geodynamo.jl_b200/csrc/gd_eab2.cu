@@ -1,35 +1,46 @@
-// gd_eab2.cu -- the exponential Adams-Bashforth 2 scheme (ts_scheme = :eab2):
-// eab2_update! (src/timestep.jl:429-487) with the dense per-l cache of
-// create_etd_cache (:37-70).  Per radial system (field, l, m):
-//   u^{n+1} = E_l u^n + dt phi1_l (3/2 N^n - 1/2 N^{n-1}),
-//   E_l = exp(dt A_l),  phi1_l = phi1(dt A_l) = (dt A_l)^{-1} (E_l - I),
-// A_l = nu (d2 + (2/r) d1) - nu l(l+1)/r^2, the operator the CNAB2 matrices are
-// built from (the handle's L_l band, same roundings).  The reference applies
-// the same E and phi1 to the velocity and magnetic fields by Krylov
-// approximations (eab2_update_krylov_cached!, :358-427, m = 20, tol 1e-8);
-// here every field uses the dense matrices.
+// gd_eab2.cu -- the exponential time schemes of apply_master_implicit_step!
+// (ts_scheme = :eab2 and :erk2, src/simulation.jl:1054-1300) with the dense
+// per-l caches of create_etd_cache (src/timestep.jl:37-70) and
+// create_erk2_cache (:896-968).  Per radial system (field, l, m):
+//   EAB2 (eab2_update!, :429-487):
+//     u^{n+1} = E u^n + dt phi1 (3/2 N^n - 1/2 N^{n-1}),
+//   ERK2 (erk2_prepare_field! / erk2_finalize_field!, :1316-1557):
+//     stage   = E_h u^n + (dt/2) phi1_h N^n,
+//     u^{n+1} = E u^n + dt (phi1 N^n + phi2 (N(stage) - N^n)),
+// E = exp(dt A_l), phi1 = phi1(dt A_l), phi2 = phi2(dt A_l), E_h and phi1_h the
+// same at dt/2; A_l = nu (d2 + (2/r) d1) - nu l(l+1)/r^2, the operator the
+// CNAB2 matrices are built from (the handle's L_l band, same roundings).  The
+// reference applies EAB2's E and phi1 to the velocity and magnetic fields by
+// Krylov approximations (eab2_update_krylov_cached!, :358-427, m = 20, tol
+// 1e-8); here every field uses the dense matrices.
 #include "gd_internal.cuh"
 
 namespace gd {
 
 // ---------------------------------------------------------------------------
-// Exponential cache.  E and phi1 of X = dt A_l by scaling and squaring with a
-// truncated Taylor series: Y = X / 2^s with ||Y||_1 <= 1/2,
-//   E(Y) = sum_{k <= K} Y^k / k!,   P(Y) = sum_{k <= K} Y^k / (k + 1)!,
-// K = 18 (the first omitted term is below 2^-19 / 19! ~ 1.6e-23 of ||Y||^0),
-// then s doublings E(2Y) = E(Y)^2 and P(2Y) = P(Y) (E(Y) + I) / 2 (functions
-// of one matrix commute: phi1(2Y) = (2Y)^-1 (e^Y - I)(e^Y + I)).  This forms
-// phi1 without the inverse of A_l, which create_etd_cache uses and which is
-// nearly singular for l = 0 (A_0 maps a constant to ~0).  One CTA per
-// (kind, l); its n x n matrices live in a global scratch slice and every
-// product is a CTA-wide tiled GEMM.  Output: table [kind][l][k][i] with
-// k < n: E[i][k], k >= n: phi1[i][k - n] (the transposed stacked [E | phi1],
-// so one k-row of the update's operand is contiguous).
+// Exponential cache.  E, phi1 and phi2 of X = dt A_l by scaling and squaring
+// with truncated Taylor series: Y = X / 2^s with ||Y||_1 <= 1/2 and s >= 1,
+//   E(Y) = sum Y^k / k!,  P(Y) = sum Y^k / (k + 1)!,  Q(Y) = sum Y^k / (k + 2)!
+// for k <= K = 18 (the first omitted term is below 2^-19 / 19! ~ 1.6e-23 of
+// ||Y||^0), then s doublings (functions of one matrix commute):
+//   E(2Y) = E(Y)^2,  P(2Y) = P(Y) (E(Y) + I) / 2,  Q(2Y) = (2 Q(Y) + P(Y)^2) / 4,
+// the last two from e^Y = I + Y P(Y) and P(Y) = I + Y Q(Y).  The half-step
+// matrices are the state before the last doubling.  This forms phi1 and phi2
+// without the inverse of A_l, which create_etd_cache and compute_phi1_function
+// use: A_l has no boundary rows, so the radial equation's two homogeneous
+// solutions leave it numerically singular (condition ~1e16 for every l).  One
+// CTA per (kind, l); its n x n matrices live in a global scratch slice and
+// every product is a CTA-wide tiled GEMM.  Output per (kind, l): five n x n
+// blocks, each transposed (block b, row k = column k of the matrix) --
+//   0: E, 1: phi1, 2: phi2, 3: E at dt/2, 4: phi1 at dt/2 --
+// so that blocks 0 and 1 together are the EAB2 operand [E | phi1] with one
+// contiguous k-row per stacked input row.
 // ---------------------------------------------------------------------------
 constexpr int EX_THREADS = 256;
 constexpr int EX_T = 64;   // GEMM output tile (EX_T x EX_T), 4 x 4 per thread
 constexpr int EX_K = 16;   // GEMM K chunk
 constexpr int EX_TAYLOR = 18;
+constexpr int ETD_BLOCKS = 5;
 
 // C = alpha A B, n x n row-major in global memory (C distinct from A and B).
 __device__ void ex_gemm(int n, const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
@@ -77,7 +88,7 @@ __device__ void ex_gemm(int n, const double* __restrict__ A, const double* __res
 }
 
 // lin: the handle's L_l bands, [kind][col][band][l] with entry (row i, col c)
-// at band KL + i - c (k_build_lu).  scratch: 5 n^2 doubles per CTA.
+// at band KL + i - c (k_build_lu).  scratch: 6 n^2 doubles per CTA.
 __global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, const double* __restrict__ lin,
                                                           double dt, double* __restrict__ scratch,
                                                           double* __restrict__ tab, int* err) {
@@ -87,11 +98,13 @@ __global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, 
   const int g = blockIdx.y, l = blockIdx.x;
   const int nb = 2 * kl + 1;
   const size_t n2 = (size_t)n * n;
-  double* X = scratch + (size_t)(g * (L + 1) + l) * 5 * n2;
+  double* X = scratch + (size_t)(g * (L + 1) + l) * 6 * n2;
   double* Pw = X + n2;
   double* T = Pw + n2;
   double* E = T + n2;
   double* P = E + n2;
+  double* Q = P + n2;
+  double* out = tab + (size_t)(g * (L + 1) + l) * ETD_BLOCKS * n2;
   const double* Lb = lin + (size_t)g * n * nb * (L + 1) + l;
   const int tid = threadIdx.x;
   // X = dt A_l (dense)
@@ -101,7 +114,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, 
     X[e] = (b >= 0 && b < nb) ? dt * Lb[((size_t)c * nb + b) * (L + 1)] : 0.0;
   }
   __syncthreads();
-  // s from the 1-norm (largest column sum)
+  // s from the 1-norm (largest column sum), at least 1 for the half step
   double cmax = 0.0;
   for (int c = tid; c < n; c += EX_THREADS) {
     double sum = 0.0;
@@ -114,11 +127,12 @@ __global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, 
   if (tid == 0) {
     double v = 0.0;
     for (int w = 0; w < EX_THREADS / 32; ++w) v = fmax(v, red[w]);
-    int s = 0;
+    int s = 1;
     if (!(v < 1e300)) {  // not finite: flag and leave the table unusable
       atomicExch(err, 1);
       s = -1;
     } else {
+      v *= 0.5;
       while (v > 0.5 && s < 1000) {
         v *= 0.5;
         ++s;
@@ -130,7 +144,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, 
   const int s = s_sh;
   if (s < 0) return;
   const double sc = ldexp(1.0, -s);
-  // Y = X / 2^s (exact); E = I + Y, P = I + Y / 2, Pw = Y
+  // Y = X / 2^s (exact); E = I + Y, P = I + Y / 2, Q = I / 2 + Y / 6, Pw = Y
   for (size_t e = tid; e < n2; e += EX_THREADS) {
     const int i = (int)(e / n), c = (int)(e % n);
     const double y = X[e] * sc, id = i == c ? 1.0 : 0.0;
@@ -138,23 +152,34 @@ __global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, 
     Pw[e] = y;
     E[e] = id + y;
     P[e] = id + 0.5 * y;
+    Q[e] = 0.5 * id + y / 6.0;
   }
   __syncthreads();
   for (int k = 2; k <= EX_TAYLOR; ++k) {
     ex_gemm(n, Pw, X, T, 1.0 / k, sA, sB);  // T = Y^k / k!
-    const double rk1 = 1.0 / (k + 1);
+    const double rk1 = 1.0 / (k + 1), rk12 = 1.0 / ((double)(k + 1) * (k + 2));
     for (size_t e = tid; e < n2; e += EX_THREADS) {
       const double t = T[e];
       Pw[e] = t;
       E[e] += t;
       P[e] += t * rk1;
+      Q[e] += t * rk12;
     }
     __syncthreads();
   }
-  // doublings
+  // doublings; before the last one E and P are the half-step matrices
   for (int it = 0; it < s; ++it) {
+    if (it == s - 1) {
+      for (size_t e = tid; e < n2; e += EX_THREADS) {
+        const int i = (int)(e / n), c = (int)(e % n);
+        out[3 * n2 + (size_t)c * n + i] = E[e];
+        out[4 * n2 + (size_t)c * n + i] = P[e];
+      }
+    }
+    ex_gemm(n, P, P, T, 1.0, sA, sB);   // P^2
     for (size_t e = tid; e < n2; e += EX_THREADS) {
       const int i = (int)(e / n), c = (int)(e % n);
+      Q[e] = 0.25 * (2.0 * Q[e] + T[e]);   // Q(2Y) = (2 Q + P^2) / 4
       X[e] = E[e] + (i == c ? 1.0 : 0.0);  // E + I
     }
     __syncthreads();
@@ -166,16 +191,16 @@ __global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, 
     }
     __syncthreads();
   }
-  double* out = tab + (size_t)(g * (L + 1) + l) * 2 * n2;
   for (size_t e = tid; e < n2; e += EX_THREADS) {
     const int i = (int)(e / n), c = (int)(e % n);
     out[(size_t)c * n + i] = E[e];
     out[n2 + (size_t)c * n + i] = P[e];
+    out[2 * n2 + (size_t)c * n + i] = Q[e];
   }
 }
 
-size_t etd_table_doubles(const Dims& d) { return (size_t)3 * (d.L + 1) * 2 * d.nr * d.nr; }
-size_t etd_scratch_doubles(const Dims& d) { return (size_t)3 * (d.L + 1) * 5 * d.nr * d.nr; }
+size_t etd_table_doubles(const Dims& d) { return (size_t)3 * (d.L + 1) * ETD_BLOCKS * d.nr * d.nr; }
+size_t etd_scratch_doubles(const Dims& d) { return (size_t)3 * (d.L + 1) * 6 * d.nr * d.nr; }
 
 void launch_etd_build(cudaStream_t st, const Dims& d, const double* lin, double dt, double* scratch, double* tab,
                       int* err) {
@@ -183,15 +208,17 @@ void launch_etd_build(cudaStream_t st, const Dims& d, const double* lin, double 
 }
 
 // ---------------------------------------------------------------------------
-// Update.  CTA = (column chunk, l, field slot): the columns of order l are
-// (m, plane) for m = 0 .. min(l, M), 64 per CTA; every thread owns an 8-row x
-// 4-column tile of the output and the K loop runs over the stacked operand
-// [u ; dt w] (2n rows, w = 3/2 N - 1/2 N_prev) against the cached [E | phi1]
-// in chunks of 16 rows, double-buffered: asynchronous 8-byte copies of the
-// next chunk's matrix rows and gathered input columns (u, or N and N_prev,
-// combined into dt w once they land) are in flight while the current chunk is
-// multiplied.  The columns are read in full before the tile is written back
-// over u.  16 x ceil(nr / 8) threads: nr <= 256.
+// Applying the cache: out = M_top x_top + M_bot (c x_bot) per (field, l, m,
+// plane) column, M_top and M_bot blocks of the (kind, l) table, x_top = u and
+// x_bot = a, 3/2 a - 1/2 b or a - b (ExpApply); epilogue out = acc or
+// out = lin + dt (k1 + acc).  CTA = (column chunk, l, field slot): the columns
+// of order l are (m, plane) for m = 0 .. min(l, M), 64 per CTA; every thread
+// owns an 8-row x 4-column tile of the output and the K loop runs over the
+// stacked operand in chunks of 16 rows, double-buffered: asynchronous 8-byte
+// copies of the next chunk's matrix rows and gathered input columns are in
+// flight while the current chunk is multiplied (bottom inputs are combined
+// once they land).  The columns are read in full before the tile is written,
+// so out may be x_top.  16 x ceil(nr / 8) threads: nr <= 256.
 // ---------------------------------------------------------------------------
 constexpr int EU_COLS = 64;
 constexpr int EU_RT = 8;   // rows per thread
@@ -206,14 +233,14 @@ __device__ __forceinline__ void eu_copy8(double* s, const double* g) {
 // MAXT = the thread bound the build is compiled for: 288 (nr <= 144, two CTAs
 // per SM) or 512 (nr <= 256, one).
 template <int MAXT>
-__global__ void __launch_bounds__(MAXT, 576 / MAXT) k_eab2(Dims d, const int* __restrict__ moff,
-                                                          const double* __restrict__ tab, Cnab2Args a) {
+__global__ void __launch_bounds__(MAXT, 576 / MAXT) k_exp_apply(Dims d, const int* __restrict__ moff,
+                                                               const double* __restrict__ tab, ExpApply a) {
   extern __shared__ __align__(16) double eu_smem[];
   const int n = d.nr;
   const int npad = ((n + EU_RT - 1) / EU_RT) * EU_RT;
-  double* sM = eu_smem;                       // [2][EU_KC][npad]: rows k of the stacked [E | phi1]^T
-  double* sA = sM + 2 * EU_KC * npad;         // [2][EU_KC][EU_COLS]: u rows, or N rows then dt w
-  double* sB = sA + 2 * EU_KC * EU_COLS;      // [2][EU_KC][EU_COLS]: N_prev rows
+  double* sM = eu_smem;                       // [2][EU_KC][npad]: k-rows of the stacked matrix
+  double* sA = sM + 2 * EU_KC * npad;         // [2][EU_KC][EU_COLS]: input rows (x_top, or a then x_bot)
+  double* sB = sA + 2 * EU_KC * EU_COLS;      // [2][EU_KC][EU_COLS]: b rows
   __shared__ int colj[EU_COLS];               // column -> mode index j (-1 past the last column)
   __shared__ unsigned char colp[EU_COLS];
   const int slot = blockIdx.z;
@@ -223,7 +250,7 @@ __global__ void __launch_bounds__(MAXT, 576 / MAXT) k_eab2(Dims d, const int* __
   const int c0 = blockIdx.x * EU_COLS;
   if (c0 >= 2 * mcount) return;
   const int g = a.kind[slot];
-  const size_t NM = d.nlm, plane = (size_t)n * NM;
+  const size_t NM = d.nlm, plane = (size_t)n * NM, n2 = (size_t)n * n;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int tx = tid % (EU_COLS / EU_CT), ty = tid / (EU_COLS / EU_CT);
   for (int c = tid; c < EU_COLS; c += nt) {
@@ -238,11 +265,16 @@ __global__ void __launch_bounds__(MAXT, 576 / MAXT) k_eab2(Dims d, const int* __
     }
   }
   __syncthreads();
-  const double* M = tab + (size_t)(g * (d.L + 1) + l) * 2 * (size_t)n * n;
-  const double* __restrict__ u = a.u[slot];
-  const double* __restrict__ nl = a.nl[slot];
-  const double* __restrict__ pv = a.prev[slot];
-  const int nch = (2 * n + EU_KC - 1) / EU_KC;
+  const double* tl = tab + (size_t)(g * (d.L + 1) + l) * ETD_BLOCKS * n2;
+  const double* Mt = a.top_block >= 0 ? tl + a.top_block * n2 : nullptr;
+  const double* Mb = a.bot_block >= 0 ? tl + a.bot_block * n2 : nullptr;
+  const double* __restrict__ xt = a.top[slot];
+  const double* __restrict__ xa = a.bot_a[slot];
+  const double* __restrict__ xb = a.bot_b[slot];
+  const int ktop = Mt ? n : 0;
+  const int K = ktop + (Mb ? n : 0);
+  const bool two = a.bot_mode != 0;
+  const int nch = (K + EU_KC - 1) / EU_KC;
   auto issue = [&](int ch, int buf) {
     const int k0 = ch * EU_KC;
     double* m_ = sM + buf * EU_KC * npad;
@@ -250,21 +282,21 @@ __global__ void __launch_bounds__(MAXT, 576 / MAXT) k_eab2(Dims d, const int* __
     double* b_ = sB + buf * EU_KC * EU_COLS;
     for (int e = tid; e < EU_KC * npad; e += nt) {
       const int r = e / npad, i = e % npad, k = k0 + r;
-      if (k < 2 * n && i < n)
-        eu_copy8(m_ + e, M + (size_t)k * n + i);
+      if (k < K && i < n)
+        eu_copy8(m_ + e, (k < ktop ? Mt + (size_t)k * n : Mb + (size_t)(k - ktop) * n) + i);
       else
         m_[e] = 0.0;
     }
     for (int e = tid; e < EU_KC * EU_COLS; e += nt) {
       const int r = e / EU_COLS, c = e % EU_COLS, k = k0 + r;
       const int j = colj[c];
-      if (j >= 0 && k < 2 * n) {
-        const size_t at = (size_t)colp[c] * plane + (size_t)(k < n ? k : k - n) * NM + j;
-        if (k < n) {
-          eu_copy8(a_ + e, u + at);
+      if (j >= 0 && k < K) {
+        const size_t at = (size_t)colp[c] * plane + (size_t)(k < ktop ? k : k - ktop) * NM + j;
+        if (k < ktop) {
+          eu_copy8(a_ + e, xt + at);
         } else {
-          eu_copy8(a_ + e, nl + at);
-          eu_copy8(b_ + e, pv + at);
+          eu_copy8(a_ + e, xa + at);
+          if (two) eu_copy8(b_ + e, xb + at);
         }
       } else {
         a_[e] = 0.0;
@@ -290,12 +322,15 @@ __global__ void __launch_bounds__(MAXT, 576 / MAXT) k_eab2(Dims d, const int* __
     __syncthreads();
     const int k0 = ch * EU_KC;
     double* a_ = sA + buf * EU_KC * EU_COLS;
-    if (k0 + EU_KC > n) {
-      // rows of the N part: dt w = dt (3/2 N - 1/2 N_prev)
+    if (k0 + EU_KC > ktop) {
+      // bottom rows: c a, c (3/2 a - 1/2 b) or c (a - b)
       const double* b_ = sB + buf * EU_KC * EU_COLS;
       for (int e = tid; e < EU_KC * EU_COLS; e += nt) {
         const int k = k0 + e / EU_COLS;
-        if (k >= n && k < 2 * n) a_[e] = a.dt * (1.5 * a_[e] - 0.5 * b_[e]);
+        if (k >= ktop && k < K) {
+          const double v = a.bot_mode == 1 ? 1.5 * a_[e] - 0.5 * b_[e] : a.bot_mode == 2 ? a_[e] - b_[e] : a_[e];
+          a_[e] = a.bot_scale * v;
+        }
       }
       __syncthreads();
     }
@@ -324,7 +359,9 @@ __global__ void __launch_bounds__(MAXT, 576 / MAXT) k_eab2(Dims d, const int* __
     }
     __syncthreads();
   }
-  double* __restrict__ uo = a.u[slot];
+  double* __restrict__ uo = a.out[slot];
+  const double* __restrict__ lin = a.lin[slot];
+  const double* __restrict__ k1 = a.k1[slot];
 #pragma unroll
   for (int q = 0; q < EU_CT; ++q) {
     const int c = tx * EU_CT + q;
@@ -335,31 +372,34 @@ __global__ void __launch_bounds__(MAXT, 576 / MAXT) k_eab2(Dims d, const int* __
     for (int p = 0; p < EU_RT; ++p) {
       const int i = ty * EU_RT + p;
       if (i >= n) continue;
+      const size_t at = base + (size_t)i * NM;
+      double v = acc[p][q];
+      if (a.epilogue == 1) v = lin[at] + a.dt * (k1[at] + v);
       // bc_mode 1 zeroes the boundary rows after the update
       const bool clamp = a.clamp_rows && (i == 0 || i == n - 1);
-      uo[base + (size_t)i * NM] = clamp ? 0.0 : acc[p][q];
+      uo[at] = clamp ? 0.0 : v;
     }
   }
 }
 
-int eab2_threads(const Dims& d) { return (EU_COLS / EU_CT) * ((d.nr + EU_RT - 1) / EU_RT); }
+int exp_apply_threads(const Dims& d) { return (EU_COLS / EU_CT) * ((d.nr + EU_RT - 1) / EU_RT); }
 
-void launch_eab2(cudaStream_t st, const Dims& d, const int* moff, const double* tab, const Cnab2Args& a) {
+void launch_exp_apply(cudaStream_t st, const Dims& d, const int* moff, const double* tab, const ExpApply& a) {
   const int npad = ((d.nr + EU_RT - 1) / EU_RT) * EU_RT;
   const size_t smem = (size_t)2 * EU_KC * (npad + 2 * EU_COLS) * sizeof(double);
   static size_t attr = 0;
   if (attr < smem) {
-    cudaFuncSetAttribute(k_eab2<288>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_eab2<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_exp_apply<288>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_exp_apply<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = smem;
   }
   const int ncc = ceil_div(2 * (d.M + 1), EU_COLS);
   const dim3 grid(ncc, d.L + 1, a.nfield);
-  const int nt = eab2_threads(d);
+  const int nt = exp_apply_threads(d);
   if (nt <= 288)
-    k_eab2<288><<<grid, nt, smem, st>>>(d, moff, tab, a);
+    k_exp_apply<288><<<grid, nt, smem, st>>>(d, moff, tab, a);
   else
-    k_eab2<512><<<grid, nt, smem, st>>>(d, moff, tab, a);
+    k_exp_apply<512><<<grid, nt, smem, st>>>(d, moff, tab, a);
 }
 
 }  // namespace gd

@@ -48,7 +48,8 @@ struct gd_handle {
   double *d_stage_spec = nullptr, *d_stage_spec2 = nullptr, *d_stage_grid = nullptr, *d_stage_grid2 = nullptr;
   // time-stepping scheme and the EAB2 exponential cache (lazy)
   int scheme = 0;             // GD_SCHEME_*
-  double* d_etd = nullptr;    // [kind][l][2 nr][nr]: transposed [E | phi1]
+  double* d_etd = nullptr;    // [kind][l][5][nr][nr]: transposed E, phi1, phi2, E(dt/2), phi1(dt/2)
+  double* d_erk2 = nullptr;   // ERK2: linear and k1 terms of the five fields
   // mixed precision state (lazy)
   gd::MixedState* mixed = nullptr;
   // graphs (index: boot flag)

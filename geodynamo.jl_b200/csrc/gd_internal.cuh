@@ -132,7 +132,24 @@ size_t etd_table_doubles(const Dims& d);
 size_t etd_scratch_doubles(const Dims& d);
 void launch_etd_build(cudaStream_t s, const Dims& d, const double* lin, double dt, double* scratch, double* tab,
                       int* err);
-void launch_eab2(cudaStream_t s, const Dims& d, const int* moff, const double* tab, const Cnab2Args& a);
+// out = M_top x_top + M_bot (bot_scale * x_bot) per (field, l, m, plane) column (gd_eab2.cu)
+struct ExpApply {
+  const double* top[5];       // per slot: x_top (u), unused without top_block
+  const double* bot_a[5];     // per slot: a
+  const double* bot_b[5];     // per slot: b (bot_mode 1, 2)
+  double* out[5];             // may equal top
+  const double* lin[5];       // epilogue 1 operands
+  const double* k1[5];
+  int kind[5];
+  int nfield;
+  int top_block, bot_block;   // table blocks 0 E, 1 phi1, 2 phi2, 3 E(dt/2), 4 phi1(dt/2); -1: none
+  int bot_mode;               // x_bot = 0: a, 1: 3/2 a - 1/2 b, 2: a - b
+  double bot_scale;
+  int epilogue;               // 0: out = acc, 1: out = lin + dt (k1 + acc)
+  double dt;
+  int clamp_rows;             // bc_mode 1: zero rows 0 and nr-1 of out
+};
+void launch_exp_apply(cudaStream_t s, const Dims& d, const int* moff, const double* tab, const ExpApply& a);
 // ---- reverse mode (gd_adjoint.cu) ----
 void launch_cnab2_pullback(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,
                            int kind, double dt, double theta, int clamp_rows, int bc_rows, int nsteps, double* lam);

@@ -112,8 +112,8 @@ function step!(h::Handle, state; nsteps::Integer = 1)
     return state
 end
 
-# ts_scheme (src/simulation.jl:1176-1300): :cnab2 or :eab2 for the steps of h.
-const SCHEME = Dict(:cnab2 => 0, :eab2 => 1)
+# ts_scheme (src/simulation.jl:1054-1300): :cnab2, :eab2 or :erk2 for the steps of h.
+const SCHEME = Dict(:cnab2 => 0, :eab2 => 1, :erk2 => 2)
 set_scheme!(h::Handle, scheme::Symbol) =
     check(h, ccall((:gd_set_scheme, LIB), Cint, (Ptr{Cvoid}, Cint), h.ptr, SCHEME[scheme]))
 

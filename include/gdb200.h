@@ -55,9 +55,10 @@ enum {
 enum { GD_PREC_FP64 = 0, GD_PREC_MIXED = 1 };
 
 /* Time-stepping schemes of gd_step (the reference's ts_scheme,
- * src/simulation.jl:1176-1300): CNAB2 (build_rhs_cnab2! + solve_implicit_step!)
- * or EAB2 (eab2_update! with the exponential cache of create_etd_cache). */
-enum { GD_SCHEME_CNAB2 = 0, GD_SCHEME_EAB2 = 1 };
+ * src/simulation.jl:1054-1300): CNAB2 (build_rhs_cnab2! + solve_implicit_step!),
+ * EAB2 (eab2_update! with the exponential cache of create_etd_cache) or ERK2
+ * (erk2_integrate_full_step! with the cache of create_erk2_cache). */
+enum { GD_SCHEME_CNAB2 = 0, GD_SCHEME_EAB2 = 1, GD_SCHEME_ERK2 = 2 };
 
 /*
  * Model configuration.  Mirrors GeoDynamoParameters (src/parameters.jl:14-76):
@@ -169,19 +170,24 @@ int gd_step_async(gd_handle* h, int nsteps);
 /* Rebuild the implicit matrices (and, under EAB2, the exponential cache) for a
  * new time step (src/simulation.jl:335-337). */
 int gd_set_dt(gd_handle* h, double dt);
-/* Select the time-stepping scheme of gd_step: ts_scheme = :cnab2 or :eab2
- * (src/simulation.jl:1183-1300).  GD_SCHEME_EAB2 builds, per field kind and
- * degree l, E = exp(dt A_l) and phi1(dt A_l) (create_etd_cache,
- * src/timestep.jl:37-70, A_l the operator of the CNAB2 matrices) on the device
- * and replaces the banded solve by u <- E u + dt phi1 (3/2 N - 1/2 N_prev)
+/* Select the time-stepping scheme of gd_step: ts_scheme = :cnab2, :eab2 or
+ * :erk2 (src/simulation.jl:1054-1300).  The exponential schemes build, per
+ * field kind and degree l, E = exp(dt A_l), phi1(dt A_l), phi2(dt A_l) and E,
+ * phi1 at dt/2 (create_etd_cache / create_erk2_cache, src/timestep.jl:37-70,
+ * 896-968; A_l the operator of the CNAB2 matrices) on the device.  EAB2
+ * replaces the banded solve by u <- E u + dt phi1 (3/2 N - 1/2 N_prev)
  * (eab2_update!, :429-487; no AB1 start: the history starts as zeros, as
- * prev_nonlinear does).  GD_ERR_UNSUPPORTED with bc_mode 2 (the reference's
- * exponential scheme has no boundary rows) or nr > 256. */
+ * prev_nonlinear does); ERK2 by the staged update of erk2_integrate_full_step!
+ * (stage E(dt/2) u + dt/2 phi1(dt/2) N, the nonlinear terms of the stage,
+ * u <- E u + dt (phi1 N + phi2 (N_stage - N)), then the nonlinear terms of
+ * the new state).  GD_ERR_UNSUPPORTED with bc_mode 2 (the reference's
+ * exponential schemes have no boundary rows) or nr > 256. */
 int gd_set_scheme(gd_handle* h, int scheme);
-/* The exponential cache of field kind `kind` (0 velocity, 1 magnetic,
- * 2 temperature) at degree l: E and phi1 as nr x nr row-major matrices.
- * GD_ERR_ARG unless the scheme is GD_SCHEME_EAB2. */
-int gd_download_etd(gd_handle* h, int kind, int l, double* E, double* phi1);
+/* One matrix of the exponential cache of field kind `kind` (0 velocity,
+ * 1 magnetic, 2 temperature) at degree l, nr x nr row-major: which = 0 E,
+ * 1 phi1, 2 phi2, 3 E at dt/2, 4 phi1 at dt/2 (the ERK2Cache fields,
+ * src/timestep.jl:830-853).  GD_ERR_ARG under GD_SCHEME_CNAB2. */
+int gd_download_etd(gd_handle* h, int kind, int l, int which, double* out);
 /* compute_kinetic_energy / compute_magnetic_energy (src/velocity.jl:782-825,
  * src/magnetic.jl:504-543), both as 0.5 sum (T^2+P^2)/max(l(l+1),1). */
 int gd_energy(gd_handle* h, double* ekin, double* emag);

@@ -245,21 +245,23 @@ class Oracle:
     def step_count(self):
         return self.lib.oc_step_count(self.h)
 
-    # -- ts_scheme = :eab2 (test restatement) -----------------------------------
+    # -- ts_scheme = :eab2 / :erk2 (test restatement) ----------------------------
     def etd_cache(self, kind):
-        """create_etd_cache (src/timestep.jl:37-70) for a field kind (0 velocity,
-        1 magnetic, 2 temperature) at the configuration's dt: per degree l the
-        dense operator A_l (the L_l band of the implicit matrices,
-        src/timestep.jl:498-543), E_l = exp(dt A_l) and phi1_l = phi1(dt A_l).
-        exp is scipy.linalg.expm (scaling and squaring with Pade approximants,
-        Al-Mohy and Higham 2009; Julia's matrix exp follows Higham 2005).  phi1
-        is the top-right block of exp([[dt A, I], [0, 0]]), the same function
-        the reference forms as A^-1 (E - I) / dt; that solve loses accuracy
-        where A_l is nearly singular, as A_0 is (it maps a constant to ~0).
-        Returns (A, E, phi1), lists indexed by l."""
+        """create_etd_cache / create_erk2_cache (src/timestep.jl:37-70, 896-968)
+        for a field kind (0 velocity, 1 magnetic, 2 temperature) at the
+        configuration's dt: per degree l the dense operator A_l (the L_l band of
+        the implicit matrices, src/timestep.jl:498-543) and the matrices E, phi1,
+        phi2 of dt A_l and E, phi1 of dt A_l / 2.  exp is scipy.linalg.expm
+        (scaling and squaring with Pade approximants, Al-Mohy and Higham 2009;
+        Julia's matrix exp follows Higham 2005); phi1 and phi2 are the blocks of
+        exp([[X, I, 0], [0, 0, I], [0, 0, 0]]) (the same functions the reference
+        forms with A^-1, compute_phi1_function / compute_phi2_function; those
+        solves are unusable here: A_l has no boundary rows and the radial
+        equation's two homogeneous solutions leave it numerically singular).
+        Returns {"A", "E", "phi1", "phi2", "E_half", "phi1_half"}, lists by l."""
         from scipy.linalg import expm
         n, kl, dt = self.nr, self.kl, self.cfg.dt
-        A, E, P = [], [], []
+        out = {k: [] for k in ("A", "E", "phi1", "phi2", "E_half", "phi1_half")}
         for l in range(self.lmax + 1):
             lin, _ = self.implicit_matrices(kind, l)   # band rows kl + i - c, columns c
             a = np.zeros((n, n))
@@ -268,14 +270,28 @@ class Oracle:
                     i = c + b - kl
                     if 0 <= i < n:
                         a[i, c] = lin[b, c]
-            big = np.zeros((2 * n, 2 * n))
-            big[:n, :n] = dt * a
-            big[:n, n:] = np.eye(n)
-            ex = expm(big)
-            A.append(a)
-            E.append(ex[:n, :n].copy())
-            P.append(ex[:n, n:].copy())
-        return A, E, P
+            out["A"].append(a)
+            for h, suffix in ((dt, ""), (0.5 * dt, "_half")):
+                big = np.zeros((3 * n, 3 * n))
+                big[:n, :n] = h * a
+                big[:n, n:2 * n] = np.eye(n)
+                big[n:2 * n, 2 * n:] = np.eye(n)
+                ex = expm(big)
+                out["E" + suffix].append(ex[:n, :n].copy())
+                out["phi1" + suffix].append(ex[:n, n:2 * n].copy())
+                if not suffix:
+                    out["phi2"].append(ex[:n, 2 * n:].copy())
+        return out
+
+    def _per_l(self, mats, x):
+        lv = np.array([p[0] for p in lm_pairs(self.lmax, self.mmax)])
+        y = np.empty_like(x)
+        for l in range(self.lmax + 1):
+            cols = lv == l
+            y[:, cols] = mats[l] @ x[:, cols]
+        return y
+
+    FIELD_KINDS = (("u_tor", 0), ("u_pol", 0), ("b_tor", 1), ("b_pol", 1), ("temp", 2))
 
     def eab2_step(self, caches, history):
         """One step of step_once! under ts_scheme = :eab2: the three nonlinear
@@ -288,19 +304,49 @@ class Oracle:
         self.temperature_nl()
         self.velocity_nl()
         self.magnetic_nl()
-        lv = np.array([p[0] for p in lm_pairs(self.lmax, self.mmax)])
-        for name, kind in (("u_tor", 0), ("u_pol", 0), ("b_tor", 1), ("b_pol", 1), ("temp", 2)):
-            _, E, P = caches[kind]
+        for name, kind in self.FIELD_KINDS:
+            c = caches[kind]
             re, im = self.get_field(name)
             nre, nim = self.get_nl(name)
             pre, pim = history.get(name, (np.zeros_like(re), np.zeros_like(im)))
-            out = []
-            for u, nn, pp in ((re, nre, pre), (im, nim, pim)):
-                w = 1.5 * nn - 0.5 * pp
-                v = np.empty_like(u)
-                for l in range(self.lmax + 1):
-                    cols = lv == l
-                    v[:, cols] = E[l] @ u[:, cols] + dt * (P[l] @ w[:, cols])
-                out.append(v)
+            out = [self._per_l(c["E"], u) + dt * self._per_l(c["phi1"], 1.5 * nn - 0.5 * pp)
+                   for u, nn, pp in ((re, nre, pre), (im, nim, pim))]
             self.set_field(name, *out)
             history[name] = (nre, nim)
+
+    def _all_nonlinear(self):
+        # compute_all_nonlinear_terms! (src/simulation.jl:800-813): velocity, magnetic, temperature
+        self.velocity_nl()
+        self.magnetic_nl()
+        self.temperature_nl()
+
+    def erk2_step(self, caches):
+        """One step of step_once! under ts_scheme = :erk2: the three nonlinear
+        phases, then erk2_integrate_full_step! (src/simulation.jl:1054-1149):
+        erk2_prepare_field! (linear = E u, k1 = phi1 N, stage = E_h u + dt/2
+        phi1_h N), the stage applied, compute_all_nonlinear_terms!,
+        erk2_finalize_field! (u = linear + dt (k1 + phi2 (N_stage - N))) and a
+        last compute_all_nonlinear_terms! at the new state
+        (src/timestep.jl:1316-1557)."""
+        dt = self.cfg.dt
+        self.temperature_nl()
+        self.velocity_nl()
+        self.magnetic_nl()
+        saved = {}
+        for name, kind in self.FIELD_KINDS:
+            c = caches[kind]
+            u = self.get_field(name)
+            nn = self.get_nl(name)
+            lin = [self._per_l(c["E"], x) for x in u]
+            k1 = [self._per_l(c["phi1"], x) for x in nn]
+            stage = [self._per_l(c["E_half"], x) + 0.5 * dt * self._per_l(c["phi1_half"], y) for x, y in zip(u, nn)]
+            saved[name] = (lin, k1, nn)
+            self.set_field(name, *stage)
+        self._all_nonlinear()
+        for name, kind in self.FIELD_KINDS:
+            c = caches[kind]
+            lin, k1, nn = saved[name]
+            ns = self.get_nl(name)
+            out = [li + dt * (ki + self._per_l(c["phi2"], s_ - n_)) for li, ki, s_, n_ in zip(lin, k1, ns, nn)]
+            self.set_field(name, *out)
+        self._all_nonlinear()
