@@ -27,6 +27,9 @@ CONFIGS = {
     # workload at a quarter of its memory (profiling captures)
     "shell_l255_nr33": dict(lmax=255, nlat=384, nlon=768, nr=33, dt=2e-6, steps=100),
     "shell_l127_nr65": dict(lmax=127, nlat=192, nlon=384, nr=65, dt=5e-6, steps=100),
+    # the headline's radial grid at lmax 127: the radial kernels' launch shape
+    # of the headline workload at a quarter of its memory (profiling captures)
+    "shell_l127_nr129": dict(lmax=127, nlat=192, nlon=384, nr=129, dt=2e-6, steps=100),
     # adjoint configuration: the reference's literal boundaries (bc_mode 0; any
     # Dirichlet row on B would pin B_pol(ro) and the misfit to constants),
     # started from adjoint_state (temperature zero)
