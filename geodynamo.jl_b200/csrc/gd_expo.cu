@@ -1,4 +1,4 @@
-// gd_eab2.cu -- the exponential time schemes of apply_master_implicit_step!
+// gd_expo.cu -- the exponential time schemes of apply_master_implicit_step!
 // (ts_scheme = :eab2 and :erk2, src/simulation.jl:1054-1300) with the dense
 // per-l caches of create_etd_cache (src/timestep.jl:37-70) and
 // create_erk2_cache (:896-968).  Per radial system (field, l, m):

@@ -127,12 +127,12 @@ struct Cnab2Args {
   double inv_dt, lin_weight;
   double dt;                  // EAB2: the time step applied to the phi1 term
 };
-// ---- exponential Adams-Bashforth 2 (gd_eab2.cu) ----
+// ---- exponential Adams-Bashforth 2 (gd_expo.cu) ----
 size_t etd_table_doubles(const Dims& d);
 size_t etd_scratch_doubles(const Dims& d);
 void launch_etd_build(cudaStream_t s, const Dims& d, const double* lin, double dt, double* scratch, double* tab,
                       int* err);
-// out = M_top x_top + M_bot (bot_scale * x_bot) per (field, l, m, plane) column (gd_eab2.cu)
+// out = M_top x_top + M_bot (bot_scale * x_bot) per (field, l, m, plane) column (gd_expo.cu)
 struct ExpApply {
   const double* top[5];       // per slot: x_top (u), unused without top_block
   const double* bot_a[5];     // per slot: a
