@@ -382,6 +382,177 @@ __global__ void __launch_bounds__(MAXT, 576 / MAXT) k_exp_apply(Dims d, const in
   }
 }
 
+// The same contraction on the FP64 tensor cores (mma.sync m8n8k4, nr <= 144):
+// 8 warps; warp (h, cp) owns row tiles h * TC_RTH .. + TC_RTH - 1 (8 rows each)
+// and column tiles 2 cp, 2 cp + 1 (8 columns each) of the CTA's npad x 64
+// output.  Fragments (lane = 4 g + t): A[g][t] = matrix row k = 4 s + t, column
+// i = 8 tile + g; B[t][g] = input row k, column 8 tile + g; the accumulators
+// hold C[g][2 t], C[g][2 t + 1].  Shared rows are strided by 4 mod 16 doubles,
+// so the fragment loads are free of bank conflicts.
+constexpr int TC_RTH = 9;              // row tiles per warp half: npad <= 144
+constexpr int TC_THREADS = 256;
+__host__ __device__ constexpr int tc_stride(int w) { return w + ((4 - w) % 16 + 16) % 16; }
+constexpr int TC_SX = tc_stride(EU_COLS);  // 68
+
+__device__ __forceinline__ void exp_dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 2) k_exp_apply_tc(Dims d, const int* __restrict__ moff,
+                                                                const double* __restrict__ tab, ExpApply a) {
+  extern __shared__ __align__(16) double eu_smem[];
+  const int n = d.nr;
+  const int npad = ((n + EU_RT - 1) / EU_RT) * EU_RT;
+  const int SM = tc_stride(npad);
+  double* sM = eu_smem;                       // [2][EU_KC][SM]
+  double* sA = sM + 2 * EU_KC * SM;           // [2][EU_KC][TC_SX]
+  double* sB = sA + 2 * EU_KC * TC_SX;        // [2][EU_KC][TC_SX]
+  __shared__ int colj[EU_COLS];
+  __shared__ unsigned char colp[EU_COLS];
+  const int slot = blockIdx.z;
+  if (slot >= a.nfield) return;
+  const int l = d.L - (int)blockIdx.y;
+  const int mcount = min(l, d.M) + 1;
+  const int c0 = blockIdx.x * EU_COLS;
+  if (c0 >= 2 * mcount) return;
+  const int g = a.kind[slot];
+  const size_t NM = d.nlm, plane = (size_t)n * NM, n2 = (size_t)n * n;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int fg = lane >> 2, ft = lane & 3;
+  const int wh = warp >> 2, wc = warp & 3;   // row half, column pair
+  for (int c = tid; c < EU_COLS; c += TC_THREADS) {
+    const int cc = c0 + c;
+    if (cc < 2 * mcount) {
+      const int m = cc >> 1;
+      colj[c] = moff[m] + l - m;
+      colp[c] = (unsigned char)(cc & 1);
+    } else {
+      colj[c] = -1;
+      colp[c] = 0;
+    }
+  }
+  __syncthreads();
+  const double* tl = tab + (size_t)(g * (d.L + 1) + l) * ETD_BLOCKS * n2;
+  const double* Mt = a.top_block >= 0 ? tl + a.top_block * n2 : nullptr;
+  const double* Mb = a.bot_block >= 0 ? tl + a.bot_block * n2 : nullptr;
+  const double* __restrict__ xt = a.top[slot];
+  const double* __restrict__ xa = a.bot_a[slot];
+  const double* __restrict__ xb = a.bot_b[slot];
+  const int ktop = Mt ? n : 0;
+  const int K = ktop + (Mb ? n : 0);
+  const bool two = a.bot_mode != 0;
+  const int nch = (K + EU_KC - 1) / EU_KC;
+  auto issue = [&](int ch, int buf) {
+    const int k0 = ch * EU_KC;
+    double* m_ = sM + buf * EU_KC * SM;
+    double* a_ = sA + buf * EU_KC * TC_SX;
+    double* b_ = sB + buf * EU_KC * TC_SX;
+    if (tid < npad) {  // thread tid copies matrix column tid of the chunk's rows
+      for (int r = 0; r < EU_KC; ++r) {
+        const int k = k0 + r;
+        double* dst = m_ + r * SM + tid;
+        if (k < K && tid < n)
+          eu_copy8(dst, (k < ktop ? Mt + (size_t)k * n : Mb + (size_t)(k - ktop) * n) + tid);
+        else
+          *dst = 0.0;
+      }
+    }
+    for (int e = tid; e < EU_KC * EU_COLS; e += TC_THREADS) {
+      const int r = e >> 6, c = e & (EU_COLS - 1), k = k0 + r;
+      const int j = colj[c];
+      double* da = a_ + r * TC_SX + c;
+      double* db = b_ + r * TC_SX + c;
+      if (j >= 0 && k < K) {
+        const size_t at = (size_t)colp[c] * plane + (size_t)(k < ktop ? k : k - ktop) * NM + j;
+        if (k < ktop) {
+          eu_copy8(da, xt + at);
+        } else {
+          eu_copy8(da, xa + at);
+          if (two) eu_copy8(db, xb + at);
+        }
+      } else {
+        *da = 0.0;
+        *db = 0.0;
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  double acc[TC_RTH][2][2];
+#pragma unroll
+  for (int i = 0; i < TC_RTH; ++i)
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj) acc[i][jj][0] = acc[i][jj][1] = 0.0;
+  const int rt0 = wh * TC_RTH;          // first row tile of this warp
+  const int nrt = npad / 8;             // row tiles of the CTA
+  issue(0, 0);
+  for (int ch = 0; ch < nch; ++ch) {
+    const int buf = ch & 1;
+    if (ch + 1 < nch) {
+      issue(ch + 1, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    const int k0 = ch * EU_KC;
+    double* a_ = sA + buf * EU_KC * TC_SX;
+    if (k0 + EU_KC > ktop) {
+      const double* b_ = sB + buf * EU_KC * TC_SX;
+      for (int e = tid; e < EU_KC * EU_COLS; e += TC_THREADS) {
+        const int r = e >> 6, c = e & (EU_COLS - 1), k = k0 + r;
+        if (k >= ktop && k < K) {
+          const int o = r * TC_SX + c;
+          const double v = a.bot_mode == 1 ? 1.5 * a_[o] - 0.5 * b_[o] : a.bot_mode == 2 ? a_[o] - b_[o] : a_[o];
+          a_[o] = a.bot_scale * v;
+        }
+      }
+      __syncthreads();
+    }
+    const double* m_ = sM + buf * EU_KC * SM;
+#pragma unroll
+    for (int ks = 0; ks < EU_KC / 4; ++ks) {
+      const int r = 4 * ks + ft;
+      double bf[2];
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj) bf[jj] = a_[r * TC_SX + (2 * wc + jj) * 8 + fg];
+#pragma unroll
+      for (int i = 0; i < TC_RTH; ++i) {
+        if (rt0 + i < nrt) {
+          const double af = m_[r * SM + (rt0 + i) * 8 + fg];
+          exp_dmma(acc[i][0][0], acc[i][0][1], af, bf[0]);
+          exp_dmma(acc[i][1][0], acc[i][1][1], af, bf[1]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  double* __restrict__ uo = a.out[slot];
+  const double* __restrict__ lin = a.lin[slot];
+  const double* __restrict__ k1 = a.k1[slot];
+#pragma unroll
+  for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = (2 * wc + jj) * 8 + 2 * ft + h;
+      const int j = colj[c];
+      if (j < 0) continue;
+      const size_t base = (size_t)colp[c] * plane + j;
+#pragma unroll
+      for (int i = 0; i < TC_RTH; ++i) {
+        const int row = (rt0 + i) * 8 + fg;
+        if (rt0 + i >= nrt || row >= n) continue;
+        const size_t at = base + (size_t)row * NM;
+        double v = acc[i][jj][h];
+        if (a.epilogue == 1) v = lin[at] + a.dt * (k1[at] + v);
+        // bc_mode 1 zeroes the boundary rows after the update
+        const bool clamp = a.clamp_rows && (row == 0 || row == n - 1);
+        uo[at] = clamp ? 0.0 : v;
+      }
+    }
+}
+
 int exp_apply_threads(const Dims& d) { return (EU_COLS / EU_CT) * ((d.nr + EU_RT - 1) / EU_RT); }
 
 void launch_exp_apply(cudaStream_t st, const Dims& d, const int* moff, const double* tab, const ExpApply& a) {
@@ -395,6 +566,16 @@ void launch_exp_apply(cudaStream_t st, const Dims& d, const int* moff, const dou
   }
   const int ncc = ceil_div(2 * (d.M + 1), EU_COLS);
   const dim3 grid(ncc, d.L + 1, a.nfield);
+  if (npad <= 2 * TC_RTH * 8) {
+    const size_t tsmem = (size_t)2 * EU_KC * (tc_stride(npad) + 2 * TC_SX) * sizeof(double);
+    static size_t tattr = 0;
+    if (tattr < tsmem) {
+      cudaFuncSetAttribute(k_exp_apply_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+      tattr = tsmem;
+    }
+    k_exp_apply_tc<<<grid, TC_THREADS, tsmem, st>>>(d, moff, tab, a);
+    return;
+  }
   const int nt = exp_apply_threads(d);
   if (nt <= 288)
     k_exp_apply<288><<<grid, nt, smem, st>>>(d, moff, tab, a);

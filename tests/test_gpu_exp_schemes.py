@@ -93,6 +93,26 @@ def test_erk2_steps_match_oracle(gdb, oracle_mod, precision, tol):
         assert rel(a[0], b[0]) < max(tol, 1e-10), k
 
 
+def test_eab2_cuda_core_apply_matches_oracle(gdb, oracle_mod):
+    # nr = 160 > 144 takes the CUDA-core apply kernel instead of the FP64
+    # tensor-core one (two steps: a zero history, then the rolled one); 1e-9 as
+    # for the cache at this size (||dt A||_1 ~ 1000)
+    g = gdb.SHTnsKitConfig(7, 12, 24, 160, dt=1e-6)
+    g.set_scheme("eab2")
+    o = oracle_mod.Oracle(lmax=7, nlat=12, nlon=24, nr=160, dt=1e-6)
+    for k, (a, b) in workloads.seeded_state(7, 7, 160, seed=12).items():
+        g.set_field(k, a, b)
+        o.set_field(k, a, b)
+    caches = [o.etd_cache(kind) for kind in range(3)]
+    history = {}
+    for n in range(2):
+        g.step(1)
+        o.eab2_step(caches, history)
+        for k in NAMES:
+            a, b = g.get_field(k), o.get_field(k)
+            assert rel(a[0], b[0]) < 1e-9 and rel(a[1], b[1]) < 1e-9, (n, k)
+
+
 @pytest.mark.parametrize("scheme", ["eab2", "erk2"])
 def test_exponential_graph_replay_and_scheme_switch(gdb, scheme):
     st = workloads.seeded_state(15, 15, 12, seed=10)
