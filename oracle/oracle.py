@@ -105,6 +105,25 @@ def lm_pairs(lmax: int, mmax: int):
     return [(l, m) for l in range(lmax + 1) for m in range(min(l, mmax) + 1)]
 
 
+# -- the exponential schemes' per-system updates (test restatements) -------------
+def eab2_update(E, phi1, u, n, n_prev, dt):
+    """eab2_update! (src/timestep.jl:429-487) for one system: u (nr, k) columns,
+    n and n_prev their nonlinear terms: E u + dt phi1 (3/2 N - 1/2 N_prev)."""
+    return E @ u + dt * (phi1 @ (1.5 * n - 0.5 * n_prev))
+
+
+def erk2_prepare(E, phi1, E_half, phi1_half, u, n, dt):
+    """erk2_prepare_field! (src/timestep.jl:1316-1431) for one system:
+    (linear, k1, stage) = (E u, phi1 N, E_h u + dt/2 phi1_h N)."""
+    return E @ u, phi1 @ n, E_half @ u + 0.5 * dt * (phi1_half @ n)
+
+
+def erk2_finalize(phi2, linear, k1, n, n_stage, dt):
+    """erk2_finalize_field! (src/timestep.jl:1449-1557) for one system:
+    linear + dt (k1 + phi2 (N_stage - N))."""
+    return linear + dt * (k1 + phi2 @ (n_stage - n))
+
+
 class Oracle:
     """One oracle instance: grid, tables, radial operators and a model state."""
 
@@ -283,13 +302,20 @@ class Oracle:
                     out["phi2"].append(ex[:n, 2 * n:].copy())
         return out
 
-    def _per_l(self, mats, x):
+    def _per_l(self, fn, *xs):
+        """fn(l, *column blocks of xs) applied per degree l; returns the
+        reassembled arrays (one, or a tuple)."""
         lv = np.array([p[0] for p in lm_pairs(self.lmax, self.mmax)])
-        y = np.empty_like(x)
+        outs = None
         for l in range(self.lmax + 1):
             cols = lv == l
-            y[:, cols] = mats[l] @ x[:, cols]
-        return y
+            r = fn(l, *[x[:, cols] for x in xs])
+            r = r if isinstance(r, tuple) else (r,)
+            if outs is None:
+                outs = [np.empty((xs[0].shape[0], xs[0].shape[1])) for _ in r]
+            for o, v in zip(outs, r):
+                o[:, cols] = v
+        return outs[0] if len(outs) == 1 else tuple(outs)
 
     FIELD_KINDS = (("u_tor", 0), ("u_pol", 0), ("b_tor", 1), ("b_pol", 1), ("temp", 2))
 
@@ -309,7 +335,7 @@ class Oracle:
             re, im = self.get_field(name)
             nre, nim = self.get_nl(name)
             pre, pim = history.get(name, (np.zeros_like(re), np.zeros_like(im)))
-            out = [self._per_l(c["E"], u) + dt * self._per_l(c["phi1"], 1.5 * nn - 0.5 * pp)
+            out = [self._per_l(lambda l, u_, n_, p_: eab2_update(c["E"][l], c["phi1"][l], u_, n_, p_, dt), u, nn, pp)
                    for u, nn, pp in ((re, nre, pre), (im, nim, pim))]
             self.set_field(name, *out)
             history[name] = (nre, nim)
@@ -337,16 +363,18 @@ class Oracle:
             c = caches[kind]
             u = self.get_field(name)
             nn = self.get_nl(name)
-            lin = [self._per_l(c["E"], x) for x in u]
-            k1 = [self._per_l(c["phi1"], x) for x in nn]
-            stage = [self._per_l(c["E_half"], x) + 0.5 * dt * self._per_l(c["phi1_half"], y) for x, y in zip(u, nn)]
-            saved[name] = (lin, k1, nn)
-            self.set_field(name, *stage)
+            prep = [self._per_l(lambda l, u_, n_: erk2_prepare(c["E"][l], c["phi1"][l], c["E_half"][l],
+                                                               c["phi1_half"][l], u_, n_, dt), x, y)
+                    for x, y in zip(u, nn)]
+            saved[name] = ([p[0] for p in prep], [p[1] for p in prep], nn)
+            self.set_field(name, *[p[2] for p in prep])
         self._all_nonlinear()
         for name, kind in self.FIELD_KINDS:
             c = caches[kind]
             lin, k1, nn = saved[name]
             ns = self.get_nl(name)
-            out = [li + dt * (ki + self._per_l(c["phi2"], s_ - n_)) for li, ki, s_, n_ in zip(lin, k1, ns, nn)]
+            out = [self._per_l(lambda l, li_, ki_, n_, s_: erk2_finalize(c["phi2"][l], li_, ki_, n_, s_, dt),
+                               li, ki, n_, s_)
+                   for li, ki, n_, s_ in zip(lin, k1, nn, ns)]
             self.set_field(name, *out)
         self._all_nonlinear()
