@@ -245,8 +245,10 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    steps = max(1, min(args.steps, 3))
-    warm = 1
+    # a bounded sample: at most 5 timed and 5 warm-up steps of the nr = 9
+    # shell sample (about 0.3-0.4 s each on the GPU box's host cores)
+    steps = max(1, min(args.steps, 5))
+    warm = max(3, min(args.warmup, 5))
     rate, dt_sample, cores = cpu_reference_rate(steps, warm)
     sample = (f"oracle (C++ FP64 restatement of step_once!) at lmax=255 nlat=384 nlon=768 on nr={CPU_SAMPLE_NR} "
               f"of 129 shells, {steps} timed steps after {warm} warm-up, {dt_sample:.3f} s per sample step, "
