@@ -225,19 +225,32 @@ __global__ void __launch_bounds__(256) k_synth_coef_image(Dims d, const int* __r
   float* h0 = a.bimg + (base + synth_step_of(0, kc, nc1)) * (2L * BT);
   float* h1 = kc < nc1 ? a.bimg + (base + synth_step_of(1, kc, nc1)) * (2L * BT) : nullptr;
   const int l0 = m + 2 * (TC_K * kc + lane);
-  for (int row = warp; row < NCS; row += 8) {
-    if (!mine[row]) continue;  // written by the field's producer kernel
-    const double* src = colp[row];
-    const double v0 = (src != nullptr && l0 <= L) ? src[l0] : 0.0;
-    const double v1 = (src != nullptr && l0 + 1 <= L) ? src[l0 + 1] : 0.0;
-    const uint32_t o = sw128_offset(row, lane) >> 2;
-    const float f0 = __double2float_rn(v0), g0 = tf32_rn(f0);
-    h0[o] = g0;
-    h0[BT + o] = tf32_rn(f0 - g0);
-    if (h1 != nullptr) {
-      const float f1 = __double2float_rn(v1), g1 = tf32_rn(f1);
-      h1[o] = g1;
-      h1[BT + o] = tf32_rn(f1 - g1);
+  // rows in batches of four per warp, every load of a batch issued before its stores
+  constexpr int RB = 4;
+  for (int row0 = warp; row0 < NCS; row0 += 8 * RB) {
+    double v0[RB], v1[RB];
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int row = row0 + 8 * u;
+      const double* src = row < NCS ? colp[row] : nullptr;
+      v0[u] = (src != nullptr && l0 <= L) ? src[l0] : 0.0;
+      v1[u] = (src != nullptr && l0 + 1 <= L) ? src[l0 + 1] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int row = row0 + 8 * u;
+      // rows of other fields are written by their producer kernels
+      if (row < NCS && mine[row]) {
+        const uint32_t o = sw128_offset(row, lane) >> 2;
+        const float f0 = __double2float_rn(v0[u]), g0 = tf32_rn(f0);
+        h0[o] = g0;
+        h0[BT + o] = tf32_rn(f0 - g0);
+        if (h1 != nullptr) {
+          const float f1 = __double2float_rn(v1[u]), g1 = tf32_rn(f1);
+          h1[o] = g1;
+          h1[BT + o] = tf32_rn(f1 - g1);
+        }
+      }
     }
   }
 }
