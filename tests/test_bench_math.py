@@ -47,3 +47,13 @@ def test_exponential_scheme_flops(headline):
     assert bench.kernel_work("eab2_update", p, nlm, "mixed")["flops"] == cols * n * 2 * n * 2
     assert bench.kernel_work("erk2_prepare", p, nlm, "mixed")["flops"] == cols * n * 4 * n * 2
     assert bench.kernel_work("erk2_finalize", p, nlm, "mixed")["flops"] == cols * n * n * 2
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    # under torchrun only rank 0 runs and prints the reference arm's line
+    import subprocess
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                        "--warmup", "3"], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0
+    assert r.stdout.strip() == ""
