@@ -57,3 +57,44 @@ def test_eab2_constant_forcing():
     got = float(eab2_update(E, P1, np.array([[u0]]), np.array([[c]]), np.array([[c]]), DT)[0, 0])
     expected = math.exp(-LAM * DT) * u0 + (1 - math.exp(-LAM * DT)) * c / LAM
     assert abs(got - expected) < 1e-14
+
+
+def taylor_doubling(X, K=18):
+    """The device's construction of the exponential cache (k_etd_build,
+    geodynamo.jl_b200/csrc/gd_expo.cu), restated in numpy: Y = X / 2^s with
+    ||Y||_1 <= 1/2 and s >= 1, truncated Taylor series of exp, phi1, phi2, then s
+    doublings E <- E^2, P <- P (E + I) / 2, Q <- (2 Q + P^2) / 4; the half-step
+    matrices are the state before the last doubling."""
+    n = X.shape[0]
+    eye = np.eye(n)
+    s, v = 1, np.max(np.sum(np.abs(X), axis=0)) / 2
+    while v > 0.5:
+        v /= 2
+        s += 1
+    Y = X / 2.0 ** s
+    E, P, Q, Pw = eye + Y, eye + Y / 2, eye / 2 + Y / 6, Y.copy()
+    for k in range(2, K + 1):
+        Pw = Pw @ Y / k
+        E, P, Q = E + Pw, P + Pw / (k + 1), Q + Pw / ((k + 1) * (k + 2))
+    half = None
+    for it in range(s):
+        if it == s - 1:
+            half = (E.copy(), P.copy())
+        Q = (2 * Q + P @ P) / 4
+        P = P @ (E + eye) / 2
+        E = E @ E
+    return E, P, Q, half[0], half[1]
+
+
+def test_device_cache_algorithm_matches_expm(oracle_mod):
+    # at nr = 12 (||dt A||_1 ~ 0.3) and at the headline radial grid (nr = 129,
+    # dt = 2e-6, ||dt A||_1 ~ 900): the tolerances the GPU tests hold the
+    # device's cache to
+    for nr, dt, tol in ((12, 1e-5, 1e-12), (129, 2e-6, 1e-9)):
+        o = oracle_mod.Oracle(lmax=3, nlat=6, nlon=12, nr=nr, dt=dt)
+        ref = o.etd_cache(2)
+        for l in (0, 3):
+            E, P, Q, Eh, Ph = taylor_doubling(dt * ref["A"][l])
+            for got, key in ((E, "E"), (P, "phi1"), (Q, "phi2"), (Eh, "E_half"), (Ph, "phi1_half")):
+                want = ref[key][l]
+                assert np.max(np.abs(got - want)) / np.max(np.abs(want)) < tol, (nr, l, key)
