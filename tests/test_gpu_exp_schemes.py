@@ -93,6 +93,29 @@ def test_erk2_steps_match_oracle(gdb, oracle_mod, precision, tol):
         assert rel(a[0], b[0]) < max(tol, 1e-10), k
 
 
+@pytest.mark.parametrize("scheme", ["eab2", "erk2"])
+def test_exponential_schemes_with_mmax_below_lmax(gdb, oracle_mod, scheme):
+    # a degree l > mmax has mmax + 1 orders, not l + 1: the column blocks of
+    # the apply kernel and the oracle's per-degree blocks must agree
+    g = gdb.SHTnsKitConfig(12, 20, 40, 10, mmax=6)
+    g.set_scheme(scheme)
+    o = oracle_mod.Oracle(lmax=12, nlat=20, nlon=40, nr=10, mmax=6)
+    for k, (a, b) in workloads.seeded_state(12, 6, 10, seed=13).items():
+        g.set_field(k, a, b)
+        o.set_field(k, a, b)
+    caches = [o.etd_cache(kind) for kind in range(3)]
+    history = {}
+    for n in range(2):
+        g.step(1)
+        if scheme == "eab2":
+            o.eab2_step(caches, history)
+        else:
+            o.erk2_step(caches)
+        for k in NAMES:
+            a, b = g.get_field(k), o.get_field(k)
+            assert rel(a[0], b[0]) < 1e-11 and rel(a[1], b[1]) < 1e-11, (n, k)
+
+
 def test_eab2_cuda_core_apply_matches_oracle(gdb, oracle_mod):
     # nr = 160 > 144 takes the CUDA-core apply kernel instead of the FP64
     # tensor-core one (two steps: a zero history, then the rolled one); 1e-9 as
