@@ -14,6 +14,15 @@ Arms:
                      129 shells, scaled by 129/9; every kernel of the step is
                      linear in the shell count).
 
+Other measurements (one JSON line each, instead of the headline):
+  --transforms       the transform-only batch (lmax 127, 97 shells x 9 fields):
+                     errors against the oracle and device times, FP64 and mixed
+  --adjoint          the adjoint configuration's gradient against FP64 finite
+                     differences and the oracle's forward mode, with timings
+  --ensemble N       the batched uneven ensemble of N shells
+  --scheme S         the headline step under ts_scheme = S (cnab2, eab2, erk2)
+  --workload W       a smaller named shell for profiling captures
+
 Multi-GPU (torchrun): the step does not shard without a transpose, so every
 rank runs an independent replica of the same workload ("replicas only", weak
 scaling); value = N x steps / max-over-ranks time.
