@@ -10,9 +10,9 @@ velocity and magnetic nonlinear terms (4 scalar + 4 vector syntheses, 1 scalar
 Arms:
   default            this package through its C ABI (libgdb200.so)
   --impl reference   the FP64 CPU restatement of the reference step (oracle/),
-                     timed on the host cores on a bounded sample (nr = 9 of the
-                     129 shells, scaled by 129/9; every kernel of the step is
-                     linear in the shell count).
+                     timed on the host cores at the full headline size
+                     (lmax 255, nr 129): 1 warm-up and up to 5 timed steps on
+                     all cores, and 1 timed step on one thread.
 
 Other measurements (one JSON line each, instead of the headline):
   --transforms       the transform-only batch (lmax 127, 97 shells x 9 fields):
@@ -44,7 +44,6 @@ sys.path.insert(0, os.path.join(ROOT, "geodynamo.jl_b200"))
 
 METRIC = "CNAB2 steps/s lmax255 nr129: mixed-prec vs FP64 GPU at 1e-9 energy err"
 WORKLOAD = "shell_l255_nr129"
-CPU_SAMPLE_NR = 9
 
 
 def load_package():
@@ -77,6 +76,8 @@ def kernel_work(name, p, nlm, precision):
     products); bytes are the coefficients, the Fourier components and the
     table (images) each read or written once."""
     L, nlat, nlon, nr = p["lmax"], p["nlat"], p["nlon"], p["nr"]
+    if name.endswith("_fp64"):
+        precision = "fp64"                    # an FP64 stage (also inside the mixed step)
     nth = nlat // 2
     G = nlat * nlon * nr                      # grid points per field
     F = nr * (L + 1) * nlat                   # Fourier coefficients per component
@@ -109,6 +110,10 @@ def kernel_work(name, p, nlm, precision):
         "nl_temperature": 6 * G * rb,
         "nl_velocity": 10 * G * rb,
         "nl_induction": 6 * G * rb,
+        "nl_coriolis": 4 * G * rb,
+        # FP64 <-> blocked FP32 Fourier components (2) and the folded-transform widening (2)
+        "fourier_convert": 2 * F * (16 + 8),
+        "fold_convert": 2 * F * (8 + 16 + 16),
         # per field: read u, N, N_prev, write u (the history roll is a bank switch)
         "cnab2_solve": 5 * 4 * S * 8,
         # the same arrays plus the exponential cache (3 kinds x (L+1) x [E | phi1])
@@ -232,11 +237,13 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------------
 def cpu_reference_rate(steps, warmup, threads=None):
-    """Oracle steps/s at lmax=255 (sample of nr = 9 shells, scaled to 129)."""
+    """Oracle steps/s on the workload's full grid (every shell), timed on the
+    host cores: `warmup` untimed steps, then `steps` timed ones; threads None =
+    all cores.  Returns (steps/s, seconds per step, threads used)."""
     from oracle.oracle import Oracle
     import workloads
     p = workload_params()
-    nr = CPU_SAMPLE_NR
+    nr = p["nr"]
     o = Oracle(lmax=p["lmax"], nlat=p["nlat"], nlon=p["nlon"], nr=nr, dt=p["dt"], threads=threads)
     for k, (a, b) in workloads.seeded_state(p["lmax"], p["lmax"], nr, seed=0).items():
         o.set_field(k, a, b)
@@ -246,27 +253,31 @@ def cpu_reference_rate(steps, warmup, threads=None):
     for _ in range(steps):
         o.step(1)
     dt = (time.perf_counter() - t0) / steps
-    full = dt * p["nr"] / nr
-    return 1.0 / full, dt, os.cpu_count() if threads is None else threads
+    del o
+    return 1.0 / dt, dt, os.cpu_count() if threads is None else threads
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    # a bounded sample: at most 5 timed and 5 warm-up steps of the nr = 9
-    # shell sample (about 0.3-0.4 s each on the GPU box's host cores)
+    # the full headline size (about 5 s per step on 16 host cores, about a
+    # minute on one): 1 warm-up and at most 5 timed steps on all cores, then 1
+    # timed step on one thread
+    p = workload_params()
     steps = max(1, min(args.steps, 5))
-    warm = max(3, min(args.warmup, 5))
-    rate, dt_sample, cores = cpu_reference_rate(steps, warm)
-    sample = (f"oracle (C++ FP64 restatement of step_once!) at lmax=255 nlat=384 nlon=768 on nr={CPU_SAMPLE_NR} "
-              f"of 129 shells, {steps} timed steps after {warm} warm-up, {dt_sample:.3f} s per sample step, "
-              f"scaled by 129/{CPU_SAMPLE_NR}")
+    warm = 1
+    rate, dt_all, cores = cpu_reference_rate(steps, warm)
+    rate1, dt_one, _ = cpu_reference_rate(1, 0, threads=1)
+    sample = (f"oracle (C++ FP64 restatement of step_once!) at the full {WORKLOAD} grid (lmax={p['lmax']} "
+              f"nlat={p['nlat']} nlon={p['nlon']} nr={p['nr']}): {steps} timed steps after {warm} warm-up on "
+              f"{cores} threads ({dt_all:.2f} s per step); 1 thread: 1 timed step ({dt_one:.1f} s)")
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "steps/s", "n_gpus": args.gpus,
             "steps": steps, "warmup": warm, "ms_per_step": 1e3 / rate, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, default_rng(0))",
-            "config": {"workload": WORKLOAD, "lmax": 255, "nlat": 384, "nlon": 768, "nr": 129},
-            "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "config": {"workload": WORKLOAD, "lmax": p["lmax"], "nlat": p["nlat"], "nlon": p["nlon"], "nr": p["nr"]},
+            "cpu_baseline": {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port", "sample": sample,
+                             "one_thread": {"value": rate1, "unit": "steps/s", "cores": 1}},
             "e2e": {"value": rate, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -463,13 +474,90 @@ def run_adjoint(args, gdb, workloads, torch):
     return 0
 
 
+def run_accuracy_study(args, gdb, workloads, torch):
+    """The headline condition's error budget at the headline workload: kinetic
+    and magnetic energy relative errors after 100 and 1000 steps of
+    (1) the FP64 step started from the seeded state perturbed by one ulp in
+        every coefficient, against the unperturbed FP64 step (the floor any
+        implementation meets), under the literal operator (bc_mode 0) and with
+        Dirichlet rows (bc_mode 2);
+    (2) the mixed step with no stage, each single stage and all stages of the
+        velocity chain returned to FP64 (gd_set_fp64_stages), against the FP64
+        step, with each configuration's device time per step."""
+    p = workload_params()
+    st = workloads.seeded_state(p["lmax"], p["lmax"], p["nr"], seed=0)
+    marks = (100, args.accuracy_steps)
+
+    def make(prec, bc, state):
+        g = gdb.SHTnsKitConfig(p["lmax"], p["nlat"], p["nlon"], p["nr"], dt=p["dt"], rratio=p["rratio"],
+                               ekman=p["ekman"], rayleigh=p["rayleigh"], prandtl=p["prandtl"],
+                               magnetic_prandtl=p["magnetic_prandtl"], implicit_theta=p["implicit_theta"],
+                               bc_mode=bc, precision=prec)
+        for k, (a, b) in state.items():
+            g.set_field(k, a, b)
+        return g
+
+    def trajectory(g):
+        out, done = [], 0
+        for m in marks:
+            g.step(m - done)
+            done = m
+            out.append(g.energy())
+        return out
+
+    def rel_err(x, y):
+        return {f"{n}_rel_err_{m}": abs(a[i] - b[i]) / abs(b[i])
+                for i, n in enumerate(("ekin", "emag")) for m, a, b in zip(marks, x, y)}
+
+    def ms_per_step(g, n=10):
+        ext = torch.cuda.ExternalStream(g.stream_ptr())
+        g.step(3)
+        g.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext); g.step_async(n); e1.record(ext); e1.synchronize(); g.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    pert = {k: (np.nextafter(a, np.inf), np.nextafter(b, np.inf)) for k, (a, b) in st.items()}
+    res = {"steps": list(marks), "floor": {}, "budget": {}}
+    for bc in (0, 2):
+        g = make("fp64", bc, st)
+        ref = trajectory(g)
+        if bc == 2:
+            res["fp64_ms_per_step"] = ms_per_step(g)
+        g.close()
+        g = make("fp64", bc, pert)
+        res["floor"][f"bc{bc}"] = rel_err(trajectory(g), ref)
+        g.close()
+        rows = ([(), ("vel_synth",), ("vel_products",), ("vel_analysis",), ("vel_synth", "vel_products", "vel_analysis")]
+                if bc == 2 else [(), ("vel_synth", "vel_products", "vel_analysis")])
+        for stages in rows:
+            g = make("mixed", bc, st)
+            g.set_fp64_stages(stages)
+            row = rel_err(trajectory(g), ref)
+            if bc == 2:
+                row["ms_per_step"] = ms_per_step(g)
+            res["budget"][f"bc{bc}:" + ("+".join(stages) or "none")] = row
+            g.close()
+    line = {"metric": "energy error budget of the mixed step (relative to the FP64 step)", "value": None,
+            "unit": "relative error", "n_gpus": 1, "higher_is_better": False,
+            "data": "synthetic (seeded default_rng(0) state, amplitude 1e-3 (l+1)^-2)",
+            "config": {"workload": WORKLOAD, "lmax": p["lmax"], "nlat": p["nlat"], "nlon": p["nlon"], "nr": p["nr"],
+                       "dt": p["dt"]}, **res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed", "mixed_vel64"],
+                    help="auto: mixed_vel64 (the mixed step with its velocity chain in FP64, the configuration "
+                         "that meets the energy condition) when the device has tcgen05, else fp64")
+    ap.add_argument("--accuracy-study", action="store_true",
+                    help="instead of the headline: the FP64 one-ulp floor and the per-stage error budget")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the FP64 vs mixed energy comparison (0 = skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -505,6 +593,8 @@ def main():
         return run_adjoint(args, gdb, workloads, torch)
     if args.transforms:
         return run_transforms(args, gdb, workloads, torch)
+    if args.accuracy_study:
+        return run_accuracy_study(args, gdb, workloads, torch)
     dist = None
     if world > 1:
         import datetime
@@ -518,8 +608,8 @@ def main():
                                ekman=p["ekman"], rayleigh=p["rayleigh"], prandtl=p["prandtl"],
                                magnetic_prandtl=p["magnetic_prandtl"], implicit_theta=p["implicit_theta"],
                                bc_mode=bc_mode, precision="fp64", device=local)
-        if precision == "mixed":
-            g.set_precision("mixed")
+        if precision != "fp64":
+            g.set_precision(precision)
         if args.scheme != "cnab2" and bc_mode != 2:
             g.set_scheme(args.scheme)
         for k, (a, b) in st.items():
@@ -532,7 +622,7 @@ def main():
             probe = gdb.SHTnsKitConfig(7, 12, 24, 9, device=local)
             probe.set_precision("mixed")
             probe.close()
-            precision = "mixed"
+            precision = "mixed_vel64"
         except gdb.GeoDynamoError:
             precision = "fp64"
 
@@ -583,7 +673,10 @@ def main():
             ent = {"name": name, "share": None, "launches_per_step": cnt / nprof, "ms_per_launch": per}
             if name.startswith("fft_"):
                 # 4-component synth launches and 2-component ones share a name; use the per-step mix
-                ncomp = (4 + 2 * 4) if "synth" in name else (1 + 2 + 2)
+                if prec == "fp64":
+                    ncomp = (4 + 2 * 4) if "synth" in name else (1 + 2 + 2)
+                else:  # the FP64 velocity stages of the mixed step: u (synthesis), its products (analysis)
+                    ncomp = 2
                 ent["gbs"] = fft_bytes(p, ncomp, prec) / (ms / nprof / 1e3) / 1e9
             elif w is not None:
                 if w["flops"] is not None:
@@ -632,7 +725,7 @@ def main():
     # ---- FP64 reference step on the GPU (denominator of the metric) ----
     fp64_value = None
     k64 = kernels
-    if precision == "mixed":
+    if precision != "fp64":
         g64 = make("fp64")
         g64.step(args.warmup)
         ms64 = timed_steps(g64, args.steps, 0)
@@ -656,19 +749,36 @@ def main():
     # bc_mode 0 is the reference's operator as written (no boundary rows; its
     # temperature grows without bound at nr = 129, dt = 2e-6 in FP64 too);
     # bc_mode 2 adds Dirichlet rows to the implicit operator.
+    # the fast mixed step (every stage in mixed precision) beside the headline
+    # configuration, when the headline is the one with its velocity chain in FP64
+    variants = {}
+    if precision == "mixed_vel64":
+        gf = make("mixed")
+        gf.step(args.warmup)
+        msf = timed_steps(gf, args.steps, 0)
+        variants["mixed"] = {"value": world * args.steps / (msf / 1e3), "unit": "steps/s",
+                             "ms_per_step": msf / args.steps,
+                             "ratio_vs_fp64_gpu": world * args.steps / (msf / 1e3) / fp64_value,
+                             "what": "every transform and product in split-TF32 / FP32"}
+        gf.close()
     accuracy = None
-    if precision == "mixed" and args.accuracy_steps > 0:
+    if precision != "fp64" and args.accuracy_steps > 0:
         accuracy = {"steps": args.accuracy_steps, "target_rel_err": 1e-9}
         for label, bc in (("literal_bc0", 0), ("dirichlet_bc2", 2)):
-            ga = make("mixed", bc)
             gb = make("fp64", bc)
-            ga.step(args.accuracy_steps)
             gb.step(args.accuracy_steps)
-            ea, eb = ga.energy(), gb.energy()
-            accuracy[label] = {"ekin_rel_err": abs(ea[0] - eb[0]) / abs(eb[0]),
-                               "emag_rel_err": abs(ea[1] - eb[1]) / abs(eb[1]),
-                               "ekin_fp64": eb[0], "emag_fp64": eb[1]}
-            ga.close(); gb.close()
+            eb = gb.energy()
+            gb.close()
+            accuracy[label] = {"ekin_fp64": eb[0], "emag_fp64": eb[1]}
+            for v in [precision] + list(variants):
+                ga = make(v, bc)
+                ga.step(args.accuracy_steps)
+                ea = ga.energy()
+                ga.close()
+                accuracy[label][v] = {"ekin_rel_err": abs(ea[0] - eb[0]) / abs(eb[0]),
+                                      "emag_rel_err": abs(ea[1] - eb[1]) / abs(eb[1])}
+        for v in variants:
+            variants[v]["accuracy_dirichlet_bc2"] = accuracy["dirichlet_bc2"][v]
 
     # ---- end to end through the C ABI with host buffers ----
     names = list(workloads.FIELD_ORDER)
@@ -709,20 +819,24 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, dts, cores = cpu_reference_rate(1, 1)
         cpu = {"value": rate, "unit": "steps/s", "cores": cores, "kind": "port",
-               "sample": f"oracle at lmax=255 nlat=384 nlon=768 nr={CPU_SAMPLE_NR} (of 129 shells), 1 timed step "
-                         f"after 1 warm-up ({dts:.3f} s), scaled by 129/{CPU_SAMPLE_NR}"}
+               "sample": f"oracle at the full {WORKLOAD} grid (lmax={p['lmax']} nlat={p['nlat']} nlon={p['nlon']} "
+                         f"nr={p['nr']}), 1 timed step after 1 warm-up on {cores} threads ({dts:.2f} s); the "
+                         f"one-thread figure is in the reference arm's line"}
 
     gpu_launches = sum(int(round(cnt / nprof)) for _, cnt in prof.values()) * args.steps
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32/tf32x3 (FP64 solves)",
+                "vs_baseline": None,
+                "dtype": {"fp64": "f64", "mixed": "f32/tf32x3 (FP64 solves)",
+                          "mixed_vel64": "f32/tf32x3, velocity chain f64 (FP64 solves)"}[precision],
                 "data": "synthetic (seeded default_rng(0) state, amplitude 1e-3 (l+1)^-2)",
                 "config": {"workload": WORKLOAD, "lmax": p["lmax"], "nlat": p["nlat"], "nlon": p["nlon"], "nr": p["nr"],
                            "dt": p["dt"], "precision": precision, "parallelism": f"replicas x{world}",
                            "l2": "working set 5+ GB of grids per step, larger than L2; no flush"},
                 "fp64_gpu_value": fp64_value, "ratio_vs_fp64_gpu": value / fp64_value if fp64_value else None,
-                "fp64_denominator": fp64_den,
+                "fp64_denominator": fp64_den, "variants": variants,
+                "fp64_kernels": k64 if precision != "fp64" else None,
                 "accuracy": accuracy, "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk}
         print(json.dumps(line), flush=True)

@@ -48,13 +48,19 @@ GRIDS = {
     "ind_th": 15, "ind_ph": 16,
 }
 PRECISIONS = {"fp64": 0, "mixed": 1}
+# Stages of the mixed-precision step that can run in FP64 (GD_STAGE_*): the
+# chain the velocity, and so the kinetic energy, depends on.
+FP64_STAGES = {"vel_synth": 1, "vel_products": 2, "vel_analysis": 4}
+# Named precision settings: the mixed step with its velocity chain in FP64.
+PRECISION_PRESETS = {"mixed_vel64": ("mixed", ("vel_synth", "vel_products", "vel_analysis"))}
 SCHEMES = {"cnab2": 0, "eab2": 1, "erk2": 2}   # ts_scheme (src/simulation.jl:1054-1300)
 ETD_MATRICES = ("E", "phi1", "phi2", "E_half", "phi1_half")   # ERK2Cache fields (src/timestep.jl:830-853)
 KINDS = {"velocity": 0, "magnetic": 1, "temperature": 2}
 
 # Every symbol include/gdb200.h declares.
 EXPORTS = (
-    "gd_create", "gd_destroy", "gd_last_error", "gd_info", "gd_grid", "gd_set_precision", "gd_synchronize",
+    "gd_create", "gd_destroy", "gd_last_error", "gd_info", "gd_grid", "gd_set_precision", "gd_set_fp64_stages",
+    "gd_synchronize",
     "gd_upload_spectral", "gd_download_spectral", "gd_download_nonlinear", "gd_download_grid",
     "gd_set_temperature_bc", "gd_spectral_to_physical", "gd_physical_to_spectral", "gd_vector_synthesis",
     "gd_vector_analysis", "gd_temperature_nonlinear", "gd_velocity_nonlinear", "gd_magnetic_nonlinear",
@@ -62,6 +68,9 @@ EXPORTS = (
     "gd_energy", "gd_check_finite",
     "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
     "gd_spectral_to_physical_noalloc",
+    "gd_compute_temperature_nonlinear", "gd_compute_velocity_nonlinear", "gd_compute_magnetic_nonlinear",
+    "gd_create_timestepping_matrices", "gd_destroy_timestepping_matrices", "gd_build_rhs_cnab2",
+    "gd_solve_implicit_step",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
     "gd_ensemble_step", "gd_ensemble_step_async", "gd_ensemble_failed_member", "gd_ensemble_get_stream",
@@ -122,6 +131,7 @@ def load_library():
         "gd_info": ([P, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_size_t)], I),
         "gd_grid": ([P, D, D, D], I),
         "gd_set_precision": ([P, I], I),
+        "gd_set_fp64_stages": ([P, I], I),
         "gd_synchronize": ([P], I),
         "gd_upload_spectral": ([P, I, D, D], I),
         "gd_download_spectral": ([P, I, D, D], I),
@@ -149,6 +159,14 @@ def load_library():
         "gd_profile_read": ([P, I, ctypes.c_char_p, D, ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "gd_spectral_to_physical_noalloc": ([P, I, ctypes.c_void_p, ctypes.c_void_p], I),
         "gd_spectral_to_physical_adjoint": ([P, I, D, D, D], I),
+        "gd_compute_temperature_nonlinear": ([P, D, D, D, D, D, D, D], I),
+        "gd_compute_velocity_nonlinear": ([P] + [D] * 14, I),
+        "gd_compute_magnetic_nonlinear": ([P] + [D] * 14, I),
+        "gd_create_timestepping_matrices": ([P, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.POINTER(P)], I),
+        "gd_destroy_timestepping_matrices": ([P], I),
+        "gd_build_rhs_cnab2": ([P, P, ctypes.c_double] + [D] * 8, I),
+        "gd_solve_implicit_step": ([P, P, D, D, D, D], I),
         "gd_magnetic_pullback": ([P, I, I, D, D, D, D], I),
         "gd_ensemble_create": ([ctypes.POINTER(GDConfig), I, I, ctypes.POINTER(P)], I),
         "gd_ensemble_destroy": ([P], I),
@@ -215,14 +233,18 @@ class SHTnsKitConfig:
                  fd_mode=0, precision="fp64", magnetic=1, device=0):
         self.lib = load_library()
         mmax = lmax if mmax is None else mmax
+        base, stages = PRECISION_PRESETS.get(precision, (precision, ()))
         self.cfg = GDConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl, magnetic_prandtl,
-                            dt, implicit_theta, ab_mode, bc_mode, fd_mode, PRECISIONS[precision], magnetic)
+                            dt, implicit_theta, ab_mode, bc_mode, fd_mode, PRECISIONS[base], magnetic)
         h = ctypes.c_void_p()
         st = self.lib.gd_create(ctypes.byref(self.cfg), int(device), ctypes.byref(h))
         if st != GD_OK:
             raise GeoDynamoError(st, "gd_create failed (see stderr)")
         self._owned = True
-        self._attach(h, precision)
+        self._attach(h, base)
+        if stages:
+            self.set_fp64_stages(stages)
+            self.precision = precision
 
     @classmethod
     def _member(cls, lib, h, cfg: GDConfig):
@@ -251,6 +273,7 @@ class SHTnsKitConfig:
         self.theta_grid, self.gauss_weights, self.r = th, w, r
         self.phi_grid = 2 * np.pi * np.arange(nlon) / nlon
         self.precision = precision
+        self.fp64_stages = 0
         self.scheme = "cnab2"
 
     # -- plumbing -------------------------------------------------------------
@@ -277,8 +300,18 @@ class SHTnsKitConfig:
         return b.value
 
     def set_precision(self, precision):
-        self._check(self.lib.gd_set_precision(self.h, PRECISIONS[precision]))
+        """"fp64", "mixed", or a preset of PRECISION_PRESETS ("mixed_vel64":
+        the mixed step with its velocity chain in FP64)."""
+        base, stages = PRECISION_PRESETS.get(precision, (precision, ()))
+        self._check(self.lib.gd_set_precision(self.h, PRECISIONS[base]))
+        self.set_fp64_stages(stages)
         self.precision = precision
+
+    def set_fp64_stages(self, stages):
+        """Stages of the mixed step to run in FP64: names of FP64_STAGES or an int mask."""
+        mask = stages if isinstance(stages, int) else sum(FP64_STAGES[n] for n in stages)
+        self._check(self.lib.gd_set_fp64_stages(self.h, int(mask)))
+        self.fp64_stages = mask
 
     def spec_shape(self):
         return (self.nr, self.nlm)
@@ -331,6 +364,38 @@ class SHTnsKitConfig:
         return out
 
     # -- model state ------------------------------------------------------------
+    # -- the reference's nonlinear functions on host arrays (FP64 kernels) ------------
+    def compute_temperature_nonlinear_arrays(self, t_re, t_im, u_theta, u_phi):
+        """compute_temperature_nonlinear! (src/thermal.jl:149-190): returns the
+        temperature with its Dirichlet rows applied, the nonlinear term and the
+        temperature grid."""
+        tr, ti = _f64(t_re).copy(), _f64(t_im).copy()
+        nre = np.zeros(self.spec_shape()); nim = np.zeros(self.spec_shape()); tg = np.zeros(self.grid_shape())
+        self._check(self.lib.gd_compute_temperature_nonlinear(self.h, _dptr(tr), _dptr(ti), _dptr(_f64(u_theta)),
+                                                              _dptr(_f64(u_phi)), _dptr(nre), _dptr(nim), _dptr(tg)))
+        return (tr, ti), (nre, nim), tg
+
+    def compute_velocity_nonlinear_arrays(self, tor, pol, j_theta=None, j_phi=None, b_theta=None, b_phi=None):
+        """compute_velocity_nonlinear! (src/velocity.jl:312-332): nonlinear terms
+        (tor, pol) and the velocity grids (u_theta, u_phi)."""
+        out = [np.zeros(self.spec_shape()) for _ in range(4)]
+        ut = np.zeros(self.grid_shape()); up = np.zeros(self.grid_shape())
+        g = [None if x is None else _dptr(_f64(x)) for x in (j_theta, j_phi, b_theta, b_phi)]
+        self._check(self.lib.gd_compute_velocity_nonlinear(
+            self.h, _dptr(_f64(tor[0])), _dptr(_f64(tor[1])), _dptr(_f64(pol[0])), _dptr(_f64(pol[1])), *g,
+            *[_dptr(o) for o in out], _dptr(ut), _dptr(up)))
+        return (out[0], out[1]), (out[2], out[3]), (ut, up)
+
+    def compute_magnetic_nonlinear_arrays(self, tor, pol, u_theta, u_phi):
+        """compute_magnetic_nonlinear! (src/magnetic.jl:131-159): nonlinear terms
+        (tor, pol) and the grids (b_theta, b_phi, j_theta, j_phi)."""
+        out = [np.zeros(self.spec_shape()) for _ in range(4)]
+        grids = [np.zeros(self.grid_shape()) for _ in range(4)]
+        self._check(self.lib.gd_compute_magnetic_nonlinear(
+            self.h, _dptr(_f64(tor[0])), _dptr(_f64(tor[1])), _dptr(_f64(pol[0])), _dptr(_f64(pol[1])),
+            _dptr(_f64(u_theta)), _dptr(_f64(u_phi)), *[_dptr(o) for o in out], *[_dptr(g) for g in grids]))
+        return (out[0], out[1]), (out[2], out[3]), tuple(grids)
+
     def set_field(self, name, re, im):
         self._check(self.lib.gd_upload_spectral(self.h, FIELDS[name], _dptr(_f64(re)), _dptr(_f64(im))))
 
@@ -429,6 +494,47 @@ class SHTnsKitConfig:
             nm = names.raw[32 * k: 32 * k + 32].split(b"\0", 1)[0].decode()
             out[nm] = (float(ms[k]), int(cnt[k]))
         return out
+
+
+class SHTnsImplicitMatrices:
+    """create_shtns_timestepping_matrices(config, domain, diffusivity, dt; theta)
+    (src/timestep.jl:489-543): per degree l the diffusivity-scaled radial
+    operator L_l and the banded LU of I/dt - theta L_l, on the model's device
+    (gd_create_timestepping_matrices)."""
+
+    def __init__(self, model: "SHTnsKitConfig", diffusivity, dt, theta=0.5):
+        self.model, self.diffusivity, self.dt, self.theta = model, float(diffusivity), float(dt), float(theta)
+        m = ctypes.c_void_p()
+        model._check(model.lib.gd_create_timestepping_matrices(model.h, self.diffusivity, self.dt, self.theta,
+                                                                ctypes.byref(m)))
+        self.m = m
+
+    def build_rhs_cnab2(self, un, nl, nl_prev, dt):
+        """build_rhs_cnab2! (src/timestep.jl:610-690) on (re, im) plane pairs."""
+        g = self.model
+        rr = np.zeros(g.spec_shape()); ri = np.zeros(g.spec_shape())
+        args = [_dptr(_f64(x)) for pair in (un, nl, nl_prev) for x in pair]
+        g._check(g.lib.gd_build_rhs_cnab2(g.h, self.m, float(dt), *args, _dptr(rr), _dptr(ri)))
+        return rr, ri
+
+    def solve_implicit_step(self, rhs):
+        """solve_implicit_step! (src/timestep.jl:692-730) on an (re, im) plane pair."""
+        g = self.model
+        sr = np.zeros(g.spec_shape()); si = np.zeros(g.spec_shape())
+        g._check(g.lib.gd_solve_implicit_step(g.h, self.m, _dptr(_f64(rhs[0])), _dptr(_f64(rhs[1])), _dptr(sr),
+                                              _dptr(si)))
+        return sr, si
+
+    def close(self):
+        if getattr(self, "m", None) and getattr(self.model, "h", None):
+            self.model.lib.gd_destroy_timestepping_matrices(self.m)
+        self.m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def radial_field_outer(model, pol_re, pol_im):
@@ -686,6 +792,25 @@ def apply_master_implicit_step(state: SimulationState, dt=None):
 def step_once(state: SimulationState):
     """``step_once!`` (scripts/bench_timestepping.jl:6-18) as one graph replay."""
     state.config.step(1)
+
+
+def create_shtns_timestepping_matrices(config: SHTnsKitConfig, diffusivity, dt, theta=0.5):
+    """create_shtns_timestepping_matrices (src/timestep.jl:498-543)."""
+    return SHTnsImplicitMatrices(config, diffusivity, dt, theta)
+
+
+def build_rhs_cnab2(rhs: SHTnsSpectralField, un: SHTnsSpectralField, nl: SHTnsSpectralField,
+                    nl_prev: SHTnsSpectralField, dt, matrices: SHTnsImplicitMatrices):
+    """build_rhs_cnab2! (src/timestep.jl:610-690): fills rhs in place."""
+    rhs.data_real[...], rhs.data_imag[...] = matrices.build_rhs_cnab2(
+        (un.data_real, un.data_imag), (nl.data_real, nl.data_imag), (nl_prev.data_real, nl_prev.data_imag), dt)
+    return rhs
+
+
+def solve_implicit_step(solution: SHTnsSpectralField, rhs: SHTnsSpectralField, matrices: SHTnsImplicitMatrices):
+    """solve_implicit_step! (src/timestep.jl:692-730): fills solution in place."""
+    solution.data_real[...], solution.data_imag[...] = matrices.solve_implicit_step((rhs.data_real, rhs.data_imag))
+    return solution
 
 
 def compute_kinetic_energy(state: SimulationState):

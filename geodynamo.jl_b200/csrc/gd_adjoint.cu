@@ -106,11 +106,7 @@ __global__ void __launch_bounds__(PB_THREADS) k_cnab2_pullback(Dims d, const int
 void launch_cnab2_pullback(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,
                            int kind, double dt, double theta, int clamp_rows, int bc_rows, int nsteps, double* lam) {
   const size_t smem = (size_t)d.nr * PB_THREADS * sizeof(double);
-  static size_t attr = 0;
-  if (attr < smem) {
-    cudaFuncSetAttribute(k_cnab2_pullback<GD_MAX_KL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = smem;
-  }
+  allow_dynamic_smem(k_cnab2_pullback<GD_MAX_KL>, smem);
   dim3 grid(ceil_div(d.nlm, PB_THREADS), 2);
   k_cnab2_pullback<GD_MAX_KL><<<grid, PB_THREADS, smem, s>>>(d, lof, lin, lu, kind, 1.0 / dt, 1.0 - theta, clamp_rows,
                                                              bc_rows, nsteps, lam);

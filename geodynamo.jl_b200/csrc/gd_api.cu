@@ -560,6 +560,15 @@ int gd_set_precision(gd_handle* h, int mode) {
   return GD_OK;
 }
 
+int gd_set_fp64_stages(gd_handle* h, int mask) {
+  if (!h) return GD_ERR_ARG;
+  if (mask < 0 || (mask & ~GD_STAGE_VEL_ALL)) return fail(h, GD_ERR_ARG, "unknown stage in the FP64 stage mask");
+  CK(cudaSetDevice(h->device));
+  if (mask != h->fp64_stages) drop_graphs(h);
+  h->fp64_stages = mask;
+  return GD_OK;
+}
+
 int gd_synchronize(gd_handle* h) {
   if (!h) return GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
@@ -791,6 +800,192 @@ int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi,
     CK(cudaMemcpyAsync(dst[i], h->d_stage_spec + plane * i, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return check_launch(h, "vector analysis");
+}
+
+// ---- the reference's argument lists on host arrays ----
+namespace {
+// host spectral planes (l-major) -> native layout at dst (through the l-major staging buffer)
+int put_spec(gd_handle* h, const double* re, const double* im, double* dst) {
+  const size_t plane = (size_t)h->d.nr * h->d.nlm;
+  CK(cudaMemcpyAsync(h->d_stage_spec, re, plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_stage_spec + plane, im, plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_lmajor_to_native(h->stream, h->d, h->d_perm, h->d_stage_spec, dst, 2);
+  return check_launch(h, "upload");
+}
+// host grid (reference layout) -> native grid at dst
+int put_grid(gd_handle* h, const double* g, double* dst) {
+  CK(cudaMemcpyAsync(h->d_stage_grid, g, h->grid_elems() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  launch_grid_to_native(h->stream, h->d, h->d_stage_grid, dst, 1);
+  return check_launch(h, "grid upload");
+}
+int get_grid(gd_handle* h, const double* src, double* g) {
+  launch_grid_to_reference(h->stream, h->d, src, h->d_stage_grid, 1);
+  CK(cudaMemcpyAsync(g, h->d_stage_grid, h->grid_elems() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "grid download");
+}
+int nl_prepare(gd_handle* h) {
+  CK(cudaSetDevice(h->device));
+  return stage_alloc(h);
+}
+}  // namespace
+
+struct gd_matrices {
+  gd_handle* h = nullptr;
+  double diffusivity = 0.0, dt = 0.0, theta = 0.0;
+  double* d_nu = nullptr;   // the diffusivity
+  double* d_lin = nullptr;  // L_l bands [col][band][l]
+  double* d_lu = nullptr;   // LU factors of I/dt - theta L_l, same layout
+};
+
+int gd_create_timestepping_matrices(gd_handle* h, double diffusivity, double dt, double theta, gd_matrices** out) {
+  if (!h || !out) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (!(dt > 0.0) || !std::isfinite(diffusivity) || !std::isfinite(theta))
+    return fail(h, GD_ERR_ARG, "need dt > 0 and finite diffusivity and theta");
+  CK(cudaSetDevice(h->device));
+  const Dims& d = h->d;
+  const size_t n = (size_t)d.nr * (2 * d.kl + 1) * (d.L + 1);
+  gd_matrices* m = new gd_matrices();
+  m->h = h;
+  m->diffusivity = diffusivity;
+  m->dt = dt;
+  m->theta = theta;
+  cudaError_t e = cudaMalloc(&m->d_nu, sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&m->d_lin, n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&m->d_lu, n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(m->d_nu, &diffusivity, sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream);
+  if (e == cudaSuccess) {
+    launch_build_lu(h->stream, d.nr, d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, m->d_nu, dt, theta, 0,
+                    m->d_lin, m->d_lu, h->d_flag, 1);
+    e = cudaGetLastError();
+  }
+  int flag = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess || flag) {
+    gd_destroy_timestepping_matrices(m);
+    if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("timestepping matrices: ") + cudaGetErrorString(e));
+    return fail(h, GD_ERR_SINGULAR, "zero pivot in a banded LU factorisation");
+  }
+  *out = m;
+  return GD_OK;
+}
+
+int gd_destroy_timestepping_matrices(gd_matrices* m) {
+  if (!m) return GD_ERR_ARG;
+  cudaSetDevice(m->h->device);
+  cudaFree(m->d_nu);
+  cudaFree(m->d_lin);
+  cudaFree(m->d_lu);
+  delete m;
+  return GD_OK;
+}
+
+// The CNAB2 column kernel on one field of host arrays: sweeps `stages` over
+// the staged field in slot 0 of the second spectral staging buffer.
+static int cnab2_host(gd_handle* h, const gd_matrices* m, double dt, int stages) {
+  Cnab2Args a{};
+  const size_t se = h->spec_elems();
+  a.u[0] = h->d_stage_spec2;
+  a.nl[0] = h->d_stage_spec2 + se;
+  a.prev[0] = h->d_stage_spec2 + 2 * se;
+  a.kind[0] = 0;
+  a.nfield = 1;
+  a.bvals = h->d_bvals;
+  a.temp_slot = -1;
+  a.inv_dt = 1.0 / dt;
+  a.lin_weight = 1.0 - m->theta;
+  a.dt = dt;
+  a.stages = stages;
+  { ProfScope p(h, "cnab2_solve"); launch_cnab2(h->stream, h->d, h->d_lof, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, m->d_nu, m->d_lu, a); }
+  return check_launch(h, "cnab2");
+}
+
+int gd_build_rhs_cnab2(gd_handle* h, const gd_matrices* m, double dt, const double* un_re, const double* un_im,
+                       const double* nl_re, const double* nl_im, const double* prev_re, const double* prev_im,
+                       double* rhs_re, double* rhs_im) {
+  if (!h || !m || !un_re || !un_im || !nl_re || !nl_im || !prev_re || !prev_im || !rhs_re || !rhs_im)
+    return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (m->h != h) return fail(h, GD_ERR_ARG, "matrices belong to another handle");
+  if (!(dt > 0.0)) return fail(h, GD_ERR_ARG, "need dt > 0");
+  int s = nl_prepare(h);
+  const size_t se = h->spec_elems();
+  if (!s) s = put_spec(h, un_re, un_im, h->d_stage_spec2);
+  if (!s) s = put_spec(h, nl_re, nl_im, h->d_stage_spec2 + se);
+  if (!s) s = put_spec(h, prev_re, prev_im, h->d_stage_spec2 + 2 * se);
+  if (!s) s = cnab2_host(h, m, dt, 1);
+  return s ? s : download_spec(h, h->d_stage_spec2, rhs_re, rhs_im);
+}
+
+int gd_solve_implicit_step(gd_handle* h, const gd_matrices* m, const double* rhs_re, const double* rhs_im,
+                           double* sol_re, double* sol_im) {
+  if (!h || !m || !rhs_re || !rhs_im || !sol_re || !sol_im) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (m->h != h) return fail(h, GD_ERR_ARG, "matrices belong to another handle");
+  int s = nl_prepare(h);
+  if (!s) s = put_spec(h, rhs_re, rhs_im, h->d_stage_spec2);
+  if (!s) s = cnab2_host(h, m, m->dt, 6);
+  return s ? s : download_spec(h, h->d_stage_spec2, sol_re, sol_im);
+}
+
+int gd_compute_temperature_nonlinear(gd_handle* h, double* t_re, double* t_im, const double* u_theta,
+                                     const double* u_phi, double* nl_re, double* nl_im, double* t_grid) {
+  if (!h || !t_re || !t_im || !u_theta || !u_phi || !nl_re || !nl_im)
+    return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  int s = nl_prepare(h);
+  if (!s) s = put_spec(h, t_re, t_im, h->field(F_TEMP));
+  if (!s) s = put_grid(h, u_theta, h->grid(GD_GRID_U_TH));
+  if (!s) s = put_grid(h, u_phi, h->grid(GD_GRID_U_PH));
+  if (!s) s = temperature_nl_fp64(h);
+  if (!s) s = download_spec(h, h->nlf(F_TEMP), nl_re, nl_im);
+  if (!s) s = download_spec(h, h->field(F_TEMP), t_re, t_im);
+  if (!s && t_grid) s = get_grid(h, h->grid(GD_GRID_T), t_grid);
+  return s;
+}
+
+int gd_compute_velocity_nonlinear(gd_handle* h, const double* tor_re, const double* tor_im, const double* pol_re,
+                                  const double* pol_im, const double* j_theta, const double* j_phi,
+                                  const double* b_theta, const double* b_phi, double* nl_tor_re, double* nl_tor_im,
+                                  double* nl_pol_re, double* nl_pol_im, double* u_theta, double* u_phi) {
+  if (!h || !tor_re || !tor_im || !pol_re || !pol_im || !nl_tor_re || !nl_tor_im || !nl_pol_re || !nl_pol_im)
+    return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  const bool grids = j_theta && j_phi && b_theta && b_phi;
+  if (h->c.magnetic && !grids) return fail(h, GD_ERR_ARG, "the Lorentz term needs the j and B grids");
+  int s = nl_prepare(h);
+  if (!s) s = put_spec(h, tor_re, tor_im, h->field(F_UTOR));
+  if (!s) s = put_spec(h, pol_re, pol_im, h->field(F_UPOL));
+  if (!s && grids) s = put_grid(h, j_theta, h->grid(GD_GRID_J_TH));
+  if (!s && grids) s = put_grid(h, j_phi, h->grid(GD_GRID_J_PH));
+  if (!s && grids) s = put_grid(h, b_theta, h->grid(GD_GRID_B_TH));
+  if (!s && grids) s = put_grid(h, b_phi, h->grid(GD_GRID_B_PH));
+  if (!s) s = velocity_nl_fp64(h);
+  if (!s) s = download_spec(h, h->nlf(F_UTOR), nl_tor_re, nl_tor_im);
+  if (!s) s = download_spec(h, h->nlf(F_UPOL), nl_pol_re, nl_pol_im);
+  if (!s && u_theta) s = get_grid(h, h->grid(GD_GRID_U_TH), u_theta);
+  if (!s && u_phi) s = get_grid(h, h->grid(GD_GRID_U_PH), u_phi);
+  return s;
+}
+
+int gd_compute_magnetic_nonlinear(gd_handle* h, const double* tor_re, const double* tor_im, const double* pol_re,
+                                  const double* pol_im, const double* u_theta, const double* u_phi,
+                                  double* nl_tor_re, double* nl_tor_im, double* nl_pol_re, double* nl_pol_im,
+                                  double* b_theta, double* b_phi, double* j_theta, double* j_phi) {
+  if (!h || !tor_re || !tor_im || !pol_re || !pol_im || !u_theta || !u_phi || !nl_tor_re || !nl_tor_im ||
+      !nl_pol_re || !nl_pol_im)
+    return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  int s = nl_prepare(h);
+  if (!s) s = put_spec(h, tor_re, tor_im, h->field(F_BTOR));
+  if (!s) s = put_spec(h, pol_re, pol_im, h->field(F_BPOL));
+  if (!s) s = put_grid(h, u_theta, h->grid(GD_GRID_U_TH));
+  if (!s) s = put_grid(h, u_phi, h->grid(GD_GRID_U_PH));
+  if (!s) s = magnetic_nl_fp64(h);
+  if (!s) s = download_spec(h, h->nlf(F_BTOR), nl_tor_re, nl_tor_im);
+  if (!s) s = download_spec(h, h->nlf(F_BPOL), nl_pol_re, nl_pol_im);
+  if (!s && b_theta) s = get_grid(h, h->grid(GD_GRID_B_TH), b_theta);
+  if (!s && b_phi) s = get_grid(h, h->grid(GD_GRID_B_PH), b_phi);
+  if (!s && j_theta) s = get_grid(h, h->grid(GD_GRID_J_TH), j_theta);
+  if (!s && j_phi) s = get_grid(h, h->grid(GD_GRID_J_PH), j_phi);
+  return s;
 }
 
 int gd_temperature_nonlinear(gd_handle* h) {

@@ -41,9 +41,11 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
   const bool boot = a.boot != 0;
   const bool rows = a.bc_rows != 0;
   const bool is_temp = slot == a.temp_slot;
+  const int stages = a.stages ? a.stages : 7;
 
   // sweep 1: right-hand side, rows in batches of RB whose loads are issued first
   constexpr int RB = 4;
+  if (stages & 1) {
   double wr[NB], wi[NB];
 #pragma unroll
   for (int t = 0; t < NB; ++t) {
@@ -99,7 +101,9 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
       wi[NB - 1] = uni[b];
     }
   }
+  }
   // sweep 2: forward substitution (unit lower factor), y[i - KL + t] in yr[t]
+  if (stages & 2) {
   double yr[KL], yi[KL];
 #pragma unroll
   for (int t = 0; t < KL; ++t) yr[t] = yi[t] = 0.0;
@@ -137,7 +141,9 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
       yi[KL - 1] = y_i;
     }
   }
+  }
   // sweep 3: back substitution, x[i + 1 + t] in xr[t]
+  if (stages & 4) {
   double xr[KL], xi[KL];
 #pragma unroll
   for (int t = 0; t < KL; ++t) xr[t] = xi[t] = 0.0;
@@ -179,6 +185,7 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
       xr[0] = x_r;
       xi[0] = x_i;
     }
+  }
   }
 }
 

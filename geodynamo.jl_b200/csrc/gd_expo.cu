@@ -558,21 +558,13 @@ int exp_apply_threads(const Dims& d) { return (EU_COLS / EU_CT) * ((d.nr + EU_RT
 void launch_exp_apply(cudaStream_t st, const Dims& d, const int* moff, const double* tab, const ExpApply& a) {
   const int npad = ((d.nr + EU_RT - 1) / EU_RT) * EU_RT;
   const size_t smem = (size_t)2 * EU_KC * (npad + 2 * EU_COLS) * sizeof(double);
-  static size_t attr = 0;
-  if (attr < smem) {
-    cudaFuncSetAttribute(k_exp_apply<288>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_exp_apply<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = smem;
-  }
+  allow_dynamic_smem(k_exp_apply<288>, smem);
+  allow_dynamic_smem(k_exp_apply<512>, smem);
   const int ncc = ceil_div(2 * (d.M + 1), EU_COLS);
   const dim3 grid(ncc, d.L + 1, a.nfield);
   if (npad <= 2 * TC_RTH * 8) {
     const size_t tsmem = (size_t)2 * EU_KC * (tc_stride(npad) + 2 * TC_SX) * sizeof(double);
-    static size_t tattr = 0;
-    if (tattr < tsmem) {
-      cudaFuncSetAttribute(k_exp_apply_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
-      tattr = tsmem;
-    }
+    allow_dynamic_smem(k_exp_apply_tc, tsmem);
     k_exp_apply_tc<<<grid, TC_THREADS, tsmem, st>>>(d, moff, tab, a);
     return;
   }

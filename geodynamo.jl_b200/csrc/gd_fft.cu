@@ -229,12 +229,8 @@ static bool launch_ct(cudaStream_t s, const Dims& d, const void* tw, const void*
   typedef typename C2<RT>::T C;
   constexpr int RS = CtGeom<RT, N>::RS, TB = CtGeom<RT, N>::TB;
   const size_t sm = (size_t)2 * TB * RS * sizeof(C);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_fft_synth_ct<RT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-    cudaFuncSetAttribute(k_fft_analysis_ct<RT, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-    attr = true;
-  }
+  allow_dynamic_smem(k_fft_synth_ct<RT, N>, 100 * 1024);
+  allow_dynamic_smem(k_fft_analysis_ct<RT, N>, 100 * 1024);
   dim3 g(ceil_div(d.nth, TB), d.nr, ncomp);
   if (synth)
     k_fft_synth_ct<RT, N><<<g, kThreads, sm, s>>>(d, (const C*)tw, (const C*)F, grid, stride);
@@ -306,11 +302,7 @@ void launch_fft_synth(cudaStream_t s, const Dims& d, const FftPlan& p0, const vo
   FftPlan p = p0;
   p.tb = pick_tb<RT>(d, p.n);
   const size_t sm = (size_t)2 * p.tb * prow(p.n) * sizeof(C);
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaFuncSetAttribute(k_fft_synth<RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done = true;
-  }
+  allow_dynamic_smem(k_fft_synth<RT>, 200 * 1024);
   dim3 grid_dim(ceil_div(d.nth, p.tb), d.nr, ncomp);
   k_fft_synth<RT><<<grid_dim, kThreads, sm, s>>>(d, p, (const C*)twiddle, (const C*)F, grid, grid_comp_stride);
 }
@@ -323,11 +315,7 @@ void launch_fft_analysis(cudaStream_t s, const Dims& d, const FftPlan& p0, const
   FftPlan p = p0;
   p.tb = pick_tb<RT>(d, p.n);
   const size_t sm = (size_t)2 * p.tb * prow(p.n) * sizeof(C);
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaFuncSetAttribute(k_fft_analysis<RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done = true;
-  }
+  allow_dynamic_smem(k_fft_analysis<RT>, 200 * 1024);
   dim3 grid_dim(ceil_div(d.nth, p.tb), d.nr, ncomp);
   k_fft_analysis<RT><<<grid_dim, kThreads, sm, s>>>(d, p, (const C*)twiddle, grid, grid_comp_stride, w, (C*)G);
 }

@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
     }
   };
   const float ur = 0.f, wr = 0.f, jr = 0.f, br = 0.f;
-  const float adv = -a.rf, mrf = -a.rf, lfr = a.lf;
+  const float adv = -a.rf, mrf = -a.cf, lfr = a.lf;
 
   // consumer of one transformed component: grid rows or the products
   // inputs: T phase [g_r, u_th, g_th, u_ph, g_ph]; V phase [u_th, u_ph,
@@ -366,11 +366,7 @@ template <int N, int PH, bool S3>
 void launch_one_k(cudaStream_t s, const Dims& d, const FftPlan& p, const float2* tw, const FusedArgs& a) {
   const int n = N > 0 ? N : p.n;
   const size_t sm = fused_smem(PH, n, N > 0);
-  static size_t attr = 0;
-  if (attr < sm) {
-    cudaFuncSetAttribute(k_fused<N, PH, S3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    attr = sm;
-  }
+  allow_dynamic_smem(k_fused<N, PH, S3>, sm);
   dim3 g(ceil_div(d.nth, FB), d.nr);
   k_fused<N, PH, S3><<<g, FNT, sm, s>>>(d, p, tw, a);
 }

@@ -17,7 +17,8 @@ struct FusedArgs {
   const double* cth;     // Coriolis cos/sin tables, indexed by min(phi index, nlat - 1)
   const double* sthc;
   const double* sources; // internal heat sources per shell
-  float rf, lf;          // Pm/E for the advection/Coriolis and Lorentz factors
+  float rf, lf;          // Pm/E for the advection and Lorentz factors
+  float cf;              // Pm/E for the Coriolis term (0: the term is formed elsewhere)
 };
 
 // Theta blocks of the blocked Fourier layout and float4 elements per component.

@@ -18,6 +18,7 @@ struct gd_handle {
   std::string err;
   long step_count = 0;
   int precision = GD_PREC_FP64;
+  int fp64_stages = 0;        // GD_STAGE_* run in FP64 inside the mixed-precision step
   size_t bytes = 0;
   std::vector<void*> allocs;
 

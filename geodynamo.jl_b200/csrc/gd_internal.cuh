@@ -45,7 +45,7 @@ void launch_rec_tables(cudaStream_t s, const Dims& d, const int* moff, const dou
                        double* ra, double* rb, double* rc, double* r1a, double* r1b, double* pmm, double* sinv);
 void launch_build_lu(cudaStream_t s, int nr, int kl, int L, const double* d1, const double* d2,
                      const double* rinv, const double* rinv2, const double* nu, double dt, double theta,
-                     int bc_rows, double* lin, double* lu, int* status);
+                     int bc_rows, double* lin, double* lu, int* status, int nkind = 3);
 
 // ---- Legendre (gd_legendre.cu) ----
 struct SynthArgs {
@@ -93,6 +93,9 @@ void launch_velocity_nl(cudaStream_t s, const Dims& d, const double* cth, const 
                         double lf, int magnetic, const R* uth, const R* uph, const R* wth, const R* wph,
                         const R* jth, const R* jph, const R* bth, const R* bph, R* ath, R* aph);
 template <typename R>
+void launch_coriolis(cudaStream_t s, const Dims& d, const double* cth, const double* sth_cor, double rf, const R* uth,
+                     const R* uph, R* ath, R* aph);
+template <typename R>
 void launch_induction(cudaStream_t s, const Dims& d, const R* uth, const R* uph, const R* bth, const R* bph,
                       R* oth, R* oph);
 
@@ -126,6 +129,7 @@ struct Cnab2Args {
   int temp_slot;              // slot index of the temperature field
   double inv_dt, lin_weight;
   double dt;                  // EAB2: the time step applied to the phi1 term
+  int stages;                 // sweeps to run: 1 rhs, 2 forward, 4 back substitution (0: all)
 };
 // ---- exponential Adams-Bashforth 2 (gd_expo.cu) ----
 size_t etd_table_doubles(const Dims& d);
@@ -162,5 +166,21 @@ void launch_energy(cudaStream_t s, const Dims& d, const int* lof, const double* 
 void launch_check_finite(cudaStream_t s, size_t n, const double* a, int* flag);
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Kernel attributes and device properties are per device, and one process may
+// hold handles on several devices from several host threads.  These helpers
+// act on the current device (every entry point makes the handle's device
+// current first) and are thread-safe.
+//
+// Raises func's dynamic shared-memory limit on the current device to at
+// least `bytes`; the largest value set so far is remembered per
+// (kernel, device), so repeated launches make no driver call.
+cudaError_t allow_dynamic_smem(const void* func, size_t bytes);
+template <typename K>
+inline cudaError_t allow_dynamic_smem(K* kernel, size_t bytes) {
+  return allow_dynamic_smem(reinterpret_cast<const void*>(kernel), bytes);
+}
+// Multiprocessor count of the current device (148 if it cannot be read).
+int current_sm_count();
 
 }  // namespace gd

@@ -754,10 +754,6 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
 }
 
 // ---------------------------------------------------------------------------
-template <typename K>
-static void smem_attr(K k, size_t bytes) {
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
 // stages + mbarriers and TMEM slot (16 bytes past the stages) + the scalar
 // kernels' per-column tables (one pointer per column, one offset per pair)
 // stages + full/empty per stage, tfull, tempty and the TMEM address slot
@@ -770,27 +766,15 @@ static size_t analysis_smem(bool vec) {
   const int B = 2 * NC * TC_K;
   return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 2) + (size_t)NC * 8 + (size_t)(NC / 2) * 8;
 }
-static bool g_attr_done = false;
 static void set_attrs() {
-  if (g_attr_done) return;
-  smem_attr(k_tc_synth4<false>, synth_smem(false));
-  smem_attr(k_tc_synth4<true>, synth_smem(true));
-  smem_attr(k_tc_analysis3<false>, analysis_smem(false));
-  smem_attr(k_tc_analysis3<true>, analysis_smem(true));
-  g_attr_done = true;
+  allow_dynamic_smem(k_tc_synth4<false>, synth_smem(false));
+  allow_dynamic_smem(k_tc_synth4<true>, synth_smem(true));
+  allow_dynamic_smem(k_tc_analysis3<false>, analysis_smem(false));
+  allow_dynamic_smem(k_tc_analysis3<true>, analysis_smem(true));
 }
 
 // One persistent CTA per SM (at most one tile each when there are fewer tiles).
-static int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
+static int sm_count() { return current_sm_count(); }
 
 void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long* cofs, const float* imgP,
                      const float* imgD, const double* sinv, const TcSynthArgs& a, bool vec) {

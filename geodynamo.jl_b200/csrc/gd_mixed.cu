@@ -182,7 +182,97 @@ FusedArgs phase_args(gd_handle* h) {
   f.sources = h->d_sources;
   f.rf = (float)(h->c.magnetic_prandtl / h->c.ekman);
   f.lf = f.rf;
+  f.cf = f.rf;
   return f;
+}
+
+// ---- the velocity chain in FP64 (GD_STAGE_*) ----
+// FP64 Fourier components: [comp][r][m][s][ith] double2, nr x (mmax+1) x nlat
+// per component (the FP64 path's layout).  The velocity components use
+// components 0 and 1 of the handle's FP64 Fourier buffer, the folded
+// transforms of the velocity products components 2 and 3.
+size_t fourier64_comp(const Dims& d) { return (size_t)d.nr * (d.M + 1) * d.nlat; }
+
+constexpr int CV_MT = 8;   // orders per CTA
+constexpr int CV_CH = 64;  // colatitude pairs per pass
+
+// FP64 Fourier (synthesis layout, s = north / south row) <-> blocked FP32
+// (float4 north Re, north Im, south Re, south Im at [comp][r][theta block][m]
+// [pair in block]).  One CTA per (component, shell) and CV_MT orders; both
+// sides are read and written in contiguous runs through shared memory.
+template <bool TO_BLOCKED>
+__global__ void __launch_bounds__(256) k_convert_fourier(Dims d, double2* __restrict__ f64, float4* __restrict__ blk,
+                                                        size_t fcomp) {
+  __shared__ double2 buf[CV_MT][2][CV_CH];
+  const int m0 = blockIdx.x * CV_MT, cr = blockIdx.y;  // cr = comp nr + r
+  const int nblk = (d.nth + FOURIER_BLOCK - 1) / FOURIER_BLOCK;
+  const size_t run = (size_t)nblk * (d.M + 1) * FOURIER_BLOCK;
+  const int comp = cr / d.nr, r = cr % d.nr;
+  double2* src64 = f64 + (size_t)cr * (d.M + 1) * 2 * d.nth;
+  float4* dst = blk + comp * fcomp + (size_t)r * run;
+  for (int i0 = 0; i0 < d.nth; i0 += CV_CH) {
+    // FP64 side: rows (m, s) of CV_CH consecutive colatitudes
+    if (TO_BLOCKED) {
+      for (int e = threadIdx.x; e < CV_MT * 2 * CV_CH; e += blockDim.x) {
+        const int mm = e / (2 * CV_CH), sr = (e / CV_CH) & 1, i = e % CV_CH;
+        const int m = m0 + mm, ith = i0 + i;
+        if (m <= d.M && ith < d.nth) buf[mm][sr][i] = src64[((size_t)m * 2 + sr) * d.nth + ith];
+      }
+      __syncthreads();
+    }
+    // blocked side: for each theta block, CV_MT orders x FOURIER_BLOCK pairs are contiguous
+    for (int e = threadIdx.x; e < CV_CH * CV_MT; e += blockDim.x) {
+      const int p = e % FOURIER_BLOCK, mm = (e / FOURIER_BLOCK) % CV_MT, bl = e / (FOURIER_BLOCK * CV_MT);
+      const int i = bl * FOURIER_BLOCK + p, ith = i0 + i, m = m0 + mm;
+      if (m > d.M || ith >= d.nth) continue;
+      float4* q = dst + ((size_t)(ith / FOURIER_BLOCK) * (d.M + 1) + m) * FOURIER_BLOCK + ith % FOURIER_BLOCK;
+      if (TO_BLOCKED) {
+        const double2 n = buf[mm][0][i], sv = buf[mm][1][i];
+        *q = make_float4((float)n.x, (float)n.y, (float)sv.x, (float)sv.y);
+      } else {
+        const float4 v = *q;
+        buf[mm][0][i] = make_double2(v.x, v.y);
+        buf[mm][1][i] = make_double2(v.z, v.w);
+      }
+    }
+    if (!TO_BLOCKED) {
+      __syncthreads();
+      for (int e = threadIdx.x; e < CV_MT * 2 * CV_CH; e += blockDim.x) {
+        const int mm = e / (2 * CV_CH), sr = (e / CV_CH) & 1, i = e % CV_CH;
+        const int m = m0 + mm, ith = i0 + i;
+        if (m <= d.M && ith < d.nth) src64[((size_t)m * 2 + sr) * d.nth + ith] = buf[mm][sr][i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+void launch_convert_fourier(cudaStream_t s, const Dims& d, double2* f64, float4* blk, size_t fcomp, int ncomp,
+                            bool to_blocked) {
+  const dim3 grid(ceil_div(d.M + 1, CV_MT), ncomp * d.nr);
+  if (to_blocked)
+    k_convert_fourier<true><<<grid, 256, 0, s>>>(d, f64, blk, fcomp);
+  else
+    k_convert_fourier<false><<<grid, 256, 0, s>>>(d, f64, blk, fcomp);
+}
+
+// Folded transforms (same layout, float2 / double2): g64 = [g64 +] g32 or g32 = g64.
+__global__ void k_fold_widen(size_t n, const float2* __restrict__ g32, double2* __restrict__ g64, int add) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float2 v = g32[i];
+    double2 o = make_double2((double)v.x, (double)v.y);
+    if (add) {
+      const double2 a = g64[i];
+      o = make_double2(a.x + o.x, a.y + o.y);
+    }
+    g64[i] = o;
+  }
+}
+__global__ void k_fold_narrow(size_t n, const double2* __restrict__ g64, float2* __restrict__ g32) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = g64[i];
+    g32[i] = make_float2((float)v.x, (float)v.y);
+  }
 }
 
 }  // namespace
@@ -299,10 +389,42 @@ int mixed_temperature_nl(gd_handle* h) {
   return launched(h, "mixed temperature nonlinear");
 }
 
+// The velocity phase.  The stages of h->fp64_stages run in FP64 with the FP64
+// path's kernels: GD_STAGE_VEL_SYNTH the vector synthesis of u (DMMA
+// Legendre; its FP32 copy for the fused kernels is converted from the FP64
+// result), GD_STAGE_VEL_PRODUCTS the phi transforms of u and the Coriolis
+// product (the FP32 fused kernel then forms the cross products only, whose
+// theta and phi components are exact zeros with zero radial components, and
+// its folded transforms are added to the FP64 ones), GD_STAGE_VEL_ANALYSIS
+// the vector analysis (DMMA Legendre).  With all three the velocity nonlinear
+// term is the FP64 step's, so u and the kinetic energy follow the FP64 run.
 int mixed_velocity_nl(gd_handle* h) {
   MixedState* x = h->mixed;
   const Dims& d = h->d;
-  int s = tc_synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), x->F(FC_U));
+  const int st = h->fp64_stages;
+  const size_t fc64 = fourier64_comp(d);
+  double2* U64 = h->d_F;             // u_theta, u_phi Fourier (FP64 synthesis layout)
+  double2* G64 = h->d_F + 2 * fc64;  // folded transforms of the velocity products (FP64)
+  const size_t nfold = 2 * fc64;     // double2 of the two folded components
+  int s;
+  if (st & GD_STAGE_VEL_SYNTH) {
+    SynthArgs a{};
+    a.table0 = h->d_dP;
+    a.table1 = h->d_Q;
+    a.coef[0] = h->field(F_UPOL);
+    a.coef[1] = h->field(F_UTOR);
+    a.nf = 1;
+    a.out = U64;
+    { ProfScope p(h, "legendre_synth_vector_fp64"); launch_synth_fp64(h->stream, d, h->d_moff, a, true); }
+    { ProfScope p(h, "fourier_convert"); launch_convert_fourier(h->stream, d, U64, x->F(FC_U), x->fcomp, 2, true); }
+    s = launched(h, "FP64 velocity synthesis");
+  } else {
+    s = tc_synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), x->F(FC_U));
+    if (!s && (st & GD_STAGE_VEL_PRODUCTS)) {
+      { ProfScope p(h, "fourier_convert"); launch_convert_fourier(h->stream, d, U64, x->F(FC_U), x->fcomp, 2, false); }
+      s = launched(h, "velocity Fourier widening");
+    }
+  }
   if (s) return s;
   { ProfScope p(h, "spectral_curl");
     launch_curl_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR),
@@ -311,6 +433,7 @@ int mixed_velocity_nl(gd_handle* h) {
   if (s) return s;
   // current density and magnetic field of the previous magnetic phase (F(FC_J), F(FC_B))
   FusedArgs f = phase_args(h);
+  if (st & GD_STAGE_VEL_PRODUCTS) f.cf = 0.f;
   const float4* fin[8] = {x->F(FC_U), x->F(FC_U + 1), x->F(FC_W), x->F(FC_W + 1),
                           x->F(FC_J), x->F(FC_J + 1), x->F(FC_B), x->F(FC_B + 1)};
   for (int i = 0; i < 8; ++i) f.fin[i] = fin[i];
@@ -318,6 +441,42 @@ int mixed_velocity_nl(gd_handle* h) {
   { ProfScope p(h, "fused_velocity_fp32"); launch_fused(h->stream, d, h->plan, h->d_twf, FUSED_VELOCITY, f); }
   s = launched(h, "fused velocity phase");
   if (s) return s;
+  if (st & GD_STAGE_VEL_PRODUCTS) {
+    const double rf = h->c.magnetic_prandtl / h->c.ekman;
+    { ProfScope p(h, "fft_synth_fp64");
+      launch_fft_synth<double>(h->stream, d, h->plan, h->d_tw, U64, h->grid(GD_GRID_U_TH), 2, h->grid_elems()); }
+    { ProfScope p(h, "nl_coriolis_fp64");
+      launch_coriolis<double>(h->stream, d, h->d_cth, h->d_sthc, rf, h->grid(GD_GRID_U_TH), h->grid(GD_GRID_U_PH),
+                              h->grid(GD_GRID_VADV_TH), h->grid(GD_GRID_VADV_PH)); }
+    { ProfScope p(h, "fft_analysis_fp64");
+      launch_fft_analysis<double>(h->stream, d, h->plan, h->d_tw, h->grid(GD_GRID_VADV_TH), h->grid_elems(), h->d_w,
+                                  G64, 2); }
+  }
+  if (st & (GD_STAGE_VEL_PRODUCTS | GD_STAGE_VEL_ANALYSIS)) {
+    // FP32 folded transforms of the fused kernel: added to the FP64 Coriolis
+    // transforms, or widened for the FP64 analysis
+    ProfScope p(h, "fold_convert");
+    const int add = (st & GD_STAGE_VEL_PRODUCTS) ? 1 : 0;
+    k_fold_widen<<<148 * 4, 256, 0, h->stream>>>(nfold, x->d_G, G64, add);
+  }
+  s = launched(h, "FP64 velocity products");
+  if (s) return s;
+  if (st & GD_STAGE_VEL_ANALYSIS) {
+    AnalysisArgs a{};
+    a.table0 = h->d_dP;
+    a.table1 = h->d_Q;
+    a.in = G64;
+    a.out[0] = h->nlf(F_UTOR);
+    a.out[1] = h->nlf(F_UPOL);
+    a.nf = 1;
+    a.epi = EPI_VECTOR;
+    { ProfScope p(h, "legendre_analysis_vector_fp64"); launch_analysis_fp64(h->stream, d, h->d_moff, a); }
+    return launched(h, "FP64 velocity analysis");
+  }
+  if (st & GD_STAGE_VEL_PRODUCTS) {
+    ProfScope p(h, "fold_convert");
+    k_fold_narrow<<<148 * 4, 256, 0, h->stream>>>(nfold, G64, x->d_G);
+  }
   return tc_analysis_vector_G(h, h->nlf(F_UTOR), h->nlf(F_UPOL), EPI_VECTOR);
 }
 

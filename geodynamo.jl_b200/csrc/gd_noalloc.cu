@@ -11,6 +11,7 @@
 // instead of a cudaMalloc'd buffer.
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 
 #include "gd_handle.cuh"
@@ -22,9 +23,42 @@
 static const size_t kScratchBytes = size_t(64) << 20;
 static __device__ __align__(256) unsigned char g_fourier_scratch[size_t(64) << 20];
 
-// Device address of g_fourier_scratch, looked up once per device (host code
-// cannot use the symbol's name as a device address).
+// Device address of g_fourier_scratch, looked up once per device with that
+// device current (host code cannot use the symbol's name as a device
+// address).  The cached address belongs to the device's primary context, which
+// lives as long as the process unless the caller resets the device; the mutex
+// makes the first lookup safe when several host threads call at once.
+static std::mutex g_scratch_mu;
 static void* g_scratch_addr[64] = {};
+
+static cudaError_t scratch_address(int device, void** out) {
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_fourier_scratch);
+    if (e != cudaSuccess) return e;
+    if (!p) return cudaErrorInvalidSymbol;
+    g_scratch_addr[device] = p;
+  }
+  *out = g_scratch_addr[device];
+  return cudaSuccess;
+}
+
+// Makes the handle's device current for the call and restores the caller's
+// current device afterwards.
+namespace {
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t enter(int device) {
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return e;
+    return cudaSetDevice(device);
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+}  // namespace
 
 extern "C" int gd_spectral_to_physical_noalloc(gd_handle* h, int nfield, const double* d_coef, double* d_grid) {
   if (!h) return GD_ERR_ARG;
@@ -38,16 +72,14 @@ extern "C" int gd_spectral_to_physical_noalloc(gd_handle* h, int nfield, const d
                              " bytes of Fourier scratch (min(nfield,4) x nr x (mmax+1) x nlat x 16); the fixed "
                              "maximum is " + std::to_string(kScratchBytes) + " bytes");
   if (h->device < 0 || h->device >= 64) return gd::set_error(h, GD_ERR_ARG, "device index out of range");
-  cudaError_t e = cudaSetDevice(h->device);
+  DeviceScope scope;
+  cudaError_t e = scope.enter(h->device);
   if (e != cudaSuccess) return gd::set_error(h, GD_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
-  if (!g_scratch_addr[h->device]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_fourier_scratch);
-    if (e != cudaSuccess || !p)
-      return gd::set_error(h, GD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_scratch_addr[h->device] = p;
-  }
-  double2* F = static_cast<double2*>(g_scratch_addr[h->device]);
+  void* scratch = nullptr;
+  e = scratch_address(h->device, &scratch);
+  if (e != cudaSuccess)
+    return gd::set_error(h, GD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  double2* F = static_cast<double2*>(scratch);
   const size_t plane = (size_t)2 * d.nr * d.nlm;  // one field: Re and Im planes
   const size_t G = (size_t)d.nlat * d.nlon * d.nr;
   for (int f0 = 0; f0 < nfield; f0 += 4) {

@@ -64,6 +64,31 @@ __global__ void k_velocity_nl(Dims d, const double* __restrict__ cth, const doub
   }
 }
 
+// The Coriolis part of k_velocity_nl alone, with the same expressions: the
+// mixed-precision step forms the cross products in FP32 in its fused kernel
+// and, when its velocity stages run in FP64, this term here (with u_r = 0 the
+// cross products contribute exact zeros to theta and phi, so the sum of the
+// two equals k_velocity_nl's result).
+template <typename R>
+__global__ void k_coriolis(Dims d, const double* __restrict__ cth, const double* __restrict__ sth, double rf,
+                           const R* __restrict__ uth, const R* __restrict__ uph, R* __restrict__ ath,
+                           R* __restrict__ aph) {
+  const int plane = d.nlat * d.nlon;
+  const size_t base = (size_t)blockIdx.y * plane;
+  const R mrf = (R)(-rf);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += gridDim.x * blockDim.x) {
+    const size_t i = base + q;
+    const int jphi = q % d.nlon;
+    const int tidx = jphi < d.nlat - 1 ? jphi : d.nlat - 1;
+    const R ct = (R)cth[tidx], st = (R)sth[tidx];
+    const R ur = 0;
+    const R u_t = uth[i], u_p = uph[i];
+    const R zt = -ct * u_p, zp = ct * u_t + st * ur;
+    ath[i] = mrf * zt;
+    aph[i] = mrf * zp;
+  }
+}
+
 // compute_velocity_cross_magnetic! (src/magnetic.jl:375-404), theta/phi.
 template <typename R>
 __global__ void k_induction(Dims d, const R* __restrict__ uth, const R* __restrict__ uph, const R* __restrict__ bth,
@@ -99,6 +124,11 @@ void launch_velocity_nl(cudaStream_t s, const Dims& d, const double* cth, const 
                                                    bth, bph, ath, aph);
 }
 template <typename R>
+void launch_coriolis(cudaStream_t s, const Dims& d, const double* cth, const double* sth_cor, double rf, const R* uth,
+                     const R* uph, R* ath, R* aph) {
+  k_coriolis<R><<<grid_blocks(d), 256, 0, s>>>(d, cth, sth_cor, rf, uth, uph, ath, aph);
+}
+template <typename R>
 void launch_induction(cudaStream_t s, const Dims& d, const R* uth, const R* uph, const R* bth, const R* bph,
                       R* oth, R* oph) {
   k_induction<R><<<grid_blocks(d), 256, 0, s>>>(d, uth, uph, bth, bph, oth, oph);
@@ -110,6 +140,8 @@ template void launch_temperature_advection<double>(cudaStream_t, const Dims&, co
 template void launch_velocity_nl<double>(cudaStream_t, const Dims&, const double*, const double*, double, double, int,
                                          const double*, const double*, const double*, const double*, const double*,
                                          const double*, const double*, const double*, double*, double*);
+template void launch_coriolis<double>(cudaStream_t, const Dims&, const double*, const double*, double, const double*,
+                                      const double*, double*, double*);
 template void launch_induction<double>(cudaStream_t, const Dims&, const double*, const double*, const double*,
                                        const double*, double*, double*);
 

@@ -6,9 +6,35 @@
 // operation.
 #include <math.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "gd_internal.cuh"
 
 namespace gd {
+
+cudaError_t allow_dynamic_smem(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& have = done[{func, dev}];
+  if (have >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
+}
+
+int current_sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    return 148;
+  return n;
+}
 
 static const double kPi = 3.14159265358979323846;
 
@@ -241,8 +267,8 @@ __global__ void k_build_lu(int N, int kl, int L, const double* d1, const double*
 
 void launch_build_lu(cudaStream_t s, int nr, int kl, int L, const double* d1, const double* d2,
                      const double* rinv, const double* rinv2, const double* nu, double dt, double theta,
-                     int bc_rows, double* lin, double* lu, int* status) {
-  dim3 grid(ceil_div(L + 1, 32), 3);
+                     int bc_rows, double* lin, double* lu, int* status, int nkind) {
+  dim3 grid(ceil_div(L + 1, 32), nkind);
   k_build_lu<<<grid, 32, 0, s>>>(nr, kl, L, d1, d2, rinv, rinv2, nu, 1.0 / dt, -theta, bc_rows, lin, lu, status);
 }
 

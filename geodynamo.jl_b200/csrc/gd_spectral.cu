@@ -70,15 +70,6 @@ static size_t radial_smem() {
   return sizeof(RadialStage<KL, NBAND>);
 }
 
-// Dynamic shared memory above the 48 KB default, allowed once per kernel.
-template <typename K>
-static void allow_smem(K kernel, size_t bytes, bool& done) {
-  if (!done) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    done = true;
-  }
-}
-
 // compute_all_gradients_spectral! (src/scalar_field_common.jl:125-345):
 // theta derivative by the reference's recurrence coefficients (:158,171), phi
 // derivative i m, radial derivative by the banded D1, then x 1/r on the
@@ -262,8 +253,7 @@ void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* ri
   const int rows = radial_rows(d.nr);
   dim3 grid(ceil_div(d.nlm, RAD_THREADS), ceil_div(d.nr, rows));
   const size_t smem = radial_smem<GD_MAX_KL, 2>();
-  static bool done = false;
-  allow_smem(k_curl<GD_MAX_KL, false>, smem, done);
+  allow_dynamic_smem(k_curl<GD_MAX_KL, false>, smem);
   k_curl<GD_MAX_KL, false><<<grid, RAD_THREADS, smem, s>>>(d, lof, nullptr, rinv, rinv2, d1, d2, tor, pol, otor,
                                                            opol, rows, SynthImageOut{});
 }
@@ -274,8 +264,7 @@ void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* m
   const int rows = radial_rows(d.nr);
   dim3 grid(ceil_div(d.nlm, RAD_THREADS), ceil_div(d.nr, rows));
   const size_t smem = radial_smem<GD_MAX_KL, 2>();
-  static bool done = false;
-  allow_smem(k_curl<GD_MAX_KL, true>, smem, done);
+  allow_dynamic_smem(k_curl<GD_MAX_KL, true>, smem);
   k_curl<GD_MAX_KL, true><<<grid, RAD_THREADS, smem, s>>>(d, lof, mof, rinv, rinv2, d1, d2, tor, pol, nullptr,
                                                           nullptr, rows, img);
 }

@@ -54,6 +54,20 @@ enum {
 /* Precision modes. */
 enum { GD_PREC_FP64 = 0, GD_PREC_MIXED = 1 };
 
+/* Stages of the mixed-precision step that gd_set_fp64_stages can return to
+ * FP64 (bit mask).  In the reference's step the theta and phi components of
+ * every cross product vanish (the synthesized vectors have zero radial
+ * components, src/shtnskit_field_functions.jl:264-279), so the velocity's
+ * nonlinear term is its Coriolis term alone (src/velocity.jl:492-496): these
+ * three stages are the whole chain the velocity, and so the kinetic energy,
+ * depends on. */
+enum {
+  GD_STAGE_VEL_SYNTH = 1,    /* vector synthesis of u (Legendre, DMMA)                */
+  GD_STAGE_VEL_PRODUCTS = 2, /* phi transforms of u and the Coriolis product          */
+  GD_STAGE_VEL_ANALYSIS = 4, /* vector analysis of the velocity's terms (Legendre)    */
+  GD_STAGE_VEL_ALL = 7
+};
+
 /* Time-stepping schemes of gd_step (the reference's ts_scheme,
  * src/simulation.jl:1054-1300): CNAB2 (build_rhs_cnab2! + solve_implicit_step!),
  * EAB2 (eab2_update! with the exponential cache of create_etd_cache) or ERK2
@@ -106,6 +120,11 @@ int gd_info(const gd_handle* h, int* nlm, size_t* device_bytes);
 int gd_grid(gd_handle* h, double* theta, double* weights, double* r);
 /* Switch precision of transforms and nonlinear terms (GD_PREC_*). */
 int gd_set_precision(gd_handle* h, int mode);
+/* Stages (GD_STAGE_* mask) that the mixed-precision step runs in FP64 with the
+ * FP64 path's kernels; 0 (the default) runs all of them in mixed precision.
+ * With GD_STAGE_VEL_ALL the velocity's nonlinear term, and so the velocity
+ * field, equals the FP64 step's.  Has no effect in GD_PREC_FP64. */
+int gd_set_fp64_stages(gd_handle* h, int mask);
 int gd_synchronize(gd_handle* h);
 
 /* ---- state ------------------------------------------------------------------
@@ -135,7 +154,8 @@ int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi,
                        double* tor_im, double* pol_re, double* pol_im);
 
 /* No counterpart in the reference.  Scalar synthesis (as
- * gd_spectral_to_physical, always FP64) for callers that must not allocate
+ * gd_spectral_to_physical, but always in FP64, whatever the handle's
+ * precision mode: it runs the FP64 kernels) for callers that must not allocate
  * device memory during the call -- for example a Julia session whose GPU memory
  * is owned by CUDA.jl's pool, or a solver loop that forbids allocation after
  * set-up.  d_coef and d_grid are the caller's device buffers in the native
@@ -145,11 +165,61 @@ int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi,
  * uses a fixed 64 MiB array in the library's device image instead of
  * cudaMalloc: min(nfield, 4) x nr x (mmax+1) x nlat x 16 bytes must fit, else
  * GD_ERR_CONFIG.  The first call on a device looks up that array's device
- * address; make it before any stream capture.  The array is shared by every
+ * address; make it before any stream capture.  The cached address assumes the
+ * device's primary context lives as long as the process (no device reset in
+ * between).  The caller's current device is restored on return.  The array is shared by every
  * call and keeps the last call's contents (each call overwrites what it
  * reads), so calls that overlap on the GPU (other streams, other threads)
  * race.  Runs asynchronously on the handle's stream; gd_synchronize() waits. */
 int gd_spectral_to_physical_noalloc(gd_handle* h, int nfield, const double* d_coef, double* d_grid);
+
+/* ---- the reference's nonlinear and time-step functions on host arrays ---------
+ * The same arguments as the reference functions (spectral planes nr x nlm,
+ * l-major; physical grids nr x nlon x nlat, theta fastest), for a caller that
+ * keeps its fields in its own arrays.  They use the handle's model state as
+ * the reference's functions use their field structs: the fields and carried
+ * grids they take are copied into the handle, so a later gd_step continues
+ * from them.  Computed with the FP64 kernels whatever the precision mode.
+ *
+ * compute_temperature_nonlinear!(temp, vel, oc) (src/thermal.jl:149-190):
+ * t_re/t_im in: the temperature; out: with the Dirichlet rows applied in place
+ * (thermal.jl:262-303, values of gd_set_temperature_bc).  u_theta/u_phi: the
+ * velocity grids it is advected by.  t_grid (may be NULL): the temperature grid. */
+int gd_compute_temperature_nonlinear(gd_handle* h, double* t_re, double* t_im, const double* u_theta,
+                                     const double* u_phi, double* nl_re, double* nl_im, double* t_grid);
+/* compute_velocity_nonlinear!(fields, temp, comp, mag, domain) (src/velocity.jl:312-332):
+ * the velocity (toroidal, poloidal), the grids j and B of the previous magnetic
+ * phase (all four may be NULL only without a magnetic field) -> the nonlinear
+ * terms and, when not NULL, the velocity grids u_theta, u_phi. */
+int gd_compute_velocity_nonlinear(gd_handle* h, const double* tor_re, const double* tor_im, const double* pol_re,
+                                  const double* pol_im, const double* j_theta, const double* j_phi,
+                                  const double* b_theta, const double* b_phi, double* nl_tor_re, double* nl_tor_im,
+                                  double* nl_pol_re, double* nl_pol_im, double* u_theta, double* u_phi);
+/* compute_magnetic_nonlinear!(mag, vel, oc, ic, rot) (src/magnetic.jl:131-159):
+ * the magnetic field (toroidal, poloidal) and the velocity grids -> the
+ * nonlinear terms and, when not NULL, the grids B and j. */
+int gd_compute_magnetic_nonlinear(gd_handle* h, const double* tor_re, const double* tor_im, const double* pol_re,
+                                  const double* pol_im, const double* u_theta, const double* u_phi,
+                                  double* nl_tor_re, double* nl_tor_im, double* nl_pol_re, double* nl_pol_im,
+                                  double* b_theta, double* b_phi, double* j_theta, double* j_phi);
+/* SHTnsImplicitMatrices from create_shtns_timestepping_matrices(config, domain,
+ * diffusivity, dt; theta) (src/timestep.jl:489-543): per degree l the operator
+ * L_l = diffusivity (d2/dr2 + (2/r) d/dr - l(l+1)/r^2) and the banded LU of
+ * I/dt - theta L_l (linear_algebra.jl:23-57), on the handle's device.
+ * GD_ERR_SINGULAR on a zero pivot. */
+typedef struct gd_matrices gd_matrices;
+int gd_create_timestepping_matrices(gd_handle* h, double diffusivity, double dt, double theta, gd_matrices** out);
+int gd_destroy_timestepping_matrices(gd_matrices* m);
+/* build_rhs_cnab2!(rhs, un, nl, nl_prev, dt, matrices) (src/timestep.jl:610-690):
+ * rhs = un/dt + (1 - theta) L_l un + 3/2 nl - 1/2 nl_prev. */
+int gd_build_rhs_cnab2(gd_handle* h, const gd_matrices* m, double dt, const double* un_re, const double* un_im,
+                       const double* nl_re, const double* nl_im, const double* prev_re, const double* prev_im,
+                       double* rhs_re, double* rhs_im);
+/* solve_implicit_step!(sol, rhs, matrices) (src/timestep.jl:692-730): per (l, m)
+ * and Re / Im plane, the banded forward and back substitution (solve_banded!,
+ * linear_algebra.jl:59-88). */
+int gd_solve_implicit_step(gd_handle* h, const gd_matrices* m, const double* rhs_re, const double* rhs_im,
+                           double* sol_re, double* sol_im);
 
 /* ---- model step ---------------------------------------------------------------
  * compute_temperature_nonlinear! (src/thermal.jl:149-190),

@@ -62,6 +62,29 @@ def test_ensemble_members_match_oracle(gdb, oracle_mod):
     ens.close()
 
 
+def test_mixed_ensemble_members_match_oracle(gdb, oracle_mod):
+    # mixed-precision members (split-TF32 Legendre, FP32 phi transforms and
+    # products, FP64 solves) against the FP64 oracle at the mixed path's
+    # few-step field tolerance
+    picks = one_per_lmax()
+    ens = gdb.Ensemble([dict(c, precision="mixed") for _, c in picks])
+    oracles = []
+    for (i, c), m in zip(picks, ens.members):
+        load(m, c["lmax"], c["nr"], i)
+        kw = {k: v for k, v in c.items() if k not in GRID_KEYS}
+        o = oracle_mod.Oracle(lmax=c["lmax"], nlat=c["nlat"], nlon=c["nlon"], nr=c["nr"], **kw)
+        load(o, c["lmax"], c["nr"], i)
+        oracles.append(o)
+    ens.step(3)
+    for o in oracles:
+        o.step(3)
+    for (i, c), m, o in zip(picks, ens.members, oracles):
+        for k in NAMES:
+            a, b = m.get_field(k), o.get_field(k)
+            assert rel(a[0], b[0]) < 1e-5 and rel(a[1], b[1]) < 1e-5, (i, k)
+    ens.close()
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_ensemble_equals_single_handles(gdb, precision):
     picks = one_per_lmax()[:3]
