@@ -70,7 +70,7 @@ EXPORTS = (
     "gd_spectral_to_physical_noalloc",
     "gd_compute_temperature_nonlinear", "gd_compute_velocity_nonlinear", "gd_compute_magnetic_nonlinear",
     "gd_create_timestepping_matrices", "gd_destroy_timestepping_matrices", "gd_build_rhs_cnab2",
-    "gd_solve_implicit_step",
+    "gd_solve_implicit_step", "gd_set_fault_test",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
     "gd_ensemble_step", "gd_ensemble_step_async", "gd_ensemble_failed_member", "gd_ensemble_get_stream",
@@ -167,6 +167,7 @@ def load_library():
         "gd_destroy_timestepping_matrices": ([P], I),
         "gd_build_rhs_cnab2": ([P, P, ctypes.c_double] + [D] * 8, I),
         "gd_solve_implicit_step": ([P, P, D, D, D, D], I),
+        "gd_set_fault_test": ([P, ctypes.c_longlong, I], I),
         "gd_magnetic_pullback": ([P, I, I, D, D, D, D], I),
         "gd_ensemble_create": ([ctypes.POINTER(GDConfig), I, I, ctypes.POINTER(P)], I),
         "gd_ensemble_destroy": ([P], I),
@@ -306,6 +307,12 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_set_precision(self.h, PRECISIONS[base]))
         self.set_fp64_stages(stages)
         self.precision = precision
+
+    def set_fault_test(self, wait_cycles=0, omit_step=-1):
+        """Error-path testing (gd_set_fault_test): bound of every tensor-core
+        wait in clock cycles (0: default) and a one-shot omission of the copies
+        of one pipeline step in the next tensor-core synthesis."""
+        self._check(self.lib.gd_set_fault_test(self.h, int(wait_cycles), int(omit_step)))
 
     def set_fp64_stages(self, stages):
         """Stages of the mixed step to run in FP64: names of FP64_STAGES or an int mask."""

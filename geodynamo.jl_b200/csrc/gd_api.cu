@@ -569,6 +569,13 @@ int gd_set_fp64_stages(gd_handle* h, int mask) {
   return GD_OK;
 }
 
+int gd_set_fault_test(gd_handle* h, long long wait_cycles, int omit_step) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  drop_graphs(h);  // captured steps hold the previous settings
+  return mixed_set_fault_test(h, wait_cycles, omit_step);
+}
+
 int gd_synchronize(gd_handle* h) {
   if (!h) return GD_ERR_ARG;
   CK(cudaSetDevice(h->device));

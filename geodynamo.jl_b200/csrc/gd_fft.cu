@@ -223,6 +223,136 @@ __global__ void __launch_bounds__(256) k_fft_analysis_ct(Dims d, const typename 
   }
 }
 
+// The Coriolis term of the velocity phase in FP64, fused.  Per (shell, TB
+// colatitude pairs, output component oc): the inverse phi transform of the
+// velocity component the output multiplies (theta output: u_phi, phi output:
+// u_theta; with u_r = 0 the Coriolis term of each component is one product),
+// the product with the Coriolis factor of latitude index min(phi index,
+// nlat - 1) (src/velocity.jl:492-496), the forward transform and the Gauss
+// folds, plus the folds g32 of the FP32 cross products.  These are the
+// operations of the unfused chain k_fft_synth_ct -> k_coriolis ->
+// k_fft_analysis_ct -> widen-and-add, in the same order, so the result is the
+// same to the last bit; the grids only stay in shared memory.
+template <int N>
+__global__ void __launch_bounds__(256) k_coriolis_fused(Dims d, const double2* __restrict__ tw,
+                                                        const double2* __restrict__ F, const double* __restrict__ cth,
+                                                        const double* __restrict__ sth, double rf,
+                                                        const double* __restrict__ w, const float2* __restrict__ g32,
+                                                        double2* __restrict__ G) {
+  typedef double2 C;
+  constexpr int RS = CtGeom<double, N>::RS, TB = CtGeom<double, N>::TB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + TB * RS;
+  const int M = d.M;
+  const int i0 = blockIdx.x * TB;
+  const int r = blockIdx.y, oc = blockIdx.z, sc = 1 - oc;
+  const int rows = min(TB, d.nth - i0);
+  for (int e = threadIdx.x; e < TB * N; e += kThreads) {
+    const int ii = e / N, k = e - ii * N;
+    if (k > M && k < N - M) { bufA[ii * RS + pidx(k)].x = 0; bufA[ii * RS + pidx(k)].y = 0; }
+  }
+  const size_t fbase = ((size_t)(sc * d.nr + r) * (M + 1)) * 2 * d.nth + i0;
+  for (int e = threadIdx.x; e < (M + 1) * TB; e += kThreads) {
+    const int m = e / TB, ii = e - m * TB;
+    C* row = bufA + ii * RS;
+    C fn, fs;
+    if (ii < rows) {
+      fn = F[fbase + ((size_t)m * 2 + 0) * d.nth + ii];
+      fs = F[fbase + ((size_t)m * 2 + 1) * d.nth + ii];
+    } else {
+      fn.x = fn.y = fs.x = fs.y = 0;
+    }
+    if (m == 0) {
+      C z; z.x = fn.x; z.y = -fs.x;
+      row[0] = z;
+    } else {
+      C z; z.x = fn.x - fs.y; z.y = -(fn.y + fs.x);
+      row[pidx(m)] = z;
+      C zc; zc.x = fn.x + fs.y; zc.y = fn.y - fs.x;
+      row[pidx(N - m)] = zc;
+    }
+  }
+  __syncthreads();
+  C* res = ct_passes<N, TB, 0, 1, C>(bufA, bufB, tw);
+  // grid rows: north z.x, south -z.y; the products packed as (north, south)
+  const double mrf = -rf;
+  for (int e = threadIdx.x; e < TB * N; e += kThreads) {
+    const int ii = e / N, j = e - ii * N;
+    C* at = res + ii * RS + pidx(j);
+    C z = *at, o;
+    if (ii < rows) {
+      const int tidx = j < d.nlat - 1 ? j : d.nlat - 1;
+      const double ct = cth[tidx], st = sth[tidx];
+      const double ur = 0;
+      const double vN = z.x, vS = -z.y;
+      if (oc == 0) {
+        const double ztN = -ct * vN, ztS = -ct * vS;
+        o.x = mrf * ztN; o.y = mrf * ztS;
+      } else {
+        const double zpN = ct * vN + st * ur, zpS = ct * vS + st * ur;
+        o.x = mrf * zpN; o.y = mrf * zpS;
+      }
+    } else {
+      o.x = 0; o.y = 0;
+    }
+    *at = o;
+  }
+  __syncthreads();
+  C* out = ct_passes<N, TB, 0, 1, C>(res, res == bufA ? bufB : bufA, tw);
+  const double scl = 2.0 * 3.14159265358979323846 / N;
+  const size_t gb = ((size_t)(oc * d.nr + r) * (M + 1)) * 2 * d.nth;
+  for (int e = threadIdx.x; e < (M + 1) * TB; e += kThreads) {
+    const int m = e / TB, ii = e - m * TB;
+    if (ii >= rows) continue;
+    const int ith = i0 + ii;
+    const C* row = out + ii * RS;
+    const C zk = row[pidx(m)];
+    C zn = row[pidx(m == 0 ? 0 : N - m)];
+    zn.y = -zn.y;
+    C X, Y;
+    X.x = 0.5 * (zk.x + zn.x); X.y = 0.5 * (zk.y + zn.y);
+    Y.x = 0.5 * (zk.y - zn.y); Y.y = -0.5 * (zk.x - zn.x);
+    C gn, gs;
+    gn.x = scl * X.x; gn.y = scl * X.y;
+    gs.x = scl * Y.x; gs.y = scl * Y.y;
+    const double wi = w[ith];
+    C gp, gm;
+    gp.x = wi * (gn.x + gs.x); gp.y = wi * (gn.y + gs.y);
+    gm.x = wi * (gn.x - gs.x); gm.y = wi * (gn.y - gs.y);
+    const size_t ip = gb + ((size_t)m * 2 + 0) * d.nth + ith, im = gb + ((size_t)m * 2 + 1) * d.nth + ith;
+    const float2 ap = g32[ip], am = g32[im];
+    G[ip] = make_double2(gp.x + (double)ap.x, gp.y + (double)ap.y);
+    G[im] = make_double2(gm.x + (double)am.x, gm.y + (double)am.y);
+  }
+}
+
+template <int N>
+static void launch_cor(cudaStream_t s, const Dims& d, const void* tw, const void* F, const double* cth,
+                       const double* sth, double rf, const double* w, const float2* g32, void* G) {
+  constexpr int RS = CtGeom<double, N>::RS, TB = CtGeom<double, N>::TB;
+  const size_t sm = (size_t)2 * TB * RS * sizeof(double2);
+  allow_dynamic_smem(k_coriolis_fused<N>, sm);
+  dim3 g(ceil_div(d.nth, TB), d.nr, 2);
+  k_coriolis_fused<N><<<g, kThreads, sm, s>>>(d, (const double2*)tw, (const double2*)F, cth, sth, rf, w, g32,
+                                              (double2*)G);
+}
+
+bool launch_coriolis_fused(cudaStream_t s, const Dims& d, int nlon, const void* tw, const void* F, const double* cth,
+                           const double* sth, double rf, const double* w, const float2* g32, void* G) {
+  switch (nlon) {
+    case 24: launch_cor<24>(s, d, tw, F, cth, sth, rf, w, g32, G); return true;
+    case 48: launch_cor<48>(s, d, tw, F, cth, sth, rf, w, g32, G); return true;
+    case 96: launch_cor<96>(s, d, tw, F, cth, sth, rf, w, g32, G); return true;
+    case 144: launch_cor<144>(s, d, tw, F, cth, sth, rf, w, g32, G); return true;
+    case 192: launch_cor<192>(s, d, tw, F, cth, sth, rf, w, g32, G); return true;
+    case 288: launch_cor<288>(s, d, tw, F, cth, sth, rf, w, g32, G); return true;
+    case 384: launch_cor<384>(s, d, tw, F, cth, sth, rf, w, g32, G); return true;
+    case 768: launch_cor<768>(s, d, tw, F, cth, sth, rf, w, g32, G); return true;
+    default: return false;
+  }
+}
+
 template <typename RT, int N>
 static bool launch_ct(cudaStream_t s, const Dims& d, const void* tw, const void* F, RT* grid, size_t stride,
                       int ncomp, bool synth, const double* w) {

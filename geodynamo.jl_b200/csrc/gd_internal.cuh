@@ -54,6 +54,11 @@ struct SynthArgs {
   const double* coef[4]; // scalar: nf fields ; vector: [0] = S (poloidal), [1] = T (toroidal)
   double2* out;          // Fourier buffer, comps consecutive
   int nf;                // scalar: number of fields (comps) ; vector: 1 (outputs 2 comps)
+  // vector only, may be null: also write the components as FP32 in the mixed
+  // step's blocked layout (float4 north Re, north Im, south Re, south Im at
+  // [comp][r][theta block of 2][m][pair in block]); out32_comp = float4 per component
+  float4* out32;
+  size_t out32_comp;
 };
 void launch_synth_fp64(cudaStream_t s, const Dims& d, const int* moff, const SynthArgs& a, bool vec);
 
@@ -83,6 +88,12 @@ template <typename R>
 void launch_fft_analysis(cudaStream_t s, const Dims& d, const FftPlan& p, const void* twiddle, const R* grid,
                          size_t grid_comp_stride, const double* w, void* G, int ncomp);
 void make_twiddles(int n, std::vector<double>& tw);
+// The Coriolis term of the velocity phase in FP64 from the velocity's FP64
+// Fourier components F (comps u_theta, u_phi) to the folded transforms G
+// (comps theta, phi) plus the FP32 folds g32; false (nothing launched) for an
+// nlon without a compile-time plan.
+bool launch_coriolis_fused(cudaStream_t s, const Dims& d, int nlon, const void* tw, const void* F, const double* cth,
+                           const double* sth, double rf, const double* w, const float2* g32, void* G);
 
 // ---- nonlinear terms (gd_nonlinear.cu) ----
 template <typename R>

@@ -9,6 +9,8 @@
 // SHsphtor_to_spat / spat_to_SHsphtor as called per shell in
 // src/shtnskit_field_functions.jl:102-123, 218-239, 252-321, batched over all
 // shells and fields in one launch.
+#include <stdint.h>
+
 #include "gd_internal.cuh"
 
 namespace gd {
@@ -19,21 +21,47 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// Asynchronous global -> shared copies of the operand tiles.  Every CTA keeps
+// LEG_STAGES K chunks in flight: chunk c + LEG_STAGES - 1 is loading while
+// chunk c is multiplied, so the tensor pipe does not wait for global latency.
+// An invalid element (past the last degree, colatitude or column) is copied
+// with a source size of 0, which writes zeros and reads nothing.
+constexpr int LEG_STAGES = 3;
+
+__device__ __forceinline__ void cpa8(double* sdst, const double* gsrc, bool valid) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cpa16(double* sdst, const double* gsrc, bool valid) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Scalar synthesis: F_m(theta) = sum_l a_lm Pbar_lm(theta), all fields/shells.
-// CTA tile: 64 theta (north) x 64 columns n = (field, r, re/im).
+// CTA tile: 64 theta (north) x 64 columns n = (field, r, re/im); K chunks of
+// 32 degrees (16 per parity) in a LEG_STAGES-deep cp.async pipeline.
 // ---------------------------------------------------------------------------
 #define SS_TM 64
 #define SS_TN 64
 #define SS_KC 32
 #define SS_SA 66
 #define SS_SB 66
+constexpr int SS_STAGE = SS_KC * SS_SA + SS_KC * SS_SB;  // doubles per pipeline stage
 
-__global__ void __launch_bounds__(256) k_synth_scalar(Dims d, const int* __restrict__ moff,
-                                                      const double* __restrict__ P, SynthArgs a) {
-  __shared__ double smem[SS_KC * SS_SA + SS_KC * SS_SB];
-  double* As = smem;                   // [q][theta]
-  double* Bs = smem + SS_KC * SS_SA;   // [q][n]
+static size_t synth_scalar_smem() { return (size_t)LEG_STAGES * SS_STAGE * sizeof(double) + SS_TN * sizeof(void*); }
+
+__global__ void __launch_bounds__(256, 2) k_synth_scalar(Dims d, const int* __restrict__ moff,
+                                                         const double* __restrict__ P, SynthArgs a) {
+  extern __shared__ double smem[];
+  // column n -> pointer to its coefficients of order m at degree 0 (null past the last column)
+  const double** colp = reinterpret_cast<const double**>(smem + LEG_STAGES * SS_STAGE);
   const int m = blockIdx.z;
   const int th0 = blockIdx.y * SS_TM;
   const int n0 = blockIdx.x * SS_TN;
@@ -45,6 +73,35 @@ __global__ void __launch_bounds__(256) k_synth_scalar(Dims d, const int* __restr
   const int g = lane >> 2, t = lane & 3;
   const int mb = moff[m];
   const size_t NM = (size_t)d.nlm;
+  for (int n = tid; n < SS_TN; n += 256) {
+    const int ng = n0 + n;
+    const double* p = nullptr;
+    if (ng < Ntot) {
+      const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, c = rem & 1;
+      p = a.coef[f] + ((size_t)c * d.nr + r) * NM + mb - m;
+    }
+    colp[n] = p;
+  }
+  __syncthreads();
+  const int nch = (d.L - m + SS_KC) / SS_KC;  // K chunks of this order
+  auto load = [&](int ch) {
+    double* As = smem + (ch % LEG_STAGES) * SS_STAGE;  // [q][theta]
+    double* Bs = As + SS_KC * SS_SA;                    // [q][n]
+    const int l0 = m + ch * SS_KC;
+    for (int e = tid; e < SS_KC * SS_TM; e += 256) {
+      const int q = e / SS_TM, th = e % SS_TM;
+      const int l = l0 + q, ith = th0 + th;
+      const bool ok = l <= d.L && ith < d.nth;
+      cpa8(As + q * SS_SA + th, ok ? P + (size_t)(mb + l - m) * d.nth + ith : P, ok);
+    }
+    for (int e = tid; e < SS_KC * SS_TN; e += 256) {
+      const int q = e % SS_KC, n = e / SS_KC;
+      const int l = l0 + q;
+      const double* c = colp[n];
+      const bool ok = c != nullptr && l <= d.L;
+      cpa8(Bs + q * SS_SB + n, ok ? c + l : P, ok);
+    }
+  };
 
   double acc[4][4][2];
 #pragma unroll
@@ -52,27 +109,18 @@ __global__ void __launch_bounds__(256) k_synth_scalar(Dims d, const int* __restr
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-  for (int l0 = m; l0 <= d.L; l0 += SS_KC) {
-    // table tile
-    for (int e = tid; e < SS_KC * SS_TM; e += 256) {
-      const int q = e / SS_TM, th = e % SS_TM;
-      const int l = l0 + q, ith = th0 + th;
-      double v = 0.0;
-      if (l <= d.L && ith < d.nth) v = P[(size_t)(mb + l - m) * d.nth + ith];
-      As[q * SS_SA + th] = v;
-    }
-    // coefficient tile
-    for (int e = tid; e < SS_KC * SS_TN; e += 256) {
-      const int q = e % SS_KC, n = e / SS_KC;
-      const int l = l0 + q, ng = n0 + n;
-      double v = 0.0;
-      if (l <= d.L && ng < Ntot) {
-        const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, c = rem & 1;
-        v = a.coef[f][((size_t)c * d.nr + r) * NM + mb + (l - m)];
-      }
-      Bs[q * SS_SB + n] = v;
-    }
-    __syncthreads();
+#pragma unroll
+  for (int c = 0; c < LEG_STAGES - 1; ++c) {
+    if (c < nch) load(c);
+    cpa_commit();
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    cpa_wait<LEG_STAGES - 2>();
+    __syncthreads();  // chunk ch landed; every warp is done with chunk ch - 1's stage
+    if (ch + LEG_STAGES - 1 < nch) load(ch + LEG_STAGES - 1);
+    cpa_commit();
+    const double* As = smem + (ch % LEG_STAGES) * SS_STAGE;
+    const double* Bs = As + SS_KC * SS_SA;
 #pragma unroll
     for (int kk = 0; kk < SS_KC / 8; ++kk) {
       const int q = 2 * (4 * kk + t) + par;
@@ -86,8 +134,9 @@ __global__ void __launch_bounds__(256) k_synth_scalar(Dims d, const int* __restr
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
-    __syncthreads();
   }
+  cpa_wait<0>();
+  __syncthreads();
   // combine parities through shared memory
   double* Es = smem;  // [wq][i][j][lane][2]
   if (par == 1) {
@@ -125,20 +174,25 @@ __global__ void __launch_bounds__(256) k_synth_scalar(Dims d, const int* __restr
 // ---------------------------------------------------------------------------
 // Vector synthesis (spheroidal S = poloidal, toroidal T):
 //   V_theta = sum dP S + i sum Q T,   V_phi = i sum Q S - sum dP T.
-// CTA tile: 32 theta x 32 columns n = (r, re/im); tables {dP, Q} x fields {S, T}.
+// CTA tile: 32 theta x 32 columns n = (r, re/im); tables {dP, Q} x fields
+// {S, T}; pipelined like the scalar synthesis.
 // ---------------------------------------------------------------------------
 #define VS_TM 32
 #define VS_TN 32
 #define VS_KC 32
 #define VS_SA 34
 #define VS_SB 34
+constexpr int VS_STAGE = 2 * VS_KC * VS_SA + 2 * VS_KC * VS_SB;
 
-__global__ void __launch_bounds__(256) k_synth_vector(Dims d, const int* __restrict__ moff,
-                                                      const double* __restrict__ dP,
-                                                      const double* __restrict__ Q, SynthArgs a) {
-  __shared__ double smem[2 * VS_KC * VS_SA + 2 * VS_KC * VS_SB];
-  double* As = smem;                       // [tab][q][theta]
-  double* Bs = smem + 2 * VS_KC * VS_SA;   // [fld][q][n]
+static size_t synth_vector_smem() {
+  return (size_t)LEG_STAGES * VS_STAGE * sizeof(double) + 2 * VS_TN * sizeof(void*);
+}
+
+__global__ void __launch_bounds__(256, 2) k_synth_vector(Dims d, const int* __restrict__ moff,
+                                                         const double* __restrict__ dP,
+                                                         const double* __restrict__ Q, SynthArgs a) {
+  extern __shared__ double smem[];
+  const double** colp = reinterpret_cast<const double**>(smem + LEG_STAGES * VS_STAGE);  // [fld][n]
   const int m = blockIdx.z;
   const int th0 = blockIdx.y * VS_TM;
   const int n0 = blockIdx.x * VS_TN;
@@ -150,6 +204,33 @@ __global__ void __launch_bounds__(256) k_synth_vector(Dims d, const int* __restr
   const int g = lane >> 2, t = lane & 3;
   const int mb = moff[m];
   const size_t NM = (size_t)d.nlm;
+  for (int e = tid; e < 2 * VS_TN; e += 256) {
+    const int fld = e / VS_TN, ng = n0 + e % VS_TN;
+    colp[e] = ng < Ntot ? a.coef[fld] + ((size_t)(ng & 1) * d.nr + (ng >> 1)) * NM + mb - m : nullptr;
+  }
+  __syncthreads();
+  const int nch = (d.L - m + VS_KC) / VS_KC;
+  auto load = [&](int ch) {
+    double* As = smem + (ch % LEG_STAGES) * VS_STAGE;  // [tab][q][theta]
+    double* Bs = As + 2 * VS_KC * VS_SA;                // [fld][q][n]
+    const int l0 = m + ch * VS_KC;
+    for (int e = tid; e < 2 * VS_KC * VS_TM; e += 256) {
+      const int tab = e / (VS_KC * VS_TM), rem = e % (VS_KC * VS_TM);
+      const int q = rem / VS_TM, th = rem % VS_TM;
+      const int l = l0 + q, ith = th0 + th;
+      const bool ok = l <= d.L && ith < d.nth;
+      const double* T = tab == 0 ? dP : Q;
+      cpa8(As + (tab * VS_KC + q) * VS_SA + th, ok ? T + (size_t)(mb + l - m) * d.nth + ith : T, ok);
+    }
+    for (int e = tid; e < 2 * VS_KC * VS_TN; e += 256) {
+      const int fld = e / (VS_KC * VS_TN), rem = e % (VS_KC * VS_TN);
+      const int q = rem % VS_KC, n = rem / VS_KC;
+      const int l = l0 + q;
+      const double* c = colp[fld * VS_TN + n];
+      const bool ok = c != nullptr && l <= d.L;
+      cpa8(Bs + (fld * VS_KC + q) * VS_SB + n, ok ? c + l : dP, ok);
+    }
+  };
 
   double acc[2][2][2][2][2];  // [tab][fld][i][j][re/im]
 #pragma unroll
@@ -161,27 +242,18 @@ __global__ void __launch_bounds__(256) k_synth_vector(Dims d, const int* __restr
 #pragma unroll
         for (int j = 0; j < 2; ++j) acc[x][y][i][j][0] = acc[x][y][i][j][1] = 0.0;
 
-  for (int l0 = m; l0 <= d.L; l0 += VS_KC) {
-    for (int e = tid; e < 2 * VS_KC * VS_TM; e += 256) {
-      const int tab = e / (VS_KC * VS_TM), rem = e % (VS_KC * VS_TM);
-      const int q = rem / VS_TM, th = rem % VS_TM;
-      const int l = l0 + q, ith = th0 + th;
-      double v = 0.0;
-      if (l <= d.L && ith < d.nth) v = (tab == 0 ? dP : Q)[(size_t)(mb + l - m) * d.nth + ith];
-      As[(tab * VS_KC + q) * VS_SA + th] = v;
-    }
-    for (int e = tid; e < 2 * VS_KC * VS_TN; e += 256) {
-      const int fld = e / (VS_KC * VS_TN), rem = e % (VS_KC * VS_TN);
-      const int q = rem % VS_KC, n = rem / VS_KC;
-      const int l = l0 + q, ng = n0 + n;
-      double v = 0.0;
-      if (l <= d.L && ng < Ntot) {
-        const int r = ng >> 1, c = ng & 1;
-        v = a.coef[fld][((size_t)c * d.nr + r) * NM + mb + (l - m)];
-      }
-      Bs[(fld * VS_KC + q) * VS_SB + n] = v;
-    }
+#pragma unroll
+  for (int c = 0; c < LEG_STAGES - 1; ++c) {
+    if (c < nch) load(c);
+    cpa_commit();
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    cpa_wait<LEG_STAGES - 2>();
     __syncthreads();
+    if (ch + LEG_STAGES - 1 < nch) load(ch + LEG_STAGES - 1);
+    cpa_commit();
+    const double* As = smem + (ch % LEG_STAGES) * VS_STAGE;
+    const double* Bs = As + 2 * VS_KC * VS_SA;
 #pragma unroll
     for (int kk = 0; kk < VS_KC / 8; ++kk) {
       const int q = 2 * (4 * kk + t) + par;
@@ -203,8 +275,9 @@ __global__ void __launch_bounds__(256) k_synth_vector(Dims d, const int* __restr
 #pragma unroll
             for (int j = 0; j < 2; ++j) dmma(acc[x][y][i][j][0], acc[x][y][i][j][1], af[x][i], bf[y][j]);
     }
-    __syncthreads();
   }
+  cpa_wait<0>();
+  __syncthreads();
   double* Es = smem;  // [wq][16 tiles][lane][2]
   if (par == 1) {
     int k = 0;
@@ -223,20 +296,6 @@ __global__ void __launch_bounds__(256) k_synth_vector(Dims d, const int* __restr
   }
   __syncthreads();
   if (par == 0) {
-    double odd[2][2][2][2][2];
-    int k = 0;
-#pragma unroll
-    for (int x = 0; x < 2; ++x)
-#pragma unroll
-      for (int y = 0; y < 2; ++y)
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int j = 0; j < 2; ++j, ++k) {
-            const int o = ((wq * 16 + k) * 32 + lane) * 2;
-            odd[x][y][i][j][0] = Es[o];
-            odd[x][y][i][j][1] = Es[o + 1];
-          }
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       const int ith = th0 + thw + 8 * i + g;
@@ -246,16 +305,27 @@ __global__ void __launch_bounds__(256) k_synth_vector(Dims d, const int* __restr
         const int ng = n0 + nw + 8 * j + 2 * t;
         if (ng >= Ntot) continue;
         const int r = ng >> 1;
+        // the odd-parity partial sums of this (i, j) tile, [tab][fld][re/im]
+        double odd[2][2][1][1][2];
+#pragma unroll
+        for (int x = 0; x < 2; ++x)
+#pragma unroll
+          for (int y = 0; y < 2; ++y) {
+            const int o = ((wq * 16 + ((x * 2 + y) * 2 + i) * 2 + j) * 32 + lane) * 2;
+            odd[x][y][0][0][0] = Es[o];
+            odd[x][y][0][0][1] = Es[o + 1];
+          }
+        double2 v32[2][2];  // [comp][s]: the values of the blocked FP32 copy
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
           // tab 0 = dP (parity opposite to P), tab 1 = Q (parity of P); fld 0 = S, 1 = T
           double DS[2], DT[2], QS[2], QT[2];
 #pragma unroll
           for (int c = 0; c < 2; ++c) {
-            const double eDS = acc[0][0][i][j][c], oDS = odd[0][0][i][j][c];
-            const double eDT = acc[0][1][i][j][c], oDT = odd[0][1][i][j][c];
-            const double eQS = acc[1][0][i][j][c], oQS = odd[1][0][i][j][c];
-            const double eQT = acc[1][1][i][j][c], oQT = odd[1][1][i][j][c];
+            const double eDS = acc[0][0][i][j][c], oDS = odd[0][0][0][0][c];
+            const double eDT = acc[0][1][i][j][c], oDT = odd[0][1][0][0][c];
+            const double eQS = acc[1][0][i][j][c], oQS = odd[1][0][0][0][c];
+            const double eQT = acc[1][1][i][j][c], oQT = odd[1][1][0][0][c];
             if (s == 0) {
               DS[c] = eDS + oDS; DT[c] = eDT + oDT; QS[c] = eQS + oQS; QT[c] = eQT + oQT;
             } else {
@@ -268,6 +338,16 @@ __global__ void __launch_bounds__(256) k_synth_vector(Dims d, const int* __restr
           const size_t b1 = (((size_t)(1 * d.nr + r) * (d.M + 1) + m) * 2 + s) * d.nth + ith;
           a.out[b0] = vth;
           a.out[b1] = vph;
+          v32[0][s] = vth;
+          v32[1][s] = vph;
+        }
+        if (a.out32 != nullptr) {
+          const size_t run = (size_t)((d.nth + 1) / 2) * (d.M + 1) * 2;
+          const size_t off = (size_t)r * run + ((size_t)(ith >> 1) * (d.M + 1) + m) * 2 + (ith & 1);
+#pragma unroll
+          for (int c = 0; c < 2; ++c)
+            a.out32[c * a.out32_comp + off] = make_float4((float)v32[c][0].x, (float)v32[c][0].y,
+                                                          (float)v32[c][1].x, (float)v32[c][1].y);
         }
       }
     }
@@ -277,30 +357,38 @@ __global__ void __launch_bounds__(256) k_synth_vector(Dims d, const int* __restr
 void launch_synth_fp64(cudaStream_t s, const Dims& d, const int* moff, const SynthArgs& a, bool vec) {
   if (!vec) {
     dim3 grid(ceil_div(a.nf * d.nr * 2, SS_TN), ceil_div(d.nth, SS_TM), d.M + 1);
-    k_synth_scalar<<<grid, 256, 0, s>>>(d, moff, a.table0, a);
+    allow_dynamic_smem(k_synth_scalar, synth_scalar_smem());
+    k_synth_scalar<<<grid, 256, synth_scalar_smem(), s>>>(d, moff, a.table0, a);
   } else {
     dim3 grid(ceil_div(d.nr * 2, VS_TN), ceil_div(d.nth, VS_TM), d.M + 1);
-    k_synth_vector<<<grid, 256, 0, s>>>(d, moff, a.table0, a.table1, a);
+    allow_dynamic_smem(k_synth_vector, synth_vector_smem());
+    k_synth_vector<<<grid, 256, synth_vector_smem(), s>>>(d, moff, a.table0, a.table1, a);
   }
 }
 
 // ---------------------------------------------------------------------------
 // Scalar analysis: a_lm = sum_{north theta} Pbar_lm(theta) G_{s(l-m)}(theta),
 // with G_+ = w (G_N + G_S), G_- = w (G_N - G_S) prepared by the phi transform.
-// CTA tile: 64 consecutive l (32 per parity) x 128 columns n = (field, r, re/im).
+// CTA tile: 64 consecutive l (32 per parity) x 64 columns n = (field, r,
+// re/im); K = colatitude in chunks of 16, pipelined.
 // ---------------------------------------------------------------------------
 #define SA_TL 64
-#define SA_TN 128
+#define SA_TN 64
 #define SA_KC 16
 #define SA_SA 18
-#define SA_SB 132
+#define SA_SB 68
 #define SA_SO 66
+constexpr int SA_STAGE = SA_TL * SA_SA + 2 * SA_KC * SA_SB;
 
-__global__ void __launch_bounds__(256) k_analysis_scalar(Dims d, const int* __restrict__ moff,
-                                                         const double* __restrict__ P, AnalysisArgs a) {
-  __shared__ double smem[SA_TL * SA_SA + 2 * SA_KC * SA_SB];
-  double* As = smem;                   // [l][theta]
-  double* Bs = smem + SA_TL * SA_SA;   // [s][theta][n]
+static size_t analysis_scalar_smem() {
+  return (size_t)LEG_STAGES * SA_STAGE * sizeof(double) + (SA_TN / 2) * sizeof(long long);
+}
+
+__global__ void __launch_bounds__(256, 2) k_analysis_scalar(Dims d, const int* __restrict__ moff,
+                                                            const double* __restrict__ P, AnalysisArgs a) {
+  extern __shared__ double smem[];
+  // column pair -> offset of its folded input of order m (-1 past the last column)
+  long long* colin = reinterpret_cast<long long*>(smem + LEG_STAGES * SA_STAGE);
   const int m = blockIdx.z;
   const int l0 = m + blockIdx.y * SA_TL;
   const int n0 = blockIdx.x * SA_TN;
@@ -308,91 +396,108 @@ __global__ void __launch_bounds__(256) k_analysis_scalar(Dims d, const int* __re
   if (l0 > d.L || n0 >= Ntot) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int par = warp >> 2, wq = warp & 3;
-  const int lw = (wq >> 1) * 16, nw = (wq & 1) * 64;
+  const int lw = (wq >> 1) * 16, nw = (wq & 1) * 32;
   const int g = lane >> 2, t = lane & 3;
   const int mb = moff[m];
   const size_t NM = (size_t)d.nlm;
   const int npairs = Ntot / 2;
-
-  double acc[2][8][2];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  for (int k0 = 0; k0 < d.nth; k0 += SA_KC) {
+  for (int pr = tid; pr < SA_TN / 2; pr += 256) {
+    const int pg = n0 / 2 + pr;
+    long long ib = -1;
+    if (pg < npairs) {
+      const int f = pg / d.nr, r = pg % d.nr;
+      ib = (long long)(((size_t)(f * d.nr + r) * (d.M + 1) + m) * 2) * d.nth;
+    }
+    colin[pr] = ib;
+  }
+  __syncthreads();
+  const double* Gin = reinterpret_cast<const double*>(a.in);
+  const int nch = (d.nth + SA_KC - 1) / SA_KC;
+  auto load = [&](int ch) {
+    double* As = smem + (ch % LEG_STAGES) * SA_STAGE;  // [l][theta]
+    double* Bs = As + SA_TL * SA_SA;                    // [s][theta][n]
+    const int k0 = ch * SA_KC;
     for (int e = tid; e < SA_TL * SA_KC; e += 256) {
       const int lq = e / SA_KC, th = e % SA_KC;
       const int l = l0 + lq, ith = k0 + th;
-      double v = 0.0;
-      if (l <= d.L && ith < d.nth) v = P[(size_t)(mb + l - m) * d.nth + ith];
-      As[lq * SA_SA + th] = v;
+      const bool ok = l <= d.L && ith < d.nth;
+      cpa8(As + lq * SA_SA + th, ok ? P + (size_t)(mb + l - m) * d.nth + ith : P, ok);
     }
     for (int e = tid; e < 2 * SA_KC * (SA_TN / 2); e += 256) {
       const int th = e % SA_KC, rest = e / SA_KC;
-      const int s = rest & 1, pr = rest >> 1;  // pr = column pair within tile
-      const int pg = n0 / 2 + pr, ith = k0 + th;
-      double2 v = make_double2(0.0, 0.0);
-      if (pg < npairs && ith < d.nth) {
-        const int f = pg / d.nr, r = pg % d.nr;
-        v = a.in[(((size_t)(f * d.nr + r) * (d.M + 1) + m) * 2 + s) * d.nth + ith];
-      }
-      Bs[(s * SA_KC + th) * SA_SB + 2 * pr] = v.x;
-      Bs[(s * SA_KC + th) * SA_SB + 2 * pr + 1] = v.y;
+      const int sp = rest & 1, pr = rest >> 1;  // pr = column pair within tile
+      const int ith = k0 + th;
+      const long long ib = colin[pr];
+      const bool ok = ib >= 0 && ith < d.nth;
+      cpa16(Bs + (sp * SA_KC + th) * SA_SB + 2 * pr, ok ? Gin + 2 * ((size_t)ib + (size_t)sp * d.nth + ith) : Gin,
+            ok);
     }
+  };
+
+  double acc[2][4][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+  for (int c = 0; c < LEG_STAGES - 1; ++c) {
+    if (c < nch) load(c);
+    cpa_commit();
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    cpa_wait<LEG_STAGES - 2>();
     __syncthreads();
+    if (ch + LEG_STAGES - 1 < nch) load(ch + LEG_STAGES - 1);
+    cpa_commit();
+    const double* As = smem + (ch % LEG_STAGES) * SA_STAGE;
+    const double* Bs = As + SA_TL * SA_SA;
 #pragma unroll
     for (int kk = 0; kk < SA_KC / 4; ++kk) {
       const int th = 4 * kk + t;
-      double af[2], bf[8];
+      double af[2], bf[4];
 #pragma unroll
       for (int i = 0; i < 2; ++i) af[i] = As[(2 * (lw + 8 * i + g) + par) * SA_SA + th];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) bf[j] = Bs[(par * SA_KC + 4 * kk + (t)) * SA_SB + nw + 8 * j + g];
+      for (int j = 0; j < 4; ++j) bf[j] = Bs[(par * SA_KC + th) * SA_SB + nw + 8 * j + g];
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
-    __syncthreads();
   }
-  // stage [n][l] in shared memory, half of the n tile at a time, then write
-  // contiguous l runs of each output plane.
+  cpa_wait<0>();
+  __syncthreads();
+  // stage [n][l] in shared memory, then write contiguous l runs of each output plane
   double* Os = smem;  // [64 n][SA_SO]
-  for (int half = 0; half < 2; ++half) {
-    if ((nw >> 6) == half) {
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int lq = 2 * (lw + 8 * i + g) + par;
-        const int l = l0 + lq;
+  for (int i = 0; i < 2; ++i) {
+    const int lq = 2 * (lw + 8 * i + g) + par;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int nl = 8 * j + 2 * t;  // within the half
-          double re = acc[i][j][0], im = acc[i][j][1];
-          if (m == 0) im = 0.0;  // store_coefficients_from_shtnskit!, :433-435
-          (void)l;
-          Os[nl * SA_SO + lq] = re;
-          Os[(nl + 1) * SA_SO + lq] = im;
-        }
-      }
+    for (int j = 0; j < 4; ++j) {
+      const int nl = nw + 8 * j + 2 * t;
+      double re = acc[i][j][0], im = acc[i][j][1];
+      if (m == 0) im = 0.0;  // store_coefficients_from_shtnskit!, :433-435
+      Os[nl * SA_SO + lq] = re;
+      Os[(nl + 1) * SA_SO + lq] = im;
     }
-    __syncthreads();
-    for (int e = tid; e < 64 * SA_TL; e += 256) {
-      const int lq = e % SA_TL, nl = e / SA_TL;
-      const int ng = n0 + half * 64 + nl, l = l0 + lq;
-      if (ng < Ntot && l <= d.L) {
-        const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, c = rem & 1;
-        a.out[f][((size_t)c * d.nr + r) * NM + mb + (l - m)] = Os[nl * SA_SO + lq];
-      }
+  }
+  __syncthreads();
+  for (int e = tid; e < SA_TN * SA_TL; e += 256) {
+    const int lq = e % SA_TL, nl = e / SA_TL;
+    const int ng = n0 + nl, l = l0 + lq;
+    if (ng < Ntot && l <= d.L) {
+      const int f = ng / (2 * d.nr), rem = ng % (2 * d.nr), r = rem >> 1, c = rem & 1;
+      a.out[f][((size_t)c * d.nr + r) * NM + mb + (l - m)] = Os[nl * SA_SO + lq];
     }
-    __syncthreads();
   }
 }
 
 // ---------------------------------------------------------------------------
 // Vector analysis (spat_to_SHsphtor):
 //   S = [sum dP G_th - i sum Q G_ph] / l(l+1),  T = [-i sum Q G_th - sum dP G_ph] / l(l+1)
-// where the dP terms use the fold of opposite parity.  Columns n = (r, re/im).
+// where the dP terms use the fold of opposite parity.  Columns n = (r, re/im);
+// pipelined like the scalar analysis.
 // ---------------------------------------------------------------------------
 #define VA_TL 64
 #define VA_TN 32
@@ -400,13 +505,14 @@ __global__ void __launch_bounds__(256) k_analysis_scalar(Dims d, const int* __re
 #define VA_SA 18
 #define VA_SB 36
 #define VA_SO 66
+constexpr int VA_STAGE = 2 * VA_TL * VA_SA + 4 * VA_KC * VA_SB;
 
-__global__ void __launch_bounds__(256) k_analysis_vector(Dims d, const int* __restrict__ moff,
-                                                         const double* __restrict__ dP,
-                                                         const double* __restrict__ Q, AnalysisArgs a) {
-  __shared__ double smem[2 * VA_TL * VA_SA + 4 * VA_KC * VA_SB];
-  double* As = smem;                        // [tab][l][theta]
-  double* Bs = smem + 2 * VA_TL * VA_SA;    // [comp][s][theta][n]
+static size_t analysis_vector_smem() { return (size_t)LEG_STAGES * VA_STAGE * sizeof(double); }
+
+__global__ void __launch_bounds__(256, 2) k_analysis_vector(Dims d, const int* __restrict__ moff,
+                                                            const double* __restrict__ dP,
+                                                            const double* __restrict__ Q, AnalysisArgs a) {
+  extern __shared__ double smem[];
   const int m = blockIdx.z;
   const int l0 = m + blockIdx.y * VA_TL;
   const int n0 = blockIdx.x * VA_TN;
@@ -419,6 +525,30 @@ __global__ void __launch_bounds__(256) k_analysis_vector(Dims d, const int* __re
   const int mb = moff[m];
   const size_t NM = (size_t)d.nlm;
   const int sP = par, sD = 1 - par;
+  const double* Gin = reinterpret_cast<const double*>(a.in);
+  const int nch = (d.nth + VA_KC - 1) / VA_KC;
+  auto load = [&](int ch) {
+    double* As = smem + (ch % LEG_STAGES) * VA_STAGE;  // [tab][l][theta]
+    double* Bs = As + 2 * VA_TL * VA_SA;                // [comp][s][theta][n]
+    const int k0 = ch * VA_KC;
+    for (int e = tid; e < 2 * VA_TL * VA_KC; e += 256) {
+      const int tab = e / (VA_TL * VA_KC), rem = e % (VA_TL * VA_KC);
+      const int lq = rem / VA_KC, th = rem % VA_KC;
+      const int l = l0 + lq, ith = k0 + th;
+      const bool ok = l <= d.L && ith < d.nth;
+      const double* T = tab == 0 ? dP : Q;
+      cpa8(As + (tab * VA_TL + lq) * VA_SA + th, ok ? T + (size_t)(mb + l - m) * d.nth + ith : T, ok);
+    }
+    for (int e = tid; e < 4 * VA_KC * (VA_TN / 2); e += 256) {
+      const int th = e % VA_KC, rest = e / VA_KC;
+      const int cs = rest & 3, pr = rest >> 2;  // cs = comp*2 + s
+      const int comp = cs >> 1, sp = cs & 1;
+      const int r = n0 / 2 + pr, ith = k0 + th;
+      const bool ok = r < d.nr && ith < d.nth;
+      const size_t at = (((size_t)(comp * d.nr + r) * (d.M + 1) + m) * 2 + sp) * d.nth + ith;
+      cpa16(Bs + (cs * VA_KC + th) * VA_SB + 2 * pr, ok ? Gin + 2 * at : Gin, ok);
+    }
+  };
 
   // acc[prod][i][j][c], prod: 0 = dP.Gth, 1 = dP.Gph, 2 = Q.Gth, 3 = Q.Gph
   double acc[4][2][2][2];
@@ -429,27 +559,18 @@ __global__ void __launch_bounds__(256) k_analysis_vector(Dims d, const int* __re
 #pragma unroll
       for (int j = 0; j < 2; ++j) acc[p][i][j][0] = acc[p][i][j][1] = 0.0;
 
-  for (int k0 = 0; k0 < d.nth; k0 += VA_KC) {
-    for (int e = tid; e < 2 * VA_TL * VA_KC; e += 256) {
-      const int tab = e / (VA_TL * VA_KC), rem = e % (VA_TL * VA_KC);
-      const int lq = rem / VA_KC, th = rem % VA_KC;
-      const int l = l0 + lq, ith = k0 + th;
-      double v = 0.0;
-      if (l <= d.L && ith < d.nth) v = (tab == 0 ? dP : Q)[(size_t)(mb + l - m) * d.nth + ith];
-      As[(tab * VA_TL + lq) * VA_SA + th] = v;
-    }
-    for (int e = tid; e < 4 * VA_KC * (VA_TN / 2); e += 256) {
-      const int th = e % VA_KC, rest = e / VA_KC;
-      const int cs = rest & 3, pr = rest >> 2;  // cs = comp*2 + s
-      const int comp = cs >> 1, s = cs & 1;
-      const int r = n0 / 2 + pr, ith = k0 + th;
-      double2 v = make_double2(0.0, 0.0);
-      if (r < d.nr && ith < d.nth)
-        v = a.in[(((size_t)(comp * d.nr + r) * (d.M + 1) + m) * 2 + s) * d.nth + ith];
-      Bs[(cs * VA_KC + th) * VA_SB + 2 * pr] = v.x;
-      Bs[(cs * VA_KC + th) * VA_SB + 2 * pr + 1] = v.y;
-    }
+#pragma unroll
+  for (int c = 0; c < LEG_STAGES - 1; ++c) {
+    if (c < nch) load(c);
+    cpa_commit();
+  }
+  for (int ch = 0; ch < nch; ++ch) {
+    cpa_wait<LEG_STAGES - 2>();
     __syncthreads();
+    if (ch + LEG_STAGES - 1 < nch) load(ch + LEG_STAGES - 1);
+    cpa_commit();
+    const double* As = smem + (ch % LEG_STAGES) * VA_STAGE;
+    const double* Bs = As + 2 * VA_TL * VA_SA;
 #pragma unroll
     for (int kk = 0; kk < VA_KC / 4; ++kk) {
       const int th = 4 * kk + t;
@@ -478,8 +599,9 @@ __global__ void __launch_bounds__(256) k_analysis_vector(Dims d, const int* __re
           dmma(acc[3][i][j][0], acc[3][i][j][1], aQ[i], bph[1][j]);
         }
     }
-    __syncthreads();
   }
+  cpa_wait<0>();
+  __syncthreads();
   double* Os = smem;  // [out field][32 n][VA_SO]
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
@@ -524,10 +646,12 @@ __global__ void __launch_bounds__(256) k_analysis_vector(Dims d, const int* __re
 void launch_analysis_fp64(cudaStream_t s, const Dims& d, const int* moff, const AnalysisArgs& a) {
   if (a.epi == EPI_SCALAR) {
     dim3 grid(ceil_div(a.nf * d.nr * 2, SA_TN), ceil_div(d.L + 1, SA_TL), d.M + 1);
-    k_analysis_scalar<<<grid, 256, 0, s>>>(d, moff, a.table0, a);
+    allow_dynamic_smem(k_analysis_scalar, analysis_scalar_smem());
+    k_analysis_scalar<<<grid, 256, analysis_scalar_smem(), s>>>(d, moff, a.table0, a);
   } else {
     dim3 grid(ceil_div(d.nr * 2, VA_TN), ceil_div(d.L + 1, VA_TL), d.M + 1);
-    k_analysis_vector<<<grid, 256, 0, s>>>(d, moff, a.table0, a.table1, a);
+    allow_dynamic_smem(k_analysis_vector, analysis_vector_smem());
+    k_analysis_vector<<<grid, 256, analysis_vector_smem(), s>>>(d, moff, a.table0, a.table1, a);
   }
 }
 

@@ -295,6 +295,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
   const uint32_t tmem = *tslot;
   const int ntiles = (d.M + 1) * ntt * ncol;
   bool ok = true;
+  int issued = -1;  // producer: last pipeline step whose bulk copies were issued
 
   if (warp == 0) {
     // producer: bulk copies only.  Step (tile tt, it): table chunk(s) and the
@@ -317,17 +318,20 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
       s1 = imgD + ch * CHUNK_FLOATS;
       sb = a.bimg + bch * (2L * BT);
     };
-    int gs = 0, issued = -1;
+    int gs = 0;
     for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
       const int m = tt / (ntt * ncol);
       const int nc1 = nck_h(L, m, 1), T = nck_h(L, m, 0) + nc1;
       for (int it = 0; it < T; ++it) {
         const int G = gs + it, s = G & 1, u = G >> 1;
-        if (u >= 1 && !mbar_wait(&empty[s], (u - 1) & 1, a.err)) {
+        if (u >= 1 && !mbar_wait(&empty[s], (u - 1) & 1, a.err, a.wait_limit)) {
           ok = false;
           break;
         }
-        if (lane == 0) {
+        // error-path tests: CTA 0 may omit one step's copies, so the MMA
+        // warp's bounded wait on that stage runs out
+        const bool omit = a.omit_plus1 == G + 1 && blockIdx.x == 0;
+        if (lane == 0 && !omit) {
           float* A = stg + s * ST_FL;
           const float *s0, *s1, *sb;
           uint32_t pa, pb;
@@ -342,13 +346,11 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
           bulk_g2s(A + A_FL, sb, pb, &full[s]);
           bulk_g2s(A + A_FL + BT, sb + BT, pb, &full[s]);
         }
-        issued = G;
+        if (!omit) issued = G;
         __syncwarp();
       }
       gs += T;
     }
-    // after an expired wait, let the last bulk copies land before the CTA exits
-    if (!ok && issued >= 0) mbar_wait(&full[issued & 1], (issued >> 1) & 1, a.err);
   } else if (warp == 1) {
     // MMA issuer
     int gs = 0, q = 0;
@@ -357,13 +359,13 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
       const int nc1 = nck_h(L, m, 1), T = nck_h(L, m, 0) + nc1;
       const int nvalid = VEC ? 4 * min(32, d.nr - ct * 32) : min(NCS, Ntot - ct * NCS);
       const uint32_t ids = idesc_tf32(TC_M, (nvalid + 15) & ~15);
-      if (q >= 1 && !mbar_wait(tempty, (q - 1) & 1, a.err)) {
+      if (q >= 1 && !mbar_wait(tempty, (q - 1) & 1, a.err, a.wait_limit)) {
         ok = false;
         break;
       }
       for (int it = 0; it < T; ++it) {
         const int G = gs + it, s = G & 1;
-        if (!mbar_wait(&full[s], (G >> 1) & 1, a.err)) {
+        if (!mbar_wait(&full[s], (G >> 1) & 1, a.err, a.wait_limit)) {
           ok = false;
           break;
         }
@@ -394,7 +396,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
     for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x, ++q) {
       const int m = tt / (ntt * ncol), tile = (tt / ncol) % ntt, ct = tt % ncol;
       const int nc1 = nck_h(L, m, 1);
-      if (!mbar_wait(tfull, q & 1, a.err)) {
+      if (!mbar_wait(tfull, q & 1, a.err, a.wait_limit)) {
         ok = false;
         break;
       }
@@ -482,6 +484,10 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
     }
   }
   ok = __syncthreads_and(ok);
+  // after an expired wait anywhere in the CTA, the producer lets its last
+  // bulk copies land before the CTA exits (a step the MMA warp consumed has
+  // completed its phase already, so this returns at once)
+  if (!ok && warp == 0 && issued >= 0) mbar_wait(&full[issued & 1], (issued >> 1) & 1, a.err, a.wait_limit);
   fence_after_sync();
   if (warp == 0) tmem_dealloc(tmem, NCOL);
 }
@@ -618,7 +624,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
     if (it < T) load_step(it);
     for (; it < T; it += 2) {
       const int u = (gs + it) >> 1;
-      if (u >= 1 && !mbar_wait(&empty[g], (u - 1) & 1, a.err)) {
+      if (u >= 1 && !mbar_wait(&empty[g], (u - 1) & 1, a.err, a.wait_limit)) {
         ok = false;
         break;
       }
@@ -657,7 +663,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   } else {
     for (int it = 0; it < T; ++it) {
       const int s = (gs + it) & 1;
-      if (!mbar_wait(&full[s], ((gs + it) >> 1) & 1, a.err)) {
+      if (!mbar_wait(&full[s], ((gs + it) >> 1) & 1, a.err, a.wait_limit)) {
         ok = false;
         break;
       }
@@ -682,7 +688,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   if (ok) {
 #pragma unroll
     for (int q = 1; q <= S; ++q)
-      if (T - q >= 0) ok = mbar_wait(&empty[(gs + T - q) & 1], ((gs + T - q) >> 1) & 1, a.err) && ok;
+      if (T - q >= 0) ok = mbar_wait(&empty[(gs + T - q) & 1], ((gs + T - q) >> 1) & 1, a.err, a.wait_limit) && ok;
   }
   ok = __syncthreads_and(ok);
   fence_after_sync();
@@ -748,7 +754,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   fence_before_sync();
   gs += T;
   }  // tiles
-  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err);
+  if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err, a.wait_limit);
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, NCOL);
 }

@@ -42,6 +42,8 @@ struct MixedState {
   long ttot = 0;               // synthesis pipeline steps over all m (one column tile)
   float* d_stage = nullptr;    // 4 FP32 grids for the host-array entry points and grid downloads
   int* d_err = nullptr;
+  long long wait_limit = 0;    // clock cycles of each bounded wait (0: the kernels' default)
+  int omit_plus1 = 0;          // error-path tests: the next synthesis omits a step's copies in CTA 0
   size_t bytes = 0;
   std::vector<void*> allocs;
   float4* F(int c) const { return d_Fall + fcomp * c; }
@@ -98,6 +100,9 @@ int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float4* out
   a.bimg = x->d_bimg_s;
   a.ttot = x->ttot;
   a.prep_mask = prep_mask;
+  a.wait_limit = x->wait_limit;
+  a.omit_plus1 = x->omit_plus1;
+  x->omit_plus1 = 0;  // one-shot
   { ProfScope p(h, "legendre_synth_scalar_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], nullptr, x->sinv, a, false); }
   return launched(h, "mixed scalar synthesis");
 }
@@ -117,6 +122,9 @@ int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float4* 
   a.bimg = pre ? x->d_bimg_vp : x->d_bimg_vc;
   a.ttot = x->ttot;
   a.prep_mask = pre ? 3 : 0;
+  a.wait_limit = x->wait_limit;
+  a.omit_plus1 = x->omit_plus1;
+  x->omit_plus1 = 0;
   { ProfScope p(h, "legendre_synth_vector_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], x->img_synth[1], x->sinv, a, true); }
   return launched(h, "mixed vector synthesis");
 }
@@ -141,6 +149,7 @@ int tc_analysis_scalar_G(gd_handle* h, int nf, double* const* out) {
   a.nf = nf;
   a.epi = EPI_SCALAR;
   a.err = x->d_err;
+  a.wait_limit = x->wait_limit;
   { ProfScope p(h, "legendre_analysis_scalar_tc"); launch_tc_analysis(h->stream, h->d, h->d_moff, x->img_anal[0], nullptr, a); }
   return launched(h, "mixed scalar analysis");
 }
@@ -154,6 +163,7 @@ int tc_analysis_vector_G(gd_handle* h, double* out_tor, double* out_pol, int epi
   a.nf = 1;
   a.epi = epi;
   a.err = x->d_err;
+  a.wait_limit = x->wait_limit;
   { ProfScope p(h, "legendre_analysis_vector_tc"); launch_tc_analysis(h->stream, h->d, h->d_moff, x->img_anal[1], x->img_anal[2], a); }
   return launched(h, "mixed vector analysis");
 }
@@ -196,64 +206,44 @@ size_t fourier64_comp(const Dims& d) { return (size_t)d.nr * (d.M + 1) * d.nlat;
 constexpr int CV_MT = 8;   // orders per CTA
 constexpr int CV_CH = 64;  // colatitude pairs per pass
 
-// FP64 Fourier (synthesis layout, s = north / south row) <-> blocked FP32
-// (float4 north Re, north Im, south Re, south Im at [comp][r][theta block][m]
-// [pair in block]).  One CTA per (component, shell) and CV_MT orders; both
-// sides are read and written in contiguous runs through shared memory.
-template <bool TO_BLOCKED>
-__global__ void __launch_bounds__(256) k_convert_fourier(Dims d, double2* __restrict__ f64, float4* __restrict__ blk,
-                                                        size_t fcomp) {
+// Blocked FP32 Fourier components (float4 north Re, north Im, south Re, south
+// Im at [comp][r][theta block][m][pair in block]) widened to the FP64
+// synthesis layout (s = north / south row), for the FP64 Coriolis stage after
+// a split-TF32 synthesis.  One CTA per (component, shell) and CV_MT orders;
+// both sides are read and written in contiguous runs through shared memory.
+__global__ void __launch_bounds__(256) k_widen_fourier(Dims d, double2* __restrict__ f64,
+                                                      const float4* __restrict__ blk, size_t fcomp) {
   __shared__ double2 buf[CV_MT][2][CV_CH];
   const int m0 = blockIdx.x * CV_MT, cr = blockIdx.y;  // cr = comp nr + r
   const int nblk = (d.nth + FOURIER_BLOCK - 1) / FOURIER_BLOCK;
   const size_t run = (size_t)nblk * (d.M + 1) * FOURIER_BLOCK;
   const int comp = cr / d.nr, r = cr % d.nr;
-  double2* src64 = f64 + (size_t)cr * (d.M + 1) * 2 * d.nth;
-  float4* dst = blk + comp * fcomp + (size_t)r * run;
+  double2* dst64 = f64 + (size_t)cr * (d.M + 1) * 2 * d.nth;
+  const float4* src = blk + comp * fcomp + (size_t)r * run;
   for (int i0 = 0; i0 < d.nth; i0 += CV_CH) {
-    // FP64 side: rows (m, s) of CV_CH consecutive colatitudes
-    if (TO_BLOCKED) {
-      for (int e = threadIdx.x; e < CV_MT * 2 * CV_CH; e += blockDim.x) {
-        const int mm = e / (2 * CV_CH), sr = (e / CV_CH) & 1, i = e % CV_CH;
-        const int m = m0 + mm, ith = i0 + i;
-        if (m <= d.M && ith < d.nth) buf[mm][sr][i] = src64[((size_t)m * 2 + sr) * d.nth + ith];
-      }
-      __syncthreads();
-    }
     // blocked side: for each theta block, CV_MT orders x FOURIER_BLOCK pairs are contiguous
     for (int e = threadIdx.x; e < CV_CH * CV_MT; e += blockDim.x) {
       const int p = e % FOURIER_BLOCK, mm = (e / FOURIER_BLOCK) % CV_MT, bl = e / (FOURIER_BLOCK * CV_MT);
       const int i = bl * FOURIER_BLOCK + p, ith = i0 + i, m = m0 + mm;
       if (m > d.M || ith >= d.nth) continue;
-      float4* q = dst + ((size_t)(ith / FOURIER_BLOCK) * (d.M + 1) + m) * FOURIER_BLOCK + ith % FOURIER_BLOCK;
-      if (TO_BLOCKED) {
-        const double2 n = buf[mm][0][i], sv = buf[mm][1][i];
-        *q = make_float4((float)n.x, (float)n.y, (float)sv.x, (float)sv.y);
-      } else {
-        const float4 v = *q;
-        buf[mm][0][i] = make_double2(v.x, v.y);
-        buf[mm][1][i] = make_double2(v.z, v.w);
-      }
+      const float4 v = src[((size_t)(ith / FOURIER_BLOCK) * (d.M + 1) + m) * FOURIER_BLOCK + ith % FOURIER_BLOCK];
+      buf[mm][0][i] = make_double2(v.x, v.y);
+      buf[mm][1][i] = make_double2(v.z, v.w);
     }
-    if (!TO_BLOCKED) {
-      __syncthreads();
-      for (int e = threadIdx.x; e < CV_MT * 2 * CV_CH; e += blockDim.x) {
-        const int mm = e / (2 * CV_CH), sr = (e / CV_CH) & 1, i = e % CV_CH;
-        const int m = m0 + mm, ith = i0 + i;
-        if (m <= d.M && ith < d.nth) src64[((size_t)m * 2 + sr) * d.nth + ith] = buf[mm][sr][i];
-      }
+    __syncthreads();
+    // FP64 side: rows (m, s) of CV_CH consecutive colatitudes
+    for (int e = threadIdx.x; e < CV_MT * 2 * CV_CH; e += blockDim.x) {
+      const int mm = e / (2 * CV_CH), sr = (e / CV_CH) & 1, i = e % CV_CH;
+      const int m = m0 + mm, ith = i0 + i;
+      if (m <= d.M && ith < d.nth) dst64[((size_t)m * 2 + sr) * d.nth + ith] = buf[mm][sr][i];
     }
     __syncthreads();
   }
 }
 
-void launch_convert_fourier(cudaStream_t s, const Dims& d, double2* f64, float4* blk, size_t fcomp, int ncomp,
-                            bool to_blocked) {
+void launch_widen_fourier(cudaStream_t s, const Dims& d, double2* f64, const float4* blk, size_t fcomp, int ncomp) {
   const dim3 grid(ceil_div(d.M + 1, CV_MT), ncomp * d.nr);
-  if (to_blocked)
-    k_convert_fourier<true><<<grid, 256, 0, s>>>(d, f64, blk, fcomp);
-  else
-    k_convert_fourier<false><<<grid, 256, 0, s>>>(d, f64, blk, fcomp);
+  k_widen_fourier<<<grid, 256, 0, s>>>(d, f64, blk, fcomp);
 }
 
 // Folded transforms (same layout, float2 / double2): g64 = [g64 +] g32 or g32 = g64.
@@ -358,7 +348,19 @@ int mixed_check_error(gd_handle* h) {
   if (s) return s;
   s = mcheck(h, cudaStreamSynchronize(h->stream), "err sync");
   if (s) return s;
-  if (flag) return set_error(h, GD_ERR_CUDA, "a tensor-core pipeline wait expired (results of that call are invalid)");
+  if (flag) {
+    // reported once: the flag is cleared so the handle's next calls run normally
+    s = mcheck(h, cudaMemsetAsync(h->mixed->d_err, 0, sizeof(int), h->stream), "err reset");
+    if (s) return s;
+    return set_error(h, GD_ERR_CUDA, "a tensor-core pipeline wait expired (results of that call are invalid)");
+  }
+  return GD_OK;
+}
+
+int mixed_set_fault_test(gd_handle* h, long long wait_cycles, int omit_step) {
+  if (!h->mixed) return set_error(h, GD_ERR_STATE, "the handle has no mixed-precision state");
+  h->mixed->wait_limit = wait_cycles > 0 ? wait_cycles : 0;
+  h->mixed->omit_plus1 = omit_step >= 0 ? omit_step + 1 : 0;
   return GD_OK;
 }
 
@@ -415,13 +417,14 @@ int mixed_velocity_nl(gd_handle* h) {
     a.coef[1] = h->field(F_UTOR);
     a.nf = 1;
     a.out = U64;
+    a.out32 = x->F(FC_U);  // the FP32 copy the fused phase kernels read
+    a.out32_comp = x->fcomp;
     { ProfScope p(h, "legendre_synth_vector_fp64"); launch_synth_fp64(h->stream, d, h->d_moff, a, true); }
-    { ProfScope p(h, "fourier_convert"); launch_convert_fourier(h->stream, d, U64, x->F(FC_U), x->fcomp, 2, true); }
     s = launched(h, "FP64 velocity synthesis");
   } else {
     s = tc_synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), x->F(FC_U));
     if (!s && (st & GD_STAGE_VEL_PRODUCTS)) {
-      { ProfScope p(h, "fourier_convert"); launch_convert_fourier(h->stream, d, U64, x->F(FC_U), x->fcomp, 2, false); }
+      { ProfScope p(h, "fourier_convert"); launch_widen_fourier(h->stream, d, U64, x->F(FC_U), x->fcomp, 2); }
       s = launched(h, "velocity Fourier widening");
     }
   }
@@ -441,7 +444,13 @@ int mixed_velocity_nl(gd_handle* h) {
   { ProfScope p(h, "fused_velocity_fp32"); launch_fused(h->stream, d, h->plan, h->d_twf, FUSED_VELOCITY, f); }
   s = launched(h, "fused velocity phase");
   if (s) return s;
+  bool fused = false;
   if (st & GD_STAGE_VEL_PRODUCTS) {
+    const double rf = h->c.magnetic_prandtl / h->c.ekman;
+    ProfScope p(h, "coriolis_fused_fp64");
+    fused = launch_coriolis_fused(h->stream, d, d.nlon, h->d_tw, U64, h->d_cth, h->d_sthc, rf, h->d_w, x->d_G, G64);
+  }
+  if ((st & GD_STAGE_VEL_PRODUCTS) && !fused) {
     const double rf = h->c.magnetic_prandtl / h->c.ekman;
     { ProfScope p(h, "fft_synth_fp64");
       launch_fft_synth<double>(h->stream, d, h->plan, h->d_tw, U64, h->grid(GD_GRID_U_TH), 2, h->grid_elems()); }
@@ -452,7 +461,7 @@ int mixed_velocity_nl(gd_handle* h) {
       launch_fft_analysis<double>(h->stream, d, h->plan, h->d_tw, h->grid(GD_GRID_VADV_TH), h->grid_elems(), h->d_w,
                                   G64, 2); }
   }
-  if (st & (GD_STAGE_VEL_PRODUCTS | GD_STAGE_VEL_ANALYSIS)) {
+  if ((st & (GD_STAGE_VEL_PRODUCTS | GD_STAGE_VEL_ANALYSIS)) && !fused) {
     // FP32 folded transforms of the fused kernel: added to the FP64 Coriolis
     // transforms, or widened for the FP64 analysis
     ProfScope p(h, "fold_convert");

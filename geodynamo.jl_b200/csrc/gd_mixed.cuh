@@ -11,6 +11,10 @@ namespace gd {
 int mixed_create(gd_handle* h);
 // GD_ERR_CUDA if a tensor-core wait expired since creation (synchronises the stream).
 int mixed_check_error(gd_handle* h);
+// Error-path tests: the bound of every tensor-core wait (clock cycles, <= 0:
+// the default) and a one-shot omission of the copies of one pipeline step in
+// CTA 0 of the next synthesis (omit_step < 0: none).
+int mixed_set_fault_test(gd_handle* h, long long wait_cycles, int omit_step);
 void mixed_destroy(gd_handle* h);
 size_t mixed_bytes(const gd_handle* h);
 int mixed_temperature_nl(gd_handle* h);

@@ -58,6 +58,8 @@ struct TcSynthArgs {
   int nblk;               // theta blocks (ceil(nth / FOURIER_BLOCK))
   int nf;
   int* err;               // set to 1 if a bounded wait expires
+  long long wait_limit;   // clock cycles of each bounded wait (0: the default)
+  int omit_plus1;         // > 0: CTA 0 omits the bulk copies of pipeline step omit_plus1 - 1 (error-path tests)
   float* bimg;            // split coefficient images (tc_synth_bimage_floats floats)
   long ttot;              // pipeline steps summed over m (one column tile)
   int prep_mask;          // fields the pre-pass writes into bimg (the others are written by their producer)
@@ -80,6 +82,7 @@ struct TcAnalysisArgs {
   int nf;
   int epi;
   int* err;
+  long long wait_limit;   // clock cycles of each bounded wait (0: the default)
 };
 
 long tc_synth_chunks(const Dims& d, std::vector<long>& cofs);

@@ -114,10 +114,15 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+// Clock cycles a bounded wait allows by default (about a second at 2 GHz).
+constexpr long long kWaitCycles = 1LL << 31;
+
 // Waits for the phase with the given parity to complete.  Gives up after
-// ~2^31 clock cycles (about a second), raising *err; returns false then.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+// `limit` clock cycles (kWaitCycles when limit <= 0), raising *err; returns
+// false then.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, long long limit = 0) {
   const uint32_t addr = smem_addr(bar);
+  const long long bound = limit > 0 ? limit : kWaitCycles;
   const long long t0 = clock64();
   while (true) {
     uint32_t done;
@@ -129,7 +134,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > (1LL << 31)) {
+    if (clock64() - t0 > bound) {
       atomicExch(err, 1);
       return false;
     }

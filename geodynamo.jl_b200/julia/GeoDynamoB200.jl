@@ -93,6 +93,109 @@ function vector_analysis!(h::Handle, vec, tor, pol)
     return tor, pol
 end
 
+# compute_temperature_nonlinear!(temp, vel, oc) (src/thermal.jl:149): the
+# Dirichlet values and sources of temp go to the handle, then one call
+# (gd_compute_temperature_nonlinear) fills temp.nonlinear, applies the boundary
+# rows to temp.spectral and writes the temperature grid.
+function temperature_nonlinear!(h::Handle, temp, vel)
+    bv = Matrix{Float64}(permutedims(temp.boundary_values))   # [nlm, 2] = C's [2][nlm]
+    src = Vector{Float64}(temp.internal_sources)
+    GC.@preserve bv src check(h, ccall((:gd_set_temperature_bc, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, bv, src))
+    tr = parent(temp.spectral.data_real); ti = parent(temp.spectral.data_imag)
+    ut = parent(vel.velocity.θ_component.data); up = parent(vel.velocity.φ_component.data)
+    nr = parent(temp.nonlinear.data_real); ni = parent(temp.nonlinear.data_imag)
+    tg = parent(temp.temperature.data)
+    GC.@preserve tr ti ut up nr ni tg check(h, ccall((:gd_compute_temperature_nonlinear, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+        h.ptr, tr, ti, ut, up, nr, ni, tg))
+    return temp
+end
+
+# compute_velocity_nonlinear!(fields, temp, comp, mag, domain) (src/velocity.jl:312):
+# the Lorentz term reads mag's current and field grids (C_NULL without mag).
+function velocity_nonlinear!(h::Handle, fields, mag)
+    tr = parent(fields.toroidal.data_real); ti = parent(fields.toroidal.data_imag)
+    pr = parent(fields.poloidal.data_real); pi = parent(fields.poloidal.data_imag)
+    nt = parent(fields.nl_toroidal.data_real); nti = parent(fields.nl_toroidal.data_imag)
+    np = parent(fields.nl_poloidal.data_real); npi = parent(fields.nl_poloidal.data_imag)
+    ut = parent(fields.velocity.θ_component.data); up = parent(fields.velocity.φ_component.data)
+    grids = mag === nothing ? (C_NULL, C_NULL, C_NULL, C_NULL) :
+        (pointer(parent(mag.current.θ_component.data)), pointer(parent(mag.current.φ_component.data)),
+         pointer(parent(mag.magnetic.θ_component.data)), pointer(parent(mag.magnetic.φ_component.data)))
+    GC.@preserve tr ti pr pi nt nti np npi ut up mag check(h, ccall((:gd_compute_velocity_nonlinear, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+         Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+         Ptr{Cdouble}),
+        h.ptr, tr, ti, pr, pi, grids..., nt, nti, np, npi, ut, up))
+    return fields
+end
+
+# compute_magnetic_nonlinear!(mag, vel, oc, ic, rot) (src/magnetic.jl:131)
+function magnetic_nonlinear!(h::Handle, mag, vel)
+    tr = parent(mag.toroidal.data_real); ti = parent(mag.toroidal.data_imag)
+    pr = parent(mag.poloidal.data_real); pi = parent(mag.poloidal.data_imag)
+    ut = parent(vel.velocity.θ_component.data); up = parent(vel.velocity.φ_component.data)
+    nt = parent(mag.nl_toroidal.data_real); nti = parent(mag.nl_toroidal.data_imag)
+    np = parent(mag.nl_poloidal.data_real); npi = parent(mag.nl_poloidal.data_imag)
+    bt = parent(mag.magnetic.θ_component.data); bp = parent(mag.magnetic.φ_component.data)
+    jt = parent(mag.current.θ_component.data); jp = parent(mag.current.φ_component.data)
+    GC.@preserve tr ti pr pi ut up nt nti np npi bt bp jt jp check(h, ccall((:gd_compute_magnetic_nonlinear, LIB),
+        Cint, (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+               Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+               Ptr{Cdouble}),
+        h.ptr, tr, ti, pr, pi, ut, up, nt, nti, np, npi, bt, bp, jt, jp))
+    return mag
+end
+
+# Device copies of SHTnsImplicitMatrices (src/timestep.jl:489-496) for
+# build_rhs_cnab2! / solve_implicit_step!, made by gd_create_timestepping_matrices
+# from the reference struct's own parameters: theta is stored; 1/dt is the
+# l = 0 system diagonal plus theta times the l = 0 operator diagonal; the
+# diffusivity is (L_0 - L_1) diagonal x r^2 / 2 at the outer node
+# (L_l = nu (lap - l(l+1)/r^2)).  Cached per matrices object.
+mutable struct DeviceMatrices
+    ptr::Ptr{Cvoid}
+    h::Handle
+end
+const MATRICES = IdDict{Any,DeviceMatrices}()
+
+function device_matrices(h::Handle, M, nr::Integer, KL::Integer)
+    get!(MATRICES, M) do
+        i0 = M.lookup[0]; i1 = M.lookup[1]
+        r = zeros(nr); check(h, ccall((:gd_grid, LIB), Cint, (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+                                      h.ptr, C_NULL, C_NULL, r))
+        L0 = M.linear_matrices[i0].data; L1 = M.linear_matrices[i1].data; S0 = M.system_matrices[i0].data
+        theta = M.theta
+        dt = 1.0 / (S0[KL + 1, nr] + theta * L0[KL + 1, nr])
+        nu = (L0[KL + 1, nr] - L1[KL + 1, nr]) * r[nr]^2 / 2
+        out = Ref{Ptr{Cvoid}}(C_NULL)
+        check(h, ccall((:gd_create_timestepping_matrices, LIB), Cint,
+                       (Ptr{Cvoid}, Cdouble, Cdouble, Cdouble, Ref{Ptr{Cvoid}}), h.ptr, nu, dt, theta, out))
+        d = DeviceMatrices(out[], h)
+        finalizer(x -> ccall((:gd_destroy_timestepping_matrices, LIB), Cint, (Ptr{Cvoid},), x.ptr), d)
+        d
+    end
+end
+
+# build_rhs_cnab2!(rhs, un, nl, nl_prev, dt, matrices) (src/timestep.jl:610)
+function build_rhs_cnab2!(h::Handle, dm::DeviceMatrices, rhs, un, nl, nl_prev, dt::Float64)
+    a = map(parent, (un.data_real, un.data_imag, nl.data_real, nl.data_imag, nl_prev.data_real, nl_prev.data_imag,
+                     rhs.data_real, rhs.data_imag))
+    GC.@preserve a check(h, ccall((:gd_build_rhs_cnab2, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Cdouble, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+         Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, dm.ptr, dt, a...))
+    return rhs
+end
+
+# solve_implicit_step!(sol, rhs, matrices) (src/timestep.jl:692)
+function solve_implicit_step!(h::Handle, dm::DeviceMatrices, sol, rhs)
+    a = map(parent, (rhs.data_real, rhs.data_imag, sol.data_real, sol.data_imag))
+    GC.@preserve a check(h, ccall((:gd_solve_implicit_step, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, dm.ptr, a...))
+    return sol
+end
+
 upload!(h::Handle, f::Symbol, field) = (re = parent(field.data_real); im = parent(field.data_imag);
     GC.@preserve re im check(h, ccall((:gd_upload_spectral, LIB), Cint,
         (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, FIELD[f], re, im)))
@@ -155,9 +258,10 @@ end
 """
     install!(GD::Module; precision = 0)
 
-Overload GeoDynamo's transform entry points so existing callers (step_once!,
-compute_*_nonlinear!) run on the B200 library.  precision = 1 selects the
-mixed-precision transforms.
+Overload GeoDynamo's transform, nonlinear and CNAB2 entry points so existing
+callers (step_once!, apply_master_implicit_step!) run on the B200 library.
+precision = 1 selects the mixed-precision transforms (the nonlinear and CNAB2
+functions on host arrays always compute in FP64).
 """
 function install!(GD::Module; precision::Integer = 0)
     @eval GD begin
@@ -178,6 +282,34 @@ function install!(GD::Module; precision::Integer = 0)
                                            pol::SHTnsSpectralField{Float64})
             h = $handle_for($GD, tor.config, size(parent(tor.data_real), 3); precision = $precision)
             $vector_analysis!(h, vec, tor, pol)
+        end
+        function compute_temperature_nonlinear!(temp::SHTnsTemperatureField{Float64}, vel, oc::RadialDomain;
+                                                geometry::Symbol = get_parameters().geometry)
+            h = $handle_for($GD, temp.spectral.config, size(parent(temp.spectral.data_real), 3))
+            $temperature_nonlinear!(h, temp, vel)
+        end
+        function compute_velocity_nonlinear!(fields::SHTnsVelocityFields{Float64}, temp, comp, mag,
+                                             oc::RadialDomain)
+            h = $handle_for($GD, fields.toroidal.config, size(parent(fields.toroidal.data_real), 3))
+            $velocity_nonlinear!(h, fields, mag)
+        end
+        function compute_magnetic_nonlinear!(mag::SHTnsMagneticFields{Float64}, vel, oc::RadialDomain,
+                                             ic::RadialDomain, rotation_rate::Float64 = 0.0; geometry::Symbol = :shell)
+            h = $handle_for($GD, mag.toroidal.config, size(parent(mag.toroidal.data_real), 3))
+            $magnetic_nonlinear!(h, mag, vel)
+        end
+        function build_rhs_cnab2!(rhs::SHTnsSpectralField{Float64}, un::SHTnsSpectralField{Float64},
+                                  nl::SHTnsSpectralField{Float64}, nl_prev::SHTnsSpectralField{Float64},
+                                  dt::Float64, M::SHTnsImplicitMatrices{Float64})
+            nr = size(parent(un.data_real), 3)
+            h = $handle_for($GD, un.config, nr)
+            $build_rhs_cnab2!(h, $device_matrices(h, M, nr, i_KL), rhs, un, nl, nl_prev, dt)
+        end
+        function solve_implicit_step!(sol::SHTnsSpectralField{Float64}, rhs::SHTnsSpectralField{Float64},
+                                      M::SHTnsImplicitMatrices{Float64})
+            nr = size(parent(rhs.data_real), 3)
+            h = $handle_for($GD, rhs.config, nr)
+            $solve_implicit_step!(h, $device_matrices(h, M, nr, i_KL), sol, rhs)
         end
     end
     return nothing

@@ -320,6 +320,18 @@ int gd_ensemble_failed_member(const gd_ensemble* e);
  * joined to it, so events recorded on it bracket whole ensemble steps. */
 int gd_ensemble_get_stream(gd_ensemble* e, void** stream);
 
+/* ---- error-path testing ----------------------------------------------------------
+ * No counterpart in the reference.  Every wait of the tensor-core pipelines is
+ * bounded: when one runs out the kernel records it, lets its copies in flight
+ * land, frees its tensor memory and returns, and the call reports GD_ERR_CUDA
+ * ("wait expired"); the flag is then cleared, so the handle's next calls run
+ * normally.  To test that path without a GPU fault: wait_cycles bounds every
+ * wait (clock cycles; <= 0 restores the default of about a second) and
+ * omit_step >= 0 makes the next tensor-core synthesis on this handle skip the
+ * bulk copies of that pipeline step in its first CTA (once), so the waits on
+ * that stage run out.  GD_ERR_STATE without mixed-precision state. */
+int gd_set_fault_test(gd_handle* h, long long wait_cycles, int omit_step);
+
 /* ---- tracing ------------------------------------------------------------------
  * The handle's CUDA stream (a cudaStream_t passed as void*), so a caller can
  * time work on it with its own events. */
