@@ -1,10 +1,13 @@
 # GeoDynamoB200.jl -- ccall shim that puts libgdb200.so (B200, sm_100a) behind
 # GeoDynamo.jl's transform, nonlinear and time-step functions.
 #
-# Usage from a GeoDynamo.jl session:
-#     include(joinpath(path_to_repo, "geodynamo.jl_b200", "julia", "GeoDynamoB200.jl"))
-#     using .GeoDynamoB200
+# Usage from a GeoDynamo.jl session (as a package, so that loading
+# ChainRulesCore also loads the reverse-mode rule of ext/):
+#     using Pkg; Pkg.develop(path = joinpath(path_to_repo, "geodynamo.jl_b200", "julia", "GeoDynamoB200"))
+#     using GeoDynamoB200
 #     GeoDynamoB200.install!(GeoDynamo)          # overloads the methods below
+# or, without the package manager,
+#     include(joinpath(path_to_repo, "geodynamo.jl_b200", "julia", "GeoDynamoB200", "src", "GeoDynamoB200.jl"))
 #
 # Array layouts need no conversion: GeoDynamo's spectral planes
 # (nlm, 1, nr) and physical fields (nlat, nlon, nr) are column-major, which is
@@ -13,7 +16,7 @@
 # as the reference does.
 module GeoDynamoB200
 
-const LIB = normpath(joinpath(@__DIR__, "..", "libgdb200.so"))
+const LIB = normpath(joinpath(@__DIR__, "..", "..", "..", "libgdb200.so"))
 
 # gd_config (include/gdb200.h)
 struct GDConfig
@@ -220,18 +223,26 @@ const SCHEME = Dict(:cnab2 => 0, :eab2 => 1, :erk2 => 2)
 set_scheme!(h::Handle, scheme::Symbol) =
     check(h, ccall((:gd_set_scheme, LIB), Cint, (Ptr{Cvoid}, Cint), h.ptr, SCHEME[scheme]))
 
-# Reverse mode.  magnetic_pullback(h, :b_pol, nsteps, λre, λim) -> (gre, gim):
-# the vector-Jacobian product of nsteps steps with respect to a magnetic
-# component at their start (gd_magnetic_pullback; planes (nlm, nr), as the
-# field data).  A ChainRulesCore rule for the step, for objectives of the
-# magnetic field, is then
-#     function ChainRulesCore.rrule(::typeof(magnetic_steps), h, bpol_re, bpol_im, nsteps)
-#         out = magnetic_steps(h, bpol_re, bpol_im, nsteps)
-#         pullback(Δ) = (NoTangent(), NoTangent(),
-#                        magnetic_pullback(h, :b_pol, nsteps, Δ[1], Δ[2])..., NoTangent())
-#         return out, pullback
-#     end
-# (written here as a comment: ChainRulesCore is not a dependency of this shim).
+# Reverse mode.  evolve_magnetic(h, re, im, nsteps; field = :b_pol) sets one
+# magnetic component of h's state, runs nsteps model steps (gd_step) and
+# returns that component afterwards; its ChainRulesCore rrule lives in
+# ext/GeoDynamoB200ChainRulesCoreExt.jl and is loaded with ChainRulesCore.
+# magnetic_pullback(h, :b_pol, nsteps, λre, λim) -> (gre, gim) is the
+# vector-Jacobian product of those steps (gd_magnetic_pullback; planes
+# (nlm, nr), as the field data).  In the reference's step the magnetic field
+# evolves by its implicit operator alone, the same for every step and state,
+# so the pullback needs no checkpoints of the forward run.
+function evolve_magnetic(h::Handle, re::AbstractArray{Float64}, im::AbstractArray{Float64}, nsteps::Integer;
+                         field::Symbol = :b_pol)
+    r = Array{Float64}(re); i = Array{Float64}(im)
+    GC.@preserve r i check(h, ccall((:gd_upload_spectral, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, FIELD[field], r, i))
+    check(h, ccall((:gd_step, LIB), Cint, (Ptr{Cvoid}, Cint), h.ptr, nsteps))
+    GC.@preserve r i check(h, ccall((:gd_download_spectral, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, FIELD[field], r, i))
+    return r, i
+end
+
 function magnetic_pullback(h::Handle, f::Symbol, nsteps::Integer, lre::AbstractArray{Float64},
                            lim::AbstractArray{Float64})
     gre = similar(lre); gim = similar(lim)
