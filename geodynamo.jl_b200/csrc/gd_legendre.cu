@@ -1,5 +1,5 @@
 // gd_legendre.cu -- FP64 Legendre synthesis and analysis as batched per-m
-// contractions on the FP64 tensor pipe (DMMA m8n8k4), with even/odd folding.
+// contractions on the FP64 tensor pipe (DMMA m16n8k8), with even/odd folding.
 //
 // For a fixed order m the l-sum is split by the parity of l - m.  Even and
 // odd partial sums come from separate warp groups (warps 0-3 even, 4-7 odd)
@@ -15,10 +15,16 @@
 
 namespace gd {
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+// D (16 x 8) += A (16 x 8, row-major) B (8 x 8, column-major) on the FP64 tensor
+// pipe, per thread (g = lane / 4, t = lane % 4):
+//   a = A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4];  b = B[t][g], B[t+4][g];
+//   d = C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1].
+__device__ __forceinline__ void dmma16(double& d0, double& d1, double& d2, double& d3, const double* a,
+                                       const double* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d0), "+d"(d1), "+d"(d2), "+d"(d3)
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 // Asynchronous global -> shared copies of the operand tiles.  Every CTA keeps
@@ -121,18 +127,29 @@ __global__ void __launch_bounds__(256, 2) k_synth_scalar(Dims d, const int* __re
     cpa_commit();
     const double* As = smem + (ch % LEG_STAGES) * SS_STAGE;
     const double* Bs = As + SS_KC * SS_SA;
+    // two K steps of 8 degrees of this warp's parity: rows q0 (k = 8 ks + t) and q1 (k + 4)
 #pragma unroll
-    for (int kk = 0; kk < SS_KC / 8; ++kk) {
-      const int q = 2 * (4 * kk + t) + par;
-      double af[4], bf[4];
+    for (int ks = 0; ks < SS_KC / 16; ++ks) {
+      const int q0 = 2 * (8 * ks + t) + par, q1 = q0 + 8;
+      double af[2][4], bf[4][2];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) af[i] = As[q * SS_SA + thw + 8 * i + g];
+      for (int i = 0; i < 2; ++i) {
+        const int r0 = thw + 16 * i + g;
+        af[i][0] = As[q0 * SS_SA + r0];
+        af[i][1] = As[q0 * SS_SA + r0 + 8];
+        af[i][2] = As[q1 * SS_SA + r0];
+        af[i][3] = As[q1 * SS_SA + r0 + 8];
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bf[j] = Bs[q * SS_SB + nw + 8 * j + g];
+      for (int j = 0; j < 4; ++j) {
+        bf[j][0] = Bs[q0 * SS_SB + nw + 8 * j + g];
+        bf[j][1] = Bs[q1 * SS_SB + nw + 8 * j + g];
+      }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        for (int j = 0; j < 4; ++j)
+          dmma16(acc[2 * i][j][0], acc[2 * i][j][1], acc[2 * i + 1][j][0], acc[2 * i + 1][j][1], af[i], bf[j]);
     }
   }
   cpa_wait<0>();
@@ -255,25 +272,33 @@ __global__ void __launch_bounds__(256, 2) k_synth_vector(Dims d, const int* __re
     const double* As = smem + (ch % LEG_STAGES) * VS_STAGE;
     const double* Bs = As + 2 * VS_KC * VS_SA;
 #pragma unroll
-    for (int kk = 0; kk < VS_KC / 8; ++kk) {
-      const int q = 2 * (4 * kk + t) + par;
-      double af[2][2], bf[2][2];
+    for (int ks = 0; ks < VS_KC / 16; ++ks) {
+      const int q0 = 2 * (8 * ks + t) + par, q1 = q0 + 8;
+      double af[2][4], bf[2][2][2];
 #pragma unroll
-      for (int x = 0; x < 2; ++x)
-#pragma unroll
-        for (int i = 0; i < 2; ++i) af[x][i] = As[(x * VS_KC + q) * VS_SA + thw + 8 * i + g];
+      for (int x = 0; x < 2; ++x) {
+        const double* A0 = As + (x * VS_KC + q0) * VS_SA + thw + g;
+        const double* A1 = As + (x * VS_KC + q1) * VS_SA + thw + g;
+        af[x][0] = A0[0];
+        af[x][1] = A0[8];
+        af[x][2] = A1[0];
+        af[x][3] = A1[8];
+      }
 #pragma unroll
       for (int y = 0; y < 2; ++y)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) bf[y][j] = Bs[(y * VS_KC + q) * VS_SB + nw + 8 * j + g];
+        for (int j = 0; j < 2; ++j) {
+          bf[y][j][0] = Bs[(y * VS_KC + q0) * VS_SB + nw + 8 * j + g];
+          bf[y][j][1] = Bs[(y * VS_KC + q1) * VS_SB + nw + 8 * j + g];
+        }
 #pragma unroll
       for (int x = 0; x < 2; ++x)
 #pragma unroll
         for (int y = 0; y < 2; ++y)
 #pragma unroll
-          for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) dmma(acc[x][y][i][j][0], acc[x][y][i][j][1], af[x][i], bf[y][j]);
+          for (int j = 0; j < 2; ++j)
+            dmma16(acc[x][y][0][j][0], acc[x][y][0][j][1], acc[x][y][1][j][0], acc[x][y][1][j][1], af[x],
+                   bf[y][j]);
     }
   }
   cpa_wait<0>();
@@ -452,18 +477,23 @@ __global__ void __launch_bounds__(256, 2) k_analysis_scalar(Dims d, const int* _
     cpa_commit();
     const double* As = smem + (ch % LEG_STAGES) * SA_STAGE;
     const double* Bs = As + SA_TL * SA_SA;
+    // two K steps of 8 colatitudes: th0 = 8 ks + t and th0 + 4
 #pragma unroll
-    for (int kk = 0; kk < SA_KC / 4; ++kk) {
-      const int th = 4 * kk + t;
-      double af[2], bf[4];
+    for (int ks = 0; ks < SA_KC / 8; ++ks) {
+      const int th0 = 8 * ks + t, th1 = th0 + 4;
+      const int lq0 = 2 * (lw + g) + par, lq1 = 2 * (lw + 8 + g) + par;
+      double af[4], bf[4][2];
+      af[0] = As[lq0 * SA_SA + th0];
+      af[1] = As[lq1 * SA_SA + th0];
+      af[2] = As[lq0 * SA_SA + th1];
+      af[3] = As[lq1 * SA_SA + th1];
 #pragma unroll
-      for (int i = 0; i < 2; ++i) af[i] = As[(2 * (lw + 8 * i + g) + par) * SA_SA + th];
+      for (int j = 0; j < 4; ++j) {
+        bf[j][0] = Bs[(par * SA_KC + th0) * SA_SB + nw + 8 * j + g];
+        bf[j][1] = Bs[(par * SA_KC + th1) * SA_SB + nw + 8 * j + g];
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bf[j] = Bs[(par * SA_KC + th) * SA_SB + nw + 8 * j + g];
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+      for (int j = 0; j < 4; ++j) dmma16(acc[0][j][0], acc[0][j][1], acc[1][j][0], acc[1][j][1], af, bf[j]);
     }
   }
   cpa_wait<0>();
@@ -572,32 +602,37 @@ __global__ void __launch_bounds__(256, 2) k_analysis_vector(Dims d, const int* _
     const double* As = smem + (ch % LEG_STAGES) * VA_STAGE;
     const double* Bs = As + 2 * VA_TL * VA_SA;
 #pragma unroll
-    for (int kk = 0; kk < VA_KC / 4; ++kk) {
-      const int th = 4 * kk + t;
-      double aD[2], aQ[2], bth[2][2], bph[2][2];  // b[fold][j]
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int lq = 2 * (lw + 8 * i + g) + par;
-        aD[i] = As[(0 * VA_TL + lq) * VA_SA + th];
-        aQ[i] = As[(1 * VA_TL + lq) * VA_SA + th];
-      }
+    for (int ks = 0; ks < VA_KC / 8; ++ks) {
+      const int th0 = 8 * ks + t, th1 = th0 + 4;
+      const int lq0 = 2 * (lw + g) + par, lq1 = 2 * (lw + 8 + g) + par;
+      double aD[4], aQ[4], bth[2][2][2], bph[2][2][2];  // b[fold][j][k half]
+      aD[0] = As[(0 * VA_TL + lq0) * VA_SA + th0];
+      aD[1] = As[(0 * VA_TL + lq1) * VA_SA + th0];
+      aD[2] = As[(0 * VA_TL + lq0) * VA_SA + th1];
+      aD[3] = As[(0 * VA_TL + lq1) * VA_SA + th1];
+      aQ[0] = As[(1 * VA_TL + lq0) * VA_SA + th0];
+      aQ[1] = As[(1 * VA_TL + lq1) * VA_SA + th0];
+      aQ[2] = As[(1 * VA_TL + lq0) * VA_SA + th1];
+      aQ[3] = As[(1 * VA_TL + lq1) * VA_SA + th1];
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int n = nw + 8 * j + g;
-        bth[0][j] = Bs[((0 * 2 + sD) * VA_KC + th) * VA_SB + n];
-        bph[0][j] = Bs[((1 * 2 + sD) * VA_KC + th) * VA_SB + n];
-        bth[1][j] = Bs[((0 * 2 + sP) * VA_KC + th) * VA_SB + n];
-        bph[1][j] = Bs[((1 * 2 + sP) * VA_KC + th) * VA_SB + n];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int th = h ? th1 : th0;
+          bth[0][j][h] = Bs[((0 * 2 + sD) * VA_KC + th) * VA_SB + n];
+          bph[0][j][h] = Bs[((1 * 2 + sD) * VA_KC + th) * VA_SB + n];
+          bth[1][j][h] = Bs[((0 * 2 + sP) * VA_KC + th) * VA_SB + n];
+          bph[1][j][h] = Bs[((1 * 2 + sP) * VA_KC + th) * VA_SB + n];
+        }
       }
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          dmma(acc[0][i][j][0], acc[0][i][j][1], aD[i], bth[0][j]);
-          dmma(acc[1][i][j][0], acc[1][i][j][1], aD[i], bph[0][j]);
-          dmma(acc[2][i][j][0], acc[2][i][j][1], aQ[i], bth[1][j]);
-          dmma(acc[3][i][j][0], acc[3][i][j][1], aQ[i], bph[1][j]);
-        }
+      for (int j = 0; j < 2; ++j) {
+        dmma16(acc[0][0][j][0], acc[0][0][j][1], acc[0][1][j][0], acc[0][1][j][1], aD, bth[0][j]);
+        dmma16(acc[1][0][j][0], acc[1][0][j][1], acc[1][1][j][0], acc[1][1][j][1], aD, bph[0][j]);
+        dmma16(acc[2][0][j][0], acc[2][0][j][1], acc[2][1][j][0], acc[2][1][j][1], aQ, bth[1][j]);
+        dmma16(acc[3][0][j][0], acc[3][0][j][1], acc[3][1][j][0], acc[3][1][j][1], aQ, bph[1][j]);
+      }
     }
   }
   cpa_wait<0>();
