@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
   uint64_t* empty = full + S;
   uint64_t* tfull = empty + S;
   uint64_t* tempty = tfull + 1;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 1);
+  uint64_t* drain = tempty + 1;  // after a failed wait: completion of the MMAs already issued
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
 
   const int L = d.L;
   const int Ntot = a.nf * d.nr * 2;
@@ -287,6 +288,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
     }
     mbar_init(tfull, 1);
     mbar_init(tempty, 128);
+    mbar_init(drain, 1);
   }
   if (warp == 0) tmem_alloc(tslot, NCOL);
   fence_before_sync();
@@ -484,10 +486,17 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
     }
   }
   ok = __syncthreads_and(ok);
-  // after an expired wait anywhere in the CTA, the producer lets its last
-  // bulk copies land before the CTA exits (a step the MMA warp consumed has
-  // completed its phase already, so this returns at once)
+  // after an expired wait anywhere in the CTA: the producer lets its last bulk
+  // copies land (a step the MMA warp consumed has completed its phase
+  // already, so this returns at once), and the MMA warp waits for the MMAs it
+  // has issued, before tensor memory is freed and the CTA exits
   if (!ok && warp == 0 && issued >= 0) mbar_wait(&full[issued & 1], (issued >> 1) & 1, a.err, a.wait_limit);
+  if (!ok && warp == 1) {
+    if (lane == 0) mma_commit(smem_addr(drain));
+    __syncwarp();
+    mbar_wait(drain, 0, a.err, a.wait_limit);
+  }
+  __syncthreads();
   fence_after_sync();
   if (warp == 0) tmem_dealloc(tmem, NCOL);
 }
@@ -528,6 +537,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)S * ST_FL * 4);
   uint64_t* empty = full + S;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(empty + S);
+  uint64_t* drain = empty + S + 1;  // after a failed wait: completion of the MMAs already issued
   // scalar: column pair -> folded-input base (-1 past the last column);
   // column -> output row (null past the last column)
   long long* colin = reinterpret_cast<long long*>(empty + S + 2);
@@ -537,11 +547,13 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   const size_t NM = d.nlm;
   const int Ntot = a.nf * d.nr * 2;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid == 0)
+  if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 128);
       mbar_init(&empty[s], 1);
     }
+    mbar_init(drain, 1);
+  }
   if (warp == 0) tmem_alloc(tslot, NCOL);
   fence_before_sync();
   __syncthreads();
@@ -755,17 +767,25 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   gs += T;
   }  // tiles
   if (!ok && issued >= 0) mbar_wait(&full[(threadIdx.x >> 7) & 1], issued & 1, a.err, a.wait_limit);
+  if (!ok && warp == 8) {
+    // the MMAs issued before the failure finish before tensor memory is freed
+    if (lane == 0) mma_commit(smem_addr(drain));
+    __syncwarp();
+    mbar_wait(drain, 0, a.err, a.wait_limit);
+  }
   __syncthreads();
+  fence_after_sync();
   if (warp == 0) tmem_dealloc(tmem, NCOL);
 }
 
 // ---------------------------------------------------------------------------
-// stages + mbarriers and TMEM slot (16 bytes past the stages) + the scalar
-// kernels' per-column tables (one pointer per column, one offset per pair)
-// stages + full/empty per stage, tfull, tempty and the TMEM address slot
+// Synthesis: stages + full/empty per stage, tfull, tempty, drain and the TMEM
+// address slot.  Analysis: stages + full/empty per stage, drain, the TMEM
+// address slot and the scalar kernels' per-column tables (one pointer per
+// column, one offset per pair).
 static size_t synth_smem(bool vec) {
   const int S = 2, NCS = vec ? TC_N2 : 2 * TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS, B = 2 * NCS * TC_K;
-  return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 3);
+  return 1024 + (size_t)S * (A + B) * 4 + 8 * (2 * S + 4);
 }
 static size_t analysis_smem(bool vec) {
   const int S = 2, NC = TC_N2, A = (vec ? 2 : 1) * CHUNK_FLOATS;

@@ -102,6 +102,28 @@ def test_mixed_step_l255_tracks_oracle(gdb, oracle_mod):
         assert rel(a[0], b[0]) < 1e-5 and rel(a[1], b[1]) < 1e-5, k
 
 
+@pytest.mark.parametrize("nr", [3, 6])
+def test_mixed_phase_products_l255(gdb, oracle_mod, nr):
+    # the fused phase kernels at nlon = 768 (register-resident transforms):
+    # the nonlinear terms of the second step, whose temperature phase advects
+    # with the first step's velocity grid
+    g = gdb.SHTnsKitConfig(255, 384, 768, nr, dt=2e-6, precision="mixed")
+    o = oracle_mod.Oracle(lmax=255, nlat=384, nlon=768, nr=nr, dt=2e-6)
+    for k, (a, b) in workloads.seeded_state(255, 255, nr, seed=5).items():
+        g.set_field(k, a, b)
+        o.set_field(k, a, b)
+    g.step(1); o.step(1)
+    g.temperature_nl(); o.temperature_nl()
+    g.velocity_nl(); o.velocity_nl()
+    g.magnetic_nl(); o.magnetic_nl()
+    for k in ("temp", "u_tor", "u_pol"):
+        a, b = g.get_nl(k), o.get_nl(k)
+        assert rel(a[0], b[0]) < TOL_T and rel(a[1], b[1]) < TOL_T, k
+    for k in ("b_tor", "b_pol"):
+        a, b = g.get_nl(k), o.get_nl(k)
+        assert np.max(np.abs(a[0])) <= 1e-30 + TOL_T * max(np.max(np.abs(b[0])), 1.0)
+
+
 def test_mixed_synthesized_grids_match_oracle(gdb, oracle_mod):
     # grids of the mixed step are formed on request from its Fourier buffers
     # (the temperature grid included): after a step they are the grids the
