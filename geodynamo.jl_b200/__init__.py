@@ -71,6 +71,7 @@ EXPORTS = (
     "gd_compute_temperature_nonlinear", "gd_compute_velocity_nonlinear", "gd_compute_magnetic_nonlinear",
     "gd_create_timestepping_matrices", "gd_destroy_timestepping_matrices", "gd_build_rhs_cnab2",
     "gd_solve_implicit_step", "gd_set_fault_test",
+    "gd_derivatives", "gd_implicit_modes", "gd_set_external_derivatives", "gd_copy_block",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
     "gd_ensemble_step", "gd_ensemble_step_async", "gd_ensemble_failed_member", "gd_ensemble_get_stream",
@@ -168,6 +169,10 @@ def load_library():
         "gd_build_rhs_cnab2": ([P, P, ctypes.c_double] + [D] * 8, I),
         "gd_solve_implicit_step": ([P, P, D, D, D, D], I),
         "gd_set_fault_test": ([P, ctypes.c_longlong, I], I),
+        "gd_derivatives": ([P, I, I], I),
+        "gd_implicit_modes": ([P, I, I], I),
+        "gd_set_external_derivatives": ([P, I], I),
+        "gd_copy_block": ([P, I, I, I, I, I, I, ctypes.c_void_p, I], I),
         "gd_magnetic_pullback": ([P, I, I, D, D, D, D], I),
         "gd_ensemble_create": ([ctypes.POINTER(GDConfig), I, I, ctypes.POINTER(P)], I),
         "gd_ensemble_destroy": ([P], I),
@@ -307,6 +312,24 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_set_precision(self.h, PRECISIONS[base]))
         self.set_fp64_stages(stages)
         self.precision = precision
+
+    # -- the step decomposed across ranks (distributed.DistributedStep) ---------------
+    def derivatives(self, j0, j1):
+        """Radial derivatives of the state for native modes [j0, j1) into the work arrays."""
+        self._check(self.lib.gd_derivatives(self.h, int(j0), int(j1)))
+
+    def implicit_modes(self, j0, j1):
+        """Temperature Dirichlet rows, CNAB2 and the history roll for native modes [j0, j1)."""
+        self._check(self.lib.gd_implicit_modes(self.h, int(j0), int(j1)))
+
+    def set_external_derivatives(self, enable=True):
+        self._check(self.lib.gd_set_external_derivatives(self.h, 1 if enable else 0))
+
+    def copy_block(self, array, field, r0, r1, j0, j1, ptr, to_buf):
+        """Block [r0, r1) x [j0, j1) of a state (0), work (1) or nonlinear (2)
+        array to or from the buffer at ptr ([2][r1 - r0][j1 - j0] doubles)."""
+        self._check(self.lib.gd_copy_block(self.h, int(array), int(field), int(r0), int(r1), int(j0), int(j1),
+                                           ctypes.c_void_p(int(ptr)), 1 if to_buf else 0))
 
     def set_fault_test(self, wait_cycles=0, omit_step=-1):
         """Error-path testing (gd_set_fault_test): bound of every tensor-core

@@ -73,6 +73,8 @@ int setup(gd_handle* h) {
   for (int l = 0; l <= d.L; ++l)
     for (int m = 0; m <= (l < d.M ? l : d.M); ++m) { h->lv.push_back(l); h->mv.push_back(m); }
   d.nlm = (int)h->lv.size();
+  d.jlo = 0;
+  d.jhi = d.nlm;
   h->moff.assign(d.M + 2, 0);
   for (int m = 0; m <= d.M; ++m) h->moff[m + 1] = h->moff[m] + (d.L - m + 1);
   h->perm.resize(d.nlm);
@@ -210,9 +212,11 @@ int analysis_vector(gd_handle* h, const double* grid_in /* 2 comps */, double* o
 // ---- the physics sequence (FP64) ----
 int temperature_nl_fp64(gd_handle* h) {
   const Dims& d = h->d;
-  { ProfScope p(h, "spectral_gradients");
+  if (!h->ext_derivs) {
+    ProfScope p(h, "spectral_gradients");
     launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), h->work(0), h->work(1),
-                     h->work(2)); }
+                     h->work(2));
+  }
   const double* coef[4] = {h->field(F_TEMP), h->work(0), h->work(1), h->work(2)};
   int s = synth_scalar(h, coef, 4, h->grid(GD_GRID_T));
   if (s) return s;
@@ -223,7 +227,10 @@ int temperature_nl_fp64(gd_handle* h) {
   double* out[1] = {h->nlf(F_TEMP)};
   s = analysis_scalar(h, h->grid(GD_GRID_TADV), 1, out);
   if (s) return s;
-  { ProfScope p(h, "temperature_bc"); launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP)); }
+  if (!h->ext_derivs) {
+    ProfScope p(h, "temperature_bc");
+    launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP));
+  }
   return check_launch(h, "temperature nonlinear");
 }
 
@@ -231,9 +238,11 @@ int velocity_nl_fp64(gd_handle* h) {
   const Dims& d = h->d;
   int s = synth_vector(h, h->field(F_UTOR), h->field(F_UPOL), h->grid(GD_GRID_U_TH));
   if (s) return s;
-  { ProfScope p(h, "spectral_curl");
+  if (!h->ext_derivs) {
+    ProfScope p(h, "spectral_curl");
     launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR), h->field(F_UPOL),
-                h->work(3), h->work(4)); }
+                h->work(3), h->work(4));
+  }
   s = synth_vector(h, h->work(3), h->work(4), h->grid(GD_GRID_W_TH));
   if (s) return s;
   const double rf = h->c.magnetic_prandtl / h->c.ekman;
@@ -249,9 +258,11 @@ int magnetic_nl_fp64(gd_handle* h) {
   const Dims& d = h->d;
   int s = synth_vector(h, h->field(F_BTOR), h->field(F_BPOL), h->grid(GD_GRID_B_TH));
   if (s) return s;
-  { ProfScope p(h, "spectral_curl");
+  if (!h->ext_derivs) {
+    ProfScope p(h, "spectral_curl");
     launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR), h->field(F_BPOL),
-                h->work(5), h->work(6)); }
+                h->work(5), h->work(6));
+  }
   s = synth_vector(h, h->work(5), h->work(6), h->grid(GD_GRID_J_TH));
   if (s) return s;
   { ProfScope p(h, "nl_induction_fp64");
@@ -566,6 +577,85 @@ int gd_set_fp64_stages(gd_handle* h, int mask) {
   CK(cudaSetDevice(h->device));
   if (mask != h->fp64_stages) drop_graphs(h);
   h->fp64_stages = mask;
+  return GD_OK;
+}
+
+int gd_set_external_derivatives(gd_handle* h, int enable) {
+  if (!h) return GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  if ((enable != 0) != h->ext_derivs) drop_graphs(h);
+  h->ext_derivs = enable != 0;
+  return GD_OK;
+}
+
+static bool mode_range_ok(const gd_handle* h, int j0, int j1) { return 0 <= j0 && j0 <= j1 && j1 <= h->d.nlm; }
+
+int gd_derivatives(gd_handle* h, int j0, int j1) {
+  if (!h) return GD_ERR_ARG;
+  if (!mode_range_ok(h, j0, j1)) return fail(h, GD_ERR_ARG, "mode range outside [0, nlm]");
+  CK(cudaSetDevice(h->device));
+  if (j1 == j0) return GD_OK;
+  Dims d = h->d;
+  d.jlo = j0;
+  d.jhi = j1;
+  { ProfScope p(h, "spectral_gradients");
+    launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), h->work(0), h->work(1),
+                     h->work(2)); }
+  { ProfScope p(h, "spectral_curl");
+    launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR), h->field(F_UPOL),
+                h->work(3), h->work(4));
+    if (h->c.magnetic)
+      launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR),
+                  h->field(F_BPOL), h->work(5), h->work(6)); }
+  int s = check_launch(h, "derivatives");
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+
+int gd_implicit_modes(gd_handle* h, int j0, int j1) {
+  if (!h) return GD_ERR_ARG;
+  if (!mode_range_ok(h, j0, j1)) return fail(h, GD_ERR_ARG, "mode range outside [0, nlm]");
+  if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the mode-range solve supports CNAB2 only");
+  CK(cudaSetDevice(h->device));
+  const int boot = (h->c.ab_mode == 1 || h->step_count == 0) ? 1 : 0;
+  int s = GD_OK;
+  if (j1 > j0) {
+    const Dims full = h->d;
+    h->d.jlo = j0;
+    h->d.jhi = j1;
+    { ProfScope p(h, "temperature_bc"); launch_temperature_bc(h->stream, h->d, h->d_bvals, h->field(F_TEMP)); }
+    s = implicit_launch(h, boot);
+    h->d = full;
+  }
+  if (s) return s;
+  s = check_launch(h, "mode-range implicit step");
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  end_step(h);
+  return GD_OK;
+}
+
+int gd_copy_block(gd_handle* h, int array, int field, int r0, int r1, int j0, int j1, void* buf, int to_buf) {
+  if (!h || !buf) return h ? fail(h, GD_ERR_ARG, "null buffer") : GD_ERR_ARG;
+  const int nf = array == 1 ? 8 : 5;
+  if (array < 0 || array > 2 || field < 0 || field >= nf) return fail(h, GD_ERR_ARG, "bad array or field");
+  if (!(0 <= r0 && r0 <= r1 && r1 <= h->d.nr) || !mode_range_ok(h, j0, j1))
+    return fail(h, GD_ERR_ARG, "block outside the handle's shells or modes");
+  CK(cudaSetDevice(h->device));
+  double* base = array == 0 ? h->field(field) : array == 1 ? h->work(field) : h->nlf(field);
+  const size_t NM = h->d.nlm, plane = (size_t)h->d.nr * NM;
+  const size_t w = (size_t)(j1 - j0) * sizeof(double), rows = (size_t)(r1 - r0);
+  if (w == 0 || rows == 0) return GD_OK;
+  for (int c = 0; c < 2; ++c) {
+    double* a = base + c * plane + (size_t)r0 * NM + j0;
+    double* b = static_cast<double*>(buf) + (size_t)c * rows * (j1 - j0);
+    if (to_buf)
+      CK(cudaMemcpy2DAsync(b, w, a, NM * sizeof(double), w, rows, cudaMemcpyDefault, h->stream));
+    else
+      CK(cudaMemcpy2DAsync(a, NM * sizeof(double), b, w, w, rows, cudaMemcpyDefault, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
   return GD_OK;
 }
 

@@ -218,8 +218,8 @@ __global__ void __launch_bounds__(128, 3) k_cnab2(Dims d, const int* __restrict_
   }
   for (int i = threadIdx.x; i < N; i += blockDim.x) srinv2[i] = rinv2[i];
   __syncthreads();
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= d.nlm) return;
+  const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.jhi) return;
   const int l = lof[j];
   const double* LUk = lu + (size_t)g * N * NB * ((size_t)d.L + 1);
   cnab2_column<KL>(d, j, l, LUk, sband, srinv2, nuk, a, slot);
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(128, 3) k_cnab2(Dims d, const int* __restrict_
 
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
                   const double* rinv, const double* rinv2, const double* nu, const double* lu, const Cnab2Args& a) {
-  dim3 grid(ceil_div(d.nlm, 128), a.nfield);
+  dim3 grid(ceil_div(d.jhi - d.jlo, 128), a.nfield);
   const size_t smem = ((size_t)d.nr * GD_NBW + d.nr) * sizeof(double);
   k_cnab2<GD_MAX_KL><<<grid, 128, smem, s>>>(d, lof, d1, d2, rinv, rinv2, nu, lu, a);
 }

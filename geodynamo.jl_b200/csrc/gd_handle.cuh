@@ -19,6 +19,10 @@ struct gd_handle {
   long step_count = 0;
   int precision = GD_PREC_FP64;
   int fp64_stages = 0;        // GD_STAGE_* run in FP64 inside the mixed-precision step
+  // the phases take the radial derivatives (grad T, curl u, curl B) from the
+  // work arrays instead of computing them, and leave the temperature
+  // Dirichlet rows to the solve side (a shell-slab handle of a distributed step)
+  bool ext_derivs = false;
   size_t bytes = 0;
   std::vector<void*> allocs;
 

@@ -31,6 +31,10 @@ enum { NGRID = 17 };
 
 struct Dims {
   int L, M, nlat, nlon, nr, nth, nlm, kl;
+  // native mode range [jlo, jhi) of the radial operators, the temperature
+  // Dirichlet rows and the CNAB2 solve (0, nlm unless a caller restricts it to
+  // the m columns one rank owns)
+  int jlo, jhi;
 };
 
 // Analysis epilogue variants.

@@ -367,11 +367,19 @@ int mixed_set_fault_test(gd_handle* h, long long wait_cycles, int omit_step) {
 int mixed_temperature_nl(gd_handle* h) {
   MixedState* x = h->mixed;
   const Dims& d = h->d;
-  // the gradient goes straight into the scalar synthesis image (field slots 1-3)
-  { ProfScope p(h, "spectral_gradients");
-    launch_gradients_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), image_out(h, x->d_bimg_s)); }
-  const double* coef[4] = {h->field(F_TEMP), nullptr, nullptr, nullptr};
-  int s = tc_synth_scalar(h, coef, 4, x->F(FC_T), 1);
+  int s;
+  if (h->ext_derivs) {
+    // the gradient was computed elsewhere into the work arrays: the pre-pass
+    // splits all four fields
+    const double* coef[4] = {h->field(F_TEMP), h->work(0), h->work(1), h->work(2)};
+    s = tc_synth_scalar(h, coef, 4, x->F(FC_T), 0xF);
+  } else {
+    // the gradient goes straight into the scalar synthesis image (field slots 1-3)
+    { ProfScope p(h, "spectral_gradients");
+      launch_gradients_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_TEMP), image_out(h, x->d_bimg_s)); }
+    const double* coef[4] = {h->field(F_TEMP), nullptr, nullptr, nullptr};
+    s = tc_synth_scalar(h, coef, 4, x->F(FC_T), 1);
+  }
   if (s) return s;
   // the velocity grid is the previous velocity phase's (carried in F(FC_U));
   // the temperature grid itself is not a factor of the products: like every
@@ -387,7 +395,10 @@ int mixed_temperature_nl(gd_handle* h) {
   double* out[1] = {h->nlf(F_TEMP)};
   s = tc_analysis_scalar_G(h, 1, out);
   if (s) return s;
-  { ProfScope p(h, "temperature_bc"); launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP)); }
+  if (!h->ext_derivs) {
+    ProfScope p(h, "temperature_bc");
+    launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP));
+  }
   return launched(h, "mixed temperature nonlinear");
 }
 
@@ -429,10 +440,14 @@ int mixed_velocity_nl(gd_handle* h) {
     }
   }
   if (s) return s;
-  { ProfScope p(h, "spectral_curl");
-    launch_curl_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR),
-                    h->field(F_UPOL), image_out(h, x->d_bimg_vc)); }
-  s = tc_synth_vector(h, nullptr, nullptr, x->F(FC_W));
+  if (h->ext_derivs) {
+    s = tc_synth_vector(h, h->work(3), h->work(4), x->F(FC_W));
+  } else {
+    { ProfScope p(h, "spectral_curl");
+      launch_curl_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_UTOR),
+                      h->field(F_UPOL), image_out(h, x->d_bimg_vc)); }
+    s = tc_synth_vector(h, nullptr, nullptr, x->F(FC_W));
+  }
   if (s) return s;
   // current density and magnetic field of the previous magnetic phase (F(FC_J), F(FC_B))
   FusedArgs f = phase_args(h);
@@ -494,10 +509,14 @@ int mixed_magnetic_nl(gd_handle* h) {
   const Dims& d = h->d;
   int s = tc_synth_vector(h, h->field(F_BTOR), h->field(F_BPOL), x->F(FC_B));
   if (s) return s;
-  { ProfScope p(h, "spectral_curl");
-    launch_curl_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR),
-                    h->field(F_BPOL), image_out(h, x->d_bimg_vc)); }
-  s = tc_synth_vector(h, nullptr, nullptr, x->F(FC_J));
+  if (h->ext_derivs) {
+    s = tc_synth_vector(h, h->work(5), h->work(6), x->F(FC_J));
+  } else {
+    { ProfScope p(h, "spectral_curl");
+      launch_curl_img(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR),
+                      h->field(F_BPOL), image_out(h, x->d_bimg_vc)); }
+    s = tc_synth_vector(h, nullptr, nullptr, x->F(FC_J));
+  }
   if (s) return s;
   FusedArgs f = phase_args(h);
   const float4* fin[4] = {x->F(FC_U), x->F(FC_U + 1), x->F(FC_B), x->F(FC_B + 1)};

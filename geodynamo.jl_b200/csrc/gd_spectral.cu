@@ -83,9 +83,9 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
                             const double* __restrict__ T, double* __restrict__ gth, double* __restrict__ gph,
                             double* __restrict__ gr, SynthImageOut img) {
   constexpr int NB = 2 * KL + 1;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
   const int k0 = blockIdx.y * RB_R;
-  if (j >= d.nlm) return;
+  if (j >= d.jhi) return;
   const int l = lof[j], m = mof[j];
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   const int N = d.nr;
@@ -159,14 +159,14 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
 
 void launch_gradients(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                       const double* d1, const double* T, double* gth, double* gph, double* gr) {
-  dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
+  dim3 grid(ceil_div(d.jhi - d.jlo, 128), ceil_div(d.nr, RB_R));
   // the band half-width is validated to GD_MAX_KL at creation
   k_gradients<GD_MAX_KL, false><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr, SynthImageOut{});
 }
 
 void launch_gradients_img(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                           const double* d1, const double* T, const SynthImageOut& img) {
-  dim3 grid(ceil_div(d.nlm, 128), ceil_div(d.nr, RB_R));
+  dim3 grid(ceil_div(d.jhi - d.jlo, 128), ceil_div(d.nr, RB_R));
   k_gradients<GD_MAX_KL, true><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, nullptr, nullptr, nullptr, img);
 }
 
@@ -188,11 +188,11 @@ __global__ void __launch_bounds__(RAD_THREADS, 4) k_curl(Dims d, const int* __re
   extern __shared__ __align__(16) unsigned char rad_smem[];
   auto& st = *reinterpret_cast<RadialStage<KL, 2>*>(rad_smem);
   const int tid = threadIdx.x;
-  const int j = blockIdx.x * RAD_THREADS + tid;
+  const int j = d.jlo + blockIdx.x * RAD_THREADS + tid;
   const int k0 = blockIdx.y * rows;
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   const int N = d.nr;
-  const bool live = j < d.nlm;
+  const bool live = j < d.jhi;
   if (live) stage_column<KL>(st.win, pol, plane, NM, N, k0, rows, j);
   stage_band<KL>(st.band[0], d1, N, k0, rows);
   stage_band<KL>(st.band[1], d2, N, k0, rows);
@@ -251,7 +251,7 @@ void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* ri
                  const double* d1, const double* d2, const double* tor, const double* pol, double* otor,
                  double* opol) {
   const int rows = radial_rows(d.nr);
-  dim3 grid(ceil_div(d.nlm, RAD_THREADS), ceil_div(d.nr, rows));
+  dim3 grid(ceil_div(d.jhi - d.jlo, RAD_THREADS), ceil_div(d.nr, rows));
   const size_t smem = radial_smem<GD_MAX_KL, 2>();
   allow_dynamic_smem(k_curl<GD_MAX_KL, false>, smem);
   k_curl<GD_MAX_KL, false><<<grid, RAD_THREADS, smem, s>>>(d, lof, nullptr, rinv, rinv2, d1, d2, tor, pol, otor,
@@ -262,7 +262,7 @@ void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* m
                      const double* rinv2, const double* d1, const double* d2, const double* tor, const double* pol,
                      const SynthImageOut& img) {
   const int rows = radial_rows(d.nr);
-  dim3 grid(ceil_div(d.nlm, RAD_THREADS), ceil_div(d.nr, rows));
+  dim3 grid(ceil_div(d.jhi - d.jlo, RAD_THREADS), ceil_div(d.nr, rows));
   const size_t smem = radial_smem<GD_MAX_KL, 2>();
   allow_dynamic_smem(k_curl<GD_MAX_KL, true>, smem);
   k_curl<GD_MAX_KL, true><<<grid, RAD_THREADS, smem, s>>>(d, lof, mof, rinv, rinv2, d1, d2, tor, pol, nullptr,
@@ -272,8 +272,8 @@ void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* m
 // apply_temperature_boundary_conditions_spectral! (src/thermal.jl:262-303):
 // Dirichlet rows r = ri and r = ro of the temperature state.
 __global__ void k_temperature_bc(Dims d, const double* __restrict__ bv, double* __restrict__ T) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= d.nlm) return;
+  const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.jhi) return;
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   T[j] = bv[j];
   T[plane + j] = 0.0;
@@ -282,7 +282,7 @@ __global__ void k_temperature_bc(Dims d, const double* __restrict__ bv, double* 
 }
 
 void launch_temperature_bc(cudaStream_t s, const Dims& d, const double* bvals_native, double* T) {
-  k_temperature_bc<<<ceil_div(d.nlm, 256), 256, 0, s>>>(d, bvals_native, T);
+  k_temperature_bc<<<ceil_div(d.jhi - d.jlo, 256), 256, 0, s>>>(d, bvals_native, T);
 }
 
 __global__ void k_perm(int nlm, size_t rows, const int* __restrict__ perm, const double* __restrict__ src,

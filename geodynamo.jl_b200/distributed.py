@@ -159,3 +159,154 @@ def energy_partial(x_mode, dec: Decomposition, rank: int, lof: np.ndarray):
     l = torch.as_tensor(lof[j0:j1], dtype=x_mode.dtype, device=x_mode.device)
     w = 1.0 / torch.clamp(l * (l + 1.0), min=1.0)
     return 0.5 * float((x_mode ** 2 * w).sum())
+
+
+class DistributedStep:
+    """The headline step of one model across the ranks of a process group.
+
+    Rank k owns the m columns ``dec.modes[k]`` (native mode range) for the radial
+    half of the step and the shells ``dec.shells[k]`` for the transform half:
+
+    1. ``mode.derivatives``: grad T, curl u, curl B of its modes (all shells);
+    2. all-to-all: the five state fields and the seven derivative arrays, its
+       modes x each rank's shells, to the shell-slab handles;
+    3. ``shell``: the three nonlinear phases on its shells (all modes), with
+       the derivatives received instead of computed
+       (``set_external_derivatives``); the grids carried from step to step
+       (the reference's ordering) stay with the shells;
+    4. all-to-all: the five nonlinear terms, its shells x each rank's modes,
+       back to the mode handles;
+    5. ``mode.implicit_modes``: temperature Dirichlet rows, CNAB2 and the
+       history roll of its modes.
+
+    Each rank keeps a full-size mode handle (only its own columns are current)
+    and a shell-slab handle of its shells.  ``device_exchange``: the blocks go
+    through device buffers (NCCL); otherwise through pinned host buffers (gloo).
+    Every kernel computes each column or row independently, so the result equals
+    the single-handle step's bit for bit (tests/test_gpu_distributed_step.py)."""
+
+    STATE_FIELDS = (0, 1, 2, 3, 4)
+    DERIVED = (0, 1, 2, 3, 4, 5, 6)
+
+    def __init__(self, gdb, cfg: dict, rank: int, world: int, group=None, device: int = 0,
+                 precision: str = "fp64", device_exchange: bool = False):
+        import torch
+
+        c = dict(cfg)
+        lmax, nlat, nlon, nr = c.pop("lmax"), c.pop("nlat"), c.pop("nlon"), c.pop("nr")
+        mmax = c.pop("mmax", None)
+        self.rank, self.world, self.group = rank, world, group
+        self.dec = Decomposition(nr, lmax, mmax, world)
+        if min(self.dec.nshell(k) for k in range(world)) < 3:
+            raise ValueError("every rank needs at least three shells")
+        self.mode = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, mmax=mmax, device=device, **c)
+        s0, s1 = self.dec.shells[rank]
+        self.shell = gdb.SHTnsKitConfig(lmax, nlat, nlon, s1 - s0, mmax=mmax, precision=precision, device=device, **c)
+        self.shell.set_external_derivatives(True)
+        self.nr = nr
+        self.magnetic = c.get("magnetic", 1)
+        self.torch = torch
+        self.dev = torch.device("cuda", device) if device_exchange else torch.device("cpu")
+        self.pin = not device_exchange and torch.cuda.is_available()
+        self._bufs = {}
+
+    # -- state ---------------------------------------------------------------------
+    def set_field(self, name, re, im):
+        self.mode.set_field(name, re, im)
+
+    def set_temperature_bc(self, bvals=None, sources=None):
+        self.mode.set_temperature_bc(bvals, None)
+        if sources is not None:
+            s0, s1 = self.dec.shells[self.rank]
+            self.shell.set_temperature_bc(None, np.asarray(sources, dtype=np.float64)[s0:s1])
+
+    def own_modes(self, name):
+        """(re, im) of this rank's m columns of a state field, shape (nr, j1 - j0) each (native order)."""
+        j0, j1 = self.dec.modes[self.rank]
+        buf = self._buf(2 * self.nr * (j1 - j0))
+        self.mode.copy_block(0, FIELD_IDS[name], 0, self.nr, j0, j1, buf.data_ptr(), True)
+        a = buf.cpu().numpy().reshape(2, self.nr, j1 - j0)
+        return a[0].copy(), a[1].copy()
+
+    def energy(self, lof_native):
+        """Kinetic and magnetic energy (the reference's formula) summed over every rank's modes."""
+        import torch.distributed as dist
+        parts = []
+        for names in (("u_tor", "u_pol"), ("b_tor", "b_pol")):
+            x = np.stack([np.stack(self.own_modes(n)) for n in names])  # (2, 2, nr, nmode)
+            parts.append(energy_partial(self.torch.as_tensor(x), self.dec, self.rank, lof_native))
+        t = self.torch.tensor(parts, dtype=self.torch.float64)
+        dist.all_reduce(t, group=self.group)
+        return float(t[0]), float(t[1])
+
+    # -- the step --------------------------------------------------------------------
+    def _buf(self, n, tag=None):
+        """An exchange buffer of n doubles; tagged buffers are kept between steps
+        (page-locking host memory costs far more than one exchange)."""
+        if tag is not None and tag in self._bufs and self._bufs[tag].numel() == n:
+            return self._bufs[tag]
+        t = self.torch.empty(n, dtype=self.torch.float64, device=self.dev)
+        t = t.pin_memory() if self.pin else t
+        if tag is not None:
+            self._bufs[tag] = t
+        return t
+
+    def _exchange(self, src_handle, dst_handle, items, send_block, recv_block):
+        """One all-to-all of spectral blocks: items = [(array, field)], send_block(k) /
+        recv_block(k) = ((r0, r1), (j0, j1)) of the block sent to / received from rank k."""
+        import torch.distributed as dist
+        sizes_s = [2 * (b[0][1] - b[0][0]) * (b[1][1] - b[1][0]) for b in map(send_block, range(self.world))]
+        sizes_r = [2 * (b[0][1] - b[0][0]) * (b[1][1] - b[1][0]) for b in map(recv_block, range(self.world))]
+        ni = len(items)
+        tag = (id(src_handle), len(items))
+        send = self._buf(ni * sum(sizes_s), ("send",) + tag)
+        recv = self._buf(ni * sum(sizes_r), ("recv",) + tag)
+        off = 0
+        for k in range(self.world):
+            (r0, r1), (j0, j1) = send_block(k)
+            for (arr, f) in items:
+                if sizes_s[k]:
+                    src_handle.copy_block(arr, f, r0, r1, j0, j1, send[off:].data_ptr(), True)
+                off += sizes_s[k]
+        dist.all_to_all_single(recv, send, [ni * n for n in sizes_r], [ni * n for n in sizes_s], group=self.group)
+        off = 0
+        for k in range(self.world):
+            (r0, r1), (j0, j1) = recv_block(k)
+            for (arr, f) in items:
+                if sizes_r[k]:
+                    dst_handle.copy_block(arr, f, r0, r1, j0, j1, recv[off:].data_ptr(), False)
+                off += sizes_r[k]
+
+    def step(self, n=1):
+        me = self.rank
+        j0, j1 = self.dec.modes[me]
+        s0, s1 = self.dec.shells[me]
+        ns = s1 - s0
+        fields = self.STATE_FIELDS if self.magnetic else (0, 1, 4)
+        derived = self.DERIVED if self.magnetic else (0, 1, 2, 3, 4)
+        out_items = [(0, f) for f in fields] + [(1, k) for k in derived]
+        nl_items = [(2, f) for f in fields]
+        for _ in range(n):
+            self.mode.derivatives(j0, j1)
+            # mode layout (its modes, every shell) -> shell layout (its shells, every mode)
+            self._exchange(self.mode, self.shell, out_items,
+                           lambda k: (self.dec.shells[k], (j0, j1)),
+                           lambda k: ((0, ns), self.dec.modes[k]))
+            # the whole handle's CNAB2 step order: the temperature phase reads the
+            # velocity grids carried from the previous step
+            self.shell.temperature_nl()
+            self.shell.velocity_nl()
+            if self.magnetic:
+                self.shell.magnetic_nl()
+            # nonlinear terms back: shell layout -> mode layout
+            self._exchange(self.shell, self.mode, nl_items,
+                           lambda k: ((0, ns), self.dec.modes[k]),
+                           lambda k: (self.dec.shells[k], (j0, j1)))
+            self.mode.implicit_modes(j0, j1)
+
+    def close(self):
+        self.shell.close()
+        self.mode.close()
+
+
+FIELD_IDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4}

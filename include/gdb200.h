@@ -320,6 +320,41 @@ int gd_ensemble_failed_member(const gd_ensemble* e);
  * joined to it, so events recorded on it bracket whole ensemble steps. */
 int gd_ensemble_get_stream(gd_ensemble* e, void** stream);
 
+/* ---- the step decomposed across ranks ---------------------------------------------
+ * The reference distributes its step over MPI pencils (src/pencil_decomps.jl:
+ * 136-284).  Here a rank owns whole m columns (native mode range [j0, j1),
+ * j = moff[m] + l - m) for the radial half of the step -- the radial
+ * derivatives and the CNAB2 solve, which couple every shell of a mode -- and a
+ * slab of shells for the transform half -- syntheses, products, analyses, which
+ * are independent per shell -- with one all-to-all of spectral blocks in each
+ * direction between the halves:
+ *   gd_derivatives(mode handle, j0, j1)          grad T, curl u, curl B -> work arrays
+ *   (exchange: state and derivatives of its modes -> the shell-slab handles)
+ *   gd_*_nonlinear(shell-slab handle)            with gd_set_external_derivatives(1)
+ *   (exchange: nonlinear terms of its shells -> the mode handles)
+ *   gd_implicit_modes(mode handle, j0, j1)       temperature Dirichlet rows, CNAB2, history roll
+ *
+ * Radial derivatives of the state (compute_all_gradients_spectral!,
+ * compute_vorticity_spectral_full!, compute_current_density_spectral!) for the
+ * modes [j0, j1) only, into the handle's work arrays (0-2: grad T theta, phi,
+ * r; 3-4: curl u toroidal, poloidal; 5-6: curl B). */
+int gd_derivatives(gd_handle* h, int j0, int j1);
+/* The temperature Dirichlet rows and the CNAB2 solve (build_rhs_cnab2! +
+ * solve_implicit_step!) for the modes [j0, j1) only, with the nonlinear terms in
+ * the handle's current bank, then the step's history roll.  CNAB2 only. */
+int gd_implicit_modes(gd_handle* h, int j0, int j1);
+/* enable != 0: the nonlinear phases take the radial derivatives from the work
+ * arrays instead of computing them, and leave the temperature Dirichlet rows to
+ * the solve side (a shell-slab handle: nr = its shells, the sources of its
+ * shells set with gd_set_temperature_bc). */
+int gd_set_external_derivatives(gd_handle* h, int enable);
+/* Copies the block [shells r0..r1) x [modes j0..j1) of one spectral array
+ * between the handle and buf (device or pinned host memory), both planes:
+ * buf = [Re, Im][r1 - r0][j1 - j0] doubles.  array 0: state field (GD_U_TOR ..
+ * GD_TEMP); 1: work array 0-7; 2: nonlinear term of the current bank.
+ * to_buf != 0 copies from the handle into buf.  Synchronises the stream. */
+int gd_copy_block(gd_handle* h, int array, int field, int r0, int r1, int j0, int j1, void* buf, int to_buf);
+
 /* ---- error-path testing ----------------------------------------------------------
  * No counterpart in the reference.  Every wait of the tensor-core pipelines is
  * bounded: when one runs out the kernel records it, lets its copies in flight

@@ -56,3 +56,12 @@ def test_transpose_roundtrip(world):
 def test_distributed_phase_matches_whole_array():
     import dist_workers
     spawn(dist_workers.phase_matches_global, 2)
+
+
+@pytest.mark.parametrize("world,magnetic", [(2, 1), (3, 1), (2, 0)])
+def test_distributed_step_exchanges(world, magnetic):
+    """The two exchanges of the distributed step (state + derivatives to the
+    shell slabs, nonlinear terms back to the mode columns) over fake handles
+    give the whole handle's result bit for bit."""
+    import dist_workers
+    spawn(dist_workers.distributed_step_fake, world, magnetic)
