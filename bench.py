@@ -23,9 +23,13 @@ Other measurements (one JSON line each, instead of the headline):
   --scheme S         the headline step under ts_scheme = S (cnab2, eab2, erk2)
   --workload W       a smaller named shell for profiling captures
 
-Multi-GPU (torchrun): the step does not shard without a transpose, so every
-rank runs an independent replica of the same workload ("replicas only", weak
-scaling); value = N x steps / max-over-ranks time.
+Multi-GPU (torchrun): by default every rank runs an independent replica of the
+same workload (weak scaling; value = N x steps / max-over-ranks time).
+  --decomposed       one model across the ranks (strong scaling): each rank
+                     owns whole m columns for the radial derivatives and CNAB2
+                     and a slab of shells for the transforms and products, with
+                     two NCCL all-to-alls per step through device buffers
+                     (distributed.DistributedStep); time = max over ranks
 """
 import argparse
 import json
@@ -322,6 +326,52 @@ def run_ensemble(args, gdb, workloads, torch):
     return 0
 
 
+def run_decomposed(args, gdb, workloads, torch, world, rank, local):
+    """One model stepped across `world` ranks by distributed.DistributedStep over
+    NCCL (device exchange buffers); steps/s of that model, time = max over ranks."""
+    import datetime
+    import torch.distributed as dist
+    import distributed as D
+    for k, v in (("MASTER_ADDR", "127.0.0.1"), ("MASTER_PORT", "29533"), ("RANK", "0"), ("WORLD_SIZE", "1")):
+        os.environ.setdefault(k, v)  # a single rank without torchrun
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                            device_id=torch.device("cuda", local))
+    p = workload_params()
+    prec = args.precision if args.precision != "auto" else "mixed_vel64"
+    keys = ("dt", "rratio", "ekman", "rayleigh", "prandtl", "magnetic_prandtl", "implicit_theta")
+    cfg = dict(lmax=p["lmax"], nlat=p["nlat"], nlon=p["nlon"], nr=p["nr"], **{k: p[k] for k in keys})
+    ds = D.DistributedStep(gdb, cfg, rank, world, device=local, precision=prec, device_exchange=True)
+    for k, (a, b) in workloads.seeded_state(p["lmax"], p["lmax"], p["nr"], seed=0).items():
+        ds.set_field(k, a, b)
+    ds.step(args.warmup)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ds.step(args.steps)
+    torch.cuda.synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t[0]) / args.steps
+    ek, em = ds.energy(D.native_l(p["lmax"], p["lmax"]))
+    xbytes = ds.dec.exchange_bytes(12) + ds.dec.exchange_bytes(5)
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"CNAB2 steps/s {WORKLOAD} decomposed over {world} ranks", "value": 1e3 / ms,
+            "unit": "steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": prec,
+            "data": "synthetic (seeded_state seed 0)",
+            "config": {"workload": WORKLOAD, "layout": "m columns (derivatives, CNAB2) / shell slabs (transforms)",
+                       "exchange": "NCCL all_to_all_single, device buffers", "exchange_bytes_per_step": xbytes},
+            "energy": {"e_kin": ek, "e_mag": em}}), flush=True)
+    ds.close()
+    dist.destroy_process_group()
+    return 0
+
+
 def run_transforms(args, gdb, workloads, torch):
     """Transform-only configuration: forward + inverse scalar transforms at
     lmax 127 over 97 shells x 9 fields (seeded, (l+1)^-1.5), FP64 and mixed:
@@ -569,6 +619,8 @@ def main():
                     help="instead of the headline: the adjoint configuration's gradient checks and timings")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead of the headline: the batched uneven ensemble of this many shells")
+    ap.add_argument("--decomposed", action="store_true",
+                    help="one model across the ranks (mode/shell decomposition, NCCL all-to-alls)")
     ap.add_argument("--scheme", default="cnab2", choices=["cnab2", "eab2", "erk2"],
                     help="time-stepping scheme of the step (ts_scheme); the headline metric is CNAB2")
     args = ap.parse_args()
@@ -589,6 +641,8 @@ def main():
     torch.cuda.set_device(local)
     if args.ensemble > 0:
         return run_ensemble(args, gdb, workloads, torch)
+    if args.decomposed:
+        return run_decomposed(args, gdb, workloads, torch, world, rank, local)
     if args.adjoint:
         return run_adjoint(args, gdb, workloads, torch)
     if args.transforms:

@@ -127,9 +127,11 @@ __global__ void __launch_bounds__(256, 2) k_synth_scalar(Dims d, const int* __re
     cpa_commit();
     const double* As = smem + (ch % LEG_STAGES) * SS_STAGE;
     const double* Bs = As + SS_KC * SS_SA;
-    // two K steps of 8 degrees of this warp's parity: rows q0 (k = 8 ks + t) and q1 (k + 4)
+    // two K steps of 8 degrees of this warp's parity: rows q0 (k = 8 ks + t) and q1 (k + 4);
+    // a step whose 16 degrees all lie past L only adds zero products and is skipped
 #pragma unroll
     for (int ks = 0; ks < SS_KC / 16; ++ks) {
+      if (m + ch * SS_KC + 16 * ks > d.L) break;
       const int q0 = 2 * (8 * ks + t) + par, q1 = q0 + 8;
       double af[2][4], bf[4][2];
 #pragma unroll
@@ -149,7 +151,8 @@ __global__ void __launch_bounds__(256, 2) k_synth_scalar(Dims d, const int* __re
       for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          dmma16(acc[2 * i][j][0], acc[2 * i][j][1], acc[2 * i + 1][j][0], acc[2 * i + 1][j][1], af[i], bf[j]);
+          if (n0 + nw + 8 * j < Ntot)  // column blocks past the last column stay zero
+            dmma16(acc[2 * i][j][0], acc[2 * i][j][1], acc[2 * i + 1][j][0], acc[2 * i + 1][j][1], af[i], bf[j]);
     }
   }
   cpa_wait<0>();
@@ -273,6 +276,7 @@ __global__ void __launch_bounds__(256, 2) k_synth_vector(Dims d, const int* __re
     const double* Bs = As + 2 * VS_KC * VS_SA;
 #pragma unroll
     for (int ks = 0; ks < VS_KC / 16; ++ks) {
+      if (m + ch * VS_KC + 16 * ks > d.L) break;  // only zero products left
       const int q0 = 2 * (8 * ks + t) + par, q1 = q0 + 8;
       double af[2][4], bf[2][2][2];
 #pragma unroll
@@ -297,8 +301,9 @@ __global__ void __launch_bounds__(256, 2) k_synth_vector(Dims d, const int* __re
         for (int y = 0; y < 2; ++y)
 #pragma unroll
           for (int j = 0; j < 2; ++j)
-            dmma16(acc[x][y][0][j][0], acc[x][y][0][j][1], acc[x][y][1][j][0], acc[x][y][1][j][1], af[x],
-                   bf[y][j]);
+            if (n0 + nw + 8 * j < Ntot)
+              dmma16(acc[x][y][0][j][0], acc[x][y][0][j][1], acc[x][y][1][j][0], acc[x][y][1][j][1], af[x],
+                     bf[y][j]);
     }
   }
   cpa_wait<0>();

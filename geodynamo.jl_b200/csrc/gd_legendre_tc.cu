@@ -46,6 +46,14 @@ __device__ __host__ __forceinline__ int nck_h(int L, int m, int p) {
   return (k + TC_K - 1) / TC_K;
 }
 
+// Degree tiles of the analysis: 128 rows of one parity each, enough for the
+// even parity of m = 0 (lmax <= 255 takes one).
+__device__ __host__ __forceinline__ int nlt_of(int L) { return ((L + 2) / 2 + TC_M - 1) / TC_M; }
+// Rows of parity p of order m that fall in degree tile lt.
+__device__ __forceinline__ int krows(int L, int m, int p, int lt) {
+  return max(0, min(TC_M, kpar(L, m, p) - TC_M * lt));
+}
+
 // chunk index of the synthesis image for (m, theta tile, parity, k chunk)
 __device__ __forceinline__ long synth_chunk(const long* cofs, int L, int m, int tile, int p, int kc) {
   const int n0 = nck_h(L, m, 0), n1 = nck_h(L, m, 1);
@@ -82,7 +90,7 @@ __device__ __forceinline__ void issue_chunk(uint32_t tmem, uint32_t dcol, const 
 // Table images.
 // Synthesis chunk (m, tile, p, kc): row r -> ith = 128 tile + r,
 //   k -> l = m + p + 2 (32 kc + k).
-// Analysis chunk (m, p, c): row i -> l = m + p + 2 i, k -> ith = 32 c + k.
+// Analysis chunk (m, p, lt, c): row i -> l = m + p + 2 (128 lt + i), k -> ith = 32 c + k.
 // ---------------------------------------------------------------------------
 __global__ void k_build_synth_image(Dims d, const int* __restrict__ moff, const long* __restrict__ cofs,
                                     const double* __restrict__ T, float* __restrict__ img) {
@@ -112,15 +120,15 @@ __global__ void k_build_synth_image(Dims d, const int* __restrict__ moff, const 
 __global__ void k_build_analysis_image(Dims d, const int* __restrict__ moff, const double* __restrict__ T,
                                        float* __restrict__ img) {
   const int m = blockIdx.z;
-  const int nthc = (d.nth + TC_K - 1) / TC_K;
-  const int p = blockIdx.y / nthc, c = blockIdx.y % nthc;
-  float* hi = img + ((long)(m * 2 + p) * nthc + c) * CHUNK_FLOATS;
+  const int nthc = (d.nth + TC_K - 1) / TC_K, nlt = nlt_of(d.L);
+  const int p = blockIdx.y / (nlt * nthc), lt = (blockIdx.y / nthc) % nlt, c = blockIdx.y % nthc;
+  float* hi = img + (((long)(m * 2 + p) * nlt + lt) * nthc + c) * CHUNK_FLOATS;
   float* lo = hi + TILE_A_FLOATS;
-  const int kp = (p == 0) ? (d.L - m + 2) / 2 : (d.L - m + 1) / 2;
+  const int kp = krows(d.L, m, p, lt);
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < TC_M * TC_K; e += gridDim.x * blockDim.x) {
     const int row = e / TC_K, k = e % TC_K;
     const int ith = TC_K * c + k;
-    const int l = m + p + 2 * row;
+    const int l = m + p + 2 * (TC_M * lt + row);
     double v = 0.0;
     if (row < kp && ith < d.nth && l <= d.L) v = T[(size_t)(moff[m] + l - m) * d.nth + ith];
     const float h = tf32_rn((float)v);
@@ -137,7 +145,9 @@ long tc_synth_chunks(const Dims& d, std::vector<long>& cofs) {
   for (int m = 0; m <= d.M; ++m) cofs[m + 1] = cofs[m] + (long)ntile * (nck_h(d.L, m, 0) + nck_h(d.L, m, 1));
   return cofs[d.M + 1];
 }
-long tc_analysis_chunks(const Dims& d) { return (long)(d.M + 1) * 2 * ((d.nth + TC_K - 1) / TC_K); }
+long tc_analysis_chunks(const Dims& d) {
+  return (long)(d.M + 1) * 2 * nlt_of(d.L) * ((d.nth + TC_K - 1) / TC_K);
+}
 size_t tc_chunk_bytes() { return (size_t)CHUNK_FLOATS * 4; }
 
 void launch_build_tc_images(cudaStream_t s, const Dims& d, const int* moff, const long* cofs, const double* T,
@@ -149,7 +159,7 @@ void launch_build_tc_images(cudaStream_t s, const Dims& d, const int* moff, cons
   }
   if (anal_img) {
     const int nthc = (d.nth + TC_K - 1) / TC_K;
-    k_build_analysis_image<<<dim3(8, 2 * nthc, d.M + 1), 256, 0, s>>>(d, moff, T, anal_img);
+    k_build_analysis_image<<<dim3(8, 2 * nlt_of(d.L) * nthc, d.M + 1), 256, 0, s>>>(d, moff, T, anal_img);
   }
 }
 
@@ -502,7 +512,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
 }
 
 // ---------------------------------------------------------------------------
-// Analysis.  CTA = (m, column tile); K = colatitude in chunks of 32; two
+// Analysis.  CTA = (m, degree tile, column tile); K = colatitude in chunks of 32; two
 // loader groups of 4 warps (group g fills stage g: bulk copies of the table
 // chunks, FP32 inputs split to TF32 hi/lo while written) and one MMA warp.
 // Scalar: 128 columns n = (field, r, re/im), one step per (theta chunk,
@@ -564,10 +574,13 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
   bool ok = true;
   int issued = -1;  // loader thread 0 of a group: last use of its stage with bulk copies issued
   int gs = 0;       // pipeline steps of the earlier tiles
-  const int ntiles = (d.M + 1) * ncol;
-  // persistent CTA: tiles (m, column tile), m-major
+  const int nlt = nlt_of(L);
+  const int ntiles = (d.M + 1) * nlt * ncol;
+  // persistent CTA: tiles (m, degree tile, column tile), m-major; a degree
+  // tile past both parities' last degree of its order has no work
   for (int tt = blockIdx.x; tt < ntiles && ok; tt += gridDim.x) {
-  const int m = tt / ncol, ct = tt % ncol;
+  const int m = tt / (nlt * ncol), lt = (tt / ncol) % nlt, ct = tt % ncol;
+  if (krows(L, m, 0, lt) == 0) continue;
   const int mb = moff[m];
   // balanced column tiles: vector csz shells, scalar csz column pairs
   const int n0 = ct * 2 * csz;
@@ -598,10 +611,10 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
     __syncthreads();
   }
 
-  const int k1 = kpar(L, m, 1);
+  const int k1 = krows(L, m, 1, lt);
   const int np = k1 > 0 ? 2 : 1;
   // scalar: steps (chunk, parity); vector: steps (chunk, fold), both folds
-  // always (with k1 = 0 the odd-parity chunks hold zeros)
+  // always (with k1 = 0 no odd-parity rows are copied or read)
   const int ns = VEC ? 2 : np;
   const int T = nthc * ns;
 
@@ -646,16 +659,16 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
         // rows the epilogue never reads: copy whole 8-row swizzle atoms of
         // the valid ones (hi and lo images separately)
         const int pa0 = VEC ? 1 - p : p, pa1 = p;  // parity of the first / second table chunk
-        const uint32_t ra0 = (uint32_t)((kpar(L, m, pa0) + 7) & ~7) * 128u;
-        const uint32_t ra1 = VEC ? (uint32_t)((kpar(L, m, pa1) + 7) & ~7) * 128u : 0u;
+        const uint32_t ra0 = (uint32_t)((krows(L, m, pa0, lt) + 7) & ~7) * 128u;
+        const uint32_t ra1 = VEC ? (uint32_t)((krows(L, m, pa1, lt) + 7) & ~7) * 128u : 0u;
         mbar_expect_tx(&full[g], 2u * (ra0 + ra1));
-        const float* s0 = img0 + ((long)(m * 2 + pa0) * nthc + cc) * CHUNK_FLOATS;
+        const float* s0 = img0 + (((long)(m * 2 + pa0) * nlt + lt) * nthc + cc) * CHUNK_FLOATS;
         if (ra0 > 0) {
           bulk_g2s(A, s0, ra0, &full[g]);
           bulk_g2s(A + TILE_A_FLOATS, s0 + TILE_A_FLOATS, ra0, &full[g]);
         }
         if (VEC && ra1 > 0) {
-          const float* s1 = img1 + ((long)(m * 2 + pa1) * nthc + cc) * CHUNK_FLOATS;
+          const float* s1 = img1 + (((long)(m * 2 + pa1) * nlt + lt) * nthc + cc) * CHUNK_FLOATS;
           bulk_g2s(A + CHUNK_FLOATS, s1, ra1, &full[g]);
           bulk_g2s(A + CHUNK_FLOATS + TILE_A_FLOATS, s1 + TILE_A_FLOATS, ra1, &full[g]);
         }
@@ -709,8 +722,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) k_tc_analysis3(Dims d, const in
     const int i = q * 32 + lane;
     const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
     for (int p = 0; p < np; ++p) {
-      const int kp = kpar(L, m, p);
-      const int l = m + p + 2 * i;
+      const int kp = krows(L, m, p, lt);
+      const int l = m + p + 2 * (TC_M * lt + i);
       if (!VEC) {
         for (int c0 = (NC / 2) * half; c0 < (NC / 2) * half + NC / 2 && c0 < nw; c0 += 8) {
           float v[8];
@@ -833,12 +846,12 @@ void launch_tc_analysis(cudaStream_t s, const Dims& d, const int* moff, const fl
   set_attrs();
   if (a.epi == EPI_SCALAR) {
     const int npair = a.nf * d.nr, ncol = ceil_div(2 * npair, TC_N2), csz = ceil_div(npair, ncol);
-    const int ntiles = (d.M + 1) * ncol;
+    const int ntiles = (d.M + 1) * nlt_of(d.L) * ncol;
     k_tc_analysis3<false><<<std::min(ntiles, sm_count()), WS_THREADS, analysis_smem(false), s>>>(d, moff, img0,
                                                                                                 img1, a, ncol, csz);
   } else {
     const int ncol = ceil_div(d.nr, 32), csz = ceil_div(d.nr, ncol);
-    const int ntiles = (d.M + 1) * ncol;
+    const int ntiles = (d.M + 1) * nlt_of(d.L) * ncol;
     k_tc_analysis3<true><<<std::min(ntiles, sm_count()), WS_THREADS, analysis_smem(true), s>>>(d, moff, img0, img1,
                                                                                               a, ncol, csz);
   }

@@ -235,7 +235,7 @@ class DistributedStep:
         for names in (("u_tor", "u_pol"), ("b_tor", "b_pol")):
             x = np.stack([np.stack(self.own_modes(n)) for n in names])  # (2, 2, nr, nmode)
             parts.append(energy_partial(self.torch.as_tensor(x), self.dec, self.rank, lof_native))
-        t = self.torch.tensor(parts, dtype=self.torch.float64)
+        t = self.torch.tensor(parts, dtype=self.torch.float64, device=self.dev)
         dist.all_reduce(t, group=self.group)
         return float(t[0]), float(t[1])
 
@@ -269,6 +269,9 @@ class DistributedStep:
                     src_handle.copy_block(arr, f, r0, r1, j0, j1, send[off:].data_ptr(), True)
                 off += sizes_s[k]
         dist.all_to_all_single(recv, send, [ni * n for n in sizes_r], [ni * n for n in sizes_s], group=self.group)
+        if self.dev.type == "cuda":
+            # the handles' copies run on their own streams: wait for the exchange
+            self.torch.cuda.current_stream(self.dev).synchronize()
         off = 0
         for k in range(self.world):
             (r0, r1), (j0, j1) = recv_block(k)

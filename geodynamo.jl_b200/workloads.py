@@ -23,6 +23,9 @@ CONFIGS = {
     "shell_l31_nr32": dict(lmax=31, nlat=48, nlon=96, nr=32, dt=1e-5, steps=100),
     "transform_l127_nr97x9": dict(lmax=127, nlat=192, nlon=384, nr=97, nfield=9),
     "shell_l255_nr129": dict(lmax=255, nlat=384, nlon=768, nr=129, dt=2e-6, steps=1000),
+    # the scale-out grid of the shell/mode decomposition (lmax 511 on the
+    # headline radial grid)
+    "shell_l511_nr129": dict(lmax=511, nlat=768, nlon=1536, nr=129, dt=1e-6, steps=100),
     # the same shell with 33 radial levels: per-shell kernel work of the headline
     # workload at a quarter of its memory (profiling captures)
     "shell_l255_nr33": dict(lmax=255, nlat=384, nlon=768, nr=33, dt=2e-6, steps=100),

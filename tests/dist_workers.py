@@ -10,12 +10,12 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "geodynamo.jl_b200"))
 
 
-def _init(rank, world, port):
+def _init(rank, world, port, backend="gloo"):
     import datetime
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    dist.init_process_group(backend, rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     return dist
 
 
@@ -212,24 +212,28 @@ def distributed_step_fake(rank, world, port, magnetic):
         dist.destroy_process_group()
 
 
-def distributed_step_device(rank, world, port, precision, steps, magnetic):
+def distributed_step_device(rank, world, port, precision, steps, magnetic, grid=(31, 48, 96, 12), nccl=False):
     """DistributedStep on the device (every rank on cuda:0, gloo over pinned host
-    buffers) against one whole handle, bit for bit."""
+    buffers; nccl: one rank, NCCL over device buffers) against one whole handle,
+    bit for bit; grid = (lmax, nlat, nlon, nr)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from conftest import load_package
     gdb = load_package()
     import distributed as D
     import workloads
-    dist = _init(rank, world, port)
+    import torch
+    if nccl:
+        torch.cuda.set_device(0)
+    dist = _init(rank, world, port, "nccl" if nccl else "gloo")
     try:
-        lmax, nlat, nlon, nr = 31, 48, 96, 12
+        lmax, nlat, nlon, nr = grid
         phys = dict(workloads.SHELL_PHYSICS)
         cfg = dict(lmax=lmax, nlat=nlat, nlon=nlon, nr=nr, dt=1e-5, magnetic=magnetic, **phys)
         st = workloads.seeded_state(lmax, lmax, nr, seed=7, amp=1e-1)
         src = np.linspace(0.5, 1.5, nr)
         c = dict(cfg)
         whole = gdb.SHTnsKitConfig(c.pop("lmax"), c.pop("nlat"), c.pop("nlon"), c.pop("nr"), precision=precision, **c)
-        ds = D.DistributedStep(gdb, cfg, rank, world, precision=precision)
+        ds = D.DistributedStep(gdb, cfg, rank, world, precision=precision, device_exchange=nccl)
         names = workloads.FIELD_ORDER if magnetic else ("u_tor", "u_pol", "temp")
         for n in names:
             whole.set_field(n, *st[n])

@@ -30,3 +30,13 @@ def test_distributed_step_matches_one_handle(precision, magnetic, world):
     import dist_workers
     mp.start_processes(dist_workers.distributed_step_device, args=(world, free_port(), precision, 5, magnetic),
                        nprocs=world, start_method="spawn", join=True)
+
+
+def test_distributed_step_nccl_device_buffers():
+    """The NCCL path (device exchange buffers) on one rank: the exchanges are
+    copies through device memory and the step still equals one handle's."""
+    import torch.multiprocessing as mp
+    import dist_workers
+    mp.start_processes(dist_workers.distributed_step_device,
+                       args=(1, free_port(), "mixed_vel64", 3, 1, (31, 48, 96, 12), True),
+                       nprocs=1, start_method="spawn", join=True)
