@@ -330,7 +330,8 @@ int gd_ensemble_get_stream(gd_ensemble* e, void** stream);
  * direction between the halves:
  *   gd_derivatives(mode handle, j0, j1)          grad T, curl u, curl B -> work arrays
  *   (exchange: state and derivatives of its modes -> the shell-slab handles)
- *   gd_*_nonlinear(shell-slab handle)            with gd_set_external_derivatives(1)
+ *   gd_temperature_nonlinear, gd_velocity_nonlinear, gd_magnetic_nonlinear
+ *     (shell-slab handle, in gd_step's order)    with gd_set_external_derivatives(1)
  *   (exchange: nonlinear terms of its shells -> the mode handles)
  *   gd_implicit_modes(mode handle, j0, j1)       temperature Dirichlet rows, CNAB2, history roll
  *
