@@ -300,6 +300,11 @@ def run_ensemble(args, gdb, workloads, torch):
         for i, (c, m) in enumerate(zip(cfgs, ens.members)):
             for k, (a, b) in workloads.seeded_state(c["lmax"], c["lmax"], c["nr"], seed=i).items():
                 m.set_field(k, a, b)
+        tune = None
+        if prec == "mixed":
+            # launch shapes chosen by measurement on a scratch copy (members unchanged)
+            tms, caps = ens.autotune(5)
+            tune = {"ms_per_step": tms, "caps": sorted(set(caps))}
         ens.step(args.warmup)
         ext = torch.cuda.ExternalStream(ens.stream_ptr())
         e0 = torch.cuda.Event(enable_timing=True)
@@ -314,12 +319,15 @@ def run_ensemble(args, gdb, workloads, torch):
         ek = sum(m.energy()[0] for m in ens.members)
         res[prec] = {"instance_steps_per_s": args.steps * len(cfgs) / (ms * 1e-3), "ms_per_step": ms / args.steps,
                      "sum_ekin": ek}
+        if tune is not None:
+            res[prec]["autotune"] = tune
         ens.close()
     line = {"metric": f"ensemble instance-steps/s ({len(cfgs)} uneven shells)", "value": res["mixed"]["instance_steps_per_s"],
             "unit": "instance-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "dtype": "f32/tf32x3 (FP64 solves)", "data": "synthetic (ensemble_draw(seed=3), seeded_state(seed=i))",
             "config": {"workload": "ensemble", "members": len(cfgs), "lmax": sorted({c["lmax"] for c in cfgs}),
-                       "nr": sorted({c["nr"] for c in cfgs}), "dt": 1e-5, "launch": "one CUDA graph per step"},
+                       "nr": sorted({c["nr"] for c in cfgs}), "dt": 1e-5,
+                       "launch": "one CUDA graph per step; mixed: tensor-core grid caps by gd_ensemble_autotune"},
             "fp64": res["fp64"], "mixed": res["mixed"],
             "ratio_vs_fp64_gpu": res["mixed"]["instance_steps_per_s"] / res["fp64"]["instance_steps_per_s"]}
     print(json.dumps(line), flush=True)

@@ -72,6 +72,7 @@ EXPORTS = (
     "gd_create_timestepping_matrices", "gd_destroy_timestepping_matrices", "gd_build_rhs_cnab2",
     "gd_solve_implicit_step", "gd_set_fault_test",
     "gd_derivatives", "gd_implicit_modes", "gd_set_external_derivatives", "gd_copy_block",
+    "gd_set_launch_shape", "gd_get_launch_shape", "gd_ensemble_autotune",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
     "gd_ensemble_step", "gd_ensemble_step_async", "gd_ensemble_failed_member", "gd_ensemble_get_stream",
@@ -172,6 +173,9 @@ def load_library():
         "gd_derivatives": ([P, I, I], I),
         "gd_implicit_modes": ([P, I, I], I),
         "gd_set_external_derivatives": ([P, I], I),
+        "gd_set_launch_shape": ([P, I], I),
+        "gd_get_launch_shape": ([P, ctypes.POINTER(I)], I),
+        "gd_ensemble_autotune": ([P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
         "gd_copy_block": ([P, I, I, I, I, I, I, ctypes.c_void_p, I], I),
         "gd_magnetic_pullback": ([P, I, I, D, D, D, D], I),
         "gd_ensemble_create": ([ctypes.POINTER(GDConfig), I, I, ctypes.POINTER(P)], I),
@@ -321,6 +325,15 @@ class SHTnsKitConfig:
     def implicit_modes(self, j0, j1):
         """Temperature Dirichlet rows, CNAB2 and the history roll for native modes [j0, j1)."""
         self._check(self.lib.gd_implicit_modes(self.h, int(j0), int(j1)))
+
+    def set_launch_shape(self, tc_ctas=0):
+        """Cap of the tensor-core kernels' persistent grid (0: one CTA per SM)."""
+        self._check(self.lib.gd_set_launch_shape(self.h, int(tc_ctas)))
+
+    def launch_shape(self):
+        n = ctypes.c_int()
+        self._check(self.lib.gd_get_launch_shape(self.h, ctypes.byref(n)))
+        return n.value
 
     def set_external_derivatives(self, enable=True):
         self._check(self.lib.gd_set_external_derivatives(self.h, 1 if enable else 0))
@@ -652,6 +665,17 @@ class Ensemble:
             i = self.lib.gd_ensemble_failed_member(self.e)
             msg = self.lib.gd_last_error(self.members[i].h).decode() if i >= 0 else ""
             raise GeoDynamoError(st, f"member {i}: {msg}")
+
+    def autotune(self, nsteps=5):
+        """Chooses the members' tensor-core grid caps by timing candidates on a
+        scratch copy of the ensemble (gd_ensemble_autotune); returns
+        (ms per ensemble step, caps)."""
+        ms = ctypes.c_float()
+        caps = (ctypes.c_int * len(self.members))()
+        st = self.lib.gd_ensemble_autotune(self.e, int(nsteps), ctypes.byref(ms), caps)
+        if st != GD_OK:
+            raise GeoDynamoError(st, "gd_ensemble_autotune failed")
+        return ms.value, list(caps)
 
     def step_async(self, n=1):
         st = self.lib.gd_ensemble_step_async(self.e, int(n))

@@ -588,6 +588,21 @@ int gd_set_external_derivatives(gd_handle* h, int enable) {
   return GD_OK;
 }
 
+int gd_set_launch_shape(gd_handle* h, int tc_ctas) {
+  if (!h || tc_ctas < 0) return h ? fail(h, GD_ERR_ARG, "tc_ctas must be >= 0") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  if (tc_ctas != h->tc_ctas) drop_graphs(h);
+  h->tc_ctas = tc_ctas;
+  return GD_OK;
+}
+
+int gd_get_launch_shape(const gd_handle* h, int* tc_ctas) {
+  if (!h || !tc_ctas) return GD_ERR_ARG;
+  *tc_ctas = h->tc_ctas;
+  return GD_OK;
+}
+
 static bool mode_range_ok(const gd_handle* h, int j0, int j1) { return 0 <= j0 && j0 <= j1 && j1 <= h->d.nlm; }
 
 int gd_derivatives(gd_handle* h, int j0, int j1) {
@@ -1405,6 +1420,76 @@ int gd_ensemble_step_async(gd_ensemble* e, int nsteps) {
       }
     }
   }
+  return GD_OK;
+}
+
+// Launch-shape search for an ensemble: candidate caps of the members'
+// tensor-core grids, each timed over nsteps graph-launched ensemble steps of a
+// scratch ensemble with the same configurations, precisions and schemes (the
+// caller's members are never stepped); the fastest is applied to the members.
+// Candidates: one cap for every member (one CTA per SM, 74, 37, 18, 8, 4), and
+// caps proportional to each member's share of the Legendre work
+// (lmax + 1)^3 nr, scaled by 2, 4, 8 and 16 SMs' worth.
+int gd_ensemble_autotune(gd_ensemble* e, int nsteps, float* best_ms, int* caps_out) {
+  if (!e || nsteps < 1) return GD_ERR_ARG;
+  if (cudaSetDevice(e->device) != cudaSuccess) return GD_ERR_CUDA;
+  const int n = (int)e->members.size();
+  std::vector<gd_config> cfgs(n);
+  for (int i = 0; i < n; ++i) {
+    cfgs[i] = e->members[i]->c;
+    cfgs[i].precision = GD_PREC_FP64;  // set below, with the member's stages
+  }
+  gd_ensemble* t = nullptr;
+  int st = gd_ensemble_create(cfgs.data(), n, e->device, &t);
+  if (st != GD_OK) return st;
+  for (int i = 0; i < n && st == GD_OK; ++i) {
+    gd_handle* src = e->members[i];
+    gd_handle* h = t->members[i];
+    if (src->precision != GD_PREC_FP64) st = gd_set_precision(h, src->precision);
+    if (st == GD_OK) st = gd_set_fp64_stages(h, src->fp64_stages);
+    if (st == GD_OK && src->scheme != h->scheme) st = gd_set_scheme(h, src->scheme);
+  }
+  const int sms = current_sm_count();
+  std::vector<double> w(n);
+  double wsum = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double l1 = e->members[i]->d.L + 1.0;
+    w[i] = l1 * l1 * l1 * e->members[i]->d.nr;
+    wsum += w[i];
+  }
+  std::vector<std::vector<int>> cands;
+  for (int cap : {0, 74, 37, 18, 8, 4}) cands.push_back(std::vector<int>(n, cap < sms ? cap : 0));
+  for (int c : {2, 4, 8, 16}) {
+    std::vector<int> v(n);
+    for (int i = 0; i < n; ++i) v[i] = std::max(1, std::min(sms, (int)std::lround(sms * c * w[i] / wsum)));
+    cands.push_back(v);
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (st == GD_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) st = GD_ERR_CUDA;
+  float best = -1.f;
+  size_t besti = 0;
+  for (size_t c = 0; c < cands.size() && st == GD_OK; ++c) {
+    for (int i = 0; i < n && st == GD_OK; ++i) st = gd_set_launch_shape(t->members[i], cands[c][i]);
+    if (st == GD_OK) st = gd_ensemble_step(t, 2);  // captures the graphs of this shape
+    if (st != GD_OK) break;
+    float ms = 0.f;
+    if (cudaEventRecord(e0, t->master) != cudaSuccess) { st = GD_ERR_CUDA; break; }
+    st = gd_ensemble_step_async(t, nsteps);
+    if (st != GD_OK) break;
+    if (cudaEventRecord(e1, t->master) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { st = GD_ERR_CUDA; break; }
+    st = gd_ensemble_step(t, 0);  // error flags of the timed steps
+    if (st == GD_OK && (best < 0.f || ms < best)) { best = ms; besti = c; }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  gd_ensemble_destroy(t);
+  if (st != GD_OK) return st;
+  for (int i = 0; i < n && st == GD_OK; ++i) st = gd_set_launch_shape(e->members[i], cands[besti][i]);
+  if (st != GD_OK) return st;
+  if (best_ms) *best_ms = best / nsteps;
+  if (caps_out)
+    for (int i = 0; i < n; ++i) caps_out[i] = cands[besti][i];
   return GD_OK;
 }
 

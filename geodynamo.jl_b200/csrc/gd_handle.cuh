@@ -23,6 +23,9 @@ struct gd_handle {
   // work arrays instead of computing them, and leave the temperature
   // Dirichlet rows to the solve side (a shell-slab handle of a distributed step)
   bool ext_derivs = false;
+  // persistent CTAs of the tensor-core Legendre kernels (0: one per SM); an
+  // ensemble caps them so that its members share the SMs
+  int tc_ctas = 0;
   size_t bytes = 0;
   std::vector<void*> allocs;
 

@@ -812,8 +812,11 @@ static void set_attrs() {
   allow_dynamic_smem(k_tc_analysis3<true>, analysis_smem(true));
 }
 
-// One persistent CTA per SM (at most one tile each when there are fewer tiles).
+// One persistent CTA per SM (at most one tile each when there are fewer
+// tiles), or fewer when the caller caps the grid: members of an ensemble then
+// share the SMs instead of each filling them in turn.
 static int sm_count() { return current_sm_count(); }
+static int cta_cap(int max_ctas) { return max_ctas > 0 ? std::min(max_ctas, sm_count()) : sm_count(); }
 
 void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long* cofs, const float* imgP,
                      const float* imgD, const double* sinv, const TcSynthArgs& a, bool vec) {
@@ -824,13 +827,13 @@ void launch_tc_synth(cudaStream_t s, const Dims& d, const int* moff, const long*
     const int ncol = ceil_div(a.nf * d.nr * 2, 2 * TC_N2);
     const int ntiles = (d.M + 1) * ntt * ncol;
     if (a.prep_mask) k_synth_coef_image<false><<<dim3(kcmax, d.M + 1, ncol), 256, 0, s>>>(d, moff, cofs, ntt, a);
-    k_tc_synth4<false><<<std::min(ntiles, sm_count()), SY_THREADS, synth_smem(false), s>>>(d, moff, cofs, imgP,
+    k_tc_synth4<false><<<std::min(ntiles, cta_cap(a.max_ctas)), SY_THREADS, synth_smem(false), s>>>(d, moff, cofs, imgP,
                                                                                           imgD, sinv, a, ntt, ncol);
   } else {
     const int ncol = ceil_div(d.nr, 32);
     const int ntiles = (d.M + 1) * ntt * ncol;
     if (a.prep_mask) k_synth_coef_image<true><<<dim3(kcmax, d.M + 1, ncol), 256, 0, s>>>(d, moff, cofs, ntt, a);
-    k_tc_synth4<true><<<std::min(ntiles, sm_count()), SY_THREADS, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD,
+    k_tc_synth4<true><<<std::min(ntiles, cta_cap(a.max_ctas)), SY_THREADS, synth_smem(true), s>>>(d, moff, cofs, imgP, imgD,
                                                                                         sinv, a, ntt, ncol);
   }
 }
@@ -847,12 +850,12 @@ void launch_tc_analysis(cudaStream_t s, const Dims& d, const int* moff, const fl
   if (a.epi == EPI_SCALAR) {
     const int npair = a.nf * d.nr, ncol = ceil_div(2 * npair, TC_N2), csz = ceil_div(npair, ncol);
     const int ntiles = (d.M + 1) * nlt_of(d.L) * ncol;
-    k_tc_analysis3<false><<<std::min(ntiles, sm_count()), WS_THREADS, analysis_smem(false), s>>>(d, moff, img0,
+    k_tc_analysis3<false><<<std::min(ntiles, cta_cap(a.max_ctas)), WS_THREADS, analysis_smem(false), s>>>(d, moff, img0,
                                                                                                 img1, a, ncol, csz);
   } else {
     const int ncol = ceil_div(d.nr, 32), csz = ceil_div(d.nr, ncol);
     const int ntiles = (d.M + 1) * nlt_of(d.L) * ncol;
-    k_tc_analysis3<true><<<std::min(ntiles, sm_count()), WS_THREADS, analysis_smem(true), s>>>(d, moff, img0, img1,
+    k_tc_analysis3<true><<<std::min(ntiles, cta_cap(a.max_ctas)), WS_THREADS, analysis_smem(true), s>>>(d, moff, img0, img1,
                                                                                               a, ncol, csz);
   }
 }

@@ -102,6 +102,7 @@ int tc_synth_scalar(gd_handle* h, const double* const* coef, int nf, float4* out
   a.prep_mask = prep_mask;
   a.wait_limit = x->wait_limit;
   a.omit_plus1 = x->omit_plus1;
+  a.max_ctas = h->tc_ctas;
   x->omit_plus1 = 0;  // one-shot
   { ProfScope p(h, "legendre_synth_scalar_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], nullptr, x->sinv, a, false); }
   return launched(h, "mixed scalar synthesis");
@@ -124,6 +125,7 @@ int tc_synth_vector(gd_handle* h, const double* tor, const double* pol, float4* 
   a.prep_mask = pre ? 3 : 0;
   a.wait_limit = x->wait_limit;
   a.omit_plus1 = x->omit_plus1;
+  a.max_ctas = h->tc_ctas;
   x->omit_plus1 = 0;
   { ProfScope p(h, "legendre_synth_vector_tc"); launch_tc_synth(h->stream, h->d, h->d_moff, x->d_cofs, x->img_synth[0], x->img_synth[1], x->sinv, a, true); }
   return launched(h, "mixed vector synthesis");
@@ -150,6 +152,7 @@ int tc_analysis_scalar_G(gd_handle* h, int nf, double* const* out) {
   a.epi = EPI_SCALAR;
   a.err = x->d_err;
   a.wait_limit = x->wait_limit;
+  a.max_ctas = h->tc_ctas;
   { ProfScope p(h, "legendre_analysis_scalar_tc"); launch_tc_analysis(h->stream, h->d, h->d_moff, x->img_anal[0], nullptr, a); }
   return launched(h, "mixed scalar analysis");
 }
@@ -164,6 +167,7 @@ int tc_analysis_vector_G(gd_handle* h, double* out_tor, double* out_pol, int epi
   a.epi = epi;
   a.err = x->d_err;
   a.wait_limit = x->wait_limit;
+  a.max_ctas = h->tc_ctas;
   { ProfScope p(h, "legendre_analysis_vector_tc"); launch_tc_analysis(h->stream, h->d, h->d_moff, x->img_anal[1], x->img_anal[2], a); }
   return launched(h, "mixed vector analysis");
 }

@@ -63,6 +63,7 @@ struct TcSynthArgs {
   float* bimg;            // split coefficient images (tc_synth_bimage_floats floats)
   long ttot;              // pipeline steps summed over m (one column tile)
   int prep_mask;          // fields the pre-pass writes into bimg (the others are written by their producer)
+  int max_ctas;           // persistent CTAs of the launch (0: one per SM)
 };
 
 // Floats of coefficient-image scratch the synthesis needs (the scalar case, 4 fields, bounds both).
@@ -83,6 +84,7 @@ struct TcAnalysisArgs {
   int epi;
   int* err;
   long long wait_limit;   // clock cycles of each bounded wait (0: the default)
+  int max_ctas;           // persistent CTAs of the launch (0: one per SM)
 };
 
 long tc_synth_chunks(const Dims& d, std::vector<long>& cofs);

@@ -319,6 +319,15 @@ int gd_ensemble_failed_member(const gd_ensemble* e);
 /* The ensemble's own stream (cudaStream_t as void*): every graph-launched step is
  * joined to it, so events recorded on it bracket whole ensemble steps. */
 int gd_ensemble_get_stream(gd_ensemble* e, void** stream);
+/* Chooses the members' launch shapes (gd_set_launch_shape) by measurement:
+ * candidate caps of the tensor-core grids -- one cap for every member, or caps
+ * proportional to each member's share of the Legendre work -- each timed over
+ * nsteps steps of a scratch ensemble built from the members' configurations,
+ * precisions and schemes (the members themselves are not stepped, and the
+ * scratch ensemble needs as much device memory again while it exists).  The
+ * fastest is applied; *best_ms = its time per ensemble step, caps_out[i] =
+ * member i's cap (either pointer may be null). */
+int gd_ensemble_autotune(gd_ensemble* e, int nsteps, float* best_ms, int* caps_out);
 
 /* ---- the step decomposed across ranks ---------------------------------------------
  * The reference distributes its step over MPI pencils (src/pencil_decomps.jl:
@@ -355,6 +364,17 @@ int gd_set_external_derivatives(gd_handle* h, int enable);
  * GD_TEMP); 1: work array 0-7; 2: nonlinear term of the current bank.
  * to_buf != 0 copies from the handle into buf.  Synchronises the stream. */
 int gd_copy_block(gd_handle* h, int array, int field, int r0, int r1, int j0, int j1, void* buf, int to_buf);
+
+/* ---- launch shape -------------------------------------------------------------------
+ * No counterpart in the reference.  tc_ctas caps the persistent grid of the
+ * tensor-core Legendre kernels (0, the default: one CTA per SM).  Each of those
+ * CTAs holds about 192 KB of shared memory, so an uncapped launch occupies
+ * every SM; members of an ensemble run side by side only when their grids are
+ * capped.  The arithmetic of every tile is the same whatever CTA runs it: the
+ * results do not depend on the cap.  gd_ensemble_autotune chooses the caps of
+ * an ensemble's members by measurement. */
+int gd_set_launch_shape(gd_handle* h, int tc_ctas);
+int gd_get_launch_shape(const gd_handle* h, int* tc_ctas);
 
 /* ---- error-path testing ----------------------------------------------------------
  * No counterpart in the reference.  Every wait of the tensor-core pipelines is

@@ -121,3 +121,30 @@ def test_ensemble_rejects_bad_member(gdb):
     good = one_per_lmax()[0][1]
     with pytest.raises(gdb.GeoDynamoError):
         gdb.Ensemble([good, dict(good, nr=2)])
+
+
+def test_autotune_chooses_caps_without_changing_results(gdb):
+    # the launch-shape search steps a scratch ensemble only; the tuned members
+    # give the same bits as untuned ones (a tile's arithmetic does not depend on
+    # which persistent CTA runs it)
+    cfgs = [dict(lmax=l, nlat=3 * (l + 1) // 2, nlon=3 * (l + 1), nr=nr, dt=1e-5)
+            for l, nr in ((15, 9), (23, 13), (31, 17), (31, 9))]
+    a = gdb.Ensemble(cfgs, precision="mixed")
+    b = gdb.Ensemble(cfgs, precision="mixed")
+    for i, c in enumerate(cfgs):
+        load(a.members[i], c["lmax"], c["nr"], seed=i)
+        load(b.members[i], c["lmax"], c["nr"], seed=i)
+    ms, caps = a.autotune(3)
+    print(f"autotune: {ms:.3f} ms per ensemble step, caps {caps}")
+    assert ms > 0 and len(caps) == len(cfgs)
+    assert all(0 <= c <= 1024 for c in caps)
+    assert [m.launch_shape() for m in a.members] == caps
+    assert all(m.step_count() == 0 for m in a.members)
+    a.step(3)
+    b.step(3)
+    for ma, mb in zip(a.members, b.members):
+        for k in workloads.FIELD_ORDER:
+            for x, y in zip(ma.get_field(k), mb.get_field(k)):
+                assert np.array_equal(x, y), k
+    a.close()
+    b.close()
