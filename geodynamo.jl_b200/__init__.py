@@ -41,11 +41,13 @@ _CSRC = os.path.join(_HERE, "csrc")
 GD_OK = 0
 STATUS_NAMES = {0: "GD_OK", 1: "GD_ERR_ARG", 2: "GD_ERR_CONFIG", 3: "GD_ERR_CUDA", 4: "GD_ERR_NONFINITE",
                 5: "GD_ERR_SINGULAR", 6: "GD_ERR_UNSUPPORTED", 7: "GD_ERR_STATE"}
-FIELDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4}
+FIELDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4, "comp": 5}
+BC_VALUE, BC_FLUX = 1, 2  # GD_BC_VALUE / GD_BC_FLUX (bc_type_inner / bc_type_outer)
 GRIDS = {
     "u_th": 0, "u_ph": 1, "w_th": 2, "w_ph": 3, "b_th": 4, "b_ph": 5, "j_th": 6, "j_ph": 7,
     "t": 8, "gth": 9, "gph": 10, "gr": 11, "tadv": 12, "vadv_th": 13, "vadv_ph": 14,
     "ind_th": 15, "ind_ph": 16,
+    "c": 17, "cgth": 18, "cgph": 19, "cgr": 20, "cadv": 21,
 }
 PRECISIONS = {"fp64": 0, "mixed": 1}
 # Stages of the mixed-precision step that can run in FP64 (GD_STAGE_*): the
@@ -73,6 +75,7 @@ EXPORTS = (
     "gd_solve_implicit_step", "gd_set_fault_test",
     "gd_derivatives", "gd_implicit_modes", "gd_set_external_derivatives", "gd_copy_block",
     "gd_set_launch_shape", "gd_get_launch_shape", "gd_ensemble_autotune",
+    "gd_set_composition_bc", "gd_set_scalar_bc_types", "gd_composition_nonlinear",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
     "gd_ensemble_step", "gd_ensemble_step_async", "gd_ensemble_failed_member", "gd_ensemble_get_stream",
@@ -95,6 +98,7 @@ class GDConfig(ctypes.Structure):
         ("dt", ctypes.c_double), ("implicit_theta", ctypes.c_double),
         ("ab_mode", ctypes.c_int), ("bc_mode", ctypes.c_int), ("fd_mode", ctypes.c_int),
         ("precision", ctypes.c_int), ("magnetic", ctypes.c_int),
+        ("composition", ctypes.c_int), ("schmidt", ctypes.c_double),
     ]
 
 
@@ -174,6 +178,9 @@ def load_library():
         "gd_implicit_modes": ([P, I, I], I),
         "gd_set_external_derivatives": ([P, I], I),
         "gd_set_launch_shape": ([P, I], I),
+        "gd_set_composition_bc": ([P, D, D], I),
+        "gd_set_scalar_bc_types": ([P, I, ctypes.POINTER(I), ctypes.POINTER(I)], I),
+        "gd_composition_nonlinear": ([P], I),
         "gd_get_launch_shape": ([P, ctypes.POINTER(I)], I),
         "gd_ensemble_autotune": ([P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
         "gd_copy_block": ([P, I, I, I, I, I, I, ctypes.c_void_p, I], I),
@@ -240,12 +247,13 @@ class SHTnsKitConfig:
 
     def __init__(self, lmax, nlat, nlon, nr, mmax=None, kl=4, rratio=0.35, ekman=3e-4, rayleigh=80.0,
                  prandtl=1.0, magnetic_prandtl=4.0, dt=1e-5, implicit_theta=0.5, ab_mode=0, bc_mode=0,
-                 fd_mode=0, precision="fp64", magnetic=1, device=0):
+                 fd_mode=0, precision="fp64", magnetic=1, device=0, composition=0, schmidt=1.0):
         self.lib = load_library()
         mmax = lmax if mmax is None else mmax
         base, stages = PRECISION_PRESETS.get(precision, (precision, ()))
         self.cfg = GDConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl, magnetic_prandtl,
-                            dt, implicit_theta, ab_mode, bc_mode, fd_mode, PRECISIONS[base], magnetic)
+                            dt, implicit_theta, ab_mode, bc_mode, fd_mode, PRECISIONS[base], magnetic,
+                            int(composition), float(schmidt))
         h = ctypes.c_void_p()
         st = self.lib.gd_create(ctypes.byref(self.cfg), int(device), ctypes.byref(h))
         if st != GD_OK:
@@ -442,6 +450,10 @@ class SHTnsKitConfig:
     def set_field(self, name, re, im):
         self._check(self.lib.gd_upload_spectral(self.h, FIELDS[name], _dptr(_f64(re)), _dptr(_f64(im))))
 
+    def field_names(self):
+        """The state fields of this configuration (composition only when configured)."""
+        return [k for k in FIELDS if k != "comp" or self.cfg.composition]
+
     def get_field(self, name):
         re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
         self._check(self.lib.gd_download_spectral(self.h, FIELDS[name], _dptr(re), _dptr(im)))
@@ -461,6 +473,24 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_set_temperature_bc(
             self.h, _dptr(_f64(bvals)) if bvals is not None else None,
             _dptr(_f64(sources)) if sources is not None else None))
+
+    def set_composition_bc(self, bvals=None, sources=None):
+        """Composition boundary values or fluxes [2][nlm] and sources [nr]."""
+        self._check(self.lib.gd_set_composition_bc(
+            self.h, _dptr(_f64(bvals)) if bvals is not None else None,
+            _dptr(_f64(sources)) if sources is not None else None))
+
+    def set_bc_types(self, name, inner, outer):
+        """bc_type_inner / bc_type_outer of "temp" or "comp": BC_VALUE or BC_FLUX per mode (l-major)."""
+        a = np.ascontiguousarray(inner, dtype=np.int32)
+        b = np.ascontiguousarray(outer, dtype=np.int32)
+        if a.size != self.nlm or b.size != self.nlm:
+            raise ValueError("one boundary type per mode")
+        IP = ctypes.POINTER(ctypes.c_int)
+        self._check(self.lib.gd_set_scalar_bc_types(self.h, FIELDS[name], a.ctypes.data_as(IP), b.ctypes.data_as(IP)))
+
+    def composition_nl(self):
+        self._check(self.lib.gd_composition_nonlinear(self.h))
 
     def temperature_nl(self):
         self._check(self.lib.gd_temperature_nonlinear(self.h))
@@ -609,7 +639,7 @@ def magnetic_misfit(model, target, nsteps, checkpoint_every=20):
     done = 0
     while done < nsteps:
         if checkpoint_every and done % checkpoint_every == 0:
-            checkpoints.append((done, {k: model.get_field(k) for k in FIELDS}))
+            checkpoints.append((done, {k: model.get_field(k) for k in model.field_names()}))
         k = min(checkpoint_every or nsteps, nsteps - done)
         model.step(k)
         done += k
@@ -647,7 +677,7 @@ class Ensemble:
                               c.pop("prandtl", 1.0), c.pop("magnetic_prandtl", 4.0), c.pop("dt", 1e-5),
                               c.pop("implicit_theta", 0.5), c.pop("ab_mode", 0), c.pop("bc_mode", 0),
                               c.pop("fd_mode", 0), PRECISIONS[c.pop("precision", precision)],
-                              c.pop("magnetic", 1))
+                              c.pop("magnetic", 1), c.pop("composition", 0), c.pop("schmidt", 1.0))
         e = ctypes.c_void_p()
         st = self.lib.gd_ensemble_create(arr, n, int(device), ctypes.byref(e))
         if st != GD_OK:

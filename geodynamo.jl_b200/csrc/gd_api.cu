@@ -16,6 +16,10 @@ using namespace gd;
 
 namespace {
 
+// State fields of the configuration: the five of the reference's step, and
+// composition when configured.
+int nfields(const gd_handle* h) { return h->c.composition ? NFIELD : NFIELD - 1; }
+
 int fail(gd_handle* h, int code, const std::string& msg) {
   if (h) h->err = msg;
   return code;
@@ -55,7 +59,7 @@ int build_implicit(gd_handle* h) {
   const Dims& d = h->d;
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
   launch_build_lu(h->stream, d.nr, d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->c.dt,
-                  h->c.implicit_theta, h->c.bc_mode == 2, h->d_lin, h->d_lu, h->d_flag);
+                  h->c.implicit_theta, h->c.bc_mode == 2, h->d_lin, h->d_lu, h->d_flag, h->c.composition ? 4 : 3);
   int s = check_launch(h, "build_lu");
   if (s) return s;
   int flag = 0;
@@ -64,6 +68,77 @@ int build_implicit(gd_handle* h) {
   if (flag) return fail(h, GD_ERR_SINGULAR, "zero pivot in a banded LU factorisation");
   return GD_OK;
 }
+
+// Tau functions of the flux boundary conditions on the radial nodes
+// (_get_tau_cache, compute_inner_tau_function, compute_outer_tau_function,
+// evaluate_tau_derivative_*, src/scalar_field_common.jl:590-790): Chebyshev
+// T_{N-1} and T_N of x = 2 (r - ri) / (ro - ri) - 1, their analytic radial
+// derivatives at the boundaries (n^2 sign(x)^(n+1) dx/dr where |x| = 1), the
+// single-boundary combinations and their D1 derivatives at the boundary they
+// serve.  Needs the radial nodes and D1 on the device.
+int build_tau(gd_handle* h) {
+  const int N = h->d.nr, KL = h->d.kl, NB = 2 * GD_MAX_KL + 1;
+  std::vector<double> r(N), d1((size_t)NB * N);
+  CK(cudaMemcpyAsync(r.data(), h->d_r, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(d1.data(), h->d_d1, sizeof(double) * NB * N, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const double ri = r[0], ro = r[N - 1];
+  auto cheb = [&](int n, double rr) {
+    double x = 2.0 * (rr - ri) / (ro - ri) - 1.0;
+    x = x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x);
+    return std::cos(n * std::acos(x));
+  };
+  auto dcheb = [&](int n, double rr) {
+    const double x = 2.0 * (rr - ri) / (ro - ri) - 1.0;
+    double dx;
+    if (std::fabs(std::fabs(x) - 1.0) < 1e-12) {
+      dx = (double)n * n * std::pow(x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0), n + 1);
+    } else {
+      const double th = std::acos(x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x));
+      dx = n * std::sin(n * th) / std::sin(th);
+    }
+    return dx * (2.0 / (ro - ri));
+  };
+  std::vector<double> t(4 * (size_t)N);
+  double* t1 = t.data();
+  double* t2 = t1 + N;
+  double* tin = t2 + N;
+  double* tout = tin + N;
+  for (int i = 0; i < N; ++i) { t1[i] = cheb(N - 1, r[i]); t2[i] = cheb(N, r[i]); }
+  TauConsts& tc = h->tau;
+  tc.dt1i = dcheb(N - 1, ri); tc.dt1o = dcheb(N - 1, ro);
+  tc.dt2i = dcheb(N, ri); tc.dt2o = dcheb(N, ro);
+  const double alpha = std::fabs(tc.dt2o) > 1e-12 ? tc.dt1o / tc.dt2o : 0.0;
+  const double beta = std::fabs(tc.dt2i) > 1e-12 ? tc.dt1i / tc.dt2i : 0.0;
+  for (int i = 0; i < N; ++i) { tin[i] = t1[i] - alpha * t2[i]; tout[i] = t1[i] - beta * t2[i]; }
+  // rows 0 and N - 1 of D1 (entry (i, col) at d1[(i - col + KL) + NB col])
+  tc.din = 0.0;
+  tc.dout = 0.0;
+  for (int col = 0; col <= KL && col < N; ++col) tc.din += d1[(size_t)(0 - col + KL) + (size_t)NB * col] * tin[col];
+  for (int col = std::max(0, N - 1 - KL); col < N; ++col)
+    tc.dout += d1[(size_t)(N - 1 - col + KL) + (size_t)NB * col] * tout[col];
+  CK(cudaMemcpyAsync(h->d_tau, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  tc.tau1 = h->d_tau;
+  tc.tau2 = h->d_tau + N;
+  tc.tau_in = h->d_tau + 2 * N;
+  tc.tau_out = h->d_tau + 3 * N;
+  return GD_OK;
+}
+
+}  // namespace
+
+// Boundary conditions of temperature (F_TEMP) or composition (F_COMP) for the
+// handle's mode range.
+void gd::scalar_bc(gd_handle* h, int field) {
+  const bool comp = field == F_COMP;
+  const size_t NL = h->d.nlm;
+  ProfScope p(h, comp ? "composition_bc" : "temperature_bc");
+  launch_scalar_bc(h->stream, h->d, comp ? h->d_cbvals : h->d_bvals, h->d_bctype + (comp ? 2 * NL : 0), h->d_d1, h->tau,
+                   h->field(field));
+}
+
+namespace {
 
 int setup(gd_handle* h) {
   const gd_config& c = h->c;
@@ -95,14 +170,16 @@ int setup(gd_handle* h) {
   AL(h->d_moff, d.M + 2); AL(h->d_lof, NL); AL(h->d_mof, NL); AL(h->d_perm, NL); AL(h->d_flag, 4);
   AL(h->d_x, d.nlat); AL(h->d_w, d.nlat); AL(h->d_th, d.nlat); AL(h->d_sth, d.nlat);
   AL(h->d_cth, d.nlat); AL(h->d_sthc, d.nlat);
-  AL(h->d_r, NR); AL(h->d_rinv, NR); AL(h->d_rinv2, NR); AL(h->d_nu, 3);
+  AL(h->d_r, NR); AL(h->d_rinv, NR); AL(h->d_rinv2, NR); AL(h->d_nu, 4);
   AL(h->d_P, NL * NT); AL(h->d_dP, NL * NT); AL(h->d_Q, NL * NT);
   AL(h->d_d1, nbw * NR); AL(h->d_d2, nbw * NR);
-  AL(h->d_lin, 3 * NR * nbw * (d.L + 1)); AL(h->d_lu, 3 * NR * nbw * (d.L + 1));
+  AL(h->d_lin, 4 * NR * nbw * (d.L + 1)); AL(h->d_lu, 4 * NR * nbw * (d.L + 1));
   AL(h->d_tw, 2 * (size_t)d.nlon); AL(h->d_twf, 2 * (size_t)d.nlon);
-  AL(h->d_state, 5 * h->spec_elems()); AL(h->d_nl, 5 * h->spec_elems()); AL(h->d_prev, 5 * h->spec_elems());
-  AL(h->d_work, 8 * h->spec_elems());
+  AL(h->d_state, NFIELD * h->spec_elems()); AL(h->d_nl, NFIELD * h->spec_elems());
+  AL(h->d_prev, NFIELD * h->spec_elems());
+  AL(h->d_work, NWORK * h->spec_elems());
   AL(h->d_bvals, 2 * NL); AL(h->d_sources, NR);
+  AL(h->d_cbvals, 2 * NL); AL(h->d_csources, NR); AL(h->d_bctype, 4 * NL); AL(h->d_tau, 4 * NR);
   AL(h->d_grid, NGRID * h->grid_elems());
   AL(h->d_F, (size_t)4 * NR * (d.M + 1) * d.nlat);
   AL(h->d_epart, 2 * 296); AL(h->d_eout, 2);
@@ -122,8 +199,10 @@ int setup(gd_handle* h) {
   CK(cudaMemcpyAsync(h->d_r, r.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(h->d_rinv, ri.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(h->d_rinv2, ri2.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
-  // Diffusivities: velocity Pm, magnetic 1, temperature Pm/Pr (src/simulation.jl:228-231).
-  const double nu[3] = {c.magnetic_prandtl, 1.0, c.magnetic_prandtl / c.prandtl};
+  // Diffusivities: velocity Pm, magnetic 1, temperature Pm/Pr, composition
+  // Pm/Sc (src/simulation.jl:228-235).
+  const double nu[4] = {c.magnetic_prandtl, 1.0, c.magnetic_prandtl / c.prandtl,
+                        c.composition ? c.magnetic_prandtl / c.schmidt : 0.0};
   CK(cudaMemcpyAsync(h->d_nu, nu, sizeof(nu), cudaMemcpyHostToDevice, s));
   std::vector<double> tw;
   make_twiddles(d.nlon, tw);
@@ -148,12 +227,27 @@ int setup(gd_handle* h) {
     CK(cudaMemcpyAsync(h->d_cth, cth.data(), sizeof(double) * d.nlat, cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
   }
-  CK(cudaMemsetAsync(h->d_state, 0, sizeof(double) * 5 * h->spec_elems(), s));
-  CK(cudaMemsetAsync(h->d_nl, 0, sizeof(double) * 5 * h->spec_elems(), s));
-  CK(cudaMemsetAsync(h->d_prev, 0, sizeof(double) * 5 * h->spec_elems(), s));
-  CK(cudaMemsetAsync(h->d_work, 0, sizeof(double) * 8 * h->spec_elems(), s));
+  CK(cudaMemsetAsync(h->d_state, 0, sizeof(double) * NFIELD * h->spec_elems(), s));
+  CK(cudaMemsetAsync(h->d_nl, 0, sizeof(double) * NFIELD * h->spec_elems(), s));
+  CK(cudaMemsetAsync(h->d_prev, 0, sizeof(double) * NFIELD * h->spec_elems(), s));
+  CK(cudaMemsetAsync(h->d_work, 0, sizeof(double) * NWORK * h->spec_elems(), s));
   CK(cudaMemsetAsync(h->d_bvals, 0, sizeof(double) * 2 * NL, s));
   CK(cudaMemsetAsync(h->d_sources, 0, sizeof(double) * NR, s));
+  CK(cudaMemsetAsync(h->d_cbvals, 0, sizeof(double) * 2 * NL, s));
+  CK(cudaMemsetAsync(h->d_csources, 0, sizeof(double) * NR, s));
+  {
+    // boundary types: temperature fixed values, composition no-flux
+    // (create_shtns_temperature_field / create_shtns_composition_field defaults)
+    std::vector<int> bt(4 * NL);
+    for (size_t q = 0; q < 2 * NL; ++q) bt[q] = GD_BC_VALUE;
+    for (size_t q = 2 * NL; q < 4 * NL; ++q) bt[q] = GD_BC_FLUX;
+    CK(cudaMemcpyAsync(h->d_bctype, bt.data(), sizeof(int) * bt.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  {
+    int st = build_tau(h);
+    if (st) return st;
+  }
   CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * NGRID * h->grid_elems(), s));
   return build_implicit(h);
 }
@@ -227,11 +321,36 @@ int temperature_nl_fp64(gd_handle* h) {
   double* out[1] = {h->nlf(F_TEMP)};
   s = analysis_scalar(h, h->grid(GD_GRID_TADV), 1, out);
   if (s) return s;
-  if (!h->ext_derivs) {
-    ProfScope p(h, "temperature_bc");
-    launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP));
-  }
+  if (!h->ext_derivs) scalar_bc(h, F_TEMP);
   return check_launch(h, "temperature nonlinear");
+}
+
+// compute_composition_nonlinear! (src/compositional.jl:219-259): gradient of C
+// (compute_all_gradients_spectral!, into work 8-10 unless received), batched
+// synthesis of C and its gradient, -u.grad C + S_C(r) with this step's velocity
+// grids (step_once! runs it after the velocity phase), analysis, then the
+// boundary conditions (apply_composition_boundary_conditions_spectral!: fixed
+// values and the tau flux correction).  The extra synthesis of C at :229 only
+// rewrites the grid the batched one writes again.
+int composition_nl_fp64(gd_handle* h) {
+  const Dims& d = h->d;
+  if (!h->ext_derivs) {
+    ProfScope p(h, "spectral_gradients");
+    launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_COMP), h->work(8), h->work(9),
+                     h->work(10));
+  }
+  const double* coef[4] = {h->field(F_COMP), h->work(8), h->work(9), h->work(10)};
+  int s = synth_scalar(h, coef, 4, h->grid(GD_GRID_C));
+  if (s) return s;
+  { ProfScope pa(h, "nl_composition_fp64");
+    launch_temperature_advection<double>(h->stream, d, h->grid(GD_GRID_U_TH), h->grid(GD_GRID_U_PH),
+                                         h->grid(GD_GRID_CGTH), h->grid(GD_GRID_CGPH), h->grid(GD_GRID_CGR),
+                                         h->d_csources, h->grid(GD_GRID_CADV)); }
+  double* out[1] = {h->nlf(F_COMP)};
+  s = analysis_scalar(h, h->grid(GD_GRID_CADV), 1, out);
+  if (s) return s;
+  if (!h->ext_derivs) scalar_bc(h, F_COMP);
+  return check_launch(h, "composition nonlinear");
 }
 
 int velocity_nl_fp64(gd_handle* h) {
@@ -284,6 +403,7 @@ ExpApply exp_apply_args(gd_handle* h, const Cnab2Args& a) {
 int temperature_nl(gd_handle* h);
 int velocity_nl(gd_handle* h);
 int magnetic_nl(gd_handle* h);
+int composition_nl(gd_handle* h);
 
 // compute_all_nonlinear_terms! (src/simulation.jl:800-813): velocity, magnetic,
 // temperature, in that order (the carried grids make the order matter).
@@ -360,9 +480,16 @@ int erk2_launch(gd_handle* h, const Cnab2Args& a) {
 
 int implicit_launch(gd_handle* h, int boot) {
   Cnab2Args a{};
-  const int order[5] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL};
-  const int kinds[5] = {2, 0, 0, 1, 1};
+  // temperature, velocity, magnetic field, composition (the exponential
+  // schemes are refused with composition: it is a CNAB2 slot only)
+  int order[6] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL, F_COMP};
+  int kinds[6] = {2, 0, 0, 1, 1, 3};
   a.nfield = h->c.magnetic ? 5 : 3;
+  if (h->c.composition && h->scheme == GD_SCHEME_CNAB2) {
+    order[a.nfield] = F_COMP;
+    kinds[a.nfield] = 3;
+    ++a.nfield;
+  }
   for (int i = 0; i < a.nfield; ++i) {
     a.u[i] = h->field(order[i]);
     a.nl[i] = h->nlf(order[i]);
@@ -430,7 +557,12 @@ int velocity_nl(gd_handle* h) {
 int magnetic_nl(gd_handle* h) {
   return h->precision == GD_PREC_MIXED ? mixed_magnetic_nl(h) : magnetic_nl_fp64(h);
 }
+int composition_nl(gd_handle* h) {
+  return h->precision == GD_PREC_MIXED ? mixed_composition_nl(h) : composition_nl_fp64(h);
+}
 
+// step_once! (scripts/bench_timestepping.jl:6-18): temperature, velocity,
+// magnetic field, composition, then the implicit step.
 int step_sequence(gd_handle* h, int boot) {
   int s = temperature_nl(h);
   if (s) return s;
@@ -438,6 +570,10 @@ int step_sequence(gd_handle* h, int boot) {
   if (s) return s;
   if (h->c.magnetic) {
     s = magnetic_nl(h);
+    if (s) return s;
+  }
+  if (h->c.composition) {
+    s = composition_nl(h);
     if (s) return s;
   }
   return implicit_launch(h, boot);
@@ -497,6 +633,9 @@ bool valid_config(const gd_config* c, std::string& why) {
   if (c->ab_mode < 0 || c->ab_mode > 1) { why = "ab_mode must be 0 or 1"; return false; }
   if (c->fd_mode < 0 || c->fd_mode > 1) { why = "fd_mode must be 0 or 1"; return false; }
   if (c->precision != GD_PREC_FP64 && c->precision != GD_PREC_MIXED) { why = "unknown precision"; return false; }
+  if (c->composition != 0 && c->composition != 1) { why = "composition must be 0 or 1"; return false; }
+  if (c->composition && !(c->schmidt > 0.0)) { why = "composition needs a positive Schmidt number"; return false; }
+  if (c->composition && c->bc_mode == 2) { why = "composition supports bc_mode 0 and 1"; return false; }
   return true;
 }
 
@@ -605,6 +744,48 @@ int gd_get_launch_shape(const gd_handle* h, int* tc_ctas) {
 
 static bool mode_range_ok(const gd_handle* h, int j0, int j1) { return 0 <= j0 && j0 <= j1 && j1 <= h->d.nlm; }
 
+int gd_set_composition_bc(gd_handle* h, const double* bvals, const double* sources) {
+  if (!h) return GD_ERR_ARG;
+  if (!h->c.composition) return fail(h, GD_ERR_STATE, "the configuration has no composition");
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  if (bvals) {
+    CK(cudaMemcpyAsync(h->d_stage_spec, bvals, 2 * (size_t)h->d.nlm * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    Dims d1 = h->d;
+    d1.nr = 1;
+    launch_lmajor_to_native(h->stream, d1, h->d_perm, h->d_stage_spec, h->d_cbvals, 2);
+  }
+  if (sources) CK(cudaMemcpyAsync(h->d_csources, sources, h->d.nr * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "set composition bc");
+}
+
+int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int* outer) {
+  if (!h || !inner || !outer) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (field != GD_TEMP && field != GD_COMP) return fail(h, GD_ERR_ARG, "boundary types are for GD_TEMP or GD_COMP");
+  if (field == GD_COMP && !h->c.composition) return fail(h, GD_ERR_STATE, "the configuration has no composition");
+  const size_t NL = h->d.nlm;
+  std::vector<int> t(2 * NL);
+  bool flux = false;
+  for (size_t q = 0; q < NL; ++q) {
+    const int a = inner[q], b = outer[q];
+    if ((a != GD_BC_VALUE && a != GD_BC_FLUX) || (b != GD_BC_VALUE && b != GD_BC_FLUX))
+      return fail(h, GD_ERR_ARG, "boundary types must be GD_BC_VALUE or GD_BC_FLUX");
+    flux |= a == GD_BC_FLUX || b == GD_BC_FLUX;
+    t[h->perm[q]] = a;  // l-major q -> native
+    t[NL + h->perm[q]] = b;
+  }
+  if (flux && h->c.bc_mode == 2)
+    return fail(h, GD_ERR_UNSUPPORTED, "flux boundaries act on the state (bc_mode 0 or 1), not inside the operator");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpyAsync(h->d_bctype + (field == GD_COMP ? 2 * NL : 0), t.data(), sizeof(int) * 2 * NL,
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+
 int gd_derivatives(gd_handle* h, int j0, int j1) {
   if (!h) return GD_ERR_ARG;
   if (!mode_range_ok(h, j0, j1)) return fail(h, GD_ERR_ARG, "mode range outside [0, nlm]");
@@ -622,6 +803,11 @@ int gd_derivatives(gd_handle* h, int j0, int j1) {
     if (h->c.magnetic)
       launch_curl(h->stream, d, h->d_lof, h->d_rinv, h->d_rinv2, h->d_d1, h->d_d2, h->field(F_BTOR),
                   h->field(F_BPOL), h->work(5), h->work(6)); }
+  if (h->c.composition) {
+    ProfScope p(h, "spectral_gradients");
+    launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_COMP), h->work(8), h->work(9),
+                     h->work(10));
+  }
   int s = check_launch(h, "derivatives");
   if (s) return s;
   CK(cudaStreamSynchronize(h->stream));
@@ -639,7 +825,8 @@ int gd_implicit_modes(gd_handle* h, int j0, int j1) {
     const Dims full = h->d;
     h->d.jlo = j0;
     h->d.jhi = j1;
-    { ProfScope p(h, "temperature_bc"); launch_temperature_bc(h->stream, h->d, h->d_bvals, h->field(F_TEMP)); }
+    scalar_bc(h, F_TEMP);
+    if (h->c.composition) scalar_bc(h, F_COMP);
     s = implicit_launch(h, boot);
     h->d = full;
   }
@@ -653,7 +840,7 @@ int gd_implicit_modes(gd_handle* h, int j0, int j1) {
 
 int gd_copy_block(gd_handle* h, int array, int field, int r0, int r1, int j0, int j1, void* buf, int to_buf) {
   if (!h || !buf) return h ? fail(h, GD_ERR_ARG, "null buffer") : GD_ERR_ARG;
-  const int nf = array == 1 ? 8 : 5;
+  const int nf = array == 1 ? NWORK : nfields(h);
   if (array < 0 || array > 2 || field < 0 || field >= nf) return fail(h, GD_ERR_ARG, "bad array or field");
   if (!(0 <= r0 && r0 <= r1 && r1 <= h->d.nr) || !mode_range_ok(h, j0, j1))
     return fail(h, GD_ERR_ARG, "block outside the handle's shells or modes");
@@ -690,7 +877,7 @@ int gd_synchronize(gd_handle* h) {
 }
 
 int gd_upload_spectral(gd_handle* h, int field, const double* re, const double* im) {
-  if (!h || !re || !im || field < 0 || field > 4) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
+  if (!h || !re || !im || field < 0 || field >= nfields(h)) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
   int s = stage_alloc(h);
   if (s) return s;
@@ -714,19 +901,20 @@ static int download_spec(gd_handle* h, const double* src, double* re, double* im
 }
 
 int gd_download_spectral(gd_handle* h, int field, double* re, double* im) {
-  if (!h || !re || !im || field < 0 || field > 4) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
+  if (!h || !re || !im || field < 0 || field >= nfields(h)) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
   return download_spec(h, h->field(field), re, im);
 }
 
 int gd_download_nonlinear(gd_handle* h, int field, double* re, double* im) {
-  if (!h || !re || !im || field < 0 || field > 4) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
+  if (!h || !re || !im || field < 0 || field >= nfields(h)) return h ? fail(h, GD_ERR_ARG, "bad field or pointer") : GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
   return download_spec(h, h->nl_bank(h->last_nl_par) + h->spec_elems() * field, re, im);
 }
 
 int gd_download_grid(gd_handle* h, int grid, double* out) {
   if (!h || !out || grid < 0 || grid >= NGRID) return h ? fail(h, GD_ERR_ARG, "bad grid id or pointer") : GD_ERR_ARG;
+  if (grid >= GD_GRID_C && !h->c.composition) return fail(h, GD_ERR_STATE, "the configuration has no composition");
   CK(cudaSetDevice(h->device));
   int s = stage_alloc(h);
   if (s) return s;
@@ -1127,6 +1315,16 @@ int gd_magnetic_nonlinear(gd_handle* h) {
   CK(cudaStreamSynchronize(h->stream));
   return h->precision == GD_PREC_MIXED ? mixed_check_error(h) : GD_OK;
 }
+int gd_composition_nonlinear(gd_handle* h) {
+  if (!h) return GD_ERR_ARG;
+  if (!h->c.composition) return fail(h, GD_ERR_STATE, "the configuration has no composition");
+  CK(cudaSetDevice(h->device));
+  int s = composition_nl(h);
+  if (s) return s;
+  h->last_nl_par = h->nl_par;
+  CK(cudaStreamSynchronize(h->stream));
+  return h->precision == GD_PREC_MIXED ? mixed_check_error(h) : GD_OK;
+}
 int gd_implicit_step(gd_handle* h) {
   if (!h) return GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
@@ -1181,6 +1379,8 @@ int gd_set_scheme(gd_handle* h, int scheme) {
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   if (scheme != GD_SCHEME_CNAB2) {
+    if (h->c.composition)
+      return fail(h, GD_ERR_UNSUPPORTED, "the exponential schemes are not built for composition (CNAB2 only)");
     if (h->c.bc_mode == 2)
       return fail(h, GD_ERR_UNSUPPORTED,
                   "the exponential schemes have no boundary rows (bc_mode 2 is a CNAB2 operator option)");
@@ -1226,7 +1426,7 @@ int gd_check_finite(gd_handle* h) {
   if (!h) return GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-  launch_check_finite(h->stream, 5 * h->spec_elems(), h->d_state, h->d_flag);
+  launch_check_finite(h->stream, nfields(h) * h->spec_elems(), h->d_state, h->d_flag);
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));

@@ -39,7 +39,7 @@ struct gd_handle {
   double *d_d1 = nullptr, *d_d2 = nullptr, *d_lin = nullptr, *d_lu = nullptr;
   double* d_tw = nullptr;
   float* d_twf = nullptr;
-  double* d_state = nullptr;  // 5 fields
+  double* d_state = nullptr;  // NFIELD fields (composition used when configured)
   // Two banks of the five nonlinear terms: a step writes bank nl_par and the
   // Adams-Bashforth history is the other bank (the previous step's terms), so
   // the history roll N_prev := N is a flip of nl_par instead of a copy.
@@ -47,8 +47,12 @@ struct gd_handle {
   double* d_prev = nullptr;   // bank 1
   int nl_par = 0;             // bank the next nonlinear terms go to
   int last_nl_par = 0;        // bank holding the most recently computed terms
-  double* d_work = nullptr;   // 8 derived spectral fields
-  double *d_bvals = nullptr, *d_sources = nullptr;
+  double* d_work = nullptr;   // NWORK derived spectral fields
+  double *d_bvals = nullptr, *d_sources = nullptr;    // temperature: [2][nlm] values or fluxes, [nr]
+  double *d_cbvals = nullptr, *d_csources = nullptr;  // composition
+  int* d_bctype = nullptr;    // [temperature, composition][inner, outer][nlm] GD_BC_*
+  double* d_tau = nullptr;    // tau1, tau2, tau_in, tau_out on the radial nodes
+  gd::TauConsts tau{};
   double* d_grid = nullptr;   // NGRID grids (FP64)
   double2* d_F = nullptr;     // Fourier buffer, 4 components
   double *d_epart = nullptr, *d_eout = nullptr;

@@ -26,8 +26,11 @@
 
 namespace gd {
 
-enum { F_UTOR = 0, F_UPOL = 1, F_BTOR = 2, F_BPOL = 3, F_TEMP = 4, NFIELD = 5 };
-enum { NGRID = 17 };
+// F_COMP is allocated with the others and used when the configuration has
+// composition; NWORK derived spectral arrays: 0-2 grad T, 3-4 curl u, 5-6 curl
+// B, 7 scratch, 8-10 grad C.
+enum { F_UTOR = 0, F_UPOL = 1, F_BTOR = 2, F_BPOL = 3, F_TEMP = 4, F_COMP = 5, NFIELD = 6 };
+enum { NGRID = 22, NWORK = 11 };
 
 struct Dims {
   int L, M, nlat, nlon, nr, nth, nlm, kl;
@@ -120,7 +123,21 @@ void launch_gradients(cudaStream_t s, const Dims& d, const int* lof, const int* 
 void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* rinv, const double* rinv2,
                  const double* d1, const double* d2, const double* tor, const double* pol, double* otor,
                  double* opol);
-void launch_temperature_bc(cudaStream_t s, const Dims& d, const double* bvals_native, double* T);
+// Tau functions of the flux boundary conditions (apply_flux_bc_tau!,
+// src/scalar_field_common.jl:629-812) on the radial nodes.
+struct TauConsts {
+  const double* tau1;     // T_{N-1}(x(r)), Chebyshev polynomial on the nodes
+  const double* tau2;     // T_N(x(r))
+  const double* tau_in;   // tau1 - alpha tau2 (zero analytic derivative at ro)
+  const double* tau_out;  // tau1 - beta tau2 (zero analytic derivative at ri)
+  double dt1i, dt1o, dt2i, dt2o;  // analytic dT_{N-1}/dr, dT_N/dr at ri and ro
+  double din, dout;               // (D1 tau_in)[ri], (D1 tau_out)[ro]
+};
+// Boundary conditions of a scalar field for the modes [jlo, jhi): fixed-value
+// rows, then the tau correction of the modes with a flux boundary.
+// types: [inner, outer][nlm] GD_BC_* (native order); bvals [2][nlm] values or fluxes.
+void launch_scalar_bc(cudaStream_t s, const Dims& d, const double* bvals_native, const int* types,
+                      const double* d1, const TauConsts& tc, double* F);
 void launch_lmajor_to_native(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,
                              double* dst, int nplanes);
 void launch_native_to_lmajor(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,
@@ -132,10 +149,10 @@ void launch_grid_cast(cudaStream_t s, size_t n, const R* src, double* dst);
 
 // ---- CNAB2 (gd_cnab2.cu) ----
 struct Cnab2Args {
-  double* u[5];
-  const double* nl[5];
-  const double* prev[5];  // the previous step's nonlinear terms (read only)
-  int kind[5];
+  double* u[6];
+  const double* nl[6];
+  const double* prev[6];  // the previous step's nonlinear terms (read only)
+  int kind[6];            // 0 velocity, 1 magnetic, 2 temperature, 3 composition
   int nfield;
   int boot;
   int clamp_rows;

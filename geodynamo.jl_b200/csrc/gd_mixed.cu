@@ -20,8 +20,11 @@ namespace gd {
 enum {
   FC_T = 0, FC_GTH = 1, FC_GPH = 2, FC_GR = 3,  // temperature phase (scalar synthesis order)
   FC_U = 4, FC_W = 6, FC_B = 8, FC_J = 10,      // theta, phi pairs
-  FC_COUNT = 12
+  FC_C = 12,                                    // composition phase: C, d_theta C, d_phi C, d_r C
+  FC_COUNT = 16
 };
+// components allocated: the composition's only with composition
+static int fc_count(const gd_handle* h) { return h->c.composition ? FC_COUNT : FC_C; }
 
 struct MixedState {
   double *ra = nullptr, *rb = nullptr, *rc = nullptr, *r1a = nullptr, *r1b = nullptr, *pmm = nullptr,
@@ -301,7 +304,7 @@ int mixed_create(gd_handle* h) {
   MAL(x->r1a, d.L + 1); MAL(x->r1b, d.L + 1);
   MAL(x->pmm, (size_t)(d.M + 1) * d.nth); MAL(x->sinv, d.nth);
   x->fcomp = fourier_comp_elems(d);
-  MAL(x->d_Fall, (size_t)FC_COUNT * x->fcomp);
+  MAL(x->d_Fall, (size_t)fc_count(h) * x->fcomp);
   MAL(x->d_G, (size_t)2 * d.nr * (d.M + 1) * 2 * d.nth);
   MAL(x->d_stage, (size_t)4 * h->grid_elems());
   MAL(x->d_err, 4);
@@ -329,7 +332,7 @@ int mixed_create(gd_handle* h) {
   if (s) return s;
   // the carried components start as zero grids (the reference's physical
   // fields are zero-filled at allocation, src/fields.jl:82)
-  s = mcheck(h, cudaMemsetAsync(x->d_Fall, 0, sizeof(float4) * FC_COUNT * x->fcomp, h->stream), "memset");
+  s = mcheck(h, cudaMemsetAsync(x->d_Fall, 0, sizeof(float4) * fc_count(h) * x->fcomp, h->stream), "memset");
   if (s) return s;
   s = mcheck(h, cudaMemsetAsync(x->d_err, 0, sizeof(int), h->stream), "memset");
   if (s) return s;
@@ -399,11 +402,39 @@ int mixed_temperature_nl(gd_handle* h) {
   double* out[1] = {h->nlf(F_TEMP)};
   s = tc_analysis_scalar_G(h, 1, out);
   if (s) return s;
-  if (!h->ext_derivs) {
-    ProfScope p(h, "temperature_bc");
-    launch_temperature_bc(h->stream, d, h->d_bvals, h->field(F_TEMP));
-  }
+  if (!h->ext_derivs) scalar_bc(h, F_TEMP);
   return launched(h, "mixed temperature nonlinear");
+}
+
+// The composition phase (compute_composition_nonlinear!, src/compositional.jl:
+// 219-259): gradient (FP64, into work 8-10, unless received), split-TF32
+// synthesis of C and its gradient, the fused advection -u.grad C + S_C(r) with
+// the velocity components of this step's velocity phase (step_once! computes
+// composition after velocity), the analysis, then the boundary conditions.
+int mixed_composition_nl(gd_handle* h) {
+  MixedState* x = h->mixed;
+  const Dims& d = h->d;
+  if (!h->ext_derivs) {
+    ProfScope p(h, "spectral_gradients");
+    launch_gradients(h->stream, d, h->d_lof, h->d_mof, h->d_rinv, h->d_d1, h->field(F_COMP), h->work(8), h->work(9),
+                     h->work(10));
+  }
+  const double* coef[4] = {h->field(F_COMP), h->work(8), h->work(9), h->work(10)};
+  int s = tc_synth_scalar(h, coef, 4, x->F(FC_C), 0xF);
+  if (s) return s;
+  FusedArgs f = phase_args(h);
+  f.sources = h->d_csources;
+  const float4* fin[5] = {x->F(FC_C + 3), x->F(FC_U), x->F(FC_C + 1), x->F(FC_U + 1), x->F(FC_C + 2)};
+  for (int i = 0; i < 5; ++i) f.fin[i] = fin[i];
+  f.nin = 5;
+  { ProfScope p(h, "fused_composition_fp32"); launch_fused(h->stream, d, h->plan, h->d_twf, FUSED_TEMPERATURE, f); }
+  s = launched(h, "fused composition phase");
+  if (s) return s;
+  double* out[1] = {h->nlf(F_COMP)};
+  s = tc_analysis_scalar_G(h, 1, out);
+  if (s) return s;
+  if (!h->ext_derivs) scalar_bc(h, F_COMP);
+  return launched(h, "mixed composition nonlinear");
 }
 
 // The velocity phase.  The stages of h->fp64_stages run in FP64 with the FP64
@@ -552,6 +583,10 @@ int mixed_grid_to_double(gd_handle* h, int grid, double* out) {
     case GD_GRID_GPH: fc = FC_GPH; break;
     case GD_GRID_GR: fc = FC_GR; break;
     case GD_GRID_T: fc = FC_T; break;
+    case GD_GRID_C: fc = FC_C; break;
+    case GD_GRID_CGTH: fc = FC_C + 1; break;
+    case GD_GRID_CGPH: fc = FC_C + 2; break;
+    case GD_GRID_CGR: fc = FC_C + 3; break;
     default:
       return set_error(h, GD_ERR_UNSUPPORTED,
                        "the mixed-precision step forms the nonlinear products in shared memory only; download "

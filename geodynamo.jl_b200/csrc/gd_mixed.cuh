@@ -18,6 +18,10 @@ int mixed_set_fault_test(gd_handle* h, long long wait_cycles, int omit_step);
 void mixed_destroy(gd_handle* h);
 size_t mixed_bytes(const gd_handle* h);
 int mixed_temperature_nl(gd_handle* h);
+int mixed_composition_nl(gd_handle* h);
+// Boundary conditions (fixed values, tau flux correction) of F_TEMP or F_COMP
+// over the handle's mode range (gd_api.cu).
+void scalar_bc(gd_handle* h, int field);
 int mixed_velocity_nl(gd_handle* h);
 int mixed_magnetic_nl(gd_handle* h);
 // GD_ERR_UNSUPPORTED for the product grids, which the mixed step does not store.

@@ -271,18 +271,65 @@ void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* m
 
 // apply_temperature_boundary_conditions_spectral! (src/thermal.jl:262-303):
 // Dirichlet rows r = ri and r = ro of the temperature state.
-__global__ void k_temperature_bc(Dims d, const double* __restrict__ bv, double* __restrict__ T) {
+// Boundary conditions of a scalar field (apply_temperature_boundary_conditions_spectral!,
+// src/thermal.jl:262-303; apply_composition_boundary_conditions_spectral!,
+// src/compositional.jl:318-370).  One thread per mode: fixed-value rows first
+// (Re = value, Im = 0), then, for a flux boundary, the tau correction of
+// apply_flux_bc_tau! (src/scalar_field_common.jl:866-935): the flux error of
+// the real profile at each flux boundary (prescribed - (D1 Re)[boundary]),
+// coefficients of the tau functions that cancel it, and the same correction
+// added to Re and, when any |Im| exceeds 1e-12, to Im.
+__global__ void k_scalar_bc(Dims d, const double* __restrict__ bv, const int* __restrict__ types,
+                            const double* __restrict__ d1, TauConsts tc, double* __restrict__ F) {
   const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.jhi) return;
-  const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
-  T[j] = bv[j];
-  T[plane + j] = 0.0;
-  T[(size_t)(d.nr - 1) * NM + j] = bv[NM + j];
-  T[plane + (size_t)(d.nr - 1) * NM + j] = 0.0;
+  const int N = d.nr, KL = d.kl, NB = 2 * GD_MAX_KL + 1;
+  const size_t NM = d.nlm, plane = (size_t)N * NM;
+  double* re = F + j;
+  double* im = F + plane + j;
+  const int ti = types[j], to = types[NM + j];
+  if (ti == GD_BC_VALUE) { re[0] = bv[j]; im[0] = 0.0; }
+  if (to == GD_BC_VALUE) { re[(size_t)(N - 1) * NM] = bv[NM + j]; im[(size_t)(N - 1) * NM] = 0.0; }
+  const bool fi = ti == GD_BC_FLUX, fo = to == GD_BC_FLUX;
+  if (!fi && !fo) return;
+  // boundary fluxes of the real profile: rows 0 and N - 1 of the banded D1
+  // (entry (i, col) at d1[(i - col + KL) + NB col])
+  double qi = 0.0, qo = 0.0;
+  for (int col = 0; col <= KL && col < N; ++col) qi += d1[(0 - col + KL) + NB * col] * re[(size_t)col * NM];
+  for (int col = N - 1 - KL < 0 ? 0 : N - 1 - KL; col < N; ++col)
+    qo += d1[(N - 1 - col + KL) + NB * col] * re[(size_t)col * NM];
+  const double ei = fi ? bv[j] - qi : 0.0, eo = fo ? bv[NM + j] - qo : 0.0;
+  double c1 = 0.0, c2 = 0.0;
+  const double *t1 = tc.tau1, *t2 = tc.tau2;
+  if (fi && fo) {  // compute_tau_coefficients_both
+    const double det = tc.dt1i * tc.dt2o - tc.dt1o * tc.dt2i;
+    if (fabs(det) > 1e-12) {
+      c1 = (ei * tc.dt2o - eo * tc.dt2i) / det;
+      c2 = (eo * tc.dt1i - ei * tc.dt1o) / det;
+    }
+  } else if (fi) {  // compute_tau_coefficients_inner
+    c1 = ei / tc.din;
+    t1 = tc.tau_in;
+    t2 = nullptr;
+  } else {          // compute_tau_coefficients_outer
+    c1 = eo / tc.dout;
+    t1 = tc.tau_out;
+    t2 = nullptr;
+  }
+  bool im_live = false;
+  for (int i = 0; i < N; ++i) im_live |= fabs(im[(size_t)i * NM]) > 1e-12;
+  for (int i = 0; i < N; ++i) {
+    // profile += c1 tau1 + c2 tau2, without contraction into fused multiply-adds
+    double corr = __dmul_rn(c1, t1[i]);
+    if (t2) corr = __dadd_rn(corr, __dmul_rn(c2, t2[i]));
+    re[(size_t)i * NM] = __dadd_rn(re[(size_t)i * NM], corr);
+    if (im_live) im[(size_t)i * NM] = __dadd_rn(im[(size_t)i * NM], corr);
+  }
 }
 
-void launch_temperature_bc(cudaStream_t s, const Dims& d, const double* bvals_native, double* T) {
-  k_temperature_bc<<<ceil_div(d.jhi - d.jlo, 256), 256, 0, s>>>(d, bvals_native, T);
+void launch_scalar_bc(cudaStream_t s, const Dims& d, const double* bvals_native, const int* types, const double* d1,
+                      const TauConsts& tc, double* F) {
+  k_scalar_bc<<<ceil_div(d.jhi - d.jlo, 128), 128, 0, s>>>(d, bvals_native, types, d1, tc, F);
 }
 
 __global__ void k_perm(int nlm, size_t rows, const int* __restrict__ perm, const double* __restrict__ src,

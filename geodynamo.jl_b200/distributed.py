@@ -205,6 +205,7 @@ class DistributedStep:
         self.shell.set_external_derivatives(True)
         self.nr = nr
         self.magnetic = c.get("magnetic", 1)
+        self.composition = c.get("composition", 0)
         self.torch = torch
         self.dev = torch.device("cuda", device) if device_exchange else torch.device("cpu")
         self.pin = not device_exchange and torch.cuda.is_available()
@@ -219,6 +220,15 @@ class DistributedStep:
         if sources is not None:
             s0, s1 = self.dec.shells[self.rank]
             self.shell.set_temperature_bc(None, np.asarray(sources, dtype=np.float64)[s0:s1])
+
+    def set_composition_bc(self, bvals=None, sources=None):
+        self.mode.set_composition_bc(bvals, None)
+        if sources is not None:
+            s0, s1 = self.dec.shells[self.rank]
+            self.shell.set_composition_bc(None, np.asarray(sources, dtype=np.float64)[s0:s1])
+
+    def set_bc_types(self, name, inner, outer):
+        self.mode.set_bc_types(name, inner, outer)  # the boundary rows act in the mode layout
 
     def own_modes(self, name):
         """(re, im) of this rank's m columns of a state field, shape (nr, j1 - j0) each (native order)."""
@@ -287,6 +297,9 @@ class DistributedStep:
         ns = s1 - s0
         fields = self.STATE_FIELDS if self.magnetic else (0, 1, 4)
         derived = self.DERIVED if self.magnetic else (0, 1, 2, 3, 4)
+        if self.composition:  # the composition and its gradient (work 8-10)
+            fields = fields + (5,)
+            derived = derived + (8, 9, 10)
         out_items = [(0, f) for f in fields] + [(1, k) for k in derived]
         nl_items = [(2, f) for f in fields]
         for _ in range(n):
@@ -301,6 +314,8 @@ class DistributedStep:
             self.shell.velocity_nl()
             if self.magnetic:
                 self.shell.magnetic_nl()
+            if self.composition:
+                self.shell.composition_nl()
             # nonlinear terms back: shell layout -> mode layout
             self._exchange(self.shell, self.mode, nl_items,
                            lambda k: ((0, ns), self.dec.modes[k]),
@@ -312,4 +327,4 @@ class DistributedStep:
         self.mode.close()
 
 
-FIELD_IDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4}
+FIELD_IDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4, "comp": 5}

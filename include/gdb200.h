@@ -39,8 +39,9 @@ enum {
   GD_ERR_STATE = 7        /* call order violated                            */
 };
 
-/* Field ids (state, nonlinear terms). */
-enum { GD_U_TOR = 0, GD_U_POL = 1, GD_B_TOR = 2, GD_B_POL = 3, GD_TEMP = 4 };
+/* Field ids (state, nonlinear terms).  GD_COMP exists when the configuration
+ * has composition. */
+enum { GD_U_TOR = 0, GD_U_POL = 1, GD_B_TOR = 2, GD_B_POL = 3, GD_TEMP = 4, GD_COMP = 5 };
 
 /* Physical grids kept by the model (velocity.jl, magnetic.jl, thermal.jl). */
 enum {
@@ -48,8 +49,16 @@ enum {
   GD_GRID_B_TH = 4, GD_GRID_B_PH = 5, GD_GRID_J_TH = 6, GD_GRID_J_PH = 7,
   GD_GRID_T = 8, GD_GRID_GTH = 9, GD_GRID_GPH = 10, GD_GRID_GR = 11,
   GD_GRID_TADV = 12, GD_GRID_VADV_TH = 13, GD_GRID_VADV_PH = 14,
-  GD_GRID_IND_TH = 15, GD_GRID_IND_PH = 16
+  GD_GRID_IND_TH = 15, GD_GRID_IND_PH = 16,
+  /* composition (compositional.jl): C, its gradient (theta, phi, r), -u.grad C + S */
+  GD_GRID_C = 17, GD_GRID_CGTH = 18, GD_GRID_CGPH = 19, GD_GRID_CGR = 20, GD_GRID_CADV = 21
 };
+
+/* Boundary-condition types of a scalar field's modes (bc_type_inner /
+ * bc_type_outer of the reference's scalar fields): fixed value, or fixed flux
+ * dC/dr applied by the tau method (apply_flux_bc_tau!,
+ * src/scalar_field_common.jl:866-935). */
+enum { GD_BC_VALUE = 1, GD_BC_FLUX = 2 };
 
 /* Precision modes. */
 enum { GD_PREC_FP64 = 0, GD_PREC_MIXED = 1 };
@@ -88,6 +97,12 @@ enum { GD_SCHEME_CNAB2 = 0, GD_SCHEME_EAB2 = 1, GD_SCHEME_ERK2 = 2 };
  *   fd_mode   0: radial difference weights from V^T w = rhs (the intent of
  *             create_derivative_matrix, linear_algebra.jl:90-132);
  *             1: the literal V c = rhs solve (ill-conditioned, kept for study).
+ * composition 1 adds the compositional field C (include_composition,
+ * src/simulation.jl:107-131): advected by the velocity after the magnetic phase
+ * (step_once!), diffusivity Pm/Sc with schmidt = d_Sc, no-flux boundaries by
+ * default (create_shtns_composition_field, src/compositional.jl:80-118).  Its
+ * buoyancy is a radial force, which the vector analysis does not keep, so C
+ * does not act on the velocity.  CNAB2 with bc_mode 0 or 1 only.
  */
 typedef struct gd_config {
   int lmax, mmax, nlat, nlon, nr;
@@ -100,6 +115,8 @@ typedef struct gd_config {
   int fd_mode;
   int precision;
   int magnetic;
+  int composition;
+  double schmidt;
 } gd_config;
 
 typedef struct gd_handle gd_handle;
@@ -128,7 +145,8 @@ int gd_set_fp64_stages(gd_handle* h, int mask);
 int gd_synchronize(gd_handle* h);
 
 /* ---- state ------------------------------------------------------------------
- * Host <-> device copies of the five spectral fields in the reference layout. */
+ * Host <-> device copies of the spectral fields in the reference layout (the
+ * five of the step, and GD_COMP with composition). */
 int gd_upload_spectral(gd_handle* h, int field, const double* re, const double* im);
 int gd_download_spectral(gd_handle* h, int field, double* re, double* im);
 int gd_download_nonlinear(gd_handle* h, int field, double* re, double* im);
@@ -137,6 +155,22 @@ int gd_download_grid(gd_handle* h, int grid, double* out);
  * thermal.jl:285,297) and internal sources [nr] (add_internal_sources_local!,
  * scalar_field_common.jl:416-443).  Either pointer may be NULL. */
 int gd_set_temperature_bc(gd_handle* h, const double* bvals, const double* sources);
+/* Composition boundary values or fluxes [2][nlm] and internal sources [nr]
+ * (boundary_values, internal_sources of SHTnsCompositionField,
+ * src/compositional.jl:106-111); GD_ERR_STATE without composition. */
+int gd_set_composition_bc(gd_handle* h, const double* bvals, const double* sources);
+/* Boundary types (GD_BC_VALUE / GD_BC_FLUX) of every mode of a scalar field
+ * (GD_TEMP or GD_COMP), inner[nlm] and outer[nlm] in the reference's l-major
+ * order (bc_type_inner / bc_type_outer).  Defaults: temperature GD_BC_VALUE,
+ * composition GD_BC_FLUX (zero flux).  Where a mode's type is GD_BC_FLUX its
+ * boundary value is the prescribed flux dC/dr, imposed by the tau method of
+ * apply_flux_bc_tau! (src/scalar_field_common.jl:866-935) on the state after
+ * the field's nonlinear term: Chebyshev T_{N-1} and T_N (or the one-sided
+ * combinations when one boundary has a flux) are added to the radial profile
+ * with the coefficients that cancel the real profile's flux error, the same
+ * correction going to the imaginary profile when it is not ~0.  Flux types
+ * need bc_mode 0 or 1. */
+int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int* outer);
 
 /* ---- transforms on host arrays (reference layout) ---------------------------
  * shtnskit_spectral_to_physical! / batch_spectral_to_physical!
@@ -228,6 +262,9 @@ int gd_solve_implicit_step(gd_handle* h, const gd_matrices* m, const double* rhs
 int gd_temperature_nonlinear(gd_handle* h);
 int gd_velocity_nonlinear(gd_handle* h);
 int gd_magnetic_nonlinear(gd_handle* h);
+/* compute_composition_nonlinear! (src/compositional.jl:219-259), with the
+ * velocity grids of the last velocity phase; GD_ERR_STATE without composition. */
+int gd_composition_nonlinear(gd_handle* h);
 /* apply_master_implicit_step! (src/simulation.jl:1151-1330) with
  * build_rhs_cnab2! + solve_implicit_step! (src/timestep.jl:610-730). */
 int gd_implicit_step(gd_handle* h);
@@ -347,7 +384,7 @@ int gd_ensemble_autotune(gd_ensemble* e, int nsteps, float* best_ms, int* caps_o
  * Radial derivatives of the state (compute_all_gradients_spectral!,
  * compute_vorticity_spectral_full!, compute_current_density_spectral!) for the
  * modes [j0, j1) only, into the handle's work arrays (0-2: grad T theta, phi,
- * r; 3-4: curl u toroidal, poloidal; 5-6: curl B). */
+ * r; 3-4: curl u toroidal, poloidal; 5-6: curl B; 8-10: grad C). */
 int gd_derivatives(gd_handle* h, int j0, int j1);
 /* The temperature Dirichlet rows and the CNAB2 solve (build_rhs_cnab2! +
  * solve_implicit_step!) for the modes [j0, j1) only, with the nonlinear terms in
@@ -361,7 +398,7 @@ int gd_set_external_derivatives(gd_handle* h, int enable);
 /* Copies the block [shells r0..r1) x [modes j0..j1) of one spectral array
  * between the handle and buf (device or pinned host memory), both planes:
  * buf = [Re, Im][r1 - r0][j1 - j0] doubles.  array 0: state field (GD_U_TOR ..
- * GD_TEMP); 1: work array 0-7; 2: nonlinear term of the current bank.
+ * GD_TEMP, GD_COMP); 1: work array 0-10; 2: nonlinear term of the current bank.
  * to_buf != 0 copies from the handle into buf.  Synchronises the stream. */
 int gd_copy_block(gd_handle* h, int array, int field, int r0, int r1, int j0, int j1, void* buf, int to_buf);
 

@@ -77,6 +77,8 @@ typedef struct oc_config {
   int fd_mode;
   int precision;   // ignored by the oracle (always FP64)
   int magnetic;    // i_B
+  int composition; // include_composition
+  double schmidt;  // d_Sc
 } oc_config;
 }
 
@@ -175,7 +177,8 @@ void dense_solve(int n, std::vector<double> A /* row-major n x n */, std::vector
   }
 }
 
-enum { F_UTOR = 0, F_UPOL = 1, F_BTOR = 2, F_BPOL = 3, F_TEMP = 4, NFIELD = 5 };
+enum { F_UTOR = 0, F_UPOL = 1, F_BTOR = 2, F_BPOL = 3, F_TEMP = 4, F_COMP = 5, NFIELD = 6 };
+enum { BC_VALUE = 1, BC_FLUX = 2 };
 
 struct Oracle {
   oc_config c{};
@@ -186,8 +189,8 @@ struct Oracle {
   std::vector<double> r, rinv, rinv2;
   std::vector<double> P, dP;      // [moff[m] + (l-m)] * nth + ith  (north half)
   std::vector<double> d1, d2, lap;  // band (2kl+1) x nr, Julia column-major
-  std::vector<double> lin[3], lu[3];  // per diffusivity kind: [l][band]
-  double nu[3] = {0, 0, 0};
+  std::vector<double> lin[4], lu[4];  // per diffusivity kind: [l][band]
+  double nu[4] = {0, 0, 0, 0};
   FFT fft;
   // state, reference layout: [r][lm] (lm fastest)
   std::vector<double> fre[NFIELD], fim[NFIELD];
@@ -195,8 +198,11 @@ struct Oracle {
   // persistent physical grids, reference layout [r][phi][theta]
   std::vector<double> u_th, u_ph, w_th, w_ph, b_th, b_ph, j_th, j_ph;
   std::vector<double> t_grid, gth_grid, gph_grid, gr_grid, tadv, vadv_th, vadv_ph, ind_th, ind_ph;
-  std::vector<double> bvals;      // [2][nlm] temperature Dirichlet values
+  std::vector<double> c_grid, cgth_grid, cgph_grid, cgr_grid, cadv;
+  std::vector<double> bvals;      // [2][nlm] temperature boundary values (or fluxes)
   std::vector<double> sources;    // [nr] internal heat sources
+  std::vector<double> cbvals, csources;  // composition
+  std::vector<int> tbc, cbc;      // [2][nlm] bc_type_inner / bc_type_outer (l-major)
   long step_count = 0;
   int nthreads = 1;
 
@@ -229,8 +235,16 @@ struct Oracle {
     for (auto* g : {&u_th, &u_ph, &w_th, &w_ph, &b_th, &b_ph, &j_th, &j_ph, &t_grid, &gth_grid,
                     &gph_grid, &gr_grid, &tadv, &vadv_th, &vadv_ph, &ind_th, &ind_ph})
       g->assign(grid_size(), 0.0);
+    if (c.composition)
+      for (auto* g : {&c_grid, &cgth_grid, &cgph_grid, &cgr_grid, &cadv}) g->assign(grid_size(), 0.0);
     bvals.assign(2 * (size_t)nlm, 0.0);
     sources.assign(c.nr, 0.0);
+    cbvals.assign(2 * (size_t)nlm, 0.0);
+    csources.assign(c.nr, 0.0);
+    // create_shtns_temperature_field: fixed temperature (thermal.jl:113-114);
+    // create_shtns_composition_field: no flux (compositional.jl:112-114)
+    tbc.assign(2 * (size_t)nlm, BC_VALUE);
+    cbc.assign(2 * (size_t)nlm, BC_FLUX);
     build_implicit();
     return 0;
   }
@@ -372,10 +386,11 @@ struct Oracle {
     nu[0] = c.magnetic_prandtl;                    // velocity (simulation.jl:229)
     nu[1] = 1.0;                                   // magnetic (simulation.jl:230)
     nu[2] = c.magnetic_prandtl / c.prandtl;        // temperature (simulation.jl:231)
+    nu[3] = c.composition ? c.magnetic_prandtl / c.schmidt : 0.0;  // composition (simulation.jl:131)
     const int N = c.nr, bw = c.kl;
     const size_t bsz = (size_t)nbw * N;
     const double inv_dt = 1.0 / c.dt, mth = -c.implicit_theta;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < (c.composition ? 4 : 3); ++k) {
       lin[k].assign(bsz * (c.lmax + 1), 0.0);
       lu[k].assign(bsz * (c.lmax + 1), 0.0);
       for (int l = 0; l <= c.lmax; ++l) {
@@ -728,12 +743,106 @@ struct Oracle {
     }
     analysis_scalar(tadv.data(), nre[F_TEMP].data(), nim[F_TEMP].data());
     // apply_temperature_boundary_conditions_spectral! (thermal.jl:262-303): on the state.
-    for (int q = 0; q < nlm; ++q) {
-      fre[F_TEMP][q] = bvals[q];
-      fim[F_TEMP][q] = 0.0;
-      fre[F_TEMP][(size_t)(c.nr - 1) * nlm + q] = bvals[(size_t)nlm + q];
-      fim[F_TEMP][(size_t)(c.nr - 1) * nlm + q] = 0.0;
+    scalar_bc(F_TEMP, bvals, tbc);
+  }
+
+  // Boundary conditions of a scalar field on its state: fixed values
+  // (thermal.jl:280-300, compositional.jl:334-360), then the tau method of
+  // apply_scalar_flux_bc_spectral! / apply_flux_bc_tau!
+  // (scalar_field_common.jl:866-935, 1166-1198) for every mode with a flux
+  // boundary.  The derivative matrix is the one of the handle's fd_mode.
+  double cheb(int n, double rr) const {  // compute_chebyshev_polynomial (:604-622)
+    const double ri = r[0], ro = r[c.nr - 1];
+    const double xx = 2.0 * (rr - ri) / (ro - ri) - 1.0;
+    return std::cos(n * std::acos(std::max(-1.0, std::min(1.0, xx))));
+  }
+  double dcheb(int n, double rr) const {  // evaluate_chebyshev_derivative (:629-650)
+    const double ri = r[0], ro = r[c.nr - 1];
+    const double xx = 2.0 * (rr - ri) / (ro - ri) - 1.0;
+    double d;
+    if (std::fabs(std::fabs(xx) - 1.0) < 1e-12) {
+      const double sg = xx > 0 ? 1.0 : (xx < 0 ? -1.0 : 0.0);
+      d = (double)n * n * std::pow(sg, n + 1);
+    } else {
+      const double t = std::acos(std::max(-1.0, std::min(1.0, xx)));
+      d = n * std::sin(n * t) / std::sin(t);
     }
+    return d * (2.0 / (ro - ri));
+  }
+  void scalar_bc(int f, const std::vector<double>& bv, const std::vector<int>& types) {
+    const int N = c.nr;
+    const double ri = r[0], ro = r[N - 1];
+    std::vector<double> t1(N), t2(N);
+    for (int i = 0; i < N; ++i) { t1[i] = cheb(N - 1, r[i]); t2[i] = cheb(N, r[i]); }
+    const double d1i = dcheb(N - 1, ri), d1o = dcheb(N - 1, ro), d2i = dcheb(N, ri), d2o = dcheb(N, ro);
+    for (int q = 0; q < nlm; ++q) {
+      const int ti = types[q], to = types[(size_t)nlm + q];
+      if (ti == BC_VALUE) { fre[f][q] = bv[q]; fim[f][q] = 0.0; }
+      if (to == BC_VALUE) {
+        fre[f][(size_t)(N - 1) * nlm + q] = bv[(size_t)nlm + q];
+        fim[f][(size_t)(N - 1) * nlm + q] = 0.0;
+      }
+    }
+    for (int q = 0; q < nlm; ++q) {
+      const bool ai = types[q] == BC_FLUX, ao = types[(size_t)nlm + q] == BC_FLUX;
+      if (!ai && !ao) continue;
+      std::vector<double> pr(N), pi(N), dp(N);
+      for (int k = 0; k < N; ++k) { pr[k] = fre[f][(size_t)k * nlm + q]; pi[k] = fim[f][(size_t)k * nlm + q]; }
+      const double fi = ai ? bv[q] : 0.0, fo = ao ? bv[(size_t)nlm + q] : 0.0;
+      band_apply(d1.data(), pr.data(), dp.data());  // compute_boundary_fluxes
+      const double ei = fi - dp[0], eo = fo - dp[N - 1];
+      std::vector<double> corr(N, 0.0);
+      if (ai && ao) {  // compute_tau_coefficients_both
+        const double det = d1i * d2o - d1o * d2i;
+        double c1 = 0.0, c2 = 0.0;
+        if (std::fabs(det) > 1e-12) {
+          c1 = (ei * d2o - eo * d2i) / det;
+          c2 = (eo * d1i - ei * d1o) / det;
+        }
+        for (int k = 0; k < N; ++k) corr[k] = c1 * t1[k] + c2 * t2[k];
+      } else {  // compute_tau_coefficients_inner / _outer
+        const double a = ai ? (std::fabs(d2o) > 1e-12 ? d1o / d2o : 0.0) : (std::fabs(d2i) > 1e-12 ? d1i / d2i : 0.0);
+        std::vector<double> tau(N), dtau(N);
+        for (int k = 0; k < N; ++k) tau[k] = t1[k] - a * t2[k];
+        band_apply(d1.data(), tau.data(), dtau.data());
+        const double cc = ai ? ei / dtau[0] : eo / dtau[N - 1];
+        for (int k = 0; k < N; ++k) corr[k] = cc * tau[k];
+      }
+      bool im_live = false;
+      for (int k = 0; k < N; ++k) im_live = im_live || std::fabs(pi[k]) > 1e-12;
+      for (int k = 0; k < N; ++k) {
+        fre[f][(size_t)k * nlm + q] = pr[k] + corr[k];
+        if (im_live) fim[f][(size_t)k * nlm + q] = pi[k] + corr[k];
+      }
+    }
+  }
+
+  // compute_composition_nonlinear! (compositional.jl:219-259): as the
+  // temperature's, with this step's velocity grids and its own sources and
+  // boundary conditions
+  void composition_nl() {
+    const size_t ss = spec_size();
+    std::vector<double> gtr(ss), gti(ss), gpr(ss), gpi(ss), grr(ss), gri(ss);
+    gradients(fre[F_COMP].data(), fim[F_COMP].data(), gtr.data(), gti.data(), gpr.data(), gpi.data(),
+              grr.data(), gri.data());
+    synth_scalar(fre[F_COMP].data(), fim[F_COMP].data(), c_grid.data());
+    synth_scalar(gtr.data(), gti.data(), cgth_grid.data());
+    synth_scalar(gpr.data(), gpi.data(), cgph_grid.data());
+    synth_scalar(grr.data(), gri.data(), cgr_grid.data());
+    const size_t plane = (size_t)c.nlat * c.nlon;
+#pragma omp parallel for num_threads(nthreads)
+    for (int k = 0; k < c.nr; ++k) {
+      const double src = csources[k];
+      for (size_t q = 0; q < plane; ++q) {
+        const size_t i = (size_t)k * plane + q;
+        const double ur = 0.0;
+        double v = -(ur * cgr_grid[i] + u_th[i] * cgth_grid[i] + u_ph[i] * cgph_grid[i]);
+        if (src != 0.0) v += src;
+        cadv[i] = v;
+      }
+    }
+    analysis_scalar(cadv.data(), nre[F_COMP].data(), nim[F_COMP].data());
+    scalar_bc(F_COMP, cbvals, cbc);
   }
 
   // compute_velocity_nonlinear! (velocity.jl:312-332, 447-548, 638-672)
@@ -811,15 +920,16 @@ struct Oracle {
   // build_rhs_cnab2! + solve_implicit_step! (timestep.jl:610-730)
   void implicit_step() {
     const bool boot = (c.ab_mode == 1) || (step_count == 0);
-    const int nf = c.magnetic ? NFIELD : 3;
-    const int fields[5] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL};
+    int fields[6] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL, F_COMP};
+    int nf = c.magnetic ? 5 : 3;
+    if (c.composition) fields[nf++] = F_COMP;
     const int N = c.nr;
     const size_t bsz = (size_t)nbw * N;
     const double inv_dt = 1.0 / c.dt, lw = 1.0 - c.implicit_theta;
     for (int fi = 0; fi < nf; ++fi) {
       const int f = fields[fi];
       if (boot) { pre[f] = nre[f]; pim[f] = nim[f]; }
-      const int kind = (f == F_TEMP) ? 2 : (f == F_UTOR || f == F_UPOL) ? 0 : 1;
+      const int kind = (f == F_TEMP) ? 2 : (f == F_COMP) ? 3 : (f == F_UTOR || f == F_UPOL) ? 0 : 1;
 #pragma omp parallel for num_threads(nthreads)
       for (int q = 0; q < nlm; ++q) {
         const int l = lv[q];
@@ -863,6 +973,7 @@ struct Oracle {
     temperature_nl();
     velocity_nl();
     if (c.magnetic) magnetic_nl();
+    if (c.composition) composition_nl();
     implicit_step();
   }
 
@@ -883,7 +994,8 @@ struct Oracle {
 
   std::vector<double>* grid_by_id(int id) {
     std::vector<double>* g[] = {&u_th, &u_ph, &w_th, &w_ph, &b_th, &b_ph, &j_th, &j_ph, &t_grid,
-                                &gth_grid, &gph_grid, &gr_grid, &tadv, &vadv_th, &vadv_ph, &ind_th, &ind_ph};
+                                &gth_grid, &gph_grid, &gr_grid, &tadv, &vadv_th, &vadv_ph, &ind_th, &ind_ph,
+                                &c_grid, &cgth_grid, &cgph_grid, &cgr_grid, &cadv};
     if (id < 0 || id >= (int)(sizeof(g) / sizeof(g[0]))) return nullptr;
     return g[id];
   }
@@ -983,7 +1095,7 @@ void oc_get_nl(void* h, int f, double* re, double* im) {
 int oc_get_grid_field(void* h, int id, double* out) {
   Oracle* o = static_cast<Oracle*>(h);
   std::vector<double>* g = o->grid_by_id(id);
-  if (!g) return 1;
+  if (!g || g->empty()) return 1;
   std::memcpy(out, g->data(), g->size() * sizeof(double));
   return 0;
 }
@@ -992,6 +1104,19 @@ void oc_set_temperature_bc(void* h, const double* bvals /* [2][nlm] */, const do
   if (bvals) std::memcpy(o->bvals.data(), bvals, 2 * (size_t)o->nlm * sizeof(double));
   if (sources) std::memcpy(o->sources.data(), sources, (size_t)o->c.nr * sizeof(double));
 }
+void oc_set_composition_bc(void* h, const double* bvals /* [2][nlm] */, const double* sources /* [nr] */) {
+  Oracle* o = static_cast<Oracle*>(h);
+  if (bvals) std::memcpy(o->cbvals.data(), bvals, 2 * (size_t)o->nlm * sizeof(double));
+  if (sources) std::memcpy(o->csources.data(), sources, (size_t)o->c.nr * sizeof(double));
+}
+// field 4 (temperature) or 5 (composition): bc_type_inner / bc_type_outer, l-major
+void oc_set_bc_types(void* h, int field, const int* inner, const int* outer) {
+  Oracle* o = static_cast<Oracle*>(h);
+  std::vector<int>& t = field == F_COMP ? o->cbc : o->tbc;
+  std::memcpy(t.data(), inner, (size_t)o->nlm * sizeof(int));
+  std::memcpy(t.data() + o->nlm, outer, (size_t)o->nlm * sizeof(int));
+}
+void oc_composition_nl(void* h) { static_cast<Oracle*>(h)->composition_nl(); }
 void oc_temperature_nl(void* h) { static_cast<Oracle*>(h)->temperature_nl(); }
 void oc_velocity_nl(void* h) { static_cast<Oracle*>(h)->velocity_nl(); }
 void oc_magnetic_nl(void* h) { static_cast<Oracle*>(h)->magnetic_nl(); }

@@ -21,11 +21,12 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libgdoracle.so")
 
-FIELD_IDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4}
+FIELD_IDS = {"u_tor": 0, "u_pol": 1, "b_tor": 2, "b_pol": 3, "temp": 4, "comp": 5}
 GRID_IDS = {
     "u_th": 0, "u_ph": 1, "w_th": 2, "w_ph": 3, "b_th": 4, "b_ph": 5, "j_th": 6, "j_ph": 7,
     "t": 8, "gth": 9, "gph": 10, "gr": 11, "tadv": 12, "vadv_th": 13, "vadv_ph": 14,
     "ind_th": 15, "ind_ph": 16,
+    "c": 17, "cgth": 18, "cgph": 19, "cgr": 20, "cadv": 21,
 }
 
 
@@ -38,6 +39,7 @@ class OcConfig(ctypes.Structure):
         ("dt", ctypes.c_double), ("implicit_theta", ctypes.c_double),
         ("ab_mode", ctypes.c_int), ("bc_mode", ctypes.c_int), ("fd_mode", ctypes.c_int),
         ("precision", ctypes.c_int), ("magnetic", ctypes.c_int),
+        ("composition", ctypes.c_int), ("schmidt", ctypes.c_double),
     ]
 
 
@@ -81,7 +83,9 @@ def _load():
         lib.oc_get_grid_field.argtypes = [P, ctypes.c_int, D]
         lib.oc_get_grid_field.restype = ctypes.c_int
         lib.oc_set_temperature_bc.argtypes = [P, D, D]
-        for name in ("oc_temperature_nl", "oc_velocity_nl", "oc_magnetic_nl", "oc_implicit_step"):
+        lib.oc_set_composition_bc.argtypes = [P, D, D]
+        lib.oc_set_bc_types.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        for name in ("oc_temperature_nl", "oc_velocity_nl", "oc_magnetic_nl", "oc_implicit_step", "oc_composition_nl"):
             getattr(lib, name).argtypes = [P]
         lib.oc_step.argtypes = [P, ctypes.c_int]
         lib.oc_energy.argtypes = [P, D, D]
@@ -129,12 +133,12 @@ class Oracle:
 
     def __init__(self, lmax, nlat, nlon, nr, mmax=None, kl=4, rratio=0.35, ekman=3e-4,
                  rayleigh=80.0, prandtl=1.0, magnetic_prandtl=4.0, dt=1e-5, implicit_theta=0.5,
-                 ab_mode=0, bc_mode=0, fd_mode=0, magnetic=1, threads=None):
+                 ab_mode=0, bc_mode=0, fd_mode=0, magnetic=1, threads=None, composition=0, schmidt=1.0):
         self.lib = _load()
         mmax = lmax if mmax is None else mmax
         self.cfg = OcConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl,
                             magnetic_prandtl, dt, implicit_theta, ab_mode, bc_mode, fd_mode, 0,
-                            magnetic)
+                            magnetic, int(composition), float(schmidt))
         self.h = self.lib.oc_create(ctypes.byref(self.cfg))
         if not self.h:
             raise ValueError("oracle rejected the configuration")
@@ -240,6 +244,21 @@ class Oracle:
         self.lib.oc_set_temperature_bc(
             self.h, _ptr(_c(bvals)) if bvals is not None else None,
             _ptr(_c(sources)) if sources is not None else None)
+
+    def set_composition_bc(self, bvals=None, sources=None):
+        self.lib.oc_set_composition_bc(
+            self.h, _ptr(_c(bvals)) if bvals is not None else None,
+            _ptr(_c(sources)) if sources is not None else None)
+
+    def set_bc_types(self, name, inner, outer):
+        """bc_type_inner / bc_type_outer (1 fixed value, 2 flux) of "temp" or "comp", l-major."""
+        a = np.ascontiguousarray(inner, dtype=np.int32)
+        b = np.ascontiguousarray(outer, dtype=np.int32)
+        IP = ctypes.POINTER(ctypes.c_int)
+        self.lib.oc_set_bc_types(self.h, FIELD_IDS[name], a.ctypes.data_as(IP), b.ctypes.data_as(IP))
+
+    def composition_nl(self):
+        self.lib.oc_composition_nl(self.h)
 
     def temperature_nl(self):
         self.lib.oc_temperature_nl(self.h)

@@ -212,7 +212,8 @@ def distributed_step_fake(rank, world, port, magnetic):
         dist.destroy_process_group()
 
 
-def distributed_step_device(rank, world, port, precision, steps, magnetic, grid=(31, 48, 96, 12), nccl=False):
+def distributed_step_device(rank, world, port, precision, steps, magnetic, grid=(31, 48, 96, 12), nccl=False,
+                            composition=False):
     """DistributedStep on the device (every rank on cuda:0, gloo over pinned host
     buffers; nccl: one rank, NCCL over device buffers) against one whole handle,
     bit for bit; grid = (lmax, nlat, nlon, nr)."""
@@ -229,6 +230,8 @@ def distributed_step_device(rank, world, port, precision, steps, magnetic, grid=
         lmax, nlat, nlon, nr = grid
         phys = dict(workloads.SHELL_PHYSICS)
         cfg = dict(lmax=lmax, nlat=nlat, nlon=nlon, nr=nr, dt=1e-5, magnetic=magnetic, **phys)
+        if composition:
+            cfg.update(composition=1, schmidt=2.0)
         st = workloads.seeded_state(lmax, lmax, nr, seed=7, amp=1e-1)
         src = np.linspace(0.5, 1.5, nr)
         c = dict(cfg)
@@ -240,6 +243,18 @@ def distributed_step_device(rank, world, port, precision, steps, magnetic, grid=
             ds.set_field(n, *st[n])
         whole.set_temperature_bc(None, src)
         ds.set_temperature_bc(None, src)
+        if composition:
+            cst = workloads.seeded_state(lmax, lmax, nr, seed=8, amp=1e-1)["temp"]
+            names = tuple(names) + ("comp",)
+            whole.set_field("comp", *cst)
+            ds.set_field("comp", *cst)
+            csrc = np.linspace(-0.5, 0.5, nr)
+            whole.set_composition_bc(None, csrc)
+            ds.set_composition_bc(None, csrc)
+            # temperature flux boundaries on every third mode (tau method)
+            t = np.where(np.arange(whole.nlm) % 3 == 0, 2, 1)
+            whole.set_bc_types("temp", t, t[::-1].copy())
+            ds.set_bc_types("temp", t, t[::-1].copy())
         whole.step(steps)
         ds.step(steps)
         j0, j1 = ds.dec.modes[rank]
