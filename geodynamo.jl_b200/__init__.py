@@ -71,6 +71,7 @@ EXPORTS = (
     "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
     "gd_spectral_to_physical_noalloc",
     "gd_compute_temperature_nonlinear", "gd_compute_velocity_nonlinear", "gd_compute_magnetic_nonlinear",
+    "gd_compute_composition_nonlinear",
     "gd_create_timestepping_matrices", "gd_destroy_timestepping_matrices", "gd_build_rhs_cnab2",
     "gd_solve_implicit_step", "gd_set_fault_test",
     "gd_derivatives", "gd_implicit_modes", "gd_set_external_derivatives", "gd_copy_block",
@@ -166,6 +167,7 @@ def load_library():
         "gd_spectral_to_physical_noalloc": ([P, I, ctypes.c_void_p, ctypes.c_void_p], I),
         "gd_spectral_to_physical_adjoint": ([P, I, D, D, D], I),
         "gd_compute_temperature_nonlinear": ([P, D, D, D, D, D, D, D], I),
+        "gd_compute_composition_nonlinear": ([P, D, D, D, D, D, D, D], I),
         "gd_compute_velocity_nonlinear": ([P] + [D] * 14, I),
         "gd_compute_magnetic_nonlinear": ([P] + [D] * 14, I),
         "gd_create_timestepping_matrices": ([P, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -425,6 +427,16 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_compute_temperature_nonlinear(self.h, _dptr(tr), _dptr(ti), _dptr(_f64(u_theta)),
                                                               _dptr(_f64(u_phi)), _dptr(nre), _dptr(nim), _dptr(tg)))
         return (tr, ti), (nre, nim), tg
+
+    def compute_composition_nonlinear_arrays(self, c_re, c_im, u_theta, u_phi):
+        """compute_composition_nonlinear! (src/compositional.jl:219-259): returns the
+        composition with its boundary conditions applied, the nonlinear term and
+        the composition grid."""
+        cr, ci = _f64(c_re).copy(), _f64(c_im).copy()
+        nre = np.zeros(self.spec_shape()); nim = np.zeros(self.spec_shape()); cg = np.zeros(self.grid_shape())
+        self._check(self.lib.gd_compute_composition_nonlinear(self.h, _dptr(cr), _dptr(ci), _dptr(_f64(u_theta)),
+                                                              _dptr(_f64(u_phi)), _dptr(nre), _dptr(nim), _dptr(cg)))
+        return (cr, ci), (nre, nim), cg
 
     def compute_velocity_nonlinear_arrays(self, tor, pol, j_theta=None, j_phi=None, b_theta=None, b_phi=None):
         """compute_velocity_nonlinear! (src/velocity.jl:312-332): nonlinear terms

@@ -1243,6 +1243,22 @@ int gd_compute_temperature_nonlinear(gd_handle* h, double* t_re, double* t_im, c
   return s;
 }
 
+int gd_compute_composition_nonlinear(gd_handle* h, double* c_re, double* c_im, const double* u_theta,
+                                     const double* u_phi, double* nl_re, double* nl_im, double* c_grid) {
+  if (!h || !c_re || !c_im || !u_theta || !u_phi || !nl_re || !nl_im)
+    return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (!h->c.composition) return fail(h, GD_ERR_STATE, "the configuration has no composition");
+  int s = nl_prepare(h);
+  if (!s) s = put_spec(h, c_re, c_im, h->field(F_COMP));
+  if (!s) s = put_grid(h, u_theta, h->grid(GD_GRID_U_TH));
+  if (!s) s = put_grid(h, u_phi, h->grid(GD_GRID_U_PH));
+  if (!s) s = composition_nl_fp64(h);
+  if (!s) s = download_spec(h, h->nlf(F_COMP), nl_re, nl_im);
+  if (!s) s = download_spec(h, h->field(F_COMP), c_re, c_im);
+  if (!s && c_grid) s = get_grid(h, h->grid(GD_GRID_C), c_grid);
+  return s;
+}
+
 int gd_compute_velocity_nonlinear(gd_handle* h, const double* tor_re, const double* tor_im, const double* pol_re,
                                   const double* pol_im, const double* j_theta, const double* j_phi,
                                   const double* b_theta, const double* b_phi, double* nl_tor_re, double* nl_tor_im,

@@ -24,13 +24,14 @@ struct GDConfig
     rratio::Cdouble; ekman::Cdouble; rayleigh::Cdouble; prandtl::Cdouble; magnetic_prandtl::Cdouble
     dt::Cdouble; implicit_theta::Cdouble
     ab_mode::Cint; bc_mode::Cint; fd_mode::Cint; precision::Cint; magnetic::Cint
+    composition::Cint; schmidt::Cdouble
 end
 
 mutable struct Handle
     ptr::Ptr{Cvoid}
 end
 
-const FIELD = Dict(:u_tor => 0, :u_pol => 1, :b_tor => 2, :b_pol => 3, :temp => 4)
+const FIELD = Dict(:u_tor => 0, :u_pol => 1, :b_tor => 2, :b_pol => 3, :temp => 4, :comp => 5)
 
 lasterror(h::Handle) = unsafe_string(ccall((:gd_last_error, LIB), Cstring, (Ptr{Cvoid},), h.ptr))
 check(h::Handle, st::Cint) = st == 0 ? nothing : error("libgdb200 status $st: $(lasterror(h))")
@@ -48,12 +49,12 @@ end
 # parameters (src/parameters.jl:14-76) on first use.
 const HANDLES = Dict{Tuple{UInt,Int,Int},Handle}()
 
-function handle_for(GD, config, nr::Integer; precision::Integer = 0)
-    key = (objectid(config), Int(nr), Int(precision))
+function handle_for(GD, config, nr::Integer; precision::Integer = 0, composition::Bool = false)
+    key = (objectid(config), Int(nr), Int(precision) + 2 * Int(composition))
     get!(HANDLES, key) do
         cfg = GDConfig(config.lmax, config.mmax, config.nlat, config.nlon, nr, GD.i_KL,
                        GD.d_rratio, GD.d_E, GD.d_Ra, GD.d_Pr, GD.d_Pm, GD.d_timestep, GD.d_implicit,
-                       0, 0, 0, precision, GD.i_B)
+                       0, 0, 0, precision, GD.i_B, composition ? 1 : 0, composition ? GD.d_Sc : 1.0)
         create(cfg)
     end
 end
@@ -101,6 +102,7 @@ end
 # (gd_compute_temperature_nonlinear) fills temp.nonlinear, applies the boundary
 # rows to temp.spectral and writes the temperature grid.
 function temperature_nonlinear!(h::Handle, temp, vel)
+    scalar_bc_types!(h, FIELD[:temp], temp)
     bv = Matrix{Float64}(permutedims(temp.boundary_values))   # [nlm, 2] = C's [2][nlm]
     src = Vector{Float64}(temp.internal_sources)
     GC.@preserve bv src check(h, ccall((:gd_set_temperature_bc, LIB), Cint,
@@ -113,6 +115,33 @@ function temperature_nonlinear!(h::Handle, temp, vel)
         (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
         h.ptr, tr, ti, ut, up, nr, ni, tg))
     return temp
+end
+
+# bc_type_inner / bc_type_outer of a scalar field (1 fixed value, 2 flux) to the handle
+function scalar_bc_types!(h::Handle, field::Integer, f)
+    ti = Vector{Cint}(f.bc_type_inner); to = Vector{Cint}(f.bc_type_outer)
+    GC.@preserve ti to check(h, ccall((:gd_set_scalar_bc_types, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cint}, Ptr{Cint}), h.ptr, field, ti, to))
+end
+
+# compute_composition_nonlinear!(comp, vel, oc) (src/compositional.jl:219): the
+# boundary types, values (or fluxes) and sources of comp go to the handle, then
+# gd_compute_composition_nonlinear fills comp.nonlinear, applies the boundary
+# conditions to comp.spectral and writes the composition grid.
+function composition_nonlinear!(h::Handle, comp, vel)
+    scalar_bc_types!(h, FIELD[:comp], comp)
+    bv = Matrix{Float64}(permutedims(comp.boundary_values))
+    src = Vector{Float64}(comp.internal_sources)
+    GC.@preserve bv src check(h, ccall((:gd_set_composition_bc, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, bv, src))
+    cr = parent(comp.spectral.data_real); ci = parent(comp.spectral.data_imag)
+    ut = parent(vel.velocity.θ_component.data); up = parent(vel.velocity.φ_component.data)
+    nr = parent(comp.nonlinear.data_real); ni = parent(comp.nonlinear.data_imag)
+    cg = parent(comp.composition.data)
+    GC.@preserve cr ci ut up nr ni cg check(h, ccall((:gd_compute_composition_nonlinear, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+        h.ptr, cr, ci, ut, up, nr, ni, cg))
+    return comp
 end
 
 # compute_velocity_nonlinear!(fields, temp, comp, mag, domain) (src/velocity.jl:312):
@@ -298,6 +327,11 @@ function install!(GD::Module; precision::Integer = 0)
                                                 geometry::Symbol = get_parameters().geometry)
             h = $handle_for($GD, temp.spectral.config, size(parent(temp.spectral.data_real), 3))
             $temperature_nonlinear!(h, temp, vel)
+        end
+        function compute_composition_nonlinear!(comp::SHTnsCompositionField{Float64}, vel, oc::RadialDomain;
+                                                geometry::Symbol = get_parameters().geometry)
+            h = $handle_for($GD, comp.spectral.config, size(parent(comp.spectral.data_real), 3); composition = true)
+            $composition_nonlinear!(h, comp, vel)
         end
         function compute_velocity_nonlinear!(fields::SHTnsVelocityFields{Float64}, temp, comp, mag,
                                              oc::RadialDomain)

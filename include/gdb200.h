@@ -221,6 +221,13 @@ int gd_spectral_to_physical_noalloc(gd_handle* h, int nfield, const double* d_co
  * velocity grids it is advected by.  t_grid (may be NULL): the temperature grid. */
 int gd_compute_temperature_nonlinear(gd_handle* h, double* t_re, double* t_im, const double* u_theta,
                                      const double* u_phi, double* nl_re, double* nl_im, double* t_grid);
+/* compute_composition_nonlinear!(comp, vel, oc) (src/compositional.jl:219-259) on
+ * host arrays, as gd_compute_temperature_nonlinear: composition in (its
+ * boundary conditions of gd_set_composition_bc / gd_set_scalar_bc_types applied
+ * in place), the velocity grids it is advected by, the nonlinear term and the
+ * composition grid (may be NULL) out.  Needs a handle with composition. */
+int gd_compute_composition_nonlinear(gd_handle* h, double* c_re, double* c_im, const double* u_theta,
+                                     const double* u_phi, double* nl_re, double* nl_im, double* c_grid);
 /* compute_velocity_nonlinear!(fields, temp, comp, mag, domain) (src/velocity.jl:312-332):
  * the velocity (toroidal, poloidal), the grids j and B of the previous magnetic
  * phase (all four may be NULL only without a magnetic field) -> the nonlinear

@@ -120,3 +120,19 @@ def test_decomposed_step_with_composition_matches_one_handle():
     mp.start_processes(dist_workers.distributed_step_device,
                        args=(2, port, "fp64", 3, 1, (31, 48, 96, 12), False, True),
                        nprocs=2, start_method="spawn", join=True)
+
+
+def test_composition_host_array_entry_matches_oracle(gdb, oracle_mod):
+    # gd_compute_composition_nonlinear: the drop-in for compute_composition_nonlinear!
+    # on the caller's arrays (velocity grids from the caller, boundary data set before)
+    g, o = model_pair(gdb, oracle_mod, 15, 24, 48, 10, seed=11)
+    o.velocity_nl()
+    ut, up = o.get_grid("u_th"), o.get_grid("u_ph")
+    c = o.get_field("comp")
+    o.composition_nl()
+    (cr, ci), (nr_, ni_), cg = g.compute_composition_nonlinear_arrays(c[0], c[1], ut, up)
+    ore, oim = o.get_field("comp")
+    assert rel(cr, ore) < 1e-12 and rel(ci, oim) < 1e-12
+    onr, oni = o.get_nl("comp")
+    assert rel(nr_, onr) < 1e-12 and rel(ni_, oni) < 1e-12
+    assert rel(cg, o.get_grid("c")) < 1e-12
