@@ -397,3 +397,72 @@ class Oracle:
                    for li, ki, n_, s_ in zip(lin, k1, nn, ns)]
             self.set_field(name, *out)
         self._all_nonlinear()
+
+
+# ---------------------------------------------------------------------------
+# The reference's Krylov actions of the EAB2 path (eab2_update_krylov_cached!,
+# src/timestep.jl:358-427), restated in numpy for the tests that compare them
+# with the dense exponential operators.
+# ---------------------------------------------------------------------------
+def band_to_dense(band, kl):
+    """(2kl+1, n) band (row kl + i - j, column j) -> dense n x n."""
+    n = band.shape[1]
+    D = np.zeros((n, n))
+    for i in range(n):
+        for j in range(max(0, i - kl), min(n, i + kl + 1)):
+            D[i, j] = band[kl + i - j, j]
+    return D
+
+
+def exp_action_krylov(A, v, dt, m=20, tol=1e-8):
+    """exp_action_krylov (src/timestep.jl:108-225): Arnoldi with the residual
+    stopping rule |H[j+1, j] y_j[end]| <= tol |y_j| and the condition-number
+    guard; returns (y, Krylov dimension used)."""
+    import scipy.linalg as sla
+    n = len(v)
+    beta = float(np.linalg.norm(v))
+    if n == 0 or beta == 0.0:
+        return np.zeros(n), 0
+    V = np.zeros((n, m))
+    H = np.zeros((m, m))
+    V[:, 0] = v / beta
+    kmax = m
+    for j in range(m):
+        w = A @ V[:, j]
+        for i in range(j + 1):
+            H[i, j] = V[:, i] @ w
+            w = w - H[i, j] * V[:, i]
+        if j < m - 1:
+            H[j + 1, j] = np.linalg.norm(w)
+            if H[j + 1, j] < np.finfo(float).eps * 100:
+                kmax = j + 1
+                break
+            V[:, j + 1] = w / H[j + 1, j]
+            Hj = dt * H[:j + 1, :j + 1]
+            if j > 0 and np.linalg.cond(Hj) > 1e12:
+                kmax = j + 1
+                break
+            e1 = np.zeros(j + 1)
+            e1[0] = 1.0
+            y = sla.expm(Hj) @ (beta * e1)
+            if abs(H[j + 1, j]) * abs(y[-1]) <= tol * np.linalg.norm(y):
+                kmax = j + 1
+                break
+    e1 = np.zeros(kmax)
+    e1[0] = 1.0
+    return V[:, :kmax] @ (sla.expm(dt * H[:kmax, :kmax]) @ (beta * e1)), kmax
+
+
+def phi1_action_krylov(A, v, dt, m=20, tol=1e-8):
+    """phi1_action_krylov (src/timestep.jl:227-268): A^-1 (exp(dt A) v - v) / dt
+    with the non-pivoting banded LU of A (factorize_banded)."""
+    ev, _ = exp_action_krylov(A, v, dt, m, tol)
+    c = ev - v
+    n = len(v)
+    U = A.astype(float).copy()
+    Lf = np.eye(n)
+    for k in range(n - 1):
+        for i in range(k + 1, n):
+            Lf[i, k] = U[i, k] / U[k, k]
+            U[i, :] -= Lf[i, k] * U[k, :]
+    return np.linalg.solve(U, np.linalg.solve(Lf, c)) / dt

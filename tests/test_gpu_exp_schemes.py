@@ -166,3 +166,22 @@ def test_exponential_schemes_reject_unsupported_configurations(gdb):
         h.set_scheme("erk2")
     with pytest.raises(gdb.GeoDynamoError):
         h.etd_matrices("velocity", 0)      # no cache under CNAB2
+
+
+@pytest.mark.parametrize("nr,dt", [(33, 2e-6), (129, 2e-6)])
+def test_device_exponential_matches_reference_krylov_action(gdb, oracle_mod, nr, dt):
+    # the reference's EAB2 applies E to velocity and magnetic fields by a Krylov
+    # action (eab2_update_krylov_cached!, src/timestep.jl:358-427, m = 20,
+    # tol 1e-8): the device's dense E gives the same vectors within that tolerance
+    g = gdb.SHTnsKitConfig(7, 12, 24, nr, dt=dt)
+    g.set_scheme("eab2")
+    o = oracle_mod.Oracle(lmax=7, nlat=12, nlon=24, nr=nr, dt=dt)
+    for k, kind in enumerate(KINDS):
+        for l in (1, 5):
+            E = g.etd_matrices(kind, l)["E"]
+            lin, _ = o.implicit_matrices(k, l)
+            A = oracle_mod.band_to_dense(lin, o.kl)
+            v = np.random.default_rng(7 * k + l).standard_normal(nr)
+            y, _ = oracle_mod.exp_action_krylov(A, v, dt)
+            assert rel(E @ v, y) <= 1e-8, (kind, l, rel(E @ v, y))
+    g.close()
