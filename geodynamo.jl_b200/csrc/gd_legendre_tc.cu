@@ -174,20 +174,21 @@ void launch_build_tc_images(cudaStream_t s, const Dims& d, const int* moff, cons
 //    K -> l = m + p + 2 (32 kc + k).  One CTA per (kc, m, ct) covers both
 //    parities, so each warp reads l-contiguous runs of every coefficient row.
 // 2. k_tc_synth4: persistent CTAs over tiles (m, 128-row theta tile, column
-//    tile), 192 threads: warp 0 feeds the two pipeline stages with bulk copies
+//    tile), 320 threads: warp 0 feeds the two pipeline stages with bulk copies
 //    only (table chunk(s) and the coefficient chunk, transaction bytes on the
 //    stage's `full` barrier), warp 1 issues the split-TF32 MMAs (3 products
 //    per 8-deep K slice) and commits them to the stage's `empty` barrier and,
-//    after a tile's last step, to `tfull`; warps 2-5 (one per TMEM lane
-//    quarter) wait on `tfull`, read the accumulators, release them on
-//    `tempty` and write the blocked Fourier layout while the next tile's
-//    stages are already loading.  Scalar: accumulators [even | odd] x 256.
+//    after a tile's last step, to `tfull`; warps 2-9 (two per TMEM lane
+//    quarter, alternate 8-column chunks) wait on `tfull`, read the
+//    accumulators, release them on `tempty` and write the blocked Fourier
+//    layout while the next tile's stages are already loading.  Scalar: accumulators [even | odd] x 256.
 //    Vector: [P even | P odd | dP even | dP odd] x 128; the m/sin(theta) of
 //    the Q = m Pbar / sin(theta) terms is applied to the Pbar sums.  Rows past
 //    the last colatitude and columns past the last shell are neither copied
 //    nor (columns) multiplied: the MMA width follows the tile's valid columns.
 // ---------------------------------------------------------------------------
-constexpr int SY_THREADS = 192;
+constexpr int SY_THREADS = 320;  // producer, MMA issuer, 8 epilogue warps (two per TMEM lane quarter)
+constexpr int SY_EPI = SY_THREADS - 64;
 
 // step it -> (parity p, K chunk kc): odd-parity chunks interleave with the
 // even ones while both exist
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
       mbar_init(&empty[s], 1);
     }
     mbar_init(tfull, 1);
-    mbar_init(tempty, 128);
+    mbar_init(tempty, SY_EPI);
     mbar_init(drain, 1);
   }
   if (warp == 0) tmem_alloc(tslot, NCOL);
@@ -399,8 +400,9 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
       gs += T;
     }
   } else {
-    // epilogue warps 2-5: TMEM lane quarter warp & 3
-    const int qw = warp & 3;
+    // epilogue warps 2-9: TMEM lane quarter warp & 3; the two warps of a
+    // quarter take alternate 8-column chunks
+    const int qw = warp & 3, half = (warp - 2) >> 2;
     // scalar columns n = (f nr + r) 2 + re/im: the pair n / 2 = f nr + r indexes the (comp, r) run
     const size_t run = (size_t)a.nblk * (d.M + 1) * FOURIER_BLOCK;
     const uint32_t trow = tmem + ((uint32_t)(qw * 32) << 16);
@@ -418,8 +420,15 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
       const size_t ioff = ((size_t)(ith / FOURIER_BLOCK) * (d.M + 1) + m) * FOURIER_BLOCK + ith % FOURIER_BLOCK;
       const int nvalid = VEC ? 4 * min(32, d.nr - ct * 32) : min(NCS, Ntot - ct * NCS);
       const int cend = (nvalid + 7) & ~7;  // accumulator columns holding valid results
+      // this warp's last chunk: after its loads the warp releases the accumulators
+      const int nch = cend / 8, mine = nch > half ? (nch - 1 - half) / 2 + 1 : 0;
+      const int clast = mine > 0 ? 8 * (half + 2 * (mine - 1)) : -1;
+      if (clast < 0) {
+        fence_before_sync();
+        mbar_arrive(tempty);
+      }
       if (!VEC) {
-        for (int c0 = 0; c0 < cend; c0 += 8) {
+        for (int c0 = 8 * half; c0 < cend; c0 += 16) {
           float e[8], o[8];
           tmem_ld8(trow + c0, e);
           if (nc1 > 0) tmem_ld8(trow + NCS + c0, o);
@@ -428,7 +437,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
 #pragma unroll
             for (int j = 0; j < 8; ++j) o[j] = 0.f;
           }
-          if (c0 + 8 >= cend) {
+          if (c0 == clast) {
             fence_before_sync();
             mbar_arrive(tempty);  // accumulators read: the next tile's MMAs may start
           }
@@ -446,7 +455,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
         // columns (shell, component, re/im): 8 columns = 2 shells x [S re, S im, T re, T im]
         const int r0 = ct * 32;
         const float ms = (ith < d.nth) ? (float)((double)m * sinv[ith]) : 0.f;
-        for (int c0 = 0; c0 < cend; c0 += 8) {
+        for (int c0 = 8 * half; c0 < cend; c0 += 16) {
           float pe[8], po[8], de[8], dq[8];
           tmem_ld8(trow + 0 * TC_N2 + c0, pe);
           tmem_ld8(trow + 2 * TC_N2 + c0, de);
@@ -459,7 +468,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1) k_tc_synth4(Dims d, const int* 
 #pragma unroll
             for (int j = 0; j < 8; ++j) po[j] = dq[j] = 0.f;
           }
-          if (c0 + 8 >= cend) {
+          if (c0 == clast) {
             fence_before_sync();
             mbar_arrive(tempty);
           }
