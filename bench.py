@@ -889,7 +889,7 @@ def main():
                          f"nr={p['nr']}), 1 timed step after 1 warm-up on {cores} threads ({dts:.2f} s); the "
                          f"one-thread figure is in the reference arm's line"}
 
-    gpu_launches = sum(int(round(cnt / nprof)) for _, cnt in prof.values()) * args.steps
+    gpu_launches = g.step_kernels() * args.steps  # kernel nodes of the step graph x timed steps
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

@@ -75,7 +75,7 @@ EXPORTS = (
     "gd_create_timestepping_matrices", "gd_destroy_timestepping_matrices", "gd_build_rhs_cnab2",
     "gd_solve_implicit_step", "gd_set_fault_test",
     "gd_derivatives", "gd_implicit_modes", "gd_set_external_derivatives", "gd_copy_block",
-    "gd_set_launch_shape", "gd_get_launch_shape", "gd_ensemble_autotune",
+    "gd_set_launch_shape", "gd_get_launch_shape", "gd_ensemble_autotune", "gd_step_kernels",
     "gd_set_composition_bc", "gd_set_scalar_bc_types", "gd_composition_nonlinear",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
@@ -184,6 +184,7 @@ def load_library():
         "gd_set_scalar_bc_types": ([P, I, ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "gd_composition_nonlinear": ([P], I),
         "gd_get_launch_shape": ([P, ctypes.POINTER(I)], I),
+        "gd_step_kernels": ([P, ctypes.POINTER(I)], I),
         "gd_ensemble_autotune": ([P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
         "gd_copy_block": ([P, I, I, I, I, I, I, ctypes.c_void_p, I], I),
         "gd_magnetic_pullback": ([P, I, I, D, D, D, D], I),
@@ -339,6 +340,12 @@ class SHTnsKitConfig:
     def set_launch_shape(self, tc_ctas=0):
         """Cap of the tensor-core kernels' persistent grid (0: one CTA per SM)."""
         self._check(self.lib.gd_set_launch_shape(self.h, int(tc_ctas)))
+
+    def step_kernels(self):
+        """Kernel launches of the next step (kernel nodes of its CUDA graph)."""
+        n = ctypes.c_int()
+        self._check(self.lib.gd_step_kernels(self.h, ctypes.byref(n)))
+        return n.value
 
     def launch_shape(self):
         n = ctypes.c_int()

@@ -604,6 +604,20 @@ int ensure_graph(gd_handle* h, int boot) {
   cudaError_t e = cudaStreamEndCapture(h->stream, &g);
   if (s) { if (g) cudaGraphDestroy(g); return s; }
   if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  {
+    // kernel launches per step (gd_step_kernels): the graph's kernel nodes
+    size_t n = 0;
+    int k = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) == cudaSuccess && n > 0) {
+      std::vector<cudaGraphNode_t> nodes(n);
+      if (cudaGraphGetNodes(g, nodes.data(), &n) == cudaSuccess)
+        for (size_t i = 0; i < n; ++i) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+        }
+    }
+    h->graph_kernels[h->nl_par][boot] = k;
+  }
   e = cudaGraphInstantiate(&ge, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
@@ -724,6 +738,16 @@ int gd_set_external_derivatives(gd_handle* h, int enable) {
   CK(cudaSetDevice(h->device));
   if ((enable != 0) != h->ext_derivs) drop_graphs(h);
   h->ext_derivs = enable != 0;
+  return GD_OK;
+}
+
+int gd_step_kernels(gd_handle* h, int* count) {
+  if (!h || !count) return GD_ERR_ARG;
+  const int boot = (h->c.ab_mode == 1 || h->step_count == 0) ? 1 : 0;
+  CK(cudaSetDevice(h->device));
+  int s = ensure_graph(h, boot);
+  if (s) return s;
+  *count = h->graph_kernels[h->nl_par][boot];
   return GD_OK;
 }
 

@@ -67,6 +67,7 @@ struct gd_handle {
   // graphs (index: boot flag)
   cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [nl_par][boot]
   int graph_gen = 0;  // bumped whenever captured step graphs become stale
+  int graph_kernels[2][2] = {{0, 0}, {0, 0}};  // kernel nodes of each captured step graph
   // per-kernel event timing (gd_profile_enable)
   bool profiling = false;
   struct ProfRec { const char* name; cudaEvent_t a, b; };

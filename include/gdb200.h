@@ -418,6 +418,9 @@ int gd_copy_block(gd_handle* h, int array, int field, int r0, int r1, int j0, in
  * results do not depend on the cap.  gd_ensemble_autotune chooses the caps of
  * an ensemble's members by measurement. */
 int gd_set_launch_shape(gd_handle* h, int tc_ctas);
+/* Kernel launches of the next step: the kernel nodes of its captured CUDA
+ * graph (captured here if needed, without running it). */
+int gd_step_kernels(gd_handle* h, int* count);
 int gd_get_launch_shape(const gd_handle* h, int* tc_ctas);
 
 /* ---- error-path testing ----------------------------------------------------------

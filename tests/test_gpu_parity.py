@@ -251,3 +251,15 @@ def test_errors_are_status_codes(gdb):
     assert e.value.status == 4
     with pytest.raises(gdb.GeoDynamoError):
         g.set_dt(-1.0)
+
+
+def test_step_kernel_count_is_the_graph_node_count(gdb):
+    # gd_step_kernels: the kernel nodes of the captured step graph; the FP64
+    # step launches gradients, 4 + 1 + 2 syntheses with their phi transforms,
+    # the products, the analyses, the boundary rows and the CNAB2 solve
+    g = gdb.SHTnsKitConfig(15, 24, 48, 9)
+    n0 = g.step_kernels()
+    g.step(2)
+    n1 = g.step_kernels()
+    assert n0 == n1 and 15 <= n1 <= 40, (n0, n1)
+    g.close()
