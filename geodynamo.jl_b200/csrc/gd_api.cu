@@ -1,5 +1,6 @@
 // gd_api.cu -- the C ABI (include/gdb200.h): handle lifetime, device-resident
 // model state, the step sequence of step_once! and its CUDA-graph replay.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -243,6 +244,7 @@ int setup(gd_handle* h) {
     for (size_t q = 2 * NL; q < 4 * NL; ++q) bt[q] = GD_BC_FLUX;
     CK(cudaMemcpyAsync(h->d_bctype, bt.data(), sizeof(int) * bt.size(), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
+    h->bctype = bt;
   }
   {
     int st = build_tau(h);
@@ -806,6 +808,125 @@ int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int*
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaMemcpyAsync(h->d_bctype + (field == GD_COMP ? 2 * NL : 0), t.data(), sizeof(int) * 2 * NL,
                      cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  std::copy(t.begin(), t.end(), h->bctype.begin() + (field == GD_COMP ? 2 * NL : 0));
+  return GD_OK;
+}
+
+// ---- reverse mode of the temperature step -------------------------------------
+int gd_snapshot_bytes(gd_handle* h, size_t* bytes) {
+  if (!h || !bytes) return GD_ERR_ARG;
+  *bytes = 64 + sizeof(double) * (3 * NFIELD * h->spec_elems() + NGRID * h->grid_elems());
+  return GD_OK;
+}
+
+int gd_snapshot(gd_handle* h, void* dev, int restore) {
+  if (!h || !dev) return h ? fail(h, GD_ERR_ARG, "null buffer") : GD_ERR_ARG;
+  if (h->precision != GD_PREC_FP64)
+    return fail(h, GD_ERR_UNSUPPORTED, "snapshots hold the FP64 path's state (the mixed step keeps Fourier buffers)");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  const size_t se = NFIELD * h->spec_elems() * sizeof(double), ge = NGRID * h->grid_elems() * sizeof(double);
+  char* b = static_cast<char*>(dev);
+  long long hdr[3] = {h->nl_par, h->last_nl_par, h->step_count};
+  char* parts[4] = {b + 64, b + 64 + se, b + 64 + 2 * se, b + 64 + 3 * se};
+  void* mine[4] = {h->d_state, h->d_nl, h->d_prev, h->d_grid};
+  const size_t sz[4] = {se, se, se, ge};
+  if (!restore) {
+    CK(cudaMemcpyAsync(b, hdr, sizeof(hdr), cudaMemcpyHostToDevice, h->stream));
+    for (int i = 0; i < 4; ++i) CK(cudaMemcpyAsync(parts[i], mine[i], sz[i], cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  } else {
+    CK(cudaMemcpyAsync(hdr, b, sizeof(hdr), cudaMemcpyDeviceToHost, h->stream));
+    for (int i = 0; i < 4; ++i) CK(cudaMemcpyAsync(mine[i], parts[i], sz[i], cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->nl_par = (int)hdr[0];
+    h->last_nl_par = (int)hdr[1];
+    h->step_count = hdr[2];
+  }
+  return GD_OK;
+}
+
+int gd_spectral_device(gd_handle* h, double* re, double* im, double* dev, int to_device) {
+  if (!h || !re || !im || !dev) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  int s = stage_alloc(h);
+  if (s) return s;
+  const size_t plane = (size_t)h->d.nr * h->d.nlm;
+  if (to_device) {
+    CK(cudaMemcpyAsync(h->d_stage_spec, re, plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_stage_spec + plane, im, plane * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    launch_lmajor_to_native(h->stream, h->d, h->d_perm, h->d_stage_spec, dev, 2);
+  } else {
+    launch_native_to_lmajor(h->stream, h->d, h->d_perm, dev, h->d_stage_spec, 2);
+    CK(cudaMemcpyAsync(re, h->d_stage_spec, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(im, h->d_stage_spec + plane, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return check_launch(h, "spectral device copy");
+}
+
+int gd_grid_device(gd_handle* h, int grid, double* dev) {
+  if (!h || !dev || grid < 0 || grid >= NGRID) return h ? fail(h, GD_ERR_ARG, "bad grid or pointer") : GD_ERR_ARG;
+  if (h->precision != GD_PREC_FP64) return fail(h, GD_ERR_UNSUPPORTED, "device grids are the FP64 path's");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(dev, h->grid(grid), h->grid_elems() * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+
+int gd_temperature_nl_adjoint(gd_handle* h, const double* u_th, const double* u_ph, const double* nu, double* out) {
+  if (!h || !u_th || !u_ph || !nu || !out) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  const size_t se = h->spec_elems(), G = h->grid_elems();
+  if (!h->d_adj) AL(h->d_adj, 3 * se + 3 * G);
+  double* nup = h->d_adj;        // D nu
+  double* ath = nup + se;        // An(-u_th g), then D' scaled
+  double* aph = ath + se;
+  double* g = h->d_adj + 3 * se; // Syn(D nu)
+  double* hth = g + G;           // -u_th g, -u_ph g (consecutive for the two-field analysis)
+  const double tp = 2.0 * 3.14159265358979323846 / h->d.nlon;
+  // An^T = W Syn D with D = 2 pi / nlon (m = 0), pi / nlon (m > 0); Syn^T = D' An W^-1
+  // with D' = D^-1: the Gauss weights cancel between them
+  CK(cudaMemcpyAsync(nup, nu, se * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  launch_scale_by_order(h->stream, 2 * (size_t)h->d.nr, h->d.nlm, h->d_mof, tp, 0.5 * tp, nup);
+  const double* coef[1] = {nup};
+  int s = synth_scalar(h, coef, 1, g);
+  if (s) return s;
+  launch_neg_product(h->stream, G, u_th, g, hth);
+  launch_neg_product(h->stream, G, u_ph, g, hth + G);
+  double* outs[2] = {ath, aph};
+  s = analysis_scalar(h, hth, 2, outs);
+  if (s) return s;
+  launch_scale_by_order(h->stream, 4 * (size_t)h->d.nr, h->d.nlm, h->d_mof, 1.0 / tp, 2.0 / tp, ath);
+  launch_gradients_adjoint(h->stream, h->d, h->d_lof, h->d_mof, h->d_rinv, ath, aph, out);
+  s = check_launch(h, "temperature nonlinear adjoint");
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+
+int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double* y) {
+  if (!h || !x || !y || (mode != 0 && mode != 1) || field < 0 || field >= nfields(h))
+    return h ? fail(h, GD_ERR_ARG, "bad field, mode or pointer") : GD_ERR_ARG;
+  if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the adjoint is of the CNAB2 step");
+  const size_t NL = h->d.nlm;
+  const bool scalar = field == GD_TEMP || field == GD_COMP;
+  const int kind = field == GD_TEMP ? 2 : field == GD_COMP ? 3 : (field == GD_U_TOR || field == GD_U_POL) ? 0 : 1;
+  const int* types = nullptr;
+  if (scalar) {
+    const size_t o = field == GD_COMP ? 2 * NL : 0;
+    for (size_t q = 0; q < 2 * NL; ++q)
+      if (h->bctype[o + q] == GD_BC_FLUX)
+        return fail(h, GD_ERR_UNSUPPORTED, "the adjoint covers fixed-value boundaries (no tau flux rows)");
+    types = h->d_bctype + o;
+  }
+  if (!scalar && mode == 1) return fail(h, GD_ERR_UNSUPPORTED, "mode 1 (P R^T) is for the scalar fields");
+  CK(cudaSetDevice(h->device));
+  launch_cnab2_adjoint(h->stream, h->d, h->d_lof, h->d_lin, h->d_lu, types, kind, mode, h->c.dt, h->c.implicit_theta,
+                       h->c.bc_mode == 1, h->c.bc_mode == 2, x, y);
+  int s = check_launch(h, "cnab2 adjoint");
+  if (s) return s;
   CK(cudaStreamSynchronize(h->stream));
   return GD_OK;
 }

@@ -51,6 +51,8 @@ struct gd_handle {
   double *d_bvals = nullptr, *d_sources = nullptr;    // temperature: [2][nlm] values or fluxes, [nr]
   double *d_cbvals = nullptr, *d_csources = nullptr;  // composition
   int* d_bctype = nullptr;    // [temperature, composition][inner, outer][nlm] GD_BC_*
+  std::vector<int> bctype;    // host copy of d_bctype
+  double* d_adj = nullptr;    // adjoint scratch (lazy): 3 spectral fields, 3 grids
   double* d_tau = nullptr;    // tau1, tau2, tau_in, tau_out on the radial nodes
   gd::TauConsts tau{};
   double* d_grid = nullptr;   // NGRID grids (FP64)

@@ -191,6 +191,13 @@ void launch_cnab2_pullback(cudaStream_t s, const Dims& d, const int* lof, const 
                            int kind, double dt, double theta, int clamp_rows, int bc_rows, int nsteps, double* lam);
 void launch_divide_by_weights(cudaStream_t s, size_t n, int nlat, const double* w, double* g);
 void launch_scale_by_order(cudaStream_t s, size_t nrows, int nlm, const int* mof, double f0, double f1, double* a);
+// Temperature adjoint pieces (gd_adjoint.cu).
+void launch_cnab2_adjoint(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,
+                          const int* types, int kind, int mode, double dt, double theta, int clamp_rows, int bc_rows,
+                          const double* x, double* y);
+void launch_gradients_adjoint(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
+                              const double* gth, const double* gph, double* out);
+void launch_neg_product(cudaStream_t s, size_t n, const double* u, const double* g, double* out);
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
                   const double* rinv, const double* rinv2, const double* nu, const double* lu, const Cnab2Args& a);
 void launch_energy(cudaStream_t s, const Dims& d, const int* lof, const double* utor, const double* upol,

@@ -409,6 +409,40 @@ int gd_set_external_derivatives(gd_handle* h, int enable);
  * to_buf != 0 copies from the handle into buf.  Synchronises the stream. */
 int gd_copy_block(gd_handle* h, int array, int field, int r0, int r1, int j0, int j1, void* buf, int to_buf);
 
+/* ---- reverse mode of the temperature step ----------------------------------------
+ * No counterpart in the reference (it has no adjoint).  The temperature obeys
+ *   T^(n+1) = C S^-1 D (R P T^n + a_n N_n T^n - b_n N_(n-1) T^(n-1)) + const
+ * (compute_temperature_nonlinear!, build_rhs_cnab2!, solve_implicit_step!):
+ * P the fixed-value boundary rows, R = I/dt + (1 - theta) L_l, S = I/dt -
+ * theta L_l, C the bc_mode 1 row clamp, D the bc_mode 2 right-hand-side rows,
+ * a_n = 1.5 and b_n = 0.5 (1 and 0 on an Adams-Bashforth start), and
+ * N_n T = An(-(u_th Syn(G_th T) + u_ph Syn(G_ph T))) the advection by the
+ * velocity grids that step n's temperature phase reads (the velocity does not
+ * depend on the temperature: its buoyancy is radial and is not kept).  These
+ * entry points are the pieces of the pullback; the caller keeps the velocity
+ * grids of each step, recomputed from snapshots (checkpoint and recompute).
+ * Spectral arguments are device arrays in the native layout [Re, Im][nr][nlm]
+ * (gd_spectral_device converts), grids device arrays in the native grid
+ * layout [nr][nlat][nlon] (gd_grid_device copies the handle's).
+ *
+ * Snapshot of the step state (fields, both banks of nonlinear terms, the
+ * grids, the bank parity and step count) into or out of a device buffer of
+ * gd_snapshot_bytes bytes; FP64 handles. */
+int gd_snapshot_bytes(gd_handle* h, size_t* bytes);
+int gd_snapshot(gd_handle* h, void* dev, int restore);
+/* Host reference-layout (l-major) Re/Im planes <-> a native device array. */
+int gd_spectral_device(gd_handle* h, double* re, double* im, double* dev, int to_device);
+/* Copy of one of the handle's grids (FP64 handles) into a device buffer. */
+int gd_grid_device(gd_handle* h, int grid, double* dev);
+/* out = N^T nu for the advection by the velocity grids u_th, u_ph: the
+ * transposed analysis, the products, the transposed synthesis and the
+ * transposed spectral gradient (theta recurrence and i m, over r), FP64. */
+int gd_temperature_nl_adjoint(gd_handle* h, const double* u_th, const double* u_ph, const double* nu, double* out);
+/* mode 0: y = D S^-T C x; mode 1: y = P R^T x (scalar fields: P zeroes the
+ * fixed-value boundary rows), with the field's implicit operators.  Fixed-value
+ * boundaries only: GD_ERR_UNSUPPORTED when the field has flux boundaries. */
+int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double* y);
+
 /* ---- launch shape -------------------------------------------------------------------
  * No counterpart in the reference.  tc_ctas caps the persistent grid of the
  * tensor-core Legendre kernels (0, the default: one CTA per SM).  Each of those
