@@ -519,6 +519,66 @@ def run_adjoint(args, gdb, workloads, torch):
         ad = dot((gre, gim), v)
         fm_err.append(abs(fwd - ad) / abs(ad))
     probe.close()
+
+    # temperature objective: J_T = 1/2 |T(r_mid) - target|^2 after the same 200
+    # steps, gradient with respect to the initial temperature by checkpoint and
+    # recompute (temperature_misfit), from the seeded temperature of config 0.
+    # With the literal operator (bc_mode 0) a nonzero temperature grows by ~1e15
+    # in 10 steps at this grid (the configuration's state has none), so this leg
+    # uses the Dirichlet rows of bc_mode 2.
+    t0s = workloads.seeded_state(c["lmax"], c["lmax"], c["nr"], seed=0)["temp"]
+    mid = c["nr"] // 2
+    tbc = 2
+
+    def make_t(t0):
+        mm = gdb.SHTnsKitConfig(c["lmax"], c["nlat"], c["nlon"], c["nr"], dt=c["dt"], bc_mode=tbc)
+        for k, (a, b) in state.items():
+            mm.set_field(k, a, b)
+        mm.set_field("temp", *t0)
+        return mm
+
+    mt = make_t(t0s)
+    tgt = np.cos(np.arange(mt.nlon * mt.nlat).reshape(mt.nlon, mt.nlat) * 0.11) * 1e-3
+    gdb.temperature_misfit(mt, tgt, c["steps"], c["checkpoint"], shell=mid)  # warm-up (graphs, scratch)
+    mt.close()
+    mt = make_t(t0s)
+    t2 = time.perf_counter()
+    JT, tgre, tgim = gdb.temperature_misfit(mt, tgt, c["steps"], c["checkpoint"], shell=mid)
+    t_temp = time.perf_counter() - t2
+    mt.close()
+
+    def misfit_t(t0):
+        mm = make_t(t0)
+        mm.step(c["steps"])
+        r = mm.synth_scalar(*mm.get_field("temp"))[mid] - tgt
+        mm.close()
+        return 0.5 * float(np.sum(r * r))
+
+    tdirs = workloads.adjoint_directions(c["lmax"], c["lmax"], c["nr"], count=8, seed=3)
+    tfd = []
+    for v in tdirs:
+        eps = 1e-3 * np.sqrt(dot(t0s, t0s) / dot(v, v))
+        fd = (misfit_t((t0s[0] + eps * v[0], t0s[1] + eps * v[1])) -
+              misfit_t((t0s[0] - eps * v[0], t0s[1] - eps * v[1]))) / (2 * eps)
+        tfd.append(abs(fd - dot((tgre, tgim), v)) / abs(fd))
+    o = Oracle(lmax=c["lmax"], nlat=c["nlat"], nlon=c["nlon"], nr=c["nr"], dt=c["dt"], bc_mode=tbc)
+    for k, (a, b) in state.items():
+        o.set_field(k, a, b)
+    o.set_field("temp", *t0s)
+    o.step(c["steps"])
+    tresid = o.synth_scalar(*o.get_field("temp"))[mid] - tgt
+    o = Oracle(lmax=c["lmax"], nlat=c["nlat"], nlon=c["nlon"], nr=c["nr"], dt=c["dt"], bc_mode=tbc)
+    for k, (a, b) in state.items():
+        o.set_field(k, a, b)
+    o.set_field("temp", *tdirs[0])  # the tangent: zero sources and boundary values
+    o.step(c["steps"])
+    tfm = float(np.sum(tresid * o.synth_scalar(*o.get_field("temp"))[mid]))
+    temperature = {"objective": "1/2 |T(r_mid) - target|^2 after the steps, w.r.t. the initial temperature",
+                   "bc_mode": tbc,
+                   "J": JT, "fd_rel_err_max": max(tfd), "fd_directions": len(tfd),
+                   "oracle_forward_mode_rel_err": abs(tfm - dot((tgre, tgim), tdirs[0])) / abs(tfm),
+                   "misfit_and_gradient_s_wall": t_temp,
+                   "reverse": "velocity grids recomputed per 20-step segment from device snapshots"}
     line = {"metric": "adjoint gradient vs FP64 finite differences (max relative error, 32 directions)",
             "value": max(fd_err), "unit": "relative error", "higher_is_better": False, "n_gpus": 1,
             "dtype": "f64", "data": "synthetic (adjoint_state(0): seeded_state(0) with zero temperature; adjoint_target(seed=1); directions default_rng(2))",
@@ -527,7 +587,8 @@ def run_adjoint(args, gdb, workloads, torch):
                        "checkpoint_every": c["checkpoint"]},
             "J": J, "fd_rel_err_max": max(fd_err), "fd_rel_err_median": float(np.median(fd_err)),
             "oracle_forward_mode_rel_err_max": max(fm_err), "forward_ms_device": fwd_ms,
-            "pullback_ms_wall": pull_ms, "misfit_and_gradient_s_wall": t_total, "checkpoints": len(ckpt)}
+            "pullback_ms_wall": pull_ms, "misfit_and_gradient_s_wall": t_total, "checkpoints": len(ckpt),
+            "temperature": temperature}
     print(json.dumps(line), flush=True)
     return 0
 
