@@ -77,7 +77,7 @@ EXPORTS = (
     "gd_derivatives", "gd_implicit_modes", "gd_set_external_derivatives", "gd_copy_block",
     "gd_set_launch_shape", "gd_get_launch_shape", "gd_ensemble_autotune", "gd_step_kernels",
     "gd_snapshot_bytes", "gd_snapshot", "gd_spectral_device", "gd_grid_device", "gd_temperature_nl_adjoint",
-    "gd_cnab2_adjoint",
+    "gd_cnab2_adjoint", "gd_temperature_forward", "gd_temperature_pullback",
     "gd_set_composition_bc", "gd_set_scalar_bc_types", "gd_composition_nonlinear",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
@@ -193,6 +193,8 @@ def load_library():
         "gd_grid_device": ([P, I, P], I),
         "gd_temperature_nl_adjoint": ([P, P, P, P, P], I),
         "gd_cnab2_adjoint": ([P, I, I, P, P], I),
+        "gd_temperature_forward": ([P, I, I], I),
+        "gd_temperature_pullback": ([P, D, D, D, D], I),
         "gd_ensemble_autotune": ([P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
         "gd_copy_block": ([P, I, I, I, I, I, I, ctypes.c_void_p, I], I),
         "gd_magnetic_pullback": ([P, I, I, D, D, D, D], I),
@@ -449,6 +451,17 @@ class SHTnsKitConfig:
         """mode 0: y = D S^-T C x; mode 1: y = P R^T x (gd_cnab2_adjoint)."""
         self._check(self.lib.gd_cnab2_adjoint(self.h, FIELDS[name], int(mode), ctypes.c_void_p(x.data_ptr()),
                                               ctypes.c_void_p(y.data_ptr())))
+
+    def temperature_forward(self, nsteps, checkpoint_every=20):
+        """nsteps steps with a device snapshot every checkpoint_every (gd_temperature_forward)."""
+        self._check(self.lib.gd_temperature_forward(self.h, int(nsteps), int(checkpoint_every)))
+
+    def temperature_pullback(self, lam_re, lam_im):
+        """Cotangent of the temperature after the checkpointed run -> at its start."""
+        re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
+        self._check(self.lib.gd_temperature_pullback(self.h, _dptr(_f64(lam_re)), _dptr(_f64(lam_im)),
+                                                     _dptr(re), _dptr(im)))
+        return re, im
 
     def magnetic_pullback(self, name, nsteps, lam_re, lam_im):
         """Pullback of nsteps steps w.r.t. the magnetic component ``name``
@@ -731,33 +744,11 @@ def temperature_misfit(model, target, nsteps, checkpoint_every=20, shell=None):
     (nlon, nlat) grid of shell ``shell``, default the middle one) and the
     gradient of J with respect to the initial temperature coefficients (nr x
     nlm Re and Im planes, l-major).  The model is left in its state after the
-    steps.
-
-    Forward: a device snapshot (gd_snapshot) every ``checkpoint_every`` steps.
-    Reverse, segment by segment from the last: restore the segment's snapshot,
-    step through it again to record the velocity grids that each step's
-    temperature phase read (the velocity does not depend on the temperature, so
-    they are the forward run's), then for n from the segment's last step down
-    with psi^n = D S^-T C lambda^n (gd_cnab2_adjoint mode 0):
-      lambda^n = P R^T psi^(n+1) + N_n^T (a_n psi^(n+1) - b_(n+1) psi^(n+2))
-    (mode 1 and gd_temperature_nl_adjoint), a = 1.5 and b = 0.5 except on an
-    Adams-Bashforth start (1 and 0)."""
-    import torch
-    dev = torch.device("cuda", model.device)
-    K, C = int(nsteps), int(checkpoint_every or nsteps)
-    nseg = (K + C - 1) // C
-    nb = model.snapshot_bytes()
-    snaps = [torch.empty(nb, dtype=torch.uint8, device=dev) for _ in range(nseg)]
-    final = torch.empty(nb, dtype=torch.uint8, device=dev)
-    s0 = model.step_count()
-    ab1 = model.cfg.ab_mode == 1
-    done = 0
-    for k in range(nseg):
-        model.snapshot(snaps[k])
-        n = min(C, K - done)
-        model.step(n)
-        done += n
-    model.snapshot(final)
+    steps.  Forward: gd_temperature_forward (a device snapshot every
+    ``checkpoint_every`` steps); reverse: the residual through the transposed
+    synthesis, then gd_temperature_pullback (the velocity grids recomputed
+    segment by segment from the snapshots)."""
+    model.temperature_forward(nsteps, checkpoint_every)
     shell = model.nr // 2 if shell is None else int(shell)
     tre, tim = model.get_field("temp")
     grid = model.synth_scalar(tre, tim)
@@ -766,46 +757,7 @@ def temperature_misfit(model, target, nsteps, checkpoint_every=20, shell=None):
     gbar = np.zeros(model.grid_shape())
     gbar[shell] = resid
     lre, lim = model.synth_scalar_adjoint(gbar)
-    size = 2 * model.nr * model.nlm
-    G = model.nr * model.nlat * model.nlon
-    f64 = dict(dtype=torch.float64, device=dev)
-    lam = torch.empty(size, **f64)
-    model.spectral_to_device(lre, lim, lam)
-    psi1 = torch.empty(size, **f64)    # psi^(n+1)
-    model.cnab2_adjoint("temp", 0, lam, psi1)
-    psi2 = torch.zeros(size, **f64)    # psi^(n+2)
-    tmp = torch.empty(size, **f64)
-    nlt = torch.empty(size, **f64)
-
-    def boot(n):
-        return ab1 or s0 + n == 0
-
-    for k in reversed(range(nseg)):
-        c0, c1 = k * C, min(K, k * C + C)
-        model.restore(snaps[k])
-        ust = []
-        for n in range(c0, c1):
-            u = torch.empty(2 * G, **f64)
-            model.grid_to_device("u_th", u[:G])
-            model.grid_to_device("u_ph", u[G:])
-            ust.append(u)
-            if n < c1 - 1:
-                model.step(1)
-        for n in reversed(range(c0, c1)):
-            a_n = 1.0 if boot(n) else 1.5
-            b_n1 = 0.0 if (n + 1 >= K or boot(n + 1)) else 0.5
-            torch.mul(psi1, a_n, out=tmp)
-            if b_n1:
-                tmp.sub_(psi2, alpha=b_n1)
-            u = ust[n - c0]
-            model.temperature_nl_adjoint(u[:G], u[G:], tmp, nlt)
-            model.cnab2_adjoint("temp", 1, psi1, lam)
-            lam.add_(nlt)
-            if n > 0:
-                psi2, psi1 = psi1, psi2
-                model.cnab2_adjoint("temp", 0, lam, psi1)
-    model.restore(final)
-    gre, gim = model.spectral_from_device(lam)
+    gre, gim = model.temperature_pullback(lre, lim)
     return J, gre, gim
 
 

@@ -271,4 +271,14 @@ void launch_neg_product(cudaStream_t s, size_t n, const double* u, const double*
   k_neg_product<<<592, 256, 0, s>>>(n, u, g, out);
 }
 
+// out = a x + b y (out may alias x or y)
+__global__ void k_axpby(size_t n, double a, const double* x, double b, const double* y, double* out) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = a * x[e] + b * y[e];
+}
+
+void launch_axpby(cudaStream_t s, size_t n, double a, const double* x, double b, const double* y, double* out) {
+  k_axpby<<<592, 256, 0, s>>>(n, a, x, b, y, out);
+}
+
 }  // namespace gd

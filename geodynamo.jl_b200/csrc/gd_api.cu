@@ -688,6 +688,8 @@ int gd_destroy(gd_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   if (h->mixed) mixed_destroy(h);
+  for (void* p : h->t_snaps) cudaFree(p);
+  if (h->t_final) cudaFree(h->t_final);
   for (void* p : h->allocs) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -753,6 +755,96 @@ int gd_step_kernels(gd_handle* h, int* count) {
   return GD_OK;
 }
 
+// Checkpointed forward run and the temperature pullback that recomputes the
+// velocity grids from its snapshots (the orchestration of the pieces above).
+static void free_tckpt(gd_handle* h) {
+  for (void* p : h->t_snaps) cudaFree(p);
+  h->t_snaps.clear();
+  if (h->t_final) cudaFree(h->t_final);
+  h->t_final = nullptr;
+  h->t_nsteps = 0;
+}
+
+int gd_temperature_forward(gd_handle* h, int nsteps, int checkpoint_every) {
+  if (!h || nsteps < 1 || checkpoint_every < 1) return h ? fail(h, GD_ERR_ARG, "need nsteps, checkpoint_every >= 1") : GD_ERR_ARG;
+  if (h->precision != GD_PREC_FP64 || h->scheme != GD_SCHEME_CNAB2)
+    return fail(h, GD_ERR_UNSUPPORTED, "the temperature pullback is of the FP64 CNAB2 step");
+  CK(cudaSetDevice(h->device));
+  free_tckpt(h);
+  size_t nb = 0;
+  gd_snapshot_bytes(h, &nb);
+  const int nseg = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  h->t_s0 = h->step_count;
+  for (int k = 0; k < nseg; ++k) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, nb) != cudaSuccess) { free_tckpt(h); return fail(h, GD_ERR_CUDA, "out of device memory for snapshots"); }
+    h->t_snaps.push_back(p);
+    int s = gd_snapshot(h, p, 0);
+    if (s == GD_OK) s = gd_step(h, std::min(checkpoint_every, nsteps - k * checkpoint_every));
+    if (s) { free_tckpt(h); return s; }
+  }
+  if (cudaMalloc(&h->t_final, nb) != cudaSuccess) { free_tckpt(h); return fail(h, GD_ERR_CUDA, "out of device memory"); }
+  int s = gd_snapshot(h, h->t_final, 0);
+  if (s) { free_tckpt(h); return s; }
+  h->t_nsteps = nsteps;
+  h->t_every = checkpoint_every;
+  return GD_OK;
+}
+
+int gd_temperature_pullback(gd_handle* h, const double* lam_re, const double* lam_im, double* out_re, double* out_im) {
+  if (!h || !lam_re || !lam_im || !out_re || !out_im) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (h->t_nsteps < 1) return fail(h, GD_ERR_STATE, "no checkpointed forward run (gd_temperature_forward)");
+  CK(cudaSetDevice(h->device));
+  const size_t se = h->spec_elems(), G = h->grid_elems();
+  const int K = h->t_nsteps, C = h->t_every, nseg = (K + C - 1) / C;
+  const bool ab1 = h->c.ab_mode == 1;
+  auto boot = [&](int n) { return ab1 || h->t_s0 + n == 0; };
+  // lam, psi1, psi2, tmp, nlt share one allocation; ust holds a segment's velocity grids
+  double *lam = nullptr, *ust = nullptr;
+  if (cudaMalloc(&lam, 5 * se * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&ust, (size_t)C * 2 * G * sizeof(double)) != cudaSuccess) {
+    if (lam) cudaFree(lam);
+    return fail(h, GD_ERR_CUDA, "out of device memory for the pullback");
+  }
+  double *psi1 = lam + se, *psi2 = psi1 + se, *tmp = psi2 + se, *nlt = tmp + se;
+  auto done = [&](int st) {
+    cudaFree(lam);
+    cudaFree(ust);
+    return st;
+  };
+  int s = gd_spectral_device(h, const_cast<double*>(lam_re), const_cast<double*>(lam_im), lam, 1);
+  if (s) return done(s);
+  s = gd_cnab2_adjoint(h, GD_TEMP, 0, lam, psi1);
+  if (s) return done(s);
+  CK(cudaMemsetAsync(psi2, 0, se * sizeof(double), h->stream));
+  for (int k = nseg - 1; k >= 0 && s == GD_OK; --k) {
+    const int c0 = k * C, c1 = std::min(K, c0 + C);
+    s = gd_snapshot(h, h->t_snaps[k], 1);
+    for (int n = c0; n < c1 && s == GD_OK; ++n) {
+      double* u = ust + (size_t)(n - c0) * 2 * G;
+      s = gd_grid_device(h, GD_GRID_U_TH, u);
+      if (s == GD_OK) s = gd_grid_device(h, GD_GRID_U_PH, u + G);
+      if (s == GD_OK && n < c1 - 1) s = gd_step(h, 1);
+    }
+    for (int n = c1 - 1; n >= c0 && s == GD_OK; --n) {
+      const double a_n = boot(n) ? 1.0 : 1.5;
+      const double b_n1 = (n + 1 >= K || boot(n + 1)) ? 0.0 : 0.5;
+      launch_axpby(h->stream, se, a_n, psi1, -b_n1, psi2, tmp);
+      const double* u = ust + (size_t)(n - c0) * 2 * G;
+      s = gd_temperature_nl_adjoint(h, u, u + G, tmp, nlt);
+      if (s == GD_OK) s = gd_cnab2_adjoint(h, GD_TEMP, 1, psi1, lam);
+      if (s == GD_OK) launch_axpby(h->stream, se, 1.0, lam, 1.0, nlt, lam);
+      if (s == GD_OK && n > 0) {
+        std::swap(psi1, psi2);
+        s = gd_cnab2_adjoint(h, GD_TEMP, 0, lam, psi1);
+      }
+    }
+  }
+  if (s == GD_OK) s = gd_snapshot(h, h->t_final, 1);
+  if (s == GD_OK) s = gd_spectral_device(h, out_re, out_im, lam, 0);
+  return done(s);
+}
+
 int gd_set_launch_shape(gd_handle* h, int tc_ctas) {
   if (!h || tc_ctas < 0) return h ? fail(h, GD_ERR_ARG, "tc_ctas must be >= 0") : GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
@@ -814,9 +906,14 @@ int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int*
 }
 
 // ---- reverse mode of the temperature step -------------------------------------
+// Grids a step reads before writing them: the velocity grids (temperature
+// phase), the magnetic field and current grids (the velocity phase's Lorentz
+// term).  A snapshot holds these and the spectral state.
+static const int kCarried[6] = {GD_GRID_U_TH, GD_GRID_U_PH, GD_GRID_B_TH, GD_GRID_B_PH, GD_GRID_J_TH, GD_GRID_J_PH};
+
 int gd_snapshot_bytes(gd_handle* h, size_t* bytes) {
   if (!h || !bytes) return GD_ERR_ARG;
-  *bytes = 64 + sizeof(double) * (3 * NFIELD * h->spec_elems() + NGRID * h->grid_elems());
+  *bytes = 64 + sizeof(double) * (3 * NFIELD * h->spec_elems() + 6 * h->grid_elems());
   return GD_OK;
 }
 
@@ -826,19 +923,23 @@ int gd_snapshot(gd_handle* h, void* dev, int restore) {
     return fail(h, GD_ERR_UNSUPPORTED, "snapshots hold the FP64 path's state (the mixed step keeps Fourier buffers)");
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
-  const size_t se = NFIELD * h->spec_elems() * sizeof(double), ge = NGRID * h->grid_elems() * sizeof(double);
+  const size_t se = NFIELD * h->spec_elems() * sizeof(double), gb = h->grid_elems() * sizeof(double);
   char* b = static_cast<char*>(dev);
   long long hdr[3] = {h->nl_par, h->last_nl_par, h->step_count};
-  char* parts[4] = {b + 64, b + 64 + se, b + 64 + 2 * se, b + 64 + 3 * se};
-  void* mine[4] = {h->d_state, h->d_nl, h->d_prev, h->d_grid};
-  const size_t sz[4] = {se, se, se, ge};
+  const cudaMemcpyKind dd = cudaMemcpyDeviceToDevice;
   if (!restore) {
     CK(cudaMemcpyAsync(b, hdr, sizeof(hdr), cudaMemcpyHostToDevice, h->stream));
-    for (int i = 0; i < 4; ++i) CK(cudaMemcpyAsync(parts[i], mine[i], sz[i], cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(b + 64, h->d_state, se, dd, h->stream));
+    CK(cudaMemcpyAsync(b + 64 + se, h->d_nl, se, dd, h->stream));
+    CK(cudaMemcpyAsync(b + 64 + 2 * se, h->d_prev, se, dd, h->stream));
+    for (int g = 0; g < 6; ++g) CK(cudaMemcpyAsync(b + 64 + 3 * se + g * gb, h->grid(kCarried[g]), gb, dd, h->stream));
     CK(cudaStreamSynchronize(h->stream));
   } else {
     CK(cudaMemcpyAsync(hdr, b, sizeof(hdr), cudaMemcpyDeviceToHost, h->stream));
-    for (int i = 0; i < 4; ++i) CK(cudaMemcpyAsync(mine[i], parts[i], sz[i], cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_state, b + 64, se, dd, h->stream));
+    CK(cudaMemcpyAsync(h->d_nl, b + 64 + se, se, dd, h->stream));
+    CK(cudaMemcpyAsync(h->d_prev, b + 64 + 2 * se, se, dd, h->stream));
+    for (int g = 0; g < 6; ++g) CK(cudaMemcpyAsync(h->grid(kCarried[g]), b + 64 + 3 * se + g * gb, gb, dd, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->nl_par = (int)hdr[0];
     h->last_nl_par = (int)hdr[1];

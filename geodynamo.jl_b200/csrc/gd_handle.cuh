@@ -53,6 +53,11 @@ struct gd_handle {
   int* d_bctype = nullptr;    // [temperature, composition][inner, outer][nlm] GD_BC_*
   std::vector<int> bctype;    // host copy of d_bctype
   double* d_adj = nullptr;    // adjoint scratch (lazy): 3 spectral fields, 3 grids
+  // checkpointed forward run of gd_temperature_forward
+  std::vector<void*> t_snaps;
+  void* t_final = nullptr;
+  int t_nsteps = 0, t_every = 0;
+  long t_s0 = 0;
   double* d_tau = nullptr;    // tau1, tau2, tau_in, tau_out on the radial nodes
   gd::TauConsts tau{};
   double* d_grid = nullptr;   // NGRID grids (FP64)

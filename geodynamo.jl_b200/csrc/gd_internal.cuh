@@ -198,6 +198,7 @@ void launch_cnab2_adjoint(cudaStream_t s, const Dims& d, const int* lof, const d
 void launch_gradients_adjoint(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                               const double* gth, const double* gph, double* out);
 void launch_neg_product(cudaStream_t s, size_t n, const double* u, const double* g, double* out);
+void launch_axpby(cudaStream_t s, size_t n, double a, const double* x, double b, const double* y, double* out);
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
                   const double* rinv, const double* rinv2, const double* nu, const double* lu, const Cnab2Args& a);
 void launch_energy(cudaStream_t s, const Dims& d, const int* lof, const double* utor, const double* upol,

@@ -1,4 +1,4 @@
-# Reverse-mode rule of GeoDynamoB200.evolve_magnetic, loaded when
+# Reverse-mode rules of GeoDynamoB200.evolve_magnetic and evolve_temperature, loaded when
 # ChainRulesCore is: the pullback of nsteps model steps with respect to the
 # magnetic component they start from is the library's hand-written transposed
 # propagator (gd_magnetic_pullback: per step the transposed band solve and the
@@ -21,6 +21,22 @@ function ChainRulesCore.rrule(::typeof(GeoDynamoB200.evolve_magnetic), h::GeoDyn
         return NoTangent(), NoTangent(), gre, gim, NoTangent()
     end
     return out, evolve_magnetic_pullback
+end
+
+# evolve_temperature: the pullback of the checkpointed run, the velocity grids of
+# each segment recomputed from its snapshot (gd_temperature_pullback).
+function ChainRulesCore.rrule(::typeof(GeoDynamoB200.evolve_temperature), h::GeoDynamoB200.Handle,
+                              re::AbstractArray{Float64}, im::AbstractArray{Float64}, nsteps::Integer;
+                              checkpoint_every::Integer = 20)
+    out = GeoDynamoB200.evolve_temperature(h, re, im, nsteps; checkpoint_every = checkpoint_every)
+    function evolve_temperature_pullback(Δ)
+        d = unthunk(Δ)
+        dre = d[1] isa AbstractZero ? zeros(size(re)) : Array{Float64}(unthunk(d[1]))
+        dim = d[2] isa AbstractZero ? zeros(size(im)) : Array{Float64}(unthunk(d[2]))
+        gre, gim = GeoDynamoB200.temperature_pullback(h, dre, dim)
+        return NoTangent(), NoTangent(), gre, gim, NoTangent()
+    end
+    return out, evolve_temperature_pullback
 end
 
 end # module

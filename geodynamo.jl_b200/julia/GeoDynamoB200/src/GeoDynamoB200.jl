@@ -281,6 +281,30 @@ function magnetic_pullback(h::Handle, f::Symbol, nsteps::Integer, lre::AbstractA
     return gre, gim
 end
 
+# evolve_temperature(h, re, im, nsteps; checkpoint_every = 20) sets the
+# temperature of h's state, runs nsteps model steps keeping a device snapshot
+# every checkpoint_every steps (gd_temperature_forward) and returns the
+# temperature afterwards; its rrule (the extension) pulls the cotangent back
+# with gd_temperature_pullback, which recomputes the velocity grids of each
+# segment from its snapshot (checkpoint and recompute).  FP64 handles, CNAB2.
+function evolve_temperature(h::Handle, re::AbstractArray{Float64}, im::AbstractArray{Float64}, nsteps::Integer;
+                            checkpoint_every::Integer = 20)
+    r = Array{Float64}(re); i = Array{Float64}(im)
+    GC.@preserve r i check(h, ccall((:gd_upload_spectral, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, FIELD[:temp], r, i))
+    check(h, ccall((:gd_temperature_forward, LIB), Cint, (Ptr{Cvoid}, Cint, Cint), h.ptr, nsteps, checkpoint_every))
+    GC.@preserve r i check(h, ccall((:gd_download_spectral, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, FIELD[:temp], r, i))
+    return r, i
+end
+
+function temperature_pullback(h::Handle, lre::AbstractArray{Float64}, lim::AbstractArray{Float64})
+    gre = similar(lre); gim = similar(lim)
+    GC.@preserve lre lim gre gim check(h, ccall((:gd_temperature_pullback, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, lre, lim, gre, gim))
+    return gre, gim
+end
+
 # Transpose of spectral_to_physical! (gd_spectral_to_physical_adjoint).
 function spectral_to_physical_adjoint!(h::Handle, phys_bar, spec_bar)
     g = parent(phys_bar.data); re = parent(spec_bar.data_real); im = parent(spec_bar.data_imag)

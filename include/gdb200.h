@@ -426,8 +426,9 @@ int gd_copy_block(gd_handle* h, int array, int field, int r0, int r1, int j0, in
  * layout [nr][nlat][nlon] (gd_grid_device copies the handle's).
  *
  * Snapshot of the step state (fields, both banks of nonlinear terms, the
- * grids, the bank parity and step count) into or out of a device buffer of
- * gd_snapshot_bytes bytes; FP64 handles. */
+ * grids a step reads before writing them -- u, B and j -- the bank parity and
+ * the step count) into or out of a device buffer of gd_snapshot_bytes bytes;
+ * FP64 handles. */
 int gd_snapshot_bytes(gd_handle* h, size_t* bytes);
 int gd_snapshot(gd_handle* h, void* dev, int restore);
 /* Host reference-layout (l-major) Re/Im planes <-> a native device array. */
@@ -442,6 +443,20 @@ int gd_temperature_nl_adjoint(gd_handle* h, const double* u_th, const double* u_
  * fixed-value boundary rows), with the field's implicit operators.  Fixed-value
  * boundaries only: GD_ERR_UNSUPPORTED when the field has flux boundaries. */
 int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double* y);
+/* The pieces composed with checkpoint and recompute.  gd_temperature_forward
+ * runs nsteps steps keeping a snapshot every checkpoint_every steps (and one
+ * of the end state) in device memory owned by the handle (FP64, CNAB2).
+ * gd_temperature_pullback then maps the cotangent of the temperature after
+ * those steps (lam, reference layout) to its cotangent at their start (out):
+ * segment by segment from the last, it restores the segment's snapshot, steps
+ * through it again recording the velocity grids each step's temperature
+ * phase reads, and applies psi^n = D S^-T C lambda^n,
+ * lambda^n = P R^T psi^(n+1) + N_n^T (a_n psi^(n+1) - b_(n+1) psi^(n+2));
+ * it leaves the handle in the end state of the forward run.  The snapshots
+ * hold the state, both banks of nonlinear terms and the grids a step reads
+ * before writing (u, B, j). */
+int gd_temperature_forward(gd_handle* h, int nsteps, int checkpoint_every);
+int gd_temperature_pullback(gd_handle* h, const double* lam_re, const double* lam_im, double* out_re, double* out_im);
 
 /* ---- launch shape -------------------------------------------------------------------
  * No counterpart in the reference.  tc_ctas caps the persistent grid of the

@@ -164,3 +164,78 @@ def test_temperature_gradient_matches_fd_and_forward_mode(gdb, oracle_mod, bc_mo
             worst_fm = abs(fm - gdot) / abs(fm)
     print(f"bc_mode {bc_mode} ab_mode {ab_mode}: J {J:.6e}, FD rel err {worst_fd:.2e}, forward-mode rel err {worst_fm:.2e}")
     assert worst_fd <= 1e-6 and worst_fm <= 1e-6
+
+
+def composed_pullback(gdb, model, lre, lim, K, C, s0, ab1, snaps, final):
+    """The reverse pass written out from the pieces (gd_snapshot,
+    gd_grid_device, gd_cnab2_adjoint, gd_temperature_nl_adjoint)."""
+    import torch
+    G = model.nr * model.nlat * model.nlon
+    size = 2 * model.nr * model.nlm
+    f64 = dict(dtype=torch.float64, device="cuda")
+    lam = torch.empty(size, **f64)
+    model.spectral_to_device(lre, lim, lam)
+    psi1, psi2 = torch.empty(size, **f64), torch.zeros(size, **f64)
+    tmp, nlt = torch.empty(size, **f64), torch.empty(size, **f64)
+    model.cnab2_adjoint("temp", 0, lam, psi1)
+    boot = lambda n: ab1 or s0 + n == 0  # noqa: E731
+    for k in reversed(range(len(snaps))):
+        c0, c1 = k * C, min(K, k * C + C)
+        model.restore(snaps[k])
+        ust = []
+        for n in range(c0, c1):
+            u = torch.empty(2 * G, **f64)
+            model.grid_to_device("u_th", u[:G])
+            model.grid_to_device("u_ph", u[G:])
+            ust.append(u)
+            if n < c1 - 1:
+                model.step(1)
+        for n in reversed(range(c0, c1)):
+            a_n = 1.0 if boot(n) else 1.5
+            b_n1 = 0.0 if (n + 1 >= K or boot(n + 1)) else 0.5
+            torch.mul(psi1, a_n, out=tmp)
+            if b_n1:
+                tmp.sub_(psi2, alpha=b_n1)
+            u = ust[n - c0]
+            model.temperature_nl_adjoint(u[:G], u[G:], tmp, nlt)
+            model.cnab2_adjoint("temp", 1, psi1, lam)
+            lam.add_(nlt)
+            if n > 0:
+                psi2, psi1 = psi1, psi2
+                model.cnab2_adjoint("temp", 0, lam, psi1)
+    model.restore(final)
+    return model.spectral_from_device(lam)
+
+
+def test_native_pullback_equals_composed_pieces(gdb):
+    import torch
+    nr, K, C = 10, 17, 5
+    st = workloads.seeded_state(15, 15, nr, seed=4, amp=0.3)
+    m = gdb.SHTnsKitConfig(15, 24, 48, nr, dt=1e-5)
+    for k, (a, b) in st.items():
+        m.set_field(k, a, b)
+    rng = np.random.default_rng(5)
+    lre, lim = rng.standard_normal(m.spec_shape()), rng.standard_normal(m.spec_shape())
+    nb = m.snapshot_bytes()
+    snaps = [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in range((K + C - 1) // C)]
+    final = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    start = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    m.snapshot(start)
+    for k in range(len(snaps)):
+        m.snapshot(snaps[k])
+        m.step(min(C, K - k * C))
+    m.snapshot(final)
+    ref = composed_pullback(gdb, m, lre, lim, K, C, 0, False, snaps, final)
+    m.restore(start)
+    m.temperature_forward(K, C)
+    got = m.temperature_pullback(lre, lim)
+    # the same kernels in the same order; a psi^(n+1) - b psi^(n+2) is one fused
+    # multiply-add in the library and two roundings in torch
+    for x, y in zip(got, ref):
+        assert np.max(np.abs(x - y)) <= 1e-13 * np.max(np.abs(y))
+    # the handle is left at the end of the forward run
+    after = m.get_field("temp")
+    m.restore(final)
+    for x, y in zip(after, m.get_field("temp")):
+        assert np.array_equal(x, y)
+    m.close()
