@@ -288,16 +288,25 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-def run_ensemble(args, gdb, workloads, torch):
+def run_ensemble(args, gdb, workloads, torch, world=1, rank=0):
     """Batched uneven ensemble: args.ensemble seeded shells (lmax 31-95, nr 33-65,
     E and Ra drawn per member), one graph launch per step for all of them;
     aggregate instance-steps/s, device-timed with CUDA events on the ensemble's
-    stream, FP64 and mixed precision."""
-    cfgs = workloads.ensemble_draw(args.ensemble)
+    stream, FP64 and mixed precision.  Over several ranks (torchrun) the whole
+    instances are dealt round-robin to the ranks (no collective in the step);
+    time = max over ranks, value = all instances' steps / that time."""
+    allc = workloads.ensemble_draw(args.ensemble)
+    mine = list(range(rank, len(allc), world))
+    cfgs = [allc[i] for i in mine]
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     res = {}
     for prec in ("fp64", "mixed"):
         ens = gdb.Ensemble(cfgs, precision=prec)
-        for i, (c, m) in enumerate(zip(cfgs, ens.members)):
+        for i, c, m in zip(mine, cfgs, ens.members):
             for k, (a, b) in workloads.seeded_state(c["lmax"], c["lmax"], c["nr"], seed=i).items():
                 m.set_field(k, a, b)
         tune = None
@@ -306,6 +315,8 @@ def run_ensemble(args, gdb, workloads, torch):
             tms, caps = ens.autotune(5)
             tune = {"ms_per_step": tms, "caps": sorted(set(caps))}
         ens.step(args.warmup)
+        if dist is not None:
+            dist.barrier()
         ext = torch.cuda.ExternalStream(ens.stream_ptr())
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -317,16 +328,27 @@ def run_ensemble(args, gdb, workloads, torch):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         ek = sum(m.energy()[0] for m in ens.members)
-        res[prec] = {"instance_steps_per_s": args.steps * len(cfgs) / (ms * 1e-3), "ms_per_step": ms / args.steps,
+        if dist is not None:
+            t = torch.tensor([ms, ek], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
+            dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+            ms, ek = float(t[0]), float(t[1])
+        res[prec] = {"instance_steps_per_s": args.steps * len(allc) / (ms * 1e-3), "ms_per_step": ms / args.steps,
                      "sum_ekin": ek}
         if tune is not None:
             res[prec]["autotune"] = tune
         ens.close()
-    line = {"metric": f"ensemble instance-steps/s ({len(cfgs)} uneven shells)", "value": res["mixed"]["instance_steps_per_s"],
-            "unit": "instance-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": f"ensemble instance-steps/s ({len(allc)} uneven shells)", "value": res["mixed"]["instance_steps_per_s"],
+            "unit": "instance-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "scaling": "strong" if world > 1 else "weak",
             "higher_is_better": True, "dtype": "f32/tf32x3 (FP64 solves)", "data": "synthetic (ensemble_draw(seed=3), seeded_state(seed=i))",
-            "config": {"workload": "ensemble", "members": len(cfgs), "lmax": sorted({c["lmax"] for c in cfgs}),
-                       "nr": sorted({c["nr"] for c in cfgs}), "dt": 1e-5,
+            "config": {"workload": "ensemble", "members": len(allc), "lmax": sorted({c["lmax"] for c in allc}),
+                       "nr": sorted({c["nr"] for c in allc}), "dt": 1e-5, "ranks": world,
+                       "placement": "whole instances round-robin over the ranks",
                        "launch": "one CUDA graph per step; mixed: tensor-core grid caps by gd_ensemble_autotune"},
             "fp64": res["fp64"], "mixed": res["mixed"],
             "ratio_vs_fp64_gpu": res["mixed"]["instance_steps_per_s"] / res["fp64"]["instance_steps_per_s"]}
@@ -709,7 +731,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if args.ensemble > 0:
-        return run_ensemble(args, gdb, workloads, torch)
+        return run_ensemble(args, gdb, workloads, torch, world, rank)
     if args.decomposed:
         return run_decomposed(args, gdb, workloads, torch, world, rank, local)
     if args.adjoint:
