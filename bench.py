@@ -294,7 +294,10 @@ def run_ensemble(args, gdb, workloads, torch, world=1, rank=0):
     aggregate instance-steps/s, device-timed with CUDA events on the ensemble's
     stream, FP64 and mixed precision.  Over several ranks (torchrun) the whole
     instances are dealt round-robin to the ranks (no collective in the step);
-    time = max over ranks, value = all instances' steps / that time."""
+    time = max over ranks, value = all instances' steps / that time.
+    Members of one (lmax, nr) class share a segmented handle (up to
+    --ensemble-group per handle, each with its own Coriolis factor); the
+    per-member-handle ensemble is timed beside it."""
     allc = workloads.ensemble_draw(args.ensemble)
     mine = list(range(rank, len(allc), world))
     cfgs = [allc[i] for i in mine]
@@ -304,8 +307,12 @@ def run_ensemble(args, gdb, workloads, torch, world=1, rank=0):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     res = {}
-    for prec in ("fp64", "mixed"):
-        ens = gdb.Ensemble(cfgs, precision=prec)
+    group = max(1, args.ensemble_group)
+    legs = [("fp64", group), ("mixed", group)]
+    if group > 1:
+        legs += [("fp64", 1), ("mixed", 1)]
+    for prec, grp in legs:
+        ens = gdb.Ensemble(cfgs, precision=prec, group=grp)
         for i, c, m in zip(mine, cfgs, ens.members):
             for k, (a, b) in workloads.seeded_state(c["lmax"], c["lmax"], c["nr"], seed=i).items():
                 m.set_field(k, a, b)
@@ -333,10 +340,11 @@ def run_ensemble(args, gdb, workloads, torch, world=1, rank=0):
             dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
             dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
             ms, ek = float(t[0]), float(t[1])
-        res[prec] = {"instance_steps_per_s": args.steps * len(allc) / (ms * 1e-3), "ms_per_step": ms / args.steps,
-                     "sum_ekin": ek}
+        key = prec if grp == group else prec + "_handle_per_member"
+        res[key] = {"instance_steps_per_s": args.steps * len(allc) / (ms * 1e-3), "ms_per_step": ms / args.steps,
+                    "sum_ekin": ek, "handles": len(ens.handles)}
         if tune is not None:
-            res[prec]["autotune"] = tune
+            res[key]["autotune"] = tune
         ens.close()
     if dist is not None:
         dist.destroy_process_group()
@@ -349,8 +357,9 @@ def run_ensemble(args, gdb, workloads, torch, world=1, rank=0):
             "config": {"workload": "ensemble", "members": len(allc), "lmax": sorted({c["lmax"] for c in allc}),
                        "nr": sorted({c["nr"] for c in allc}), "dt": 1e-5, "ranks": world,
                        "placement": "whole instances round-robin over the ranks",
-                       "launch": "one CUDA graph per step; mixed: tensor-core grid caps by gd_ensemble_autotune"},
-            "fp64": res["fp64"], "mixed": res["mixed"],
+                       "launch": "one CUDA graph per step; mixed: tensor-core grid caps by gd_ensemble_autotune",
+                       "grouping": f"members of one (lmax, nr) class share a segmented handle, <= {group} per handle"},
+            **res,
             "ratio_vs_fp64_gpu": res["mixed"]["instance_steps_per_s"] / res["fp64"]["instance_steps_per_s"]}
     print(json.dumps(line), flush=True)
     return 0
@@ -708,6 +717,8 @@ def main():
                     help="instead of the headline: the transform-only batch's errors and timings")
     ap.add_argument("--adjoint", action="store_true",
                     help="instead of the headline: the adjoint configuration's gradient checks and timings")
+    ap.add_argument("--ensemble-group", type=int, default=64,
+                    help="ensemble: members of one (lmax, nr) class per segmented handle, at most this many (1: a handle each)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead of the headline: the batched uneven ensemble of this many shells")
     ap.add_argument("--decomposed", action="store_true",

@@ -67,7 +67,7 @@ EXPORTS = (
     "gd_set_temperature_bc", "gd_spectral_to_physical", "gd_physical_to_spectral", "gd_vector_synthesis",
     "gd_vector_analysis", "gd_temperature_nonlinear", "gd_velocity_nonlinear", "gd_magnetic_nonlinear",
     "gd_implicit_step", "gd_step", "gd_step_async", "gd_set_dt", "gd_set_scheme", "gd_download_etd",
-    "gd_energy", "gd_check_finite",
+    "gd_energy", "gd_segment_energy", "gd_set_segment_ekman", "gd_check_finite",
     "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
     "gd_spectral_to_physical_noalloc",
     "gd_compute_temperature_nonlinear", "gd_compute_velocity_nonlinear", "gd_compute_magnetic_nonlinear",
@@ -102,6 +102,7 @@ class GDConfig(ctypes.Structure):
         ("ab_mode", ctypes.c_int), ("bc_mode", ctypes.c_int), ("fd_mode", ctypes.c_int),
         ("precision", ctypes.c_int), ("magnetic", ctypes.c_int),
         ("composition", ctypes.c_int), ("schmidt", ctypes.c_double),
+        ("segments", ctypes.c_int),
     ]
 
 
@@ -161,6 +162,8 @@ def load_library():
         "gd_set_scheme": ([P, I], I),
         "gd_download_etd": ([P, I, I, I, D], I),
         "gd_energy": ([P, D, D], I),
+        "gd_segment_energy": ([P, D, D], I),
+        "gd_set_segment_ekman": ([P, D], I),
         "gd_check_finite": ([P], I),
         "gd_step_count": ([P], ctypes.c_long),
         "gd_get_stream": ([P, ctypes.POINTER(P)], I),
@@ -260,13 +263,13 @@ class SHTnsKitConfig:
 
     def __init__(self, lmax, nlat, nlon, nr, mmax=None, kl=4, rratio=0.35, ekman=3e-4, rayleigh=80.0,
                  prandtl=1.0, magnetic_prandtl=4.0, dt=1e-5, implicit_theta=0.5, ab_mode=0, bc_mode=0,
-                 fd_mode=0, precision="fp64", magnetic=1, device=0, composition=0, schmidt=1.0):
+                 fd_mode=0, precision="fp64", magnetic=1, device=0, composition=0, schmidt=1.0, segments=0):
         self.lib = load_library()
         mmax = lmax if mmax is None else mmax
         base, stages = PRECISION_PRESETS.get(precision, (precision, ()))
         self.cfg = GDConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl, magnetic_prandtl,
                             dt, implicit_theta, ab_mode, bc_mode, fd_mode, PRECISIONS[base], magnetic,
-                            int(composition), float(schmidt))
+                            int(composition), float(schmidt), int(segments))
         h = ctypes.c_void_p()
         st = self.lib.gd_create(ctypes.byref(self.cfg), int(device), ctypes.byref(h))
         if st != GD_OK:
@@ -352,6 +355,24 @@ class SHTnsKitConfig:
     def set_launch_shape(self, tc_ctas=0):
         """Cap of the tensor-core kernels' persistent grid (0: one CTA per SM)."""
         self._check(self.lib.gd_set_launch_shape(self.h, int(tc_ctas)))
+
+    def segments(self):
+        """Independent shells stacked along r in this handle (1: one shell)."""
+        return max(1, int(self.cfg.segments))
+
+    def set_segment_ekman(self, ekman):
+        """Ekman number of each segment (the Coriolis and Lorentz factor Pm/E of its shells)."""
+        e = _f64(np.asarray(ekman, dtype=np.float64).reshape(-1))
+        if e.size != self.segments():
+            raise ValueError(f"need {self.segments()} Ekman numbers")
+        self._check(self.lib.gd_set_segment_ekman(self.h, _dptr(e)))
+
+    def segment_energy(self):
+        """(kinetic, magnetic) energy of each segment, arrays of segments values."""
+        n = self.segments()
+        ek = np.zeros(n); em = np.zeros(n)
+        self._check(self.lib.gd_segment_energy(self.h, _dptr(ek), _dptr(em)))
+        return ek, em
 
     def step_kernels(self):
         """Kernel launches of the next step (kernel nodes of its CUDA graph)."""
@@ -763,16 +784,40 @@ def temperature_misfit(model, target, nsteps, checkpoint_every=20, shell=None):
 
 class Ensemble:
     """Independent shells stepped together (gd_ensemble_*): one CUDA graph
-    launch per step runs every member's step as its own branch.  ``members``
+    launch per step runs every handle's step as its own branch.  ``members``
     are SHTnsKitConfig views of the member handles (upload, download, energy,
-    nonlinear terms as for a single model); the ensemble owns the handles."""
+    nonlinear terms as for a single model); the ensemble owns the handles.
 
-    def __init__(self, configs, precision="fp64", device=0):
+    ``group`` > 1 stacks up to that many members whose configurations differ
+    only in the Ekman number (and the Rayleigh number, which the step does not
+    read: the vector analysis drops the radial buoyancy force) into one
+    segmented handle (gd_config.segments), each member with its own Coriolis
+    factor: every per-shell kernel then serves the whole group in one launch.
+    Its members are EnsembleSegment views of their levels."""
+
+    def __init__(self, configs, precision="fp64", device=0, group=1):
         self.lib = load_library()
-        n = len(configs)
+        configs = [dict(c) for c in configs]
+        slots = []
+        if group > 1:
+            open_ = {}
+            for i, c in enumerate(configs):
+                key = tuple(sorted((k, repr(v)) for k, v in c.items() if k not in ("ekman", "rayleigh")))
+                lst = open_.get(key)
+                if lst is None or len(lst) >= group:
+                    lst = []
+                    open_[key] = lst
+                    slots.append(lst)
+                lst.append(i)
+        else:
+            slots = [[i] for i in range(len(configs))]
+        n = len(slots)
         arr = (GDConfig * n)()
-        for i, c in enumerate(configs):
-            c = dict(c)
+        for i, slot in enumerate(slots):
+            c = dict(configs[slot[0]])
+            if len(slot) > 1:
+                c["nr"] = c["nr"] * len(slot)
+                c["segments"] = len(slot)
             lmax = c.pop("lmax")
             mmax = c.pop("mmax", None)
             mmax = lmax if mmax is None else mmax
@@ -781,14 +826,23 @@ class Ensemble:
                               c.pop("prandtl", 1.0), c.pop("magnetic_prandtl", 4.0), c.pop("dt", 1e-5),
                               c.pop("implicit_theta", 0.5), c.pop("ab_mode", 0), c.pop("bc_mode", 0),
                               c.pop("fd_mode", 0), PRECISIONS[c.pop("precision", precision)],
-                              c.pop("magnetic", 1), c.pop("composition", 0), c.pop("schmidt", 1.0))
+                              c.pop("magnetic", 1), c.pop("composition", 0), c.pop("schmidt", 1.0),
+                              c.pop("segments", 0))
         e = ctypes.c_void_p()
         st = self.lib.gd_ensemble_create(arr, n, int(device), ctypes.byref(e))
         if st != GD_OK:
             raise GeoDynamoError(st, "gd_ensemble_create failed (see stderr)")
         self.e = e
-        self.members = [SHTnsKitConfig._member(self.lib, ctypes.c_void_p(self.lib.gd_ensemble_member(e, i)), arr[i])
+        self.handles = [SHTnsKitConfig._member(self.lib, ctypes.c_void_p(self.lib.gd_ensemble_member(e, i)), arr[i])
                         for i in range(n)]
+        self.members = [None] * len(configs)
+        for hv, slot in zip(self.handles, slots):
+            if len(slot) == 1:
+                self.members[slot[0]] = hv
+                continue
+            hv.set_segment_ekman([configs[i].get("ekman", 3e-4) for i in slot])
+            for g, i in enumerate(slot):
+                self.members[i] = EnsembleSegment(hv, g, configs[i]["nr"])
 
     def __len__(self):
         return len(self.members)
@@ -803,9 +857,9 @@ class Ensemble:
     def autotune(self, nsteps=5):
         """Chooses the members' tensor-core grid caps by timing candidates on a
         scratch copy of the ensemble (gd_ensemble_autotune); returns
-        (ms per ensemble step, caps)."""
+        (ms per ensemble step, caps), one cap per handle."""
         ms = ctypes.c_float()
-        caps = (ctypes.c_int * len(self.members))()
+        caps = (ctypes.c_int * len(self.handles))()
         st = self.lib.gd_ensemble_autotune(self.e, int(nsteps), ctypes.byref(ms), caps)
         if st != GD_OK:
             raise GeoDynamoError(st, "gd_ensemble_autotune failed")
@@ -825,7 +879,7 @@ class Ensemble:
 
     def close(self):
         if getattr(self, "e", None):
-            for m in self.members:
+            for m in self.handles:
                 m.h = None
             self.lib.gd_ensemble_destroy(self.e)
             self.e = None
@@ -835,6 +889,50 @@ class Ensemble:
             self.close()
         except Exception:
             pass
+
+
+class EnsembleSegment:
+    """One member of a grouped ensemble: levels [seg nr, (seg + 1) nr) of a
+    segmented handle.  Fields, nonlinear terms and energies of the member
+    alone; the step runs for the whole handle."""
+
+    def __init__(self, handle, seg, nr):
+        self.handle = handle
+        self.seg = int(seg)
+        self.nr = int(nr)
+        self.lmax, self.mmax, self.nlat, self.nlon, self.nlm = (handle.lmax, handle.mmax, handle.nlat,
+                                                                handle.nlon, handle.nlm)
+        self.rows = slice(self.seg * self.nr, (self.seg + 1) * self.nr)
+
+    def spec_shape(self):
+        return (self.nr, self.nlm)
+
+    def field_names(self):
+        return self.handle.field_names()
+
+    def set_field(self, name, re, im):
+        fr, fi = self.handle.get_field(name)
+        fr[self.rows] = np.asarray(re, dtype=np.float64).reshape(self.spec_shape())
+        fi[self.rows] = np.asarray(im, dtype=np.float64).reshape(self.spec_shape())
+        self.handle.set_field(name, fr, fi)
+
+    def get_field(self, name):
+        fr, fi = self.handle.get_field(name)
+        return fr[self.rows].copy(), fi[self.rows].copy()
+
+    def get_nl(self, name):
+        fr, fi = self.handle.get_nl(name)
+        return fr[self.rows].copy(), fi[self.rows].copy()
+
+    def energy(self):
+        ek, em = self.handle.segment_energy()
+        return float(ek[self.seg]), float(em[self.seg])
+
+    def step_count(self):
+        return self.handle.step_count()
+
+    def launch_shape(self):
+        return self.handle.launch_shape()
 
 
 # ---------------------------------------------------------------------------

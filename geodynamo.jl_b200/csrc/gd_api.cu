@@ -50,6 +50,11 @@ int dalloc(gd_handle* h, T** p, size_t n) {
     if (s_) return s_;                         \
   } while (0)
 
+// Entry points built for one shell per handle refuse a segmented handle.
+static int refuse_segments(gd_handle* h, const char* what) {
+  return fail(h, GD_ERR_UNSUPPORTED, std::string(what) + " is not built for a segmented handle");
+}
+
 int check_launch(gd_handle* h, const char* what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(h, GD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -59,7 +64,7 @@ int check_launch(gd_handle* h, const char* what) {
 int build_implicit(gd_handle* h) {
   const Dims& d = h->d;
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-  launch_build_lu(h->stream, d.nr, d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->c.dt,
+  launch_build_lu(h->stream, d.nrs, d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->c.dt,
                   h->c.implicit_theta, h->c.bc_mode == 2, h->d_lin, h->d_lu, h->d_flag, h->c.composition ? 4 : 3);
   int s = check_launch(h, "build_lu");
   if (s) return s;
@@ -78,7 +83,7 @@ int build_implicit(gd_handle* h) {
 // single-boundary combinations and their D1 derivatives at the boundary they
 // serve.  Needs the radial nodes and D1 on the device.
 int build_tau(gd_handle* h) {
-  const int N = h->d.nr, KL = h->d.kl, NB = 2 * GD_MAX_KL + 1;
+  const int N = h->d.nrs, KL = h->d.kl, NB = 2 * GD_MAX_KL + 1;
   std::vector<double> r(N), d1((size_t)NB * N);
   CK(cudaMemcpyAsync(r.data(), h->d_r, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(d1.data(), h->d_d1, sizeof(double) * NB * N, cudaMemcpyDeviceToHost, h->stream));
@@ -151,6 +156,10 @@ int setup(gd_handle* h) {
   d.nlm = (int)h->lv.size();
   d.jlo = 0;
   d.jhi = d.nlm;
+  d.nseg = c.segments > 1 ? c.segments : 1;
+  d.nrs = d.nr / d.nseg;
+  d.rfs = nullptr;
+  d.rfs32 = nullptr;
   h->moff.assign(d.M + 2, 0);
   for (int m = 0; m <= d.M; ++m) h->moff[m + 1] = h->moff[m] + (d.L - m + 1);
   h->perm.resize(d.nlm);
@@ -183,7 +192,7 @@ int setup(gd_handle* h) {
   AL(h->d_cbvals, 2 * NL); AL(h->d_csources, NR); AL(h->d_bctype, 4 * NL); AL(h->d_tau, 4 * NR);
   AL(h->d_grid, NGRID * h->grid_elems());
   AL(h->d_F, (size_t)4 * NR * (d.M + 1) * d.nlat);
-  AL(h->d_epart, 2 * 296); AL(h->d_eout, 2);
+  AL(h->d_epart, 2 * GD_ENERGY_BLOCKS * d.nseg); AL(h->d_eout, 2 * d.nseg);
 
   cudaStream_t s = h->stream;
   CK(cudaMemcpyAsync(h->d_moff, h->moff.data(), sizeof(int) * (d.M + 2), cudaMemcpyHostToDevice, s));
@@ -195,7 +204,10 @@ int setup(gd_handle* h) {
   std::vector<double> r(NR), ri(NR), ri2(NR);
   const double rin = c.rratio / (1.0 - c.rratio);
   const double kPi = 3.14159265358979323846;
-  for (int n = 1; n <= d.nr; ++n) r[n - 1] = 0.5 * (1.0 + std::cos(kPi * (double)(d.nr - n) / (double)(d.nr - 1))) + rin;
+  // one segment's nodes, repeated for every segment
+  const int NS = d.nrs;
+  for (int n = 1; n <= NS; ++n) r[n - 1] = 0.5 * (1.0 + std::cos(kPi * (double)(NS - n) / (double)(NS - 1))) + rin;
+  for (int n = NS; n < d.nr; ++n) r[n] = r[n % NS];
   for (int n = 0; n < d.nr; ++n) { ri[n] = std::pow(r[n], -1.0); ri2[n] = std::pow(r[n], -2.0); }
   CK(cudaMemcpyAsync(h->d_r, r.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(h->d_rinv, ri.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
@@ -215,7 +227,7 @@ int setup(gd_handle* h) {
 
   launch_gauss(s, d.nlat, h->d_x, h->d_w, h->d_th, h->d_sth);
   launch_tables(s, d, h->d_moff, h->d_x, h->d_sth, h->d_P, h->d_dP, h->d_Q);
-  launch_fd_weights(s, d.nr, d.kl, c.fd_mode, h->d_r, h->d_d1, h->d_d2);
+  launch_fd_weights(s, d.nrs, d.kl, c.fd_mode, h->d_r, h->d_d1, h->d_d2);
   int st = check_launch(h, "set-up kernels");
   if (st) return st;
   // Coriolis factors sin/cos of the colatitude grid (src/velocity.jl:278-282).
@@ -652,6 +664,9 @@ bool valid_config(const gd_config* c, std::string& why) {
   if (c->composition != 0 && c->composition != 1) { why = "composition must be 0 or 1"; return false; }
   if (c->composition && !(c->schmidt > 0.0)) { why = "composition needs a positive Schmidt number"; return false; }
   if (c->composition && c->bc_mode == 2) { why = "composition supports bc_mode 0 and 1"; return false; }
+  if (c->segments < 0 || (c->segments > 1 && c->nr % c->segments)) { why = "segments must divide nr"; return false; }
+  if (c->segments > 1 && c->nr / c->segments < 3) { why = "each segment needs at least 3 levels"; return false; }
+  if (c->segments > 1 && c->composition) { why = "segments carry no composition"; return false; }
   return true;
 }
 
@@ -739,6 +754,7 @@ int gd_set_fp64_stages(gd_handle* h, int mask) {
 
 int gd_set_external_derivatives(gd_handle* h, int enable) {
   if (!h) return GD_ERR_ARG;
+  if (enable && h->d.nseg > 1) return refuse_segments(h, "the distributed step");
   CK(cudaSetDevice(h->device));
   if ((enable != 0) != h->ext_derivs) drop_graphs(h);
   h->ext_derivs = enable != 0;
@@ -769,6 +785,7 @@ int gd_temperature_forward(gd_handle* h, int nsteps, int checkpoint_every) {
   if (!h || nsteps < 1 || checkpoint_every < 1) return h ? fail(h, GD_ERR_ARG, "need nsteps, checkpoint_every >= 1") : GD_ERR_ARG;
   if (h->precision != GD_PREC_FP64 || h->scheme != GD_SCHEME_CNAB2)
     return fail(h, GD_ERR_UNSUPPORTED, "the temperature pullback is of the FP64 CNAB2 step");
+  if (h->d.nseg > 1) return refuse_segments(h, "the temperature pullback");
   CK(cudaSetDevice(h->device));
   free_tckpt(h);
   size_t nb = 0;
@@ -860,7 +877,36 @@ int gd_get_launch_shape(const gd_handle* h, int* tc_ctas) {
   return GD_OK;
 }
 
+int gd_set_segment_ekman(gd_handle* h, const double* ekman) {
+  if (!h || !ekman) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  const int nseg = h->d.nseg, nrs = h->d.nrs;
+  for (int g = 0; g < nseg; ++g)
+    if (!(ekman[g] > 0.0) || !std::isfinite(ekman[g])) return fail(h, GD_ERR_ARG, "Ekman numbers must be positive");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  // rossby_factor (src/velocity.jl:456): Pm / E of each shell's segment, in
+  // FP64 for the FP64 kernels and rounded once to FP32 for the fused kernel
+  std::vector<double> rf(h->d.nr);
+  std::vector<float> rf32(h->d.nr);
+  for (int k = 0; k < h->d.nr; ++k) {
+    rf[k] = h->c.magnetic_prandtl / ekman[k / nrs];
+    rf32[k] = (float)rf[k];
+  }
+  if (!h->d_rfs) {
+    AL(h->d_rfs, h->d.nr);
+    AL(h->d_rfs32, h->d.nr);
+  }
+  CK(cudaMemcpyAsync(h->d_rfs, rf.data(), sizeof(double) * h->d.nr, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_rfs32, rf32.data(), sizeof(float) * h->d.nr, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  drop_graphs(h);
+  h->d.rfs = h->d_rfs;
+  h->d.rfs32 = h->d_rfs32;
+  return GD_OK;
+}
+
 static bool mode_range_ok(const gd_handle* h, int j0, int j1) { return 0 <= j0 && j0 <= j1 && j1 <= h->d.nlm; }
+
 
 int gd_set_composition_bc(gd_handle* h, const double* bvals, const double* sources) {
   if (!h) return GD_ERR_ARG;
@@ -978,6 +1024,7 @@ int gd_grid_device(gd_handle* h, int grid, double* dev) {
 
 int gd_temperature_nl_adjoint(gd_handle* h, const double* u_th, const double* u_ph, const double* nu, double* out) {
   if (!h || !u_th || !u_ph || !nu || !out) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (h->d.nseg > 1) return refuse_segments(h, "the nonlinear-term adjoint");
   CK(cudaSetDevice(h->device));
   const size_t se = h->spec_elems(), G = h->grid_elems();
   if (!h->d_adj) AL(h->d_adj, 3 * se + 3 * G);
@@ -1011,6 +1058,7 @@ int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double*
   if (!h || !x || !y || (mode != 0 && mode != 1) || field < 0 || field >= nfields(h))
     return h ? fail(h, GD_ERR_ARG, "bad field, mode or pointer") : GD_ERR_ARG;
   if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the adjoint is of the CNAB2 step");
+  if (h->d.nseg > 1) return refuse_segments(h, "the CNAB2 adjoint");
   const size_t NL = h->d.nlm;
   const bool scalar = field == GD_TEMP || field == GD_COMP;
   const int kind = field == GD_TEMP ? 2 : field == GD_COMP ? 3 : (field == GD_U_TOR || field == GD_U_POL) ? 0 : 1;
@@ -1034,6 +1082,7 @@ int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double*
 
 int gd_derivatives(gd_handle* h, int j0, int j1) {
   if (!h) return GD_ERR_ARG;
+  if (h->d.nseg > 1) return refuse_segments(h, "the mode-range derivatives");
   if (!mode_range_ok(h, j0, j1)) return fail(h, GD_ERR_ARG, "mode range outside [0, nlm]");
   CK(cudaSetDevice(h->device));
   if (j1 == j0) return GD_OK;
@@ -1062,6 +1111,7 @@ int gd_derivatives(gd_handle* h, int j0, int j1) {
 
 int gd_implicit_modes(gd_handle* h, int j0, int j1) {
   if (!h) return GD_ERR_ARG;
+  if (h->d.nseg > 1) return refuse_segments(h, "the mode-range solve");
   if (!mode_range_ok(h, j0, j1)) return fail(h, GD_ERR_ARG, "mode range outside [0, nlm]");
   if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the mode-range solve supports CNAB2 only");
   CK(cudaSetDevice(h->device));
@@ -1282,6 +1332,7 @@ int gd_magnetic_pullback(gd_handle* h, int field, int nsteps, const double* lam_
   if (!h || !lam_re || !lam_im || !out_re || !out_im || nsteps < 0 || (field != GD_B_TOR && field != GD_B_POL))
     return h ? fail(h, GD_ERR_ARG, "bad arguments (field must be GD_B_TOR or GD_B_POL)") : GD_ERR_ARG;
   if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the pullback is of the CNAB2 propagator");
+  if (h->d.nseg > 1) return refuse_segments(h, "the magnetic pullback");
   CK(cudaSetDevice(h->device));
   int s = stage_alloc(h);
   if (s) return s;
@@ -1388,6 +1439,7 @@ int gd_create_timestepping_matrices(gd_handle* h, double diffusivity, double dt,
   if (!h || !out) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
   if (!(dt > 0.0) || !std::isfinite(diffusivity) || !std::isfinite(theta))
     return fail(h, GD_ERR_ARG, "need dt > 0 and finite diffusivity and theta");
+  if (h->d.nseg > 1) return refuse_segments(h, "a standalone timestepping operator");
   CK(cudaSetDevice(h->device));
   const Dims& d = h->d;
   const size_t n = (size_t)d.nr * (2 * d.kl + 1) * (d.L + 1);
@@ -1641,6 +1693,7 @@ int gd_set_scheme(gd_handle* h, int scheme) {
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   if (scheme != GD_SCHEME_CNAB2) {
+    if (h->d.nseg > 1) return refuse_segments(h, "an exponential scheme");
     if (h->c.composition)
       return fail(h, GD_ERR_UNSUPPORTED, "the exponential schemes are not built for composition (CNAB2 only)");
     if (h->c.bc_mode == 2)
@@ -1676,12 +1729,32 @@ int gd_energy(gd_handle* h, double* ekin, double* emag) {
   CK(cudaSetDevice(h->device));
   launch_energy(h->stream, h->d, h->d_lof, h->field(F_UTOR), h->field(F_UPOL), h->c.magnetic ? h->field(F_BTOR) : nullptr,
                 h->field(F_BPOL), h->d_epart, h->d_eout);
-  double e[2];
-  CK(cudaMemcpyAsync(e, h->d_eout, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<double> e(2 * (size_t)h->d.nseg);
+  CK(cudaMemcpyAsync(e.data(), h->d_eout, sizeof(double) * e.size(), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  // a segmented handle: the sum over its segments
   *ekin = e[0];
   *emag = e[1];
+  for (int g = 1; g < h->d.nseg; ++g) {
+    *ekin += e[2 * g];
+    *emag += e[2 * g + 1];
+  }
   return check_launch(h, "energy");
+}
+
+int gd_segment_energy(gd_handle* h, double* ekin, double* emag) {
+  if (!h || !ekin || !emag) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  launch_energy(h->stream, h->d, h->d_lof, h->field(F_UTOR), h->field(F_UPOL), h->c.magnetic ? h->field(F_BTOR) : nullptr,
+                h->field(F_BPOL), h->d_epart, h->d_eout);
+  std::vector<double> e(2 * (size_t)h->d.nseg);
+  CK(cudaMemcpyAsync(e.data(), h->d_eout, sizeof(double) * e.size(), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int g = 0; g < h->d.nseg; ++g) {
+    ekin[g] = e[2 * g];
+    emag[g] = e[2 * g + 1];
+  }
+  return check_launch(h, "segment energy");
 }
 
 int gd_check_finite(gd_handle* h) {

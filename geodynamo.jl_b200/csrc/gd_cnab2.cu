@@ -25,18 +25,20 @@ namespace gd {
 template <int KL>
 __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const double* __restrict__ LU,
                                              const double* __restrict__ sband, const double* __restrict__ srinv2,
-                                             double nu, const Cnab2Args& a, int slot) {
-  const int N = d.nr;
-  const size_t NM = d.nlm, plane = (size_t)N * NM;
+                                             double nu, const Cnab2Args& a, int slot, int seg) {
+  // the segment's N levels start at shell seg N; the planes span all shells
+  const int N = d.nrs;
+  const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   const size_t Lp1 = (size_t)d.L + 1;
   constexpr int NB = 2 * KL + 1;
   const double nulf = __dmul_rn(nu, (double)l * (l + 1));
-  double* __restrict__ ure = a.u[slot] + j;
-  double* __restrict__ uim = a.u[slot] + plane + j;
-  const double* __restrict__ nre = a.nl[slot] + j;
-  const double* __restrict__ nim = a.nl[slot] + plane + j;
-  const double* __restrict__ pre = a.prev[slot] + j;
-  const double* __restrict__ pim = a.prev[slot] + plane + j;
+  const size_t s0 = (size_t)seg * N * NM + j;
+  double* __restrict__ ure = a.u[slot] + s0;
+  double* __restrict__ uim = a.u[slot] + plane + s0;
+  const double* __restrict__ nre = a.nl[slot] + s0;
+  const double* __restrict__ nim = a.nl[slot] + plane + s0;
+  const double* __restrict__ pre = a.prev[slot] + s0;
+  const double* __restrict__ pim = a.prev[slot] + plane + s0;
   const double* __restrict__ F = LU + l;
   const bool boot = a.boot != 0;
   const bool rows = a.bc_rows != 0;
@@ -200,12 +202,13 @@ __global__ void __launch_bounds__(128, 3) k_cnab2(Dims d, const int* __restrict_
   constexpr int NB = 2 * KL + 1;
   extern __shared__ double sm[];
   double* sband = sm;                 // nu * lap, [col][band]
-  double* srinv2 = sm + (size_t)d.nr * NB;
+  double* srinv2 = sm + (size_t)d.nrs * NB;
   const int slot = blockIdx.y;
   if (slot >= a.nfield) return;
   const int g = a.kind[slot];
   const double nuk = nu[g];
-  const int N = d.nr;
+  // every segment has the same radial nodes: one band, one set of factors
+  const int N = d.nrs;
   for (int e = threadIdx.x; e < N * NB; e += blockDim.x) {
     const int col = e / NB, b = e % NB, i = col + b - KL;
     double v = 0.0;
@@ -222,25 +225,33 @@ __global__ void __launch_bounds__(128, 3) k_cnab2(Dims d, const int* __restrict_
   if (j >= d.jhi) return;
   const int l = lof[j];
   const double* LUk = lu + (size_t)g * N * NB * ((size_t)d.L + 1);
-  cnab2_column<KL>(d, j, l, LUk, sband, srinv2, nuk, a, slot);
+  cnab2_column<KL>(d, j, l, LUk, sband, srinv2, nuk, a, slot, blockIdx.z);
 }
 
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
                   const double* rinv, const double* rinv2, const double* nu, const double* lu, const Cnab2Args& a) {
-  dim3 grid(ceil_div(d.jhi - d.jlo, 128), a.nfield);
-  const size_t smem = ((size_t)d.nr * GD_NBW + d.nr) * sizeof(double);
+  dim3 grid(ceil_div(d.jhi - d.jlo, 128), a.nfield, d.nseg);
+  const size_t smem = ((size_t)d.nrs * GD_NBW + d.nrs) * sizeof(double);
   k_cnab2<GD_MAX_KL><<<grid, 128, smem, s>>>(d, lof, d1, d2, rinv, rinv2, nu, lu, a);
 }
 
 // 0.5 sum over (r, l, m) of (T^2 + P^2) / max(l(l+1), 1) for velocity and
-// magnetic fields (src/magnetic.jl:519-542).  Deterministic two-level sum.
+// magnetic fields (src/magnetic.jl:519-542).  Deterministic two-level sum,
+// one per segment (blockIdx.y), each in the order of an unsegmented handle.
 __global__ void k_energy_partial(Dims d, const int* __restrict__ lof, const double* __restrict__ ut,
                                  const double* __restrict__ up, const double* __restrict__ bt,
                                  const double* __restrict__ bp, double* __restrict__ partial) {
   __shared__ double sk[256], sm[256];
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
+  const size_t seg0 = (size_t)blockIdx.y * d.nrs * NM, segn = (size_t)d.nrs * NM;
+  ut += seg0;
+  up += seg0;
+  if (bt) {
+    bt += seg0;
+    bp += seg0;
+  }
   double ek = 0.0, em = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane; i += (size_t)gridDim.x * blockDim.x) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < segn; i += (size_t)gridDim.x * blockDim.x) {
     const int l = lof[i % NM];
     const double lfv = (double)l * (l + 1.0);
     const double w = 1.0 / (lfv > 1.0 ? lfv : 1.0);
@@ -254,22 +265,29 @@ __global__ void k_energy_partial(Dims d, const int* __restrict__ lof, const doub
     if (threadIdx.x < s) { sk[threadIdx.x] += sk[threadIdx.x + s]; sm[threadIdx.x] += sm[threadIdx.x + s]; }
     __syncthreads();
   }
-  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = sk[0]; partial[2 * blockIdx.x + 1] = sm[0]; }
+  if (threadIdx.x == 0) {
+    const size_t q = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+    partial[2 * q] = sk[0];
+    partial[2 * q + 1] = sm[0];
+  }
 }
 
-__global__ void k_energy_final(int nblk, const double* __restrict__ partial, double* __restrict__ out) {
-  if (threadIdx.x != 0) return;
+// out[2 g], out[2 g + 1]: kinetic and magnetic energy of segment g
+__global__ void k_energy_final(int nblk, int nseg, const double* __restrict__ partial, double* __restrict__ out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nseg) return;
+  partial += (size_t)2 * nblk * g;
   double ek = 0.0, em = 0.0;
   for (int b = 0; b < nblk; ++b) { ek += partial[2 * b]; em += partial[2 * b + 1]; }
-  out[0] = 0.5 * ek;
-  out[1] = 0.5 * em;
+  out[2 * g] = 0.5 * ek;
+  out[2 * g + 1] = 0.5 * em;
 }
 
 void launch_energy(cudaStream_t s, const Dims& d, const int* lof, const double* utor, const double* upol,
                    const double* btor, const double* bpol, double* partial, double* out) {
-  const int nblk = 296;
-  k_energy_partial<<<nblk, 256, 0, s>>>(d, lof, utor, upol, btor, bpol, partial);
-  k_energy_final<<<1, 32, 0, s>>>(nblk, partial, out);
+  const int nblk = GD_ENERGY_BLOCKS;
+  k_energy_partial<<<dim3(nblk, d.nseg), 256, 0, s>>>(d, lof, utor, upol, btor, bpol, partial);
+  k_energy_final<<<ceil_div(d.nseg, 32), 32, 0, s>>>(nblk, d.nseg, partial, out);
 }
 
 __global__ void k_check_finite(size_t n, const double* __restrict__ a, int* flag) {

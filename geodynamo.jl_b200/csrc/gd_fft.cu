@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(256) k_coriolis_fused(Dims d, const double2* _
   __syncthreads();
   C* res = ct_passes<N, TB, 0, 1, C>(bufA, bufB, tw);
   // grid rows: north z.x, south -z.y; the products packed as (north, south)
-  const double mrf = -rf;
+  const double mrf = -(d.rfs ? d.rfs[r] : rf);
   for (int e = threadIdx.x; e < TB * N; e += kThreads) {
     const int ii = e / N, j = e - ii * N;
     C* at = res + ii * RS + pidx(j);

@@ -209,7 +209,9 @@ __global__ void __launch_bounds__(FNT, 4) k_fused(Dims d, FftPlan p, const float
     }
   };
   const float ur = 0.f, wr = 0.f, jr = 0.f, br = 0.f;
-  const float adv = -a.rf, mrf = -a.cf, lfr = a.lf;
+  // per-shell factors when the handle's segments have their own Ekman numbers
+  const float rf_r = d.rfs32 ? d.rfs32[r] : a.rf;
+  const float adv = -rf_r, mrf = a.cf != 0.f ? -rf_r : -a.cf, lfr = d.rfs32 ? rf_r : a.lf;
 
   // consumer of one transformed component: grid rows or the products
   // inputs: T phase [g_r, u_th, g_th, u_ph, g_ph]; V phase [u_th, u_ph,

@@ -53,6 +53,9 @@ struct gd_handle {
   int* d_bctype = nullptr;    // [temperature, composition][inner, outer][nlm] GD_BC_*
   std::vector<int> bctype;    // host copy of d_bctype
   double* d_adj = nullptr;    // adjoint scratch (lazy): 3 spectral fields, 3 grids
+  // per-shell Coriolis / Lorentz factors of a segmented handle (gd_set_segment_ekman)
+  double* d_rfs = nullptr;
+  float* d_rfs32 = nullptr;
   // checkpointed forward run of gd_temperature_forward
   std::vector<void*> t_snaps;
   void* t_final = nullptr;

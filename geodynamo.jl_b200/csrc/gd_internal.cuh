@@ -38,6 +38,13 @@ struct Dims {
   // Dirichlet rows and the CNAB2 solve (0, nlm unless a caller restricts it to
   // the m columns one rank owns)
   int jlo, jhi;
+  // independent segments of nrs = nr / nseg shells stacked along r: the radial
+  // operators act within each segment (blockIdx.z); rfs / rfs32 the Coriolis
+  // and Lorentz factor of each shell when the segments' Ekman numbers differ
+  // (null: the scalar factor of the configuration)
+  int nseg, nrs;
+  const double* rfs;
+  const float* rfs32;
 };
 
 // Analysis epilogue variants.
@@ -201,6 +208,8 @@ void launch_neg_product(cudaStream_t s, size_t n, const double* u, const double*
 void launch_axpby(cudaStream_t s, size_t n, double a, const double* x, double b, const double* y, double* out);
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
                   const double* rinv, const double* rinv2, const double* nu, const double* lu, const Cnab2Args& a);
+// partial sums per segment of the energy reduction: partial holds 2 x this x nseg
+constexpr int GD_ENERGY_BLOCKS = 296;
 void launch_energy(cudaStream_t s, const Dims& d, const int* lof, const double* utor, const double* upol,
                    const double* btor, const double* bpol, double* partial, double* out);
 void launch_check_finite(cudaStream_t s, size_t n, const double* a, int* flag);

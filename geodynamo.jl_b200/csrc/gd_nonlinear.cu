@@ -41,6 +41,8 @@ __global__ void k_velocity_nl(Dims d, const double* __restrict__ cth, const doub
                               R* __restrict__ ath, R* __restrict__ aph) {
   const int plane = d.nlat * d.nlon;
   const size_t base = (size_t)blockIdx.y * plane;
+  // per-shell factors when the handle's segments have their own Ekman numbers
+  if (d.rfs) rf = lf = d.rfs[blockIdx.y];
   const R adv = (R)(-rf), mrf = (R)(-rf), lfr = (R)lf;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += gridDim.x * blockDim.x) {
     const size_t i = base + q;
@@ -75,6 +77,7 @@ __global__ void k_coriolis(Dims d, const double* __restrict__ cth, const double*
                            R* __restrict__ aph) {
   const int plane = d.nlat * d.nlon;
   const size_t base = (size_t)blockIdx.y * plane;
+  if (d.rfs) rf = d.rfs[blockIdx.y];
   const R mrf = (R)(-rf);
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < plane; q += gridDim.x * blockDim.x) {
     const size_t i = base + q;

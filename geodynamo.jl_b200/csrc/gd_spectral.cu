@@ -88,7 +88,15 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
   if (j >= d.jhi) return;
   const int l = lof[j], m = mof[j];
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
-  const int N = d.nr;
+  // segment blockIdx.z: levels base .. base + N - 1 (the whole column when nseg = 1)
+  const int N = d.nrs, base = blockIdx.z * N;
+  T += (size_t)base * NM;
+  rinv += base;
+  if (!IMG) {
+    gth += (size_t)base * NM;
+    gph += (size_t)base * NM;
+    gr += (size_t)base * NM;
+  }
   const bool up = l + 1 <= d.L, dn = l >= 1 && l - 1 >= m;
   const double Ap = up ? sqrt((double)(l + 1) * (l + 1) - (double)m * m) * sqrt((double)(l + 1 + m) * (double)(l + 1 - m)) /
                              (2.0 * l + 1.0)
@@ -116,7 +124,7 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
         if (jj >= 0 && jj < N) sr += d1[(KL + k - jj) + (size_t)NB * jj] * w[t];
       }
       if (IMG) {
-        const int n = (3 * N + k) * 2 + c;
+        const int n = (3 * d.nr + base + k) * 2 + c;
         synth_image_put(img, 256, ip, n >> 8, n & 255, sr);
       } else {
         gr[c * plane + at] = sr;
@@ -145,7 +153,7 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
     if (IMG) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int n = ((1 + (q >> 1)) * N + k) * 2 + (q & 1);
+        const int n = ((1 + (q >> 1)) * d.nr + base + k) * 2 + (q & 1);
         synth_image_put(img, 256, ip, n >> 8, n & 255, v[q]);
       }
     } else {
@@ -159,14 +167,14 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
 
 void launch_gradients(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                       const double* d1, const double* T, double* gth, double* gph, double* gr) {
-  dim3 grid(ceil_div(d.jhi - d.jlo, 128), ceil_div(d.nr, RB_R));
+  dim3 grid(ceil_div(d.jhi - d.jlo, 128), ceil_div(d.nrs, RB_R), d.nseg);
   // the band half-width is validated to GD_MAX_KL at creation
   k_gradients<GD_MAX_KL, false><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, gth, gph, gr, SynthImageOut{});
 }
 
 void launch_gradients_img(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                           const double* d1, const double* T, const SynthImageOut& img) {
-  dim3 grid(ceil_div(d.jhi - d.jlo, 128), ceil_div(d.nr, RB_R));
+  dim3 grid(ceil_div(d.jhi - d.jlo, 128), ceil_div(d.nrs, RB_R), d.nseg);
   k_gradients<GD_MAX_KL, true><<<grid, 128, 0, s>>>(d, lof, mof, rinv, d1, T, nullptr, nullptr, nullptr, img);
 }
 
@@ -191,7 +199,16 @@ __global__ void __launch_bounds__(RAD_THREADS, 4) k_curl(Dims d, const int* __re
   const int j = d.jlo + blockIdx.x * RAD_THREADS + tid;
   const int k0 = blockIdx.y * rows;
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
-  const int N = d.nr;
+  // segment blockIdx.z: levels base .. base + N - 1 (the whole column when nseg = 1)
+  const int N = d.nrs, base = blockIdx.z * N;
+  tor += (size_t)base * NM;
+  pol += (size_t)base * NM;
+  rinv += base;
+  rinv2 += base;
+  if (!IMG) {
+    otor += (size_t)base * NM;
+    opol += (size_t)base * NM;
+  }
   const bool live = j < d.jhi;
   if (live) stage_column<KL>(st.win, pol, plane, NM, N, k0, rows, j);
   stage_band<KL>(st.band[0], d1, N, k0, rows);
@@ -236,9 +253,10 @@ __global__ void __launch_bounds__(RAD_THREADS, 4) k_curl(Dims d, const int* __re
       const double vt = lf * st.rv[1][b] * st.win[c][b + KL][tid] - a2 - 2.0 * st.rv[0][b] * a1;
       const double vp = -lf * st.rv[1][b] * tv[c][b];
       if (IMG) {
-        const int col = (k & 31) * 4 + c;
-        synth_image_put(img, 128, ip, k >> 5, col, vp);
-        synth_image_put(img, 128, ip, k >> 5, col + 2, vt);
+        const int kg = base + k;  // column tiles run over all shells
+        const int col = (kg & 31) * 4 + c;
+        synth_image_put(img, 128, ip, kg >> 5, col, vp);
+        synth_image_put(img, 128, ip, kg >> 5, col + 2, vt);
       } else {
         otor[c * plane + at] = vt;
         opol[c * plane + at] = vp;
@@ -250,8 +268,8 @@ __global__ void __launch_bounds__(RAD_THREADS, 4) k_curl(Dims d, const int* __re
 void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* rinv, const double* rinv2,
                  const double* d1, const double* d2, const double* tor, const double* pol, double* otor,
                  double* opol) {
-  const int rows = radial_rows(d.nr);
-  dim3 grid(ceil_div(d.jhi - d.jlo, RAD_THREADS), ceil_div(d.nr, rows));
+  const int rows = radial_rows(d.nrs);
+  dim3 grid(ceil_div(d.jhi - d.jlo, RAD_THREADS), ceil_div(d.nrs, rows), d.nseg);
   const size_t smem = radial_smem<GD_MAX_KL, 2>();
   allow_dynamic_smem(k_curl<GD_MAX_KL, false>, smem);
   k_curl<GD_MAX_KL, false><<<grid, RAD_THREADS, smem, s>>>(d, lof, nullptr, rinv, rinv2, d1, d2, tor, pol, otor,
@@ -261,8 +279,8 @@ void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* ri
 void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* mof, const double* rinv,
                      const double* rinv2, const double* d1, const double* d2, const double* tor, const double* pol,
                      const SynthImageOut& img) {
-  const int rows = radial_rows(d.nr);
-  dim3 grid(ceil_div(d.jhi - d.jlo, RAD_THREADS), ceil_div(d.nr, rows));
+  const int rows = radial_rows(d.nrs);
+  dim3 grid(ceil_div(d.jhi - d.jlo, RAD_THREADS), ceil_div(d.nrs, rows), d.nseg);
   const size_t smem = radial_smem<GD_MAX_KL, 2>();
   allow_dynamic_smem(k_curl<GD_MAX_KL, true>, smem);
   k_curl<GD_MAX_KL, true><<<grid, RAD_THREADS, smem, s>>>(d, lof, mof, rinv, rinv2, d1, d2, tor, pol, nullptr,
@@ -283,8 +301,10 @@ __global__ void k_scalar_bc(Dims d, const double* __restrict__ bv, const int* __
                             const double* __restrict__ d1, TauConsts tc, double* __restrict__ F) {
   const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.jhi) return;
-  const int N = d.nr, KL = d.kl, NB = 2 * GD_MAX_KL + 1;
-  const size_t NM = d.nlm, plane = (size_t)N * NM;
+  // segment blockIdx.y: its own boundary rows and radial profile
+  const int N = d.nrs, KL = d.kl, NB = 2 * GD_MAX_KL + 1;
+  const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
+  F += (size_t)blockIdx.y * N * NM;
   double* re = F + j;
   double* im = F + plane + j;
   const int ti = types[j], to = types[NM + j];
@@ -329,7 +349,7 @@ __global__ void k_scalar_bc(Dims d, const double* __restrict__ bv, const int* __
 
 void launch_scalar_bc(cudaStream_t s, const Dims& d, const double* bvals_native, const int* types, const double* d1,
                       const TauConsts& tc, double* F) {
-  k_scalar_bc<<<ceil_div(d.jhi - d.jlo, 128), 128, 0, s>>>(d, bvals_native, types, d1, tc, F);
+  k_scalar_bc<<<dim3(ceil_div(d.jhi - d.jlo, 128), d.nseg), 128, 0, s>>>(d, bvals_native, types, d1, tc, F);
 }
 
 __global__ void k_perm(int nlm, size_t rows, const int* __restrict__ perm, const double* __restrict__ src,

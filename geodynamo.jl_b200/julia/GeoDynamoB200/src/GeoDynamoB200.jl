@@ -25,6 +25,7 @@ struct GDConfig
     dt::Cdouble; implicit_theta::Cdouble
     ab_mode::Cint; bc_mode::Cint; fd_mode::Cint; precision::Cint; magnetic::Cint
     composition::Cint; schmidt::Cdouble
+    segments::Cint
 end
 
 mutable struct Handle
@@ -54,7 +55,7 @@ function handle_for(GD, config, nr::Integer; precision::Integer = 0, composition
     get!(HANDLES, key) do
         cfg = GDConfig(config.lmax, config.mmax, config.nlat, config.nlon, nr, GD.i_KL,
                        GD.d_rratio, GD.d_E, GD.d_Ra, GD.d_Pr, GD.d_Pm, GD.d_timestep, GD.d_implicit,
-                       0, 0, 0, precision, GD.i_B, composition ? 1 : 0, composition ? GD.d_Sc : 1.0)
+                       0, 0, 0, precision, GD.i_B, composition ? 1 : 0, composition ? GD.d_Sc : 1.0, 0)
         create(cfg)
     end
 end

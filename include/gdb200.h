@@ -103,6 +103,14 @@ enum { GD_SCHEME_CNAB2 = 0, GD_SCHEME_EAB2 = 1, GD_SCHEME_ERK2 = 2 };
  * default (create_shtns_composition_field, src/compositional.jl:80-118).  Its
  * buoyancy is a radial force, which the vector analysis does not keep, so C
  * does not act on the velocity.  CNAB2 with bc_mode 0 or 1 only.
+ * segments > 1 stacks that many independent shells of nr / segments levels
+ * each (same grid, diffusivities, dt and modes; their own Ekman numbers through
+ * gd_set_segment_ekman) along r: every per-shell kernel serves them all in one
+ * launch, and the radial operators act within each segment.  The ensemble
+ * groups its members this way.  CNAB2, no composition; the mode-range,
+ * reverse-mode and standalone-operator entry points refuse such a handle
+ * (GD_ERR_UNSUPPORTED).  Boundary values and types apply to every segment;
+ * heat sources are given per shell.  0 or 1: one shell.
  */
 typedef struct gd_config {
   int lmax, mmax, nlat, nlon, nr;
@@ -117,6 +125,7 @@ typedef struct gd_config {
   int magnetic;
   int composition;
   double schmidt;
+  int segments;
 } gd_config;
 
 typedef struct gd_handle gd_handle;
@@ -305,6 +314,10 @@ int gd_download_etd(gd_handle* h, int kind, int l, int which, double* out);
 /* compute_kinetic_energy / compute_magnetic_energy (src/velocity.jl:782-825,
  * src/magnetic.jl:504-543), both as 0.5 sum (T^2+P^2)/max(l(l+1),1). */
 int gd_energy(gd_handle* h, double* ekin, double* emag);
+/* The same per segment of a segmented handle (segments values each; gd_energy
+ * returns their sums).  Each segment's sum runs in the order of an
+ * unsegmented handle of nr / segments levels. */
+int gd_segment_energy(gd_handle* h, double* ekin, double* emag);
 /* Scan the five fields for NaN/Inf; returns GD_ERR_NONFINITE if found. */
 int gd_check_finite(gd_handle* h);
 long gd_step_count(const gd_handle* h);
@@ -467,6 +480,9 @@ int gd_temperature_pullback(gd_handle* h, const double* lam_re, const double* la
  * results do not depend on the cap.  gd_ensemble_autotune chooses the caps of
  * an ensemble's members by measurement. */
 int gd_set_launch_shape(gd_handle* h, int tc_ctas);
+/* Ekman number of each segment (segments values): the Coriolis and Lorentz
+ * factor Pm/E of its shells (rossby_factor, src/velocity.jl:456). */
+int gd_set_segment_ekman(gd_handle* h, const double* ekman);
 /* Kernel launches of the next step: the kernel nodes of its captured CUDA
  * graph (captured here if needed, without running it). */
 int gd_step_kernels(gd_handle* h, int* count);
