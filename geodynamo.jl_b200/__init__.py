@@ -55,7 +55,8 @@ PRECISIONS = {"fp64": 0, "mixed": 1}
 FP64_STAGES = {"vel_synth": 1, "vel_products": 2, "vel_analysis": 4}
 # Named precision settings: the mixed step with its velocity chain in FP64.
 PRECISION_PRESETS = {"mixed_vel64": ("mixed", ("vel_synth", "vel_products", "vel_analysis"))}
-SCHEMES = {"cnab2": 0, "eab2": 1, "erk2": 2}   # ts_scheme (src/simulation.jl:1054-1300)
+SCHEMES = {"cnab2": 0, "eab2": 1, "erk2": 2}
+GEOMETRIES = {"shell": 0, "ball": 1}   # geometry (src/parameters.jl:75)   # ts_scheme (src/simulation.jl:1054-1300)
 ETD_MATRICES = ("E", "phi1", "phi2", "E_half", "phi1_half")   # ERK2Cache fields (src/timestep.jl:830-853)
 KINDS = {"velocity": 0, "magnetic": 1, "temperature": 2}
 
@@ -65,7 +66,8 @@ EXPORTS = (
     "gd_synchronize",
     "gd_upload_spectral", "gd_download_spectral", "gd_download_nonlinear", "gd_download_grid",
     "gd_set_temperature_bc", "gd_spectral_to_physical", "gd_physical_to_spectral", "gd_vector_synthesis",
-    "gd_vector_analysis", "gd_temperature_nonlinear", "gd_velocity_nonlinear", "gd_magnetic_nonlinear",
+    "gd_vector_analysis", "gd_ball_physical_to_spectral", "gd_ball_vector_analysis", "gd_enforce_regularity",
+    "gd_temperature_nonlinear", "gd_velocity_nonlinear", "gd_magnetic_nonlinear",
     "gd_implicit_step", "gd_step", "gd_step_async", "gd_set_dt", "gd_set_scheme", "gd_download_etd",
     "gd_energy", "gd_segment_energy", "gd_set_segment_ekman", "gd_check_finite",
     "gd_step_count", "gd_get_stream", "gd_profile_enable", "gd_profile_read",
@@ -102,7 +104,7 @@ class GDConfig(ctypes.Structure):
         ("ab_mode", ctypes.c_int), ("bc_mode", ctypes.c_int), ("fd_mode", ctypes.c_int),
         ("precision", ctypes.c_int), ("magnetic", ctypes.c_int),
         ("composition", ctypes.c_int), ("schmidt", ctypes.c_double),
-        ("segments", ctypes.c_int),
+        ("segments", ctypes.c_int), ("geometry", ctypes.c_int), ("r_outer", ctypes.c_double),
     ]
 
 
@@ -152,6 +154,9 @@ def load_library():
         "gd_physical_to_spectral": ([P, I, D, D, D], I),
         "gd_vector_synthesis": ([P, D, D, D, D, D, D], I),
         "gd_vector_analysis": ([P, D, D, D, D, D, D], I),
+        "gd_ball_physical_to_spectral": ([P, I, D, D, D], I),
+        "gd_ball_vector_analysis": ([P, D, D, D, D, D, D], I),
+        "gd_enforce_regularity": ([P, I], I),
         "gd_temperature_nonlinear": ([P], I),
         "gd_velocity_nonlinear": ([P], I),
         "gd_magnetic_nonlinear": ([P], I),
@@ -263,13 +268,14 @@ class SHTnsKitConfig:
 
     def __init__(self, lmax, nlat, nlon, nr, mmax=None, kl=4, rratio=0.35, ekman=3e-4, rayleigh=80.0,
                  prandtl=1.0, magnetic_prandtl=4.0, dt=1e-5, implicit_theta=0.5, ab_mode=0, bc_mode=0,
-                 fd_mode=0, precision="fp64", magnetic=1, device=0, composition=0, schmidt=1.0, segments=0):
+                 fd_mode=0, precision="fp64", magnetic=1, device=0, composition=0, schmidt=1.0, segments=0,
+                 geometry="shell", r_outer=1.0):
         self.lib = load_library()
         mmax = lmax if mmax is None else mmax
         base, stages = PRECISION_PRESETS.get(precision, (precision, ()))
         self.cfg = GDConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl, magnetic_prandtl,
                             dt, implicit_theta, ab_mode, bc_mode, fd_mode, PRECISIONS[base], magnetic,
-                            int(composition), float(schmidt), int(segments))
+                            int(composition), float(schmidt), int(segments), GEOMETRIES[geometry], float(r_outer))
         h = ctypes.c_void_p()
         st = self.lib.gd_create(ctypes.byref(self.cfg), int(device), ctypes.byref(h))
         if st != GD_OK:
@@ -420,13 +426,20 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_spectral_to_physical(self.h, nf, _dptr(re), _dptr(im), _dptr(out)))
         return out
 
-    def analysis_scalar(self, grid):
+    def analysis_scalar(self, grid, ball=False):
+        """shtnskit_physical_to_spectral!; ball=True: ball_physical_to_spectral!
+        (the first radial level then 0 for l >= 1)."""
         grid = _f64(grid)
         nf = grid.size // (self.nr * self.nlat * self.nlon)
         shape = ((nf,) + self.spec_shape()) if grid.ndim == 4 else self.spec_shape()
         re = np.zeros(shape); im = np.zeros(shape)
-        self._check(self.lib.gd_physical_to_spectral(self.h, nf, _dptr(grid), _dptr(re), _dptr(im)))
+        fn = self.lib.gd_ball_physical_to_spectral if ball else self.lib.gd_physical_to_spectral
+        self._check(fn(self.h, nf, _dptr(grid), _dptr(re), _dptr(im)))
         return re, im
+
+    def enforce_regularity(self, name):
+        """enforce_ball_scalar_regularity! / enforce_ball_vector_regularity! on a state field."""
+        self._check(self.lib.gd_enforce_regularity(self.h, FIELDS[name]))
 
     def synth_scalar_adjoint(self, grid):
         """Transpose of synth_scalar: grid cotangent -> (re, im) cotangents."""
@@ -498,9 +511,11 @@ class SHTnsKitConfig:
                                                  _dptr(_f64(pim)), _dptr(vt), _dptr(vp)))
         return vt, vp
 
-    def analysis_vector(self, vt, vp):
+    def analysis_vector(self, vt, vp, ball=False):
+        """shtnskit_vector_analysis!; ball=True: ball_vector_analysis!."""
         out = [np.zeros(self.spec_shape()) for _ in range(4)]
-        self._check(self.lib.gd_vector_analysis(self.h, _dptr(_f64(vt)), _dptr(_f64(vp)), *[_dptr(o) for o in out]))
+        fn = self.lib.gd_ball_vector_analysis if ball else self.lib.gd_vector_analysis
+        self._check(fn(self.h, _dptr(_f64(vt)), _dptr(_f64(vp)), *[_dptr(o) for o in out]))
         return out
 
     # -- model state ------------------------------------------------------------
@@ -827,7 +842,7 @@ class Ensemble:
                               c.pop("implicit_theta", 0.5), c.pop("ab_mode", 0), c.pop("bc_mode", 0),
                               c.pop("fd_mode", 0), PRECISIONS[c.pop("precision", precision)],
                               c.pop("magnetic", 1), c.pop("composition", 0), c.pop("schmidt", 1.0),
-                              c.pop("segments", 0))
+                              c.pop("segments", 0), GEOMETRIES[c.pop("geometry", "shell")], c.pop("r_outer", 1.0))
         e = ctypes.c_void_p()
         st = self.lib.gd_ensemble_create(arr, n, int(device), ctypes.byref(e))
         if st != GD_OK:

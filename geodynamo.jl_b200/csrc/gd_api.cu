@@ -50,9 +50,11 @@ int dalloc(gd_handle* h, T** p, size_t n) {
     if (s_) return s_;                         \
   } while (0)
 
-// Entry points built for one shell per handle refuse a segmented handle.
-static int refuse_segments(gd_handle* h, const char* what) {
-  return fail(h, GD_ERR_UNSUPPORTED, std::string(what) + " is not built for a segmented handle");
+// Entry points built for one spherical shell per handle refuse a segmented
+// handle, and those whose operators divide by r, a ball.
+static int refuse_layout(gd_handle* h, const char* what) {
+  return fail(h, GD_ERR_UNSUPPORTED, std::string(what) + " is not built for a " +
+                                         (h->d.ball ? "ball" : "segmented") + " handle");
 }
 
 int check_launch(gd_handle* h, const char* what) {
@@ -140,8 +142,20 @@ void gd::scalar_bc(gd_handle* h, int field) {
   const bool comp = field == F_COMP;
   const size_t NL = h->d.nlm;
   ProfScope p(h, comp ? "composition_bc" : "temperature_bc");
-  launch_scalar_bc(h->stream, h->d, comp ? h->d_cbvals : h->d_bvals, h->d_bctype + (comp ? 2 * NL : 0), h->d_d1, h->tau,
-                   h->field(field));
+  launch_scalar_bc(h->stream, h->d, h->d_lof, comp ? h->d_cbvals : h->d_bvals, h->d_bctype + (comp ? 2 * NL : 0),
+                   h->d_d1, h->tau, h->field(field));
+}
+
+// ball_physical_to_spectral! / ball_vector_analysis! (src/Ball/Ball.jl:214-245)
+// as called from compute_temperature_nonlinear! (src/thermal.jl:177-178),
+// compute_composition_nonlinear! (src/compositional.jl:245-246) and
+// compute_induction_term! (src/magnetic.jl:362-364): regularity on the analysed
+// nonlinear terms.  The induction's spectral curl scales each (l, m, r) alone,
+// so zeroing after it equals zeroing before it.
+void gd::regular_nl(gd_handle* h, int field, int nf) {
+  if (!h->d.ball) return;
+  ProfScope p(h, "ball_regularity");
+  launch_regularity(h->stream, h->d, h->d_lof, h->nlf(field), nf, h->spec_elems());
 }
 
 namespace {
@@ -160,6 +174,7 @@ int setup(gd_handle* h) {
   d.nrs = d.nr / d.nseg;
   d.rfs = nullptr;
   d.rfs32 = nullptr;
+  d.ball = c.geometry == GD_GEOM_BALL;
   h->moff.assign(d.M + 2, 0);
   for (int m = 0; m <= d.M; ++m) h->moff[m + 1] = h->moff[m] + (d.L - m + 1);
   h->perm.resize(d.nlm);
@@ -204,9 +219,13 @@ int setup(gd_handle* h) {
   std::vector<double> r(NR), ri(NR), ri2(NR);
   const double rin = c.rratio / (1.0 - c.rratio);
   const double kPi = 3.14159265358979323846;
-  // one segment's nodes, repeated for every segment
+  // one segment's nodes, repeated for every segment.  Ball: the same cosine
+  // nodes on [0, R] (create_ball_radial_domain, src/Ball/Ball.jl:34-71), r_1 = 0
   const int NS = d.nrs;
-  for (int n = 1; n <= NS; ++n) r[n - 1] = 0.5 * (1.0 + std::cos(kPi * (double)(NS - n) / (double)(NS - 1))) + rin;
+  for (int n = 1; n <= NS; ++n) {
+    const double x = 0.5 * (1.0 + std::cos(kPi * (double)(NS - n) / (double)(NS - 1)));
+    r[n - 1] = d.ball ? (c.r_outer != 1.0 ? x * c.r_outer : x) : x + rin;
+  }
   for (int n = NS; n < d.nr; ++n) r[n] = r[n % NS];
   for (int n = 0; n < d.nr; ++n) { ri[n] = std::pow(r[n], -1.0); ri2[n] = std::pow(r[n], -2.0); }
   CK(cudaMemcpyAsync(h->d_r, r.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
@@ -335,6 +354,7 @@ int temperature_nl_fp64(gd_handle* h) {
   double* out[1] = {h->nlf(F_TEMP)};
   s = analysis_scalar(h, h->grid(GD_GRID_TADV), 1, out);
   if (s) return s;
+  regular_nl(h, F_TEMP, 1);
   if (!h->ext_derivs) scalar_bc(h, F_TEMP);
   return check_launch(h, "temperature nonlinear");
 }
@@ -363,6 +383,7 @@ int composition_nl_fp64(gd_handle* h) {
   double* out[1] = {h->nlf(F_COMP)};
   s = analysis_scalar(h, h->grid(GD_GRID_CADV), 1, out);
   if (s) return s;
+  regular_nl(h, F_COMP, 1);
   if (!h->ext_derivs) scalar_bc(h, F_COMP);
   return check_launch(h, "composition nonlinear");
 }
@@ -401,7 +422,10 @@ int magnetic_nl_fp64(gd_handle* h) {
   { ProfScope p(h, "nl_induction_fp64");
     launch_induction<double>(h->stream, d, h->grid(GD_GRID_U_TH), h->grid(GD_GRID_U_PH), h->grid(GD_GRID_B_TH),
                              h->grid(GD_GRID_B_PH), h->grid(GD_GRID_IND_TH), h->grid(GD_GRID_IND_PH)); }
-  return analysis_vector(h, h->grid(GD_GRID_IND_TH), h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
+  s = analysis_vector(h, h->grid(GD_GRID_IND_TH), h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
+  if (s) return s;
+  regular_nl(h, F_BTOR, 2);
+  return check_launch(h, "magnetic nonlinear");
 }
 
 ExpApply exp_apply_args(gd_handle* h, const Cnab2Args& a) {
@@ -656,7 +680,10 @@ bool valid_config(const gd_config* c, std::string& why) {
   if (c->kl != GD_MAX_KL) { why = "kl must be 4 (i_KL)"; return false; }
   if (!(c->dt > 0.0)) { why = "dt must be positive"; return false; }
   if (c->ekman == 0.0) { why = "Ekman number must be nonzero (src/velocity.jl:450-452)"; return false; }
-  if (c->rratio <= 0.0 || c->rratio >= 1.0) { why = "rratio must lie in (0, 1)"; return false; }
+  if (c->geometry != GD_GEOM_BALL && (c->rratio <= 0.0 || c->rratio >= 1.0)) {
+    why = "rratio must lie in (0, 1)";
+    return false;
+  }
   if (c->bc_mode < 0 || c->bc_mode > 2) { why = "bc_mode must be 0, 1 or 2"; return false; }
   if (c->ab_mode < 0 || c->ab_mode > 1) { why = "ab_mode must be 0 or 1"; return false; }
   if (c->fd_mode < 0 || c->fd_mode > 1) { why = "fd_mode must be 0 or 1"; return false; }
@@ -667,6 +694,15 @@ bool valid_config(const gd_config* c, std::string& why) {
   if (c->segments < 0 || (c->segments > 1 && c->nr % c->segments)) { why = "segments must divide nr"; return false; }
   if (c->segments > 1 && c->nr / c->segments < 3) { why = "each segment needs at least 3 levels"; return false; }
   if (c->segments > 1 && c->composition) { why = "segments carry no composition"; return false; }
+  if (c->geometry != GD_GEOM_SHELL && c->geometry != GD_GEOM_BALL) { why = "geometry must be GD_GEOM_SHELL or GD_GEOM_BALL"; return false; }
+  if (c->geometry == GD_GEOM_BALL) {
+    if (!(c->r_outer > 0.0)) { why = "r_outer must be > 0 for ball geometry"; return false; }
+    if (c->bc_mode != 2) {
+      why = "ball geometry needs bc_mode 2: the literal operator holds 1/r and 1/r^2 at r = 0";
+      return false;
+    }
+    if (c->composition) { why = "ball geometry carries no composition (bc_mode 2 has no composition rows)"; return false; }
+  }
   return true;
 }
 
@@ -754,7 +790,7 @@ int gd_set_fp64_stages(gd_handle* h, int mask) {
 
 int gd_set_external_derivatives(gd_handle* h, int enable) {
   if (!h) return GD_ERR_ARG;
-  if (enable && h->d.nseg > 1) return refuse_segments(h, "the distributed step");
+  if (enable && (h->d.nseg > 1 || h->d.ball)) return refuse_layout(h, "the distributed step");
   CK(cudaSetDevice(h->device));
   if ((enable != 0) != h->ext_derivs) drop_graphs(h);
   h->ext_derivs = enable != 0;
@@ -785,7 +821,7 @@ int gd_temperature_forward(gd_handle* h, int nsteps, int checkpoint_every) {
   if (!h || nsteps < 1 || checkpoint_every < 1) return h ? fail(h, GD_ERR_ARG, "need nsteps, checkpoint_every >= 1") : GD_ERR_ARG;
   if (h->precision != GD_PREC_FP64 || h->scheme != GD_SCHEME_CNAB2)
     return fail(h, GD_ERR_UNSUPPORTED, "the temperature pullback is of the FP64 CNAB2 step");
-  if (h->d.nseg > 1) return refuse_segments(h, "the temperature pullback");
+  if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "the temperature pullback");
   CK(cudaSetDevice(h->device));
   free_tckpt(h);
   size_t nb = 0;
@@ -1024,7 +1060,7 @@ int gd_grid_device(gd_handle* h, int grid, double* dev) {
 
 int gd_temperature_nl_adjoint(gd_handle* h, const double* u_th, const double* u_ph, const double* nu, double* out) {
   if (!h || !u_th || !u_ph || !nu || !out) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
-  if (h->d.nseg > 1) return refuse_segments(h, "the nonlinear-term adjoint");
+  if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "the nonlinear-term adjoint");
   CK(cudaSetDevice(h->device));
   const size_t se = h->spec_elems(), G = h->grid_elems();
   if (!h->d_adj) AL(h->d_adj, 3 * se + 3 * G);
@@ -1058,7 +1094,7 @@ int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double*
   if (!h || !x || !y || (mode != 0 && mode != 1) || field < 0 || field >= nfields(h))
     return h ? fail(h, GD_ERR_ARG, "bad field, mode or pointer") : GD_ERR_ARG;
   if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the adjoint is of the CNAB2 step");
-  if (h->d.nseg > 1) return refuse_segments(h, "the CNAB2 adjoint");
+  if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "the CNAB2 adjoint");
   const size_t NL = h->d.nlm;
   const bool scalar = field == GD_TEMP || field == GD_COMP;
   const int kind = field == GD_TEMP ? 2 : field == GD_COMP ? 3 : (field == GD_U_TOR || field == GD_U_POL) ? 0 : 1;
@@ -1082,7 +1118,7 @@ int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double*
 
 int gd_derivatives(gd_handle* h, int j0, int j1) {
   if (!h) return GD_ERR_ARG;
-  if (h->d.nseg > 1) return refuse_segments(h, "the mode-range derivatives");
+  if (h->d.nseg > 1) return refuse_layout(h, "the mode-range derivatives");
   if (!mode_range_ok(h, j0, j1)) return fail(h, GD_ERR_ARG, "mode range outside [0, nlm]");
   CK(cudaSetDevice(h->device));
   if (j1 == j0) return GD_OK;
@@ -1111,7 +1147,7 @@ int gd_derivatives(gd_handle* h, int j0, int j1) {
 
 int gd_implicit_modes(gd_handle* h, int j0, int j1) {
   if (!h) return GD_ERR_ARG;
-  if (h->d.nseg > 1) return refuse_segments(h, "the mode-range solve");
+  if (h->d.nseg > 1) return refuse_layout(h, "the mode-range solve");
   if (!mode_range_ok(h, j0, j1)) return fail(h, GD_ERR_ARG, "mode range outside [0, nlm]");
   if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the mode-range solve supports CNAB2 only");
   CK(cudaSetDevice(h->device));
@@ -1270,7 +1306,16 @@ int gd_spectral_to_physical(gd_handle* h, int nfield, const double* re, const do
   return check_launch(h, "spectral_to_physical");
 }
 
-int gd_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double* re, double* im) {
+// The r = 0 level (the first of each segment) of nf spectral fields, stride
+// fstride, set to 0 for l >= 1 whatever the geometry, as the reference's
+// enforce_ball_*_regularity! do (src/Ball/Ball.jl:153-195).
+static void zero_first_level(gd_handle* h, double* F, int nf, size_t fstride) {
+  Dims dz = h->d;
+  dz.ball = 1;
+  launch_regularity(h->stream, dz, h->d_lof, F, nf, fstride);
+}
+
+static int physical_to_spectral(gd_handle* h, int nfield, const double* grid, double* re, double* im, bool regular) {
   if (!h || !re || !im || !grid || nfield < 1) return h ? fail(h, GD_ERR_ARG, "bad arguments") : GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
   int s = stage_alloc(h);
@@ -1285,6 +1330,7 @@ int gd_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double
     if (h->precision == GD_PREC_MIXED) s = mixed_api_analysis_scalar(h, h->d_stage_grid2, nf, out);
     else s = analysis_scalar(h, h->d_stage_grid2, nf, out);
     if (s) return s;
+    if (regular) zero_first_level(h, h->d_stage_spec2, nf, 2 * plane);
     launch_native_to_lmajor(h->stream, h->d, h->d_perm, h->d_stage_spec2, h->d_stage_spec, 2 * nf);
     for (int i = 0; i < nf; ++i) {
       CK(cudaMemcpyAsync(re + plane * (f0 + i), h->d_stage_spec + 2 * plane * i, plane * sizeof(double),
@@ -1295,6 +1341,24 @@ int gd_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double
     CK(cudaStreamSynchronize(h->stream));
   }
   return check_launch(h, "physical_to_spectral");
+}
+
+int gd_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double* re, double* im) {
+  return physical_to_spectral(h, nfield, grid, re, im, false);
+}
+
+int gd_ball_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double* re, double* im) {
+  return physical_to_spectral(h, nfield, grid, re, im, true);
+}
+
+int gd_enforce_regularity(gd_handle* h, int field) {
+  if (!h || field < 0 || field >= nfields(h)) return h ? fail(h, GD_ERR_ARG, "bad field") : GD_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  zero_first_level(h, h->field(field), 1, 0);
+  int s = check_launch(h, "enforce regularity");
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
 }
 
 int gd_spectral_to_physical_adjoint(gd_handle* h, int nfield, const double* grid, double* re, double* im) {
@@ -1332,7 +1396,7 @@ int gd_magnetic_pullback(gd_handle* h, int field, int nsteps, const double* lam_
   if (!h || !lam_re || !lam_im || !out_re || !out_im || nsteps < 0 || (field != GD_B_TOR && field != GD_B_POL))
     return h ? fail(h, GD_ERR_ARG, "bad arguments (field must be GD_B_TOR or GD_B_POL)") : GD_ERR_ARG;
   if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the pullback is of the CNAB2 propagator");
-  if (h->d.nseg > 1) return refuse_segments(h, "the magnetic pullback");
+  if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "the magnetic pullback");
   CK(cudaSetDevice(h->device));
   int s = stage_alloc(h);
   if (s) return s;
@@ -1375,8 +1439,8 @@ int gd_vector_synthesis(gd_handle* h, const double* tor_re, const double* tor_im
   return check_launch(h, "vector synthesis");
 }
 
-int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re, double* tor_im,
-                       double* pol_re, double* pol_im) {
+static int vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re, double* tor_im,
+                           double* pol_re, double* pol_im, bool regular) {
   if (!h || !tor_re || !tor_im || !pol_re || !pol_im || !v_theta || !v_phi)
     return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
   CK(cudaSetDevice(h->device));
@@ -1391,12 +1455,23 @@ int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi,
   if (h->precision == GD_PREC_MIXED) s = mixed_api_analysis_vector(h, h->d_stage_grid2, tor, pol);
   else s = analysis_vector(h, h->d_stage_grid2, tor, pol, EPI_VECTOR);
   if (s) return s;
+  if (regular) zero_first_level(h, tor, 2, 2 * plane);
   launch_native_to_lmajor(h->stream, h->d, h->d_perm, h->d_stage_spec2, h->d_stage_spec, 4);
   double* dst[4] = {tor_re, tor_im, pol_re, pol_im};
   for (int i = 0; i < 4; ++i)
     CK(cudaMemcpyAsync(dst[i], h->d_stage_spec + plane * i, plane * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return check_launch(h, "vector analysis");
+}
+
+int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re, double* tor_im,
+                       double* pol_re, double* pol_im) {
+  return vector_analysis(h, v_theta, v_phi, tor_re, tor_im, pol_re, pol_im, false);
+}
+
+int gd_ball_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re, double* tor_im,
+                            double* pol_re, double* pol_im) {
+  return vector_analysis(h, v_theta, v_phi, tor_re, tor_im, pol_re, pol_im, true);
 }
 
 // ---- the reference's argument lists on host arrays ----
@@ -1439,7 +1514,7 @@ int gd_create_timestepping_matrices(gd_handle* h, double diffusivity, double dt,
   if (!h || !out) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
   if (!(dt > 0.0) || !std::isfinite(diffusivity) || !std::isfinite(theta))
     return fail(h, GD_ERR_ARG, "need dt > 0 and finite diffusivity and theta");
-  if (h->d.nseg > 1) return refuse_segments(h, "a standalone timestepping operator");
+  if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "a standalone timestepping operator");
   CK(cudaSetDevice(h->device));
   const Dims& d = h->d;
   const size_t n = (size_t)d.nr * (2 * d.kl + 1) * (d.L + 1);
@@ -1693,7 +1768,7 @@ int gd_set_scheme(gd_handle* h, int scheme) {
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   if (scheme != GD_SCHEME_CNAB2) {
-    if (h->d.nseg > 1) return refuse_segments(h, "an exponential scheme");
+    if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "an exponential scheme");
     if (h->c.composition)
       return fail(h, GD_ERR_UNSUPPORTED, "the exponential schemes are not built for composition (CNAB2 only)");
     if (h->c.bc_mode == 2)

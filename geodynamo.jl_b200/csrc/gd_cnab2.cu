@@ -92,7 +92,8 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
       vr += a.lin_weight * Lr;
       vi += a.lin_weight * Li;
       if (rows && (i == 0 || i == N - 1)) {
-        vr = is_temp ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
+        // ball: the r = 0 row of l >= 1 is the regularity condition (value 0)
+        vr = (is_temp && !(d.ball && i == 0 && l > 0)) ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
         vi = 0.0;
       }
       ure[at] = vr;

@@ -45,6 +45,8 @@ struct Dims {
   int nseg, nrs;
   const double* rfs;
   const float* rfs32;
+  // ball geometry: the first level of each segment is r = 0
+  int ball;
 };
 
 // Analysis epilogue variants.
@@ -143,8 +145,10 @@ struct TauConsts {
 // Boundary conditions of a scalar field for the modes [jlo, jhi): fixed-value
 // rows, then the tau correction of the modes with a flux boundary.
 // types: [inner, outer][nlm] GD_BC_* (native order); bvals [2][nlm] values or fluxes.
-void launch_scalar_bc(cudaStream_t s, const Dims& d, const double* bvals_native, const int* types,
+void launch_scalar_bc(cudaStream_t s, const Dims& d, const int* lof, const double* bvals_native, const int* types,
                       const double* d1, const TauConsts& tc, double* F);
+// ball: r = 0 level of nf fields (stride fstride doubles) set to 0 for l >= 1
+void launch_regularity(cudaStream_t s, const Dims& d, const int* lof, double* F, int nf, size_t fstride);
 void launch_lmajor_to_native(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,
                              double* dst, int nplanes);
 void launch_native_to_lmajor(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,

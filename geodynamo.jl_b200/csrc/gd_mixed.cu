@@ -402,6 +402,7 @@ int mixed_temperature_nl(gd_handle* h) {
   double* out[1] = {h->nlf(F_TEMP)};
   s = tc_analysis_scalar_G(h, 1, out);
   if (s) return s;
+  regular_nl(h, F_TEMP, 1);
   if (!h->ext_derivs) scalar_bc(h, F_TEMP);
   return launched(h, "mixed temperature nonlinear");
 }
@@ -433,6 +434,7 @@ int mixed_composition_nl(gd_handle* h) {
   double* out[1] = {h->nlf(F_COMP)};
   s = tc_analysis_scalar_G(h, 1, out);
   if (s) return s;
+  regular_nl(h, F_COMP, 1);
   if (!h->ext_derivs) scalar_bc(h, F_COMP);
   return launched(h, "mixed composition nonlinear");
 }
@@ -560,7 +562,10 @@ int mixed_magnetic_nl(gd_handle* h) {
   { ProfScope p(h, "fused_induction_fp32"); launch_fused(h->stream, d, h->plan, h->d_twf, FUSED_INDUCTION, f); }
   s = launched(h, "fused induction phase");
   if (s) return s;
-  return tc_analysis_vector_G(h, h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
+  s = tc_analysis_vector_G(h, h->nlf(F_BTOR), h->nlf(F_BPOL), EPI_CURL_INDUCTION);
+  if (s) return s;
+  regular_nl(h, F_BTOR, 2);
+  return launched(h, "ball regularity");
 }
 
 // Grid download in the mixed path: synthesized components are transformed

@@ -22,6 +22,8 @@ int mixed_composition_nl(gd_handle* h);
 // Boundary conditions (fixed values, tau flux correction) of F_TEMP or F_COMP
 // over the handle's mode range (gd_api.cu).
 void scalar_bc(gd_handle* h, int field);
+// ball: the r = 0 level of nf consecutive nonlinear terms from field set to 0 for l >= 1
+void regular_nl(gd_handle* h, int field, int nf);
 int mixed_velocity_nl(gd_handle* h);
 int mixed_magnetic_nl(gd_handle* h);
 // GD_ERR_UNSUPPORTED for the product grids, which the mixed step does not store.

@@ -149,7 +149,9 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
       di += Am * T[plane + at - 1];
     }
     const double ri = rinv[k];
-    const double v[4] = {dr * ri, di * ri, (-(double)m * T[plane + at]) * ri, ((double)m * T[at]) * ri};
+    double v[4] = {dr * ri, di * ri, (-(double)m * T[plane + at]) * ri, ((double)m * T[at]) * ri};
+    // ball: the angular components stay 0 at r = 0 (src/scalar_field_common.jl:300-310)
+    if (d.ball && k == 0) v[0] = v[1] = v[2] = v[3] = 0.0;
     if (IMG) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -250,8 +252,11 @@ __global__ void __launch_bounds__(RAD_THREADS, 4) k_curl(Dims d, const int* __re
         }
       }
       const size_t at = (size_t)k * NM + j;
-      const double vt = lf * st.rv[1][b] * st.win[c][b + KL][tid] - a2 - 2.0 * st.rv[0][b] * a1;
-      const double vp = -lf * st.rv[1][b] * tv[c][b];
+      double vt = lf * st.rv[1][b] * st.win[c][b + KL][tid] - a2 - 2.0 * st.rv[0][b] * a1;
+      double vp = -lf * st.rv[1][b] * tv[c][b];
+      // ball: both components are set to 0 at r = 0 (src/velocity.jl:417-422,
+      // src/magnetic.jl:325-330)
+      if (d.ball && k == 0) vt = vp = 0.0;
       if (IMG) {
         const int kg = base + k;  // column tiles run over all shells
         const int col = (kg & 31) * 4 + c;
@@ -297,8 +302,9 @@ void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* m
 // the real profile at each flux boundary (prescribed - (D1 Re)[boundary]),
 // coefficients of the tau functions that cancel it, and the same correction
 // added to Re and, when any |Im| exceeds 1e-12, to Im.
-__global__ void k_scalar_bc(Dims d, const double* __restrict__ bv, const int* __restrict__ types,
-                            const double* __restrict__ d1, TauConsts tc, double* __restrict__ F) {
+__global__ void k_scalar_bc(Dims d, const int* __restrict__ lof, const double* __restrict__ bv,
+                            const int* __restrict__ types, const double* __restrict__ d1, TauConsts tc,
+                            double* __restrict__ F) {
   const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.jhi) return;
   // segment blockIdx.y: its own boundary rows and radial profile
@@ -307,11 +313,17 @@ __global__ void k_scalar_bc(Dims d, const double* __restrict__ bv, const int* __
   F += (size_t)blockIdx.y * N * NM;
   double* re = F + j;
   double* im = F + plane + j;
-  const int ti = types[j], to = types[NM + j];
+  // ball: no inner boundary at r = 0 (src/thermal.jl:281-282); regularity
+  // after the boundary rows (src/thermal.jl:310-312, src/Ball/Ball.jl:153-170)
+  const int ti = d.ball ? -1 : types[j], to = types[NM + j];
+  const bool regular = d.ball && lof[j] > 0;
   if (ti == GD_BC_VALUE) { re[0] = bv[j]; im[0] = 0.0; }
   if (to == GD_BC_VALUE) { re[(size_t)(N - 1) * NM] = bv[NM + j]; im[(size_t)(N - 1) * NM] = 0.0; }
   const bool fi = ti == GD_BC_FLUX, fo = to == GD_BC_FLUX;
-  if (!fi && !fo) return;
+  if (!fi && !fo) {
+    if (regular) re[0] = im[0] = 0.0;
+    return;
+  }
   // boundary fluxes of the real profile: rows 0 and N - 1 of the banded D1
   // (entry (i, col) at d1[(i - col + KL) + NB col])
   double qi = 0.0, qo = 0.0;
@@ -345,11 +357,29 @@ __global__ void k_scalar_bc(Dims d, const double* __restrict__ bv, const int* __
     re[(size_t)i * NM] = __dadd_rn(re[(size_t)i * NM], corr);
     if (im_live) im[(size_t)i * NM] = __dadd_rn(im[(size_t)i * NM], corr);
   }
+  if (regular) re[0] = im[0] = 0.0;
 }
 
-void launch_scalar_bc(cudaStream_t s, const Dims& d, const double* bvals_native, const int* types, const double* d1,
-                      const TauConsts& tc, double* F) {
-  k_scalar_bc<<<dim3(ceil_div(d.jhi - d.jlo, 128), d.nseg), 128, 0, s>>>(d, bvals_native, types, d1, tc, F);
+// enforce_ball_scalar_regularity! / enforce_ball_vector_regularity!
+// (src/Ball/Ball.jl:153-195): the r = 0 level (the first of every segment) of
+// each of nf fields is set to 0 for l >= 1.
+__global__ void k_regularity(Dims d, const int* __restrict__ lof, double* __restrict__ F, int nf, size_t fstride) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.nlm || lof[j] < 1) return;
+  const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
+  double* f = F + blockIdx.z * fstride + (size_t)blockIdx.y * d.nrs * NM + j;
+  f[0] = 0.0;
+  f[plane] = 0.0;
+}
+
+void launch_regularity(cudaStream_t s, const Dims& d, const int* lof, double* F, int nf, size_t fstride) {
+  if (!d.ball || nf < 1) return;
+  k_regularity<<<dim3(ceil_div(d.nlm, 128), d.nseg, nf), 128, 0, s>>>(d, lof, F, nf, fstride);
+}
+
+void launch_scalar_bc(cudaStream_t s, const Dims& d, const int* lof, const double* bvals_native, const int* types,
+                      const double* d1, const TauConsts& tc, double* F) {
+  k_scalar_bc<<<dim3(ceil_div(d.jhi - d.jlo, 128), d.nseg), 128, 0, s>>>(d, lof, bvals_native, types, d1, tc, F);
 }
 
 __global__ void k_perm(int nlm, size_t rows, const int* __restrict__ perm, const double* __restrict__ src,

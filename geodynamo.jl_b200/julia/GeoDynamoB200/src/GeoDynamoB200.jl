@@ -25,7 +25,7 @@ struct GDConfig
     dt::Cdouble; implicit_theta::Cdouble
     ab_mode::Cint; bc_mode::Cint; fd_mode::Cint; precision::Cint; magnetic::Cint
     composition::Cint; schmidt::Cdouble
-    segments::Cint
+    segments::Cint; geometry::Cint; r_outer::Cdouble
 end
 
 mutable struct Handle
@@ -53,9 +53,13 @@ const HANDLES = Dict{Tuple{UInt,Int,Int},Handle}()
 function handle_for(GD, config, nr::Integer; precision::Integer = 0, composition::Bool = false)
     key = (objectid(config), Int(nr), Int(precision) + 2 * Int(composition))
     get!(HANDLES, key) do
+        # a ball (geometry = :ball) steps with the boundary-row operator (bc_mode 2):
+        # the reference's own operator holds 1/r at r = 0
+        ball = GD.geometry === :ball
         cfg = GDConfig(config.lmax, config.mmax, config.nlat, config.nlon, nr, GD.i_KL,
                        GD.d_rratio, GD.d_E, GD.d_Ra, GD.d_Pr, GD.d_Pm, GD.d_timestep, GD.d_implicit,
-                       0, 0, 0, precision, GD.i_B, composition ? 1 : 0, composition ? GD.d_Sc : 1.0, 0)
+                       0, ball ? 2 : 0, 0, precision, GD.i_B, composition ? 1 : 0, composition ? GD.d_Sc : 1.0, 0,
+                       ball ? 1 : 0, ball ? GD.d_R_outer : 1.0)
         create(cfg)
     end
 end

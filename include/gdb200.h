@@ -82,6 +82,8 @@ enum {
  * EAB2 (eab2_update! with the exponential cache of create_etd_cache) or ERK2
  * (erk2_integrate_full_step! with the cache of create_erk2_cache). */
 enum { GD_SCHEME_CNAB2 = 0, GD_SCHEME_EAB2 = 1, GD_SCHEME_ERK2 = 2 };
+/* geometry (src/parameters.jl:75): a spherical shell or a solid ball */
+enum { GD_GEOM_SHELL = 0, GD_GEOM_BALL = 1 };
 
 /*
  * Model configuration.  Mirrors GeoDynamoParameters (src/parameters.jl:14-76):
@@ -111,6 +113,19 @@ enum { GD_SCHEME_CNAB2 = 0, GD_SCHEME_EAB2 = 1, GD_SCHEME_ERK2 = 2 };
  * reverse-mode and standalone-operator entry points refuse such a handle
  * (GD_ERR_UNSUPPORTED).  Boundary values and types apply to every segment;
  * heat sources are given per shell.  0 or 1: one shell.
+ * geometry GD_GEOM_BALL is the solid sphere of GeoDynamoBall
+ * (src/Ball/Ball.jl): cosine nodes on [0, r_outer] (r_outer = d_R_outer,
+ * rratio unused), the angular gradient and both curl components 0 at r = 0
+ * (src/scalar_field_common.jl:300-310, src/velocity.jl:417-422,
+ * src/magnetic.jl:325-330), regularity (the r = 0 level 0 for l >= 1) on the
+ * analysed temperature and induction terms and on the temperature after its
+ * boundary rows, no inner boundary row at r = 0 (src/thermal.jl:281-312).
+ * The reference's implicit operator holds 1/r and 1/r^2 at r = 0 (infinite;
+ * 0 x inf at l = 0), so a ball needs bc_mode 2, whose r = 0 row is the
+ * regularity condition for l >= 1 and the inner boundary value for the l = 0
+ * temperature; CNAB2, no composition, no flux boundaries.  Entry points whose
+ * operators divide by r (reverse mode, exponential schemes, the standalone
+ * timestepping operator, the distributed step) refuse a ball.
  */
 typedef struct gd_config {
   int lmax, mmax, nlat, nlon, nr;
@@ -126,6 +141,8 @@ typedef struct gd_config {
   int composition;
   double schmidt;
   int segments;
+  int geometry;
+  double r_outer;
 } gd_config;
 
 typedef struct gd_handle gd_handle;
@@ -195,6 +212,16 @@ int gd_vector_synthesis(gd_handle* h, const double* tor_re, const double* tor_im
 /* shtnskit_vector_analysis!(vec, tor, pol) (src/shtnskit_field_functions.jl:291-321). */
 int gd_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re,
                        double* tor_im, double* pol_re, double* pol_im);
+/* ball_physical_to_spectral! / ball_vector_analysis! (src/Ball/Ball.jl:214-245):
+ * the analyses above, then the first radial level set to 0 for l >= 1 (as the
+ * reference does, whatever the geometry). */
+int gd_ball_physical_to_spectral(gd_handle* h, int nfield, const double* grid, double* re, double* im);
+int gd_ball_vector_analysis(gd_handle* h, const double* v_theta, const double* v_phi, double* tor_re,
+                            double* tor_im, double* pol_re, double* pol_im);
+/* enforce_ball_scalar_regularity! / enforce_ball_vector_regularity!
+ * (src/Ball/Ball.jl:153-195) on a state field (GD_U_TOR .. GD_COMP): its first
+ * radial level set to 0 for l >= 1. */
+int gd_enforce_regularity(gd_handle* h, int field);
 
 /* No counterpart in the reference.  Scalar synthesis (as
  * gd_spectral_to_physical, but always in FP64, whatever the handle's

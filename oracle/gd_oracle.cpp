@@ -79,6 +79,9 @@ typedef struct oc_config {
   int magnetic;    // i_B
   int composition; // include_composition
   double schmidt;  // d_Sc
+  int segments;    // ignored by the oracle (one shell per oracle)
+  int geometry;    // 0 shell, 1 ball (src/parameters.jl:75)
+  double r_outer;  // d_R_outer of the ball
 } oc_config;
 }
 
@@ -333,12 +336,17 @@ struct Oracle {
   }
 
   // Radial grid (fields.jl:108-131) and banded operators (linear_algebra.jl:90-151).
+  // Ball: create_ball_radial_domain (Ball/Ball.jl:34-71), the same cosine
+  // nodes on [0, 1] scaled by d_R_outer when it is not 1; r^-1 and r^-2 are
+  // infinite at r = 0 as in the reference's r[:, 3] and r[:, 2].
+  bool ball() const { return c.geometry == 1; }
   void radial() {
     const int N = c.nr;
     r.assign(N, 0); rinv.assign(N, 0); rinv2.assign(N, 0);
     const double ri = c.rratio / (1.0 - c.rratio);
     for (int n = 1; n <= N; ++n) {
-      r[n - 1] = 0.5 * (1.0 + std::cos(kPi * (double)(N - n) / (double)(N - 1))) + ri;
+      const double x = 0.5 * (1.0 + std::cos(kPi * (double)(N - n) / (double)(N - 1)));
+      r[n - 1] = ball() ? (c.r_outer != 1.0 ? x * c.r_outer : x) : x + ri;
     }
     for (int n = 0; n < N; ++n) { rinv[n] = std::pow(r[n], -1.0); rinv2[n] = std::pow(r[n], -2.0); }
     d1 = fd_matrix(1);
@@ -679,6 +687,10 @@ struct Oracle {
         gt_im[(size_t)k * nlm + q] = di * ri_;
         gp_re[(size_t)k * nlm + q] = (-(double)m * im[(size_t)k * nlm + q]) * ri_;
         gp_im[(size_t)k * nlm + q] = ((double)m * re[(size_t)k * nlm + q]) * ri_;
+        if (r[k] == 0.0) {  // r = 0: angular gradient left zero (scalar_field_common.jl:300-310)
+          gt_re[(size_t)k * nlm + q] = gt_im[(size_t)k * nlm + q] = 0.0;
+          gp_re[(size_t)k * nlm + q] = gp_im[(size_t)k * nlm + q] = 0.0;
+        }
         double sr = 0, si = 0;
         for (int j = std::max(0, k - bw); j <= std::min(N - 1, k + bw); ++j) {
           const double cf = d1[(bw + k - j) + (size_t)nbw * j];
@@ -707,6 +719,11 @@ struct Oracle {
       band_apply(d2.data(), pi.data(), d2i.data());
       (void)bw;
       for (int k = 0; k < N; ++k) {
+        if (r[k] == 0.0) {  // r = 0 (velocity.jl:417-422, magnetic.jl:325-330)
+          otre[(size_t)k * nlm + q] = otim[(size_t)k * nlm + q] = 0.0;
+          opre[(size_t)k * nlm + q] = opim[(size_t)k * nlm + q] = 0.0;
+          continue;
+        }
         otre[(size_t)k * nlm + q] = lf * rinv2[k] * pr[k] - d2r[k] - 2.0 * rinv[k] * d1r[k];
         otim[(size_t)k * nlm + q] = lf * rinv2[k] * pi[k] - d2i[k] - 2.0 * rinv[k] * d1i[k];
         opre[(size_t)k * nlm + q] = -lf * rinv2[k] * tre[(size_t)k * nlm + q];
@@ -742,8 +759,17 @@ struct Oracle {
       }
     }
     analysis_scalar(tadv.data(), nre[F_TEMP].data(), nim[F_TEMP].data());
+    // ball_physical_to_spectral! (thermal.jl:177-178)
+    if (ball()) regularity(nre[F_TEMP].data(), nim[F_TEMP].data());
     // apply_temperature_boundary_conditions_spectral! (thermal.jl:262-303): on the state.
     scalar_bc(F_TEMP, bvals, tbc);
+  }
+
+  // enforce_ball_scalar_regularity! / enforce_ball_vector_regularity!
+  // (Ball/Ball.jl:153-195): the inner radial level set to 0 for l >= 1.
+  void regularity(double* re, double* im) const {
+    for (int q = 0; q < nlm; ++q)
+      if (lv[q] > 0) { re[q] = 0.0; im[q] = 0.0; }
   }
 
   // Boundary conditions of a scalar field on its state: fixed values
@@ -776,7 +802,8 @@ struct Oracle {
     for (int i = 0; i < N; ++i) { t1[i] = cheb(N - 1, r[i]); t2[i] = cheb(N, r[i]); }
     const double d1i = dcheb(N - 1, ri), d1o = dcheb(N - 1, ro), d2i = dcheb(N, ri), d2o = dcheb(N, ro);
     for (int q = 0; q < nlm; ++q) {
-      const int ti = types[q], to = types[(size_t)nlm + q];
+      // ball: no inner row at r = 0 (thermal.jl:281-282)
+      const int ti = ball() ? -1 : types[q], to = types[(size_t)nlm + q];
       if (ti == BC_VALUE) { fre[f][q] = bv[q]; fim[f][q] = 0.0; }
       if (to == BC_VALUE) {
         fre[f][(size_t)(N - 1) * nlm + q] = bv[(size_t)nlm + q];
@@ -784,7 +811,7 @@ struct Oracle {
       }
     }
     for (int q = 0; q < nlm; ++q) {
-      const bool ai = types[q] == BC_FLUX, ao = types[(size_t)nlm + q] == BC_FLUX;
+      const bool ai = !ball() && types[q] == BC_FLUX, ao = types[(size_t)nlm + q] == BC_FLUX;
       if (!ai && !ao) continue;
       std::vector<double> pr(N), pi(N), dp(N);
       for (int k = 0; k < N; ++k) { pr[k] = fre[f][(size_t)k * nlm + q]; pi[k] = fim[f][(size_t)k * nlm + q]; }
@@ -815,6 +842,9 @@ struct Oracle {
         if (im_live) fim[f][(size_t)k * nlm + q] = pi[k] + corr[k];
       }
     }
+    // apply_ball_temperature_regularity! / _composition_ (thermal.jl:310-312,
+    // compositional.jl:368-370)
+    if (ball()) regularity(fre[f].data(), fim[f].data());
   }
 
   // compute_composition_nonlinear! (compositional.jl:219-259): as the
@@ -842,6 +872,7 @@ struct Oracle {
       }
     }
     analysis_scalar(cadv.data(), nre[F_COMP].data(), nim[F_COMP].data());
+    if (ball()) regularity(nre[F_COMP].data(), nim[F_COMP].data());  // compositional.jl:245-246
     scalar_bc(F_COMP, cbvals, cbc);
   }
 
@@ -914,6 +945,12 @@ struct Oracle {
         nre[F_BPOL][i] = -lfq * wtr[i];
         nim[F_BPOL][i] = -lfq * wti[i];
       }
+    // ball_vector_analysis! (magnetic.jl:362-364) zeroes the analysed u x B
+    // before the curl, which scales each (l, m, r) alone
+    if (ball()) {
+      regularity(nre[F_BTOR].data(), nim[F_BTOR].data());
+      regularity(nre[F_BPOL].data(), nim[F_BPOL].data());
+    }
   }
 
   // apply_master_implicit_step! (simulation.jl:1151-1330) with
@@ -946,7 +983,8 @@ struct Oracle {
           xr[k] = vr; xi[k] = vi;
         }
         if (c.bc_mode == 2) {
-          xr[0] = (f == F_TEMP) ? bvals[q] : 0.0;
+          // ball: the r = 0 row of l >= 1 is the regularity condition (value 0)
+          xr[0] = (f == F_TEMP && !(ball() && l > 0)) ? bvals[q] : 0.0;
           xr[N - 1] = (f == F_TEMP) ? bvals[(size_t)nlm + q] : 0.0;
           xi[0] = 0.0;
           xi[N - 1] = 0.0;
@@ -1057,6 +1095,8 @@ void oc_synth_scalar(void* h, const double* re, const double* im, double* grid) 
 void oc_analysis_scalar(void* h, const double* grid, double* re, double* im) {
   static_cast<Oracle*>(h)->analysis_scalar(grid, re, im);
 }
+// enforce_ball_scalar_regularity! on one [r][lm] field (Ball/Ball.jl:153-170)
+void oc_regularity(void* h, double* re, double* im) { static_cast<Oracle*>(h)->regularity(re, im); }
 void oc_synth_vector(void* h, const double* tre, const double* tim, const double* pre_, const double* pim_,
                      double* vth, double* vph) {
   static_cast<Oracle*>(h)->synth_vector(tre, tim, pre_, pim_, vth, vph);

@@ -40,6 +40,7 @@ class OcConfig(ctypes.Structure):
         ("ab_mode", ctypes.c_int), ("bc_mode", ctypes.c_int), ("fd_mode", ctypes.c_int),
         ("precision", ctypes.c_int), ("magnetic", ctypes.c_int),
         ("composition", ctypes.c_int), ("schmidt", ctypes.c_double),
+        ("segments", ctypes.c_int), ("geometry", ctypes.c_int), ("r_outer", ctypes.c_double),
     ]
 
 
@@ -72,6 +73,7 @@ def _load():
         lib.oc_lu.argtypes = [P, ctypes.c_int, ctypes.c_int, D, D]
         lib.oc_band_solve.argtypes = [P, ctypes.c_int, ctypes.c_int, D]
         lib.oc_synth_scalar.argtypes = [P, D, D, D]
+        lib.oc_regularity.argtypes = [P, D, D]
         lib.oc_analysis_scalar.argtypes = [P, D, D, D]
         lib.oc_synth_vector.argtypes = [P, D, D, D, D, D, D]
         lib.oc_analysis_vector.argtypes = [P, D, D, D, D, D, D]
@@ -133,12 +135,14 @@ class Oracle:
 
     def __init__(self, lmax, nlat, nlon, nr, mmax=None, kl=4, rratio=0.35, ekman=3e-4,
                  rayleigh=80.0, prandtl=1.0, magnetic_prandtl=4.0, dt=1e-5, implicit_theta=0.5,
-                 ab_mode=0, bc_mode=0, fd_mode=0, magnetic=1, threads=None, composition=0, schmidt=1.0):
+                 ab_mode=0, bc_mode=0, fd_mode=0, magnetic=1, threads=None, composition=0, schmidt=1.0,
+                 geometry="shell", r_outer=1.0):
         self.lib = _load()
         mmax = lmax if mmax is None else mmax
         self.cfg = OcConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl,
                             magnetic_prandtl, dt, implicit_theta, ab_mode, bc_mode, fd_mode, 0,
-                            magnetic, int(composition), float(schmidt))
+                            magnetic, int(composition), float(schmidt), 0,
+                            {"shell": 0, "ball": 1}[geometry], float(r_outer))
         self.h = self.lib.oc_create(ctypes.byref(self.cfg))
         if not self.h:
             raise ValueError("oracle rejected the configuration")
@@ -194,9 +198,11 @@ class Oracle:
         self.lib.oc_synth_scalar(self.h, _ptr(_c(re)), _ptr(_c(im)), _ptr(g))
         return g
 
-    def analysis_scalar(self, grid):
+    def analysis_scalar(self, grid, ball=False):
         re = np.zeros(self.spec_shape()); im = np.zeros(self.spec_shape())
         self.lib.oc_analysis_scalar(self.h, _ptr(_c(grid)), _ptr(re), _ptr(im))
+        if ball:  # ball_physical_to_spectral! (Ball/Ball.jl:214-220)
+            self.lib.oc_regularity(self.h, _ptr(re), _ptr(im))
         return re, im
 
     def synth_vector(self, tre, tim, pre, pim):
@@ -205,9 +211,12 @@ class Oracle:
                                  _ptr(vt), _ptr(vp))
         return vt, vp
 
-    def analysis_vector(self, vt, vp):
+    def analysis_vector(self, vt, vp, ball=False):
         out = [np.zeros(self.spec_shape()) for _ in range(4)]
         self.lib.oc_analysis_vector(self.h, _ptr(_c(vt)), _ptr(_c(vp)), *[_ptr(o) for o in out])
+        if ball:  # ball_vector_analysis! (Ball/Ball.jl:236-245)
+            self.lib.oc_regularity(self.h, _ptr(out[0]), _ptr(out[1]))
+            self.lib.oc_regularity(self.h, _ptr(out[2]), _ptr(out[3]))
         return out  # tor re, tor im, pol re, pol im
 
     def gradients(self, re, im):
