@@ -102,6 +102,25 @@ function vector_analysis!(h::Handle, vec, tor, pol)
     return tor, pol
 end
 
+# ball_physical_to_spectral! / ball_vector_analysis! (src/Ball/Ball.jl:214-245):
+# the analyses, then the first radial level set to 0 for l >= 1 on the device
+function ball_physical_to_spectral!(h::Handle, phys, spec)
+    re = parent(spec.data_real); im = parent(spec.data_imag); g = parent(phys.data)
+    GC.@preserve re im g check(h, ccall((:gd_ball_physical_to_spectral, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, 1, g, re, im))
+    return spec
+end
+
+function ball_vector_analysis!(h::Handle, vec, tor, pol)
+    tr = parent(tor.data_real); ti = parent(tor.data_imag)
+    pr = parent(pol.data_real); pi = parent(pol.data_imag)
+    vt = parent(vec.θ_component.data); vp = parent(vec.φ_component.data)
+    GC.@preserve tr ti pr pi vt vp check(h, ccall((:gd_ball_vector_analysis, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+        h.ptr, vt, vp, tr, ti, pr, pi))
+    return tor, pol
+end
+
 # compute_temperature_nonlinear!(temp, vel, oc) (src/thermal.jl:149): the
 # Dirichlet values and sources of temp go to the handle, then one call
 # (gd_compute_temperature_nonlinear) fills temp.nonlinear, applies the boundary
@@ -384,6 +403,21 @@ function install!(GD::Module; precision::Integer = 0)
             nr = size(parent(rhs.data_real), 3)
             h = $handle_for($GD, rhs.config, nr)
             $solve_implicit_step!(h, $device_matrices(h, M, nr, i_KL), sol, rhs)
+        end
+    end
+    if isdefined(GD, :GeoDynamoBall)
+        B = getfield(GD, :GeoDynamoBall)
+        @eval B begin
+            function ball_physical_to_spectral!(phys::$GD.SHTnsPhysicalField{Float64},
+                                                spec::$GD.SHTnsSpectralField{Float64})
+                h = $handle_for($GD, spec.config, size(parent(spec.data_real), 3); precision = $precision)
+                $ball_physical_to_spectral!(h, phys, spec)
+            end
+            function ball_vector_analysis!(vec::$GD.SHTnsVectorField{Float64}, tor::$GD.SHTnsSpectralField{Float64},
+                                           pol::$GD.SHTnsSpectralField{Float64})
+                h = $handle_for($GD, tor.config, size(parent(tor.data_real), 3); precision = $precision)
+                $ball_vector_analysis!(h, vec, tor, pol)
+            end
         end
     end
     return nothing
