@@ -90,15 +90,25 @@ __global__ void __launch_bounds__(256, 2) k_synth_scalar(Dims d, const int* __re
   }
   __syncthreads();
   const int nch = (d.L - m + SS_KC) / SS_KC;  // K chunks of this order
+  const bool pairs = (d.nth & 1) == 0;
   auto load = [&](int ch) {
     double* As = smem + (ch % LEG_STAGES) * SS_STAGE;  // [q][theta]
     double* Bs = As + SS_KC * SS_SA;                    // [q][n]
     const int l0 = m + ch * SS_KC;
-    for (int e = tid; e < SS_KC * SS_TM; e += 256) {
-      const int q = e / SS_TM, th = e % SS_TM;
-      const int l = l0 + q, ith = th0 + th;
-      const bool ok = l <= d.L && ith < d.nth;
-      cpa8(As + q * SS_SA + th, ok ? P + (size_t)(mb + l - m) * d.nth + ith : P, ok);
+    if (pairs) {  // two colatitudes per 16-byte copy (rows 16-byte aligned: nth even)
+      for (int e = tid; e < SS_KC * SS_TM / 2; e += 256) {
+        const int q = e / (SS_TM / 2), th = 2 * (e % (SS_TM / 2));
+        const int l = l0 + q, ith = th0 + th;
+        const bool ok = l <= d.L && ith < d.nth;
+        cpa16(As + q * SS_SA + th, ok ? P + (size_t)(mb + l - m) * d.nth + ith : P, ok);
+      }
+    } else {
+      for (int e = tid; e < SS_KC * SS_TM; e += 256) {
+        const int q = e / SS_TM, th = e % SS_TM;
+        const int l = l0 + q, ith = th0 + th;
+        const bool ok = l <= d.L && ith < d.nth;
+        cpa8(As + q * SS_SA + th, ok ? P + (size_t)(mb + l - m) * d.nth + ith : P, ok);
+      }
     }
     for (int e = tid; e < SS_KC * SS_TN; e += 256) {
       const int q = e % SS_KC, n = e / SS_KC;
@@ -230,17 +240,29 @@ __global__ void __launch_bounds__(256, 2) k_synth_vector(Dims d, const int* __re
   }
   __syncthreads();
   const int nch = (d.L - m + VS_KC) / VS_KC;
+  const bool pairs = (d.nth & 1) == 0;
   auto load = [&](int ch) {
     double* As = smem + (ch % LEG_STAGES) * VS_STAGE;  // [tab][q][theta]
     double* Bs = As + 2 * VS_KC * VS_SA;                // [fld][q][n]
     const int l0 = m + ch * VS_KC;
-    for (int e = tid; e < 2 * VS_KC * VS_TM; e += 256) {
-      const int tab = e / (VS_KC * VS_TM), rem = e % (VS_KC * VS_TM);
-      const int q = rem / VS_TM, th = rem % VS_TM;
-      const int l = l0 + q, ith = th0 + th;
-      const bool ok = l <= d.L && ith < d.nth;
-      const double* T = tab == 0 ? dP : Q;
-      cpa8(As + (tab * VS_KC + q) * VS_SA + th, ok ? T + (size_t)(mb + l - m) * d.nth + ith : T, ok);
+    if (pairs) {  // two colatitudes per 16-byte copy (rows 16-byte aligned: nth even)
+      for (int e = tid; e < VS_KC * VS_TM; e += 256) {
+        const int tab = e / (VS_KC * VS_TM / 2), rem = e % (VS_KC * VS_TM / 2);
+        const int q = rem / (VS_TM / 2), th = 2 * (rem % (VS_TM / 2));
+        const int l = l0 + q, ith = th0 + th;
+        const bool ok = l <= d.L && ith < d.nth;
+        const double* T = tab == 0 ? dP : Q;
+        cpa16(As + (tab * VS_KC + q) * VS_SA + th, ok ? T + (size_t)(mb + l - m) * d.nth + ith : T, ok);
+      }
+    } else {
+      for (int e = tid; e < 2 * VS_KC * VS_TM; e += 256) {
+        const int tab = e / (VS_KC * VS_TM), rem = e % (VS_KC * VS_TM);
+        const int q = rem / VS_TM, th = rem % VS_TM;
+        const int l = l0 + q, ith = th0 + th;
+        const bool ok = l <= d.L && ith < d.nth;
+        const double* T = tab == 0 ? dP : Q;
+        cpa8(As + (tab * VS_KC + q) * VS_SA + th, ok ? T + (size_t)(mb + l - m) * d.nth + ith : T, ok);
+      }
     }
     for (int e = tid; e < 2 * VS_KC * VS_TN; e += 256) {
       const int fld = e / (VS_KC * VS_TN), rem = e % (VS_KC * VS_TN);
@@ -443,15 +465,25 @@ __global__ void __launch_bounds__(256, 2) k_analysis_scalar(Dims d, const int* _
   __syncthreads();
   const double* Gin = reinterpret_cast<const double*>(a.in);
   const int nch = (d.nth + SA_KC - 1) / SA_KC;
+  const bool pairs = (d.nth & 1) == 0;
   auto load = [&](int ch) {
     double* As = smem + (ch % LEG_STAGES) * SA_STAGE;  // [l][theta]
     double* Bs = As + SA_TL * SA_SA;                    // [s][theta][n]
     const int k0 = ch * SA_KC;
-    for (int e = tid; e < SA_TL * SA_KC; e += 256) {
-      const int lq = e / SA_KC, th = e % SA_KC;
-      const int l = l0 + lq, ith = k0 + th;
-      const bool ok = l <= d.L && ith < d.nth;
-      cpa8(As + lq * SA_SA + th, ok ? P + (size_t)(mb + l - m) * d.nth + ith : P, ok);
+    if (pairs) {  // two colatitudes per 16-byte copy (rows 16-byte aligned: nth even)
+      for (int e = tid; e < SA_TL * SA_KC / 2; e += 256) {
+        const int lq = e / (SA_KC / 2), th = 2 * (e % (SA_KC / 2));
+        const int l = l0 + lq, ith = k0 + th;
+        const bool ok = l <= d.L && ith < d.nth;
+        cpa16(As + lq * SA_SA + th, ok ? P + (size_t)(mb + l - m) * d.nth + ith : P, ok);
+      }
+    } else {
+      for (int e = tid; e < SA_TL * SA_KC; e += 256) {
+        const int lq = e / SA_KC, th = e % SA_KC;
+        const int l = l0 + lq, ith = k0 + th;
+        const bool ok = l <= d.L && ith < d.nth;
+        cpa8(As + lq * SA_SA + th, ok ? P + (size_t)(mb + l - m) * d.nth + ith : P, ok);
+      }
     }
     for (int e = tid; e < 2 * SA_KC * (SA_TN / 2); e += 256) {
       const int th = e % SA_KC, rest = e / SA_KC;
