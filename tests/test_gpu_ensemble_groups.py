@@ -131,3 +131,43 @@ def test_segmented_handle_refusals(gdb):
     g.check_finite()
     ek, em = g.segment_energy()
     assert ek.shape == (2,) and np.all(np.isfinite(ek)) and np.all(ek > 0)
+
+
+@pytest.mark.parametrize("bc_mode", [0, 1, 2])
+def test_segments_keep_their_own_boundary_rows(gdb, bc_mode):
+    # two members of one shape on one segmented handle against two single
+    # handles: boundary values and flux types (bc_mode 0/1: tau rows on the
+    # state; 2: Dirichlet rows in the operator), sources per shell, clamped
+    # rows (bc_mode 1); every row operation must act at each segment's own ends
+    lmax, nlat, nlon, nr = 15, 24, 48, 9
+    members = [dict(lmax=lmax, nlat=nlat, nlon=nlon, nr=nr, ekman=e, bc_mode=bc_mode, dt=2e-6) for e in (3e-4, 7e-4)]
+    ens = gdb.Ensemble(members, group=2)
+    assert len(ens.handles) == 1
+    h = ens.handles[0]
+    rng = np.random.default_rng(11)
+    nlm = h.nlm
+    bv = rng.standard_normal((2, nlm)) * 1e-2
+    src = rng.standard_normal(nr)
+    inner = np.where(rng.random(nlm) < 0.5, 1, 2) if bc_mode != 2 else np.ones(nlm, dtype=int)
+    outer = np.where(rng.random(nlm) < 0.5, 1, 2) if bc_mode != 2 else np.ones(nlm, dtype=int)
+    h.set_bc_types("temp", inner, outer)
+    h.set_temperature_bc(bv, np.concatenate([src, src]))
+    singles = []
+    for i, (c, m) in enumerate(zip(members, ens.members)):
+        kw = {k: v for k, v in c.items() if k not in ("lmax", "nlat", "nlon", "nr")}
+        s = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, **kw)
+        s.set_bc_types("temp", inner, outer)
+        s.set_temperature_bc(bv, src)
+        for k, (a, b) in workloads.seeded_state(lmax, lmax, nr, seed=20 + i, amp=1e-1).items():
+            m.set_field(k, a, b)
+            s.set_field(k, a, b)
+        singles.append(s)
+    ens.step(3)
+    for s in singles:
+        s.step(3)
+    for m, s in zip(ens.members, singles):
+        for k in NAMES:
+            a, b = m.get_field(k), s.get_field(k)
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), (bc_mode, k)
+        assert m.energy() == s.energy()
+    ens.close()
