@@ -155,3 +155,21 @@ def test_literal_operator_amplifies_temperature(oracle_mod):
         growth[bc] = np.abs(o.get_field("temp")[0]).max() / t0
     assert growth[0] > 1e6
     assert growth[2] < 1.0
+
+
+def test_uniform_boundary_pattern_is_l0_only(orc6):
+    # test/shell_boundaries.jl:17-37: uniform inner / outer temperature
+    # patterns (100 and 250) analysed to spectral boundary values carry only
+    # l = 0 (|a_l>0| <= 1e-8 max); with orthonormal Y_00 = 1 / sqrt(4 pi) the
+    # l = 0 value is the pattern times sqrt(4 pi)
+    nlm = orc6.nlm
+    lv = np.array([l for l in range(7) for m in range(l + 1)])
+    for val in (100.0, 250.0):
+        re, im = orc6.analysis_scalar(np.full(orc6.grid_shape(), val))
+        for k in range(orc6.nr):
+            mx = np.max(np.abs(re[k]))
+            assert mx > 0
+            assert np.all(np.abs(re[k, lv > 0]) <= 1e-8 * max(1.0, mx))
+            assert np.all(np.abs(im[k]) <= 1e-8 * max(1.0, mx))
+            assert re[k, 0] == pytest.approx(val * np.sqrt(4.0 * np.pi), rel=1e-13)
+    assert nlm == lv.size
