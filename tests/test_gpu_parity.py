@@ -265,16 +265,18 @@ def test_step_kernel_count_is_the_graph_node_count(gdb):
     g.close()
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("mixed", 5e-6)])
-def test_uniform_boundary_pattern_is_l0_only(gdb, precision, tol):
+@pytest.mark.parametrize("precision,tol,leak", [("fp64", 1e-13, 1e-8), ("mixed", 5e-6, 5e-6)])
+def test_uniform_boundary_pattern_is_l0_only(gdb, precision, tol, leak):
     # test/shell_boundaries.jl:17-37 on the device: uniform patterns analyse to
-    # l = 0 only (|a_l>0| <= 1e-8 of the largest), a_00 = value * sqrt(4 pi)
+    # l = 0 only (|a_l>0| <= 1e-8 of the largest in FP64, the reference's bound;
+    # the split-TF32 analysis' own error level in mixed precision),
+    # a_00 = value * sqrt(4 pi)
     g = gdb.SHTnsKitConfig(6, 12, 24, 6, precision=precision)
     lv = np.array([l for l in range(7) for m in range(l + 1)])
     for val in (100.0, 250.0):
         re, im = g.analysis_scalar(np.full(g.grid_shape(), val))
         for k in range(g.nr):
             mx = float(np.max(np.abs(re[k])))
-            assert np.all(np.abs(re[k, lv > 0]) <= 1e-8 * max(1.0, mx))
-            assert np.all(np.abs(im[k]) <= 1e-8 * max(1.0, mx))
+            assert np.all(np.abs(re[k, lv > 0]) <= leak * max(1.0, mx))
+            assert np.all(np.abs(im[k]) <= leak * max(1.0, mx))
             assert abs(re[k, 0] - val * np.sqrt(4.0 * np.pi)) <= tol * val * np.sqrt(4.0 * np.pi)
