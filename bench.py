@@ -877,6 +877,12 @@ def main():
             roofline["traffic_unit"] = "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)"
             if len(bounds) > 1:
                 roofline["other"] = {k: bounds[1][k] for k in ("bound", "achieved", "peak", "unit", "frac")}
+            if top["name"].startswith("fused_"):
+                # what does bind the fused phase kernels (one-launch ncu capture at nr = 33,
+                # profiles/fused_velocity_fp32_shell_l255_nr33.md): neither HBM nor a tensor pipe
+                roofline["binding_unit"] = {"unit": "shared-memory (LSU) wavefronts and issue",
+                                            "lsu_frac": 0.61, "issue_active_frac": 0.58,
+                                            "source": "ncu, k_fused<768, 2, 0>, shell_l255_nr33"}
 
     # ---- FP64 reference step on the GPU (denominator of the metric) ----
     fp64_value = None
