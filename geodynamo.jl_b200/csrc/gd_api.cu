@@ -269,10 +269,12 @@ int setup(gd_handle* h) {
   CK(cudaMemsetAsync(h->d_csources, 0, sizeof(double) * NR, s));
   {
     // boundary types: temperature fixed values, composition no-flux
-    // (create_shtns_temperature_field / create_shtns_composition_field defaults)
+    // (create_shtns_temperature_field / create_shtns_composition_field
+    // defaults); with the boundary-row operator (bc_mode 2) composition has
+    // fixed values too, those of its rows
     std::vector<int> bt(4 * NL);
     for (size_t q = 0; q < 2 * NL; ++q) bt[q] = GD_BC_VALUE;
-    for (size_t q = 2 * NL; q < 4 * NL; ++q) bt[q] = GD_BC_FLUX;
+    for (size_t q = 2 * NL; q < 4 * NL; ++q) bt[q] = c.bc_mode == 2 ? GD_BC_VALUE : GD_BC_FLUX;
     CK(cudaMemcpyAsync(h->d_bctype, bt.data(), sizeof(int) * bt.size(), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
     h->bctype = bt;
@@ -537,8 +539,10 @@ int implicit_launch(gd_handle* h, int boot) {
   a.boot = boot;
   a.clamp_rows = h->c.bc_mode == 1;
   a.bc_rows = h->c.bc_mode == 2;
-  a.bvals = h->d_bvals;
-  a.temp_slot = 0;
+  // Dirichlet rows of bc_mode 2: the temperature's and the composition's
+  // boundary values, zero for the velocity and magnetic potentials
+  for (int i = 0; i < a.nfield; ++i)
+    a.rowvals[i] = order[i] == F_TEMP ? h->d_bvals : order[i] == F_COMP ? h->d_cbvals : nullptr;
   a.inv_dt = 1.0 / h->c.dt;
   a.lin_weight = 1.0 - h->c.implicit_theta;
   a.dt = h->c.dt;
@@ -690,7 +694,6 @@ bool valid_config(const gd_config* c, std::string& why) {
   if (c->precision != GD_PREC_FP64 && c->precision != GD_PREC_MIXED) { why = "unknown precision"; return false; }
   if (c->composition != 0 && c->composition != 1) { why = "composition must be 0 or 1"; return false; }
   if (c->composition && !(c->schmidt > 0.0)) { why = "composition needs a positive Schmidt number"; return false; }
-  if (c->composition && c->bc_mode == 2) { why = "composition supports bc_mode 0 and 1"; return false; }
   if (c->segments < 0 || (c->segments > 1 && c->nr % c->segments)) { why = "segments must divide nr"; return false; }
   if (c->segments > 1 && c->nr / c->segments < 3) { why = "each segment needs at least 3 levels"; return false; }
   if (c->segments > 1 && c->composition) { why = "segments carry no composition"; return false; }
@@ -701,7 +704,6 @@ bool valid_config(const gd_config* c, std::string& why) {
       why = "ball geometry needs bc_mode 2: the literal operator holds 1/r and 1/r^2 at r = 0";
       return false;
     }
-    if (c->composition) { why = "ball geometry carries no composition (bc_mode 2 has no composition rows)"; return false; }
   }
   return true;
 }
@@ -1565,8 +1567,7 @@ static int cnab2_host(gd_handle* h, const gd_matrices* m, double dt, int stages)
   a.prev[0] = h->d_stage_spec2 + 2 * se;
   a.kind[0] = 0;
   a.nfield = 1;
-  a.bvals = h->d_bvals;
-  a.temp_slot = -1;
+  a.rowvals[0] = nullptr;  // no boundary rows of a given value
   a.inv_dt = 1.0 / dt;
   a.lin_weight = 1.0 - m->theta;
   a.dt = dt;

@@ -42,7 +42,7 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
   const double* __restrict__ F = LU + l;
   const bool boot = a.boot != 0;
   const bool rows = a.bc_rows != 0;
-  const bool is_temp = slot == a.temp_slot;
+  const double* __restrict__ rowv = a.rowvals[slot];
   const int stages = a.stages ? a.stages : 7;
 
   // sweep 1: right-hand side, rows in batches of RB whose loads are issued first
@@ -93,7 +93,7 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
       vi += a.lin_weight * Li;
       if (rows && (i == 0 || i == N - 1)) {
         // ball: the r = 0 row of l >= 1 is the regularity condition (value 0)
-        vr = (is_temp && !(d.ball && i == 0 && l > 0)) ? a.bvals[(i == 0 ? 0 : NM) + j] : 0.0;
+        vr = (rowv != nullptr && !(d.ball && i == 0 && l > 0)) ? rowv[(i == 0 ? 0 : NM) + j] : 0.0;
         vi = 0.0;
       }
       ure[at] = vr;

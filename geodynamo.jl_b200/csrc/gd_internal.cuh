@@ -167,9 +167,8 @@ struct Cnab2Args {
   int nfield;
   int boot;
   int clamp_rows;
-  int bc_rows;                // Dirichlet rows in the operator: boundary rhs = bval (temperature) or 0
-  const double* bvals;        // temperature boundary values [2][nlm] (native order)
-  int temp_slot;              // slot index of the temperature field
+  int bc_rows;                // Dirichlet rows in the operator: boundary rhs = the slot's value or 0
+  const double* rowvals[6];   // per slot: boundary values [2][nlm] (native order) of its rows (null: 0)
   double inv_dt, lin_weight;
   double dt;                  // EAB2: the time step applied to the phi1 term
   int stages;                 // sweeps to run: 1 rhs, 2 forward, 4 back substitution (0: all)

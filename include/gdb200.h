@@ -104,7 +104,8 @@ enum { GD_GEOM_SHELL = 0, GD_GEOM_BALL = 1 };
  * (step_once!), diffusivity Pm/Sc with schmidt = d_Sc, no-flux boundaries by
  * default (create_shtns_composition_field, src/compositional.jl:80-118).  Its
  * buoyancy is a radial force, which the vector analysis does not keep, so C
- * does not act on the velocity.  CNAB2 with bc_mode 0 or 1 only.
+ * does not act on the velocity.  CNAB2 only; under bc_mode 2 its boundary
+ * types are fixed values, the right-hand sides of its Dirichlet rows.
  * segments > 1 stacks that many independent shells of nr / segments levels
  * each (same grid, diffusivities, dt and modes; their own Ekman numbers through
  * gd_set_segment_ekman) along r: every per-shell kernel serves them all in one
@@ -123,7 +124,8 @@ enum { GD_GEOM_SHELL = 0, GD_GEOM_BALL = 1 };
  * The reference's implicit operator holds 1/r and 1/r^2 at r = 0 (infinite;
  * 0 x inf at l = 0), so a ball needs bc_mode 2, whose r = 0 row is the
  * regularity condition for l >= 1 and the inner boundary value for the l = 0
- * temperature; CNAB2, no composition, no flux boundaries.  Entry points whose
+ * temperature and composition (centre values); CNAB2, no flux boundaries.
+ * Entry points whose
  * operators divide by r (reverse mode, exponential schemes, the standalone
  * timestepping operator, the distributed step) refuse a ball.
  */

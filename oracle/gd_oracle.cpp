@@ -247,7 +247,9 @@ struct Oracle {
     // create_shtns_temperature_field: fixed temperature (thermal.jl:113-114);
     // create_shtns_composition_field: no flux (compositional.jl:112-114)
     tbc.assign(2 * (size_t)nlm, BC_VALUE);
-    cbc.assign(2 * (size_t)nlm, BC_FLUX);
+    // with the boundary-row operator (bc_mode 2, an added option) composition
+    // has fixed values, those of its rows
+    cbc.assign(2 * (size_t)nlm, c.bc_mode == 2 ? BC_VALUE : BC_FLUX);
     build_implicit();
     return 0;
   }
@@ -984,8 +986,9 @@ struct Oracle {
         }
         if (c.bc_mode == 2) {
           // ball: the r = 0 row of l >= 1 is the regularity condition (value 0)
-          xr[0] = (f == F_TEMP && !(ball() && l > 0)) ? bvals[q] : 0.0;
-          xr[N - 1] = (f == F_TEMP) ? bvals[(size_t)nlm + q] : 0.0;
+          const std::vector<double>* bv = f == F_TEMP ? &bvals : f == F_COMP ? &cbvals : nullptr;
+          xr[0] = (bv && !(ball() && l > 0)) ? (*bv)[q] : 0.0;
+          xr[N - 1] = bv ? (*bv)[(size_t)nlm + q] : 0.0;
           xi[0] = 0.0;
           xi[N - 1] = 0.0;
         }

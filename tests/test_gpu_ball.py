@@ -173,8 +173,6 @@ def test_ball_refusals(gdb):
         gdb.SHTnsKitConfig(7, 12, 24, 9, geometry="ball", bc_mode=0)
     with pytest.raises(gdb.GeoDynamoError):
         gdb.SHTnsKitConfig(7, 12, 24, 9, geometry="ball", bc_mode=2, r_outer=0.0)
-    with pytest.raises(gdb.GeoDynamoError):
-        gdb.SHTnsKitConfig(7, 12, 24, 9, geometry="ball", bc_mode=2, composition=1, schmidt=2.0)
     g = gdb.SHTnsKitConfig(7, 12, 24, 9, geometry="ball", bc_mode=2)
     with pytest.raises(gdb.GeoDynamoError):
         g.set_scheme("eab2")
@@ -184,3 +182,33 @@ def test_ball_refusals(gdb):
         g.temperature_forward(2, 1)
     g.step(1)
     g.check_finite()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 5e-6)])
+def test_ball_with_composition_matches_oracle(gdb, oracle_mod, precision, tol):
+    # composition in the ball: regularity of its analysed term and of its state
+    # (src/compositional.jl:245-246, 368-370), the centre value of its l = 0 row
+    lmax, nlat, nlon, nr = 15, 24, 48, 12
+    kw = dict(geometry="ball", bc_mode=2, composition=1, schmidt=2.0, dt=2e-6)
+    g = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, precision=precision, **kw)
+    o = oracle_mod.Oracle(lmax=lmax, nlat=nlat, nlon=nlon, nr=nr, **kw)
+    st = regular_state(lmax, nr, seed=3)
+    cst = regular_state(lmax, nr, seed=103)["temp"]
+    cbv = np.zeros((2, g.nlm))
+    cbv[0, 0] = -0.3
+    cbv[1] = np.random.default_rng(5).standard_normal(g.nlm) * 1e-2
+    for m in (g, o):
+        for k, (a, b) in st.items():
+            m.set_field(k, a, b)
+        m.set_field("comp", *cst)
+        m.set_composition_bc(cbv, np.linspace(0.1, 0.4, nr))
+    g.step(3)
+    o.step(3)
+    lpos = l_of(lmax) > 0
+    for k in NAMES + ("comp",):
+        for x, y in zip(g.get_field(k), o.get_field(k)):
+            assert rel(x, y) < tol, k
+            assert np.all(x[0, lpos] == 0.0), k
+    for x in g.get_nl("comp"):
+        assert np.all(x[0, lpos] == 0.0)
+    assert g.get_field("comp")[0][0, 0] == -0.3

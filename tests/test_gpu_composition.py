@@ -91,9 +91,35 @@ def test_composition_phase_alone_matches_oracle(gdb, oracle_mod):
         assert rel(x, y) < 1e-12
 
 
-def test_composition_refusals(gdb):
+def test_composition_with_boundary_rows_matches_oracle(gdb, oracle_mod):
+    # bc_mode 2: composition's Dirichlet rows take its boundary values (and its
+    # boundary types default to fixed values); the flux types are refused there
+    lmax, nlat, nlon, nr = 15, 24, 48, 12
+    g = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, composition=1, schmidt=2.5, bc_mode=2, dt=2e-6)
+    o = oracle_mod.Oracle(lmax=lmax, nlat=nlat, nlon=nlon, nr=nr, composition=1, schmidt=2.5, bc_mode=2, dt=2e-6)
+    rng = np.random.default_rng(4)
+    st = workloads.seeded_state(lmax, lmax, nr, seed=4, amp=1e-1)
+    cst = workloads.seeded_state(lmax, lmax, nr, seed=104, amp=1e-1)["temp"]
+    tbv = rng.standard_normal((2, g.nlm)) * 1e-2
+    cbv = rng.standard_normal((2, g.nlm)) * 1e-2
+    for m in (g, o):
+        for k, (a, b) in st.items():
+            m.set_field(k, a, b)
+        m.set_field("comp", *cst)
+        m.set_temperature_bc(tbv, np.linspace(0.2, 1.0, nr))
+        m.set_composition_bc(cbv, np.linspace(-0.3, 0.3, nr))
+    g.step(3)
+    o.step(3)
+    for k in NAMES:
+        for x, y in zip(g.get_field(k), o.get_field(k)):
+            assert rel(x, y) < 1e-12, k
+    cre, _ = g.get_field("comp")
+    assert np.array_equal(cre[0], cbv[0]) and np.array_equal(cre[-1], cbv[1])
     with pytest.raises(gdb.GeoDynamoError):
-        gdb.SHTnsKitConfig(7, 12, 24, 9, composition=1, schmidt=1.0, bc_mode=2)
+        g.set_bc_types("comp", np.full(g.nlm, 2), np.full(g.nlm, 1))
+
+
+def test_composition_refusals(gdb):
     with pytest.raises(gdb.GeoDynamoError):
         gdb.SHTnsKitConfig(7, 12, 24, 9, composition=1, schmidt=0.0)
     g = gdb.SHTnsKitConfig(7, 12, 24, 9, composition=1, schmidt=1.0)
