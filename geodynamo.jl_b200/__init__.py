@@ -58,7 +58,7 @@ PRECISION_PRESETS = {"mixed_vel64": ("mixed", ("vel_synth", "vel_products", "vel
 SCHEMES = {"cnab2": 0, "eab2": 1, "erk2": 2}
 GEOMETRIES = {"shell": 0, "ball": 1}   # geometry (src/parameters.jl:75)   # ts_scheme (src/simulation.jl:1054-1300)
 ETD_MATRICES = ("E", "phi1", "phi2", "E_half", "phi1_half")   # ERK2Cache fields (src/timestep.jl:830-853)
-KINDS = {"velocity": 0, "magnetic": 1, "temperature": 2}
+KINDS = {"velocity": 0, "magnetic": 1, "temperature": 2, "composition": 3}
 
 # Every symbol include/gdb200.h declares.
 EXPORTS = (

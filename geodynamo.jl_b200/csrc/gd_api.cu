@@ -444,9 +444,11 @@ int temperature_nl(gd_handle* h);
 int velocity_nl(gd_handle* h);
 int magnetic_nl(gd_handle* h);
 int composition_nl(gd_handle* h);
+int step_slots(const gd_handle* h, int* order, int* kinds);
 
 // compute_all_nonlinear_terms! (src/simulation.jl:800-813): velocity, magnetic,
-// temperature, in that order (the carried grids make the order matter).
+// temperature, composition, in that order (the carried grids make the order
+// matter).
 int all_nonlinear(gd_handle* h) {
   int s = velocity_nl(h);
   if (s) return s;
@@ -454,7 +456,9 @@ int all_nonlinear(gd_handle* h) {
     s = magnetic_nl(h);
     if (s) return s;
   }
-  return temperature_nl(h);
+  s = temperature_nl(h);
+  if (s || !h->c.composition) return s;
+  return composition_nl(h);
 }
 
 // erk2_integrate_full_step! (src/simulation.jl:1054-1149) after the step's
@@ -467,12 +471,13 @@ int all_nonlinear(gd_handle* h) {
 int erk2_launch(gd_handle* h, const Cnab2Args& a) {
   const size_t se = h->spec_elems();
   ExpApply e = exp_apply_args(h, a);
-  const int order[5] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL};
-  double* lin[5];
-  double* k1[5];
+  int order[6], kinds[6];
+  step_slots(h, order, kinds);
+  double* lin[6];
+  double* k1[6];
   for (int i = 0; i < a.nfield; ++i) {
     lin[i] = h->d_erk2 + (size_t)order[i] * se;
-    k1[i] = h->d_erk2 + (size_t)(5 + order[i]) * se;
+    k1[i] = h->d_erk2 + (size_t)(NFIELD + order[i]) * se;
   }
   {
     ProfScope p(h, "erk2_prepare");
@@ -518,18 +523,26 @@ int erk2_launch(gd_handle* h, const Cnab2Args& a) {
   return all_nonlinear(h);
 }
 
+// The implicit slots of a step: temperature, velocity, magnetic field (when
+// evolved), composition (when configured); their fields and diffusivity kinds.
+int step_slots(const gd_handle* h, int* order, int* kinds) {
+  int n = 0;
+  const int f[6] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL, F_COMP};
+  const int k[6] = {2, 0, 0, 1, 1, 3};
+  for (int i = 0; i < 6; ++i) {
+    if ((f[i] == F_BTOR || f[i] == F_BPOL) && !h->c.magnetic) continue;
+    if (f[i] == F_COMP && !h->c.composition) continue;
+    order[n] = f[i];
+    kinds[n] = k[i];
+    ++n;
+  }
+  return n;
+}
+
 int implicit_launch(gd_handle* h, int boot) {
   Cnab2Args a{};
-  // temperature, velocity, magnetic field, composition (the exponential
-  // schemes are refused with composition: it is a CNAB2 slot only)
-  int order[6] = {F_TEMP, F_UTOR, F_UPOL, F_BTOR, F_BPOL, F_COMP};
-  int kinds[6] = {2, 0, 0, 1, 1, 3};
-  a.nfield = h->c.magnetic ? 5 : 3;
-  if (h->c.composition && h->scheme == GD_SCHEME_CNAB2) {
-    order[a.nfield] = F_COMP;
-    kinds[a.nfield] = 3;
-    ++a.nfield;
-  }
+  int order[6], kinds[6];
+  a.nfield = step_slots(h, order, kinds);
   for (int i = 0; i < a.nfield; ++i) {
     a.u[i] = h->field(order[i]);
     a.nl[i] = h->nlf(order[i]);
@@ -573,12 +586,13 @@ int implicit_launch(gd_handle* h, int boot) {
 // src/timestep.jl:37-70), from the L_l bands of build_implicit.
 int build_etd(gd_handle* h) {
   const Dims& d = h->d;
-  if (!h->d_etd) AL(h->d_etd, etd_table_doubles(d));
+  const int nkind = h->c.composition ? 4 : 3;
+  if (!h->d_etd) AL(h->d_etd, etd_table_doubles(d, nkind));
   double* scratch = nullptr;
-  CK(cudaMalloc(&scratch, etd_scratch_doubles(d) * sizeof(double)));
+  CK(cudaMalloc(&scratch, etd_scratch_doubles(d, nkind) * sizeof(double)));
   cudaError_t e = cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream);
   if (e == cudaSuccess) {
-    launch_etd_build(h->stream, d, h->d_lin, h->c.dt, scratch, h->d_etd, h->d_flag);
+    launch_etd_build(h->stream, d, h->d_lin, h->c.dt, scratch, h->d_etd, h->d_flag, nkind);
     e = cudaGetLastError();
   }
   int flag = 0;
@@ -1770,13 +1784,11 @@ int gd_set_scheme(gd_handle* h, int scheme) {
   CK(cudaStreamSynchronize(h->stream));
   if (scheme != GD_SCHEME_CNAB2) {
     if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "an exponential scheme");
-    if (h->c.composition)
-      return fail(h, GD_ERR_UNSUPPORTED, "the exponential schemes are not built for composition (CNAB2 only)");
     if (h->c.bc_mode == 2)
       return fail(h, GD_ERR_UNSUPPORTED,
                   "the exponential schemes have no boundary rows (bc_mode 2 is a CNAB2 operator option)");
     if (h->d.nr > 256) return fail(h, GD_ERR_UNSUPPORTED, "the exponential schemes support nr <= 256");
-    if (scheme == GD_SCHEME_ERK2 && !h->d_erk2) AL(h->d_erk2, 10 * h->spec_elems());
+    if (scheme == GD_SCHEME_ERK2 && !h->d_erk2) AL(h->d_erk2, 2 * NFIELD * h->spec_elems());
     int s = build_etd(h);
     if (s) return s;
   }
@@ -1786,7 +1798,8 @@ int gd_set_scheme(gd_handle* h, int scheme) {
 }
 
 int gd_download_etd(gd_handle* h, int kind, int l, int which, double* out) {
-  if (!h || !out || kind < 0 || kind > 2 || l < 0 || l > h->d.L || which < 0 || which > 4)
+  if (!h || !out || kind < 0 || kind > (h && h->c.composition ? 3 : 2) || l < 0 || l > h->d.L || which < 0 ||
+      which > 4)
     return h ? fail(h, GD_ERR_ARG, "bad kind, degree, matrix or pointer") : GD_ERR_ARG;
   if (h->scheme == GD_SCHEME_CNAB2 || !h->d_etd) return fail(h, GD_ERR_ARG, "no exponential scheme is selected");
   CK(cudaSetDevice(h->device));

@@ -12,7 +12,8 @@
 // CNAB2 matrices are built from (the handle's L_l band, same roundings).  The
 // reference applies EAB2's E and phi1 to the velocity and magnetic fields by
 // Krylov approximations (eab2_update_krylov_cached!, :358-427, m = 20, tol
-// 1e-8); here every field uses the dense matrices.
+// 1e-8); here every field uses the dense matrices, composition (kind 3)
+// included.
 #include "gd_internal.cuh"
 
 namespace gd {
@@ -199,12 +200,14 @@ __global__ void __launch_bounds__(EX_THREADS) k_etd_build(int n, int kl, int L, 
   }
 }
 
-size_t etd_table_doubles(const Dims& d) { return (size_t)3 * (d.L + 1) * ETD_BLOCKS * d.nr * d.nr; }
-size_t etd_scratch_doubles(const Dims& d) { return (size_t)3 * (d.L + 1) * 6 * d.nr * d.nr; }
+size_t etd_table_doubles(const Dims& d, int nkind) {
+  return (size_t)nkind * (d.L + 1) * ETD_BLOCKS * d.nr * d.nr;
+}
+size_t etd_scratch_doubles(const Dims& d, int nkind) { return (size_t)nkind * (d.L + 1) * 6 * d.nr * d.nr; }
 
 void launch_etd_build(cudaStream_t st, const Dims& d, const double* lin, double dt, double* scratch, double* tab,
-                      int* err) {
-  k_etd_build<<<dim3(d.L + 1, 3), EX_THREADS, 0, st>>>(d.nr, d.kl, d.L, lin, dt, scratch, tab, err);
+                      int* err, int nkind) {
+  k_etd_build<<<dim3(d.L + 1, nkind), EX_THREADS, 0, st>>>(d.nr, d.kl, d.L, lin, dt, scratch, tab, err);
 }
 
 // ---------------------------------------------------------------------------

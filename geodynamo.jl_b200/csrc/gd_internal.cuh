@@ -174,19 +174,20 @@ struct Cnab2Args {
   int stages;                 // sweeps to run: 1 rhs, 2 forward, 4 back substitution (0: all)
 };
 // ---- exponential Adams-Bashforth 2 (gd_expo.cu) ----
-size_t etd_table_doubles(const Dims& d);
-size_t etd_scratch_doubles(const Dims& d);
+// nkind: 3 (velocity, magnetic, temperature), 4 with composition
+size_t etd_table_doubles(const Dims& d, int nkind);
+size_t etd_scratch_doubles(const Dims& d, int nkind);
 void launch_etd_build(cudaStream_t s, const Dims& d, const double* lin, double dt, double* scratch, double* tab,
-                      int* err);
+                      int* err, int nkind);
 // out = M_top x_top + M_bot (bot_scale * x_bot) per (field, l, m, plane) column (gd_expo.cu)
 struct ExpApply {
-  const double* top[5];       // per slot: x_top (u), unused without top_block
-  const double* bot_a[5];     // per slot: a
-  const double* bot_b[5];     // per slot: b (bot_mode 1, 2)
-  double* out[5];             // may equal top
-  const double* lin[5];       // epilogue 1 operands
-  const double* k1[5];
-  int kind[5];
+  const double* top[6];       // per slot: x_top (u), unused without top_block
+  const double* bot_a[6];     // per slot: a
+  const double* bot_b[6];     // per slot: b (bot_mode 1, 2)
+  double* out[6];             // may equal top
+  const double* lin[6];       // epilogue 1 operands
+  const double* k1[6];
+  int kind[6];
   int nfield;
   int top_block, bot_block;   // table blocks 0 E, 1 phi1, 2 phi2, 3 E(dt/2), 4 phi1(dt/2); -1: none
   int bot_mode;               // x_bot = 0: a, 1: 3/2 a - 1/2 b, 2: a - b

@@ -104,7 +104,8 @@ enum { GD_GEOM_SHELL = 0, GD_GEOM_BALL = 1 };
  * (step_once!), diffusivity Pm/Sc with schmidt = d_Sc, no-flux boundaries by
  * default (create_shtns_composition_field, src/compositional.jl:80-118).  Its
  * buoyancy is a radial force, which the vector analysis does not keep, so C
- * does not act on the velocity.  CNAB2 only; under bc_mode 2 its boundary
+ * does not act on the velocity.  Every time scheme (the exponential ones
+ * with composition as a fourth operator kind); under bc_mode 2 its boundary
  * types are fixed values, the right-hand sides of its Dirichlet rows.
  * segments > 1 stacks that many independent shells of nr / segments levels
  * each (same grid, diffusivities, dt and modes; their own Ekman numbers through

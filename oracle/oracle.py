@@ -295,7 +295,7 @@ class Oracle:
     # -- ts_scheme = :eab2 / :erk2 (test restatement) ----------------------------
     def etd_cache(self, kind):
         """create_etd_cache / create_erk2_cache (src/timestep.jl:37-70, 896-968)
-        for a field kind (0 velocity, 1 magnetic, 2 temperature) at the
+        for a field kind (0 velocity, 1 magnetic, 2 temperature, 3 composition) at the
         configuration's dt: per degree l the dense operator A_l (the L_l band of
         the implicit matrices, src/timestep.jl:498-543) and the matrices E, phi1,
         phi2 of dt A_l and E, phi1 of dt A_l / 2.  exp is scipy.linalg.expm
@@ -347,6 +347,10 @@ class Oracle:
 
     FIELD_KINDS = (("u_tor", 0), ("u_pol", 0), ("b_tor", 1), ("b_pol", 1), ("temp", 2))
 
+    def field_kinds(self):
+        """The implicit fields and their diffusivity kinds (composition when configured)."""
+        return self.FIELD_KINDS + ((("comp", 3),) if self.cfg.composition else ())
+
     def eab2_step(self, caches, history):
         """One step of step_once! under ts_scheme = :eab2: the three nonlinear
         phases, then for every field u <- E_l u + dt phi1_l (3/2 N - 1/2 N_prev)
@@ -358,7 +362,9 @@ class Oracle:
         self.temperature_nl()
         self.velocity_nl()
         self.magnetic_nl()
-        for name, kind in self.FIELD_KINDS:
+        if self.cfg.composition:
+            self.composition_nl()
+        for name, kind in self.field_kinds():
             c = caches[kind]
             re, im = self.get_field(name)
             nre, nim = self.get_nl(name)
@@ -369,10 +375,13 @@ class Oracle:
             history[name] = (nre, nim)
 
     def _all_nonlinear(self):
-        # compute_all_nonlinear_terms! (src/simulation.jl:800-813): velocity, magnetic, temperature
+        # compute_all_nonlinear_terms! (src/simulation.jl:800-813): velocity,
+        # magnetic, temperature, composition
         self.velocity_nl()
         self.magnetic_nl()
         self.temperature_nl()
+        if self.cfg.composition:
+            self.composition_nl()
 
     def erk2_step(self, caches):
         """One step of step_once! under ts_scheme = :erk2: the three nonlinear
@@ -386,8 +395,10 @@ class Oracle:
         self.temperature_nl()
         self.velocity_nl()
         self.magnetic_nl()
+        if self.cfg.composition:
+            self.composition_nl()
         saved = {}
-        for name, kind in self.FIELD_KINDS:
+        for name, kind in self.field_kinds():
             c = caches[kind]
             u = self.get_field(name)
             nn = self.get_nl(name)
@@ -397,7 +408,7 @@ class Oracle:
             saved[name] = ([p[0] for p in prep], [p[1] for p in prep], nn)
             self.set_field(name, *[p[2] for p in prep])
         self._all_nonlinear()
-        for name, kind in self.FIELD_KINDS:
+        for name, kind in self.field_kinds():
             c = caches[kind]
             lin, k1, nn = saved[name]
             ns = self.get_nl(name)

@@ -185,3 +185,38 @@ def test_device_exponential_matches_reference_krylov_action(gdb, oracle_mod, nr,
             y, _ = oracle_mod.exp_action_krylov(A, v, dt)
             assert rel(E @ v, y) <= 1e-8, (kind, l, rel(E @ v, y))
     g.close()
+
+
+@pytest.mark.parametrize("scheme", ["eab2", "erk2"])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("mixed", 1e-5)])
+def test_exponential_schemes_with_composition(gdb, oracle_mod, scheme, precision, tol):
+    # composition (kind 3, nu = Pm/Sc) steps with the same dense operators: the
+    # reference's EAB2 applies them by Krylov (src/simulation.jl:1286-1290), its
+    # ERK2 with the dense caches (:1094-1145); compute_all_nonlinear_terms!
+    # ends with the composition phase
+    kw = dict(composition=1, schmidt=2.5, dt=2e-6)
+    g = gdb.SHTnsKitConfig(15, 24, 48, 12, precision=precision, **kw)
+    g.set_scheme(scheme)
+    o = oracle_mod.Oracle(lmax=15, nlat=24, nlon=48, nr=12, **kw)
+    for k, (a, b) in workloads.seeded_state(15, 15, 12, seed=13).items():
+        g.set_field(k, a, b)
+        o.set_field(k, a, b)
+    cst = workloads.seeded_state(15, 15, 12, seed=113)["temp"]
+    g.set_field("comp", *cst)
+    o.set_field("comp", *cst)
+    cbv = np.random.default_rng(6).standard_normal((2, g.nlm)) * 1e-3
+    g.set_composition_bc(cbv, np.linspace(-0.2, 0.2, 12))
+    o.set_composition_bc(cbv, np.linspace(-0.2, 0.2, 12))
+    got = g.etd_matrices("composition", 3)
+    caches = [o.etd_cache(kind) for kind in range(4)]
+    assert rel(got["E"], caches[3]["E"][3]) < 1e-12
+    history = {}
+    for n in range(3):
+        g.step(1)
+        if scheme == "eab2":
+            o.eab2_step(caches, history)
+        else:
+            o.erk2_step(caches)
+        for k in NAMES + ("comp",):
+            a, b = g.get_field(k), o.get_field(k)
+            assert rel(a[0], b[0]) < tol and rel(a[1], b[1]) < tol, (n, k)
