@@ -79,7 +79,8 @@ EXPORTS = (
     "gd_derivatives", "gd_implicit_modes", "gd_set_external_derivatives", "gd_copy_block",
     "gd_set_launch_shape", "gd_get_launch_shape", "gd_ensemble_autotune", "gd_step_kernels",
     "gd_snapshot_bytes", "gd_snapshot", "gd_spectral_device", "gd_grid_device", "gd_temperature_nl_adjoint",
-    "gd_cnab2_adjoint", "gd_temperature_forward", "gd_temperature_pullback",
+    "gd_cnab2_adjoint", "gd_temperature_forward", "gd_temperature_pullback", "gd_velocity_nl_adjoint",
+    "gd_velocity_pullback",
     "gd_set_composition_bc", "gd_set_scalar_bc_types", "gd_composition_nonlinear",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
@@ -201,6 +202,8 @@ def load_library():
         "gd_grid_device": ([P, I, P], I),
         "gd_temperature_nl_adjoint": ([P, P, P, P, P], I),
         "gd_cnab2_adjoint": ([P, I, I, P, P], I),
+        "gd_velocity_nl_adjoint": ([P, P, P], I),
+        "gd_velocity_pullback": ([P, I] + [D] * 8, I),
         "gd_temperature_forward": ([P, I, I], I),
         "gd_temperature_pullback": ([P, D, D, D, D], I),
         "gd_ensemble_autotune": ([P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
@@ -496,6 +499,22 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_temperature_pullback(self.h, _dptr(_f64(lam_re)), _dptr(_f64(lam_im)),
                                                      _dptr(re), _dptr(im)))
         return re, im
+
+    def velocity_nl_adjoint(self, psi, out):
+        """out = N^T psi for the velocity's (Coriolis) nonlinear term; psi, out:
+        device tensors holding (tor, pol) in gd_snapshot's spectral layout."""
+        self._check(self.lib.gd_velocity_nl_adjoint(self.h, ctypes.c_void_p(psi.data_ptr()),
+                                                    ctypes.c_void_p(out.data_ptr())))
+
+    def velocity_pullback(self, nsteps, lam_tor, lam_pol):
+        """Pullback of the handle's last nsteps steps w.r.t. (u_tor, u_pol) at
+        their start: the cotangents (re, im) of the velocity after them ->
+        (tor (re, im), pol (re, im))."""
+        out = [np.zeros(self.spec_shape()) for _ in range(4)]
+        self._check(self.lib.gd_velocity_pullback(self.h, int(nsteps), _dptr(_f64(lam_tor[0])), _dptr(_f64(lam_tor[1])),
+                                                  _dptr(_f64(lam_pol[0])), _dptr(_f64(lam_pol[1])),
+                                                  *[_dptr(o) for o in out]))
+        return (out[0], out[1]), (out[2], out[3])
 
     def magnetic_pullback(self, name, nsteps, lam_re, lam_im):
         """Pullback of nsteps steps w.r.t. the magnetic component ``name``

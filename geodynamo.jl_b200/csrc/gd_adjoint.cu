@@ -136,6 +136,22 @@ void launch_scale_by_order(cudaStream_t s, size_t nrows, int nlm, const int* mof
   k_scale_by_order<<<592, 256, 0, s>>>(nrows, nlm, mof, f0, f1, a);
 }
 
+// a *= f l(l+1) (inverse 0) or f / (l(l+1)) with 0 at l = 0 (inverse 1), per
+// native mode j of every row
+__global__ void k_scale_by_degree(size_t nrows, int nlm, const int* __restrict__ lof, double f, int inverse,
+                                  double* __restrict__ a) {
+  const size_t n = nrows * (size_t)nlm;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int l = lof[e % nlm];
+    const double lf = (double)l * (l + 1.0);
+    a[e] *= inverse ? (l > 0 ? f / lf : 0.0) : f * lf;
+  }
+}
+
+void launch_scale_by_degree(cudaStream_t s, size_t nrows, int nlm, const int* lof, double f, int inverse, double* a) {
+  k_scale_by_degree<<<592, 256, 0, s>>>(nrows, nlm, lof, f, inverse, a);
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint of the temperature step (reverse mode of step_once! with respect to
 // the temperature).  In the reference's step the temperature obeys
@@ -202,7 +218,8 @@ __global__ void __launch_bounds__(128) k_cnab2_adjoint(Dims d, const int* __rest
       double acc = 0.0;
       for (int k = i - KL < 0 ? 0 : i - KL; k <= i + KL && k < N; ++k) acc += band(Lb, k, i) * xc[(size_t)k * NM];
       double v = inv_dt * xc[(size_t)i * NM] + lin_weight * acc;
-      if ((i == 0 && types[j] == GD_BC_VALUE) || (i == N - 1 && types[NM + j] == GD_BC_VALUE)) v = 0.0;
+      // P: the scalar fields' fixed-value rows (no projection for the potentials, types null)
+      if (types && ((i == 0 && types[j] == GD_BC_VALUE) || (i == N - 1 && types[NM + j] == GD_BC_VALUE))) v = 0.0;
       yc[(size_t)i * NM] = v;
     }
   }

@@ -1079,7 +1079,7 @@ int gd_temperature_nl_adjoint(gd_handle* h, const double* u_th, const double* u_
   if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "the nonlinear-term adjoint");
   CK(cudaSetDevice(h->device));
   const size_t se = h->spec_elems(), G = h->grid_elems();
-  if (!h->d_adj) AL(h->d_adj, 3 * se + 3 * G);
+  if (!h->d_adj) AL(h->d_adj, 3 * se + 4 * G);
   double* nup = h->d_adj;        // D nu
   double* ath = nup + se;        // An(-u_th g), then D' scaled
   double* aph = ath + se;
@@ -1122,7 +1122,6 @@ int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double*
         return fail(h, GD_ERR_UNSUPPORTED, "the adjoint covers fixed-value boundaries (no tau flux rows)");
     types = h->d_bctype + o;
   }
-  if (!scalar && mode == 1) return fail(h, GD_ERR_UNSUPPORTED, "mode 1 (P R^T) is for the scalar fields");
   CK(cudaSetDevice(h->device));
   launch_cnab2_adjoint(h->stream, h->d, h->d_lof, h->d_lin, h->d_lu, types, kind, mode, h->c.dt, h->c.implicit_theta,
                        h->c.bc_mode == 1, h->c.bc_mode == 2, x, y);
@@ -1405,6 +1404,105 @@ int gd_spectral_to_physical_adjoint(gd_handle* h, int nfield, const double* grid
     CK(cudaStreamSynchronize(h->stream));
   }
   return check_launch(h, "spectral_to_physical_adjoint");
+}
+
+// The velocity's nonlinear term of the literal step is its Coriolis term alone
+// (u x w and j x B vanish with zero radial components), linear in u:
+//   N = VecAn Cor VecSyn,  Cor = pointwise [[0, -c], [c, 0]], c = Pm/E cos(theta(min(j, nlat - 1))),
+// with VecAn = Lambda^-1 VecSyn^T W D^-1 (Lambda = l(l+1), W the Gauss weights
+// and D = 2 pi / nlon (m = 0), pi / nlon (m > 0) the real-coefficient
+// weighting of the phi sums), so VecSyn^T = D^-1 Lambda VecAn W^-1 and
+// VecAn^T = W VecSyn Lambda^-1 D; Cor is antisymmetric, hence
+//   N^T = -D^-1 Lambda N Lambda^-1 D,
+// evaluated with the FP64 forward kernels.  psi, out: (tor, pol) consecutive,
+// spec_elems each, native layout on the device.
+int gd_velocity_nl_adjoint(gd_handle* h, const double* psi, double* out) {
+  if (!h || !psi || !out) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "the velocity nonlinear-term adjoint");
+  CK(cudaSetDevice(h->device));
+  const size_t se = h->spec_elems(), G = h->grid_elems();
+  if (!h->d_adj) AL(h->d_adj, 3 * se + 4 * G);
+  const Dims& d = h->d;
+  double* x = h->d_adj;               // Lambda^-1 D psi, tor then pol
+  double* g = h->d_adj + 3 * se;      // VecSyn x: theta, phi
+  double* z = g + 2 * G;              // Cor VecSyn x: theta, phi
+  const double tp = 2.0 * 3.14159265358979323846 / d.nlon;
+  CK(cudaMemcpyAsync(x, psi, 2 * se * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  launch_scale_by_order(h->stream, 4 * (size_t)d.nr, d.nlm, h->d_mof, tp, 0.5 * tp, x);
+  launch_scale_by_degree(h->stream, 4 * (size_t)d.nr, d.nlm, h->d_lof, 1.0, 1, x);
+  int s = synth_vector(h, x, x + se, g);
+  if (s) return s;
+  const double rf = h->c.magnetic_prandtl / h->c.ekman;
+  launch_coriolis<double>(h->stream, d, h->d_cth, h->d_sthc, rf, g, g + G, z, z + G);
+  s = analysis_vector(h, z, out, out + se, EPI_VECTOR);
+  if (s) return s;
+  launch_scale_by_degree(h->stream, 4 * (size_t)d.nr, d.nlm, h->d_lof, -1.0, 0, out);
+  launch_scale_by_order(h->stream, 4 * (size_t)d.nr, d.nlm, h->d_mof, 1.0 / tp, 2.0 / tp, out);
+  s = check_launch(h, "velocity nonlinear adjoint");
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
+}
+
+// Reverse mode of the last nsteps CNAB2 steps of the velocity (those that end
+// at the handle's step count; the bootstrap pattern follows from it):
+// u^(n+1) = C S^-1 D (R u^n + a_n N u^n - b_n N u^(n-1)) (AB2 weights
+// a = 3/2, b = 1/2; a = 1, b = 0 on a bootstrap step), so with
+// psi^(n+1) = D S^-T C lambda^(n+1):
+//   lambda^n = R^T psi^(n+1) + N^T (a_n psi^(n+1) - b_(n+1) psi^(n+2)).
+// Linear and independent of the state (N is the Coriolis term), so no
+// checkpoints; lambda^0 is the gradient with respect to (u_tor, u_pol) at the
+// start.  The pullback of the FP64 step, whatever the handle's precision.
+int gd_velocity_pullback(gd_handle* h, int nsteps, const double* lam_tor_re, const double* lam_tor_im,
+                         const double* lam_pol_re, const double* lam_pol_im, double* out_tor_re, double* out_tor_im,
+                         double* out_pol_re, double* out_pol_im) {
+  if (!h || nsteps < 0 || !lam_tor_re || !lam_tor_im || !lam_pol_re || !lam_pol_im || !out_tor_re || !out_tor_im ||
+      !out_pol_re || !out_pol_im)
+    return h ? fail(h, GD_ERR_ARG, "bad arguments") : GD_ERR_ARG;
+  if (h->scheme != GD_SCHEME_CNAB2) return fail(h, GD_ERR_UNSUPPORTED, "the pullback is of the CNAB2 step");
+  if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "the velocity pullback");
+  if (h->step_count < nsteps) return fail(h, GD_ERR_STATE, "the handle has not run the steps to pull back");
+  CK(cudaSetDevice(h->device));
+  const size_t se = h->spec_elems();
+  const long s0 = h->step_count - nsteps;
+  const bool ab1 = h->c.ab_mode == 1;
+  auto boot = [&](int n) { return ab1 || s0 + n == 0; };
+  double* lam = nullptr;  // lam, psi1, psi2, tmp, nlt: (tor, pol) each
+  if (cudaMalloc(&lam, 10 * se * sizeof(double)) != cudaSuccess)
+    return fail(h, GD_ERR_CUDA, "out of device memory for the pullback");
+  double *psi1 = lam + 2 * se, *psi2 = psi1 + 2 * se, *tmp = psi2 + 2 * se, *nlt = tmp + 2 * se;
+  auto done = [&](int st) {
+    cudaFree(lam);
+    return st;
+  };
+  auto solveT = [&](const double* x, double* y) {  // D S^-T C per potential
+    int st = gd_cnab2_adjoint(h, GD_U_TOR, 0, x, y);
+    return st ? st : gd_cnab2_adjoint(h, GD_U_POL, 0, x + se, y + se);
+  };
+  int s = gd_spectral_device(h, const_cast<double*>(lam_tor_re), const_cast<double*>(lam_tor_im), lam, 1);
+  if (!s) s = gd_spectral_device(h, const_cast<double*>(lam_pol_re), const_cast<double*>(lam_pol_im), lam + se, 1);
+  if (s) return done(s);
+  if (nsteps > 0) {
+    s = solveT(lam, psi1);
+    CK(cudaMemsetAsync(psi2, 0, 2 * se * sizeof(double), h->stream));
+  }
+  for (int n = nsteps - 1; n >= 0 && s == GD_OK; --n) {
+    const double a_n = boot(n) ? 1.0 : 1.5;
+    const double b_n1 = (n + 1 >= nsteps || boot(n + 1)) ? 0.0 : 0.5;
+    launch_axpby(h->stream, 2 * se, a_n, psi1, -b_n1, psi2, tmp);
+    s = gd_velocity_nl_adjoint(h, tmp, nlt);
+    if (s == GD_OK) s = gd_cnab2_adjoint(h, GD_U_TOR, 1, psi1, lam);
+    if (s == GD_OK) s = gd_cnab2_adjoint(h, GD_U_POL, 1, psi1 + se, lam + se);
+    if (s == GD_OK) launch_axpby(h->stream, 2 * se, 1.0, lam, 1.0, nlt, lam);
+    if (s == GD_OK && n > 0) {
+      std::swap(psi1, psi2);
+      s = solveT(lam, psi1);
+    }
+  }
+  if (s == GD_OK) s = gd_spectral_device(h, out_tor_re, out_tor_im, lam, 0);
+  if (s == GD_OK) s = gd_spectral_device(h, out_pol_re, out_pol_im, lam + se, 0);
+  if (s == GD_OK) s = check_launch(h, "velocity pullback");
+  return done(s);
 }
 
 int gd_magnetic_pullback(gd_handle* h, int field, int nsteps, const double* lam_re, const double* lam_im,

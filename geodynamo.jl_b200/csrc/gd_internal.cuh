@@ -202,6 +202,7 @@ void launch_cnab2_pullback(cudaStream_t s, const Dims& d, const int* lof, const 
                            int kind, double dt, double theta, int clamp_rows, int bc_rows, int nsteps, double* lam);
 void launch_divide_by_weights(cudaStream_t s, size_t n, int nlat, const double* w, double* g);
 void launch_scale_by_order(cudaStream_t s, size_t nrows, int nlm, const int* mof, double f0, double f1, double* a);
+void launch_scale_by_degree(cudaStream_t s, size_t nrows, int nlm, const int* lof, double f, int inverse, double* a);
 // Temperature adjoint pieces (gd_adjoint.cu).
 void launch_cnab2_adjoint(cudaStream_t s, const Dims& d, const int* lof, const double* lin, const double* lu,
                           const int* types, int kind, int mode, double dt, double theta, int clamp_rows, int bc_rows,

@@ -1,4 +1,5 @@
-# Reverse-mode rules of GeoDynamoB200.evolve_magnetic and evolve_temperature, loaded when
+# Reverse-mode rules of GeoDynamoB200.evolve_magnetic, evolve_temperature and
+# evolve_velocity, loaded when
 # ChainRulesCore is: the pullback of nsteps model steps with respect to the
 # magnetic component they start from is the library's hand-written transposed
 # propagator (gd_magnetic_pullback: per step the transposed band solve and the
@@ -37,6 +38,23 @@ function ChainRulesCore.rrule(::typeof(GeoDynamoB200.evolve_temperature), h::Geo
         return NoTangent(), NoTangent(), gre, gim, NoTangent()
     end
     return out, evolve_temperature_pullback
+end
+
+# evolve_velocity: the pullback of the steps just run with respect to the velocity
+# potentials they started from (gd_velocity_pullback).
+function ChainRulesCore.rrule(::typeof(GeoDynamoB200.evolve_velocity), h::GeoDynamoB200.Handle,
+                              tor::Tuple, pol::Tuple, nsteps::Integer)
+    out = GeoDynamoB200.evolve_velocity(h, tor, pol, nsteps)
+    z(x, like) = x isa AbstractZero ? zeros(size(like)) : Array{Float64}(unthunk(x))
+    function evolve_velocity_pullback(Δ)
+        d = unthunk(Δ)
+        dt = d[1] isa AbstractZero ? (zeros(size(tor[1])), zeros(size(tor[2]))) : unthunk(d[1])
+        dp = d[2] isa AbstractZero ? (zeros(size(pol[1])), zeros(size(pol[2]))) : unthunk(d[2])
+        gt, gp = GeoDynamoB200.velocity_pullback(h, nsteps, (z(dt[1], tor[1]), z(dt[2], tor[2])),
+                                                 (z(dp[1], pol[1]), z(dp[2], pol[2])))
+        return NoTangent(), NoTangent(), Tangent{typeof(tor)}(gt...), Tangent{typeof(pol)}(gp...), NoTangent()
+    end
+    return out, evolve_velocity_pullback
 end
 
 end # module

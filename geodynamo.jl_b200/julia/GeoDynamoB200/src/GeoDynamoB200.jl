@@ -329,6 +329,36 @@ function temperature_pullback(h::Handle, lre::AbstractArray{Float64}, lim::Abstr
     return gre, gim
 end
 
+# evolve_velocity(h, (tre, tim), (pre, pim), nsteps) sets the velocity
+# potentials of h's state, runs nsteps model steps and returns them afterwards;
+# its rrule (the extension) pulls the cotangents back with
+# gd_velocity_pullback.  The literal step's velocity depends on itself alone
+# and linearly (its nonlinear term is the Coriolis term), so no checkpoints.
+function evolve_velocity(h::Handle, tor::Tuple, pol::Tuple, nsteps::Integer)
+    tr = Array{Float64}(tor[1]); ti = Array{Float64}(tor[2])
+    pr = Array{Float64}(pol[1]); pi = Array{Float64}(pol[2])
+    for (f, a, b) in ((:u_tor, tr, ti), (:u_pol, pr, pi))
+        GC.@preserve a b check(h, ccall((:gd_upload_spectral, LIB), Cint,
+            (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, FIELD[f], a, b))
+    end
+    check(h, ccall((:gd_step, LIB), Cint, (Ptr{Cvoid}, Cint), h.ptr, nsteps))
+    for (f, a, b) in ((:u_tor, tr, ti), (:u_pol, pr, pi))
+        GC.@preserve a b check(h, ccall((:gd_download_spectral, LIB), Cint,
+            (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}), h.ptr, FIELD[f], a, b))
+    end
+    return (tr, ti), (pr, pi)
+end
+
+function velocity_pullback(h::Handle, nsteps::Integer, ltor::Tuple, lpol::Tuple)
+    out = [similar(Array{Float64}(ltor[1])) for _ in 1:4]
+    a = [Array{Float64}(x) for x in (ltor[1], ltor[2], lpol[1], lpol[2])]
+    GC.@preserve a out check(h, ccall((:gd_velocity_pullback, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+         Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+        h.ptr, nsteps, a[1], a[2], a[3], a[4], out[1], out[2], out[3], out[4]))
+    return (out[1], out[2]), (out[3], out[4])
+end
+
 # Transpose of spectral_to_physical! (gd_spectral_to_physical_adjoint).
 function spectral_to_physical_adjoint!(h::Handle, phys_bar, spec_bar)
     g = parent(phys_bar.data); re = parent(spec_bar.data_real); im = parent(spec_bar.data_imag)

@@ -483,9 +483,27 @@ int gd_grid_device(gd_handle* h, int grid, double* dev);
  * transposed spectral gradient (theta recurrence and i m, over r), FP64. */
 int gd_temperature_nl_adjoint(gd_handle* h, const double* u_th, const double* u_ph, const double* nu, double* out);
 /* mode 0: y = D S^-T C x; mode 1: y = P R^T x (scalar fields: P zeroes the
- * fixed-value boundary rows), with the field's implicit operators.  Fixed-value
- * boundaries only: GD_ERR_UNSUPPORTED when the field has flux boundaries. */
+ * fixed-value boundary rows; the potentials have no P), with the field's
+ * implicit operators.  Fixed-value boundaries only: GD_ERR_UNSUPPORTED when the
+ * field has flux boundaries. */
 int gd_cnab2_adjoint(gd_handle* h, int field, int mode, const double* x, double* y);
+/* out = N^T psi for the velocity's nonlinear term, which in the literal step is
+ * its Coriolis term alone (u x w and j x B vanish with zero radial components;
+ * src/velocity.jl:492-496): N = VecAn Cor VecSyn with Cor antisymmetric per
+ * grid point, so N^T = -D^-1 Lambda N Lambda^-1 D (Lambda = l(l+1), D the
+ * real-coefficient weights of the phi sums).  psi, out: (tor, pol) consecutive
+ * device arrays of gd_snapshot's spectral layout (spec_elems doubles each), FP64. */
+int gd_velocity_nl_adjoint(gd_handle* h, const double* psi, double* out);
+/* Vector-Jacobian product of the last nsteps CNAB2 steps the handle ran (those
+ * ending at its step count; GD_ERR_STATE if it ran fewer) with respect to
+ * (u_tor, u_pol) at their start: lambda (host, l-major (nr, nlm) planes) is the
+ * cotangent of the velocity after the steps.  The velocity
+ * of the literal step depends on nothing but itself (Q2: no buoyancy; the
+ * Lorentz term vanishes), linearly, so no checkpoints are needed.  The
+ * pullback of the FP64 step. */
+int gd_velocity_pullback(gd_handle* h, int nsteps, const double* lam_tor_re, const double* lam_tor_im,
+                         const double* lam_pol_re, const double* lam_pol_im, double* out_tor_re, double* out_tor_im,
+                         double* out_pol_re, double* out_pol_im);
 /* The pieces composed with checkpoint and recompute.  gd_temperature_forward
  * runs nsteps steps keeping a snapshot every checkpoint_every steps (and one
  * of the end state) in device memory owned by the handle (FP64, CNAB2).
