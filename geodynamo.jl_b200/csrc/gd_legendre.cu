@@ -12,6 +12,7 @@
 #include <stdint.h>
 
 #include "gd_internal.cuh"
+#include "gd_mixed_kernels.cuh"
 
 namespace gd {
 
@@ -394,8 +395,9 @@ __global__ void __launch_bounds__(256, 2) k_synth_vector(Dims d, const int* __re
           v32[1][s] = vph;
         }
         if (a.out32 != nullptr) {
-          const size_t run = (size_t)((d.nth + 1) / 2) * (d.M + 1) * 2;
-          const size_t off = (size_t)r * run + ((size_t)(ith >> 1) * (d.M + 1) + m) * 2 + (ith & 1);
+          constexpr int FBK = FOURIER_BLOCK;
+          const size_t run = (size_t)((d.nth + FBK - 1) / FBK) * (d.M + 1) * FBK;
+          const size_t off = (size_t)r * run + ((size_t)(ith / FBK) * (d.M + 1) + m) * FBK + ith % FBK;
 #pragma unroll
           for (int c = 0; c < 2; ++c)
             a.out32[c * a.out32_comp + off] = make_float4((float)v32[c][0].x, (float)v32[c][0].y,
