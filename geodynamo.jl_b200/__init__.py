@@ -80,7 +80,7 @@ EXPORTS = (
     "gd_set_launch_shape", "gd_get_launch_shape", "gd_ensemble_autotune", "gd_step_kernels",
     "gd_snapshot_bytes", "gd_snapshot", "gd_spectral_device", "gd_grid_device", "gd_temperature_nl_adjoint",
     "gd_cnab2_adjoint", "gd_temperature_forward", "gd_temperature_pullback", "gd_velocity_nl_adjoint",
-    "gd_velocity_pullback",
+    "gd_velocity_pullback", "gd_temperature_pullback_full", "gd_temperature_u_adjoint",
     "gd_set_composition_bc", "gd_set_scalar_bc_types", "gd_composition_nonlinear",
     "gd_spectral_to_physical_adjoint", "gd_magnetic_pullback",
     "gd_ensemble_create", "gd_ensemble_destroy", "gd_ensemble_size", "gd_ensemble_member",
@@ -204,6 +204,8 @@ def load_library():
         "gd_cnab2_adjoint": ([P, I, I, P, P], I),
         "gd_velocity_nl_adjoint": ([P, P, P], I),
         "gd_velocity_pullback": ([P, I] + [D] * 8, I),
+        "gd_temperature_pullback_full": ([P] + [D] * 8, I),
+        "gd_temperature_u_adjoint": ([P, P, P, P, P], I),
         "gd_temperature_forward": ([P, I, I], I),
         "gd_temperature_pullback": ([P, D, D, D, D], I),
         "gd_ensemble_autotune": ([P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
@@ -499,6 +501,14 @@ class SHTnsKitConfig:
         self._check(self.lib.gd_temperature_pullback(self.h, _dptr(_f64(lam_re)), _dptr(_f64(lam_im)),
                                                      _dptr(re), _dptr(im)))
         return re, im
+
+    def temperature_pullback_full(self, lam_re, lam_im):
+        """Cotangent of the temperature after the checkpointed run -> (temperature
+        (re, im), u_tor (re, im), u_pol (re, im)) at its start (gd_temperature_pullback_full)."""
+        out = [np.zeros(self.spec_shape()) for _ in range(6)]
+        self._check(self.lib.gd_temperature_pullback_full(self.h, _dptr(_f64(lam_re)), _dptr(_f64(lam_im)),
+                                                          *[_dptr(o) for o in out]))
+        return (out[0], out[1]), (out[2], out[3]), (out[4], out[5])
 
     def velocity_nl_adjoint(self, psi, out):
         """out = N^T psi for the velocity's (Coriolis) nonlinear term; psi, out:

@@ -860,58 +860,146 @@ int gd_temperature_forward(gd_handle* h, int nsteps, int checkpoint_every) {
   return GD_OK;
 }
 
-int gd_temperature_pullback(gd_handle* h, const double* lam_re, const double* lam_im, double* out_re, double* out_im) {
+// The reverse pass of gd_temperature_forward's run.  Temperature:
+//   lambda_T^n = P R^T psi^(n+1) + N_n^T nu_n,  nu_n = a_n psi^(n+1) - b_(n+1) psi^(n+2),
+//   psi^n = D S^-T C lambda_T^n.
+// With uv (the velocity outputs), also the gradient with respect to the
+// velocity at the start: step n's advection reads the velocity grids
+// VecSyn(u^(n-1)) of the previous velocity phase (the grids carried into the
+// window at n = 0, constant), so u^(n-1) receives
+//   s^(n-1) = VecSyn^T(-(An^T nu_n) (G_th T^n, G_ph T^n))   (gd_temperature_u_adjoint)
+// and the velocity recursion of gd_velocity_pullback carries it back:
+//   lambda_u^n = R^T psi_u^(n+1) + N_u^T(a_n psi_u^(n+1) - b_(n+1) psi_u^(n+2)) + s^n.
+static int temperature_pullback_impl(gd_handle* h, const double* lam_re, const double* lam_im, double* out_re,
+                                     double* out_im, double* const* uv) {
   if (!h || !lam_re || !lam_im || !out_re || !out_im) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
   if (h->t_nsteps < 1) return fail(h, GD_ERR_STATE, "no checkpointed forward run (gd_temperature_forward)");
   CK(cudaSetDevice(h->device));
   const size_t se = h->spec_elems(), G = h->grid_elems();
   const int K = h->t_nsteps, C = h->t_every, nseg = (K + C - 1) / C;
   const bool ab1 = h->c.ab_mode == 1;
+  const bool vel = uv != nullptr;
+  const int ng = vel ? 4 : 2;  // grids kept per step: u_th, u_ph (and G_th T, G_ph T)
   auto boot = [&](int n) { return ab1 || h->t_s0 + n == 0; };
-  // lam, psi1, psi2, tmp, nlt share one allocation; ust holds a segment's velocity grids
+  // temperature: lam, psi1, psi2, tmp, nlt; velocity: lam, psi1, psi2, tmp, nlt, src (2 se each)
   double *lam = nullptr, *ust = nullptr;
-  if (cudaMalloc(&lam, 5 * se * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&ust, (size_t)C * 2 * G * sizeof(double)) != cudaSuccess) {
+  if (cudaMalloc(&lam, (5 + (vel ? 12 : 0)) * se * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&ust, (size_t)C * ng * G * sizeof(double)) != cudaSuccess) {
     if (lam) cudaFree(lam);
     return fail(h, GD_ERR_CUDA, "out of device memory for the pullback");
   }
   double *psi1 = lam + se, *psi2 = psi1 + se, *tmp = psi2 + se, *nlt = tmp + se;
+  double* ul = nlt + se;  // velocity block
+  double *upsi1 = ul + 2 * se, *upsi2 = upsi1 + 2 * se, *utmp = upsi2 + 2 * se, *unlt = utmp + 2 * se,
+         *usrc = unlt + 2 * se;
   auto done = [&](int st) {
     cudaFree(lam);
     cudaFree(ust);
     return st;
+  };
+  auto usolve = [&](const double* x, double* y) {  // D S^-T C per potential
+    int st = gd_cnab2_adjoint(h, GD_U_TOR, 0, x, y);
+    return st ? st : gd_cnab2_adjoint(h, GD_U_POL, 0, x + se, y + se);
   };
   int s = gd_spectral_device(h, const_cast<double*>(lam_re), const_cast<double*>(lam_im), lam, 1);
   if (s) return done(s);
   s = gd_cnab2_adjoint(h, GD_TEMP, 0, lam, psi1);
   if (s) return done(s);
   CK(cudaMemsetAsync(psi2, 0, se * sizeof(double), h->stream));
+  if (vel) {
+    // the velocity after the run carries no cotangent of its own here
+    CK(cudaMemsetAsync(ul, 0, 12 * se * sizeof(double), h->stream));
+  }
   for (int k = nseg - 1; k >= 0 && s == GD_OK; --k) {
     const int c0 = k * C, c1 = std::min(K, c0 + C);
     s = gd_snapshot(h, h->t_snaps[k], 1);
     for (int n = c0; n < c1 && s == GD_OK; ++n) {
-      double* u = ust + (size_t)(n - c0) * 2 * G;
+      double* u = ust + (size_t)(n - c0) * ng * G;
       s = gd_grid_device(h, GD_GRID_U_TH, u);
       if (s == GD_OK) s = gd_grid_device(h, GD_GRID_U_PH, u + G);
-      if (s == GD_OK && n < c1 - 1) s = gd_step(h, 1);
+      if (s == GD_OK && (vel || n < c1 - 1)) s = gd_step(h, 1);
+      // the temperature gradient grids of step n's temperature phase
+      if (s == GD_OK && vel) s = gd_grid_device(h, GD_GRID_GTH, u + 2 * G);
+      if (s == GD_OK && vel) s = gd_grid_device(h, GD_GRID_GPH, u + 3 * G);
     }
     for (int n = c1 - 1; n >= c0 && s == GD_OK; --n) {
       const double a_n = boot(n) ? 1.0 : 1.5;
       const double b_n1 = (n + 1 >= K || boot(n + 1)) ? 0.0 : 0.5;
-      launch_axpby(h->stream, se, a_n, psi1, -b_n1, psi2, tmp);
-      const double* u = ust + (size_t)(n - c0) * 2 * G;
+      launch_axpby(h->stream, se, a_n, psi1, -b_n1, psi2, tmp);  // nu_n
+      const double* u = ust + (size_t)(n - c0) * ng * G;
       s = gd_temperature_nl_adjoint(h, u, u + G, tmp, nlt);
       if (s == GD_OK) s = gd_cnab2_adjoint(h, GD_TEMP, 1, psi1, lam);
       if (s == GD_OK) launch_axpby(h->stream, se, 1.0, lam, 1.0, nlt, lam);
+      if (s == GD_OK && vel) {
+        // lambda_u^n with the source s^n of step n + 1 (usrc), then the source of step n
+        launch_axpby(h->stream, 2 * se, a_n, upsi1, -b_n1, upsi2, utmp);
+        s = gd_velocity_nl_adjoint(h, utmp, unlt);
+        if (s == GD_OK) s = gd_cnab2_adjoint(h, GD_U_TOR, 1, upsi1, ul);
+        if (s == GD_OK) s = gd_cnab2_adjoint(h, GD_U_POL, 1, upsi1 + se, ul + se);
+        if (s == GD_OK) launch_axpby(h->stream, 2 * se, 1.0, ul, 1.0, unlt, ul);
+        if (s == GD_OK) launch_axpby(h->stream, 2 * se, 1.0, ul, 1.0, usrc, ul);
+        if (s == GD_OK && n >= 1) s = gd_temperature_u_adjoint(h, u + 2 * G, u + 3 * G, tmp, usrc);
+        if (s == GD_OK && n == 0) CK(cudaMemsetAsync(usrc, 0, 2 * se * sizeof(double), h->stream));
+      }
       if (s == GD_OK && n > 0) {
         std::swap(psi1, psi2);
         s = gd_cnab2_adjoint(h, GD_TEMP, 0, lam, psi1);
+        if (s == GD_OK && vel) {
+          std::swap(upsi1, upsi2);
+          s = usolve(ul, upsi1);
+        }
       }
     }
   }
   if (s == GD_OK) s = gd_snapshot(h, h->t_final, 1);
   if (s == GD_OK) s = gd_spectral_device(h, out_re, out_im, lam, 0);
+  if (s == GD_OK && vel) s = gd_spectral_device(h, uv[0], uv[1], ul, 0);
+  if (s == GD_OK && vel) s = gd_spectral_device(h, uv[2], uv[3], ul + se, 0);
   return done(s);
+}
+
+int gd_temperature_pullback(gd_handle* h, const double* lam_re, const double* lam_im, double* out_re, double* out_im) {
+  return temperature_pullback_impl(h, lam_re, lam_im, out_re, out_im, nullptr);
+}
+
+int gd_temperature_pullback_full(gd_handle* h, const double* lam_re, const double* lam_im, double* out_re,
+                                 double* out_im, double* out_tor_re, double* out_tor_im, double* out_pol_re,
+                                 double* out_pol_im) {
+  if (!out_tor_re || !out_tor_im || !out_pol_re || !out_pol_im)
+    return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  double* uv[4] = {out_tor_re, out_tor_im, out_pol_re, out_pol_im};
+  return temperature_pullback_impl(h, lam_re, lam_im, out_re, out_im, uv);
+}
+
+// s = VecSyn^T(-(An^T nu) (gth, gph)) with An^T = W Syn D and VecSyn^T =
+// D^-1 Lambda VecAn W^-1 (the Gauss weights cancel): the cotangent of the
+// velocity potentials whose synthesized grids advect the temperature.
+int gd_temperature_u_adjoint(gd_handle* h, const double* gth, const double* gph, const double* nu, double* out) {
+  if (!h || !gth || !gph || !nu || !out) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
+  if (h->d.nseg > 1 || h->d.ball) return refuse_layout(h, "the temperature-velocity adjoint");
+  CK(cudaSetDevice(h->device));
+  const size_t se = h->spec_elems(), G = h->grid_elems();
+  if (!h->d_adj) AL(h->d_adj, 3 * se + 4 * G);
+  const Dims& d = h->d;
+  double* nup = h->d_adj;            // D nu
+  double* g = h->d_adj + 3 * se;     // Syn(D nu)
+  double* hq = g + G;                // -g gth, -g gph (consecutive for the vector analysis)
+  const double tp = 2.0 * 3.14159265358979323846 / d.nlon;
+  CK(cudaMemcpyAsync(nup, nu, se * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  launch_scale_by_order(h->stream, 2 * (size_t)d.nr, d.nlm, h->d_mof, tp, 0.5 * tp, nup);
+  const double* coef[1] = {nup};
+  int s = synth_scalar(h, coef, 1, g);
+  if (s) return s;
+  launch_neg_product(h->stream, G, gth, g, hq);
+  launch_neg_product(h->stream, G, gph, g, hq + G);
+  s = analysis_vector(h, hq, out, out + se, EPI_VECTOR);
+  if (s) return s;
+  launch_scale_by_degree(h->stream, 4 * (size_t)d.nr, d.nlm, h->d_lof, 1.0, 0, out);
+  launch_scale_by_order(h->stream, 4 * (size_t)d.nr, d.nlm, h->d_mof, 1.0 / tp, 2.0 / tp, out);
+  s = check_launch(h, "temperature-velocity adjoint");
+  if (s) return s;
+  CK(cudaStreamSynchronize(h->stream));
+  return GD_OK;
 }
 
 int gd_set_launch_shape(gd_handle* h, int tc_ctas) {

@@ -359,6 +359,18 @@ function velocity_pullback(h::Handle, nsteps::Integer, ltor::Tuple, lpol::Tuple)
     return (out[1], out[2]), (out[3], out[4])
 end
 
+# The checkpointed run's pullback with respect to the temperature and the
+# velocity potentials at its start (gd_temperature_pullback_full):
+# ((gTre, gTim), (gtor_re, gtor_im), (gpol_re, gpol_im)).
+function temperature_pullback_full(h::Handle, lre::AbstractArray{Float64}, lim::AbstractArray{Float64})
+    out = [similar(lre) for _ in 1:6]
+    GC.@preserve lre lim out check(h, ccall((:gd_temperature_pullback_full, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+         Ptr{Cdouble}, Ptr{Cdouble}),
+        h.ptr, lre, lim, out[1], out[2], out[3], out[4], out[5], out[6]))
+    return (out[1], out[2]), (out[3], out[4]), (out[5], out[6])
+end
+
 # Transpose of spectral_to_physical! (gd_spectral_to_physical_adjoint).
 function spectral_to_physical_adjoint!(h::Handle, phys_bar, spec_bar)
     g = parent(phys_bar.data); re = parent(spec_bar.data_real); im = parent(spec_bar.data_imag)

@@ -518,6 +518,21 @@ int gd_velocity_pullback(gd_handle* h, int nsteps, const double* lam_tor_re, con
  * before writing (u, B, j). */
 int gd_temperature_forward(gd_handle* h, int nsteps, int checkpoint_every);
 int gd_temperature_pullback(gd_handle* h, const double* lam_re, const double* lam_im, double* out_re, double* out_im);
+/* The same, and the gradient with respect to the velocity potentials at the
+ * start of the run: step n's advection reads the grids VecSyn(u^(n-1)) of the
+ * previous velocity phase, so u^(n-1) receives
+ * s^(n-1) = VecSyn^T(-(An^T nu_n) (G_th T^n, G_ph T^n)) (nu_n the cotangent of
+ * step n's nonlinear term) and the velocity recursion of gd_velocity_pullback
+ * carries the sources back; the grids carried into the run (read by its first
+ * step) are constants.  The recompute also keeps each step's temperature
+ * gradient grids (4 grids per step of a segment). */
+int gd_temperature_pullback_full(gd_handle* h, const double* lam_re, const double* lam_im, double* out_re,
+                                 double* out_im, double* out_tor_re, double* out_tor_im, double* out_pol_re,
+                                 double* out_pol_im);
+/* out (tor, pol) = VecSyn^T(-(An^T nu) (gth, gph)): the velocity cotangent of
+ * one step's advection for the temperature gradient grids gth, gph (device
+ * arrays, gd_grid_device layout) and the cotangent nu of its nonlinear term. */
+int gd_temperature_u_adjoint(gd_handle* h, const double* gth, const double* gph, const double* nu, double* out);
 
 /* ---- launch shape -------------------------------------------------------------------
  * No counterpart in the reference.  tc_ctas caps the persistent grid of the

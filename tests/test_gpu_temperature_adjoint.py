@@ -239,3 +239,66 @@ def test_native_pullback_equals_composed_pieces(gdb):
     for x, y in zip(after, m.get_field("temp")):
         assert np.array_equal(x, y)
     m.close()
+
+
+@pytest.mark.parametrize("bc_mode,ab_mode", [(0, 0), (2, 0), (0, 1)])
+def test_temperature_gradient_wrt_velocity_matches_fd(gdb, bc_mode, ab_mode):
+    # J(T^K) depends on the initial velocity through the advection of every
+    # step after the first (each reads the previous velocity phase's grids);
+    # gd_temperature_pullback_full returns that gradient with the temperature's
+    nr, K, C = 12, 20, 6
+    cfg = dict(dt=1e-5, bc_mode=bc_mode, ab_mode=ab_mode)
+    st = workloads.seeded_state(15, 15, nr, seed=3, amp=0.3)
+    rng = np.random.default_rng(17)
+    L, M = workloads.lm_arrays(15, 15)
+    nlm = L.size
+    bv = rng.standard_normal((2, nlm)) * 1e-3
+    src = np.linspace(0.1, 0.4, nr)
+    shell = nr // 2
+
+    def model(ut, up):
+        m = gdb.SHTnsKitConfig(15, 24, 48, nr, **cfg)
+        for k, (a, b) in st.items():
+            m.set_field(k, a, b)
+        m.set_field("u_tor", *ut)
+        m.set_field("u_pol", *up)
+        m.set_temperature_bc(bv, src)
+        return m
+
+    m = model(st["u_tor"], st["u_pol"])
+    target = np.cos(np.arange(m.nlon * m.nlat).reshape(m.nlon, m.nlat) * 0.21) * 1e-2
+    m.temperature_forward(K, C)
+    tK = m.get_field("temp")
+    resid = m.synth_scalar(*tK)[shell] - target
+    gbar = np.zeros(m.grid_shape())
+    gbar[shell] = resid
+    lre, lim = m.synth_scalar_adjoint(gbar)
+    (gtr, gti), (utr, uti), (upr, upi) = m.temperature_pullback_full(lre, lim)
+    ptr, pti = m.temperature_pullback(lre, lim)
+    assert np.allclose(gtr, ptr, rtol=0, atol=1e-14 * np.max(np.abs(ptr)))
+    assert np.allclose(gti, pti, rtol=0, atol=1e-14 * np.max(np.abs(ptr)))
+    m.close()
+
+    def Jof(ut, up):
+        mm = model(ut, up)
+        mm.step(K)
+        r = mm.synth_scalar(*mm.get_field("temp"))[shell] - target
+        mm.close()
+        return 0.5 * float(np.sum(r * r))
+
+    worst = 0.0
+    for d in range(3):
+        dv = [rng.standard_normal((nr, nlm)) * 1e-3 for _ in range(4)]
+        for x in (dv[1], dv[3]):
+            x[:, M == 0] = 0.0
+        gdot = float(np.sum(utr * dv[0]) + np.sum(uti * dv[1]) + np.sum(upr * dv[2]) + np.sum(upi * dv[3]))
+        eps = 1.0
+        plus = Jof((st["u_tor"][0] + eps * dv[0], st["u_tor"][1] + eps * dv[1]),
+                   (st["u_pol"][0] + eps * dv[2], st["u_pol"][1] + eps * dv[3]))
+        minus = Jof((st["u_tor"][0] - eps * dv[0], st["u_tor"][1] - eps * dv[1]),
+                    (st["u_pol"][0] - eps * dv[2], st["u_pol"][1] - eps * dv[3]))
+        fd = (plus - minus) / (2 * eps)
+        assert abs(fd) > 0
+        worst = max(worst, abs(fd - gdot) / abs(fd))
+    print(f"bc_mode {bc_mode} ab_mode {ab_mode}: velocity-gradient FD rel err {worst:.2e}")
+    assert worst <= 1e-5
