@@ -295,8 +295,8 @@ def run_ensemble(args, gdb, workloads, torch, world=1, rank=0):
     stream, FP64 and mixed precision.  Over several ranks (torchrun) the whole
     instances are dealt round-robin to the ranks (no collective in the step);
     time = max over ranks, value = all instances' steps / that time.
-    Members of one (lmax, nr) class share a segmented handle (up to
-    --ensemble-group per handle, each with its own Coriolis factor); the
+    Members of one lmax share a segmented handle (up to --ensemble-group per
+    handle, each with its own radial grid, operators and Coriolis factor); the
     per-member-handle ensemble is timed beside it."""
     allc = workloads.ensemble_draw(args.ensemble)
     mine = list(range(rank, len(allc), world))
@@ -358,7 +358,7 @@ def run_ensemble(args, gdb, workloads, torch, world=1, rank=0):
                        "nr": sorted({c["nr"] for c in allc}), "dt": 1e-5, "ranks": world,
                        "placement": "whole instances round-robin over the ranks",
                        "launch": "one CUDA graph per step; mixed: tensor-core grid caps by gd_ensemble_autotune",
-                       "grouping": f"members of one (lmax, nr) class share a segmented handle, <= {group} per handle"},
+                       "grouping": f"members of one lmax share a segmented handle, <= {group} per handle"},
             **res,
             "ratio_vs_fp64_gpu": res["mixed"]["instance_steps_per_s"] / res["fp64"]["instance_steps_per_s"]}
     print(json.dumps(line), flush=True)
@@ -718,7 +718,7 @@ def main():
     ap.add_argument("--adjoint", action="store_true",
                     help="instead of the headline: the adjoint configuration's gradient checks and timings")
     ap.add_argument("--ensemble-group", type=int, default=64,
-                    help="ensemble: members of one (lmax, nr) class per segmented handle, at most this many (1: a handle each)")
+                    help="ensemble: members of one lmax per segmented handle, at most this many (1: a handle each)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead of the headline: the batched uneven ensemble of this many shells")
     ap.add_argument("--decomposed", action="store_true",

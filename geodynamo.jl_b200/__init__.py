@@ -106,6 +106,7 @@ class GDConfig(ctypes.Structure):
         ("precision", ctypes.c_int), ("magnetic", ctypes.c_int),
         ("composition", ctypes.c_int), ("schmidt", ctypes.c_double),
         ("segments", ctypes.c_int), ("geometry", ctypes.c_int), ("r_outer", ctypes.c_double),
+        ("segment_nr", ctypes.POINTER(ctypes.c_int)),
     ]
 
 
@@ -274,13 +275,16 @@ class SHTnsKitConfig:
     def __init__(self, lmax, nlat, nlon, nr, mmax=None, kl=4, rratio=0.35, ekman=3e-4, rayleigh=80.0,
                  prandtl=1.0, magnetic_prandtl=4.0, dt=1e-5, implicit_theta=0.5, ab_mode=0, bc_mode=0,
                  fd_mode=0, precision="fp64", magnetic=1, device=0, composition=0, schmidt=1.0, segments=0,
-                 geometry="shell", r_outer=1.0):
+                 geometry="shell", r_outer=1.0, segment_nr=None):
         self.lib = load_library()
         mmax = lmax if mmax is None else mmax
         base, stages = PRECISION_PRESETS.get(precision, (precision, ()))
         self.cfg = GDConfig(lmax, mmax, nlat, nlon, nr, kl, rratio, ekman, rayleigh, prandtl, magnetic_prandtl,
                             dt, implicit_theta, ab_mode, bc_mode, fd_mode, PRECISIONS[base], magnetic,
                             int(composition), float(schmidt), int(segments), GEOMETRIES[geometry], float(r_outer))
+        if segment_nr is not None:
+            self._segnr = (ctypes.c_int * len(segment_nr))(*[int(v) for v in segment_nr])
+            self.cfg.segment_nr = ctypes.cast(self._segnr, ctypes.POINTER(ctypes.c_int))
         h = ctypes.c_void_p()
         st = self.lib.gd_create(ctypes.byref(self.cfg), int(device), ctypes.byref(h))
         if st != GD_OK:
@@ -833,11 +837,12 @@ class Ensemble:
     nonlinear terms as for a single model); the ensemble owns the handles.
 
     ``group`` > 1 stacks up to that many members whose configurations differ
-    only in the Ekman number (and the Rayleigh number, which the step does not
-    read: the vector analysis drops the radial buoyancy force) into one
-    segmented handle (gd_config.segments), each member with its own Coriolis
-    factor: every per-shell kernel then serves the whole group in one launch.
-    Its members are EnsembleSegment views of their levels."""
+    only in the Ekman number, the number of radial levels and the Rayleigh
+    number (which the step does not read: the vector analysis drops the radial
+    buoyancy force) into one segmented handle (gd_config.segments,
+    segment_nr), each member with its own radial grid and operators and its
+    own Coriolis factor: every per-shell kernel then serves the whole group in
+    one launch.  Its members are EnsembleSegment views of their levels."""
 
     def __init__(self, configs, precision="fp64", device=0, group=1):
         self.lib = load_library()
@@ -846,7 +851,7 @@ class Ensemble:
         if group > 1:
             open_ = {}
             for i, c in enumerate(configs):
-                key = tuple(sorted((k, repr(v)) for k, v in c.items() if k not in ("ekman", "rayleigh")))
+                key = tuple(sorted((k, repr(v)) for k, v in c.items() if k not in ("ekman", "rayleigh", "nr")))
                 lst = open_.get(key)
                 if lst is None or len(lst) >= group:
                     lst = []
@@ -857,11 +862,17 @@ class Ensemble:
             slots = [[i] for i in range(len(configs))]
         n = len(slots)
         arr = (GDConfig * n)()
+        self._segnr = []  # segment lengths, alive while the handles are created
         for i, slot in enumerate(slots):
             c = dict(configs[slot[0]])
+            segnr = None
             if len(slot) > 1:
-                c["nr"] = c["nr"] * len(slot)
+                lens = [int(configs[j]["nr"]) for j in slot]
+                c["nr"] = sum(lens)
                 c["segments"] = len(slot)
+                if len(set(lens)) > 1:
+                    segnr = (ctypes.c_int * len(lens))(*lens)
+                    self._segnr.append(segnr)
             lmax = c.pop("lmax")
             mmax = c.pop("mmax", None)
             mmax = lmax if mmax is None else mmax
@@ -872,6 +883,8 @@ class Ensemble:
                               c.pop("fd_mode", 0), PRECISIONS[c.pop("precision", precision)],
                               c.pop("magnetic", 1), c.pop("composition", 0), c.pop("schmidt", 1.0),
                               c.pop("segments", 0), GEOMETRIES[c.pop("geometry", "shell")], c.pop("r_outer", 1.0))
+            if segnr is not None:
+                arr[i].segment_nr = ctypes.cast(segnr, ctypes.POINTER(ctypes.c_int))
         e = ctypes.c_void_p()
         st = self.lib.gd_ensemble_create(arr, n, int(device), ctypes.byref(e))
         if st != GD_OK:
@@ -885,8 +898,10 @@ class Ensemble:
                 self.members[slot[0]] = hv
                 continue
             hv.set_segment_ekman([configs[i].get("ekman", 3e-4) for i in slot])
+            base = 0
             for g, i in enumerate(slot):
-                self.members[i] = EnsembleSegment(hv, g, configs[i]["nr"])
+                self.members[i] = EnsembleSegment(hv, g, configs[i]["nr"], base)
+                base += int(configs[i]["nr"])
 
     def __len__(self):
         return len(self.members)
@@ -936,17 +951,18 @@ class Ensemble:
 
 
 class EnsembleSegment:
-    """One member of a grouped ensemble: levels [seg nr, (seg + 1) nr) of a
+    """One member of a grouped ensemble: levels [base, base + nr) of a
     segmented handle.  Fields, nonlinear terms and energies of the member
     alone; the step runs for the whole handle."""
 
-    def __init__(self, handle, seg, nr):
+    def __init__(self, handle, seg, nr, base=None):
         self.handle = handle
         self.seg = int(seg)
         self.nr = int(nr)
+        base = self.seg * self.nr if base is None else int(base)
         self.lmax, self.mmax, self.nlat, self.nlon, self.nlm = (handle.lmax, handle.mmax, handle.nlat,
                                                                 handle.nlon, handle.nlm)
-        self.rows = slice(self.seg * self.nr, (self.seg + 1) * self.nr)
+        self.rows = slice(base, base + self.nr)
 
     def spec_shape(self):
         return (self.nr, self.nlm)

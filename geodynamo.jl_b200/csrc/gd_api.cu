@@ -66,8 +66,12 @@ int check_launch(gd_handle* h, const char* what) {
 int build_implicit(gd_handle* h) {
   const Dims& d = h->d;
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-  launch_build_lu(h->stream, d.nrs, d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->c.dt,
-                  h->c.implicit_theta, h->c.bc_mode == 2, h->d_lin, h->d_lu, h->d_flag, h->c.composition ? 4 : 3);
+  // one set of operators per segment length (variant), on its own radial nodes
+  for (size_t v = 0; v < h->var_n.size(); ++v)
+    launch_build_lu(h->stream, h->var_n[v], d.kl, d.L, h->d_d1 + h->var_band[v], h->d_d2 + h->var_band[v],
+                    h->d_rinv + h->var_rep[v], h->d_rinv2 + h->var_rep[v], h->d_nu, h->c.dt, h->c.implicit_theta,
+                    h->c.bc_mode == 2, h->d_lin + h->var_op[v], h->d_lu + h->var_op[v], h->d_flag,
+                    h->c.composition ? 4 : 3);
   int s = check_launch(h, "build_lu");
   if (s) return s;
   int flag = 0;
@@ -85,7 +89,8 @@ int build_implicit(gd_handle* h) {
 // single-boundary combinations and their D1 derivatives at the boundary they
 // serve.  Needs the radial nodes and D1 on the device.
 int build_tau(gd_handle* h) {
-  const int N = h->d.nrs, KL = h->d.kl, NB = 2 * GD_MAX_KL + 1;
+  // variant 0 (flux boundaries are refused with several variants)
+  const int N = h->var_n[0], KL = h->d.kl, NB = 2 * GD_MAX_KL + 1;
   std::vector<double> r(N), d1((size_t)NB * N);
   CK(cudaMemcpyAsync(r.data(), h->d_r, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(d1.data(), h->d_d1, sizeof(double) * NB * N, cudaMemcpyDeviceToHost, h->stream));
@@ -171,7 +176,31 @@ int setup(gd_handle* h) {
   d.jlo = 0;
   d.jhi = d.nlm;
   d.nseg = c.segments > 1 ? c.segments : 1;
-  d.nrs = d.nr / d.nseg;
+  // segment lengths (equal unless listed) and their operator variants
+  h->seg_n.assign(d.nseg, d.nr / d.nseg);
+  if (d.nseg > 1 && c.segment_nr)
+    for (int z = 0; z < d.nseg; ++z) h->seg_n[z] = c.segment_nr[z];
+  h->seg_base.assign(d.nseg, 0);
+  h->seg_var.assign(d.nseg, 0);
+  h->var_n.clear(); h->var_rep.clear(); h->var_band.clear(); h->var_op.clear();
+  const long nbw_h = 2 * GD_MAX_KL + 1;
+  for (int z = 0, b = 0; z < d.nseg; b += h->seg_n[z], ++z) {
+    h->seg_base[z] = b;
+    int v = 0;
+    while (v < (int)h->var_n.size() && h->var_n[v] != h->seg_n[z]) ++v;
+    if (v == (int)h->var_n.size()) {
+      const long band = h->var_n.empty() ? 0 : h->var_band.back() + nbw_h * h->var_n.back();
+      const long op = h->var_n.empty() ? 0 : h->var_op.back() + 4 * nbw_h * h->var_n.back() * (c.lmax + 1);
+      h->var_n.push_back(h->seg_n[z]);
+      h->var_rep.push_back(b);
+      h->var_band.push_back(band);
+      h->var_op.push_back(op);
+    }
+    h->seg_var[z] = v;
+  }
+  d.nrs = *std::max_element(h->seg_n.begin(), h->seg_n.end());
+  d.seg_info = nullptr;
+  d.var_off = nullptr;
   d.rfs = nullptr;
   d.rfs32 = nullptr;
   d.ball = c.geometry == GD_GEOM_BALL;
@@ -219,14 +248,36 @@ int setup(gd_handle* h) {
   std::vector<double> r(NR), ri(NR), ri2(NR);
   const double rin = c.rratio / (1.0 - c.rratio);
   const double kPi = 3.14159265358979323846;
-  // one segment's nodes, repeated for every segment.  Ball: the same cosine
+  // every segment its own nodes for its level count.  Ball: the same cosine
   // nodes on [0, R] (create_ball_radial_domain, src/Ball/Ball.jl:34-71), r_1 = 0
-  const int NS = d.nrs;
-  for (int n = 1; n <= NS; ++n) {
-    const double x = 0.5 * (1.0 + std::cos(kPi * (double)(NS - n) / (double)(NS - 1)));
-    r[n - 1] = d.ball ? (c.r_outer != 1.0 ? x * c.r_outer : x) : x + rin;
+  for (int z = 0; z < d.nseg; ++z) {
+    const int NS = h->seg_n[z], b = h->seg_base[z];
+    for (int n = 1; n <= NS; ++n) {
+      const double x = 0.5 * (1.0 + std::cos(kPi * (double)(NS - n) / (double)(NS - 1)));
+      r[b + n - 1] = d.ball ? (c.r_outer != 1.0 ? x * c.r_outer : x) : x + rin;
+    }
   }
-  for (int n = NS; n < d.nr; ++n) r[n] = r[n % NS];
+  if (h->var_n.size() > 1) {
+    // several segment lengths: the kernels look each segment's shells and operators up
+    std::vector<int> info(3 * (size_t)d.nseg);
+    std::vector<long> voff(2 * h->var_n.size());
+    for (int z = 0; z < d.nseg; ++z) {
+      info[3 * z] = h->seg_base[z];
+      info[3 * z + 1] = h->seg_n[z];
+      info[3 * z + 2] = h->seg_var[z];
+    }
+    for (size_t v = 0; v < h->var_n.size(); ++v) {
+      voff[2 * v] = h->var_band[v];
+      voff[2 * v + 1] = h->var_op[v];
+    }
+    AL(h->d_seg_info, info.size());
+    AL(h->d_var_off, voff.size());
+    CK(cudaMemcpyAsync(h->d_seg_info, info.data(), sizeof(int) * info.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->d_var_off, voff.data(), sizeof(long) * voff.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    d.seg_info = h->d_seg_info;
+    d.var_off = h->d_var_off;
+  }
   for (int n = 0; n < d.nr; ++n) { ri[n] = std::pow(r[n], -1.0); ri2[n] = std::pow(r[n], -2.0); }
   CK(cudaMemcpyAsync(h->d_r, r.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(h->d_rinv, ri.data(), sizeof(double) * NR, cudaMemcpyHostToDevice, s));
@@ -246,7 +297,9 @@ int setup(gd_handle* h) {
 
   launch_gauss(s, d.nlat, h->d_x, h->d_w, h->d_th, h->d_sth);
   launch_tables(s, d, h->d_moff, h->d_x, h->d_sth, h->d_P, h->d_dP, h->d_Q);
-  launch_fd_weights(s, d.nrs, d.kl, c.fd_mode, h->d_r, h->d_d1, h->d_d2);
+  for (size_t v = 0; v < h->var_n.size(); ++v)
+    launch_fd_weights(s, h->var_n[v], d.kl, c.fd_mode, h->d_r + h->var_rep[v], h->d_d1 + h->var_band[v],
+                      h->d_d2 + h->var_band[v]);
   int st = check_launch(h, "set-up kernels");
   if (st) return st;
   // Coriolis factors sin/cos of the colatitude grid (src/velocity.jl:278-282).
@@ -708,8 +761,18 @@ bool valid_config(const gd_config* c, std::string& why) {
   if (c->precision != GD_PREC_FP64 && c->precision != GD_PREC_MIXED) { why = "unknown precision"; return false; }
   if (c->composition != 0 && c->composition != 1) { why = "composition must be 0 or 1"; return false; }
   if (c->composition && !(c->schmidt > 0.0)) { why = "composition needs a positive Schmidt number"; return false; }
-  if (c->segments < 0 || (c->segments > 1 && c->nr % c->segments)) { why = "segments must divide nr"; return false; }
-  if (c->segments > 1 && c->nr / c->segments < 3) { why = "each segment needs at least 3 levels"; return false; }
+  if (c->segments < 0) { why = "segments must be >= 0"; return false; }
+  if (c->segments > 1 && c->segment_nr) {
+    long sum = 0;
+    for (int z = 0; z < c->segments; ++z) {
+      if (c->segment_nr[z] < 3) { why = "each segment needs at least 3 levels"; return false; }
+      sum += c->segment_nr[z];
+    }
+    if (sum != c->nr) { why = "segment_nr must sum to nr"; return false; }
+  } else {
+    if (c->segments > 1 && c->nr % c->segments) { why = "segments must divide nr"; return false; }
+    if (c->segments > 1 && c->nr / c->segments < 3) { why = "each segment needs at least 3 levels"; return false; }
+  }
   if (c->segments > 1 && c->composition) { why = "segments carry no composition"; return false; }
   if (c->geometry != GD_GEOM_SHELL && c->geometry != GD_GEOM_BALL) { why = "geometry must be GD_GEOM_SHELL or GD_GEOM_BALL"; return false; }
   if (c->geometry == GD_GEOM_BALL) {
@@ -739,6 +802,7 @@ int gd_create(const gd_config* cfg, int device, gd_handle** out) {
   h->c = *cfg;
   h->device = device;
   int s = setup(h);
+  h->c.segment_nr = nullptr;  // read by the set-up only; the lengths live in seg_n
   if (s == GD_OK && cfg->precision == GD_PREC_MIXED) s = gd_set_precision(h, GD_PREC_MIXED);
   if (s != GD_OK) {
     fprintf(stderr, "gd_create: %s\n", h->err.c_str());
@@ -1019,7 +1083,7 @@ int gd_get_launch_shape(const gd_handle* h, int* tc_ctas) {
 
 int gd_set_segment_ekman(gd_handle* h, const double* ekman) {
   if (!h || !ekman) return h ? fail(h, GD_ERR_ARG, "null pointer") : GD_ERR_ARG;
-  const int nseg = h->d.nseg, nrs = h->d.nrs;
+  const int nseg = h->d.nseg;
   for (int g = 0; g < nseg; ++g)
     if (!(ekman[g] > 0.0) || !std::isfinite(ekman[g])) return fail(h, GD_ERR_ARG, "Ekman numbers must be positive");
   CK(cudaSetDevice(h->device));
@@ -1029,7 +1093,8 @@ int gd_set_segment_ekman(gd_handle* h, const double* ekman) {
   std::vector<double> rf(h->d.nr);
   std::vector<float> rf32(h->d.nr);
   for (int k = 0; k < h->d.nr; ++k) {
-    rf[k] = h->c.magnetic_prandtl / ekman[k / nrs];
+    rf[k] = h->c.magnetic_prandtl / ekman[std::upper_bound(h->seg_base.begin(), h->seg_base.end(), k) -
+                                          h->seg_base.begin() - 1];
     rf32[k] = (float)rf[k];
   }
   if (!h->d_rfs) {
@@ -1082,6 +1147,8 @@ int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int*
   }
   if (flux && h->c.bc_mode == 2)
     return fail(h, GD_ERR_UNSUPPORTED, "flux boundaries act on the state (bc_mode 0 or 1), not inside the operator");
+  if (flux && h->var_n.size() > 1)
+    return fail(h, GD_ERR_UNSUPPORTED, "flux boundaries need segments of one length (one set of tau functions)");
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaMemcpyAsync(h->d_bctype + (field == GD_COMP ? 2 * NL : 0), t.data(), sizeof(int) * 2 * NL,
@@ -2247,6 +2314,8 @@ int gd_ensemble_autotune(gd_ensemble* e, int nsteps, float* best_ms, int* caps_o
   std::vector<gd_config> cfgs(n);
   for (int i = 0; i < n; ++i) {
     cfgs[i] = e->members[i]->c;
+    // the member's segment lengths (the caller's array was read at creation only)
+    if (e->members[i]->d.nseg > 1) cfgs[i].segment_nr = e->members[i]->seg_n.data();
     cfgs[i].precision = GD_PREC_FP64;  // set below, with the member's stages
   }
   gd_ensemble* t = nullptr;

@@ -25,14 +25,13 @@ namespace gd {
 template <int KL>
 __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const double* __restrict__ LU,
                                              const double* __restrict__ sband, const double* __restrict__ srinv2,
-                                             double nu, const Cnab2Args& a, int slot, int seg) {
-  // the segment's N levels start at shell seg N; the planes span all shells
-  const int N = d.nrs;
+                                             double nu, const Cnab2Args& a, int slot, int N, int base) {
+  // the segment's N levels start at shell base; the planes span all shells
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   const size_t Lp1 = (size_t)d.L + 1;
   constexpr int NB = 2 * KL + 1;
   const double nulf = __dmul_rn(nu, (double)l * (l + 1));
-  const size_t s0 = (size_t)seg * N * NM + j;
+  const size_t s0 = (size_t)base * NM + j;
   double* __restrict__ ure = a.u[slot] + s0;
   double* __restrict__ uim = a.u[slot] + plane + s0;
   const double* __restrict__ nre = a.nl[slot] + s0;
@@ -208,8 +207,14 @@ __global__ void __launch_bounds__(128, 3) k_cnab2(Dims d, const int* __restrict_
   if (slot >= a.nfield) return;
   const int g = a.kind[slot];
   const double nuk = nu[g];
-  // every segment has the same radial nodes: one band, one set of factors
-  const int N = d.nrs;
+  // the segment's radial operators (its variant's band, its shells' 1/r)
+  const SegView sv = seg_view(d, blockIdx.z);
+  const int N = sv.n;
+  d1 += sv.band_off;
+  d2 += sv.band_off;
+  rinv += sv.base;
+  rinv2 += sv.base;
+  lu += sv.op_off;
   for (int e = threadIdx.x; e < N * NB; e += blockDim.x) {
     const int col = e / NB, b = e % NB, i = col + b - KL;
     double v = 0.0;
@@ -226,7 +231,7 @@ __global__ void __launch_bounds__(128, 3) k_cnab2(Dims d, const int* __restrict_
   if (j >= d.jhi) return;
   const int l = lof[j];
   const double* LUk = lu + (size_t)g * N * NB * ((size_t)d.L + 1);
-  cnab2_column<KL>(d, j, l, LUk, sband, srinv2, nuk, a, slot, blockIdx.z);
+  cnab2_column<KL>(d, j, l, LUk, sband, srinv2, nuk, a, slot, N, sv.base);
 }
 
 void launch_cnab2(cudaStream_t s, const Dims& d, const int* lof, const double* d1, const double* d2,
@@ -244,7 +249,8 @@ __global__ void k_energy_partial(Dims d, const int* __restrict__ lof, const doub
                                  const double* __restrict__ bp, double* __restrict__ partial) {
   __shared__ double sk[256], sm[256];
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
-  const size_t seg0 = (size_t)blockIdx.y * d.nrs * NM, segn = (size_t)d.nrs * NM;
+  const SegView sv = seg_view(d, blockIdx.y);
+  const size_t seg0 = (size_t)sv.base * NM, segn = (size_t)sv.n * NM;
   ut += seg0;
   up += seg0;
   if (bt) {

@@ -56,6 +56,12 @@ struct gd_handle {
   // per-shell Coriolis / Lorentz factors of a segmented handle (gd_set_segment_ekman)
   double* d_rfs = nullptr;
   float* d_rfs32 = nullptr;
+  // segments: first shell, levels, operator variant; variants: levels, first
+  // shell of a segment of that length, offsets of its bands and operators
+  std::vector<int> seg_base, seg_n, seg_var, var_n, var_rep;
+  std::vector<long> var_band, var_op;
+  int* d_seg_info = nullptr;
+  long* d_var_off = nullptr;
   // checkpointed forward run of gd_temperature_forward
   std::vector<void*> t_snaps;
   void* t_final = nullptr;

@@ -47,7 +47,24 @@ struct Dims {
   const float* rfs32;
   // ball geometry: the first level of each segment is r = 0
   int ball;
+  // segments of unequal length (null: nseg segments of nrs levels, one set of
+  // radial operators): seg_info [nseg][3] = first shell, levels, operator
+  // variant; var_off [variant][2] = offset (doubles) of the variant's D1 / D2
+  // bands and of its implicit operators; nrs is then the longest segment
+  const int* seg_info;
+  const long* var_off;
 };
+
+// The shells and radial operators of segment z.
+struct SegView {
+  int base, n;
+  long band_off, op_off;
+};
+__device__ __forceinline__ SegView seg_view(const Dims& d, int z) {
+  if (d.seg_info == nullptr) return SegView{z * d.nrs, d.nrs, 0, 0};
+  const int v = d.seg_info[3 * z + 2];
+  return SegView{d.seg_info[3 * z], d.seg_info[3 * z + 1], d.var_off[2 * v], d.var_off[2 * v + 1]};
+}
 
 // Analysis epilogue variants.
 enum { EPI_SCALAR = 0, EPI_VECTOR = 1, EPI_CURL_INDUCTION = 2 };

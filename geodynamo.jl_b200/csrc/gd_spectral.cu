@@ -89,7 +89,10 @@ __global__ void k_gradients(Dims d, const int* __restrict__ lof, const int* __re
   const int l = lof[j], m = mof[j];
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   // segment blockIdx.z: levels base .. base + N - 1 (the whole column when nseg = 1)
-  const int N = d.nrs, base = blockIdx.z * N;
+  const SegView sv = seg_view(d, blockIdx.z);
+  const int N = sv.n, base = sv.base;
+  if (k0 >= N) return;
+  d1 += sv.band_off;
   T += (size_t)base * NM;
   rinv += base;
   if (!IMG) {
@@ -202,7 +205,11 @@ __global__ void __launch_bounds__(RAD_THREADS, 4) k_curl(Dims d, const int* __re
   const int k0 = blockIdx.y * rows;
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
   // segment blockIdx.z: levels base .. base + N - 1 (the whole column when nseg = 1)
-  const int N = d.nrs, base = blockIdx.z * N;
+  const SegView sv = seg_view(d, blockIdx.z);
+  const int N = sv.n, base = sv.base;
+  if (k0 >= N) return;  // the whole block: a shorter segment
+  d1 += sv.band_off;
+  d2 += sv.band_off;
   tor += (size_t)base * NM;
   pol += (size_t)base * NM;
   rinv += base;
@@ -307,10 +314,13 @@ __global__ void k_scalar_bc(Dims d, const int* __restrict__ lof, const double* _
                             double* __restrict__ F) {
   const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.jhi) return;
-  // segment blockIdx.y: its own boundary rows and radial profile
-  const int N = d.nrs, KL = d.kl, NB = 2 * GD_MAX_KL + 1;
+  // segment blockIdx.y: its own boundary rows and radial profile (flux rows
+  // only with one operator variant: the tau functions are of variant 0)
+  const SegView sv = seg_view(d, blockIdx.y);
+  const int N = sv.n, KL = d.kl, NB = 2 * GD_MAX_KL + 1;
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
-  F += (size_t)blockIdx.y * N * NM;
+  F += (size_t)sv.base * NM;
+  d1 += sv.band_off;
   double* re = F + j;
   double* im = F + plane + j;
   // ball: no inner boundary at r = 0 (src/thermal.jl:281-282); regularity
@@ -367,7 +377,7 @@ __global__ void k_regularity(Dims d, const int* __restrict__ lof, double* __rest
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.nlm || lof[j] < 1) return;
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
-  double* f = F + blockIdx.z * fstride + (size_t)blockIdx.y * d.nrs * NM + j;
+  double* f = F + blockIdx.z * fstride + (size_t)seg_view(d, blockIdx.y).base * NM + j;
   f[0] = 0.0;
   f[plane] = 0.0;
 }

@@ -26,6 +26,7 @@ struct GDConfig
     ab_mode::Cint; bc_mode::Cint; fd_mode::Cint; precision::Cint; magnetic::Cint
     composition::Cint; schmidt::Cdouble
     segments::Cint; geometry::Cint; r_outer::Cdouble
+    segment_nr::Ptr{Cint}
 end
 
 mutable struct Handle
@@ -59,7 +60,7 @@ function handle_for(GD, config, nr::Integer; precision::Integer = 0, composition
         cfg = GDConfig(config.lmax, config.mmax, config.nlat, config.nlon, nr, GD.i_KL,
                        GD.d_rratio, GD.d_E, GD.d_Ra, GD.d_Pr, GD.d_Pm, GD.d_timestep, GD.d_implicit,
                        0, ball ? 2 : 0, 0, precision, GD.i_B, composition ? 1 : 0, composition ? GD.d_Sc : 1.0, 0,
-                       ball ? 1 : 0, ball ? GD.d_R_outer : 1.0)
+                       ball ? 1 : 0, ball ? GD.d_R_outer : 1.0, C_NULL)
         create(cfg)
     end
 end

@@ -114,7 +114,9 @@ enum { GD_GEOM_SHELL = 0, GD_GEOM_BALL = 1 };
  * groups its members this way.  CNAB2, no composition; the mode-range,
  * reverse-mode and standalone-operator entry points refuse such a handle
  * (GD_ERR_UNSUPPORTED).  Boundary values and types apply to every segment;
- * heat sources are given per shell.  0 or 1: one shell.
+ * heat sources are given per shell.  0 or 1: one shell.  segment_nr (read at
+ * creation only) gives segments of unequal length, each with the radial grid
+ * and operators of its own level count; flux boundaries then are refused.
  * geometry GD_GEOM_BALL is the solid sphere of GeoDynamoBall
  * (src/Ball/Ball.jl): cosine nodes on [0, r_outer] (r_outer = d_R_outer,
  * rratio unused), the angular gradient and both curl components 0 at r = 0
@@ -146,6 +148,7 @@ typedef struct gd_config {
   int segments;
   int geometry;
   double r_outer;
+  const int* segment_nr;  /* segments > 1: the levels of each segment (summing to nr; null: equal) */
 } gd_config;
 
 typedef struct gd_handle gd_handle;

@@ -1,6 +1,8 @@
 """GPU tests of grouped ensembles: members whose configurations differ only in
-the Ekman and Rayleigh numbers share one segmented handle (gd_config.segments),
-their shells stacked along r, each segment with its own Coriolis factor.
+the Ekman and Rayleigh numbers and the number of radial levels share one
+segmented handle (gd_config.segments, segment_nr), their shells stacked along
+r, each segment with its own radial grid and operators (one set per length)
+and its own Coriolis factor.
 
 A grouped member runs the same arithmetic on the same inputs as the member
 stepped on its own handle (every per-shell kernel treats the shells alike, the
@@ -47,8 +49,9 @@ def test_grouped_members_equal_single_handles(gdb, precision):
     order = [picks[0], picks[3], picks[1], picks[4], picks[2]]
     assert len({c["ekman"] for _, c in order}) == len(order)
     ens = gdb.Ensemble([dict(c, precision=precision) for _, c in order], group=8)
-    assert len(ens.handles) == 2
-    assert sorted(h.segments() for h in ens.handles) == [2, 3]
+    # the two classes share lmax 31: one handle, segments of 33 and 49 levels
+    assert {c["nr"] for _, c in order} == {33, 49}
+    assert len(ens.handles) == 1 and ens.handles[0].segments() == 5
     singles = []
     for (i, c), m in zip(order, ens.members):
         load(m, c["lmax"], c["nr"], i)
