@@ -174,3 +174,42 @@ def test_segments_keep_their_own_boundary_rows(gdb, bc_mode):
             assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), (bc_mode, k)
         assert m.energy() == s.energy()
     ens.close()
+
+
+@pytest.mark.parametrize("bc_mode,precision", [(0, "fp64"), (1, "fp64"), (2, "fp64"), (2, "mixed")])
+def test_unequal_segments_equal_single_handles(gdb, bc_mode, precision):
+    # members of 9, 13 and 9 levels on one handle (two operator variants):
+    # boundary values, per-shell sources, clamped rows (bc_mode 1) and
+    # Dirichlet rows (bc_mode 2) at each segment's own ends; flux boundaries
+    # need one segment length and are refused
+    lmax, nlat, nlon = 15, 24, 48
+    nrs = (9, 13, 9)
+    members = [dict(lmax=lmax, nlat=nlat, nlon=nlon, nr=n, ekman=e, bc_mode=bc_mode, dt=2e-6, precision=precision)
+               for n, e in zip(nrs, (3e-4, 5e-4, 8e-4))]
+    ens = gdb.Ensemble(members, group=3)
+    assert len(ens.handles) == 1 and ens.handles[0].segments() == 3
+    h = ens.handles[0]
+    rng = np.random.default_rng(12)
+    bv = rng.standard_normal((2, h.nlm)) * 1e-2
+    srcs = [rng.standard_normal(n) for n in nrs]
+    h.set_temperature_bc(bv, np.concatenate(srcs))
+    with pytest.raises(gdb.GeoDynamoError):
+        h.set_bc_types("temp", np.full(h.nlm, 2), np.full(h.nlm, 1))
+    singles = []
+    for i, (c, m) in enumerate(zip(members, ens.members)):
+        kw = {k: v for k, v in c.items() if k not in ("lmax", "nlat", "nlon", "nr")}
+        s = gdb.SHTnsKitConfig(lmax, nlat, nlon, c["nr"], **kw)
+        s.set_temperature_bc(bv, srcs[i])
+        for k, (a, b) in workloads.seeded_state(lmax, lmax, c["nr"], seed=30 + i, amp=1e-1).items():
+            m.set_field(k, a, b)
+            s.set_field(k, a, b)
+        singles.append(s)
+    ens.step(3)
+    for s in singles:
+        s.step(3)
+    for m, s in zip(ens.members, singles):
+        for k in NAMES:
+            a, b = m.get_field(k), s.get_field(k)
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), (bc_mode, k)
+        assert m.energy() == s.energy()
+    ens.close()
