@@ -78,6 +78,25 @@ int build_implicit(gd_handle* h) {
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   if (flag) return fail(h, GD_ERR_SINGULAR, "zero pivot in a banded LU factorisation");
+  // bc_mode 2 with one segment length: the factors for prescribed fluxes (the
+  // linear operator is the same; a scratch block takes the build's copy).  A
+  // zero pivot there only disables flux rows (gd_set_scalar_bc_types refuses them)
+  if (h->d_lu_flux) {
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    for (int fv = 1; fv <= 3; ++fv)
+      launch_build_lu(h->stream, h->var_n[0], d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->c.dt,
+                      h->c.implicit_theta, 1 | (fv << 1), h->d_lu_flux + 3 * h->lu_flux_stride,
+                      h->d_lu_flux + (size_t)(fv - 1) * h->lu_flux_stride, h->d_flag, h->c.composition ? 4 : 3);
+    s = check_launch(h, "build_lu (flux rows)");
+    if (s) return s;
+    CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->flux_rows_ok = flag == 0;
+    bool any_flux = false;
+    for (int t : h->bctype) any_flux |= t == GD_BC_FLUX;
+    if (!h->flux_rows_ok && any_flux)
+      return fail(h, GD_ERR_SINGULAR, "zero pivot in the factorisation with flux boundary rows");
+  }
   return GD_OK;
 }
 
@@ -148,7 +167,7 @@ void gd::scalar_bc(gd_handle* h, int field) {
   const size_t NL = h->d.nlm;
   ProfScope p(h, comp ? "composition_bc" : "temperature_bc");
   launch_scalar_bc(h->stream, h->d, h->d_lof, comp ? h->d_cbvals : h->d_bvals, h->d_bctype + (comp ? 2 * NL : 0),
-                   h->d_d1, h->tau, h->field(field));
+                   h->d_d1, h->tau, h->field(field), h->c.bc_mode == 2);
 }
 
 // ball_physical_to_spectral! / ball_vector_analysis! (src/Ball/Ball.jl:214-245)
@@ -228,6 +247,12 @@ int setup(gd_handle* h) {
   AL(h->d_P, NL * NT); AL(h->d_dP, NL * NT); AL(h->d_Q, NL * NT);
   AL(h->d_d1, nbw * NR); AL(h->d_d2, nbw * NR);
   AL(h->d_lin, 4 * NR * nbw * (d.L + 1)); AL(h->d_lu, 4 * NR * nbw * (d.L + 1));
+  if (c.bc_mode == 2 && h->var_n.size() == 1) {
+    // three flux-row variants of the factors, and a block that takes the
+    // build's copy of the linear operator
+    h->lu_flux_stride = (size_t)4 * h->var_n[0] * nbw * (d.L + 1);
+    AL(h->d_lu_flux, 4 * h->lu_flux_stride);
+  }
   AL(h->d_tw, 2 * (size_t)d.nlon); AL(h->d_twf, 2 * (size_t)d.nlon);
   AL(h->d_state, NFIELD * h->spec_elems()); AL(h->d_nl, NFIELD * h->spec_elems());
   AL(h->d_prev, NFIELD * h->spec_elems());
@@ -606,9 +631,15 @@ int implicit_launch(gd_handle* h, int boot) {
   a.clamp_rows = h->c.bc_mode == 1;
   a.bc_rows = h->c.bc_mode == 2;
   // Dirichlet rows of bc_mode 2: the temperature's and the composition's
-  // boundary values, zero for the velocity and magnetic potentials
-  for (int i = 0; i < a.nfield; ++i)
+  // boundary values (or fluxes, by their boundary types), zero for the
+  // velocity and magnetic potentials
+  const size_t NLm = h->d.nlm;
+  for (int i = 0; i < a.nfield; ++i) {
     a.rowvals[i] = order[i] == F_TEMP ? h->d_bvals : order[i] == F_COMP ? h->d_cbvals : nullptr;
+    a.rowtypes[i] = order[i] == F_TEMP ? h->d_bctype : order[i] == F_COMP ? h->d_bctype + 2 * NLm : nullptr;
+  }
+  a.lu_flux = h->d_lu_flux;
+  a.lu_flux_stride = h->lu_flux_stride;
   a.inv_dt = 1.0 / h->c.dt;
   a.lin_weight = 1.0 - h->c.implicit_theta;
   a.dt = h->c.dt;
@@ -1145,10 +1176,14 @@ int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int*
     t[h->perm[q]] = a;  // l-major q -> native
     t[NL + h->perm[q]] = b;
   }
-  if (flux && h->c.bc_mode == 2)
-    return fail(h, GD_ERR_UNSUPPORTED, "flux boundaries act on the state (bc_mode 0 or 1), not inside the operator");
+  bool inner_flux = false;
+  for (size_t q = 0; q < NL; ++q) inner_flux |= inner[q] == GD_BC_FLUX;
+  if (inner_flux && h->d.ball)
+    return fail(h, GD_ERR_UNSUPPORTED, "a ball has no inner boundary: its centre row is the regularity condition");
   if (flux && h->var_n.size() > 1)
     return fail(h, GD_ERR_UNSUPPORTED, "flux boundaries need segments of one length (one set of tau functions)");
+  if (flux && h->c.bc_mode == 2 && !h->flux_rows_ok)
+    return fail(h, GD_ERR_SINGULAR, "the implicit factorisation with flux boundary rows has a zero pivot");
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaMemcpyAsync(h->d_bctype + (field == GD_COMP ? 2 * NL : 0), t.data(), sizeof(int) * 2 * NL,

@@ -62,6 +62,11 @@ struct gd_handle {
   std::vector<long> var_band, var_op;
   int* d_seg_info = nullptr;
   long* d_var_off = nullptr;
+  // bc_mode 2: the implicit factors with D1 rows for prescribed fluxes at the
+  // inner (1), outer (2) or both (3) boundaries, each block laid out as d_lu
+  double* d_lu_flux = nullptr;
+  size_t lu_flux_stride = 0;
+  bool flux_rows_ok = false;
   // checkpointed forward run of gd_temperature_forward
   std::vector<void*> t_snaps;
   void* t_final = nullptr;

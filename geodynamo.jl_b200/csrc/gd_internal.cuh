@@ -163,7 +163,7 @@ struct TauConsts {
 // rows, then the tau correction of the modes with a flux boundary.
 // types: [inner, outer][nlm] GD_BC_* (native order); bvals [2][nlm] values or fluxes.
 void launch_scalar_bc(cudaStream_t s, const Dims& d, const int* lof, const double* bvals_native, const int* types,
-                      const double* d1, const TauConsts& tc, double* F);
+                      const double* d1, const TauConsts& tc, double* F, int op_rows);
 // ball: r = 0 level of nf fields (stride fstride doubles) set to 0 for l >= 1
 void launch_regularity(cudaStream_t s, const Dims& d, const int* lof, double* F, int nf, size_t fstride);
 void launch_lmajor_to_native(cudaStream_t s, const Dims& d, const int* native_of_lmajor, const double* src,
@@ -186,6 +186,12 @@ struct Cnab2Args {
   int clamp_rows;
   int bc_rows;                // Dirichlet rows in the operator: boundary rhs = the slot's value or 0
   const double* rowvals[6];   // per slot: boundary values [2][nlm] (native order) of its rows (null: 0)
+  // per slot, may be null: boundary types [2][nlm] (native order); a GD_BC_FLUX
+  // row takes the factors with the row of D1 there, lu_flux + (v - 1) lu_flux_stride
+  // with v = inner flux | 2 outer flux (the layout of lu)
+  const int* rowtypes[6];
+  const double* lu_flux;
+  size_t lu_flux_stride;
   double inv_dt, lin_weight;
   double dt;                  // EAB2: the time step applied to the phi1 term
   int stages;                 // sweeps to run: 1 rhs, 2 forward, 4 back substitution (0: all)

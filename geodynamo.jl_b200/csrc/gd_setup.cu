@@ -220,6 +220,9 @@ void launch_fd_weights(cudaStream_t s, int nr, int kl, int fd_mode, const double
 //   L_l = nu (D2 + (2/r) D1) - nu l(l+1)/r^2,   S_l = I/dt - theta L_l,
 // then factorize_banded (src/linear_algebra.jl:23-57, no pivoting).
 // One thread per (kind, l).  Bands in [kind][col][band][l] order.
+// bc_rows (the boundary-row operator, bc_mode 2): bit 0 replaces rows 0 and
+// N - 1 by boundary rows, identity rows (fixed values) unless bit 1 (inner)
+// or bit 2 (outer) asks for the row of D1 there (a prescribed radial flux).
 __global__ void k_build_lu(int N, int kl, int L, const double* d1, const double* d2, const double* rinv,
                            const double* rinv2, const double* nu, double inv_dt, double mth, int bc_rows,
                            double* lin, double* lu, int* status) {
@@ -236,16 +239,20 @@ __global__ void k_build_lu(int N, int kl, int L, const double* d1, const double*
   for (int j = 0; j < N; ++j) {
     for (int b = 0; b < nbw; ++b) {
       const int i = j + b - kl;
-      double lv = 0.0;
+      double lv = 0.0, d1v = 0.0;
       if (i >= 0 && i < N) {
         const size_t q = b + (size_t)nbw * j;
+        d1v = d1[q];
         const double lapv = __dadd_rn(d2[q], __dmul_rn(__dmul_rn(2.0, rinv[i]), d1[q]));
         lv = __dmul_rn(nk, lapv);
         if (i == j) lv = __dsub_rn(lv, __dmul_rn(__dmul_rn(nk, lf), rinv2[i]));
       }
       double sv = __dmul_rn(lv, mth);
       if (i == j) sv = __dadd_rn(sv, inv_dt);
-      if (bc_rows && (i == 0 || i == N - 1)) sv = (i == j) ? 1.0 : 0.0;  // Dirichlet rows (bc_mode 2)
+      if (bc_rows && (i == 0 || i == N - 1)) {  // boundary rows (bc_mode 2)
+        const bool flux = (i == 0) ? (bc_rows & 2) != 0 : (bc_rows & 4) != 0;
+        sv = flux ? d1v : ((i == j) ? 1.0 : 0.0);
+      }
       lin[(((size_t)kind * N + j) * nbw + b) * Lp1 + l] = lv;
       lu[(((size_t)kind * N + j) * nbw + b) * Lp1 + l] = sv;
     }

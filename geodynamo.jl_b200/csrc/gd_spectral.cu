@@ -311,7 +311,7 @@ void launch_curl_img(cudaStream_t s, const Dims& d, const int* lof, const int* m
 // added to Re and, when any |Im| exceeds 1e-12, to Im.
 __global__ void k_scalar_bc(Dims d, const int* __restrict__ lof, const double* __restrict__ bv,
                             const int* __restrict__ types, const double* __restrict__ d1, TauConsts tc,
-                            double* __restrict__ F) {
+                            double* __restrict__ F, int op_rows) {
   const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.jhi) return;
   // segment blockIdx.y: its own boundary rows and radial profile (flux rows
@@ -329,7 +329,9 @@ __global__ void k_scalar_bc(Dims d, const int* __restrict__ lof, const double* _
   const bool regular = d.ball && lof[j] > 0;
   if (ti == GD_BC_VALUE) { re[0] = bv[j]; im[0] = 0.0; }
   if (to == GD_BC_VALUE) { re[(size_t)(N - 1) * NM] = bv[NM + j]; im[(size_t)(N - 1) * NM] = 0.0; }
-  const bool fi = ti == GD_BC_FLUX, fo = to == GD_BC_FLUX;
+  // with the boundary-row operator (op_rows) a flux is a row of the implicit
+  // solve, not a correction of the state
+  const bool fi = !op_rows && ti == GD_BC_FLUX, fo = !op_rows && to == GD_BC_FLUX;
   if (!fi && !fo) {
     if (regular) re[0] = im[0] = 0.0;
     return;
@@ -388,8 +390,9 @@ void launch_regularity(cudaStream_t s, const Dims& d, const int* lof, double* F,
 }
 
 void launch_scalar_bc(cudaStream_t s, const Dims& d, const int* lof, const double* bvals_native, const int* types,
-                      const double* d1, const TauConsts& tc, double* F) {
-  k_scalar_bc<<<dim3(ceil_div(d.jhi - d.jlo, 128), d.nseg), 128, 0, s>>>(d, lof, bvals_native, types, d1, tc, F);
+                      const double* d1, const TauConsts& tc, double* F, int op_rows) {
+  k_scalar_bc<<<dim3(ceil_div(d.jhi - d.jlo, 128), d.nseg), 128, 0, s>>>(d, lof, bvals_native, types, d1, tc, F,
+                                                                        op_rows);
 }
 
 __global__ void k_perm(int nlm, size_t rows, const int* __restrict__ perm, const double* __restrict__ src,

@@ -106,7 +106,7 @@ enum { GD_GEOM_SHELL = 0, GD_GEOM_BALL = 1 };
  * buoyancy is a radial force, which the vector analysis does not keep, so C
  * does not act on the velocity.  Every time scheme (the exponential ones
  * with composition as a fourth operator kind); under bc_mode 2 its boundary
- * types are fixed values, the right-hand sides of its Dirichlet rows.
+ * types default to fixed values, the right-hand sides of its Dirichlet rows.
  * segments > 1 stacks that many independent shells of nr / segments levels
  * each (same grid, diffusivities, dt and modes; their own Ekman numbers through
  * gd_set_segment_ekman) along r: every per-shell kernel serves them all in one
@@ -127,7 +127,8 @@ enum { GD_GEOM_SHELL = 0, GD_GEOM_BALL = 1 };
  * The reference's implicit operator holds 1/r and 1/r^2 at r = 0 (infinite;
  * 0 x inf at l = 0), so a ball needs bc_mode 2, whose r = 0 row is the
  * regularity condition for l >= 1 and the inner boundary value for the l = 0
- * temperature and composition (centre values); CNAB2, no flux boundaries.
+ * temperature and composition (centre values); CNAB2; an outer flux row is
+ * allowed, an inner flux refused (the centre row is the regularity condition).
  * Entry points whose
  * operators divide by r (reverse mode, exponential schemes, the standalone
  * timestepping operator, the distributed step) refuse a ball.
@@ -200,8 +201,12 @@ int gd_set_composition_bc(gd_handle* h, const double* bvals, const double* sourc
  * the field's nonlinear term: Chebyshev T_{N-1} and T_N (or the one-sided
  * combinations when one boundary has a flux) are added to the radial profile
  * with the coefficients that cancel the real profile's flux error, the same
- * correction going to the imaginary profile when it is not ~0.  Flux types
- * need bc_mode 0 or 1. */
+ * correction going to the imaginary profile when it is not ~0.  Under
+ * bc_mode 2 (boundary rows in the implicit operator) a flux mode's boundary
+ * row is the row of D1 instead of the identity, its right-hand side the
+ * prescribed flux; the tau correction is then not applied.  GD_ERR_UNSUPPORTED:
+ * a flux type on segments of unequal length, or at a ball's centre;
+ * GD_ERR_SINGULAR: a zero pivot in the bc_mode 2 factors with flux rows. */
 int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int* outer);
 
 /* ---- transforms on host arrays (reference layout) ---------------------------

@@ -193,6 +193,9 @@ struct Oracle {
   std::vector<double> P, dP;      // [moff[m] + (l-m)] * nth + ith  (north half)
   std::vector<double> d1, d2, lap;  // band (2kl+1) x nr, Julia column-major
   std::vector<double> lin[4], lu[4];  // per diffusivity kind: [l][band]
+  // bc_mode 2: the factors whose inner (1), outer (2) or both (3) boundary
+  // rows are rows of D1 (prescribed fluxes)
+  std::vector<double> luf[3][4];
   double nu[4] = {0, 0, 0, 0};
   FFT fft;
   // state, reference layout: [r][lm] (lm fastest)
@@ -412,6 +415,17 @@ struct Oracle {
         for (size_t q = 0; q < bsz; ++q) A[q] = L[q] * mth;
         for (int n = 0; n < N; ++n) A[bw + (size_t)nbw * n] = A[bw + (size_t)nbw * n] + inv_dt;
         if (c.bc_mode == 2) {
+          for (int fv = 1; fv <= 3; ++fv) {
+            luf[fv - 1][k].resize(bsz * (c.lmax + 1));
+            double* F = &luf[fv - 1][k][bsz * l];
+            for (size_t q = 0; q < bsz; ++q) F[q] = A[q];
+            for (int i : {0, N - 1}) {
+              const bool flux = (i == 0) ? (fv & 1) : (fv & 2);
+              for (int j = std::max(0, i - bw); j <= std::min(N - 1, i + bw); ++j)
+                F[(bw + i - j) + (size_t)nbw * j] = flux ? d1[(bw + i - j) + (size_t)nbw * j] : (i == j ? 1.0 : 0.0);
+            }
+            factorize(F);
+          }
           for (int i : {0, N - 1})
             for (int j = std::max(0, i - bw); j <= std::min(N - 1, i + bw); ++j)
               A[(bw + i - j) + (size_t)nbw * j] = (i == j) ? 1.0 : 0.0;
@@ -813,6 +827,8 @@ struct Oracle {
       }
     }
     for (int q = 0; q < nlm; ++q) {
+      // with the boundary-row operator (bc_mode 2) a flux is a row of the solve
+      if (c.bc_mode == 2) break;
       const bool ai = !ball() && types[q] == BC_FLUX, ao = types[(size_t)nlm + q] == BC_FLUX;
       if (!ai && !ao) continue;
       std::vector<double> pr(N), pi(N), dp(N);
@@ -992,8 +1008,14 @@ struct Oracle {
           xi[0] = 0.0;
           xi[N - 1] = 0.0;
         }
-        solve(&lu[kind][bsz * l], xr.data());
-        solve(&lu[kind][bsz * l], xi.data());
+        const double* F = &lu[kind][bsz * l];
+        if (c.bc_mode == 2 && (f == F_TEMP || f == F_COMP)) {
+          const std::vector<int>& ty = f == F_TEMP ? tbc : cbc;
+          const int fv = (ty[q] == BC_FLUX ? 1 : 0) | (ty[(size_t)nlm + q] == BC_FLUX ? 2 : 0);
+          if (fv) F = &luf[fv - 1][kind][bsz * l];
+        }
+        solve(F, xr.data());
+        solve(F, xi.data());
         for (int k = 0; k < N; ++k) { fre[f][(size_t)k * nlm + q] = xr[k]; fim[f][(size_t)k * nlm + q] = xi[k]; }
       }
     }

@@ -212,3 +212,21 @@ def test_ball_with_composition_matches_oracle(gdb, oracle_mod, precision, tol):
     for x in g.get_nl("comp"):
         assert np.all(x[0, lpos] == 0.0)
     assert g.get_field("comp")[0][0, 0] == -0.3
+
+
+def test_ball_with_outer_flux_matches_oracle(gdb, oracle_mod):
+    # a full sphere with a prescribed heat flux at its surface: the outer row of
+    # the implicit solve is the row of D1; the centre keeps its regularity row
+    lmax, nlat, nlon, nr = 15, 24, 48, 12
+    g, o = pair(gdb, oracle_mod, lmax, nlat, nlon, nr, dt=2e-6)
+    inner = np.ones(g.nlm, dtype=int)
+    outer = np.full(g.nlm, 2)
+    for m in (g, o):
+        m.set_bc_types("temp", inner, outer)
+    g.step(3)
+    o.step(3)
+    lpos = l_of(lmax) > 0
+    for k in NAMES:
+        for x, y in zip(g.get_field(k), o.get_field(k)):
+            assert rel(x, y) < 1e-12, k
+            assert np.all(x[0, lpos] == 0.0), k

@@ -115,8 +115,51 @@ def test_composition_with_boundary_rows_matches_oracle(gdb, oracle_mod):
             assert rel(x, y) < 1e-12, k
     cre, _ = g.get_field("comp")
     assert np.array_equal(cre[0], cbv[0]) and np.array_equal(cre[-1], cbv[1])
-    with pytest.raises(gdb.GeoDynamoError):
-        g.set_bc_types("comp", np.full(g.nlm, 2), np.full(g.nlm, 1))
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 5e-6)])
+def test_flux_rows_of_the_boundary_row_operator(gdb, oracle_mod, precision, tol):
+    # bc_mode 2 with prescribed fluxes: the boundary row of the implicit solve is
+    # the row of D1 (rhs: the flux) instead of the identity; every (inner, outer)
+    # pair of types on temperature and composition, against the oracle, and the
+    # rows hold after the steps
+    lmax, nlat, nlon, nr = 15, 24, 48, 12
+    kw = dict(composition=1, schmidt=2.5, bc_mode=2, dt=2e-6)
+    g = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, precision=precision, **kw)
+    o = oracle_mod.Oracle(lmax=lmax, nlat=nlat, nlon=nlon, nr=nr, **kw)
+    rng = np.random.default_rng(9)
+    st = workloads.seeded_state(lmax, lmax, nr, seed=6, amp=1e-1)
+    cst = workloads.seeded_state(lmax, lmax, nr, seed=106, amp=1e-1)["temp"]
+    pairs = np.array([[1, 1], [1, 2], [2, 1], [2, 2]])
+    tt = pairs[rng.integers(0, 4, g.nlm)].T.copy()
+    ct = pairs[rng.integers(0, 4, g.nlm)].T.copy()
+    tbv = rng.standard_normal((2, g.nlm)) * 1e-2
+    cbv = rng.standard_normal((2, g.nlm)) * 1e-2
+    for m in (g, o):
+        for k, (a, b) in st.items():
+            m.set_field(k, a, b)
+        m.set_field("comp", *cst)
+        m.set_bc_types("temp", tt[0], tt[1])
+        m.set_bc_types("comp", ct[0], ct[1])
+        m.set_temperature_bc(tbv, np.linspace(0.2, 1.0, nr))
+        m.set_composition_bc(cbv, np.linspace(-0.3, 0.3, nr))
+    g.step(3)
+    o.step(3)
+    for k in NAMES:
+        for x, y in zip(g.get_field(k), o.get_field(k)):
+            assert rel(x, y) < tol, k
+    D = o.fd_matrix(1)
+    kl = o.kl
+    dense = np.zeros((nr, nr))
+    for i in range(nr):
+        for j in range(max(0, i - kl), min(nr, i + kl + 1)):
+            dense[i, j] = D[kl + i - j, j]
+    for name, types, bv in (("temp", tt, tbv), ("comp", ct, cbv)):
+        re, _ = g.get_field(name)
+        dp = dense @ re
+        for side, row in ((0, 0), (1, -1)):
+            got = np.where(types[side] == 2, dp[row], re[row])
+            assert np.max(np.abs(got - bv[side])) <= 1e-9, (name, side)
 
 
 def test_composition_refusals(gdb):
@@ -131,9 +174,10 @@ def test_composition_refusals(gdb):
         h.get_field("comp")
     with pytest.raises(gdb.GeoDynamoError):
         h.get_grid("c")
-    k = gdb.SHTnsKitConfig(7, 12, 24, 9, bc_mode=2)
-    with pytest.raises(gdb.GeoDynamoError):
+    k = gdb.SHTnsKitConfig(7, 12, 24, 9, bc_mode=2, geometry="ball")
+    with pytest.raises(gdb.GeoDynamoError):  # a ball has no inner boundary
         k.set_bc_types("temp", np.full(k.nlm, 2), np.full(k.nlm, 1))
+    k.set_bc_types("temp", np.full(k.nlm, 1), np.full(k.nlm, 2))  # an outer flux is fine
 
 
 def test_decomposed_step_with_composition_matches_one_handle():

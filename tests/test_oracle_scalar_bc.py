@@ -143,3 +143,34 @@ def test_composition_defaults_to_no_flux_and_steps():
         assert np.max(np.abs(x - y)) <= 1e-13 * np.max(np.abs(y))
     o.step(3)
     assert np.all(np.isfinite(o.get_field("comp")[0]))
+
+
+def test_flux_rows_of_the_boundary_row_operator():
+    # bc_mode 2 (the boundary-row operator, an added option): a prescribed flux
+    # is the boundary row D1 u = flux of the implicit solve, a fixed value the
+    # identity row; after each step both hold exactly (to rounding), for every
+    # (inner, outer) pair of types, temperature and composition alike
+    lmax, nr = 7, 11
+    o = O.Oracle(lmax=lmax, nlat=12, nlon=24, nr=nr, composition=1, schmidt=3.0, bc_mode=2, dt=1e-5)
+    rng = np.random.default_rng(31)
+    for k, (a, b) in workloads.seeded_state(lmax, lmax, nr, seed=4).items():
+        o.set_field(k, a, b)
+    o.set_field("comp", *workloads.seeded_state(lmax, lmax, nr, seed=5)["temp"])
+    D = dense_d1(o)
+    nlm = o.nlm
+    bvs = {}
+    for name, setter in (("temp", o.set_temperature_bc), ("comp", o.set_composition_bc)):
+        types = _types(nlm, rng)
+        bv = rng.standard_normal((2, nlm)) * 1e-2
+        o.set_bc_types(name, types[0], types[1])
+        setter(bv, None)
+        bvs[name] = (types, bv)
+    o.step(3)
+    for name, (types, bv) in bvs.items():
+        re, im = o.get_field(name)
+        dp = D @ re
+        for side, row in ((0, 0), (1, -1)):
+            flux = types[side] == FLUX
+            got = np.where(flux, dp[row], re[row])
+            assert np.max(np.abs(got - bv[side])) <= 1e-10 * (1 + np.max(np.abs(bv[side]))), (name, side)
+            assert np.max(np.abs(np.where(flux, (D @ im)[row], im[row]))) <= 1e-10, (name, side)
