@@ -703,7 +703,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed", "mixed_vel64"],
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed", "mixed_vel64", "mixed_vel64i8"],
                     help="auto: mixed_vel64 (the mixed step with its velocity chain in FP64, the configuration "
                          "that meets the energy condition) when the device has tcgen05, else fp64")
     ap.add_argument("--accuracy-study", action="store_true",
@@ -914,7 +914,7 @@ def main():
     # the fast mixed step (every stage in mixed precision) beside the headline
     # configuration, when the headline is the one with its velocity chain in FP64
     variants = {}
-    if precision == "mixed_vel64":
+    if precision in ("mixed_vel64", "mixed_vel64i8"):
         gf = make("mixed")
         gf.step(args.warmup)
         msf = timed_steps(gf, args.steps, 0)
@@ -995,7 +995,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None,
                 "dtype": {"fp64": "f64", "mixed": "f32/tf32x3 (FP64 solves)",
-                          "mixed_vel64": "f32/tf32x3, velocity chain f64 (FP64 solves)"}[precision],
+                          "mixed_vel64": "f32/tf32x3, velocity chain f64 (FP64 solves)",
+                          "mixed_vel64i8": "f32/tf32x3, velocity chain f64 with its synthesis in int8 "
+                                           "digit slices (FP64 solves)"}[precision],
                 "data": "synthetic (seeded default_rng(0) state, amplitude 1e-3 (l+1)^-2)",
                 "config": {"workload": WORKLOAD, "lmax": p["lmax"], "nlat": p["nlat"], "nlon": p["nlon"], "nr": p["nr"],
                            "dt": p["dt"], "precision": precision, "parallelism": f"replicas x{world}",

@@ -52,9 +52,13 @@ GRIDS = {
 PRECISIONS = {"fp64": 0, "mixed": 1}
 # Stages of the mixed-precision step that can run in FP64 (GD_STAGE_*): the
 # chain the velocity, and so the kinetic energy, depends on.
-FP64_STAGES = {"vel_synth": 1, "vel_products": 2, "vel_analysis": 4}
-# Named precision settings: the mixed step with its velocity chain in FP64.
-PRECISION_PRESETS = {"mixed_vel64": ("mixed", ("vel_synth", "vel_products", "vel_analysis"))}
+# "vel_synth_i8": the vector synthesis of u on the tensor cores by int8 digit
+# slices (FP64-accurate; replaces the DMMA synthesis of "vel_synth").
+FP64_STAGES = {"vel_synth": 1, "vel_products": 2, "vel_analysis": 4, "vel_synth_i8": 8}
+# Named precision settings: the mixed step with its velocity chain in FP64
+# ("mixed_vel64"), or with the chain's synthesis by int8 slices ("mixed_vel64i8").
+PRECISION_PRESETS = {"mixed_vel64": ("mixed", ("vel_synth", "vel_products", "vel_analysis")),
+                     "mixed_vel64i8": ("mixed", ("vel_synth_i8", "vel_products", "vel_analysis"))}
 SCHEMES = {"cnab2": 0, "eab2": 1, "erk2": 2}
 GEOMETRIES = {"shell": 0, "ball": 1}   # geometry (src/parameters.jl:75)   # ts_scheme (src/simulation.jl:1054-1300)
 ETD_MATRICES = ("E", "phi1", "phi2", "E_half", "phi1_half")   # ERK2Cache fields (src/timestep.jl:830-853)
@@ -63,6 +67,7 @@ KINDS = {"velocity": 0, "magnetic": 1, "temperature": 2, "composition": 3}
 # Every symbol include/gdb200.h declares.
 EXPORTS = (
     "gd_create", "gd_destroy", "gd_last_error", "gd_info", "gd_grid", "gd_set_precision", "gd_set_fp64_stages",
+    "gd_set_int8_digits",
     "gd_synchronize",
     "gd_upload_spectral", "gd_download_spectral", "gd_download_nonlinear", "gd_download_grid",
     "gd_set_temperature_bc", "gd_spectral_to_physical", "gd_physical_to_spectral", "gd_vector_synthesis",
@@ -146,6 +151,7 @@ def load_library():
         "gd_grid": ([P, D, D, D], I),
         "gd_set_precision": ([P, I], I),
         "gd_set_fp64_stages": ([P, I], I),
+        "gd_set_int8_digits": ([P, I], I),
         "gd_synchronize": ([P], I),
         "gd_upload_spectral": ([P, I, D, D], I),
         "gd_download_spectral": ([P, I, D, D], I),
@@ -420,6 +426,10 @@ class SHTnsKitConfig:
         mask = stages if isinstance(stages, int) else sum(FP64_STAGES[n] for n in stages)
         self._check(self.lib.gd_set_fp64_stages(self.h, int(mask)))
         self.fp64_stages = mask
+
+    def set_int8_digits(self, digits):
+        """Digits of 7 bits per operand of the int8-slice synthesis (5 or 6)."""
+        self._check(self.lib.gd_set_int8_digits(self.h, int(digits)))
 
     def spec_shape(self):
         return (self.nr, self.nlm)

@@ -11,6 +11,7 @@
 #include "gd_handle.cuh"
 #include "gd_internal.cuh"
 #include "gd_mixed.cuh"
+#include "gd_ozaki.cuh"
 
 using namespace gd;
 
@@ -892,10 +893,24 @@ int gd_set_precision(gd_handle* h, int mode) {
 
 int gd_set_fp64_stages(gd_handle* h, int mask) {
   if (!h) return GD_ERR_ARG;
-  if (mask < 0 || (mask & ~GD_STAGE_VEL_ALL)) return fail(h, GD_ERR_ARG, "unknown stage in the FP64 stage mask");
+  if (mask < 0 || (mask & ~(GD_STAGE_VEL_ALL | GD_STAGE_VEL_SYNTH_I8)))
+    return fail(h, GD_ERR_ARG, "unknown stage in the FP64 stage mask");
+  if ((mask & GD_STAGE_VEL_SYNTH_I8) && !oz_supported(h->d))
+    return fail(h, GD_ERR_UNSUPPORTED, "the int8-slice synthesis takes one shell range (no segments, no ball) and lmax <= 511");
   CK(cudaSetDevice(h->device));
   if (mask != h->fp64_stages) drop_graphs(h);
   h->fp64_stages = mask;
+  if ((mask & GD_STAGE_VEL_SYNTH_I8) && h->mixed) return mixed_prepare_int8(h);
+  return GD_OK;
+}
+
+int gd_set_int8_digits(gd_handle* h, int digits) {
+  if (!h) return GD_ERR_ARG;
+  if (digits != 5 && digits != 6) return fail(h, GD_ERR_ARG, "int8 digits must be 5 or 6");
+  CK(cudaSetDevice(h->device));
+  if (digits != h->int8_digits) drop_graphs(h);
+  h->int8_digits = digits;
+  if ((h->fp64_stages & GD_STAGE_VEL_SYNTH_I8) && h->mixed) return mixed_prepare_int8(h);
   return GD_OK;
 }
 
@@ -2360,6 +2375,7 @@ int gd_ensemble_autotune(gd_ensemble* e, int nsteps, float* best_ms, int* caps_o
     gd_handle* src = e->members[i];
     gd_handle* h = t->members[i];
     if (src->precision != GD_PREC_FP64) st = gd_set_precision(h, src->precision);
+    if (st == GD_OK) st = gd_set_int8_digits(h, src->int8_digits);
     if (st == GD_OK) st = gd_set_fp64_stages(h, src->fp64_stages);
     if (st == GD_OK && src->scheme != h->scheme) st = gd_set_scheme(h, src->scheme);
   }

@@ -18,6 +18,7 @@ struct gd_handle {
   std::string err;
   long step_count = 0;
   int precision = GD_PREC_FP64;
+  int int8_digits = 6;        // digits per operand of GD_STAGE_VEL_SYNTH_I8
   int fp64_stages = 0;        // GD_STAGE_* run in FP64 inside the mixed-precision step
   // the phases take the radial derivatives (grad T, curl u, curl B) from the
   // work arrays instead of computing them, and leave the temperature

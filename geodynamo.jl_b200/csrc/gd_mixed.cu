@@ -2,6 +2,7 @@
 // grid products; split-TF32 tensor-core Legendre contractions
 // (gd_legendre_tc.cu); FP64 spectral operators, CNAB2 solves and energies
 // (shared with the FP64 path).
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -11,6 +12,7 @@
 #include "gd_mixed.cuh"
 #include "gd_fused.cuh"
 #include "gd_mixed_kernels.cuh"
+#include "gd_ozaki.cuh"
 
 namespace gd {
 
@@ -47,6 +49,15 @@ struct MixedState {
   int* d_err = nullptr;
   long long wait_limit = 0;    // clock cycles of each bounded wait (0: the kernels' default)
   int omit_plus1 = 0;          // error-path tests: the next synthesis omits a step's copies in CTA 0
+  // int8-slice velocity synthesis (GD_STAGE_VEL_SYNTH_I8): table images and
+  // row exponents (built once per digit count), coefficient images and
+  // column exponents (rewritten every step)
+  int oz_digits = 0;
+  OzLayout oz{};
+  signed char* oz_imgA = nullptr;
+  signed char* oz_imgB = nullptr;
+  double* oz_rs = nullptr;
+  double* oz_cs = nullptr;
   size_t bytes = 0;
   std::vector<void*> allocs;
   float4* F(int c) const { return d_Fall + fcomp * c; }
@@ -336,7 +347,43 @@ int mixed_create(gd_handle* h) {
   if (s) return s;
   s = mcheck(h, cudaMemsetAsync(x->d_err, 0, sizeof(int), h->stream), "memset");
   if (s) return s;
-  return mcheck(h, cudaStreamSynchronize(h->stream), "mixed set-up");
+  s = mcheck(h, cudaStreamSynchronize(h->stream), "mixed set-up");
+  if (s) return s;
+  return (h->fp64_stages & GD_STAGE_VEL_SYNTH_I8) ? mixed_prepare_int8(h) : GD_OK;
+}
+
+int mixed_prepare_int8(gd_handle* h) {
+  MixedState* x = h->mixed;
+  if (!x) return GD_OK;
+  if (x->oz_digits == h->int8_digits) return GD_OK;
+  const Dims& d = h->d;
+  for (void* p : {(void*)x->oz_imgA, (void*)x->oz_imgB, (void*)x->oz_rs, (void*)x->oz_cs}) {
+    if (!p) continue;
+    cudaFree(p);
+    x->allocs.erase(std::find(x->allocs.begin(), x->allocs.end(), p));
+  }
+  x->bytes -= x->oz.a_bytes + x->oz.b_bytes + sizeof(double) * (x->oz.rs_elems + x->oz.cs_elems);
+  x->oz_digits = 0;
+  x->oz = oz_layout(d, h->int8_digits);
+  auto al = [&](size_t bytes, void** p) -> int {
+    int s = mcheck(h, cudaMalloc(p, bytes), "int8 slice images");
+    if (s) return s;
+    x->allocs.push_back(*p);
+    x->bytes += bytes;
+    return GD_OK;
+  };
+  int s = al(x->oz.a_bytes, (void**)&x->oz_imgA);
+  if (!s) s = al(x->oz.b_bytes, (void**)&x->oz_imgB);
+  if (!s) s = al(sizeof(double) * x->oz.rs_elems, (void**)&x->oz_rs);
+  if (!s) s = al(sizeof(double) * x->oz.cs_elems, (void**)&x->oz_cs);
+  if (s) return s;
+  launch_oz_tables(h->stream, d, h->d_moff, h->d_dP, h->d_Q, x->oz, x->oz_imgA, x->oz_rs);
+  s = launched(h, "int8 table images");
+  if (s) return s;
+  s = mcheck(h, cudaStreamSynchronize(h->stream), "int8 table images");
+  if (s) return s;
+  x->oz_digits = h->int8_digits;
+  return GD_OK;
 }
 
 void mixed_destroy(gd_handle* h) {
@@ -457,7 +504,19 @@ int mixed_velocity_nl(gd_handle* h) {
   double2* G64 = h->d_F + 2 * fc64;  // folded transforms of the velocity products (FP64)
   const size_t nfold = 2 * fc64;     // double2 of the two folded components
   int s;
-  if (st & GD_STAGE_VEL_SYNTH) {
+  if (st & GD_STAGE_VEL_SYNTH_I8) {
+    OzSynthArgs a{};
+    a.out = U64;
+    a.out32 = x->F(FC_U);  // the FP32 copy the fused phase kernels read
+    a.out32_comp = x->fcomp;
+    a.err = x->d_err;
+    a.wait_limit = x->wait_limit;
+    a.max_ctas = h->tc_ctas;
+    { ProfScope p(h, "legendre_synth_vector_i8");
+      launch_oz_synth_vector(h->stream, d, h->d_moff, x->oz, h->field(F_UPOL), h->field(F_UTOR), x->oz_imgA, x->oz_rs,
+                             x->oz_imgB, x->oz_cs, a); }
+    s = launched(h, "int8-slice velocity synthesis");
+  } else if (st & GD_STAGE_VEL_SYNTH) {
     SynthArgs a{};
     a.table0 = h->d_dP;
     a.table1 = h->d_Q;

@@ -9,6 +9,9 @@ struct gd_handle;
 
 namespace gd {
 int mixed_create(gd_handle* h);
+// Slice images and scratch of the int8-slice velocity synthesis
+// (GD_STAGE_VEL_SYNTH_I8) for h->int8_digits; nothing if they exist already.
+int mixed_prepare_int8(gd_handle* h);
 // GD_ERR_CUDA if a tensor-core wait expired since creation (synchronises the stream).
 int mixed_check_error(gd_handle* h);
 // Error-path tests: the bound of every tensor-core wait (clock cycles, <= 0:

@@ -74,7 +74,13 @@ enum {
   GD_STAGE_VEL_SYNTH = 1,    /* vector synthesis of u (Legendre, DMMA)                */
   GD_STAGE_VEL_PRODUCTS = 2, /* phi transforms of u and the Coriolis product          */
   GD_STAGE_VEL_ANALYSIS = 4, /* vector analysis of the velocity's terms (Legendre)    */
-  GD_STAGE_VEL_ALL = 7
+  GD_STAGE_VEL_ALL = 7,
+  /* the vector synthesis of u on the tcgen05 tensor cores by int8 digit slices
+   * (error-free products, int32 accumulation; FP64-accurate to about 2^-40
+   * of row max x column max with 6 digits), writing what GD_STAGE_VEL_SYNTH
+   * writes; takes precedence over GD_STAGE_VEL_SYNTH.  One shell range, lmax
+   * <= 511: not with segments or a ball (GD_ERR_UNSUPPORTED). */
+  GD_STAGE_VEL_SYNTH_I8 = 8
 };
 
 /* Time-stepping schemes of gd_step (the reference's ts_scheme,
@@ -175,6 +181,9 @@ int gd_set_precision(gd_handle* h, int mode);
  * With GD_STAGE_VEL_ALL the velocity's nonlinear term, and so the velocity
  * field, equals the FP64 step's.  Has no effect in GD_PREC_FP64. */
 int gd_set_fp64_stages(gd_handle* h, int mask);
+/* Digits of 7 bits per operand of GD_STAGE_VEL_SYNTH_I8: 6 (default; 21 digit
+ * products per term) or 5 (15 products, about 2^-33). */
+int gd_set_int8_digits(gd_handle* h, int digits);
 int gd_synchronize(gd_handle* h);
 
 /* ---- state ------------------------------------------------------------------
