@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(256) k_oz_coef_image(Dims d, const int* __rest
                                                        int ncb) {
   constexpr int BSL = N * OZ_KS;
   extern __shared__ double cv[];  // [N][L - m + 1]: the tile's columns, degree fastest
-  __shared__ double sc[2][N];
+  __shared__ double sc[1][N];
   const int ct = blockIdx.x, m = blockIdx.y;
   const int nks = oz_nksmax(d.L);
   const int nl = d.L - m + 1;
@@ -219,38 +219,58 @@ __global__ void __launch_bounds__(256) k_oz_coef_image(Dims d, const int* __rest
   const int mb = moff[m];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr int NW = 256 / 32;
-  // one coalesced read of every coefficient of the tile
+  // one coalesced read of every coefficient of the tile, eight loads in flight
+  // per lane, and the column maximum over the degrees of both parities
   for (int c = warp; c < N; c += NW) {
     const int r = ct * (N / 4) + (c >> 2), fld = (c >> 1) & 1, ci = c & 1;
     const double* src = r < d.nr ? (fld == 0 ? S : T) + ((size_t)ci * d.nr + r) * NM + mb : nullptr;
-    for (int j = lane; j < nl; j += 32) cv[c * nl + j] = src != nullptr ? src[j] : 0.0;
-  }
-  __syncthreads();
-  // one exponent per column for both parities
-  for (int c = warp; c < N; c += NW) {
     double amax = 0.0;
-    for (int j = lane; j < nl; j += 32) amax = fmax(amax, fabs(cv[c * nl + j]));
+    for (int j0 = 0; j0 < nl; j0 += 256) {
+      double x[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = j0 + 32 * u + lane;
+        x[u] = (src != nullptr && j < nl) ? __ldg(src + j) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = j0 + 32 * u + lane;
+        if (j < nl) cv[c * nl + j] = x[u];
+        amax = fmax(amax, fabs(x[u]));
+      }
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
     if (lane == 0) {
       const int e = oz_exp(amax);
-      sc[0][c] = sc[1][c] = ldexp(1.0, 7 * G - 1 - e);
+      sc[0][c] = ldexp(1.0, 7 * G - 1 - e);
       csc[((size_t)m * ncb + ct) * N + c] = ldexp(1.0, e);
     }
   }
   __syncthreads();
+  // digits: each thread four consecutive degrees of one column, one 32-bit
+  // word per slice (the four bytes stay together under the 32-byte swizzle)
   for (int p = 0; p < 2; ++p) {
     const int nk = oz_nks(d.L, m, p);
     for (int ks = 0; ks < nk; ++ks) {
       signed char* out = img + ((((size_t)m * 2 + p) * ncb + ct) * nks + ks) * (size_t)G * BSL;
-      const int j = p + 2 * (ks * OZ_KS + lane);  // degree m + j
-      for (int c = warp; c < N; c += NW) {
-        const double x = j < nl ? cv[c * nl + j] : 0.0;
-        signed char dg[G];
-        oz_digits<G>(x, sc[p][c], dg);
-        const uint32_t o = sw32_byte(c, lane);
+      for (int e = tid; e < N * (OZ_KS / 4); e += blockDim.x) {
+        const int c = e / (OZ_KS / 4), k0 = 4 * (e % (OZ_KS / 4));
+        uint32_t w[G];
 #pragma unroll
-        for (int i = 0; i < G; ++i) out[(size_t)i * BSL + o] = dg[i];
+        for (int i = 0; i < G; ++i) w[i] = 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = p + 2 * (ks * OZ_KS + k0 + u);  // degree m + j
+          const double x = j < nl ? cv[c * nl + j] : 0.0;
+          signed char dg[G];
+          oz_digits<G>(x, sc[0][c], dg);
+#pragma unroll
+          for (int i = 0; i < G; ++i) w[i] |= (uint32_t)(uint8_t)dg[i] << (8 * u);
+        }
+        const uint32_t o = sw32_byte(c, k0);
+#pragma unroll
+        for (int i = 0; i < G; ++i) *reinterpret_cast<uint32_t*>(out + (size_t)i * BSL + o) = w[i];
       }
     }
   }
