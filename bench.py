@@ -103,6 +103,17 @@ def kernel_work(name, p, nlm, precision):
         "legendre_analysis_scalar": (2.0 * nlm * nlat * nr, F * cb + S * 8 + anal_table),
         "legendre_analysis_vector": (8.0 * nlm * nlat * nr, 2 * F * cb + 2 * S * 8 + 2 * anal_table),
     }
+    if name == "legendre_synth_vector_i8":
+        # int8 digit slices (6 digits): 21 int8 products per FP64 product; bytes:
+        # the FP64 coefficients, the FP64 Fourier output and its FP32 copy, the
+        # coefficient digit images (written, then read once per colatitude
+        # tile) and the table digit images
+        ksteps = sum(-(-((L - m + 2) // 2) // 32) + -(-((L - m + 1) // 2) // 32) for m in range(L + 1))
+        ncb = -(-4 * nr // 32)
+        b_img = ksteps * ncb * 6 * 32 * 32
+        a_img = ksteps * (-(-nth // 64)) * 6 * 128 * 32
+        return {"flops": 8.0 * nlm * nlat * nr * 21, "int8": True,
+                "bytes": 2 * S * 8 + 2 * F * 16 + 2 * F * 8 + b_img * (1 + -(-nth // 64)) + a_img}
     for k, (fl, by) in legendre.items():
         if name.startswith(k):
             return {"flops": fl, "bytes": by}
@@ -704,8 +715,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed", "mixed_vel64", "mixed_vel64i8"],
-                    help="auto: mixed_vel64 (the mixed step with its velocity chain in FP64, the configuration "
-                         "that meets the energy condition) when the device has tcgen05, else fp64")
+                    help="auto: mixed_vel64i8 (the mixed step with its velocity chain at FP64 accuracy, its "
+                         "synthesis by int8 digit slices on the tensor cores: the configuration that meets the energy "
+                         "condition) when the device has tcgen05, else fp64")
     ap.add_argument("--accuracy-study", action="store_true",
                     help="instead of the headline: the FP64 one-ulp floor and the per-stage error budget")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
@@ -778,7 +790,7 @@ def main():
             probe = gdb.SHTnsKitConfig(7, 12, 24, 9, device=local)
             probe.set_precision("mixed")
             probe.close()
-            precision = "mixed_vel64"
+            precision = "mixed_vel64i8"
         except gdb.GeoDynamoError:
             precision = "fp64"
 
@@ -865,6 +877,8 @@ def main():
         if "tflops" in top:
             if top["name"].endswith("fp64") or top["name"].startswith(("eab2", "erk2")):
                 pk, src = dgemm, "cuBLAS FP64 GEMM 4096^3 measured in this run (torch.matmul)"
+            elif top["name"].endswith("_i8"):
+                pk, src = peaks.get("bf16_tflops", 1590.0) * 2.0, "twice the measured bf16 burst peak (int8 rate)"
             else:
                 pk, src = peaks.get("bf16_tflops", 1590.0) / 2.0, "half the measured bf16 burst peak (tf32 rate)"
             bounds.append({"bound": "tensor", "achieved": top["tflops"], "peak": pk, "unit": "TFLOP/s",

@@ -511,7 +511,9 @@ int mixed_velocity_nl(gd_handle* h) {
     a.out32_comp = x->fcomp;
     a.err = x->d_err;
     a.wait_limit = x->wait_limit;
+    a.omit_plus1 = x->omit_plus1;
     a.max_ctas = h->tc_ctas;
+    x->omit_plus1 = 0;  // one-shot
     { ProfScope p(h, "legendre_synth_vector_i8");
       launch_oz_synth_vector(h->stream, d, h->d_moff, x->oz, h->field(F_UPOL), h->field(F_UTOR), x->oz_imgA, x->oz_rs,
                              x->oz_imgB, x->oz_cs, a); }

@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_synth_vector(Dims d, const
   const uint32_t tmem = *tslot;
   const int ntiles = (d.M + 1) * ntt * ncb;
   bool ok = true;
-  int issued = -1;  // producer: last pipeline step whose bulk copies were issued
+  int issued = -1;   // producer: last pipeline step whose bulk copies were issued
+  int omitted = -1;  // producer: the step an error-path test left out
 
   if (warp == 0) {
     int gs = 0;
@@ -352,7 +353,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_synth_vector(Dims d, const
             ok = false;
             break;
           }
-          if (lane == 0) {
+          // error-path tests: CTA 0 may omit one step's copies, so the MMA
+          // warp's bounded wait on that stage runs out
+          const bool omit = a.omit_plus1 == Gs + 1 && blockIdx.x == 0;
+          if (lane == 0 && !omit) {
             unsigned char* A = stg + (size_t)s * SM::ST;
             const size_t ta = (((size_t)t.m * ntt + t.th) * 2 + p) * nksm + ks;
             const size_t tb = (((size_t)t.m * 2 + p) * ncb + t.ct) * nksm + ks;
@@ -360,7 +364,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_synth_vector(Dims d, const
             bulk_g2s(A, imgA + ta * (G * OZ_A_SLICE), G * OZ_A_SLICE, &full[s]);
             bulk_g2s(A + G * OZ_A_SLICE, imgB + tb * (G * BSL), G * BSL, &full[s]);
           }
-          issued = Gs;
+          if (!omit) issued = Gs;
+          else omitted = Gs;
           __syncwarp();
         }
       }
@@ -528,8 +533,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_synth_vector(Dims d, const
   // after an expired wait anywhere in the CTA: the producer lets its last bulk
   // copies land and the MMA warp waits for the MMAs it has issued, before
   // tensor memory is freed and the CTA exits
-  if (!ok && warp == 0 && issued >= 0)
-    mbar_wait(&full[issued % S], (issued / S) & 1, a.err, a.wait_limit);
+  if (!ok && warp == 0)
+    for (int g = max(0, issued - S + 1); g <= issued; ++g)  // every stage's last issued copies
+      if (g != omitted) mbar_wait(&full[g % S], (g / S) & 1, a.err, a.wait_limit);
   if (!ok && warp == 1) {
     if (lane == 0) mma_commit(smem_addr(drain));
     __syncwarp();

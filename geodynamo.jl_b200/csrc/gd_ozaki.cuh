@@ -27,6 +27,7 @@ struct OzSynthArgs {
   size_t out32_comp;  // float4 per component of out32
   int* err;           // set to 1 if a bounded wait expires
   long long wait_limit;
+  int omit_plus1;     // > 0: CTA 0 omits the bulk copies of pipeline step omit_plus1 - 1 (error-path tests)
   int max_ctas;       // persistent CTAs (0: one per SM)
 };
 

@@ -55,3 +55,26 @@ def test_fault_test_needs_mixed_state(gdb):
     with pytest.raises(gdb.GeoDynamoError) as e:
         g.set_fault_test(1 << 24, 0)
     assert e.value.status == 7
+
+
+def test_expired_wait_in_int8_synthesis_is_reported_and_handle_recovers(gdb, oracle_mod):
+    # the same failure in the int8-slice velocity synthesis (the first
+    # tensor-core launch of the velocity phase with GD_STAGE_VEL_SYNTH_I8)
+    lmax, nlat, nlon, nr = 31, 48, 96, 8
+    g = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, precision="mixed_vel64i8", bc_mode=2, dt=1e-5)
+    o = oracle_mod.Oracle(lmax=lmax, nlat=nlat, nlon=nlon, nr=nr, bc_mode=2, dt=1e-5)
+    st = workloads.seeded_state(lmax, lmax, nr, seed=2)
+    for k, (a, b) in st.items():
+        g.set_field(k, a, b)
+        o.set_field(k, a, b)
+    g.set_fault_test(wait_cycles=1 << 24, omit_step=0)
+    with pytest.raises(gdb.GeoDynamoError) as e:
+        g.velocity_nl()
+    assert e.value.status == 3 and "wait expired" in str(e.value)
+    g.set_fault_test(0, -1)
+    for k, (a, b) in st.items():
+        g.set_field(k, a, b)
+    g.step(2)
+    o.step(2)
+    for k in ("u_tor", "u_pol"):
+        assert rel(g.get_field(k)[0], o.get_field(k)[0]) < 1e-11, k
