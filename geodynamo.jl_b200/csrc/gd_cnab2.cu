@@ -10,6 +10,8 @@
 // factors.  The AB bootstrap (src/simulation.jl:1153-1170) is folded into the
 // same pass; the history roll (:1312-1329) is the handle's switch of the two
 // banks of nonlinear terms after the step (N_prev is read from the other bank).
+#include <type_traits>
+
 #include "gd_internal.cuh"
 
 namespace gd {
@@ -44,68 +46,103 @@ __device__ __forceinline__ void cnab2_column(const Dims& d, int j, int l, const 
   const double* __restrict__ rowv = a.rowvals[slot];
   const int stages = a.stages ? a.stages : 7;
 
-  // sweep 1: right-hand side, rows in batches of RB whose loads are issued first
+  // sweep 1: right-hand side, rows in batches of RB whose loads are issued
+  // first.  With FWD the forward substitution of sweep 2 runs in the same pass
+  // (both walk r upward; the window keeps the original u the band still
+  // needs), so y is written over u without a second pass through memory.
   constexpr int RB = 4;
-  if (stages & 1) {
-  double wr[NB], wi[NB];
+  auto rhs_sweep = [&](auto fwd_tag) {
+    constexpr bool FWD = decltype(fwd_tag)::value;
+    constexpr int RBF = FWD ? 3 : 4;  // the factor rows take the registers of a fourth row
+    double wr[NB], wi[NB];
+    double yr[KL], yi[KL];
 #pragma unroll
-  for (int t = 0; t < NB; ++t) {
-    const int idx = t - KL;
-    wr[t] = (idx >= 0 && idx < N) ? ure[(size_t)idx * NM] : 0.0;
-    wi[t] = (idx >= 0 && idx < N) ? uim[(size_t)idx * NM] : 0.0;
-  }
-  for (int i0 = 0; i0 < N; i0 += RB) {
-    double unr[RB], uni[RB], nr_[RB], ni_[RB], pr_[RB], pi_[RB];
+    for (int t = 0; t < KL; ++t) yr[t] = yi[t] = 0.0;
 #pragma unroll
-    for (int b = 0; b < RB; ++b) {
-      const int i = i0 + b, nxt = i + KL + 1;
-      unr[b] = (nxt < N) ? ure[(size_t)nxt * NM] : 0.0;
-      uni[b] = (nxt < N) ? uim[(size_t)nxt * NM] : 0.0;
-      if (i < N) {
-        nr_[b] = nre[(size_t)i * NM];
-        ni_[b] = nim[(size_t)i * NM];
-        pr_[b] = boot ? nr_[b] : pre[(size_t)i * NM];
-        pi_[b] = boot ? ni_[b] : pim[(size_t)i * NM];
-      } else {
-        nr_[b] = ni_[b] = pr_[b] = pi_[b] = 0.0;
-      }
+    for (int t = 0; t < NB; ++t) {
+      const int idx = t - KL;
+      wr[t] = (idx >= 0 && idx < N) ? ure[(size_t)idx * NM] : 0.0;
+      wi[t] = (idx >= 0 && idx < N) ? uim[(size_t)idx * NM] : 0.0;
     }
+    for (int i0 = 0; i0 < N; i0 += RBF) {
+      double unr[RBF], uni[RBF], nr_[RBF], ni_[RBF], pr_[RBF], pi_[RBF];
+      double lf[RBF][FWD ? KL : 1];
 #pragma unroll
-    for (int b = 0; b < RB; ++b) {
-      const int i = i0 + b;
-      if (i >= N) break;
-      const size_t at = (size_t)i * NM;
-      double Lr = 0.0, Li = 0.0;
+      for (int b = 0; b < RBF; ++b) {
+        const int i = i0 + b, nxt = i + KL + 1;
+        unr[b] = (nxt < N) ? ure[(size_t)nxt * NM] : 0.0;
+        uni[b] = (nxt < N) ? uim[(size_t)nxt * NM] : 0.0;
+        if (i < N) {
+          nr_[b] = nre[(size_t)i * NM];
+          ni_[b] = nim[(size_t)i * NM];
+          pr_[b] = boot ? nr_[b] : pre[(size_t)i * NM];
+          pi_[b] = boot ? ni_[b] : pim[(size_t)i * NM];
+        } else {
+          nr_[b] = ni_[b] = pr_[b] = pi_[b] = 0.0;
+        }
+        if constexpr (FWD) {
 #pragma unroll
-      for (int t = 0; t < NB; ++t) {
-        const int col = i - KL + t;
-        if (col >= 0 && col < N) {
-          double cf = sband[col * NB + (KL + i - col)];
-          if (t == KL) cf = __dsub_rn(cf, __dmul_rn(nulf, srinv2[i]));
-          Lr += cf * wr[t];
-          Li += cf * wi[t];
+          for (int t = 0; t < KL; ++t) {
+            const int col = i - KL + t;
+            lf[b][t] = (i < N && col >= 0) ? F[((size_t)col * NB + (KL + i - col)) * Lp1] : 0.0;
+          }
         }
       }
-      double vr = a.inv_dt * wr[KL] + 1.5 * nr_[b] - 0.5 * pr_[b];
-      double vi = a.inv_dt * wi[KL] + 1.5 * ni_[b] - 0.5 * pi_[b];
-      vr += a.lin_weight * Lr;
-      vi += a.lin_weight * Li;
-      if (rows && (i == 0 || i == N - 1)) {
-        // ball: the r = 0 row of l >= 1 is the regularity condition (value 0)
-        vr = (rowv != nullptr && !(d.ball && i == 0 && l > 0)) ? rowv[(i == 0 ? 0 : NM) + j] : 0.0;
-        vi = 0.0;
-      }
-      ure[at] = vr;
-      uim[at] = vi;
 #pragma unroll
-      for (int t = 0; t < NB - 1; ++t) { wr[t] = wr[t + 1]; wi[t] = wi[t + 1]; }
-      wr[NB - 1] = unr[b];
-      wi[NB - 1] = uni[b];
+      for (int b = 0; b < RBF; ++b) {
+        const int i = i0 + b;
+        if (i >= N) break;
+        const size_t at = (size_t)i * NM;
+        double Lr = 0.0, Li = 0.0;
+#pragma unroll
+        for (int t = 0; t < NB; ++t) {
+          const int col = i - KL + t;
+          if (col >= 0 && col < N) {
+            double cf = sband[col * NB + (KL + i - col)];
+            if (t == KL) cf = __dsub_rn(cf, __dmul_rn(nulf, srinv2[i]));
+            Lr += cf * wr[t];
+            Li += cf * wi[t];
+          }
+        }
+        double vr = a.inv_dt * wr[KL] + 1.5 * nr_[b] - 0.5 * pr_[b];
+        double vi = a.inv_dt * wi[KL] + 1.5 * ni_[b] - 0.5 * pi_[b];
+        vr += a.lin_weight * Lr;
+        vi += a.lin_weight * Li;
+        if (rows && (i == 0 || i == N - 1)) {
+          // ball: the r = 0 row of l >= 1 is the regularity condition (value 0)
+          vr = (rowv != nullptr && !(d.ball && i == 0 && l > 0)) ? rowv[(i == 0 ? 0 : NM) + j] : 0.0;
+          vi = 0.0;
+        }
+        if constexpr (FWD) {
+          double sr = 0.0, si = 0.0;
+#pragma unroll
+          for (int t = 0; t < KL; ++t) {
+            if (i - KL + t >= 0) {
+              sr += lf[b][t] * yr[t];
+              si += lf[b][t] * yi[t];
+            }
+          }
+          vr = vr - sr;
+          vi = vi - si;
+#pragma unroll
+          for (int t = 0; t < KL - 1; ++t) { yr[t] = yr[t + 1]; yi[t] = yi[t + 1]; }
+          yr[KL - 1] = vr;
+          yi[KL - 1] = vi;
+        }
+        ure[at] = vr;
+        uim[at] = vi;
+#pragma unroll
+        for (int t = 0; t < NB - 1; ++t) { wr[t] = wr[t + 1]; wi[t] = wi[t + 1]; }
+        wr[NB - 1] = unr[b];
+        wi[NB - 1] = uni[b];
+      }
     }
-  }
-  }
+  };
+  const bool fused = (stages & 3) == 3;
+  if (fused) rhs_sweep(std::true_type{});
+  else if (stages & 1) rhs_sweep(std::false_type{});
   // sweep 2: forward substitution (unit lower factor), y[i - KL + t] in yr[t]
-  if (stages & 2) {
+  if ((stages & 2) && !fused) {
   double yr[KL], yi[KL];
 #pragma unroll
   for (int t = 0; t < KL; ++t) yr[t] = yi[t] = 0.0;

@@ -82,7 +82,9 @@ def test_single_fp64_stages_match_oracle(gdb, oracle_mod, stages):
 
 def test_stage_mask_is_validated(gdb):
     g = gdb.SHTnsKitConfig(7, 12, 24, 9, precision="mixed")
-    with pytest.raises(gdb.GeoDynamoError):
-        g.set_fp64_stages(8)
+    for bad in (16, -1):
+        with pytest.raises(gdb.GeoDynamoError):
+            g.set_fp64_stages(bad)
     g.set_fp64_stages(7)
+    g.set_fp64_stages(8 | 6)  # the int8-slice synthesis with the FP64 products and analysis
     g.set_fp64_stages(0)
