@@ -580,12 +580,9 @@ static void run_synth(cudaStream_t s, const Dims& d, const int* moff, const OzLa
                       const double* T, const signed char* imgA, const double* rsc, signed char* imgB, double* csc,
                       const OzSynthArgs& a) {
   const size_t cbytes = sizeof(double) * N * (d.L + 1);
-  static bool attr = false;
-  if (!attr) {
-    allow_dynamic_smem(k_oz_synth_vector<G, N>, OzSmem<G, N>::BYTES);
-    allow_dynamic_smem(k_oz_coef_image<G, N>, OZ_COEF_SMEM);
-    attr = true;
-  }
+  // cached per device (and thread-safe) inside allow_dynamic_smem
+  allow_dynamic_smem(k_oz_synth_vector<G, N>, OzSmem<G, N>::BYTES);
+  allow_dynamic_smem(k_oz_coef_image<G, N>, OZ_COEF_SMEM);
   k_oz_coef_image<G, N><<<dim3(o.ncb, d.M + 1), 256, cbytes, s>>>(d, moff, S, T, imgB, csc, o.ncb);
   const int ntiles = (d.M + 1) * ceil_div(d.nth, OZ_TH) * o.ncb;
   const int ctas = std::min(ntiles, a.max_ctas > 0 ? std::min(a.max_ctas, current_sm_count()) : current_sm_count());
