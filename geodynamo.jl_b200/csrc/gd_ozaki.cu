@@ -61,6 +61,7 @@ constexpr int OZ_EPI = OZ_THREADS - 64;
 constexpr int OZ_PB = 256;                // TMEM columns per parity
 constexpr int OZ_SMEM_MAX = 232448;       // 227 KB of dynamic shared memory per CTA
 constexpr int OZ_COEF_SMEM = 200 * 1024;  // the coefficient columns of one image tile (lmax <= 511)
+constexpr int OZ_CT = 512;                // threads of a coefficient-image CTA
 
 __host__ __device__ __forceinline__ int oz_kpar(int L, int m, int p) {
   return p == 0 ? (L - m + 2) / 2 : (L - m + 1) / 2;
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(OZ_M) k_oz_table_image(Dims d, const int* __re
 // others).
 // ---------------------------------------------------------------------------
 template <int G, int N>
-__global__ void __launch_bounds__(256) k_oz_coef_image(Dims d, const int* __restrict__ moff,
+__global__ void __launch_bounds__(OZ_CT) k_oz_coef_image(Dims d, const int* __restrict__ moff,
                                                        const double* __restrict__ S, const double* __restrict__ T,
                                                        signed char* __restrict__ img, double* __restrict__ csc,
                                                        int ncb) {
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(256) k_oz_coef_image(Dims d, const int* __rest
   const size_t NM = d.nlm;
   const int mb = moff[m];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  constexpr int NW = 256 / 32;
+  constexpr int NW = OZ_CT / 32;
   // one coalesced read of every coefficient of the tile, eight loads in flight
   // per lane, and the column maximum over the degrees of both parities
   for (int c = warp; c < N; c += NW) {
@@ -583,7 +584,7 @@ static void run_synth(cudaStream_t s, const Dims& d, const int* moff, const OzLa
   // cached per device (and thread-safe) inside allow_dynamic_smem
   allow_dynamic_smem(k_oz_synth_vector<G, N>, OzSmem<G, N>::BYTES);
   allow_dynamic_smem(k_oz_coef_image<G, N>, OZ_COEF_SMEM);
-  k_oz_coef_image<G, N><<<dim3(o.ncb, d.M + 1), 256, cbytes, s>>>(d, moff, S, T, imgB, csc, o.ncb);
+  k_oz_coef_image<G, N><<<dim3(o.ncb, d.M + 1), OZ_CT, cbytes, s>>>(d, moff, S, T, imgB, csc, o.ncb);
   const int ntiles = (d.M + 1) * ceil_div(d.nth, OZ_TH) * o.ncb;
   const int ctas = std::min(ntiles, a.max_ctas > 0 ? std::min(a.max_ctas, current_sm_count()) : current_sm_count());
   k_oz_synth_vector<G, N><<<ctas, OZ_THREADS, OzSmem<G, N>::BYTES, s>>>(d, imgA, rsc, imgB, csc, o.ncb, a);
