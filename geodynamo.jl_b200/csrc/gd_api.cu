@@ -79,15 +79,19 @@ int build_implicit(gd_handle* h) {
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   if (flag) return fail(h, GD_ERR_SINGULAR, "zero pivot in a banded LU factorisation");
-  // bc_mode 2 with one segment length: the factors for prescribed fluxes (the
-  // linear operator is the same; a scratch block takes the build's copy).  A
-  // zero pivot there only disables flux rows (gd_set_scalar_bc_types refuses them)
+  // bc_mode 2: the factors for prescribed fluxes, per segment length at the
+  // same offsets as the main factors (the linear operator is the same; a
+  // scratch block takes the build's copy).  A zero pivot there only disables
+  // flux rows (gd_set_scalar_bc_types refuses them)
   if (h->d_lu_flux) {
     CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
     for (int fv = 1; fv <= 3; ++fv)
-      launch_build_lu(h->stream, h->var_n[0], d.kl, d.L, h->d_d1, h->d_d2, h->d_rinv, h->d_rinv2, h->d_nu, h->c.dt,
-                      h->c.implicit_theta, 1 | (fv << 1), h->d_lu_flux + 3 * h->lu_flux_stride,
-                      h->d_lu_flux + (size_t)(fv - 1) * h->lu_flux_stride, h->d_flag, h->c.composition ? 4 : 3);
+      for (size_t v = 0; v < h->var_n.size(); ++v)
+        launch_build_lu(h->stream, h->var_n[v], d.kl, d.L, h->d_d1 + h->var_band[v], h->d_d2 + h->var_band[v],
+                        h->d_rinv + h->var_rep[v], h->d_rinv2 + h->var_rep[v], h->d_nu, h->c.dt,
+                        h->c.implicit_theta, 1 | (fv << 1), h->d_lu_flux + 3 * h->lu_flux_stride + h->var_op[v],
+                        h->d_lu_flux + (size_t)(fv - 1) * h->lu_flux_stride + h->var_op[v], h->d_flag,
+                        h->c.composition ? 4 : 3);
     s = check_launch(h, "build_lu (flux rows)");
     if (s) return s;
     CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -248,10 +252,11 @@ int setup(gd_handle* h) {
   AL(h->d_P, NL * NT); AL(h->d_dP, NL * NT); AL(h->d_Q, NL * NT);
   AL(h->d_d1, nbw * NR); AL(h->d_d2, nbw * NR);
   AL(h->d_lin, 4 * NR * nbw * (d.L + 1)); AL(h->d_lu, 4 * NR * nbw * (d.L + 1));
-  if (c.bc_mode == 2 && h->var_n.size() == 1) {
-    // three flux-row variants of the factors, and a block that takes the
+  if (c.bc_mode == 2) {
+    // three flux-row variants of the factors (each laid out like d_lu: one
+    // operator set per segment length at var_op), and a block that takes the
     // build's copy of the linear operator
-    h->lu_flux_stride = (size_t)4 * h->var_n[0] * nbw * (d.L + 1);
+    h->lu_flux_stride = h->var_op.back() + (size_t)4 * h->var_n.back() * nbw * (d.L + 1);
     AL(h->d_lu_flux, 4 * h->lu_flux_stride);
   }
   AL(h->d_tw, 2 * (size_t)d.nlon); AL(h->d_twf, 2 * (size_t)d.nlon);
@@ -1195,8 +1200,9 @@ int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int*
   for (size_t q = 0; q < NL; ++q) inner_flux |= inner[q] == GD_BC_FLUX;
   if (inner_flux && h->d.ball)
     return fail(h, GD_ERR_UNSUPPORTED, "a ball has no inner boundary: its centre row is the regularity condition");
-  if (flux && h->var_n.size() > 1)
-    return fail(h, GD_ERR_UNSUPPORTED, "flux boundaries need segments of one length (one set of tau functions)");
+  if (flux && h->var_n.size() > 1 && h->c.bc_mode != 2)
+    return fail(h, GD_ERR_UNSUPPORTED,
+                "tau flux boundaries need segments of one length (one set of tau functions); bc_mode 2 takes them");
   if (flux && h->c.bc_mode == 2 && !h->flux_rows_ok)
     return fail(h, GD_ERR_SINGULAR, "the implicit factorisation with flux boundary rows has a zero pivot");
   CK(cudaSetDevice(h->device));

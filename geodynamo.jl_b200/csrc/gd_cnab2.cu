@@ -272,7 +272,8 @@ __global__ void __launch_bounds__(128, 3) k_cnab2(Dims d, const int* __restrict_
   if (a.bc_rows && rt != nullptr && a.lu_flux != nullptr) {
     // a prescribed flux at a boundary: the factors with the row of D1 there
     const int fv = (rt[j] == GD_BC_FLUX ? 1 : 0) | (rt[d.nlm + j] == GD_BC_FLUX ? 2 : 0);
-    if (fv) LUk = a.lu_flux + (size_t)(fv - 1) * a.lu_flux_stride + (size_t)g * N * NB * ((size_t)d.L + 1);
+    if (fv)
+      LUk = a.lu_flux + (size_t)(fv - 1) * a.lu_flux_stride + sv.op_off + (size_t)g * N * NB * ((size_t)d.L + 1);
   }
   cnab2_column<KL>(d, j, l, LUk, sband, srinv2, nuk, a, slot, N, sv.base);
 }
