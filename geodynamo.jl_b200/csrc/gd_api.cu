@@ -113,53 +113,62 @@ int build_implicit(gd_handle* h) {
 // single-boundary combinations and their D1 derivatives at the boundary they
 // serve.  Needs the radial nodes and D1 on the device.
 int build_tau(gd_handle* h) {
-  // variant 0 (flux boundaries are refused with several variants)
-  const int N = h->var_n[0], KL = h->d.kl, NB = 2 * GD_MAX_KL + 1;
-  std::vector<double> r(N), d1((size_t)NB * N);
-  CK(cudaMemcpyAsync(r.data(), h->d_r, sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaMemcpyAsync(d1.data(), h->d_d1, sizeof(double) * NB * N, cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  const double ri = r[0], ro = r[N - 1];
-  auto cheb = [&](int n, double rr) {
-    double x = 2.0 * (rr - ri) / (ro - ri) - 1.0;
-    x = x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x);
-    return std::cos(n * std::acos(x));
-  };
-  auto dcheb = [&](int n, double rr) {
-    const double x = 2.0 * (rr - ri) / (ro - ri) - 1.0;
-    double dx;
-    if (std::fabs(std::fabs(x) - 1.0) < 1e-12) {
-      dx = (double)n * n * std::pow(x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0), n + 1);
-    } else {
-      const double th = std::acos(x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x));
-      dx = n * std::sin(n * th) / std::sin(th);
+  // one set per segment length (variant), on its own nodes and D1, copied to
+  // every segment of that length
+  const int KL = h->d.kl, NB = 2 * GD_MAX_KL + 1, nseg = h->d.nseg;
+  std::vector<double> all(4 * (size_t)h->d.nr, 0.0), cons(6 * (size_t)nseg, 0.0);
+  for (size_t v = 0; v < h->var_n.size(); ++v) {
+    const int N = h->var_n[v];
+    std::vector<double> r(N), d1((size_t)NB * N);
+    CK(cudaMemcpyAsync(r.data(), h->d_r + h->var_rep[v], sizeof(double) * N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(d1.data(), h->d_d1 + h->var_band[v], sizeof(double) * NB * N, cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const double ri = r[0], ro = r[N - 1];
+    auto cheb = [&](int n, double rr) {
+      double x = 2.0 * (rr - ri) / (ro - ri) - 1.0;
+      x = x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x);
+      return std::cos(n * std::acos(x));
+    };
+    auto dcheb = [&](int n, double rr) {
+      const double x = 2.0 * (rr - ri) / (ro - ri) - 1.0;
+      double dx;
+      if (std::fabs(std::fabs(x) - 1.0) < 1e-12) {
+        dx = (double)n * n * std::pow(x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0), n + 1);
+      } else {
+        const double th = std::acos(x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x));
+        dx = n * std::sin(n * th) / std::sin(th);
+      }
+      return dx * (2.0 / (ro - ri));
+    };
+    std::vector<double> t(4 * (size_t)N);
+    double* t1 = t.data();
+    double* t2 = t1 + N;
+    double* tin = t2 + N;
+    double* tout = tin + N;
+    for (int i = 0; i < N; ++i) { t1[i] = cheb(N - 1, r[i]); t2[i] = cheb(N, r[i]); }
+    const double dt1i = dcheb(N - 1, ri), dt1o = dcheb(N - 1, ro);
+    const double dt2i = dcheb(N, ri), dt2o = dcheb(N, ro);
+    const double alpha = std::fabs(dt2o) > 1e-12 ? dt1o / dt2o : 0.0;
+    const double beta = std::fabs(dt2i) > 1e-12 ? dt1i / dt2i : 0.0;
+    for (int i = 0; i < N; ++i) { tin[i] = t1[i] - alpha * t2[i]; tout[i] = t1[i] - beta * t2[i]; }
+    // rows 0 and N - 1 of D1 (entry (i, col) at d1[(i - col + KL) + NB col])
+    double din = 0.0, dout = 0.0;
+    for (int col = 0; col <= KL && col < N; ++col) din += d1[(size_t)(0 - col + KL) + (size_t)NB * col] * tin[col];
+    for (int col = std::max(0, N - 1 - KL); col < N; ++col)
+      dout += d1[(size_t)(N - 1 - col + KL) + (size_t)NB * col] * tout[col];
+    for (int z = 0; z < nseg; ++z) {
+      if (h->seg_var[z] != (int)v) continue;
+      std::copy(t.begin(), t.end(), all.begin() + 4 * (size_t)h->seg_base[z]);
+      const double k[6] = {dt1i, dt1o, dt2i, dt2o, din, dout};
+      std::copy(k, k + 6, cons.begin() + 6 * (size_t)z);
     }
-    return dx * (2.0 / (ro - ri));
-  };
-  std::vector<double> t(4 * (size_t)N);
-  double* t1 = t.data();
-  double* t2 = t1 + N;
-  double* tin = t2 + N;
-  double* tout = tin + N;
-  for (int i = 0; i < N; ++i) { t1[i] = cheb(N - 1, r[i]); t2[i] = cheb(N, r[i]); }
-  TauConsts& tc = h->tau;
-  tc.dt1i = dcheb(N - 1, ri); tc.dt1o = dcheb(N - 1, ro);
-  tc.dt2i = dcheb(N, ri); tc.dt2o = dcheb(N, ro);
-  const double alpha = std::fabs(tc.dt2o) > 1e-12 ? tc.dt1o / tc.dt2o : 0.0;
-  const double beta = std::fabs(tc.dt2i) > 1e-12 ? tc.dt1i / tc.dt2i : 0.0;
-  for (int i = 0; i < N; ++i) { tin[i] = t1[i] - alpha * t2[i]; tout[i] = t1[i] - beta * t2[i]; }
-  // rows 0 and N - 1 of D1 (entry (i, col) at d1[(i - col + KL) + NB col])
-  tc.din = 0.0;
-  tc.dout = 0.0;
-  for (int col = 0; col <= KL && col < N; ++col) tc.din += d1[(size_t)(0 - col + KL) + (size_t)NB * col] * tin[col];
-  for (int col = std::max(0, N - 1 - KL); col < N; ++col)
-    tc.dout += d1[(size_t)(N - 1 - col + KL) + (size_t)NB * col] * tout[col];
-  CK(cudaMemcpyAsync(h->d_tau, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(cudaMemcpyAsync(h->d_tau, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_tauc, cons.data(), sizeof(double) * cons.size(), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  tc.tau1 = h->d_tau;
-  tc.tau2 = h->d_tau + N;
-  tc.tau_in = h->d_tau + 2 * N;
-  tc.tau_out = h->d_tau + 3 * N;
+  h->tau.tau = h->d_tau;
+  h->tau.consts = h->d_tauc;
   return GD_OK;
 }
 
@@ -265,6 +274,7 @@ int setup(gd_handle* h) {
   AL(h->d_work, NWORK * h->spec_elems());
   AL(h->d_bvals, 2 * NL); AL(h->d_sources, NR);
   AL(h->d_cbvals, 2 * NL); AL(h->d_csources, NR); AL(h->d_bctype, 4 * NL); AL(h->d_tau, 4 * NR);
+  AL(h->d_tauc, 6 * (size_t)d.nseg);
   AL(h->d_grid, NGRID * h->grid_elems());
   AL(h->d_F, (size_t)4 * NR * (d.M + 1) * d.nlat);
   AL(h->d_epart, 2 * GD_ENERGY_BLOCKS * d.nseg); AL(h->d_eout, 2 * d.nseg);
@@ -1200,9 +1210,6 @@ int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int*
   for (size_t q = 0; q < NL; ++q) inner_flux |= inner[q] == GD_BC_FLUX;
   if (inner_flux && h->d.ball)
     return fail(h, GD_ERR_UNSUPPORTED, "a ball has no inner boundary: its centre row is the regularity condition");
-  if (flux && h->var_n.size() > 1 && h->c.bc_mode != 2)
-    return fail(h, GD_ERR_UNSUPPORTED,
-                "tau flux boundaries need segments of one length (one set of tau functions); bc_mode 2 takes them");
   if (flux && h->c.bc_mode == 2 && !h->flux_rows_ok)
     return fail(h, GD_ERR_SINGULAR, "the implicit factorisation with flux boundary rows has a zero pivot");
   CK(cudaSetDevice(h->device));

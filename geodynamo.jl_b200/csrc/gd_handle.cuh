@@ -73,6 +73,7 @@ struct gd_handle {
   void* t_final = nullptr;
   int t_nsteps = 0, t_every = 0;
   long t_s0 = 0;
+  double* d_tauc = nullptr;   // per segment: the six tau constants
   double* d_tau = nullptr;    // tau1, tau2, tau_in, tau_out on the radial nodes
   gd::TauConsts tau{};
   double* d_grid = nullptr;   // NGRID grids (FP64)

@@ -151,13 +151,14 @@ void launch_curl(cudaStream_t s, const Dims& d, const int* lof, const double* ri
                  double* opol);
 // Tau functions of the flux boundary conditions (apply_flux_bc_tau!,
 // src/scalar_field_common.jl:629-812) on the radial nodes.
+// Tau functions of every segment, on its own N nodes, at 4 base of `tau`:
+// tau1 = T_{N-1}(x(r)), tau2 = T_N(x(r)), tau_in = tau1 - alpha tau2 (zero
+// analytic derivative at ro), tau_out = tau1 - beta tau2 (zero at ri); and its
+// constants at 6 z of `consts`: the analytic dT_{N-1}/dr, dT_N/dr at ri and ro
+// (dt1i, dt1o, dt2i, dt2o), (D1 tau_in)[ri], (D1 tau_out)[ro].
 struct TauConsts {
-  const double* tau1;     // T_{N-1}(x(r)), Chebyshev polynomial on the nodes
-  const double* tau2;     // T_N(x(r))
-  const double* tau_in;   // tau1 - alpha tau2 (zero analytic derivative at ro)
-  const double* tau_out;  // tau1 - beta tau2 (zero analytic derivative at ri)
-  double dt1i, dt1o, dt2i, dt2o;  // analytic dT_{N-1}/dr, dT_N/dr at ri and ro
-  double din, dout;               // (D1 tau_in)[ri], (D1 tau_out)[ro]
+  const double* tau;
+  const double* consts;
 };
 // Boundary conditions of a scalar field for the modes [jlo, jhi): fixed-value
 // rows, then the tau correction of the modes with a flux boundary.

@@ -314,8 +314,7 @@ __global__ void k_scalar_bc(Dims d, const int* __restrict__ lof, const double* _
                             double* __restrict__ F, int op_rows) {
   const int j = d.jlo + blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= d.jhi) return;
-  // segment blockIdx.y: its own boundary rows and radial profile (flux rows
-  // only with one operator variant: the tau functions are of variant 0)
+  // segment blockIdx.y: its own boundary rows, radial profile and tau functions
   const SegView sv = seg_view(d, blockIdx.y);
   const int N = sv.n, KL = d.kl, NB = 2 * GD_MAX_KL + 1;
   const size_t NM = d.nlm, plane = (size_t)d.nr * NM;
@@ -344,20 +343,23 @@ __global__ void k_scalar_bc(Dims d, const int* __restrict__ lof, const double* _
     qo += d1[(N - 1 - col + KL) + NB * col] * re[(size_t)col * NM];
   const double ei = fi ? bv[j] - qi : 0.0, eo = fo ? bv[NM + j] - qo : 0.0;
   double c1 = 0.0, c2 = 0.0;
-  const double *t1 = tc.tau1, *t2 = tc.tau2;
+  const double* tb = tc.tau + 4 * (size_t)sv.base;
+  const double* kc = tc.consts + 6 * (size_t)blockIdx.y;
+  const double dt1i = kc[0], dt1o = kc[1], dt2i = kc[2], dt2o = kc[3], din = kc[4], dout = kc[5];
+  const double *t1 = tb, *t2 = tb + N;
   if (fi && fo) {  // compute_tau_coefficients_both
-    const double det = tc.dt1i * tc.dt2o - tc.dt1o * tc.dt2i;
+    const double det = dt1i * dt2o - dt1o * dt2i;
     if (fabs(det) > 1e-12) {
-      c1 = (ei * tc.dt2o - eo * tc.dt2i) / det;
-      c2 = (eo * tc.dt1i - ei * tc.dt1o) / det;
+      c1 = (ei * dt2o - eo * dt2i) / det;
+      c2 = (eo * dt1i - ei * dt1o) / det;
     }
   } else if (fi) {  // compute_tau_coefficients_inner
-    c1 = ei / tc.din;
-    t1 = tc.tau_in;
+    c1 = ei / din;
+    t1 = tb + 2 * N;
     t2 = nullptr;
   } else {          // compute_tau_coefficients_outer
-    c1 = eo / tc.dout;
-    t1 = tc.tau_out;
+    c1 = eo / dout;
+    t1 = tb + 3 * N;
     t2 = nullptr;
   }
   bool im_live = false;

@@ -122,8 +122,8 @@ enum { GD_GEOM_SHELL = 0, GD_GEOM_BALL = 1 };
  * (GD_ERR_UNSUPPORTED).  Boundary values and types apply to every segment;
  * heat sources are given per shell.  0 or 1: one shell.  segment_nr (read at
  * creation only) gives segments of unequal length, each with the radial grid
- * and operators of its own level count; tau flux boundaries (bc_mode 0/1)
- * then are refused, flux rows (bc_mode 2) are built per segment length.
+ * and operators of its own level count (tau functions and flux-row factors
+ * included, so flux boundaries work in every bc_mode).
  * geometry GD_GEOM_BALL is the solid sphere of GeoDynamoBall
  * (src/Ball/Ball.jl): cosine nodes on [0, r_outer] (r_outer = d_R_outer,
  * rratio unused), the angular gradient and both curl components 0 at r = 0
@@ -215,8 +215,7 @@ int gd_set_composition_bc(gd_handle* h, const double* bvals, const double* sourc
  * bc_mode 2 (boundary rows in the implicit operator) a flux mode's boundary
  * row is the row of D1 instead of the identity, its right-hand side the
  * prescribed flux; the tau correction is then not applied.  GD_ERR_UNSUPPORTED:
- * a flux type on segments of unequal length under bc_mode 0/1 (the tau
- * functions take one length), or at a ball's centre;
+ * an inner flux type on a ball (its centre row is the regularity condition);
  * GD_ERR_SINGULAR: a zero pivot in the bc_mode 2 factors with flux rows. */
 int gd_set_scalar_bc_types(gd_handle* h, int field, const int* inner, const int* outer);
 

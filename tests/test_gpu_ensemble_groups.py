@@ -180,9 +180,9 @@ def test_segments_keep_their_own_boundary_rows(gdb, bc_mode):
 def test_unequal_segments_equal_single_handles(gdb, bc_mode, precision):
     # members of 9, 13 and 9 levels on one handle (two operator variants):
     # boundary values, per-shell sources, clamped rows (bc_mode 1) and
-    # Dirichlet rows (bc_mode 2) at each segment's own ends; under bc_mode 2
-    # flux rows too (factors per segment length), while the tau flux
-    # correction (bc_mode 0/1) needs one segment length and is refused
+    # Dirichlet rows (bc_mode 2) at each segment's own ends, and random flux
+    # boundaries: the tau correction (bc_mode 0/1) with each segment's own tau
+    # functions, flux rows (bc_mode 2) with factors per segment length
     lmax, nlat, nlon = 15, 24, 48
     nrs = (9, 13, 9)
     members = [dict(lmax=lmax, nlat=nlat, nlon=nlon, nr=n, ekman=e, bc_mode=bc_mode, dt=2e-6, precision=precision)
@@ -196,17 +196,12 @@ def test_unequal_segments_equal_single_handles(gdb, bc_mode, precision):
     h.set_temperature_bc(bv, np.concatenate(srcs))
     inner = np.where(rng.random(h.nlm) < 0.5, 1, 2)
     outer = np.where(rng.random(h.nlm) < 0.5, 1, 2)
-    if bc_mode != 2:
-        with pytest.raises(gdb.GeoDynamoError):
-            h.set_bc_types("temp", inner, outer)
-    else:
-        h.set_bc_types("temp", inner, outer)
+    h.set_bc_types("temp", inner, outer)
     singles = []
     for i, (c, m) in enumerate(zip(members, ens.members)):
         kw = {k: v for k, v in c.items() if k not in ("lmax", "nlat", "nlon", "nr")}
         s = gdb.SHTnsKitConfig(lmax, nlat, nlon, c["nr"], **kw)
-        if bc_mode == 2:
-            s.set_bc_types("temp", inner, outer)
+        s.set_bc_types("temp", inner, outer)
         s.set_temperature_bc(bv, srcs[i])
         for k, (a, b) in workloads.seeded_state(lmax, lmax, c["nr"], seed=30 + i, amp=1e-1).items():
             m.set_field(k, a, b)
