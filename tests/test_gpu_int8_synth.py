@@ -94,3 +94,20 @@ def test_int8_stage_refusals(gdb):
     g.set_fp64_stages(I8)
     g.step(1)
     g.check_finite()
+
+
+@pytest.mark.parametrize("scheme", ["eab2", "erk2"])
+def test_exponential_schemes_with_int8_synthesis(gdb, scheme):
+    # the exponential schemes call the same velocity phase: with the int8
+    # synthesis their velocity follows the FP64 chain's run of the same scheme
+    lmax, nlat, nlon, nr = 15, 24, 48, 12
+    ref, i8 = pair(gdb, (lmax, nlat, nlon, nr), 6, seed=5, dt=1e-5)
+    for g in (ref, i8):
+        g.set_scheme(scheme)
+        g.step(3)
+        g.check_finite()
+    for k in ("u_tor", "u_pol"):
+        for x, y in zip(i8.get_field(k), ref.get_field(k)):
+            assert rel(x, y) < 1e-10, (scheme, k)
+    ref.close()
+    i8.close()
