@@ -913,9 +913,13 @@ int gd_set_fp64_stages(gd_handle* h, int mask) {
   if ((mask & GD_STAGE_VEL_SYNTH_I8) && !oz_supported(h->d))
     return fail(h, GD_ERR_UNSUPPORTED, "the int8-slice synthesis takes one shell range (no segments, no ball) and lmax <= 511");
   CK(cudaSetDevice(h->device));
+  // the slice images first: the mask changes only once they exist
+  if ((mask & GD_STAGE_VEL_SYNTH_I8) && h->mixed) {
+    const int s = mixed_prepare_int8(h);
+    if (s) return s;
+  }
   if (mask != h->fp64_stages) drop_graphs(h);
   h->fp64_stages = mask;
-  if ((mask & GD_STAGE_VEL_SYNTH_I8) && h->mixed) return mixed_prepare_int8(h);
   return GD_OK;
 }
 

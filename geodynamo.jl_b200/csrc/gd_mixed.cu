@@ -357,12 +357,19 @@ int mixed_prepare_int8(gd_handle* h) {
   if (!x) return GD_OK;
   if (x->oz_digits == h->int8_digits) return GD_OK;
   const Dims& d = h->d;
-  for (void* p : {(void*)x->oz_imgA, (void*)x->oz_imgB, (void*)x->oz_rs, (void*)x->oz_cs}) {
+  // the images of another digit count go first (and their pointers with them,
+  // so that a failed allocation below leaves nothing to free twice)
+  void** old[4] = {(void**)&x->oz_imgA, (void**)&x->oz_imgB, (void**)&x->oz_rs, (void**)&x->oz_cs};
+  const size_t old_bytes[4] = {x->oz.a_bytes, x->oz.b_bytes, sizeof(double) * x->oz.rs_elems,
+                               sizeof(double) * x->oz.cs_elems};
+  for (int i = 0; i < 4; ++i) {
+    void* p = *old[i];
     if (!p) continue;
     cudaFree(p);
     x->allocs.erase(std::find(x->allocs.begin(), x->allocs.end(), p));
+    x->bytes -= old_bytes[i];
+    *old[i] = nullptr;
   }
-  x->bytes -= x->oz.a_bytes + x->oz.b_bytes + sizeof(double) * (x->oz.rs_elems + x->oz.cs_elems);
   x->oz_digits = 0;
   x->oz = oz_layout(d, h->int8_digits);
   auto al = [&](size_t bytes, void** p) -> int {
@@ -505,6 +512,8 @@ int mixed_velocity_nl(gd_handle* h) {
   const size_t nfold = 2 * fc64;     // double2 of the two folded components
   int s;
   if (st & GD_STAGE_VEL_SYNTH_I8) {
+    if (x->oz_digits != h->int8_digits || !x->oz_imgA)
+      return set_error(h, GD_ERR_STATE, "the int8 slice images are not built (set-up failed)");
     OzSynthArgs a{};
     a.out = U64;
     a.out32 = x->F(FC_U);  // the FP32 copy the fused phase kernels read
