@@ -65,6 +65,17 @@ function handle_for(GD, config, nr::Integer; precision::Integer = 0, composition
     end
 end
 
+# The mixed-precision step's velocity chain at FP64 accuracy (gd_set_fp64_stages
+# with GD_STAGE_VEL_PRODUCTS | GD_STAGE_VEL_ANALYSIS and either the DMMA
+# synthesis, GD_STAGE_VEL_SYNTH = 1, or the int8-slice synthesis on the tensor
+# cores, GD_STAGE_VEL_SYNTH_I8 = 8, with `digits` 7-bit digits per operand).
+function velocity_chain_fp64!(h::Handle; int8::Bool = true, digits::Integer = 6)
+    int8 && check(h, ccall((:gd_set_int8_digits, LIB), Cint, (Ptr{Cvoid}, Cint), h.ptr, digits))
+    mask = (int8 ? 8 : 1) | 2 | 4
+    check(h, ccall((:gd_set_fp64_stages, LIB), Cint, (Ptr{Cvoid}, Cint), h.ptr, mask))
+    return h
+end
+
 # shtnskit_spectral_to_physical! (src/shtnskit_field_functions.jl:11)
 function spectral_to_physical!(h::Handle, spec, phys)
     re = parent(spec.data_real); im = parent(spec.data_imag); g = parent(phys.data)
