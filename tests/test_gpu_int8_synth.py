@@ -111,3 +111,21 @@ def test_exponential_schemes_with_int8_synthesis(gdb, scheme):
             assert rel(x, y) < 1e-10, (scheme, k)
     ref.close()
     i8.close()
+
+
+@pytest.mark.parametrize("lmax,mmax,nlat,nlon,nr", [(31, 20, 48, 96, 10), (511, 511, 768, 1536, 5)])
+def test_truncations_and_largest_lmax(gdb, lmax, mmax, nlat, nlon, nr):
+    # mmax < lmax (orders past mmax absent), and lmax = 511, the largest the
+    # int8 synthesis takes (eight 32-degree K steps per parity at m = 0)
+    ref = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, mmax=mmax, precision="mixed_vel64")
+    i8 = gdb.SHTnsKitConfig(lmax, nlat, nlon, nr, mmax=mmax, precision="mixed_vel64i8")
+    for k, (a, b) in workloads.seeded_state(lmax, mmax, nr, seed=9, amp=1e-1).items():
+        ref.set_field(k, a, b)
+        i8.set_field(k, a, b)
+    ref.velocity_nl()
+    i8.velocity_nl()
+    worst = max(rel(x, y) for k in ("u_tor", "u_pol") for x, y in zip(i8.get_nl(k), ref.get_nl(k)))
+    print(f"int8 synthesis, lmax {lmax} mmax {mmax}: velocity term {worst:.2e}")
+    assert worst < 1e-9
+    ref.close()
+    i8.close()
