@@ -576,9 +576,10 @@ int gd_get_launch_shape(const gd_handle* h, int* tc_ctas);
  * ("wait expired"); the flag is then cleared, so the handle's next calls run
  * normally.  To test that path without a GPU fault: wait_cycles bounds every
  * wait (clock cycles; <= 0 restores the default of about a second) and
- * omit_step >= 0 makes the next tensor-core synthesis on this handle skip the
- * bulk copies of that pipeline step in its first CTA (once), so the waits on
- * that stage run out.  GD_ERR_STATE without mixed-precision state. */
+ * omit_step >= 0 makes the next tensor-core synthesis on this handle (the
+ * split-TF32 one, or the int8-slice synthesis of u when GD_STAGE_VEL_SYNTH_I8
+ * is set and a velocity phase comes first) skip the bulk copies of that
+ * pipeline step in its first CTA (once), so the waits on that stage run out.  GD_ERR_STATE without mixed-precision state. */
 int gd_set_fault_test(gd_handle* h, long long wait_cycles, int omit_step);
 
 /* ---- tracing ------------------------------------------------------------------
