@@ -4,8 +4,8 @@
 //
 // Splitting.  Every operand value x is scaled by a power of two (one exponent
 // e per table row, one per coefficient column, both over the degrees of both
-// parities, with |x| < 2^e) and rounded to the integer X = rint(x 2^(7G-1-e)), which is
-// written as G signed digits in balanced base 128,
+// parities, with |x| < 2^e) and rounded to the integer X = rint(x 2^(7G-1-e)),
+// which is written as G signed digits in balanced base 128,
 //   X = sum_{i<G} d_i 128^(G-1-i),  d_0 in [-64, 64], d_i in [-64, 63],
 // so x = 2^e sum_i d_i 2^(-6-7i) + r with |r| <= 2^(e-7G) (round to nearest:
 // unbiased).  A digit product d_i d'_j is exact in int32, and so is every sum
@@ -14,8 +14,9 @@
 // accumulator; groups g >= G are not formed.  The epilogue forms
 // sum_g acc_g 128^(G-1-g) exactly in int64 (|sum| < 2^58), combines the even
 // and odd parities exactly, converts once to FP64 and multiplies by the row
-// and column scales 2^(e_row - 12 - 7(G-1)) and 2^(e_col).  This is the error-free transformation
-// of Ozaki, Ogita, Oishi and Rump (Numer. Algorithms 59, 2012) on int8 digits
+// and column scales 2^(e_row - 12 - 7(G-1)) and 2^(e_col).  This is the
+// error-free transformation of Ozaki, Ogita, Oishi and Rump (Numer.
+// Algorithms 59, 2012) on int8 digits
 // with the product triangle cut at G groups; the error of one term is about
 // 2^(-7G) of (row max)(column max), against 2^-53 of |x y| in FP64.
 //
@@ -34,8 +35,8 @@
 // pipeline step is one 32-degree K step of one parity: the G table slices
 // and the G coefficient slices of that step (K-major, SWIZZLE_32B: 32-byte
 // rows, so a step copies exactly its degrees), and G MMAs: table digit i
-// against coefficient digits 0 .. G-1-i as one B operand of (G - i) N columns.  The
-// even-parity accumulators are drained while the odd-parity MMAs run and are
+// against coefficient digits 0 .. G-1-i as one B operand of (G - i) N
+// columns.  The even-parity accumulators are drained while the odd-parity MMAs run and are
 // free again for the next tile's even MMAs.  The dP and Q rows of one
 // colatitude sit in different TMEM lane quarters: their partial results meet
 // in shared memory.
